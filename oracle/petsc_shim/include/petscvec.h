@@ -1,0 +1,2 @@
+/* Forwards to the serial PETSc shim (test infrastructure only). */
+#include "petscshim.h"

@@ -1,0 +1,91 @@
+/*
+ * CPU restatement of the reference's compressible RHS + SSP-RK stage update.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker: tests/, the smoke entry
+ * point and the CPU-baseline leg of bench.py may call it; the product never
+ * links or calls it.
+ *
+ * Layout: every field is a separate plane (SoA) over the padded node box
+ * (mx+4) x (my+4) x (mz+4): node (i,j,k) of the reference's DMDA, with
+ * i in [-2, mx+1], lives at ((k+2)*(my+4) + (j+2))*(mx+4) + (i+2).  The two
+ * ghost layers of a periodic direction hold the DMDA wrap-around copies
+ * (index -1 -> mx-1, -2 -> mx-2, mx -> 0, mx+1 -> 1); those of a
+ * non-periodic direction are unused.
+ */
+#ifndef CB_ORACLE_H
+#define CB_ORACLE_H
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int mx, my, mz;          /* DMDA node counts including boundary nodes 0 and m-1 */
+  int bctype[6];           /* bcs.dat codes, 7 = periodic */
+  int les;                 /* -les: 0 off, 1 constant Smagorinsky */
+  int inviscid;            /* -inv */
+  int fluxorder;           /* -fluxorder: 1 first order, 2 MUSCL, 3 WENO3 */
+  int eno_order;           /* -ENOorder */
+  int central;             /* -central: 2 skew-symmetric, 3 Fp_1, other: 2-point */
+  int isothermal;          /* -isothermal */
+  double s_x, s_y, s_z;    /* -s_x/-s_y/-s_z hybrid weights */
+  double ren, ma, pr, gamma, dt, st;
+  double cs_const;         /* constant Smagorinsky coefficient (CS field value) */
+  double ci;               /* Yoshizawa constant CI */
+  double ratio;            /* channel forcing ratio (0 unless channel/wavy) */
+} cbo_config;
+
+/* Fill the two ghost layers of each periodic direction of one padded plane
+ * from the owned nodes by wrap-around (DMGlobalToLocal semantics). */
+void cbo_fill_ghosts(const cbo_config *c, double *f);
+
+/* FormMetrics: coordinates (3 padded planes) -> csi,eta,zet (3 planes each),
+ * aj (1 plane); ghost layers of periodic directions filled. */
+void cbo_metrics(const cbo_config *c, const double *const coor[3], double *const csi[3],
+                 double *const eta[3], double *const zet[3], double *aj);
+
+/* EqOfState on every node of the padded box. */
+void cbo_eos(const cbo_config *c, const double *const q[5], double *p);
+
+/* Hybrid weights field (3 planes) as formConvectionLES sets it at istage 0
+ * when the sensor is off. */
+void cbo_sigma(const cbo_config *c, double *const sig[3]);
+
+/* formRHS: q = ghosted stage state, nut/sig may be NULL when les == 0.
+ * rhs: 5 padded planes; interior nodes written, every other node zeroed. */
+int cbo_rhs(const cbo_config *c, const double *const q[5], const double *const csi[3],
+            const double *const eta[3], const double *const zet[3], const double *aj,
+            const double *nvert, const double *nut, const double *const sig[3],
+            double *const rhs[5]);
+
+/* Compute_eddy_viscosity_LES: u from the ghosted state qu (NULL: zero
+ * velocity, as before the first CalcUCat), nut written on interior nodes,
+ * boundary nodes untouched, then ghost layers refreshed. */
+void cbo_eddy_viscosity(const cbo_config *c, const double *const qu[5], const double *const csi[3],
+                        const double *const eta[3], const double *const zet[3], const double *aj,
+                        const double *nvert, double *nut);
+
+/* One SSP-RK stage update on every node: qout = combination of qold, qin, rhs. */
+void cbo_rk_combine(const cbo_config *c, int istage, const double *const qold[5],
+                    const double *const qin[5], const double *const rhs[5], double *const qout[5]);
+
+/* FormBCS periodic part: boundary nodes of qout from the stale ghosted stage
+ * input qin, then DMGlobalToLocal of qout. */
+int cbo_bc_periodic(const cbo_config *c, const double *const qin[5], double *const qout[5]);
+
+/* Full time steps (Flow_Solver + main loop): q (ghosted, in/out), qold,
+ * quc (ghosted state of the last CalcUCat; in/out), have_uc (in/out flag),
+ * nut (in/out).  Scratch buffers are allocated inside. */
+int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const qold[5],
+              double *const quc[5], int *have_uc, double *nut, const double *const csi[3],
+              const double *const eta[3], const double *const zet[3], const double *aj,
+              const double *nvert);
+
+/* Number of RK stages the reference runs for this config (= fluxorder). */
+int cbo_nstages(const cbo_config *c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
