@@ -1,0 +1,84 @@
+"""ctypes binding of libchimera_b200.so (the C-ABI in include/chimera_b200.h).
+
+The library is loaded from the package directory only.  A missing library is
+an error: there is no CPU fallback for the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libchimera_b200.so")
+
+CB_OK, CB_E_ARG, CB_E_CUDA, CB_E_STATE, CB_E_NONFINITE, CB_E_UNSUPPORTED = 0, 1, 2, 3, 4, 5
+CB_FP64, CB_MIXED = 0, 1
+
+
+class CbConfig(C.Structure):
+    _fields_ = [
+        ("mx", C.c_int), ("my", C.c_int), ("mz", C.c_int), ("bctype", C.c_int * 6),
+        ("les", C.c_int), ("inviscid", C.c_int), ("fluxorder", C.c_int), ("eno_order", C.c_int),
+        ("central", C.c_int), ("isothermal", C.c_int),
+        ("s_x", C.c_double), ("s_y", C.c_double), ("s_z", C.c_double),
+        ("ren", C.c_double), ("ma", C.c_double), ("pr", C.c_double), ("gamma", C.c_double),
+        ("dt", C.c_double), ("st", C.c_double), ("cs_const", C.c_double), ("ci", C.c_double),
+        ("ratio", C.c_double), ("precision", C.c_int), ("device", C.c_int),
+    ]
+
+
+_lib = None
+
+
+class ChimeraError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"chimera_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m chimera_comp_les_b200.build` "
+            "(nvcc, sm_100a); the product has no CPU fallback")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    lib.cb_abi_version.restype = C.c_int
+    lib.cb_config_default.argtypes = [C.POINTER(CbConfig), C.c_int, C.c_int, C.c_int]
+    lib.cb_create.argtypes = [C.POINTER(CbConfig), C.POINTER(P)]
+    lib.cb_destroy.argtypes = [P]
+    lib.cb_destroy.restype = None
+    for name, args in [
+        ("cb_set_grid", [P, D]), ("cb_set_metrics", [P, D, D, D, D]), ("cb_get_metrics", [P, D, D, D, D]), ("cb_set_nvert", [P, D]),
+        ("cb_upload_state", [P, D]), ("cb_download_state", [P, D, D]), ("cb_rhs", [P, C.c_int, D]),
+        ("cb_calc_ucat", [P]), ("cb_eddy_viscosity", [P]), ("cb_get_nut", [P, D]),
+        ("cb_rk_step", [P, C.c_int]), ("cb_sync", [P]), ("cb_capture_graph", [P]),
+        ("cb_timing_enable", [P, C.c_int]),
+        ("cb_timing_read", [P, D, C.POINTER(C.c_int), D, C.POINTER(C.c_int)]),
+    ]:
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    lib.cb_stream.argtypes = [P]
+    lib.cb_stream.restype = P
+    lib.cb_interior_nodes.argtypes = [P]
+    lib.cb_interior_nodes.restype = C.c_longlong
+    lib.cb_stages.argtypes = [P]
+    lib.cb_stages.restype = C.c_int
+    lib.cb_launches_per_step.argtypes = [P]
+    lib.cb_launches_per_step.restype = C.c_int
+    lib.cb_last_error.argtypes = [P]
+    lib.cb_last_error.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+def dptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_double))

@@ -1,0 +1,623 @@
+// C-ABI of libchimera_b200.so (declared in include/chimera_b200.h).
+//
+// One context = one block of the reference's DMDA resident on one GPU:
+//   3 rotating state buffers (Q of the stage input, Q of the stage output and
+//   Qold never collide, so no Q -> Qold copy is ever made), metrics, nvert and
+//   nu_t, all as padded SoA planes in a single device allocation.
+// A time step enqueues: [eddy viscosity + its ghost fill] then per RK stage
+// [fused RHS/combine kernel, boundary + ghost fill kernel].  Steady-state
+// steps replay CUDA graphs keyed by the buffer rotation.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/chimera_b200.h"
+#include "cb_aux.cuh"
+#include "cb_common.cuh"
+#include "cb_stage.cuh"
+
+using namespace cb;
+
+namespace {
+
+constexpr int BX = 32, BY = 8;
+using TS = TileShape<BX, BY>;
+
+struct GraphSlot {
+  cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace
+
+struct cb_ctx {
+  cb_config cfg{};
+  DevCfg dc{};
+  int dev = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  double *arena = nullptr;
+  size_t plane = 0;
+  double *qb[3][5] = {};
+  double *met[3][3] = {};
+  double *aj = nullptr, *nvert = nullptr, *nut = nullptr;
+  double *rhsb[5] = {};
+  double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
+  double **ptab = nullptr;    // device pointer tables
+  unsigned *status = nullptr;
+  int cur = 0;                // buffer with the current Q (== Qold between steps)
+  int uc = -1;                // buffer of the last CalcUCat state, -1: none
+  bool have_grid = false, have_state = false;
+  int kchunk = 16;
+  GraphSlot graphs[3][4];
+  bool use_graphs = true;
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_pairs_rhs, ev_pairs_other;
+  double acc_rhs_ms = 0, acc_other_ms = 0;
+  int acc_rhs_n = 0, acc_other_n = 0;
+  std::string err;
+};
+
+static int fail(cb_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CB_CUDA(ctx, call)                                                                  \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(ctx, CB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+// device pointer tables inside ctx->ptab
+enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27, PT_NUT = 32, PT_MISC = 33, PT_N = 48 };
+
+static int grid_for(const cb_ctx *c, long long work, int block = 256) {
+  long long b = (work + block - 1) / block;
+  long long cap = (long long)c->sms * 8;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
+  DevFields F{};
+  for (int q = 0; q < 5; q++) {
+    F.q[q] = c->qb[in][q];
+    F.qold[q] = c->qb[old][q];
+    F.qout[q] = out >= 0 ? c->qb[out][q] : nullptr;
+    F.rhs[q] = c->rhsb[q];
+  }
+  for (int e = 0; e < 3; e++)
+    for (int q = 0; q < 3; q++) F.met[e][q] = c->met[e][q];
+  F.aj = c->aj;
+  F.nvert = c->nvert;
+  F.nut = c->nut;
+  F.status = c->status;
+  return F;
+}
+
+template <bool LES, bool VISC, bool RHSM>
+static cudaError_t set_stage_attr() {
+  return cudaFuncSetAttribute(stage_kernel<LES, VISC, RHSM, BX, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)TS::smem_bytes);
+}
+
+// Opt every stage-kernel variant into its dynamic shared memory on the
+// current device (done at context creation, never during graph capture).
+static cudaError_t set_stage_attrs() {
+  cudaError_t e;
+  if ((e = set_stage_attr<true, true, false>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<true, false, false>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<false, true, false>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<false, false, false>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<true, true, true>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<true, false, true>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<false, true, true>()) != cudaSuccess) return e;
+  return set_stage_attr<false, false, true>();
+}
+
+template <bool LES, bool VISC, bool RHSM>
+static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt) {
+  auto kern = stage_kernel<LES, VISC, RHSM, BX, BY>;
+  const int nkin = c->dc.mz - 2;
+  dim3 grid((c->dc.mx - 2 + BX - 1) / BX, (c->dc.my - 2 + BY - 1) / BY, (nkin + c->kchunk - 1) / c->kchunk);
+  dim3 block(BX, BY);
+  kern<<<grid, block, TS::smem_bytes, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_stage(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt, bool rhs_mode) {
+  const bool les = c->cfg.les != 0, visc = c->cfg.inviscid == 0;
+  if (rhs_mode) {
+    if (les && visc) return launch_stage_t<true, true, true>(c, F, istage, alfa, beta, adt);
+    if (les) return launch_stage_t<true, false, true>(c, F, istage, alfa, beta, adt);
+    if (visc) return launch_stage_t<false, true, true>(c, F, istage, alfa, beta, adt);
+    return launch_stage_t<false, false, true>(c, F, istage, alfa, beta, adt);
+  }
+  if (les && visc) return launch_stage_t<true, true, false>(c, F, istage, alfa, beta, adt);
+  if (les) return launch_stage_t<true, false, false>(c, F, istage, alfa, beta, adt);
+  if (visc) return launch_stage_t<false, true, false>(c, F, istage, alfa, beta, adt);
+  return launch_stage_t<false, false, false>(c, F, istage, alfa, beta, adt);
+}
+
+static cudaEvent_t ev_get(cb_ctx *c, int idx) {
+  while ((int)c->ev_pool.size() <= idx) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->ev_pool.push_back(e);
+  }
+  return c->ev_pool[idx];
+}
+
+// timing helpers: record a pair of events around a launch
+struct TimedScope {
+  cb_ctx *c;
+  bool rhs;
+  int a = -1;
+  TimedScope(cb_ctx *ctx, bool is_rhs) : c(ctx), rhs(is_rhs) {
+    if (!c->timing) return;
+    a = (int)(c->ev_pairs_rhs.size() + c->ev_pairs_other.size()) * 2;
+    cudaEventRecord(ev_get(c, a), c->stream);
+  }
+  ~TimedScope() {
+    if (!c->timing) return;
+    cudaEventRecord(ev_get(c, a + 1), c->stream);
+    (rhs ? c->ev_pairs_rhs : c->ev_pairs_other).push_back({a, a + 1});
+  }
+};
+
+static void harvest_timing(cb_ctx *c) {
+  if (c->ev_pairs_rhs.empty() && c->ev_pairs_other.empty()) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto &p : c->ev_pairs_rhs) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev_pool[p.first], c->ev_pool[p.second]);
+    c->acc_rhs_ms += ms;
+    c->acc_rhs_n++;
+  }
+  for (auto &p : c->ev_pairs_other) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev_pool[p.first], c->ev_pool[p.second]);
+    c->acc_other_ms += ms;
+    c->acc_other_n++;
+  }
+  c->ev_pairs_rhs.clear();
+  c->ev_pairs_other.clear();
+}
+
+static int nut_update(cb_ctx *c) {
+  // Compute_eddy_viscosity_LES from the recorded state (or zero velocity).
+  const long long work = (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2);
+  {
+    TimedScope ts(c, false);
+    eddy_viscosity_kernel<<<grid_for(c, work), 256, 0, c->stream>>>(
+        c->dc, c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr,
+        (const double *const *)(c->ptab + PT_MET), c->aj, c->nvert, c->nut);
+  }
+  {
+    TimedScope ts(c, false);
+    const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
+    ghost_fill_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->ptab + PT_NUT, 1);
+  }
+  CB_CUDA(c, cudaGetLastError());
+  return CB_OK;
+}
+
+static void rk_coeffs(const cb_ctx *c, int s, double *alfa, double *beta) {
+  double a[3] = {1., 1 / 4., 2 / 3.}, b[3] = {1., 3 / 4., 1 / 3.};  // solvers.c:233-234
+  if (c->cfg.fluxorder < 3) { a[1] = 1 / 2.; b[1] = 1 / 2.; }       // solvers.c:239-241
+  *alfa = a[s];
+  *beta = b[s];
+}
+
+// Enqueue one time step (no graph).
+static int enqueue_step(cb_ctx *c) {
+  if (c->cfg.les && !c->cfg.inviscid) {
+    int e = nut_update(c);
+    if (e) return e;
+  }
+  const int ns = c->cfg.fluxorder;
+  const int old = c->cur;
+  const int A = (c->cur + 1) % 3, B = (c->cur + 2) % 3;
+  int in = c->cur;
+  const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
+  for (int s = 0; s < ns; s++) {
+    const int out = (s % 2 == 0) ? A : B;
+    double alfa, beta;
+    rk_coeffs(c, s, &alfa, &beta);
+    const double adt = alfa * c->cfg.dt * c->cfg.st;
+    DevFields F = fields_for(c, in, old, out);
+    {
+      TimedScope ts(c, true);
+      CB_CUDA(c, launch_stage(c, F, s, alfa, beta, adt, false));
+    }
+    {
+      TimedScope ts(c, false);
+      bc_periodic_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, F);
+    }
+    CB_CUDA(c, cudaGetLastError());
+    if (!c->cfg.inviscid) c->uc = in;  // CalcUCat inside formRHS keeps the stage input
+    in = out;
+  }
+  c->cur = in;
+  return CB_OK;
+}
+
+static int fill_ptab(cb_ctx *c) {
+  double *h[PT_N] = {};
+  for (int b = 0; b < 3; b++)
+    for (int q = 0; q < 5; q++) h[5 * b + q] = c->qb[b][q];
+  for (int e = 0; e < 3; e++)
+    for (int q = 0; q < 3; q++) h[PT_MET + 3 * e + q] = c->met[e][q];
+  for (int q = 0; q < 5; q++) h[PT_RHS + q] = c->rhsb[q];
+  h[PT_NUT] = c->nut;
+  h[PT_MISC + 0] = c->aj;
+  h[PT_MISC + 1] = c->nvert;
+  for (int e = 0; e < 3; e++)
+    for (int q = 0; q < 3; q++) h[PT_MISC + 2 + 3 * e + q] = c->met[e][q];
+  h[PT_MISC + 11] = c->aj;
+  CB_CUDA(c, cudaMemcpyAsync(c->ptab, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+static void invalidate_graphs(cb_ctx *c) {
+  for (auto &row : c->graphs)
+    for (auto &g : row)
+      if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
+}
+
+extern "C" {
+
+int cb_abi_version(void) { return CB_ABI_VERSION; }
+
+void cb_config_default(cb_config *cfg, int mx, int my, int mz) {
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->mx = mx; cfg->my = my; cfg->mz = mz;
+  for (int b = 0; b < 6; b++) cfg->bctype[b] = 7;
+  cfg->les = 0; cfg->inviscid = 0; cfg->fluxorder = 3; cfg->eno_order = 2; cfg->central = 2; cfg->isothermal = 0;
+  cfg->s_x = cfg->s_y = cfg->s_z = 1.0;
+  cfg->ren = 3000.; cfg->ma = 2.81; cfg->pr = 0.72; cfg->gamma = 1.4; cfg->dt = 0.01; cfg->st = 1.;
+  cfg->cs_const = 0.03; cfg->ci = 0.06; cfg->ratio = 0.;
+  cfg->precision = CB_FP64;
+  cfg->device = 0;
+}
+
+int cb_create(const cb_config *cfg, cb_ctx **out) {
+  if (!cfg || !out) return CB_E_ARG;
+  *out = nullptr;
+  cb_ctx *c = new cb_ctx();
+  c->cfg = *cfg;
+  auto bail = [&](int code, const char *msg) {
+    fprintf(stderr, "chimera_b200: cb_create: %s\n", msg);
+    cb_destroy(c);
+    return code;
+  };
+  if (cfg->mx < 5 || cfg->my < 5 || cfg->mz < 5) return bail(CB_E_ARG, "grid must have at least 5 nodes per direction");
+  for (int b = 0; b < 6; b++)
+    if (cfg->bctype[b] != 7) return bail(CB_E_UNSUPPORTED, "only fully periodic blocks (bctype 7) are built");
+  if (cfg->fluxorder < 1 || cfg->fluxorder > 3) return bail(CB_E_ARG, "fluxorder must be 1, 2 or 3");
+  if (cfg->eno_order != 2 && cfg->eno_order != 3) return bail(CB_E_ARG, "ENOorder must be 2 or 3");
+  if (cfg->les != 0 && cfg->les != 1) return bail(CB_E_UNSUPPORTED, "only les 0 or 1 (constant Smagorinsky) is built");
+  if (cfg->precision != CB_FP64) return bail(CB_E_UNSUPPORTED, "precision form not built");
+  c->dev = cfg->device;
+  if (cudaSetDevice(c->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice failed");
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(CB_E_CUDA, "stream");
+  if (set_stage_attrs() != cudaSuccess) return bail(CB_E_CUDA, "stage kernel shared-memory opt-in failed");
+  DevCfg &d = c->dc;
+  d.mx = cfg->mx; d.my = cfg->my; d.mz = cfg->mz;
+  d.px = ((cfg->mx + 4 + 15) / 16) * 16;
+  d.py = cfg->my + 4;
+  d.pz = cfg->mz + 4;
+  d.plane = (long long)d.px * d.py * d.pz;
+  for (int b = 0; b < 6; b++) d.bctype[b] = cfg->bctype[b];
+  d.les = cfg->les; d.inviscid = cfg->inviscid; d.fluxorder = cfg->fluxorder; d.eno_order = cfg->eno_order;
+  d.central = cfg->central; d.isothermal = cfg->isothermal;
+  d.s_x = cfg->s_x; d.s_y = cfg->s_y; d.s_z = cfg->s_z;
+  d.ren = cfg->ren; d.ma = cfg->ma; d.pr = cfg->pr; d.gamma = cfg->gamma; d.dt = cfg->dt; d.st = cfg->st;
+  d.cs_const = cfg->cs_const; d.ci = cfg->ci; d.ratio = cfg->ratio;
+  c->plane = (size_t)d.plane;
+  // planes: 15 state + 9 metrics + aj + nvert + nut = 27
+  const int nplanes = 27;
+  const size_t bytes = sizeof(double) * c->plane * nplanes;
+  if (cudaMalloc(&c->arena, bytes) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc arena");
+  if (cudaMemsetAsync(c->arena, 0, bytes, c->stream) != cudaSuccess) return bail(CB_E_CUDA, "memset");
+  int p = 0;
+  for (int b = 0; b < 3; b++)
+    for (int q = 0; q < 5; q++) c->qb[b][q] = c->arena + c->plane * (p++);
+  for (int e = 0; e < 3; e++)
+    for (int q = 0; q < 3; q++) c->met[e][q] = c->arena + c->plane * (p++);
+  c->aj = c->arena + c->plane * (p++);
+  c->nvert = c->arena + c->plane * (p++);
+  c->nut = c->arena + c->plane * (p++);
+  const size_t nn = (size_t)cfg->mx * cfg->my * cfg->mz;
+  if (cudaMalloc(&c->staging, sizeof(double) * 5 * nn) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc staging");
+  if (cudaMalloc(&c->ptab, sizeof(double *) * PT_N) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab");
+  if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc status");
+  cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream);
+  if (fill_ptab(c)) return bail(CB_E_CUDA, "pointer table");
+  // k-chunk: aim for a whole number of waves of one block per SM
+  {
+    const int tiles = ((cfg->mx - 2 + BX - 1) / BX) * ((cfg->my - 2 + BY - 1) / BY);
+    const int nk = cfg->mz - 2;
+    double best = 1e30;
+    for (int kc = 4; kc <= nk; kc++) {
+      const int chunks = (nk + kc - 1) / kc;
+      const long long blocks = (long long)tiles * chunks;
+      const long long waves = (blocks + c->sms - 1) / c->sms;
+      const double cost = (double)waves * (kc + 3.0);  // ~3 extra plane loads per chunk prologue
+      if (cost < best) { best = cost; c->kchunk = kc; }
+    }
+  }
+  *out = c;
+  return CB_OK;
+}
+
+void cb_destroy(cb_ctx *c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  invalidate_graphs(c);
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  if (c->rhsb[0]) cudaFree(c->rhsb[0]);
+  if (c->arena) cudaFree(c->arena);
+  if (c->staging) cudaFree(c->staging);
+  if (c->ptab) cudaFree(c->ptab);
+  if (c->status) cudaFree(c->status);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char *cb_last_error(const cb_ctx *c) { return c ? c->err.c_str() : "null context"; }
+void *cb_stream(cb_ctx *c) { return c ? (void *)c->stream : nullptr; }
+long long cb_interior_nodes(const cb_ctx *c) {
+  return c ? (long long)(c->cfg.mx - 2) * (c->cfg.my - 2) * (c->cfg.mz - 2) : 0;
+}
+int cb_stages(const cb_ctx *c) { return c ? c->cfg.fluxorder : 0; }
+int cb_launches_per_step(const cb_ctx *c) {
+  if (!c) return 0;
+  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + 2 * c->cfg.fluxorder;
+}
+
+static int upload_planes(cb_ctx *c, const double *host, int nc, int pt_first, bool pinned_hint) {
+  (void)pinned_hint;
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  CB_CUDA(c, cudaMemcpyAsync(c->staging, host, sizeof(double) * nc * nn, cudaMemcpyHostToDevice, c->stream));
+  unpack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, c->staging, nc, c->ptab + pt_first);
+  CB_CUDA(c, cudaGetLastError());
+  const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
+  ghost_fill_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->ptab + pt_first, nc);
+  CB_CUDA(c, cudaGetLastError());
+  return CB_OK;
+}
+
+int cb_set_grid(cb_ctx *c, const double *coor) {
+  if (!c || !coor) return CB_E_ARG;
+  // coordinates go into state buffer 2 temporarily (overwritten by uploads/steps)
+  double *X[3] = {c->qb[2][0], c->qb[2][1], c->qb[2][2]};
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  CB_CUDA(c, cudaMemcpyAsync(c->staging, coor, sizeof(double) * 3 * nn, cudaMemcpyHostToDevice, c->stream));
+  unpack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, c->staging, 3, c->ptab + PT_Q2);
+  const long long work = (long long)nn;
+  metrics_interior_kernel<<<grid_for(c, work), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_Q2),
+                                                                      c->ptab + PT_MET, c->aj);
+  for (int f = 0; f < 6; f++)
+    metrics_boundary_kernel<<<grid_for(c, work / 4 + 1), 256, 0, c->stream>>>(c->dc, c->ptab + PT_MET, c->aj, f);
+  const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
+  ghost_fill_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->ptab + PT_MISC + 2, 10);
+  CB_CUDA(c, cudaGetLastError());
+  // scrub buffer 2 (coordinates) so later ghost reads see zeros until written
+  for (int q = 0; q < 3; q++) CB_CUDA(c, cudaMemsetAsync(X[q], 0, sizeof(double) * c->plane, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->have_grid = true;
+  invalidate_graphs(c);
+  return CB_OK;
+}
+
+int cb_set_metrics(cb_ctx *c, const double *csi, const double *eta, const double *zet, const double *aj) {
+  if (!c || !csi || !eta || !zet || !aj) return CB_E_ARG;
+  int e;
+  if ((e = upload_planes(c, csi, 3, PT_MET + 0, false))) return e;
+  if ((e = upload_planes(c, eta, 3, PT_MET + 3, false))) return e;
+  if ((e = upload_planes(c, zet, 3, PT_MET + 6, false))) return e;
+  if ((e = upload_planes(c, aj, 1, PT_MISC + 0, false))) return e;
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->have_grid = true;
+  invalidate_graphs(c);
+  return CB_OK;
+}
+
+int cb_get_metrics(cb_ctx *c, double *csi, double *eta, double *zet, double *aj) {
+  if (!c || !csi || !eta || !zet || !aj) return CB_E_ARG;
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  double *outs[4] = {csi, eta, zet, aj};
+  const int firsts[4] = {PT_MET + 0, PT_MET + 3, PT_MET + 6, PT_MISC + 0};
+  const int ncs[4] = {3, 3, 3, 1};
+  for (int f = 0; f < 4; f++) {
+    pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + firsts[f]),
+                                                                     ncs[f], c->staging);
+    CB_CUDA(c, cudaGetLastError());
+    CB_CUDA(c, cudaMemcpyAsync(outs[f], c->staging, sizeof(double) * ncs[f] * nn, cudaMemcpyDeviceToHost, c->stream));
+    CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  return CB_OK;
+}
+
+int cb_set_nvert(cb_ctx *c, const double *nvert) {
+  if (!c || !nvert) return CB_E_ARG;
+  int e = upload_planes(c, nvert, 1, PT_MISC + 1, false);
+  if (e) return e;
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_upload_state(cb_ctx *c, const double *q) {
+  if (!c || !q) return CB_E_ARG;
+  c->cur = 0;
+  c->uc = -1;
+  int e = upload_planes(c, q, 5, PT_Q0, false);
+  if (e) return e;
+  CB_CUDA(c, cudaMemsetAsync(c->nut, 0, sizeof(double) * c->plane, c->stream));
+  c->have_state = true;
+  return CB_OK;
+}
+
+int cb_download_state(cb_ctx *c, double *q, double *p) {
+  if (!c || !q) return CB_E_ARG;
+  if (!c->have_state) return fail(c, CB_E_STATE, "no state uploaded");
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), 5, c->staging);
+  CB_CUDA(c, cudaGetLastError());
+  CB_CUDA(c, cudaMemcpyAsync(q, c->staging, sizeof(double) * 5 * nn, cudaMemcpyDeviceToHost, c->stream));
+  if (p) {
+    CB_CUDA(c, cudaStreamSynchronize(c->stream));
+    eos_pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), c->staging);
+    CB_CUDA(c, cudaGetLastError());
+    CB_CUDA(c, cudaMemcpyAsync(p, c->staging, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_rhs(cb_ctx *c, int istage, double *rhs) {
+  if (!c || !rhs) return CB_E_ARG;
+  if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set before cb_rhs");
+  if (!c->rhsb[0]) {
+    double *b = nullptr;
+    CB_CUDA(c, cudaMalloc(&b, sizeof(double) * c->plane * 5));
+    CB_CUDA(c, cudaMemsetAsync(b, 0, sizeof(double) * c->plane * 5, c->stream));
+    for (int q = 0; q < 5; q++) c->rhsb[q] = b + c->plane * q;
+    int e = fill_ptab(c);
+    if (e) return e;
+  }
+  double alfa, beta;
+  rk_coeffs(c, istage < 0 ? 0 : (istage > 2 ? 2 : istage), &alfa, &beta);
+  DevFields F = fields_for(c, c->cur, c->cur, -1);
+  CB_CUDA(c, launch_stage(c, F, istage, alfa, beta, 0.0, true));
+  if (!c->cfg.inviscid) c->uc = c->cur;
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_RHS), 5, c->staging);
+  CB_CUDA(c, cudaGetLastError());
+  CB_CUDA(c, cudaMemcpyAsync(rhs, c->staging, sizeof(double) * 5 * nn, cudaMemcpyDeviceToHost, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_calc_ucat(cb_ctx *c) {
+  if (!c) return CB_E_ARG;
+  if (!c->have_state) return fail(c, CB_E_STATE, "no state");
+  c->uc = c->cur;
+  return CB_OK;
+}
+
+int cb_eddy_viscosity(cb_ctx *c) {
+  if (!c) return CB_E_ARG;
+  if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set");
+  if (!c->cfg.les) return fail(c, CB_E_ARG, "eddy viscosity needs les = 1");
+  int e = nut_update(c);
+  if (e) return e;
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_get_nut(cb_ctx *c, double *nut) {
+  if (!c || !nut) return CB_E_ARG;
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_NUT), 1, c->staging);
+  CB_CUDA(c, cudaGetLastError());
+  CB_CUDA(c, cudaMemcpyAsync(nut, c->staging, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_rk_step(cb_ctx *c, int nsteps) {
+  if (!c || nsteps < 0) return CB_E_ARG;
+  if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set before cb_rk_step");
+  for (int n = 0; n < nsteps; n++) {
+    const int ucslot = c->uc + 1;  // 0: none, 1..3: buffer
+    GraphSlot &g = c->graphs[c->cur][ucslot];
+    if (c->use_graphs && !c->timing && g.exec) {
+      const int ns = c->cfg.fluxorder;
+      CB_CUDA(c, cudaGraphLaunch(g.exec, c->stream));
+      // replay the bookkeeping of enqueue_step
+      const int A = (c->cur + 1) % 3, B = (c->cur + 2) % 3;
+      int in = c->cur;
+      for (int s = 0; s < ns; s++) {
+        const int out = (s % 2 == 0) ? A : B;
+        if (!c->cfg.inviscid) c->uc = in;
+        in = out;
+      }
+      c->cur = in;
+      continue;
+    }
+    if (c->use_graphs && !c->timing) {
+      // capture this rotation state once, then replay it
+      const int cur0 = c->cur, uc0 = c->uc;
+      cudaGraph_t graph;
+      CB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int e = enqueue_step(c);
+      cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+      if (e) return e;
+      if (ce != cudaSuccess) return fail(c, CB_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return fail(c, CB_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      (void)cur0; (void)uc0;
+      CB_CUDA(c, cudaGraphLaunch(g.exec, c->stream));
+      continue;
+    }
+    int e = enqueue_step(c);
+    if (e) return e;
+  }
+  return CB_OK;
+}
+
+int cb_capture_graph(cb_ctx *c) {
+  if (!c) return CB_E_ARG;
+  if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set");
+  c->use_graphs = true;
+  return CB_OK;
+}
+
+int cb_sync(cb_ctx *c) {
+  if (!c) return CB_E_ARG;
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  unsigned st = 0;
+  CB_CUDA(c, cudaMemcpy(&st, c->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (st) {
+    CB_CUDA(c, cudaMemset(c->status, 0, sizeof(unsigned)));
+    char buf[160];
+    snprintf(buf, sizeof(buf), "device status 0x%x:%s%s%s", st, (st & ST_NONFINITE) ? " non-finite" : "",
+             (st & ST_NEG_RHO) ? " rho<=0" : "", (st & ST_NEG_P) ? " p<=0" : "");
+    return fail(c, CB_E_NONFINITE, buf);
+  }
+  return CB_OK;
+}
+
+int cb_timing_enable(cb_ctx *c, int on) {
+  if (!c) return CB_E_ARG;
+  harvest_timing(c);
+  c->timing = on != 0;
+  c->acc_rhs_ms = c->acc_other_ms = 0;
+  c->acc_rhs_n = c->acc_other_n = 0;
+  return CB_OK;
+}
+
+int cb_timing_read(cb_ctx *c, double *rhs_ms, int *rhs_n, double *other_ms, int *other_n) {
+  if (!c) return CB_E_ARG;
+  harvest_timing(c);
+  if (rhs_ms) *rhs_ms = c->acc_rhs_ms;
+  if (rhs_n) *rhs_n = c->acc_rhs_n;
+  if (other_ms) *other_ms = c->acc_other_ms;
+  if (other_n) *other_n = c->acc_other_n;
+  return CB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,200 @@
+// Auxiliary kernels: periodic boundary/ghost fill (FormBCS + DMGlobalToLocal),
+// eddy viscosity (Compute_eddy_viscosity_LES), device metrics (FormMetrics),
+// AoS <-> padded SoA packing and the EOS for downloads.  All are HBM-bound
+// elementwise/stencil sweeps; grids are sized in multiples of the SM count
+// by the host and every kernel uses a grid-stride loop.
+#pragma once
+#include "cb_common.cuh"
+
+namespace cb {
+
+__device__ __forceinline__ int wrapi(int x, int m) { return x < 0 ? x + m : (x >= m ? x - m : x); }
+
+// Final value source of a non-interior node after FormBCS (fully periodic):
+// boundary nodes take the stale stage input at the periodic image two nodes
+// across (rhs.c:1107-1227; later copies win: k faces, then j, then i), the
+// ghost layers then wrap onto the updated global vector (DMGlobalToLocal).
+// Returns true and sets (si,sj,sk,from_in) for a boundary/ghost node.
+__device__ __forceinline__ void bc_source(const DevCfg &c, int i, int j, int k, int &si, int &sj, int &sk, bool &from_in) {
+  // ghost -> owned image
+  int oi = wrapi(i, c.mx), oj = wrapi(j, c.my), ok = wrapi(k, c.mz);
+  si = oi; sj = oj; sk = ok; from_in = false;
+  const bool bnd = oi == 0 || oi == c.mx - 1 || oj == 0 || oj == c.my - 1 || ok == 0 || ok == c.mz - 1;
+  if (!bnd) return;  // image is interior: value of the stage output
+  from_in = true;
+  if (ok == 0) sk = ok - 2;
+  else if (ok == c.mz - 1) sk = ok + 2;
+  else if (oj == 0) sj = oj - 2;
+  else if (oj == c.my - 1) sj = oj + 2;
+  else if (oi == 0) si = oi - 2;
+  else si = oi + 2;  // oi == mx-1
+}
+
+// Writes every non-interior node (boundary layer + both ghost layers) of qout.
+__global__ void bc_periodic_kernel(const DevCfg c, DevFields F) {
+  const long long nx = c.mx + 4, ny = c.my + 4, nz = c.mz + 4, total = nx * ny * nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx) - 2, j = (int)((t / nx) % ny) - 2, k = (int)(t / (nx * ny)) - 2;
+    if (i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2) continue;
+    int si, sj, sk;
+    bool from_in;
+    bc_source(c, i, j, k, si, sj, sk, from_in);
+    const long long g = gidx(c, i, j, k), s = gidx(c, si, sj, sk);
+#pragma unroll
+    for (int q = 0; q < 5; q++) F.qout[q][g] = from_in ? F.q[q][s] : F.qout[q][s];
+  }
+}
+
+// Ghost layers of periodic planes from their owned images (DMGlobalToLocal).
+__global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, int nplanes) {
+  const long long nx = c.mx + 4, ny = c.my + 4, nz = c.mz + 4, total = nx * ny * nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx) - 2, j = (int)((t / nx) % ny) - 2, k = (int)(t / (nx * ny)) - 2;
+    const bool gi = i < 0 || i >= c.mx, gj = j < 0 || j >= c.my, gk = k < 0 || k >= c.mz;
+    if (!(gi || gj || gk)) continue;
+    const bool pi = c.bctype[0] == 7, pj = c.bctype[2] == 7, pk = c.bctype[4] == 7;
+    if ((gi && !pi) || (gj && !pj) || (gk && !pk)) continue;
+    const long long g = gidx(c, i, j, k), s = gidx(c, wrapi(i, c.mx), wrapi(j, c.my), wrapi(k, c.mz));
+    for (int p = 0; p < nplanes; p++) planes[p][g] = planes[p][s];
+  }
+}
+
+// Compute_eddy_viscosity_LES (les.c:1523-1567) with constant CS
+// (les.c:135-150): interior nodes only; velocity from the recorded state qu
+// (nullptr: zero velocity before the first CalcUCat).
+__global__ void eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met,
+                                      const double *aj, const double *nvert, double *nut) {
+  const long long nx = c.mx - 2, ny = c.my - 2, nz = c.mz - 2, total = nx * ny * nz;
+  const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / (nx * ny));
+    const long long n = gidx(c, i, j, k);
+    if (ldg(nvert + n) > 0.1) { nut[n] = 0.; continue; }
+    double dd[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if (!qu) { dd[a][0] = dd[a][1] = dd[a][2] = 0.; continue; }
+      const double *r = qu[0], *m = qu[1 + a];
+      dd[a][0] = (ldg(m + n + si) / ldg(r + n + si) - ldg(m + n - si) / ldg(r + n - si)) * 0.5;
+      dd[a][1] = (ldg(m + n + sj) / ldg(r + n + sj) - ldg(m + n - sj) / ldg(r + n - sj)) * 0.5;
+      dd[a][2] = (ldg(m + n + sk) / ldg(r + n + sk) - ldg(m + n - sk) / ldg(r + n - sk)) * 0.5;
+    }
+    const double ajc = ldg(aj + n);
+    double g[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int x = 0; x < 3; x++)
+        g[a][x] = (dd[a][0] * ldg(met[0 * 3 + x] + n) + dd[a][1] * ldg(met[1 * 3 + x] + n) + dd[a][2] * ldg(met[2 * 3 + x] + n)) * ajc;
+    const double Sdd = 2. / 3. * (g[0][0] + g[1][1] + g[2][2]);
+    const double Sxx = 0.5 * (g[0][0] + g[0][0]) - Sdd, Sxy = 0.5 * (g[0][1] + g[1][0]), Sxz = 0.5 * (g[0][2] + g[2][0]);
+    const double Syy = 0.5 * (g[1][1] + g[1][1]) - Sdd, Syz = 0.5 * (g[1][2] + g[2][1]);
+    const double Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
+    const double Sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Sxy * Sxy + Syy * Syy + Syz * Syz + Sxz * Sxz +
+                                    Syz * Syz + Szz * Szz));
+    const double filter = pow(1. / ajc, 1. / 3.);
+    nut[n] = c.cs_const * (filter * filter) * Sabs;
+  }
+}
+
+// ---------------------------------------------------------------- metrics --
+// FormMetrics (metrics.c:52-136): csi on (k,j) interior for every i, eta on
+// (k,i) interior for every j, zet on (j,i) interior for every k, aj on the
+// interior; everything else zero.
+__global__ void metrics_interior_kernel(const DevCfg c, const double *const *X, double *const *met, double *aj) {
+  const long long nx = c.mx, ny = c.my, nz = c.mz, total = nx * ny * nz;
+  const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx), j = (int)((t / nx) % ny), k = (int)(t / (nx * ny));
+    const long long n = gidx(c, i, j, k);
+    const bool ii = i > 0 && i < c.mx - 1, jj = j > 0 && j < c.my - 1, kk = k > 0 && k < c.mz - 1;
+    double dc[3], de[3], dz[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      dc[a] = ii ? 0.5 * (X[a][n + si] - X[a][n - si]) : 0.;
+      de[a] = jj ? 0.5 * (X[a][n + sj] - X[a][n - sj]) : 0.;
+      dz[a] = kk ? 0.5 * (X[a][n + sk] - X[a][n - sk]) : 0.;
+    }
+    double v[10];
+    for (int a = 0; a < 10; a++) v[a] = 0.;
+    if (kk && jj) {
+      v[0] = de[1] * dz[2] - de[2] * dz[1];
+      v[1] = -de[0] * dz[2] + de[2] * dz[0];
+      v[2] = de[0] * dz[1] - de[1] * dz[0];
+    }
+    if (kk && ii) {
+      v[3] = dz[1] * dc[2] - dz[2] * dc[1];
+      v[4] = -dz[0] * dc[2] + dz[2] * dc[0];
+      v[5] = dz[0] * dc[1] - dz[1] * dc[0];
+    }
+    if (jj && ii) {
+      v[6] = dc[1] * de[2] - dc[2] * de[1];
+      v[7] = -dc[0] * de[2] + dc[2] * de[0];
+      v[8] = dc[0] * de[1] - dc[1] * de[0];
+    }
+    if (ii && jj && kk) {
+      const double det = dc[0] * (de[1] * dz[2] - de[2] * dz[1]) - dc[1] * (de[0] * dz[2] - de[2] * dz[0]) +
+                         dc[2] * (de[0] * dz[1] - de[1] * dz[0]);
+      v[9] = 1. / det;
+    }
+    for (int a = 0; a < 9; a++) met[a][n] = v[a];
+    aj[n] = v[9];
+  }
+}
+
+// One boundary-copy pass of FormMetrics (metrics.c:138-246).  face: 0 i-lo,
+// 1 i-hi, 2 j-lo, 3 j-hi, 4 k-lo, 5 k-hi.  The passes must run in this order.
+__global__ void metrics_boundary_kernel(const DevCfg c, double *const *met, double *aj, int face) {
+  const int d = face / 2, hi = face & 1;
+  const int na = d == 0 ? c.my : c.mx, nb = d == 2 ? c.my : c.mz;  // the two transverse extents
+  const long long total = (long long)na * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t % na), b = (int)(t / na);
+    int i, j, k;
+    if (d == 0) { i = hi ? c.mx - 1 : 0; j = a; k = b; }
+    else if (d == 1) { j = hi ? c.my - 1 : 0; i = a; k = b; }
+    else { k = hi ? c.mz - 1 : 0; i = a; j = b; }
+    const long long n = gidx(c, i, j, k);
+    const long long s = hi ? -gstride(c, d) : gstride(c, d);
+    // i faces copy eta,zet; j faces csi,zet; k faces eta,csi (plus aj always)
+    const int m1 = d == 0 ? 1 : 0, m2 = d == 2 ? 1 : 2;
+    for (int q = 0; q < 3; q++) {
+      met[m1 * 3 + q][n] = met[m1 * 3 + q][n + s];
+      met[m2 * 3 + q][n] = met[m2 * 3 + q][n + s];
+    }
+    aj[n] = aj[n + s];
+  }
+}
+
+// --------------------------------------------------------- pack / unpack --
+// AoS natural (mz,my,mx,nc) <-> owned nodes of nc padded planes.
+__global__ void unpack_kernel(const DevCfg c, const double *__restrict__ aos, int nc, double *const *planes) {
+  const long long total = (long long)c.mx * c.my * c.mz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % c.mx), j = (int)((t / c.mx) % c.my), k = (int)(t / ((long long)c.mx * c.my));
+    const long long g = gidx(c, i, j, k);
+    for (int q = 0; q < nc; q++) planes[q][g] = aos[t * nc + q];
+  }
+}
+
+__global__ void pack_kernel(const DevCfg c, const double *const *planes, int nc, double *__restrict__ aos) {
+  const long long total = (long long)c.mx * c.my * c.mz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % c.mx), j = (int)((t / c.mx) % c.my), k = (int)(t / ((long long)c.mx * c.my));
+    const long long g = gidx(c, i, j, k);
+    for (int q = 0; q < nc; q++) aos[t * nc + q] = planes[q][g];
+  }
+}
+
+// EqOfState (rhs.c:4845-4856) on owned nodes, written AoS (1 per node).
+__global__ void eos_pack_kernel(const DevCfg c, const double *const *q, double *__restrict__ p) {
+  const long long total = (long long)c.mx * c.my * c.mz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % c.mx), j = (int)((t / c.mx) % c.my), k = (int)(t / ((long long)c.mx * c.my));
+    const long long g = gidx(c, i, j, k);
+    const double r = q[0][g], ru = q[1][g], rv = q[2][g], rw = q[3][g], re = q[4][g];
+    p[t] = (c.gamma - 1) * (re - 0.5 * (ru * ru + rv * rv + rw * rw) / r);
+  }
+}
+
+}  // namespace cb

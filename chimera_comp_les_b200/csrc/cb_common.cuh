@@ -1,0 +1,66 @@
+// Device-side definitions shared by the kernels of libchimera_b200.so.
+//
+// HBM layout (one block of the reference's DMDA):
+//   every field is its own plane (SoA) over the padded node box
+//   px x (my+4) x (mz+4), node (i,j,k) at ((k+2)*(my+4) + (j+2))*px + (i+2),
+//   i in [-2, mx+1].  px = mx+4 rounded up to a multiple of 16 doubles so each
+//   row starts on a 128-byte boundary.  The two ghost layers of a periodic
+//   direction hold the DMDA wrap-around images (local index -1 -> m-1,
+//   -2 -> m-2, m -> 0, m+1 -> 1), exactly what DMGlobalToLocal gives the
+//   reference (init.c:156 stencil width 2).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cb {
+
+// Status bits of the sticky device status word.
+enum : unsigned { ST_NONFINITE = 1u, ST_NEG_RHO = 2u, ST_NEG_P = 4u };
+
+struct DevCfg {
+  int mx, my, mz;
+  int px, py, pz;          // padded extents (px = row pitch in doubles)
+  long long plane;         // px*py*pz doubles per field
+  int bctype[6];
+  int les, inviscid, fluxorder, eno_order, central, isothermal;
+  double s_x, s_y, s_z;
+  double ren, ma, pr, gamma, dt, st, cs_const, ci, ratio;
+};
+
+struct DevFields {
+  const double *q[5];      // stage input (ghosted)
+  const double *qold[5];   // Qold
+  double *qout[5];         // stage output
+  const double *met[3][3]; // met[0]=csi, met[1]=eta, met[2]=zet; [component]
+  const double *aj;
+  const double *nvert;
+  const double *nut;
+  double *rhs[5];          // formRHS output (rhs mode only)
+  unsigned *status;        // sticky status word
+};
+
+__host__ __device__ __forceinline__ long long gidx(const DevCfg &c, int i, int j, int k) {
+  return ((long long)(k + 2) * c.py + (j + 2)) * (long long)c.px + (i + 2);
+}
+
+__host__ __device__ __forceinline__ long long gstride(const DevCfg &c, int d) {
+  return d == 0 ? 1LL : (d == 1 ? (long long)c.px : (long long)c.px * c.py);
+}
+
+__device__ __forceinline__ double ldg(const double *p) { return __ldg(p); }
+
+// Hybrid weight sigma of direction d at node (i,j,k) when the shock sensor is
+// off (rhs.c:3322-3441): every node starts at (s_x, s_y, s_z); interior nodes
+// then take y = z = min(z, y).  Ghost nodes carry the wrap-around image.
+__device__ __forceinline__ double sigma_at(const DevCfg &c, int d, int i, int j, int k) {
+  if (d == 0) return c.s_x;
+  // wrap ghost indices to their owned image (periodic directions only reach ghosts)
+  int ii = i < 0 ? i + c.mx : (i >= c.mx ? i - c.mx : i);
+  int jj = j < 0 ? j + c.my : (j >= c.my ? j - c.my : j);
+  int kk = k < 0 ? k + c.mz : (k >= c.mz ? k - c.mz : k);
+  bool interior = ii > 0 && ii < c.mx - 1 && jj > 0 && jj < c.my - 1 && kk > 0 && kk < c.mz - 1;
+  if (interior) return c.s_z < c.s_y ? c.s_z : c.s_y;
+  return d == 1 ? c.s_y : c.s_z;
+}
+
+}  // namespace cb

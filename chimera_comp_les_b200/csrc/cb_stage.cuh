@@ -1,0 +1,575 @@
+// Fused stage kernel: formRHS (inviscid + viscous + SGS face fluxes, flux
+// difference, MultAj) followed by the SSP-RK stage combination, FP64.
+//
+// Reference arithmetic restated (rhs.c):
+//   formConvection      2570-3224   (non-LES upwind: first order / MUSCL / WENO3, Rusanov)
+//   formConvectionLES   3231-4291   (upwind blended with a 4-point central flux by sigma)
+//   formViscous         1367-2254   (stress, heat flux, eddy viscosity, Yoshizawa, LES energy)
+//   MultAj / formRHS    4575-4736
+//   RungeKutta          solvers.c:232-271 (stage combination)
+//
+// Execution shape (B200): a block owns a BX x BY column of interior nodes and
+// marches along k through a chunk of planes.  A ring of four node planes
+// (k-1 .. k+2, each with a two-node halo in i and j) lives in shared memory
+// holding the conserved state and the derived p, u, v, w, T=p/rho, so every
+// division of the EOS / CalcUCat happens once per node.  Each face flux is
+// computed exactly once: i- and j-faces of the current plane go to shared
+// memory, the k-face k+1/2 stays in registers and becomes k-1/2 of the next
+// plane.  Metrics, nvert and nu_t are read through the read-only cache.
+#pragma once
+#include "cb_common.cuh"
+
+namespace cb {
+
+constexpr int NF = 10;  // fields per node in the plane ring
+enum { F_RHO = 0, F_RU, F_RV, F_RW, F_RE, F_P, F_U, F_V, F_W, F_T };
+constexpr int NG = 8;   // per face: G[0..4] = Fvisc - Fconv, A[0..2] = LES stress part
+
+constexpr double BLANKWALL = 2.9;
+constexpr double BLANK = 0.1;
+constexpr double SOLID = 0.5;
+constexpr double INNERBLANK = 7.;
+constexpr double GAMMA_CONV = 1.4;  // formConvection[LES] fix gamma = 1.4 (rhs.c:2596, 3257)
+
+template <int BX, int BY>
+struct TileShape {
+  static constexpr int PX = BX + 4, PY = BY + 4, PN = PX * PY;
+  static constexpr int NXF = (BX + 1) * BY;
+  static constexpr int NYF = BX * (BY + 1);
+  static constexpr size_t smem_bytes = sizeof(double) * ((size_t)4 * NF * PN + (size_t)NG * (NXF + NYF));
+};
+
+struct NRef {
+  int r, y, x;  // relative plane (-1..2), tile-local row, tile-local column
+};
+
+__device__ __forceinline__ NRef nshift(NRef n, int d, int s) {
+  if (d == 0) n.x += s;
+  else if (d == 1) n.y += s;
+  else n.r += s;
+  return n;
+}
+
+template <int BX, int BY>
+struct Ring {
+  double *pl;
+  int slot[4];
+  __device__ __forceinline__ double get(int f, NRef n) const {
+    return pl[((slot[n.r + 1] * NF + f) * TileShape<BX, BY>::PY + n.y) * TileShape<BX, BY>::PX + n.x];
+  }
+  __device__ __forceinline__ double *ptr(int s, int f) const {
+    return pl + (size_t)(s * NF + f) * TileShape<BX, BY>::PN;
+  }
+};
+
+// ---------------------------------------------------------------- recon --
+__device__ __forceinline__ double d_sgn(double a) { return (a >= 0) ? ((a == 0) ? 0. : 1.) : -1.; }
+__device__ __forceinline__ double d_minmod(double a, double b) {
+  if (a * b < 0) return 0.;
+  double fa = fabs(a), fb = fabs(b);
+  return d_sgn(a) * ((fa < fb) ? fa : fb);
+}
+__device__ __forceinline__ double muscl_l(double qm, double q0, double qp) { return q0 + 0.5 * d_minmod(qp - q0, q0 - qm); }
+__device__ __forceinline__ double muscl_r(double qm, double q0, double qp) { return q0 - 0.5 * d_minmod(qp - q0, q0 - qm); }
+__device__ __forceinline__ double weno3_l(double qm, double q0, double qp) {
+  const double d0 = 0.6666667, d1 = 0.3333333, eps = 1e-6;  // rhs.c:2386 (truncated weights)
+  double r0 = 0.5 * q0 + 0.5 * qp, r1 = -0.5 * qm + 1.5 * q0;
+  double b0 = (qp - q0) * (qp - q0), b1 = (qm - q0) * (qm - q0);
+  double a0 = d0 / ((eps + b0) * (eps + b0)), a1 = d1 / ((eps + b1) * (eps + b1));
+  double as = a0 + a1;
+  return (a0 / as) * r0 + (a1 / as) * r1;
+}
+__device__ __forceinline__ double weno3_r(double qm, double q0, double qp) {
+  const double d0 = 0.6666667, d1 = 0.3333333, eps = 1e-6;
+  double r0 = 1.5 * q0 - 0.5 * qp, r1 = 0.5 * qm + 0.5 * q0;
+  double b0 = (qp - q0) * (qp - q0), b1 = (qm - q0) * (qm - q0);
+  double a0 = d0 / ((eps + b0) * (eps + b0)), a1 = d1 / ((eps + b1) * (eps + b1));
+  double as = a0 + a1;
+  return (a0 / as) * r0 + (a1 / as) * r1;
+}
+__device__ __forceinline__ double eno_r(double qm, double q0, double qp, int k) {
+  if (k == 2) return 0.5 * q0 + 0.5 * qp;
+  return -qm * 0.1666666666666666 + q0 * 0.8333333333333333 + qp * 0.3333333333333333;
+}
+__device__ __forceinline__ double eno_l(double qm, double q0, double qp, int k) {
+  if (k == 2) return 0.5 * q0 + 0.5 * qm;
+  return qm * 0.3333333333333333 + q0 * 0.8333333333333333 - qp * 0.1666666666666666;
+}
+
+// Rusanov flux on reconstructed states (rhs.c:2769-2810).
+__device__ __forceinline__ void rusanov(const double QL[5], const double QR[5], double pL, double pR,
+                                        const double h[3], bool use_qr_for_l, bool r_from_l, double F[5]) {
+  double iL = 1.0 / QL[0], iR = 1.0 / QR[0];
+  double uconL = use_qr_for_l ? (h[0] * (QR[1] * iR) + h[1] * (QR[2] * iR) + h[2] * (QR[3] * iR))
+                              : (h[0] * (QL[1] * iL) + h[1] * (QL[2] * iL) + h[2] * (QL[3] * iL));
+  double uconR = r_from_l ? uconL : (h[0] * (QR[1] * iR) + h[1] * (QR[2] * iR) + h[2] * (QR[3] * iR));
+  double gii = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+  double cL = GAMMA_CONV * pL * iL, cR = GAMMA_CONV * pR * iR;
+  double saL = fabs(uconL) + sqrt(fabs(cL) * gii);
+  double saR = fabs(uconR) + sqrt(fabs(cR) * gii);
+  double SA = (saL < saR) ? saR : saL;
+  F[0] = 0.5 * (QL[0] * uconL + QR[0] * uconR) - 0.5 * SA * (QR[0] - QL[0]);
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    F[1 + a] = 0.5 * ((QL[1 + a] * uconL + QR[1 + a] * uconR) + (pL * h[a] + pR * h[a])) - 0.5 * SA * (QR[1 + a] - QL[1 + a]);
+  F[4] = 0.5 * ((pL + QL[4]) * uconL + (pR + QR[4]) * uconR) - 0.5 * SA * (QR[4] - QL[4]);
+}
+
+// ------------------------------------------------------- inviscid face ----
+// Face between node A (tile ref a, global (gi,gj,gk)) and A + e_d.
+template <bool LES, int BX, int BY>
+__device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, const Ring<BX, BY> &R, int d, NRef a,
+                                          int gi, int gj, int gk, double Fc[5]) {
+  const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d);
+  const int pos = d == 0 ? gi : (d == 1 ? gj : gk);
+  const int m = d == 0 ? c.mx : (d == 1 ? c.my : c.mz);
+  const double nvm = ldg(F.nvert + g0 - sd), nv0 = ldg(F.nvert + g0), nv1 = ldg(F.nvert + g0 + sd),
+               nv2 = ldg(F.nvert + g0 + 2 * sd);
+  const double *const *met = F.met[d];
+  double h[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) h[q] = 0.5 * (ldg(met[q] + g0) + ldg(met[q] + g0 + sd));
+
+  // stencil values along d: s=0..3 -> node offsets -1..2
+  double Q[4][5], P[4];
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    NRef n = nshift(a, d, s - 1);
+#pragma unroll
+    for (int q = 0; q < 5; q++) Q[s][q] = R.get(F_RHO + q, n);
+    P[s] = R.get(F_P, n);
+  }
+
+  double QL[5], QR[5], pL, pR;
+  const int fo = c.fluxorder;
+  bool first;
+  if (LES) {
+    double nsum2 = (d == 2) ? nv0 + ldg(F.nvert + gidx(c, 1, gj, gk + 1)) : nv0 + nv1;  // quirk rhs.c:4046
+    first = fo == 1 || ((pos == 0 || pos == m - 2) && c.bctype[2 * d] != 7) || nsum2 > BLANKWALL;
+  } else {
+    first = fo == 1 || pos == 0 || pos == m - 2 || (nv0 + nv1) > BLANKWALL;
+  }
+  int iso_case = 0;
+  if (!LES && d == 1 && c.isothermal) {
+    if (gj == 0 && c.bctype[2] == 1) iso_case = 1;           // rhs.c:2822
+    else if (gj == m - 2 && c.bctype[3] == 1) iso_case = 2;  // rhs.c:2828
+  }
+  if (iso_case == 1) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) QL[q] = QR[q] = Q[1][q];
+    pL = pR = P[1];
+  } else if (iso_case == 2) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) QL[q] = QR[q] = Q[2][q];
+    pL = pR = P[2];
+  } else if (first) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) { QL[q] = Q[1][q]; QR[q] = Q[2][q]; }
+    pL = P[1]; pR = P[2];
+  } else if (fo == 2 || (!LES && d > 0 && gj < 30 && gk < 7)) {  // quirk rhs.c:2840, 2997
+    const int im = (nvm > BLANKWALL) ? 2 : 0;  // qm = q[i+1] when i-1 is a wall
+    const int ip = (nv2 > BLANKWALL) ? 1 : 3;  // qp = q[i] when i+2 is a wall
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      QL[q] = muscl_l(Q[im][q], Q[1][q], Q[2][q]);
+      QR[q] = muscl_r(Q[1][q], Q[2][q], Q[ip][q]);
+    }
+    pL = muscl_l(P[im], P[1], P[2]);
+    pR = muscl_r(P[1], P[2], P[ip]);
+  } else {
+    const int ord = c.eno_order;
+    const bool el = nvm > BLANKWALL && (d != 0 || (gi + 2) < c.mx);
+    const bool er = nv2 > BLANKWALL;
+    if (el) {
+#pragma unroll
+      for (int q = 0; q < 5; q++) QL[q] = eno_l(Q[1][q], Q[2][q], Q[3][q], ord);
+      pL = eno_l(P[1], P[2], P[3], ord);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 5; q++) QL[q] = weno3_l(Q[0][q], Q[1][q], Q[2][q]);
+      pL = weno3_l(P[0], P[1], P[2]);
+      if (!LES && d == 1 && gj == 1 && c.isothermal && c.bctype[2] == 1) {  // rhs.c:2926
+        QL[0] = eno_l(Q[1][0], Q[2][0], Q[3][0], ord);
+        QL[4] = eno_l(Q[1][4], Q[2][4], Q[3][4], ord);
+        pL = eno_l(P[1], P[2], P[3], ord);
+      }
+    }
+    if (er) {
+#pragma unroll
+      for (int q = 0; q < 5; q++) QR[q] = eno_r(Q[0][q], Q[1][q], Q[2][q], ord);
+      pR = eno_r(P[0], P[1], P[2], ord);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 5; q++) QR[q] = weno3_r(Q[1][q], Q[2][q], Q[3][q]);
+      pR = weno3_r(P[1], P[2], P[3]);
+    }
+  }
+  double Fw[5];
+  if (LES) {
+    rusanov(QL, QR, pL, pR, h, false, false, Fw);
+  } else {
+    const bool use_qr_l = (pos == m - 2 && c.bctype[2 * d + 1] == 1);
+    const bool r_from_l = (pos == 0 && c.bctype[2 * d] == 1);
+    rusanov(QL, QR, pL, pR, h, use_qr_l, r_from_l, Fw);
+  }
+  if (!LES) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) Fc[q] = Fw[q];
+    return;
+  }
+
+  // central flux (rhs.c:3483-3547) and blend
+  double Fcen[5];
+  bool four = false;
+  if (pos > 0 && pos < m - 2) {
+    double nsum = (d == 0) ? nv0 + nv1 + nv2 + nvm : nvm + nv0 + nv1 + nv2;
+    four = nsum < 2.9;
+  }
+  if (four && (c.central == 2 || c.central == 3)) {
+    double U[4], EP[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const long long gs = g0 + (s - 1) * sd;
+      U[s] = 1. / Q[s][0] * (ldg(met[0] + gs) * Q[s][1] + ldg(met[1] + gs) * Q[s][2] + ldg(met[2] + gs) * Q[s][3]);
+      EP[s] = P[s] + Q[s][4];
+    }
+    const double fp4 = 1.0 / 12.0 * (-P[0] + 7 * P[1] + 7 * P[2] - P[3]);
+    if (c.central == 2) {
+#define CB_FP2(A0, A1, A2, A3) ((A1 + A2) * (U[1] + U[2]) / 3.0 - 1. / 24. * (A0 * U[0] + A0 * U[2] + A1 * U[1] + A1 * U[3] + A2 * U[2] + A2 * U[0] + A3 * U[1] + A3 * U[3]))
+      Fcen[0] = CB_FP2(Q[0][0], Q[1][0], Q[2][0], Q[3][0]);
+      Fcen[1] = CB_FP2(Q[0][1], Q[1][1], Q[2][1], Q[3][1]) + fp4 * h[0];
+      Fcen[2] = CB_FP2(Q[0][2], Q[1][2], Q[2][2], Q[3][2]) + fp4 * h[1];
+      Fcen[3] = CB_FP2(Q[0][3], Q[1][3], Q[2][3], Q[3][3]) + fp4 * h[2];
+      Fcen[4] = CB_FP2(EP[0], EP[1], EP[2], EP[3]);
+#undef CB_FP2
+    } else {
+#define CB_FP1(A0, A1, A2, A3) (1.0 / 12.0 * (-A0 * U[0] + 7 * A1 * U[1] + 7 * A2 * U[2] - A3 * U[3]))
+      Fcen[0] = CB_FP1(Q[0][0], Q[1][0], Q[2][0], Q[3][0]);
+      Fcen[1] = CB_FP1(Q[0][1], Q[1][1], Q[2][1], Q[3][1]) + fp4 * h[0];
+      Fcen[2] = CB_FP1(Q[0][2], Q[1][2], Q[2][2], Q[3][2]) + fp4 * h[1];
+      Fcen[3] = CB_FP1(Q[0][3], Q[1][3], Q[2][3], Q[3][3]) + fp4 * h[2];
+      Fcen[4] = CB_FP1(EP[0], EP[1], EP[2], EP[3]);
+#undef CB_FP1
+    }
+  } else {
+    const double rc = 0.5 * (Q[1][0] + Q[2][0]), uc = 0.5 * (Q[1][1] + Q[2][1]), vc = 0.5 * (Q[1][2] + Q[2][2]);
+    const double wc = 0.5 * (Q[1][3] + Q[2][3]), ec = 0.5 * (Q[1][4] + Q[2][4]);
+    const double Uc = (h[0] * uc + h[1] * vc + h[2] * wc) / rc;
+    const double pa = 0.5 * (P[1] + P[2]);
+    Fcen[0] = rc * Uc;
+    Fcen[1] = uc * Uc + pa * h[0];
+    Fcen[2] = vc * Uc + pa * h[1];
+    Fcen[3] = wc * Uc + pa * h[2];
+    Fcen[4] = Uc * (ec + pa);
+  }
+  const double sigma = sigma_at(c, d, gi, gj, gk);
+#pragma unroll
+  for (int q = 0; q < 5; q++) Fc[q] = Fw[q] * (1.0 - sigma) + Fcen[q] * sigma;
+}
+
+// -------------------------------------------------------- viscous face ----
+__device__ __forceinline__ bool blocked(double v) { return v > SOLID && v < INNERBLANK; }
+
+template <bool LES, int BX, int BY>
+__device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, const Ring<BX, BY> &R, int d, NRef a,
+                                          int gi, int gj, int gk, double Fv[5], double A[3]) {
+  const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d), g1 = g0 + sd;
+  const int pos = d == 0 ? gi : (d == 1 ? gj : gk);
+  const int m = d == 0 ? c.mx : (d == 1 ? c.my : c.mz);
+  const NRef b = nshift(a, d, 1);
+  // D[f][e]: derivative of (u, v, w, T) along computational direction e
+  double D[4][3];
+#pragma unroll
+  for (int f = 0; f < 4; f++) D[f][d] = R.get(F_U + f, b) - R.get(F_U + f, a);
+#pragma unroll
+  for (int e = 0; e < 3; e++) {
+    if (e == d) continue;
+    const long long te = gstride(c, e);
+    const bool plus_blocked = blocked(ldg(F.nvert + g0 + te)) || blocked(ldg(F.nvert + g1 + te));
+    const bool minus_blocked = blocked(ldg(F.nvert + g0 - te)) || blocked(ldg(F.nvert + g1 - te));
+    const NRef ap = nshift(a, e, 1), am = nshift(a, e, -1), bp = nshift(b, e, 1), bm = nshift(b, e, -1);
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      const int fi = F_U + f;
+      if (plus_blocked) {
+        if (f == 3 && d == 0 && e == 2)  // quirk: dpdz typo rhs.c:1544-1545
+          D[f][e] = (R.get(fi, b) + R.get(fi, a) - R.get(fi, bm) - R.get(fi, a)) * 0.5;
+        else
+          D[f][e] = (R.get(fi, b) + R.get(fi, a) - R.get(fi, bm) - R.get(fi, am)) * 0.5;
+      } else if (minus_blocked) {
+        D[f][e] = (R.get(fi, bp) + R.get(fi, ap) - R.get(fi, b) - R.get(fi, a)) * 0.5;
+      } else {
+        D[f][e] = (R.get(fi, bp) + R.get(fi, ap) - R.get(fi, bm) - R.get(fi, am)) * 0.25;
+      }
+    }
+  }
+  const double dudc = D[0][0], dude = D[0][1], dudz = D[0][2];
+  const double dvdc = D[1][0], dvde = D[1][1], dvdz = D[1][2];
+  const double dwdc = D[2][0], dwde = D[2][1], dwdz = D[2][2];
+  const double dpdc = D[3][0], dpde = D[3][1], dpdz = D[3][2];
+
+  double mh[3][3];
+#pragma unroll
+  for (int e = 0; e < 3; e++)
+#pragma unroll
+    for (int q = 0; q < 3; q++) mh[e][q] = 0.5 * (ldg(F.met[e][q] + g0) + ldg(F.met[e][q] + g1));
+  const double md0 = mh[d][0], md1 = mh[d][1], md2 = mh[d][2];
+  const double csi0 = mh[0][0], csi1 = mh[0][1], csi2 = mh[0][2];
+  const double eta0 = mh[1][0], eta1 = mh[1][1], eta2 = mh[1][2];
+  const double zet0 = mh[2][0], zet1 = mh[2][1], zet2 = mh[2][2];
+  const double g11 = csi0 * md0 + csi1 * md1 + csi2 * md2;
+  const double g21 = eta0 * md0 + eta1 * md1 + eta2 * md2;
+  const double g31 = zet0 * md0 + zet1 * md1 + zet2 * md2;
+
+  const double r11 = dudc * csi0 + dude * eta0 + dudz * zet0;
+  const double r21 = dvdc * csi0 + dvde * eta0 + dvdz * zet0;
+  const double r31 = dwdc * csi0 + dwde * eta0 + dwdz * zet0;
+  const double r12 = dudc * csi1 + dude * eta1 + dudz * zet1;
+  const double r22 = dvdc * csi1 + dvde * eta1 + dvdz * zet1;
+  const double r32 = dwdc * csi1 + dwde * eta1 + dwdz * zet1;
+  const double r13 = dudc * csi2 + dude * eta2 + dudz * zet2;
+  const double r23 = dvdc * csi2 + dvde * eta2 + dvdz * zet2;
+  const double r33 = dwdc * csi2 + dwde * eta2 + dwdz * zet2;
+
+  const double ajc = 0.5 * (ldg(F.aj + g0) + ldg(F.aj + g1));
+  double nu = 1. / c.ren;
+  if (LES) {
+    // quirk: eta/zeta faces average rho over i and i+1 (rhs.c:1835, 2034)
+    const double rhs_rho = (d == 0) ? R.get(F_RHO, b) : R.get(F_RHO, nshift(a, 0, 1));
+    nu = 1. / c.ren * 0.5 * (R.get(F_RHO, a) + rhs_rho);
+  }
+  const double div = 2. / 3. * (dudc * csi0 + dude * eta0 + dudz * zet0 + dvdc * csi1 + dvde * eta1 + dvdz * zet1 +
+                                dwdc * csi2 + dwde * eta2 + dwdz * zet2);
+  const double tu = g11 * dudc + g21 * dude + g31 * dudz + r11 * md0 + r21 * md1 + r31 * md2;
+  const double tv = g11 * dvdc + g21 * dvde + g31 * dvdz + r12 * md0 + r22 * md1 + r32 * md2;
+  const double tw = g11 * dwdc + g21 * dwde + g31 * dwdz + r13 * md0 + r23 * md1 + r33 * md2;
+  Fv[0] = 0.;
+  Fv[1] = tu * ajc * nu - div * md0 * ajc * nu;
+  Fv[2] = tv * ajc * nu - div * md1 * ajc * nu;
+  Fv[3] = tw * ajc * nu - div * md2 * ajc * nu;
+
+  double uh[3];
+  if (pos == 0 && c.bctype[2 * d] == 1) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) uh[q] = R.get(F_U + q, a);
+  } else if (pos == m - 2 && c.bctype[2 * d + 1] == 1) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) uh[q] = R.get(F_U + q, b);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 3; q++) uh[q] = 0.5 * (R.get(F_U + q, b) + R.get(F_U + q, a));
+  }
+  const double gm = c.gamma;
+  Fv[4] = (Fv[1] * uh[0] + Fv[2] * uh[1] + Fv[3] * uh[2]) +
+          (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (gm * nu / c.pr / (gm - 1.0));
+
+  A[0] = A[1] = A[2] = 0.;
+  if (LES) {  // rhs.c:1677-1710
+    const double sa = sigma_at(c, d, gi, gj, gk);
+    const int bi = gi + (d == 0), bj = gj + (d == 1), bk = gk + (d == 2);
+    const double sb = sigma_at(c, d, bi, bj, bk);
+    double nut = 0.5 * (ldg(F.nut + g0) * sa + ldg(F.nut + g1) * sb);
+    const double rho_c = 0.5 * (R.get(F_RHO, a) + R.get(F_RHO, b));
+    const double sigma_c = 0.5 * (sa + sb);
+    if ((c.bctype[2 * d] == 1 && pos == 0) || (c.bctype[2 * d + 1] == 1 && pos == m - 2)) nut = 0;
+    const double tx = (tu - div * md0) * ajc * (nut * rho_c);
+    const double ty = (tv - div * md1) * ajc * (nut * rho_c);
+    const double tz = (tw - div * md2) * ajc * (nut * rho_c);
+    const double S2 = .5 * ((r11 - div) * (r11 - div) + r12 * r12 + r13 * r13 + r21 * r21 + (r22 - div) * (r22 - div) +
+                            r23 * r23 + r31 * r31 + r32 * r32 + (r33 - div) * (r33 - div));
+    const double filter = pow(1. / ldg(F.aj + g0), 1. / 3.);
+    const double pf = filter * filter;
+    const double sgs = -S2 * pf * c.ci * 2.0 / 3.0;
+    A[0] = tx + sgs * md0 * rho_c * sigma_c;
+    A[1] = ty + sgs * md1 * rho_c * sigma_c;
+    A[2] = tz + sgs * md2 * rho_c * sigma_c;
+    Fv[1] += A[0];
+    Fv[2] += A[1];
+    Fv[3] += A[2];
+  }
+}
+
+// ---------------------------------------------------------- the kernel ----
+template <bool LES, bool VISC, bool RHS_MODE, int BX, int BY>
+__global__ void __launch_bounds__(BX *BY, 1)
+    stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
+  using TS = TileShape<BX, BY>;
+  extern __shared__ double smem[];
+  Ring<BX, BY> R;
+  R.pl = smem;
+  double *gxb = smem + (size_t)4 * NF * TS::PN;  // [NG][BY][BX+1]
+  double *gyb = gxb + (size_t)NG * TS::NXF;      // [NG][BY+1][BX]
+
+  const int tid = threadIdx.x + BX * threadIdx.y;
+  const int nthr = BX * BY;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = 1 + blockIdx.x * BX, j0 = 1 + blockIdx.y * BY;
+  const int kb = 1 + blockIdx.z * kchunk;
+  const int ke = min(c.mz - 1, kb + kchunk);  // exclusive
+  const int gi = i0 + tx, gj = j0 + ty;
+  const bool active = gi <= c.mx - 2 && gj <= c.my - 2;
+
+  // load global plane kk into ring slot s (conserved + derived fields)
+  auto load_plane = [&](int kk, int s) {
+    for (int idx = tid; idx < TS::PN; idx += nthr) {
+      const int lx = idx % TS::PX, ly = idx / TS::PX;
+      const int xi = i0 - 2 + lx, yj = j0 - 2 + ly;
+      double v[NF];
+      bool ok = xi <= c.mx + 1 && yj <= c.my + 1 && kk >= -2 && kk <= c.mz + 1;
+      if (ok) {
+        const long long g = gidx(c, xi, yj, kk);
+#pragma unroll
+        for (int q = 0; q < 5; q++) v[q] = ldg(F.q[q] + g);
+      }
+      if (ok && v[0] != 0.0) {
+        const double r = v[0];
+        v[F_P] = (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / r);  // rhs.c:4850
+        v[F_U] = v[1] / r;
+        v[F_V] = v[2] / r;
+        v[F_W] = v[3] / r;
+        v[F_T] = v[F_P] / r;
+      } else {
+#pragma unroll
+        for (int q = 0; q < NF; q++) v[q] = 0.0;
+      }
+      double *base = R.pl + (size_t)s * NF * TS::PN + idx;
+#pragma unroll
+      for (int q = 0; q < NF; q++) base[(size_t)q * TS::PN] = v[q];
+    }
+  };
+
+  // combined face value G = Fvisc - Fconv (5) plus LES stress part (3)
+  auto face = [&](int d, NRef a, int fi, int fj, int fk, double G[NG]) {
+    double Fc[5];
+    conv_face<LES, BX, BY>(c, F, R, d, a, fi, fj, fk, Fc);
+    double Fv[5] = {0., 0., 0., 0., 0.}, A[3] = {0., 0., 0.};
+    if (VISC) visc_face<LES, BX, BY>(c, F, R, d, a, fi, fj, fk, Fv, A);
+#pragma unroll
+    for (int q = 0; q < 5; q++) G[q] = Fv[q] - Fc[q];
+    G[5] = A[0]; G[6] = A[1]; G[7] = A[2];
+  };
+
+  // prologue: planes kb-2 .. kb+1, then the k-face kb-1/2
+  for (int r = -1; r < 3; r++) R.slot[r + 1] = (r + 1) & 3;
+  // slots: plane kb-2 -> slot of r=-1 shifted; set ring so that r=-1 is kb-2 for the prologue
+  load_plane(kb - 2, 0);
+  load_plane(kb - 1, 1);
+  load_plane(kb, 2);
+  load_plane(kb + 1, 3);
+  __syncthreads();
+  double Gz[NG];  // face k-1/2 of the current plane
+  {
+    // ring view for the prologue: r=-1 -> kb-2 (slot 0), r=0 -> kb-1 (slot 1), ...
+    R.slot[0] = 0; R.slot[1] = 1; R.slot[2] = 2; R.slot[3] = 3;
+    if (active) face(2, NRef{0, ty + 2, tx + 2}, gi, gj, kb - 1, Gz);
+  }
+  __syncthreads();
+  load_plane(kb + 2, 0);  // slot 0 now holds kb+2
+  __syncthreads();
+  int base = 1;  // slot of plane k-1
+
+  for (int k = kb; k < ke; k++) {
+    R.slot[0] = base & 3; R.slot[1] = (base + 1) & 3; R.slot[2] = (base + 2) & 3; R.slot[3] = (base + 3) & 3;
+    // i-faces of plane k: left node x = i0-1+fx, row j0+fy
+    for (int f = tid; f < TS::NXF; f += nthr) {
+      const int fx = f % (BX + 1), fy = f / (BX + 1);
+      const int fi = i0 - 1 + fx, fj = j0 + fy;
+      double G[NG];
+      if (fi <= c.mx - 2 && fj <= c.my - 2) face(0, NRef{0, fy + 2, fx + 1}, fi, fj, k, G);
+      else {
+#pragma unroll
+        for (int q = 0; q < NG; q++) G[q] = 0.;
+      }
+#pragma unroll
+      for (int q = 0; q < NG; q++) gxb[(size_t)q * TS::NXF + f] = G[q];
+    }
+    // j-faces of plane k: lower node row j0-1+fy, column i0+fx
+    for (int f = tid; f < TS::NYF; f += nthr) {
+      const int fx = f % BX, fy = f / BX;
+      const int fi = i0 + fx, fj = j0 - 1 + fy;
+      double G[NG];
+      if (fi <= c.mx - 2 && fj <= c.my - 2) face(1, NRef{0, fy + 1, fx + 2}, fi, fj, k, G);
+      else {
+#pragma unroll
+        for (int q = 0; q < NG; q++) G[q] = 0.;
+      }
+#pragma unroll
+      for (int q = 0; q < NG; q++) gyb[(size_t)q * TS::NYF + f] = G[q];
+    }
+    // k-face k+1/2
+    double Gzn[NG];
+    if (active) face(2, NRef{0, ty + 2, tx + 2}, gi, gj, k, Gzn);
+    __syncthreads();
+
+    if (active) {
+      const long long g = gidx(c, gi, gj, k);
+      const double nv = ldg(F.nvert + g);
+      const int fxr = ty * (BX + 1) + tx + 1, fxl = fxr - 1;  // i+1/2, i-1/2
+      const int fyu = (ty + 1) * BX + tx, fyd = ty * BX + tx; // j+1/2, j-1/2
+      double rhs[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        // (Fv - Fc) differences: visc - conv of the reference, summed per direction
+        const double dx = gxb[(size_t)q * TS::NXF + fxr] - gxb[(size_t)q * TS::NXF + fxl];
+        const double dy = gyb[(size_t)q * TS::NYF + fyu] - gyb[(size_t)q * TS::NYF + fyd];
+        const double dz = Gzn[q] - Gz[q];
+        rhs[q] = dx + dy + dz;
+      }
+      if (LES) {
+        const NRef n{0, ty + 2, tx + 2};
+        const double aj = ldg(F.aj + g);
+        if (nv < BLANK) {  // channel forcing terms (rhs.c:4226-4235), zero unless ratio != 0
+          rhs[3] += c.ratio / aj * R.get(F_RHO, n) / c.dt;
+          rhs[4] += c.ratio / aj * R.get(F_RW, n) / c.dt;
+        }
+        if (VISC && gj > 2 && gj < c.my - 2 && nv < 0.5) {  // rhs.c:2153-2197
+          const double r0 = R.get(F_RHO, n);
+          const double rL = (r0 + R.get(F_RHO, nshift(n, 0, -1))) * 0.5, rR = (R.get(F_RHO, nshift(n, 0, 1)) + r0) * 0.5;
+          const double rD = (r0 + R.get(F_RHO, nshift(n, 1, -1))) * 0.5, rU = (R.get(F_RHO, nshift(n, 1, 1)) + r0) * 0.5;
+          const double rB = (r0 + R.get(F_RHO, nshift(n, 2, -1))) * 0.5, rF = (R.get(F_RHO, nshift(n, 2, 1)) + r0) * 0.5;
+          double e = 0.;
+#pragma unroll
+          for (int q = 0; q < 3; q++) {
+            const double t = rR * gxb[(size_t)(5 + q) * TS::NXF + fxr] - rL * gxb[(size_t)(5 + q) * TS::NXF + fxl] +
+                             rU * gyb[(size_t)(5 + q) * TS::NYF + fyu] - rD * gyb[(size_t)(5 + q) * TS::NYF + fyd] +
+                             rF * Gzn[5 + q] - rB * Gz[5 + q];
+            e += R.get(F_U + q, n) * t;
+          }
+          rhs[4] += e;
+        }
+      }
+      const double aj = ldg(F.aj + g);
+#pragma unroll
+      for (int q = 0; q < 5; q++) rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;
+      if (RHS_MODE) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) F.rhs[q][g] = rhs[q];
+      } else {
+        const NRef n{0, ty + 2, tx + 2};
+        double out[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+          const double qo = ldg(F.qold[q] + g);
+          out[q] = (istage == 0) ? qo + adt * rhs[q] : beta * qo + adt * rhs[q] + alfa * R.get(F_RHO + q, n);
+          F.qout[q][g] = out[q];
+        }
+        // EqOfState sanity (rhs.c:4862 prints p<0): sticky status instead
+        const double p = (c.gamma - 1) * (out[4] - 0.5 * (out[1] * out[1] + out[2] * out[2] + out[3] * out[3]) / out[0]);
+        unsigned st = 0;
+        if (!isfinite(out[0] + out[1] + out[2] + out[3] + out[4])) st |= ST_NONFINITE;
+        if (!(out[0] > 0.)) st |= ST_NEG_RHO;
+        if (!(p > 0.)) st |= ST_NEG_P;
+        if (st) atomicOr(F.status, st);
+      }
+#pragma unroll
+      for (int q = 0; q < NG; q++) Gz[q] = Gzn[q];
+    }
+    __syncthreads();
+    // advance the ring: plane k-1's slot receives k+3
+    if (k + 1 < ke) load_plane(k + 3, base & 3);
+    base++;
+    __syncthreads();
+  }
+}
+
+}  // namespace cb

@@ -1,0 +1,200 @@
+"""Host-side mirror of the reference's hot-path interface over the C-ABI.
+
+``Block`` is one DMDA block of the reference resident on a B200.  Its methods
+carry the names of the reference functions they replace and take/return the
+arrays behind the reference's PETSc global Vecs as numpy arrays in natural
+AoS order (mz, my, mx, ncomp):
+
+  FormMetrics(coor)                  metrics.c:3      (cb_set_grid)
+  SetInitialCondition(Q)             rhs.c:420-433    (cb_upload_state)
+  formRHS(istage)                    rhs.c:4703       (cb_rhs)
+  CalcUCat()                         rhs.c:1322       (cb_calc_ucat)
+  Compute_eddy_viscosity_LES()       les.c:1477       (cb_eddy_viscosity)
+  RungeKutta(nsteps) / Flow_Solver   solvers.c:13,223 (cb_rk_step)
+  EqOfState()                        rhs.c:4820       (pressure download)
+
+Options may be given as the reference's command-line flags via
+``Block.from_options``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import shlex
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import CbConfig, ChimeraError, dptr
+
+_OPT_MAP = {
+    "-les": ("les", int), "-inv": ("inviscid", int), "-fluxorder": ("fluxorder", int),
+    "-ENOorder": ("eno_order", int), "-central": ("central", int), "-isothermal": ("isothermal", int),
+    "-s_x": ("s_x", float), "-s_y": ("s_y", float), "-s_z": ("s_z", float), "-ren": ("ren", float),
+    "-Ma": ("ma", float), "-Pr": ("pr", float), "-gamma": ("gamma", float), "-dt": ("dt", float),
+}
+
+
+def _f64(a: np.ndarray, shape) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.shape != tuple(shape):
+        a = a.reshape(shape)
+    return a
+
+
+class Block:
+    """One curvilinear block of the reference's solver, resident on one GPU."""
+
+    def __init__(self, mx: int, my: int, mz: int, bctype: Sequence[int] = (7, 7, 7, 7, 7, 7), les: int = 0,
+                 inviscid: int = 0, fluxorder: int = 3, eno_order: int = 2, central: int = 2,
+                 isothermal: int = 0, s_x: float = 1.0, s_y: float = 1.0, s_z: float = 1.0,
+                 ren: float = 3000.0, ma: float = 2.81, pr: float = 0.72, gamma: float = 1.4,
+                 dt: float = 0.01, st: float = 1.0, cs_const: float = 0.03, ci: float = 0.06,
+                 ratio: float = 0.0, precision: str = "fp64", device: int = 0):
+        self.lib = _lib.load()
+        cfg = CbConfig()
+        self.lib.cb_config_default(C.byref(cfg), mx, my, mz)
+        cfg.bctype = (C.c_int * 6)(*bctype)
+        for k, v in dict(les=les, inviscid=inviscid, fluxorder=fluxorder, eno_order=eno_order, central=central,
+                         isothermal=isothermal, s_x=s_x, s_y=s_y, s_z=s_z, ren=ren, ma=ma, pr=pr, gamma=gamma,
+                         dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device).items():
+            setattr(cfg, k, v)
+        cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]
+        self.cfg = cfg
+        self.shape = (mz, my, mx)
+        self._ctx = C.c_void_p()
+        rc = self.lib.cb_create(C.byref(cfg), C.byref(self._ctx))
+        if rc != 0:
+            raise ChimeraError(rc, "cb_create failed (see stderr)")
+
+    @classmethod
+    def from_options(cls, mx: int, my: int, mz: int, options: str, bctype=(7, 7, 7, 7, 7, 7), **kw) -> "Block":
+        """Build from the reference's option flags, e.g. "-les 1 -fluxorder 2 -ren 1600"."""
+        toks = shlex.split(options)
+        args = dict(kw)
+        for name, val in zip(toks[::2], toks[1::2]):
+            if name in _OPT_MAP:
+                key, typ = _OPT_MAP[name]
+                args[key] = typ(val)
+        return cls(mx, my, mz, bctype=bctype, **args)
+
+    # ------------------------------------------------------------ helpers --
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self.lib.cb_last_error(self._ctx)
+            raise ChimeraError(rc, msg.decode() if msg else "")
+
+    @property
+    def nnodes(self) -> int:
+        mz, my, mx = self.shape
+        return mx * my * mz
+
+    @property
+    def interior_nodes(self) -> int:
+        return int(self.lib.cb_interior_nodes(self._ctx))
+
+    @property
+    def stages(self) -> int:
+        return int(self.lib.cb_stages(self._ctx))
+
+    @property
+    def launches_per_step(self) -> int:
+        return int(self.lib.cb_launches_per_step(self._ctx))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.cb_stream(self._ctx) or 0)
+
+    # ----------------------------------------------------- reference calls --
+    def FormMetrics(self, coor: np.ndarray):
+        c = _f64(coor, self.shape + (3,))
+        self._check(self.lib.cb_set_grid(self._ctx, dptr(c)))
+
+    def set_metrics(self, csi, eta, zet, aj):
+        a = [_f64(x, self.shape + (3,)) for x in (csi, eta, zet)] + [_f64(aj, self.shape)]
+        self._check(self.lib.cb_set_metrics(self._ctx, *[dptr(x) for x in a]))
+
+    def metrics(self):
+        """(csi, eta, zet, aj) as resident on the device, natural AoS order."""
+        csi, eta, zet = (np.empty(self.shape + (3,)) for _ in range(3))
+        aj = np.empty(self.shape)
+        self._check(self.lib.cb_get_metrics(self._ctx, dptr(csi), dptr(eta), dptr(zet), dptr(aj)))
+        return csi, eta, zet, aj
+
+    def set_nvert(self, nvert: np.ndarray):
+        n = _f64(nvert, self.shape)
+        self._check(self.lib.cb_set_nvert(self._ctx, dptr(n)))
+
+    def SetInitialCondition(self, q: np.ndarray):
+        a = _f64(q, self.shape + (5,))
+        self._check(self.lib.cb_upload_state(self._ctx, dptr(a)))
+        self._check(self.lib.cb_sync(self._ctx))
+
+    upload_state = SetInitialCondition
+
+    def formRHS(self, istage: int = 0) -> np.ndarray:
+        out = np.empty(self.shape + (5,))
+        self._check(self.lib.cb_rhs(self._ctx, istage, dptr(out)))
+        return out
+
+    def CalcUCat(self):
+        self._check(self.lib.cb_calc_ucat(self._ctx))
+
+    def Compute_eddy_viscosity_LES(self):
+        self._check(self.lib.cb_eddy_viscosity(self._ctx))
+
+    def nu_t(self) -> np.ndarray:
+        out = np.empty(self.shape)
+        self._check(self.lib.cb_get_nut(self._ctx, dptr(out)))
+        return out
+
+    def RungeKutta(self, nsteps: int = 1, sync: bool = True):
+        self._check(self.lib.cb_rk_step(self._ctx, int(nsteps)))
+        if sync:
+            self.sync()
+
+    Flow_Solver = RungeKutta
+
+    def sync(self):
+        self._check(self.lib.cb_sync(self._ctx))
+
+    def Q(self) -> np.ndarray:
+        out = np.empty(self.shape + (5,))
+        self._check(self.lib.cb_download_state(self._ctx, dptr(out), None))
+        return out
+
+    def EqOfState(self) -> np.ndarray:
+        q = np.empty(self.shape + (5,))
+        p = np.empty(self.shape)
+        self._check(self.lib.cb_download_state(self._ctx, dptr(q), dptr(p)))
+        return p
+
+    def download(self, q_out: np.ndarray, p_out: Optional[np.ndarray] = None):
+        self._check(self.lib.cb_download_state(self._ctx, dptr(q_out), dptr(p_out)))
+
+    # --------------------------------------------------------------- timing --
+    def timing(self, on: bool):
+        self._check(self.lib.cb_timing_enable(self._ctx, 1 if on else 0))
+
+    def timing_read(self):
+        a, b = C.c_double(), C.c_double()
+        na, nb = C.c_int(), C.c_int()
+        self._check(self.lib.cb_timing_read(self._ctx, C.byref(a), C.byref(na), C.byref(b), C.byref(nb)))
+        return a.value, na.value, b.value, nb.value
+
+    def close(self):
+        if self._ctx:
+            self.lib.cb_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

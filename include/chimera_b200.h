@@ -1,0 +1,159 @@
+/*
+ * chimera_b200.h -- C-ABI of libchimera_b200.so, the B200 (sm_100a) drop-in for
+ * the compressible right-hand side and SSP-RK time advance of
+ * madvait/Chimera_Comp_LES.
+ *
+ * The reference's host code keeps its PETSc vectors; it hands this library
+ * plain pointers to the arrays behind them (VecGetArray of the GLOBAL Vecs on
+ * one rank: AoS, natural k-j-i order, i fastest) and sizes.  State, metrics,
+ * nvert mask and eddy viscosity stay resident on the GPU between calls.
+ *
+ * Conventions
+ *   - Node counts mx,my,mz include the boundary nodes 0 and m-1, exactly as the
+ *     reference's DMDA (init.c:206-218).  A periodic direction with N unique
+ *     points has m = N+2 nodes (node 0 images node m-2, node m-1 images node 1).
+ *   - Q is 5 doubles per node (rho, rhoU, rhoV, rhoW, rhoE) -- CompVars,
+ *     variables.h:22-24.  Metrics are 3 doubles per node (Cmpnts).
+ *   - Every function returns 0 on success or a CB_E* code; cb_last_error()
+ *     gives a one-line message.  Calls on one context are stream-ordered and
+ *     not thread-safe (one context per host thread, as the reference runs one
+ *     rank per process).
+ *   - No function allocates device memory except cb_create, cb_rhs (first
+ *     call: its output planes) and cb_capture_graph (graph instantiation).
+ */
+#ifndef CHIMERA_B200_H
+#define CHIMERA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CB_ABI_VERSION 1
+
+/* status codes */
+#define CB_OK 0
+#define CB_E_ARG 1          /* invalid argument / unsupported option combination */
+#define CB_E_CUDA 2         /* CUDA runtime error (message in cb_last_error) */
+#define CB_E_STATE 3        /* call out of order (e.g. step before grid/state upload) */
+#define CB_E_NONFINITE 4    /* device status: NaN/Inf or rho<=0 / p<=0 seen */
+#define CB_E_UNSUPPORTED 5  /* option valid in the reference but not built here */
+
+/* precision forms */
+#define CB_FP64 0   /* FP64 throughout (parity form) */
+#define CB_MIXED 1  /* FP32 flux arithmetic, FP64 state / EOS / RK combine / metrics */
+
+/* Options the reference reads from its PETSc options database on the hot
+ * path; names in the comments are the reference's command-line flags. */
+typedef struct {
+  int mx, my, mz;       /* -im/-jm/-km (DMDA node counts) */
+  int bctype[6];        /* bcs.dat: i-lo,i-hi,j-lo,j-hi,k-lo,k-hi; 7 = periodic */
+  int les;              /* -les     : 0 off, 1 constant Smagorinsky */
+  int inviscid;         /* -inv     : 1 skips formViscous */
+  int fluxorder;        /* -fluxorder: 1 first order, 2 MUSCL-minmod, 3 WENO3; also the RK stage count */
+  int eno_order;        /* -ENOorder: 2 or 3 */
+  int central;          /* -central : 2 skew-symmetric 4-point, 3 Fp_1, other: 2-point average */
+  int isothermal;       /* -isothermal */
+  double s_x, s_y, s_z; /* -s_x -s_y -s_z: hybrid central weights (sensor off) */
+  double ren;           /* -ren : Reynolds number */
+  double ma;            /* -Ma  */
+  double pr;            /* -Pr  */
+  double gamma;         /* -gamma (EOS; the reference's flux code fixes 1.4) */
+  double dt;            /* -dt  */
+  double st;            /* Strouhal scaling of dt (init.c:98 sets 1) */
+  double cs_const;      /* constant Smagorinsky coefficient (les.c:146 fixes 0.03) */
+  double ci;            /* Yoshizawa constant (rhs.c:13: 0.06) */
+  double ratio;         /* channel forcing ratio (0 unless channel/wavy) */
+  int precision;        /* CB_FP64 or CB_MIXED */
+  int device;           /* CUDA device ordinal */
+} cb_config;
+
+/* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */
+void cb_config_default(cb_config *cfg, int mx, int my, int mz);
+
+typedef struct cb_ctx cb_ctx;
+
+/* Creates a context and allocates the resident device arrays.
+ * Replaces the vector set-up of MG_Initial (init.c:956-1090). */
+int cb_create(const cb_config *cfg, cb_ctx **out);
+void cb_destroy(cb_ctx *ctx);
+
+/* Node coordinates (3 doubles per node, AoS) -> metrics on the device.
+ * Replaces FormMetrics (metrics.c:3-782). */
+int cb_set_grid(cb_ctx *ctx, const double *coor);
+
+/* Host-computed metrics instead (lCsi/lEta/lZet: 3 doubles per node, lAj: 1),
+ * global (unghosted) natural order. */
+int cb_set_metrics(cb_ctx *ctx, const double *csi, const double *eta, const double *zet, const double *aj);
+
+/* Metrics currently resident (lCsi/lEta/lZet 3 per node, lAj 1 per node),
+ * global natural order -- what FormMetrics left in the reference's vectors. */
+int cb_get_metrics(cb_ctx *ctx, double *csi, double *eta, double *zet, double *aj);
+
+/* IBM mask, 1 double per node (Nvert, variables.h:191).  Re-upload only when
+ * the body moves (ibm_search_advanced, ibm_iso.c:87). */
+int cb_set_nvert(cb_ctx *ctx, const double *nvert);
+
+/* Conserved state Q (5 doubles per node).  Sets Q and Qold, as the tail of
+ * SetInitialCondition does (rhs.c:420-433); the eddy viscosity and the
+ * velocity field of the last CalcUCat are reset to zero. */
+int cb_upload_state(cb_ctx *ctx, const double *q);
+
+/* Copies Q (5 per node) and, if p != NULL, the EOS pressure (1 per node) back.
+ * Replaces reading user->Q / user->P after RungeKutta. */
+int cb_download_state(cb_ctx *ctx, double *q, double *p);
+
+/* formRHS(user, Rhs, istage) (rhs.c:4703) on the current state: writes Rhs,
+ * 5 doubles per node, zero on boundary nodes.  In LES mode the current eddy
+ * viscosity is used (see cb_eddy_viscosity). */
+int cb_rhs(cb_ctx *ctx, int istage, double *rhs);
+
+/* CalcUCat (rhs.c:1322): records the current state as the velocity source of
+ * the next eddy-viscosity evaluation. */
+int cb_calc_ucat(cb_ctx *ctx);
+
+/* Compute_Smagorinsky_Constant_1 + Compute_eddy_viscosity_LES
+ * (les.c:135-150, 1477-1661) from the recorded velocity field. */
+int cb_eddy_viscosity(cb_ctx *ctx);
+
+/* Eddy viscosity Nu_t (1 double per node, global order). */
+int cb_get_nut(cb_ctx *ctx, double *nut);
+
+/* nsteps physical time steps: per step Flow_Solver (solvers.c:13-64: LES
+ * eddy viscosity, then RungeKutta solvers.c:223-294 with FormBCS and
+ * EqOfState per stage) and the Q -> Qold copy of main.c:971.  Asynchronous on
+ * the context's stream; returns after enqueueing. */
+int cb_rk_step(cb_ctx *ctx, int nsteps);
+
+/* Waits for the context's stream and checks the device status word
+ * (CB_E_NONFINITE when a NaN/Inf or non-positive rho/p was produced). */
+int cb_sync(cb_ctx *ctx);
+
+/* Captures one full time step into a CUDA graph; later cb_rk_step calls
+ * replay it.  Returns CB_E_STATE if the state/grid are not set. */
+int cb_capture_graph(cb_ctx *ctx);
+
+/* The CUDA stream all work of this context is enqueued on (cudaStream_t). */
+void *cb_stream(cb_ctx *ctx);
+
+/* Per-kernel timing with CUDA events on the context stream (0: off, 1: on).
+ * cb_timing_read returns the summed milliseconds and launch count of the
+ * fused RHS/stage kernel since it was enabled, and of the whole step. */
+int cb_timing_enable(cb_ctx *ctx, int on);
+int cb_timing_read(cb_ctx *ctx, double *rhs_ms, int *rhs_launches, double *other_ms, int *other_launches);
+
+/* Number of interior nodes ((mx-2)(my-2)(mz-2)) and RK stages per step. */
+long long cb_interior_nodes(const cb_ctx *ctx);
+int cb_stages(const cb_ctx *ctx);
+
+/* Kernel launches one cb_rk_step(ctx, 1) enqueues. */
+int cb_launches_per_step(const cb_ctx *ctx);
+
+const char *cb_last_error(const cb_ctx *ctx);
+int cb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -30,6 +30,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(_HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(_HERE, "_ref", "libchimera_ref.so")
+REF_SO_O3 = os.path.join(_HERE, "_ref", "libchimera_ref_O3.so")
 REF_SRC_DIR = os.environ.get("CHIMERA_REF_DIR", "/root/reference")
 
 
@@ -239,21 +240,22 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO) or os.path.isdir(REF_SRC_DIR)
 
 
-def build_ref(force: bool = False) -> str:
-    if force or not os.path.exists(REF_SO):
+def build_ref(force: bool = False, optimized: bool = False) -> str:
+    so = REF_SO_O3 if optimized else REF_SO
+    if force or not os.path.exists(so):
         if not os.path.isdir(REF_SRC_DIR):
             raise FileNotFoundError("reference sources not present; cannot build oracle/_ref")
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_DIR={REF_SRC_DIR}"], check=True)
-    return REF_SO
+    return so
 
 
 class RefOracle:
     """The reference's own hot-path C (via the PETSc shim); one live instance
     per process (the reference keeps its state in globals)."""
 
-    def __init__(self, cfg: Config, coords_nat: np.ndarray):
+    def __init__(self, cfg: Config, coords_nat: np.ndarray, optimized: bool = False):
         self.cfg = cfg
-        self.lib = C.CDLL(build_ref())
+        self.lib = C.CDLL(build_ref(optimized=optimized))
         L = self.lib
         D = C.POINTER(C.c_double)
         L.ref_setup.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), D, C.c_char_p]

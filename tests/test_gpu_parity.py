@@ -1,0 +1,161 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the reference's own
+outputs (golden fixtures) and against the oracle restatement.
+
+Bar (FP64 form): per conserved field, relative L2 <= 1e-12 (RTOL_L2).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from chimera_comp_les_b200 import ChimeraError
+from chimera_comp_les_b200 import workloads as W
+
+from _common import RTOL_L2, golden_names, gpu_block, load_golden, oracle_run, per_field_rel_l2
+
+pytestmark = pytest.mark.gpu
+
+NAMES = golden_names()
+
+
+def _setup(cfg, coords, q, nvert):
+    b = gpu_block(cfg)
+    b.FormMetrics(coords)
+    b.set_nvert(nvert)
+    b.SetInitialCondition(q)
+    return b
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_device_metrics_match_reference(name):
+    cfg, meta, g = load_golden(name)
+    with _setup(cfg, g["coords"], g["q"], g["nvert"]) as b:
+        csi, eta, zet, aj = b.metrics()
+    for k, got in (("csi", csi), ("eta", eta), ("zet", zet), ("aj", aj)):
+        ref = g["metrics_" + k].reshape(got.shape)
+        assert O.rel_l2(got, ref) <= 1e-14, k
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_rhs_matches_reference(name):
+    cfg, meta, g = load_golden(name)
+    with _setup(cfg, g["coords"], g["q"], g["nvert"]) as b:
+        if cfg.les and not cfg.inviscid:
+            b.CalcUCat()
+            b.Compute_eddy_viscosity_LES()
+            nut = b.nu_t()
+            assert O.rel_l2(nut, g["nut"]) <= RTOL_L2
+        rhs = b.formRHS(0)
+    errs = per_field_rel_l2(rhs, g["rhs"])
+    assert max(errs) <= RTOL_L2, errs
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_time_steps_match_reference(name):
+    cfg, meta, g = load_golden(name)
+    with _setup(cfg, g["coords"], g["q"], g["nvert"]) as b:
+        b.RungeKutta(meta["steps"])
+        q = b.Q()
+    errs = per_field_rel_l2(q, g["q_steps"])
+    assert max(errs) <= RTOL_L2, errs
+
+
+# Odd sizes: several tiles in i and j, several k chunks, partial tiles.
+ORACLE_CASES = [
+    ("les_visc_muscl", (37, 21, 26), dict(les=1, inviscid=0, fluxorder=2, ren=1600., ma=0.1, pr=0.71, dt=0.002), False),
+    ("les_visc_weno_mask", (33, 17, 23), dict(les=1, inviscid=0, fluxorder=3, s_x=0.2, s_y=0.5, s_z=0.9, ren=500., ma=0.3, pr=0.71, dt=0.002), True),
+    ("std_visc_weno_mask", (35, 41, 20), dict(les=0, inviscid=0, fluxorder=3, ren=500., ma=0.3, pr=0.71, dt=0.002), True),
+    ("std_inv_muscl", (40, 12, 31), dict(les=0, inviscid=1, fluxorder=2, dt=0.002), False),
+]
+
+
+def _mask(shape, seed):
+    rng = np.random.default_rng(seed)
+    mz, my, mx = shape
+    z, y, x = np.meshgrid(np.arange(mz), np.arange(my), np.arange(mx), indexing="ij")
+    nv = np.zeros(shape)
+    for _ in range(3):
+        c = rng.uniform(4, np.array([mx, my, mz]) - 4)
+        r = np.sqrt((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2)
+        nv[r < 3.0] = np.maximum(nv[r < 3.0], 1.0)
+        nv[r < 1.9] = 3.0
+    return nv
+
+
+@pytest.mark.parametrize("name,n,kw,mask", ORACLE_CASES, ids=[c[0] for c in ORACLE_CASES])
+def test_rhs_and_steps_match_oracle(name, n, kw, mask):
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, **kw)
+    q = W.random_smooth_state(shape, seed=11)
+    nv = _mask(shape, 5) if mask else np.zeros(shape)
+    ref = oracle_run(cfg, coords, q, nv, steps=2)
+    with _setup(cfg, coords, q, nv) as b:
+        if cfg.les and not cfg.inviscid:
+            b.CalcUCat()
+            b.Compute_eddy_viscosity_LES()
+            assert O.rel_l2(b.nu_t(), ref["nut"]) <= RTOL_L2
+        rhs = b.formRHS(0)
+        assert max(per_field_rel_l2(rhs, ref["rhs"])) <= RTOL_L2
+    with _setup(cfg, coords, q, nv) as b:
+        b.RungeKutta(2)
+        assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= RTOL_L2
+
+
+def test_tgv_full_size_parity():
+    """Viscous LES of the compressible TGV at 128^3 (m = 130^3), curvilinear
+    perturbed grid: one RHS and one time step against the oracle."""
+    n = 128
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    cfg = O.Config(mx=n + 2, my=n + 2, mz=n + 2, les=1, inviscid=0, fluxorder=2, ren=1600., ma=0.1,
+                   pr=0.71, gamma=1.4, dt=1e-3)
+    q = W.tgv_state(coords, gamma=1.4, ma=0.1)
+    nv = np.zeros(coords.shape[:3])
+    ref = oracle_run(cfg, coords, q, nv, steps=1)
+    with _setup(cfg, coords, q, nv) as b:
+        b.CalcUCat()
+        b.Compute_eddy_viscosity_LES()
+        rhs = b.formRHS(0)
+    assert max(per_field_rel_l2(rhs, ref["rhs"])) <= RTOL_L2
+    with _setup(cfg, coords, q, nv) as b:
+        b.RungeKutta(1)
+        q1 = b.Q()
+    assert max(per_field_rel_l2(q1, ref["q_steps"])) <= RTOL_L2
+
+
+def test_graph_replay_equals_eager_launches():
+    n = (30, 20, 18)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=1, inviscid=0, fluxorder=3, ren=800., ma=0.2,
+                   pr=0.71, dt=0.002)
+    q = W.random_smooth_state(coords.shape[:3], seed=3)
+    nv = np.zeros(coords.shape[:3])
+    with _setup(cfg, coords, q, nv) as b:
+        b.RungeKutta(7)  # graphs captured and replayed
+        qa = b.Q()
+    with _setup(cfg, coords, q, nv) as b:
+        b.timing(True)   # timing forces eager launches
+        b.RungeKutta(7)
+        qb = b.Q()
+    assert np.array_equal(qa, qb)
+
+
+def test_nonfinite_state_reports_status_not_fault():
+    """Host-side fault injection: a NaN in the uploaded state makes the step
+    report CB_E_NONFINITE through the device status word."""
+    n = (16, 12, 10)
+    coords = W.periodic_grid(n, 2 * np.pi)
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=0, inviscid=1, fluxorder=2, dt=0.001)
+    q = W.random_smooth_state(coords.shape[:3], seed=1)
+    q[5, 6, 7, 4] = np.nan
+    with _setup(cfg, coords, q, np.zeros(coords.shape[:3])) as b:
+        with pytest.raises(ChimeraError) as ei:
+            b.RungeKutta(1)
+        assert ei.value.code == 4
+        # the context stays usable after the error
+        b.SetInitialCondition(W.random_smooth_state(coords.shape[:3], seed=2))
+        b.RungeKutta(1)
+
+
+def test_unsupported_options_fail_loudly():
+    with pytest.raises(ChimeraError):
+        gpu_block(O.Config(mx=12, my=12, mz=12, bctype=(1, 1, 7, 7, 7, 7)))
