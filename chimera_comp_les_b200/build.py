@@ -15,9 +15,11 @@ REPO = os.path.dirname(PKG_DIR)
 LIB_PATH = os.path.join(PKG_DIR, "libchimera_b200.so")
 SOURCES = [os.path.join(PKG_DIR, "csrc", "cb_api.cu")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+# The FP64 form reproduces the reference's IEEE operation order: no FMA
+# contraction (-fmad=false), IEEE division and square root.
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17",
+    "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
     "-Xcompiler", "-fPIC", "-shared",
 ]
 

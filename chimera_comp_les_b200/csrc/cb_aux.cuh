@@ -93,7 +93,7 @@ __global__ void eddy_viscosity_kernel(const DevCfg c, const double *const *qu, c
     const double Sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Sxy * Sxy + Syy * Syy + Syz * Syz + Sxz * Sxz +
                                     Syz * Syz + Szz * Szz));
     const double filter = pow(1. / ajc, 1. / 3.);
-    nut[n] = c.cs_const * (filter * filter) * Sabs;
+    nut[n] = c.cs_const * pow(filter, 2.0) * Sabs;
   }
 }
 

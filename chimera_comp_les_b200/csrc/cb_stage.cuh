@@ -23,7 +23,7 @@ namespace cb {
 
 constexpr int NF = 10;  // fields per node in the plane ring
 enum { F_RHO = 0, F_RU, F_RV, F_RW, F_RE, F_P, F_U, F_V, F_W, F_T };
-constexpr int NG = 8;   // per face: G[0..4] = Fvisc - Fconv, A[0..2] = LES stress part
+constexpr int NG = 13;  // per face: Fconv[0..4], Fvisc[5..9], LES stress part A[10..12]
 
 constexpr double BLANKWALL = 2.9;
 constexpr double BLANK = 0.1;
@@ -96,15 +96,15 @@ __device__ __forceinline__ double eno_l(double qm, double q0, double qp, int k) 
   return qm * 0.3333333333333333 + q0 * 0.8333333333333333 - qp * 0.1666666666666666;
 }
 
-// Rusanov flux on reconstructed states (rhs.c:2769-2810).
+// Rusanov flux on reconstructed states (rhs.c:2769-2810), same operation
+// order as the reference (divisions, no reciprocal reuse).
 __device__ __forceinline__ void rusanov(const double QL[5], const double QR[5], double pL, double pR,
                                         const double h[3], bool use_qr_for_l, bool r_from_l, double F[5]) {
-  double iL = 1.0 / QL[0], iR = 1.0 / QR[0];
-  double uconL = use_qr_for_l ? (h[0] * (QR[1] * iR) + h[1] * (QR[2] * iR) + h[2] * (QR[3] * iR))
-                              : (h[0] * (QL[1] * iL) + h[1] * (QL[2] * iL) + h[2] * (QL[3] * iL));
-  double uconR = r_from_l ? uconL : (h[0] * (QR[1] * iR) + h[1] * (QR[2] * iR) + h[2] * (QR[3] * iR));
+  double uconL = use_qr_for_l ? (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]))
+                              : (h[0] * (QL[1] / QL[0]) + h[1] * (QL[2] / QL[0]) + h[2] * (QL[3] / QL[0]));
+  double uconR = r_from_l ? uconL : (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
   double gii = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
-  double cL = GAMMA_CONV * pL * iL, cR = GAMMA_CONV * pR * iR;
+  double cL = GAMMA_CONV * pL / QL[0], cR = GAMMA_CONV * pR / QR[0];
   double saL = fabs(uconL) + sqrt(fabs(cL) * gii);
   double saR = fabs(uconR) + sqrt(fabs(cR) * gii);
   double SA = (saL < saR) ? saR : saL;
@@ -344,9 +344,12 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   const double tv = g11 * dvdc + g21 * dvde + g31 * dvdz + r12 * md0 + r22 * md1 + r32 * md2;
   const double tw = g11 * dwdc + g21 * dwde + g31 * dwdz + r13 * md0 + r23 * md1 + r33 * md2;
   Fv[0] = 0.;
-  Fv[1] = tu * ajc * nu - div * md0 * ajc * nu;
-  Fv[2] = tv * ajc * nu - div * md1 * ajc * nu;
-  Fv[3] = tw * ajc * nu - div * md2 * ajc * nu;
+  Fv[1] = tu * ajc * (nu);
+  Fv[2] = tv * ajc * (nu);
+  Fv[3] = tw * ajc * (nu);
+  Fv[1] -= div * md0 * ajc * nu;
+  Fv[2] -= div * md1 * ajc * nu;
+  Fv[3] -= div * md2 * ajc * nu;
 
   double uh[3];
   if (pos == 0 && c.bctype[2 * d] == 1) {
@@ -378,7 +381,7 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
     const double S2 = .5 * ((r11 - div) * (r11 - div) + r12 * r12 + r13 * r13 + r21 * r21 + (r22 - div) * (r22 - div) +
                             r23 * r23 + r31 * r31 + r32 * r32 + (r33 - div) * (r33 - div));
     const double filter = pow(1. / ldg(F.aj + g0), 1. / 3.);
-    const double pf = filter * filter;
+    const double pf = pow(filter, 2.0);
     const double sgs = -S2 * pf * c.ci * 2.0 / 3.0;
     A[0] = tx + sgs * md0 * rho_c * sigma_c;
     A[1] = ty + sgs * md1 * rho_c * sigma_c;
@@ -438,15 +441,15 @@ __global__ void __launch_bounds__(BX *BY, 1)
     }
   };
 
-  // combined face value G = Fvisc - Fconv (5) plus LES stress part (3)
+  // face value: inviscid flux (5), viscous flux (5), LES stress part (3)
   auto face = [&](int d, NRef a, int fi, int fj, int fk, double G[NG]) {
-    double Fc[5];
-    conv_face<LES, BX, BY>(c, F, R, d, a, fi, fj, fk, Fc);
-    double Fv[5] = {0., 0., 0., 0., 0.}, A[3] = {0., 0., 0.};
-    if (VISC) visc_face<LES, BX, BY>(c, F, R, d, a, fi, fj, fk, Fv, A);
+    conv_face<LES, BX, BY>(c, F, R, d, a, fi, fj, fk, G);
+    if (VISC) {
+      visc_face<LES, BX, BY>(c, F, R, d, a, fi, fj, fk, G + 5, G + 10);
+    } else {
 #pragma unroll
-    for (int q = 0; q < 5; q++) G[q] = Fv[q] - Fc[q];
-    G[5] = A[0]; G[6] = A[1]; G[7] = A[2];
+      for (int q = 5; q < NG; q++) G[q] = 0.;
+    }
   };
 
   // prologue: planes kb-2 .. kb+1, then the k-face kb-1/2
@@ -506,21 +509,24 @@ __global__ void __launch_bounds__(BX *BY, 1)
       const double nv = ldg(F.nvert + g);
       const int fxr = ty * (BX + 1) + tx + 1, fxl = fxr - 1;  // i+1/2, i-1/2
       const int fyu = (ty + 1) * BX + tx, fyd = ty * BX + tx; // j+1/2, j-1/2
-      double rhs[5];
+      // flux differences in the reference's order (rhs.c:3159-3205, 2123-2151):
+      // ((((F_i - F_i-1) + F_j) - F_j-1) + F_k) - F_k-1, conv and visc apart
+      auto fdiff = [&](int q) {
+        return gxb[(size_t)q * TS::NXF + fxr] - gxb[(size_t)q * TS::NXF + fxl] + gyb[(size_t)q * TS::NYF + fyu] -
+               gyb[(size_t)q * TS::NYF + fyd] + Gzn[q] - Gz[q];
+      };
+      double conv[5], visc[5];
 #pragma unroll
-      for (int q = 0; q < 5; q++) {
-        // (Fv - Fc) differences: visc - conv of the reference, summed per direction
-        const double dx = gxb[(size_t)q * TS::NXF + fxr] - gxb[(size_t)q * TS::NXF + fxl];
-        const double dy = gyb[(size_t)q * TS::NYF + fyu] - gyb[(size_t)q * TS::NYF + fyd];
-        const double dz = Gzn[q] - Gz[q];
-        rhs[q] = dx + dy + dz;
-      }
+      for (int q = 0; q < 5; q++) conv[q] = (nv < BLANK) ? fdiff(q) : 0.;
+      visc[0] = 0.;
+#pragma unroll
+      for (int q = 1; q < 5; q++) visc[q] = VISC ? fdiff(5 + q) : 0.;
       if (LES) {
         const NRef n{0, ty + 2, tx + 2};
-        const double aj = ldg(F.aj + g);
         if (nv < BLANK) {  // channel forcing terms (rhs.c:4226-4235), zero unless ratio != 0
-          rhs[3] += c.ratio / aj * R.get(F_RHO, n) / c.dt;
-          rhs[4] += c.ratio / aj * R.get(F_RW, n) / c.dt;
+          const double ajn = ldg(F.aj + g);
+          conv[3] = conv[3] - c.ratio / ajn * R.get(F_RHO, n) / c.dt;
+          conv[4] = conv[4] - c.ratio / ajn * R.get(F_RW, n) / c.dt;
         }
         if (VISC && gj > 2 && gj < c.my - 2 && nv < 0.5) {  // rhs.c:2153-2197
           const double r0 = R.get(F_RHO, n);
@@ -530,14 +536,18 @@ __global__ void __launch_bounds__(BX *BY, 1)
           double e = 0.;
 #pragma unroll
           for (int q = 0; q < 3; q++) {
-            const double t = rR * gxb[(size_t)(5 + q) * TS::NXF + fxr] - rL * gxb[(size_t)(5 + q) * TS::NXF + fxl] +
-                             rU * gyb[(size_t)(5 + q) * TS::NYF + fyu] - rD * gyb[(size_t)(5 + q) * TS::NYF + fyd] +
-                             rF * Gzn[5 + q] - rB * Gz[5 + q];
-            e += R.get(F_U + q, n) * t;
+            const int a = 10 + q;
+            const double t = rR * gxb[(size_t)a * TS::NXF + fxr] - rL * gxb[(size_t)a * TS::NXF + fxl] +
+                             rU * gyb[(size_t)a * TS::NYF + fyu] - rD * gyb[(size_t)a * TS::NYF + fyd] +
+                             rF * Gzn[a] - rB * Gz[a];
+            e = (q == 0) ? R.get(F_U + q, n) * t : e + R.get(F_U + q, n) * t;
           }
-          rhs[4] += e;
+          visc[4] += e;
         }
       }
+      double rhs[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) rhs[q] = visc[q] - conv[q];  // VecWAXPY(Rhs, -1, Conv, Visc)
       const double aj = ldg(F.aj + g);
 #pragma unroll
       for (int q = 0; q < 5; q++) rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;
