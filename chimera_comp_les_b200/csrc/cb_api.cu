@@ -25,8 +25,7 @@ using namespace cb;
 
 namespace {
 
-constexpr int BX = 32, BY = 8;
-using TS = TileShape<BX, BY>;
+constexpr int BX = SBX, BY = SBY;
 
 struct GraphSlot {
   cudaGraphExec_t exec = nullptr;
@@ -44,7 +43,7 @@ struct cb_ctx {
   size_t plane = 0;
   double *qb[3][5] = {};
   double *met[3][3] = {};
-  double *aj = nullptr, *nvert = nullptr, *nut = nullptr;
+  double *aj = nullptr, *nvert = nullptr, *nut = nullptr, *delta2 = nullptr;
   double *rhsb[5] = {};
   double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
   double **ptab = nullptr;    // device pointer tables
@@ -99,14 +98,15 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
   F.aj = c->aj;
   F.nvert = c->nvert;
   F.nut = c->nut;
+  F.delta2 = c->delta2;
   F.status = c->status;
   return F;
 }
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t set_stage_attr() {
-  return cudaFuncSetAttribute(stage_kernel<LES, VISC, RHSM, BX, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)TS::smem_bytes);
+  return cudaFuncSetAttribute(stage_kernel<LES, VISC, RHSM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)STAGE_SMEM_BYTES);
 }
 
 // Opt every stage-kernel variant into its dynamic shared memory on the
@@ -125,11 +125,10 @@ static cudaError_t set_stage_attrs() {
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt) {
-  auto kern = stage_kernel<LES, VISC, RHSM, BX, BY>;
+  auto kern = stage_kernel<LES, VISC, RHSM>;
   const int nkin = c->dc.mz - 2;
   dim3 grid((c->dc.mx - 2 + BX - 1) / BX, (c->dc.my - 2 + BY - 1) / BY, (nkin + c->kchunk - 1) / c->kchunk);
-  dim3 block(BX, BY);
-  kern<<<grid, block, TS::smem_bytes, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
+  kern<<<grid, SNT, STAGE_SMEM_BYTES, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
   return cudaGetLastError();
 }
 
@@ -199,7 +198,7 @@ static int nut_update(cb_ctx *c) {
     TimedScope ts(c, false);
     eddy_viscosity_kernel<<<grid_for(c, work), 256, 0, c->stream>>>(
         c->dc, c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr,
-        (const double *const *)(c->ptab + PT_MET), c->aj, c->nvert, c->nut);
+        (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvert, c->nut);
   }
   {
     TimedScope ts(c, false);
@@ -324,9 +323,12 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.s_x = cfg->s_x; d.s_y = cfg->s_y; d.s_z = cfg->s_z;
   d.ren = cfg->ren; d.ma = cfg->ma; d.pr = cfg->pr; d.gamma = cfg->gamma; d.dt = cfg->dt; d.st = cfg->st;
   d.cs_const = cfg->cs_const; d.ci = cfg->ci; d.ratio = cfg->ratio;
+  d.inv_ren = 1. / cfg->ren;
+  d.inv_ren_half = 1. / cfg->ren * 0.5;
+  d.gm1 = cfg->gamma - 1.0;
   c->plane = (size_t)d.plane;
-  // planes: 15 state + 9 metrics + aj + nvert + nut = 27
-  const int nplanes = 27;
+  // planes: 15 state + 9 metrics + aj + nvert + nut + LES filter width = 28
+  const int nplanes = 28;
   const size_t bytes = sizeof(double) * c->plane * nplanes;
   if (cudaMalloc(&c->arena, bytes) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc arena");
   if (cudaMemsetAsync(c->arena, 0, bytes, c->stream) != cudaSuccess) return bail(CB_E_CUDA, "memset");
@@ -338,6 +340,7 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   c->aj = c->arena + c->plane * (p++);
   c->nvert = c->arena + c->plane * (p++);
   c->nut = c->arena + c->plane * (p++);
+  c->delta2 = c->arena + c->plane * (p++);
   const size_t nn = (size_t)cfg->mx * cfg->my * cfg->mz;
   if (cudaMalloc(&c->staging, sizeof(double) * 5 * nn) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc staging");
   if (cudaMalloc(&c->ptab, sizeof(double *) * PT_N) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab");
@@ -412,6 +415,7 @@ int cb_set_grid(cb_ctx *c, const double *coor) {
     metrics_boundary_kernel<<<grid_for(c, work / 4 + 1), 256, 0, c->stream>>>(c->dc, c->ptab + PT_MET, c->aj, f);
   const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
   ghost_fill_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->ptab + PT_MISC + 2, 10);
+  delta2_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->aj, c->delta2);
   CB_CUDA(c, cudaGetLastError());
   // scrub buffer 2 (coordinates) so later ghost reads see zeros until written
   for (int q = 0; q < 3; q++) CB_CUDA(c, cudaMemsetAsync(X[q], 0, sizeof(double) * c->plane, c->stream));
@@ -428,6 +432,9 @@ int cb_set_metrics(cb_ctx *c, const double *csi, const double *eta, const double
   if ((e = upload_planes(c, eta, 3, PT_MET + 3, false))) return e;
   if ((e = upload_planes(c, zet, 3, PT_MET + 6, false))) return e;
   if ((e = upload_planes(c, aj, 1, PT_MISC + 0, false))) return e;
+  const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
+  delta2_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->aj, c->delta2);
+  CB_CUDA(c, cudaGetLastError());
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_grid = true;
   invalidate_graphs(c);

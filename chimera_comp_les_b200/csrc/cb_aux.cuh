@@ -63,7 +63,7 @@ __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, int npl
 // (les.c:135-150): interior nodes only; velocity from the recorded state qu
 // (nullptr: zero velocity before the first CalcUCat).
 __global__ void eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met,
-                                      const double *aj, const double *nvert, double *nut) {
+                                      const double *aj, const double *delta2, const double *nvert, double *nut) {
   const long long nx = c.mx - 2, ny = c.my - 2, nz = c.mz - 2, total = nx * ny * nz;
   const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -92,8 +92,18 @@ __global__ void eddy_viscosity_kernel(const DevCfg c, const double *const *qu, c
     const double Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
     const double Sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Sxy * Sxy + Syy * Syy + Syz * Syz + Sxz * Sxz +
                                     Syz * Syz + Szz * Szz));
-    const double filter = pow(1. / ajc, 1. / 3.);
-    nut[n] = c.cs_const * pow(filter, 2.0) * Sabs;
+    nut[n] = c.cs_const * ldg(delta2 + n) * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
+  }
+}
+
+// LES filter width squared per node, pow(pow(1/aj, 1/3), 2.0) -- the value
+// formViscous (rhs.c:1694-1696) and Compute_eddy_viscosity_LES (les.c:1560-1561)
+// recompute at every use; aj is fixed after FormMetrics, so once per grid.
+__global__ void delta2_kernel(const DevCfg c, const double *aj, double *delta2) {
+  const long long total = (long long)c.px * c.py * c.pz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const double a = aj[t];
+    delta2[t] = a != 0.0 ? pow(pow(1. / a, 1. / 3.), 2.0) : 0.0;
   }
 }
 

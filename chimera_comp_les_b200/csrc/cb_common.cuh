@@ -25,6 +25,9 @@ struct DevCfg {
   int les, inviscid, fluxorder, eno_order, central, isothermal;
   double s_x, s_y, s_z;
   double ren, ma, pr, gamma, dt, st, cs_const, ci, ratio;
+  double inv_ren;       // 1./ren
+  double inv_ren_half;  // 1./ren*0.5
+  double gm1;           // gamma-1.0
 };
 
 struct DevFields {
@@ -35,6 +38,7 @@ struct DevFields {
   const double *aj;
   const double *nvert;
   const double *nut;
+  const double *delta2;    // LES filter width squared, pow(pow(1/aj,1/3),2), per node
   double *rhs[5];          // formRHS output (rhs mode only)
   unsigned *status;        // sticky status word
 };

@@ -39,6 +39,14 @@ struct TileShape {
   static constexpr size_t smem_bytes = sizeof(double) * ((size_t)4 * NF * PN + (size_t)NG * (NXF + NYF));
 };
 
+// Selections by a runtime direction d without dynamic indexing (which would
+// place the indexed array in local memory).
+__device__ __forceinline__ const double *met_ptr(const DevFields &F, int d, int q) {
+  return d == 0 ? F.met[0][q] : (d == 1 ? F.met[1][q] : F.met[2][q]);
+}
+__device__ __forceinline__ int bc_lo(const DevCfg &c, int d) { return d == 0 ? c.bctype[0] : (d == 1 ? c.bctype[2] : c.bctype[4]); }
+__device__ __forceinline__ int bc_hi(const DevCfg &c, int d) { return d == 0 ? c.bctype[1] : (d == 1 ? c.bctype[3] : c.bctype[5]); }
+
 struct NRef {
   int r, y, x;  // relative plane (-1..2), tile-local row, tile-local column
 };
@@ -125,7 +133,7 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   const int m = d == 0 ? c.mx : (d == 1 ? c.my : c.mz);
   const double nvm = ldg(F.nvert + g0 - sd), nv0 = ldg(F.nvert + g0), nv1 = ldg(F.nvert + g0 + sd),
                nv2 = ldg(F.nvert + g0 + 2 * sd);
-  const double *const *met = F.met[d];
+  const double *met[3] = {met_ptr(F, d, 0), met_ptr(F, d, 1), met_ptr(F, d, 2)};
   double h[3];
 #pragma unroll
   for (int q = 0; q < 3; q++) h[q] = 0.5 * (ldg(met[q] + g0) + ldg(met[q] + g0 + sd));
@@ -145,7 +153,7 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   bool first;
   if (LES) {
     double nsum2 = (d == 2) ? nv0 + ldg(F.nvert + gidx(c, 1, gj, gk + 1)) : nv0 + nv1;  // quirk rhs.c:4046
-    first = fo == 1 || ((pos == 0 || pos == m - 2) && c.bctype[2 * d] != 7) || nsum2 > BLANKWALL;
+    first = fo == 1 || ((pos == 0 || pos == m - 2) && bc_lo(c, d) != 7) || nsum2 > BLANKWALL;
   } else {
     first = fo == 1 || pos == 0 || pos == m - 2 || (nv0 + nv1) > BLANKWALL;
   }
@@ -208,8 +216,8 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   if (LES) {
     rusanov(QL, QR, pL, pR, h, false, false, Fw);
   } else {
-    const bool use_qr_l = (pos == m - 2 && c.bctype[2 * d + 1] == 1);
-    const bool r_from_l = (pos == 0 && c.bctype[2 * d] == 1);
+    const bool use_qr_l = (pos == m - 2 && bc_hi(c, d) == 1);
+    const bool r_from_l = (pos == 0 && bc_lo(c, d) == 1);
     rusanov(QL, QR, pL, pR, h, use_qr_l, r_from_l, Fw);
   }
   if (!LES) {
@@ -280,10 +288,12 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   // D[f][e]: derivative of (u, v, w, T) along computational direction e
   double D[4][3];
 #pragma unroll
-  for (int f = 0; f < 4; f++) D[f][d] = R.get(F_U + f, b) - R.get(F_U + f, a);
-#pragma unroll
   for (int e = 0; e < 3; e++) {
-    if (e == d) continue;
+    if (e == d) {
+#pragma unroll
+      for (int f = 0; f < 4; f++) D[f][e] = R.get(F_U + f, b) - R.get(F_U + f, a);
+      continue;
+    }
     const long long te = gstride(c, e);
     const bool plus_blocked = blocked(ldg(F.nvert + g0 + te)) || blocked(ldg(F.nvert + g1 + te));
     const bool minus_blocked = blocked(ldg(F.nvert + g0 - te)) || blocked(ldg(F.nvert + g1 - te));
@@ -313,7 +323,9 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   for (int e = 0; e < 3; e++)
 #pragma unroll
     for (int q = 0; q < 3; q++) mh[e][q] = 0.5 * (ldg(F.met[e][q] + g0) + ldg(F.met[e][q] + g1));
-  const double md0 = mh[d][0], md1 = mh[d][1], md2 = mh[d][2];
+  const double md0 = d == 0 ? mh[0][0] : (d == 1 ? mh[1][0] : mh[2][0]);
+  const double md1 = d == 0 ? mh[0][1] : (d == 1 ? mh[1][1] : mh[2][1]);
+  const double md2 = d == 0 ? mh[0][2] : (d == 1 ? mh[1][2] : mh[2][2]);
   const double csi0 = mh[0][0], csi1 = mh[0][1], csi2 = mh[0][2];
   const double eta0 = mh[1][0], eta1 = mh[1][1], eta2 = mh[1][2];
   const double zet0 = mh[2][0], zet1 = mh[2][1], zet2 = mh[2][2];
@@ -332,11 +344,11 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   const double r33 = dwdc * csi2 + dwde * eta2 + dwdz * zet2;
 
   const double ajc = 0.5 * (ldg(F.aj + g0) + ldg(F.aj + g1));
-  double nu = 1. / c.ren;
+  double nu = c.inv_ren;  // 1./ren (evaluated once on the host, same value)
   if (LES) {
     // quirk: eta/zeta faces average rho over i and i+1 (rhs.c:1835, 2034)
     const double rhs_rho = (d == 0) ? R.get(F_RHO, b) : R.get(F_RHO, nshift(a, 0, 1));
-    nu = 1. / c.ren * 0.5 * (R.get(F_RHO, a) + rhs_rho);
+    nu = c.inv_ren_half * (R.get(F_RHO, a) + rhs_rho);  // (1./ren*0.5)*(...)
   }
   const double div = 2. / 3. * (dudc * csi0 + dude * eta0 + dudz * zet0 + dvdc * csi1 + dvde * eta1 + dvdz * zet1 +
                                 dwdc * csi2 + dwde * eta2 + dwdz * zet2);
@@ -352,10 +364,10 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   Fv[3] -= div * md2 * ajc * nu;
 
   double uh[3];
-  if (pos == 0 && c.bctype[2 * d] == 1) {
+  if (pos == 0 && bc_lo(c, d) == 1) {
 #pragma unroll
     for (int q = 0; q < 3; q++) uh[q] = R.get(F_U + q, a);
-  } else if (pos == m - 2 && c.bctype[2 * d + 1] == 1) {
+  } else if (pos == m - 2 && bc_hi(c, d) == 1) {
 #pragma unroll
     for (int q = 0; q < 3; q++) uh[q] = R.get(F_U + q, b);
   } else {
@@ -364,7 +376,7 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   }
   const double gm = c.gamma;
   Fv[4] = (Fv[1] * uh[0] + Fv[2] * uh[1] + Fv[3] * uh[2]) +
-          (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (gm * nu / c.pr / (gm - 1.0));
+          (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (gm * nu / c.pr / c.gm1);
 
   A[0] = A[1] = A[2] = 0.;
   if (LES) {  // rhs.c:1677-1710
@@ -374,14 +386,14 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
     double nut = 0.5 * (ldg(F.nut + g0) * sa + ldg(F.nut + g1) * sb);
     const double rho_c = 0.5 * (R.get(F_RHO, a) + R.get(F_RHO, b));
     const double sigma_c = 0.5 * (sa + sb);
-    if ((c.bctype[2 * d] == 1 && pos == 0) || (c.bctype[2 * d + 1] == 1 && pos == m - 2)) nut = 0;
+    if ((bc_lo(c, d) == 1 && pos == 0) || (bc_hi(c, d) == 1 && pos == m - 2)) nut = 0;
     const double tx = (tu - div * md0) * ajc * (nut * rho_c);
     const double ty = (tv - div * md1) * ajc * (nut * rho_c);
     const double tz = (tw - div * md2) * ajc * (nut * rho_c);
     const double S2 = .5 * ((r11 - div) * (r11 - div) + r12 * r12 + r13 * r13 + r21 * r21 + (r22 - div) * (r22 - div) +
                             r23 * r23 + r31 * r31 + r32 * r32 + (r33 - div) * (r33 - div));
-    const double filter = pow(1. / ldg(F.aj + g0), 1. / 3.);
-    const double pf = pow(filter, 2.0);
+    // pow(pow(1/aj, 1/3), 2) of the left node, precomputed once per node
+    const double pf = ldg(F.delta2 + g0);
     const double sgs = -S2 * pf * c.ci * 2.0 / 3.0;
     A[0] = tx + sgs * md0 * rho_c * sigma_c;
     A[1] = ty + sgs * md1 * rho_c * sigma_c;
@@ -393,127 +405,177 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
 }
 
 // ---------------------------------------------------------- the kernel ----
-template <bool LES, bool VISC, bool RHS_MODE, int BX, int BY>
-__global__ void __launch_bounds__(BX *BY, 1)
+// Tile of SBX x SBY interior nodes, SNT threads.  Per plane the block
+// computes (SBX+1)*SBY i-faces, SBX*(SBY+1) j-faces and SBX*SBY k-faces in
+// three warp-uniform rounds: virtual face v = round*SNT + tid maps to
+// [0,256) i-faces, [256,512) j-faces, [512,736) k-faces, so every warp runs
+// one face direction per round (no divergence between directions).
+constexpr int SBX = 32, SBY = 7, SNT = 256;
+using STile = TileShape<SBX, SBY>;
+constexpr int S_NXF = STile::NXF;  // 231
+constexpr int S_NYF = STile::NYF;  // 256
+constexpr int S_NZF = SBX * SBY;   // 224
+constexpr size_t STAGE_SMEM_BYTES =
+    sizeof(double) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF) + (size_t)5 * STile::PN);
+static_assert(S_NXF <= 256 && S_NYF <= 256 && S_NZF <= 224, "face schedule segments");
+static_assert(STAGE_SMEM_BYTES <= 232448, "shared memory budget of one block");
+
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  const int sz = valid ? 8 : 0;  // src-size 0 zero-fills the destination
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <bool LES, bool VISC, bool RHS_MODE>
+__global__ void __launch_bounds__(SNT, 1)
     stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
-  using TS = TileShape<BX, BY>;
+  constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
   extern __shared__ double smem[];
   Ring<BX, BY> R;
   R.pl = smem;
-  double *gxb = smem + (size_t)4 * NF * TS::PN;  // [NG][BY][BX+1]
-  double *gyb = gxb + (size_t)NG * TS::NXF;      // [NG][BY+1][BX]
+  double *gxb = smem + (size_t)4 * NF * PN;  // [NG][S_NXF]
+  double *gyb = gxb + (size_t)NG * S_NXF;    // [NG][S_NYF]
+  double *gzb = gyb + (size_t)NG * S_NYF;    // [NG][S_NZF]
+  double *stg = gzb + (size_t)NG * S_NZF;    // [5][PN] raw Q of the next plane
 
-  const int tid = threadIdx.x + BX * threadIdx.y;
-  const int nthr = BX * BY;
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = threadIdx.x;
   const int i0 = 1 + blockIdx.x * BX, j0 = 1 + blockIdx.y * BY;
   const int kb = 1 + blockIdx.z * kchunk;
   const int ke = min(c.mz - 1, kb + kchunk);  // exclusive
-  const int gi = i0 + tx, gj = j0 + ty;
-  const bool active = gi <= c.mx - 2 && gj <= c.my - 2;
+  // node updated by this thread (threads 224..255 only load and compute faces)
+  const int utx = tid % BX, uty = tid / BX;
+  const int ugi = i0 + utx, ugj = j0 + uty;
+  const bool uact = uty < BY && ugi <= c.mx - 2 && ugj <= c.my - 2;
 
-  // load global plane kk into ring slot s (conserved + derived fields)
-  auto load_plane = [&](int kk, int s) {
-    for (int idx = tid; idx < TS::PN; idx += nthr) {
-      const int lx = idx % TS::PX, ly = idx / TS::PX;
+  // async copy of the raw state of plane kk (with its halo) into the staging buffer
+  auto issue_stage = [&](int kk) {
+    for (int e = tid; e < 5 * PN; e += NT) {
+      const int q = e / PN, idx = e - q * PN;
+      const int lx = idx % PX, ly = idx / PX;
       const int xi = i0 - 2 + lx, yj = j0 - 2 + ly;
+      const bool ok = xi <= c.mx + 1 && yj <= c.my + 1 && kk >= -2 && kk <= c.mz + 1;
+      const double *src = ok ? F.q[q] + gidx(c, xi, yj, kk) : F.q[q];
+      cp_async8(stg + e, src, ok);
+    }
+    cp_async_commit();
+  };
+  // staging -> ring slot s with the derived p, u, v, w, T (EqOfState rhs.c:4850, CalcUCat rhs.c:1349)
+  auto derive = [&](int s) {
+    for (int idx = tid; idx < PN; idx += NT) {
       double v[NF];
-      bool ok = xi <= c.mx + 1 && yj <= c.my + 1 && kk >= -2 && kk <= c.mz + 1;
-      if (ok) {
-        const long long g = gidx(c, xi, yj, kk);
 #pragma unroll
-        for (int q = 0; q < 5; q++) v[q] = ldg(F.q[q] + g);
-      }
-      if (ok && v[0] != 0.0) {
+      for (int q = 0; q < 5; q++) v[q] = stg[q * PN + idx];
+      if (v[0] != 0.0) {
         const double r = v[0];
-        v[F_P] = (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / r);  // rhs.c:4850
+        v[F_P] = (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / r);
         v[F_U] = v[1] / r;
         v[F_V] = v[2] / r;
         v[F_W] = v[3] / r;
         v[F_T] = v[F_P] / r;
       } else {
 #pragma unroll
-        for (int q = 0; q < NF; q++) v[q] = 0.0;
+        for (int q = 5; q < NF; q++) v[q] = 0.0;
       }
-      double *base = R.pl + (size_t)s * NF * TS::PN + idx;
+      double *base = R.pl + (size_t)s * NF * PN + idx;
 #pragma unroll
-      for (int q = 0; q < NF; q++) base[(size_t)q * TS::PN] = v[q];
+      for (int q = 0; q < NF; q++) base[(size_t)q * PN] = v[q];
+    }
+  };
+  auto load_plane_sync = [&](int kk, int s) {
+    issue_stage(kk);
+    cp_async_wait_all();
+    __syncthreads();
+    derive(s);
+    __syncthreads();
+  };
+
+  // all face fluxes of plane k (zonly: just the k-faces, for the prologue)
+  auto faces = [&](int k, bool zonly) {
+#pragma unroll 1
+    for (int r = zonly ? 2 : 0; r < 3; r++) {
+      const int v = r * NT + tid;
+      int d, u, fi, fj;
+      NRef a;
+      double *dst;
+      int nslot;
+      if (v < 256) {
+        d = 0; u = v;
+        const int fx = u % (BX + 1), fy = u / (BX + 1);
+        fi = i0 - 1 + fx; fj = j0 + fy;
+        a = NRef{0, fy + 2, fx + 1};
+        dst = gxb; nslot = S_NXF;
+        if (u >= S_NXF) continue;
+      } else if (v < 512) {
+        d = 1; u = v - 256;
+        const int fx = u % BX, fy = u / BX;
+        fi = i0 + fx; fj = j0 - 1 + fy;
+        a = NRef{0, fy + 1, fx + 2};
+        dst = gyb; nslot = S_NYF;
+      } else {
+        d = 2; u = v - 512;
+        if (u >= S_NZF) continue;
+        const int fx = u % BX, fy = u / BX;
+        fi = i0 + fx; fj = j0 + fy;
+        a = NRef{0, fy + 2, fx + 2};
+        dst = gzb; nslot = S_NZF;
+      }
+      double G[NG];
+      if (fi <= c.mx - 2 && fj <= c.my - 2) {
+        conv_face<LES, BX, BY>(c, F, R, d, a, fi, fj, k, G);
+        if (VISC) {
+          visc_face<LES, BX, BY>(c, F, R, d, a, fi, fj, k, G + 5, G + 10);
+        } else {
+#pragma unroll
+          for (int q = 5; q < NG; q++) G[q] = 0.;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < NG; q++) G[q] = 0.;
+      }
+#pragma unroll
+      for (int q = 0; q < NG; q++) dst[(size_t)q * nslot + u] = G[q];
     }
   };
 
-  // face value: inviscid flux (5), viscous flux (5), LES stress part (3)
-  auto face = [&](int d, NRef a, int fi, int fj, int fk, double G[NG]) {
-    conv_face<LES, BX, BY>(c, F, R, d, a, fi, fj, fk, G);
-    if (VISC) {
-      visc_face<LES, BX, BY>(c, F, R, d, a, fi, fj, fk, G + 5, G + 10);
-    } else {
+  // prologue: planes kb-2 .. kb+1 in slots 0..3, k-face kb-1/2, then kb+2
+  R.slot[0] = 0; R.slot[1] = 1; R.slot[2] = 2; R.slot[3] = 3;
+  load_plane_sync(kb - 2, 0);
+  load_plane_sync(kb - 1, 1);
+  load_plane_sync(kb, 2);
+  load_plane_sync(kb + 1, 3);
+  faces(kb - 1, true);  // r = 0 -> plane kb-1
+  __syncthreads();
+  double Gzp[NG];  // k-face k-1/2 of the node this thread updates
 #pragma unroll
-      for (int q = 5; q < NG; q++) G[q] = 0.;
-    }
-  };
-
-  // prologue: planes kb-2 .. kb+1, then the k-face kb-1/2
-  for (int r = -1; r < 3; r++) R.slot[r + 1] = (r + 1) & 3;
-  // slots: plane kb-2 -> slot of r=-1 shifted; set ring so that r=-1 is kb-2 for the prologue
-  load_plane(kb - 2, 0);
-  load_plane(kb - 1, 1);
-  load_plane(kb, 2);
-  load_plane(kb + 1, 3);
+  for (int q = 0; q < NG; q++) Gzp[q] = uact ? gzb[(size_t)q * S_NZF + tid] : 0.;
   __syncthreads();
-  double Gz[NG];  // face k-1/2 of the current plane
-  {
-    // ring view for the prologue: r=-1 -> kb-2 (slot 0), r=0 -> kb-1 (slot 1), ...
-    R.slot[0] = 0; R.slot[1] = 1; R.slot[2] = 2; R.slot[3] = 3;
-    if (active) face(2, NRef{0, ty + 2, tx + 2}, gi, gj, kb - 1, Gz);
-  }
-  __syncthreads();
-  load_plane(kb + 2, 0);  // slot 0 now holds kb+2
-  __syncthreads();
+  load_plane_sync(kb + 2, 0);
   int base = 1;  // slot of plane k-1
 
   for (int k = kb; k < ke; k++) {
     R.slot[0] = base & 3; R.slot[1] = (base + 1) & 3; R.slot[2] = (base + 2) & 3; R.slot[3] = (base + 3) & 3;
-    // i-faces of plane k: left node x = i0-1+fx, row j0+fy
-    for (int f = tid; f < TS::NXF; f += nthr) {
-      const int fx = f % (BX + 1), fy = f / (BX + 1);
-      const int fi = i0 - 1 + fx, fj = j0 + fy;
-      double G[NG];
-      if (fi <= c.mx - 2 && fj <= c.my - 2) face(0, NRef{0, fy + 2, fx + 1}, fi, fj, k, G);
-      else {
-#pragma unroll
-        for (int q = 0; q < NG; q++) G[q] = 0.;
-      }
-#pragma unroll
-      for (int q = 0; q < NG; q++) gxb[(size_t)q * TS::NXF + f] = G[q];
-    }
-    // j-faces of plane k: lower node row j0-1+fy, column i0+fx
-    for (int f = tid; f < TS::NYF; f += nthr) {
-      const int fx = f % BX, fy = f / BX;
-      const int fi = i0 + fx, fj = j0 - 1 + fy;
-      double G[NG];
-      if (fi <= c.mx - 2 && fj <= c.my - 2) face(1, NRef{0, fy + 1, fx + 2}, fi, fj, k, G);
-      else {
-#pragma unroll
-        for (int q = 0; q < NG; q++) G[q] = 0.;
-      }
-#pragma unroll
-      for (int q = 0; q < NG; q++) gyb[(size_t)q * TS::NYF + f] = G[q];
-    }
-    // k-face k+1/2
-    double Gzn[NG];
-    if (active) face(2, NRef{0, ty + 2, tx + 2}, gi, gj, k, Gzn);
+    const bool more = k + 1 < ke;
+    if (more) issue_stage(k + 3);  // overlaps the face computation
+    faces(k, false);
+    // the only plane k-1 value the update needs, read before that slot is refilled
+    const NRef n{0, uty + 2, utx + 2};
+    const double rho_km1 = (LES && VISC && uact) ? R.get(F_RHO, nshift(n, 2, -1)) : 0.;
+    cp_async_wait_all();
     __syncthreads();
 
-    if (active) {
-      const long long g = gidx(c, gi, gj, k);
+    if (uact) {
+      const long long g = gidx(c, ugi, ugj, k);
       const double nv = ldg(F.nvert + g);
-      const int fxr = ty * (BX + 1) + tx + 1, fxl = fxr - 1;  // i+1/2, i-1/2
-      const int fyu = (ty + 1) * BX + tx, fyd = ty * BX + tx; // j+1/2, j-1/2
+      const int fxr = uty * (BX + 1) + utx + 1, fxl = fxr - 1;   // i+1/2, i-1/2
+      const int fyu = (uty + 1) * BX + utx, fyd = uty * BX + utx;  // j+1/2, j-1/2
+      const int fz = tid;                                          // k+1/2 (k-1/2 in Gzp)
       // flux differences in the reference's order (rhs.c:3159-3205, 2123-2151):
       // ((((F_i - F_i-1) + F_j) - F_j-1) + F_k) - F_k-1, conv and visc apart
       auto fdiff = [&](int q) {
-        return gxb[(size_t)q * TS::NXF + fxr] - gxb[(size_t)q * TS::NXF + fxl] + gyb[(size_t)q * TS::NYF + fyu] -
-               gyb[(size_t)q * TS::NYF + fyd] + Gzn[q] - Gz[q];
+        return gxb[(size_t)q * S_NXF + fxr] - gxb[(size_t)q * S_NXF + fxl] + gyb[(size_t)q * S_NYF + fyu] -
+               gyb[(size_t)q * S_NYF + fyd] + gzb[(size_t)q * S_NZF + fz] - Gzp[q];
       };
       double conv[5], visc[5];
 #pragma unroll
@@ -522,48 +584,47 @@ __global__ void __launch_bounds__(BX *BY, 1)
 #pragma unroll
       for (int q = 1; q < 5; q++) visc[q] = VISC ? fdiff(5 + q) : 0.;
       if (LES) {
-        const NRef n{0, ty + 2, tx + 2};
-        if (nv < BLANK) {  // channel forcing terms (rhs.c:4226-4235), zero unless ratio != 0
+        if (nv < BLANK && c.ratio != 0.0) {  // channel forcing terms (rhs.c:4226-4235); exact no-op at ratio 0
           const double ajn = ldg(F.aj + g);
           conv[3] = conv[3] - c.ratio / ajn * R.get(F_RHO, n) / c.dt;
           conv[4] = conv[4] - c.ratio / ajn * R.get(F_RW, n) / c.dt;
         }
-        if (VISC && gj > 2 && gj < c.my - 2 && nv < 0.5) {  // rhs.c:2153-2197
+        if (VISC && ugj > 2 && ugj < c.my - 2 && nv < 0.5) {  // rhs.c:2153-2197
           const double r0 = R.get(F_RHO, n);
           const double rL = (r0 + R.get(F_RHO, nshift(n, 0, -1))) * 0.5, rR = (R.get(F_RHO, nshift(n, 0, 1)) + r0) * 0.5;
           const double rD = (r0 + R.get(F_RHO, nshift(n, 1, -1))) * 0.5, rU = (R.get(F_RHO, nshift(n, 1, 1)) + r0) * 0.5;
-          const double rB = (r0 + R.get(F_RHO, nshift(n, 2, -1))) * 0.5, rF = (R.get(F_RHO, nshift(n, 2, 1)) + r0) * 0.5;
+          const double rB = (r0 + rho_km1) * 0.5, rF = (R.get(F_RHO, nshift(n, 2, 1)) + r0) * 0.5;
           double e = 0.;
 #pragma unroll
           for (int q = 0; q < 3; q++) {
             const int a = 10 + q;
-            const double t = rR * gxb[(size_t)a * TS::NXF + fxr] - rL * gxb[(size_t)a * TS::NXF + fxl] +
-                             rU * gyb[(size_t)a * TS::NYF + fyu] - rD * gyb[(size_t)a * TS::NYF + fyd] +
-                             rF * Gzn[a] - rB * Gz[a];
+            const double t = rR * gxb[(size_t)a * S_NXF + fxr] - rL * gxb[(size_t)a * S_NXF + fxl] +
+                             rU * gyb[(size_t)a * S_NYF + fyu] - rD * gyb[(size_t)a * S_NYF + fyd] +
+                             rF * gzb[(size_t)a * S_NZF + fz] - rB * Gzp[a];
             e = (q == 0) ? R.get(F_U + q, n) * t : e + R.get(F_U + q, n) * t;
           }
           visc[4] += e;
         }
       }
+      const double aj = ldg(F.aj + g);
       double rhs[5];
 #pragma unroll
-      for (int q = 0; q < 5; q++) rhs[q] = visc[q] - conv[q];  // VecWAXPY(Rhs, -1, Conv, Visc)
-      const double aj = ldg(F.aj + g);
-#pragma unroll
-      for (int q = 0; q < 5; q++) rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;
+      for (int q = 0; q < 5; q++) {
+        rhs[q] = visc[q] - conv[q];                  // VecWAXPY(Rhs, -1, Conv, Visc)
+        rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;     // MultAj
+      }
       if (RHS_MODE) {
 #pragma unroll
         for (int q = 0; q < 5; q++) F.rhs[q][g] = rhs[q];
       } else {
-        const NRef n{0, ty + 2, tx + 2};
         double out[5];
 #pragma unroll
         for (int q = 0; q < 5; q++) {
           const double qo = ldg(F.qold[q] + g);
+          // solvers.c:257 (VecWAXPY) and 269 (VecAXPBYPCZ)
           out[q] = (istage == 0) ? qo + adt * rhs[q] : beta * qo + adt * rhs[q] + alfa * R.get(F_RHO + q, n);
           F.qout[q][g] = out[q];
         }
-        // EqOfState sanity (rhs.c:4862 prints p<0): sticky status instead
         const double p = (c.gamma - 1) * (out[4] - 0.5 * (out[1] * out[1] + out[2] * out[2] + out[3] * out[3]) / out[0]);
         unsigned st = 0;
         if (!isfinite(out[0] + out[1] + out[2] + out[3] + out[4])) st |= ST_NONFINITE;
@@ -572,11 +633,9 @@ __global__ void __launch_bounds__(BX *BY, 1)
         if (st) atomicOr(F.status, st);
       }
 #pragma unroll
-      for (int q = 0; q < NG; q++) Gz[q] = Gzn[q];
+      for (int q = 0; q < NG; q++) Gzp[q] = gzb[(size_t)q * S_NZF + fz];
     }
-    __syncthreads();
-    // advance the ring: plane k-1's slot receives k+3
-    if (k + 1 < ke) load_plane(k + 3, base & 3);
+    if (more) derive(base & 3);  // plane k+3 into the slot of plane k-1
     base++;
     __syncthreads();
   }
