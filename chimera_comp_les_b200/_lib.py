@@ -64,6 +64,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = C.c_int
+    lib.cb_rhs_noalloc.argtypes = [C.POINTER(CbConfig), P, P, P, P, P, P]
+    lib.cb_rhs_noalloc.restype = C.c_int
     lib.cb_stream.argtypes = [P]
     lib.cb_stream.restype = P
     lib.cb_interior_nodes.argtypes = [P]

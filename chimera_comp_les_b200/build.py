@@ -13,7 +13,7 @@ import sys
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(PKG_DIR)
 LIB_PATH = os.path.join(PKG_DIR, "libchimera_b200.so")
-SOURCES = [os.path.join(PKG_DIR, "csrc", "cb_api.cu")]
+SOURCES = [os.path.join(PKG_DIR, "csrc", "cb_api.cu"), os.path.join(PKG_DIR, "csrc", "cb_noalloc.cu")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # The FP64 form reproduces the reference's IEEE operation order: no FMA
 # contraction (-fmad=false), IEEE division and square root.

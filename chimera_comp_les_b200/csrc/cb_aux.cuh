@@ -31,7 +31,7 @@ __device__ __forceinline__ void bc_source(const DevCfg &c, int i, int j, int k, 
 }
 
 // Writes every non-interior node (boundary layer + both ghost layers) of qout.
-__global__ void bc_periodic_kernel(const DevCfg c, DevFields F) {
+static __global__ void bc_periodic_kernel(const DevCfg c, DevFields F) {
   const long long nx = c.mx + 4, ny = c.my + 4, nz = c.mz + 4, total = nx * ny * nz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % nx) - 2, j = (int)((t / nx) % ny) - 2, k = (int)(t / (nx * ny)) - 2;
@@ -46,7 +46,7 @@ __global__ void bc_periodic_kernel(const DevCfg c, DevFields F) {
 }
 
 // Ghost layers of periodic planes from their owned images (DMGlobalToLocal).
-__global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, int nplanes) {
+static __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, int nplanes) {
   const long long nx = c.mx + 4, ny = c.my + 4, nz = c.mz + 4, total = nx * ny * nz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % nx) - 2, j = (int)((t / nx) % ny) - 2, k = (int)(t / (nx * ny)) - 2;
@@ -62,7 +62,7 @@ __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, int npl
 // Compute_eddy_viscosity_LES (les.c:1523-1567) with constant CS
 // (les.c:135-150): interior nodes only; velocity from the recorded state qu
 // (nullptr: zero velocity before the first CalcUCat).
-__global__ void eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met,
+static __global__ void eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met,
                                       const double *aj, const double *delta2, const double *nvert, double *nut) {
   const long long nx = c.mx - 2, ny = c.my - 2, nz = c.mz - 2, total = nx * ny * nz;
   const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
@@ -99,7 +99,7 @@ __global__ void eddy_viscosity_kernel(const DevCfg c, const double *const *qu, c
 // LES filter width squared per node, pow(pow(1/aj, 1/3), 2.0) -- the value
 // formViscous (rhs.c:1694-1696) and Compute_eddy_viscosity_LES (les.c:1560-1561)
 // recompute at every use; aj is fixed after FormMetrics, so once per grid.
-__global__ void delta2_kernel(const DevCfg c, const double *aj, double *delta2) {
+static __global__ void delta2_kernel(const DevCfg c, const double *aj, double *delta2) {
   const long long total = (long long)c.px * c.py * c.pz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const double a = aj[t];
@@ -111,7 +111,7 @@ __global__ void delta2_kernel(const DevCfg c, const double *aj, double *delta2) 
 // FormMetrics (metrics.c:52-136): csi on (k,j) interior for every i, eta on
 // (k,i) interior for every j, zet on (j,i) interior for every k, aj on the
 // interior; everything else zero.
-__global__ void metrics_interior_kernel(const DevCfg c, const double *const *X, double *const *met, double *aj) {
+static __global__ void metrics_interior_kernel(const DevCfg c, const double *const *X, double *const *met, double *aj) {
   const long long nx = c.mx, ny = c.my, nz = c.mz, total = nx * ny * nz;
   const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -154,7 +154,7 @@ __global__ void metrics_interior_kernel(const DevCfg c, const double *const *X, 
 
 // One boundary-copy pass of FormMetrics (metrics.c:138-246).  face: 0 i-lo,
 // 1 i-hi, 2 j-lo, 3 j-hi, 4 k-lo, 5 k-hi.  The passes must run in this order.
-__global__ void metrics_boundary_kernel(const DevCfg c, double *const *met, double *aj, int face) {
+static __global__ void metrics_boundary_kernel(const DevCfg c, double *const *met, double *aj, int face) {
   const int d = face / 2, hi = face & 1;
   const int na = d == 0 ? c.my : c.mx, nb = d == 2 ? c.my : c.mz;  // the two transverse extents
   const long long total = (long long)na * nb;
@@ -178,7 +178,7 @@ __global__ void metrics_boundary_kernel(const DevCfg c, double *const *met, doub
 
 // --------------------------------------------------------- pack / unpack --
 // AoS natural (mz,my,mx,nc) <-> owned nodes of nc padded planes.
-__global__ void unpack_kernel(const DevCfg c, const double *__restrict__ aos, int nc, double *const *planes) {
+static __global__ void unpack_kernel(const DevCfg c, const double *__restrict__ aos, int nc, double *const *planes) {
   const long long total = (long long)c.mx * c.my * c.mz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % c.mx), j = (int)((t / c.mx) % c.my), k = (int)(t / ((long long)c.mx * c.my));
@@ -187,7 +187,7 @@ __global__ void unpack_kernel(const DevCfg c, const double *__restrict__ aos, in
   }
 }
 
-__global__ void pack_kernel(const DevCfg c, const double *const *planes, int nc, double *__restrict__ aos) {
+static __global__ void pack_kernel(const DevCfg c, const double *const *planes, int nc, double *__restrict__ aos) {
   const long long total = (long long)c.mx * c.my * c.mz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % c.mx), j = (int)((t / c.mx) % c.my), k = (int)(t / ((long long)c.mx * c.my));
@@ -197,7 +197,7 @@ __global__ void pack_kernel(const DevCfg c, const double *const *planes, int nc,
 }
 
 // EqOfState (rhs.c:4845-4856) on owned nodes, written AoS (1 per node).
-__global__ void eos_pack_kernel(const DevCfg c, const double *const *q, double *__restrict__ p) {
+static __global__ void eos_pack_kernel(const DevCfg c, const double *const *q, double *__restrict__ p) {
   const long long total = (long long)c.mx * c.my * c.mz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % c.mx), j = (int)((t / c.mx) % c.my), k = (int)(t / ((long long)c.mx * c.my));

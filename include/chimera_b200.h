@@ -153,6 +153,30 @@ int cb_launches_per_step(const cb_ctx *ctx);
 const char *cb_last_error(const cb_ctx *ctx);
 int cb_abi_version(void);
 
+/* formRHS without any device allocation, for callers that may not call
+ * cudaMalloc (a solver running inside a memory pool owned by another
+ * framework, or a host that forbids device allocation after start-up).
+ * No counterpart in the reference: there every call allocates its
+ * temporaries with VecDuplicate.
+ *
+ * The caller owns every input and the output, all device pointers in natural
+ * AoS order: d_coor 3 doubles per node, d_q 5, d_nvert 1, d_nut 1 (NULL: zero
+ * eddy viscosity), d_rhs 5 (written: the RHS of formRHS at istage 0, zero on
+ * boundary nodes).  Work is enqueued on `stream` (a cudaStream_t, NULL for the
+ * default stream); the caller synchronises.
+ *
+ * Scratch lives in a file-scope device array sized for
+ * CB_NOALLOC_MAX_PLANE padded nodes per field, (mx+4 rounded up to 16) *
+ * (my+4) * (mz+4); larger grids are rejected with CB_E_ARG.  The array
+ * (about 20 MB) is held by every GPU that loads the library until the
+ * process exits.  All calls share it and it keeps the last call's contents,
+ * so calls that overlap on the GPU race: serialise them.  The first call on a
+ * device does a one-time set-up (symbol lookup, kernel attributes); make it
+ * before any stream capture.  Only fully periodic blocks are accepted. */
+#define CB_NOALLOC_MAX_PLANE 98304LL
+int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const double *d_q, const double *d_nvert,
+                   const double *d_nut, double *d_rhs, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
