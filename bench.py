@@ -4,16 +4,19 @@ Workload (the configuration the metric is quoted on): viscous LES of the
 compressible Taylor-Green vortex, 128^3 unique nodes (DMDA 130^3 with the
 periodic boundary layers) on [0, 2*pi]^3, curvilinear grid perturbed by
 x_i += 0.05 sin(xi_j) sin(xi_k), Ma 0.1, Re 1600, Pr 0.71, gamma 1.4, constant
-viscosity, the reference's LES scheme: MUSCL-minmod + Rusanov upwind blended
-with the 4-point skew-symmetric central flux (-central 2, -s_x/y/z 1), constant
-Smagorinsky eddy viscosity (CS 0.03) with Yoshizawa term; SSP-RK with
--fluxorder 2 (the reference runs 2 stages per step for MUSCL).  Synthetic
-inputs from a formula (no dataset).
+viscosity, the reference's LES scheme: WENO3 + Rusanov upwind blended with the
+4-point skew-symmetric central flux (-central 2, -s_x/y/z 1), constant
+Smagorinsky eddy viscosity (CS 0.03) with Yoshizawa term; SSP-RK3
+(-fluxorder 3: the reference ties the RK stage count to the flux order), dt
+2e-3 (CFL ~0.44).  Synthetic inputs from a formula (no dataset).
 
 A "step" is one physical time step (eddy viscosity + every RK stage with its
 periodic boundary/ghost fill).  value = interior nodes x stages x steps x
-n_gpus / max-over-ranks device time.  Inputs (state 5 + metrics 10 + nvert +
-nu_t planes, ~0.5 GB) exceed the 126 MB L2, so no explicit flush is needed.
+n_gpus / max-over-ranks device time of the MIXED form (FP32 fluxes, FP64
+state); the FP64 parity form is measured the same way and reported beside it,
+with the mixed-vs-FP64 per-field error after 100 steps and the kinetic-energy
+and enstrophy history deviation.  Inputs (~0.6 GB resident per stage) exceed
+the 126 MB L2, so no explicit flush is needed.
 
 Run: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -37,20 +40,25 @@ sys.path.insert(0, REPO)
 METRIC = "RHS cell-updates/s per RK3 stage, mixed vs FP64 on 1 B200 at stated L2 error"
 UNIT = "cell-updates/s"
 N_UNIQUE = 128
-B_ALG_LES = 216  # bytes per cell-update: Q in/out/old 120, metrics 72, aj 8, nvert 8, nu_t 8
+# algorithmic bytes per cell-update of the stage kernel
+B_ALG = {
+    "fp64": 216,   # Q in/old/out 120, metrics 72, aj 8, nvert 8, nu_t 8
+    "mixed": 208,  # Q in/old/out 120, FP32 metrics 36, aj 8, nvert 8, nu_t 8, FP64 metric divergence 24, FP32 filter width 4
+}
+ACC_STEPS = 100
 
-CFG = dict(les=1, inviscid=0, fluxorder=2, eno_order=2, central=2, s_x=1.0, s_y=1.0, s_z=1.0,
+CFG = dict(les=1, inviscid=0, fluxorder=3, eno_order=2, central=2, s_x=1.0, s_y=1.0, s_z=1.0,
            ren=1600.0, ma=0.1, pr=0.71, gamma=1.4, dt=2e-3)
 
 
 def workload_config(n):
     return {
         "workload": f"compressible Taylor-Green vortex LES, {n}^3 (DMDA {n + 2}^3), perturbed curvilinear grid, "
-                    "MUSCL+Rusanov blended with skew-symmetric central (sigma=1), Smagorinsky CS=0.03, "
-                    "viscous Re 1600 Ma 0.1, SSP-RK fluxorder 2 (2 stages/step)",
+                    "WENO3+Rusanov blended with skew-symmetric central (sigma=1), Smagorinsky CS=0.03, "
+                    "viscous Re 1600 Ma 0.1, SSP-RK3 (fluxorder 3, 3 stages/step), dt 2e-3",
         "grid": [n + 2, n + 2, n + 2],
         "interior_nodes": n ** 3,
-        "stages_per_step": 2,
+        "stages_per_step": 3,
         "l2_policy": "inputs larger than L2 (~0.5 GB resident per stage vs 126 MB L2); no flush",
         "parallelism": "replicas (one independent block per GPU)",
     }
@@ -132,13 +140,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per stage-kernel launch from the committed ncu summary (scaled to the bench size)."""
-    p = os.path.join(REPO, "profiles", "stage_kernel_traffic.json")
+def profile_traffic(precision):
+    """DRAM bytes per stage-kernel launch from the committed ncu summary of
+    this workload (None when no summary for this form is committed)."""
+    p = os.path.join(REPO, "profiles", f"stage_kernel_traffic_{precision}.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         d = json.load(f)
+    if d.get("workload_id") != "tgv128-fluxorder3":
+        return None
     return d.get("dram_bytes_per_launch_scaled_to_bench")
 
 
@@ -193,10 +204,73 @@ def run_reference(args, ws, rank):
 
 
 # ------------------------------------------------------------------ our arm --
+def _block(precision, local, coords, q0, nv):
+    from chimera_comp_les_b200 import Block
+    n = coords.shape[0] - 2
+    blk = Block(n + 2, n + 2, n + 2, precision=precision, device=local, **CFG)
+    blk.FormMetrics(coords)
+    blk.set_nvert(nv)
+    blk.SetInitialCondition(q0)
+    return blk
+
+
+def _timed(blk, steps, warmup, ws, local, sample_clocks=False):
+    """Device time of `steps` resident time steps (max over ranks), clocks."""
+    import torch
+    stream = torch.cuda.ExternalStream(blk.stream, device=f"cuda:{local}")
+    blk.RungeKutta(max(warmup, 3))  # also captures the CUDA graphs of the buffer rotation
+    sampler = ClockSampler(gpu_identifier(local)) if sample_clocks else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    blk.RungeKutta(steps, sync=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = sampler.stop() if sampler else None
+    blk.sync()  # device status word: raises on NaN/Inf or rho/p <= 0
+    return max_over_ranks(e0.elapsed_time(e1), ws, local), clocks
+
+
+def _kernel_ms(blk, steps):
+    blk.timing(True)
+    blk.RungeKutta(steps)
+    rhs_ms, rhs_n, _, _ = blk.timing_read()
+    blk.timing(False)
+    return rhs_ms / max(rhs_n, 1)
+
+
+def _accuracy(fp64, mixed, q0):
+    """Both forms from the same state for ACC_STEPS steps: per-field error of
+    mixed vs FP64 at the end, KE / enstrophy history deviation."""
+    from chimera_comp_les_b200 import diagnostics as D
+    csi, eta, zet, aj = fp64.metrics()
+    hist = {"fp64": [], "mixed": []}
+    final = {}
+    for name, blk in (("fp64", fp64), ("mixed", mixed)):
+        blk.SetInitialCondition(q0)
+        for c in range(5):
+            if c:
+                blk.RungeKutta(ACC_STEPS // 4)
+            q = blk.Q()
+            hist[name].append((D.kinetic_energy(q, aj), D.enstrophy(q, csi, eta, zet, aj)))
+        final[name] = q
+    l2, linf = D.field_errors(final["mixed"], final["fp64"])
+    ke_dev = max(abs(m[0] - f[0]) / abs(f[0]) for m, f in zip(hist["mixed"], hist["fp64"]))
+    en_dev = max(abs(m[1] - f[1]) / abs(f[1]) for m, f in zip(hist["mixed"], hist["fp64"]))
+    return {"steps": ACC_STEPS, "rel_l2": l2, "rel_linf": linf, "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"],
+            "ke_history_max_rel_dev": ke_dev, "enstrophy_history_max_rel_dev": en_dev,
+            "ke": [h[0] for h in hist["fp64"]], "checkpoints_every": ACC_STEPS // 4}
+
+
 def run_ours(args, ws, rank, local):
+    import ctypes
     import torch
 
-    from chimera_comp_les_b200 import Block
     from chimera_comp_les_b200 import workloads as W
 
     torch.cuda.set_device(local)
@@ -204,50 +278,32 @@ def run_ours(args, ws, rank, local):
     coords = W.periodic_grid(n, 2 * math.pi, amp=0.05)
     q0 = W.tgv_state(coords, gamma=CFG["gamma"], ma=CFG["ma"])
     nv = np.zeros(coords.shape[:3])
-    blk = Block(n + 2, n + 2, n + 2, precision=args.precision, device=local, **CFG)
-    blk.FormMetrics(coords)
-    blk.set_nvert(nv)
-    blk.SetInitialCondition(q0)
-    stream = torch.cuda.ExternalStream(blk.stream, device=f"cuda:{local}")
-    interior = blk.interior_nodes
-    stages = blk.stages
-
-    # warm-up (also captures the CUDA graphs of the buffer rotation)
-    blk.RungeKutta(max(args.warmup, 3))
-
-    sampler = ClockSampler(gpu_identifier(local))
-    sampler.start()
-    time.sleep(0.3)
-    barrier(ws)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    blk.RungeKutta(args.steps, sync=False)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier(ws)
-    clocks = sampler.stop()
-    blk.sync()  # device status word: raises on NaN/Inf or rho/p <= 0
-    ms = e0.elapsed_time(e1)
-    ms = max_over_ranks(ms, ws, local)
-    value = ws * interior * stages * args.steps / (ms / 1e3)
-
-    # kernel timing (eager launches, events around every kernel on the library stream)
-    blk.timing(True)
-    kt_steps = max(3, min(args.steps, 10))
-    blk.RungeKutta(kt_steps)
-    rhs_ms, rhs_n, other_ms, other_n = blk.timing_read()
-    blk.timing(False)
-    avg_stage_ms = rhs_ms / max(rhs_n, 1)
-    achieved = B_ALG_LES * interior / (avg_stage_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
+
+    forms = {}
+    blocks = {}
+    for prec in ("fp64", "mixed"):
+        blk = _block(prec, local, coords, q0, nv)
+        blocks[prec] = blk
+        ms, clocks = _timed(blk, args.steps, args.warmup, ws, local, sample_clocks=(prec == args.precision))
+        interior, stages = blk.interior_nodes, blk.stages
+        kms = _kernel_ms(blk, max(3, min(args.steps, 10)))
+        achieved = B_ALG[prec] * interior / (kms / 1e3) / 1e9
+        forms[prec] = {"value": ws * interior * stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                       "clocks": clocks, "kernel_avg_ms": kms, "achieved_gbs": achieved,
+                       "launches_per_step": blk.launches_per_step}
+    head = forms[args.precision]
+    acc = _accuracy(blocks["fp64"], blocks["mixed"], q0) if rank == 0 else None
 
     # end-to-end through the C-ABI with host buffers: H2D of the step's input
     # state from pinned memory, one time step, D2H of the new state
+    blk = blocks[args.precision]
+    stream = torch.cuda.ExternalStream(blk.stream, device=f"cuda:{local}")
     e2e_steps = max(3, min(args.steps, 10))
     q_host = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True).numpy()
     q_host[...] = q0
     q_out = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    qptr = q_host.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     blk.SetInitialCondition(q_host)
     blk.RungeKutta(1)
     blk.download(q_out)
@@ -256,44 +312,53 @@ def run_ours(args, ws, rank, local):
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(e2e_steps):
-        blk.lib.cb_upload_state(blk._ctx, q_host.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_double)))
+        rc = blk.lib.cb_upload_state(blk._ctx, qptr)  # cb_upload_state: H2D + unpack, stream-ordered
+        if rc:
+            raise RuntimeError(f"cb_upload_state failed ({rc})")
         blk.RungeKutta(1, sync=False)
-        blk.download(q_out)
+        blk.download(q_out)  # cb_download_state: pack + D2H, waits for the stream
     f1.record(stream)
     torch.cuda.synchronize()
     barrier(ws)
     e2e_ms = max_over_ranks(f0.elapsed_time(f1), ws, local)
-    e2e_value = ws * interior * stages * e2e_steps / (e2e_ms / 1e3)
+    e2e_value = ws * blk.interior_nodes * blk.stages * e2e_steps / (e2e_ms / 1e3)
     if not np.isfinite(q_out).all():
         raise RuntimeError("non-finite state after end-to-end steps")
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import cpu_baseline as cb
-        r = cb.run(n, steps=2, warmup=0, cfgkw=CFG)
+        r = cb.run(n, steps=1, warmup=0, cfgkw=CFG)
         cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
 
     if rank == 0:
         cfg = workload_config(n)
         cfg["precision_form"] = args.precision
+        other = "fp64" if args.precision == "mixed" else "mixed"
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-state",
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32-flux/f64-state" if args.precision == "mixed" else "f64",
             "data": "synthetic", "config": cfg,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": profile_traffic(),
-                         "kernel": "stage_kernel (fused RHS + RK combine)",
-                         "kernel_avg_ms": avg_stage_ms, "bytes_per_cell": B_ALG_LES,
-                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback"},
-            "clocks": clocks,
+            "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": head["achieved_gbs"] / peak,
+                         "traffic": profile_traffic(args.precision),
+                         "kernel": f"stage_kernel ({args.precision} form: fused RHS + RK combine)",
+                         "kernel_avg_ms": head["kernel_avg_ms"], "bytes_per_cell": B_ALG[args.precision],
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "clocks": head["clocks"],
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(q0.nbytes), "d2h_bytes_per_step": int(q0.nbytes)},
-            "gpu_launches": blk.launches_per_step * args.steps,
+            "gpu_launches": head["launches_per_step"] * args.steps,
             "cpu_baseline": cpu,
+            other: {k: v for k, v in forms[other].items() if k != "clocks"},
+            "speedup_mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"],
+            "mixed_vs_fp64_error": acc,
         }
         print(json.dumps(line), flush=True)
-    blk.close()
+    for b in blocks.values():
+        b.close()
 
 
 def main():
@@ -302,7 +367,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="form reported as the headline value (both are measured)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

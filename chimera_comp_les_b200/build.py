@@ -13,14 +13,20 @@ import sys
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(PKG_DIR)
 LIB_PATH = os.path.join(PKG_DIR, "libchimera_b200.so")
-SOURCES = [os.path.join(PKG_DIR, "csrc", "cb_api.cu"), os.path.join(PKG_DIR, "csrc", "cb_noalloc.cu")]
+# (source, extra flags): the FP64 parity form reproduces the reference's IEEE
+# operation order (no FMA contraction, IEEE division and square root); the
+# mixed form (FP32 fluxes) is compiled with contraction and fast FP32 division.
+FP64_FLAGS = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]
+MIXED_FLAGS = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]
+SOURCES = [
+    (os.path.join(PKG_DIR, "csrc", "cb_api.cu"), FP64_FLAGS),
+    (os.path.join(PKG_DIR, "csrc", "cb_noalloc.cu"), FP64_FLAGS),
+    (os.path.join(PKG_DIR, "csrc", "cb_mixed.cu"), MIXED_FLAGS),
+]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-# The FP64 form reproduces the reference's IEEE operation order: no FMA
-# contraction (-fmad=false), IEEE division and square root.
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 ]
 
 
@@ -35,16 +41,26 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in _deps())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB_PATH
-    cmd = [NVCC] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB_PATH] + SOURCES
+def _run(cmd, verbose):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libchimera_b200.so")
+        raise RuntimeError("nvcc failed building libchimera_b200.so: " + " ".join(cmd))
     if verbose:
         sys.stderr.write(r.stderr)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not needs_build():
+        return LIB_PATH
+    objdir = os.path.join(PKG_DIR, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    for src, flags in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
+        _run([NVCC] + NVCC_FLAGS + flags + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj, src], verbose)
+        objs.append(obj)
+    _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB_PATH] + objs, verbose)
     return LIB_PATH
 
 

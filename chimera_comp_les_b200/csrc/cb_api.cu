@@ -19,6 +19,7 @@
 #include "../../include/chimera_b200.h"
 #include "cb_aux.cuh"
 #include "cb_common.cuh"
+#include "cb_launch.h"
 #include "cb_stage.cuh"
 
 using namespace cb;
@@ -45,6 +46,13 @@ struct cb_ctx {
   double *met[3][3] = {};
   double *aj = nullptr, *nvert = nullptr, *nut = nullptr, *delta2 = nullptr;
   double *rhsb[5] = {};
+  // mixed form: FP32 metric copies, FP32 filter width, FP64 metric divergence
+  void *arena_mixed = nullptr;
+  float *met32[3][3] = {};
+  float *delta2_32 = nullptr;
+  double *gcl[3] = {};
+  float **ptab32 = nullptr;
+  bool have_refs = false;
   double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
   double **ptab = nullptr;    // device pointer tables
   unsigned *status = nullptr;
@@ -75,7 +83,7 @@ static int fail(cb_ctx *c, int code, const std::string &msg) {
   } while (0)
 
 // device pointer tables inside ctx->ptab
-enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27, PT_NUT = 32, PT_MISC = 33, PT_N = 48 };
+enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27, PT_NUT = 32, PT_MISC = 33, PT_GCL = 48, PT_N = 56 };
 
 static int grid_for(const cb_ctx *c, long long work, int block = 256) {
   long long b = (work + block - 1) / block;
@@ -99,13 +107,17 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
   F.nvert = c->nvert;
   F.nut = c->nut;
   F.delta2 = c->delta2;
+  for (int e = 0; e < 3; e++)
+    for (int q = 0; q < 3; q++) F.met32[e][q] = c->met32[e][q];
+  F.delta2_32 = c->delta2_32;
+  for (int a = 0; a < 3; a++) F.gcl[a] = c->gcl[a];
   F.status = c->status;
   return F;
 }
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t set_stage_attr() {
-  return cudaFuncSetAttribute(stage_kernel<LES, VISC, RHSM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)STAGE_SMEM_BYTES);
 }
 
@@ -125,7 +137,7 @@ static cudaError_t set_stage_attrs() {
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt) {
-  auto kern = stage_kernel<LES, VISC, RHSM>;
+  auto kern = stage_kernel<double, false, LES, VISC, RHSM>;
   const int nkin = c->dc.mz - 2;
   dim3 grid((c->dc.mx - 2 + BX - 1) / BX, (c->dc.my - 2 + BY - 1) / BY, (nkin + c->kchunk - 1) / c->kchunk);
   kern<<<grid, SNT, STAGE_SMEM_BYTES, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
@@ -134,6 +146,8 @@ static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, dou
 
 static cudaError_t launch_stage(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt, bool rhs_mode) {
   const bool les = c->cfg.les != 0, visc = c->cfg.inviscid == 0;
+  if (c->cfg.precision == CB_MIXED)
+    return launch_stage_mixed(c->dc, F, istage, alfa, beta, adt, c->kchunk, les, visc, rhs_mode, c->stream);
   if (rhs_mode) {
     if (les && visc) return launch_stage_t<true, true, true>(c, F, istage, alfa, beta, adt);
     if (les) return launch_stage_t<true, false, true>(c, F, istage, alfa, beta, adt);
@@ -262,7 +276,15 @@ static int fill_ptab(cb_ctx *c) {
   for (int e = 0; e < 3; e++)
     for (int q = 0; q < 3; q++) h[PT_MISC + 2 + 3 * e + q] = c->met[e][q];
   h[PT_MISC + 11] = c->aj;
+  for (int a = 0; a < 3; a++) h[PT_GCL + a] = c->gcl[a];
   CB_CUDA(c, cudaMemcpyAsync(c->ptab, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  if (c->ptab32) {
+    float *h32[16] = {};
+    for (int e = 0; e < 3; e++)
+      for (int q = 0; q < 3; q++) h32[3 * e + q] = c->met32[e][q];
+    h32[9] = c->delta2_32;
+    CB_CUDA(c, cudaMemcpyAsync(c->ptab32, h32, sizeof(h32), cudaMemcpyHostToDevice, c->stream));
+  }
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
   return CB_OK;
 }
@@ -305,12 +327,14 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3) return bail(CB_E_ARG, "fluxorder must be 1, 2 or 3");
   if (cfg->eno_order != 2 && cfg->eno_order != 3) return bail(CB_E_ARG, "ENOorder must be 2 or 3");
   if (cfg->les != 0 && cfg->les != 1) return bail(CB_E_UNSUPPORTED, "only les 0 or 1 (constant Smagorinsky) is built");
-  if (cfg->precision != CB_FP64) return bail(CB_E_UNSUPPORTED, "precision form not built");
+  if (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) return bail(CB_E_ARG, "precision must be CB_FP64 or CB_MIXED");
   c->dev = cfg->device;
   if (cudaSetDevice(c->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice failed");
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(CB_E_CUDA, "stream");
   if (set_stage_attrs() != cudaSuccess) return bail(CB_E_CUDA, "stage kernel shared-memory opt-in failed");
+  if (cfg->precision == CB_MIXED && set_stage_attrs_mixed() != cudaSuccess)
+    return bail(CB_E_CUDA, "mixed stage kernel shared-memory opt-in failed");
   DevCfg &d = c->dc;
   d.mx = cfg->mx; d.my = cfg->my; d.mz = cfg->mz;
   d.px = ((cfg->mx + 4 + 15) / 16) * 16;
@@ -343,6 +367,18 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   c->delta2 = c->arena + c->plane * (p++);
   const size_t nn = (size_t)cfg->mx * cfg->my * cfg->mz;
   if (cudaMalloc(&c->staging, sizeof(double) * 5 * nn) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc staging");
+  if (cfg->precision == CB_MIXED) {
+    const size_t mbytes = sizeof(float) * c->plane * 10 + sizeof(double) * c->plane * 3;
+    if (cudaMalloc(&c->arena_mixed, mbytes) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc mixed planes");
+    if (cudaMemsetAsync(c->arena_mixed, 0, mbytes, c->stream) != cudaSuccess) return bail(CB_E_CUDA, "memset");
+    float *f = (float *)c->arena_mixed;
+    for (int e = 0; e < 3; e++)
+      for (int q = 0; q < 3; q++) c->met32[e][q] = f + c->plane * (3 * e + q);
+    c->delta2_32 = f + c->plane * 9;
+    double *g = (double *)(f + c->plane * 10);
+    for (int a = 0; a < 3; a++) c->gcl[a] = g + c->plane * a;
+    if (cudaMalloc(&c->ptab32, sizeof(float *) * 16) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab32");
+  }
   if (cudaMalloc(&c->ptab, sizeof(double *) * PT_N) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab");
   if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc status");
   cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream);
@@ -372,6 +408,8 @@ void cb_destroy(cb_ctx *c) {
   if (c->rhsb[0]) cudaFree(c->rhsb[0]);
   if (c->arena) cudaFree(c->arena);
   if (c->staging) cudaFree(c->staging);
+  if (c->arena_mixed) cudaFree(c->arena_mixed);
+  if (c->ptab32) cudaFree(c->ptab32);
   if (c->ptab) cudaFree(c->ptab);
   if (c->status) cudaFree(c->status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -417,6 +455,9 @@ int cb_set_grid(cb_ctx *c, const double *coor) {
   ghost_fill_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->ptab + PT_MISC + 2, 10);
   delta2_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->aj, c->delta2);
   CB_CUDA(c, cudaGetLastError());
+  if (c->cfg.precision == CB_MIXED)
+    CB_CUDA(c, launch_mixed_prep(c->dc, (const double *const *)(c->ptab + PT_MET), c->delta2, c->ptab32, c->delta2_32,
+                                 c->ptab + PT_GCL, grid_for(c, (long long)c->plane), c->stream));
   // scrub buffer 2 (coordinates) so later ghost reads see zeros until written
   for (int q = 0; q < 3; q++) CB_CUDA(c, cudaMemsetAsync(X[q], 0, sizeof(double) * c->plane, c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -435,6 +476,9 @@ int cb_set_metrics(cb_ctx *c, const double *csi, const double *eta, const double
   const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
   delta2_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->aj, c->delta2);
   CB_CUDA(c, cudaGetLastError());
+  if (c->cfg.precision == CB_MIXED)
+    CB_CUDA(c, launch_mixed_prep(c->dc, (const double *const *)(c->ptab + PT_MET), c->delta2, c->ptab32, c->delta2_32,
+                                 c->ptab + PT_GCL, grid_for(c, (long long)c->plane), c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_grid = true;
   invalidate_graphs(c);
@@ -465,8 +509,29 @@ int cb_set_nvert(cb_ctx *c, const double *nvert) {
   return CB_OK;
 }
 
+// Mixed form: the reference state subtracted before FP32 rounding, the means
+// of p, rhoE and T=p/rho over the owned nodes of the first uploaded state.
+static void set_reference_state(cb_ctx *c, const double *q) {
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  double sp = 0, se = 0, st = 0;
+  for (size_t t = 0; t < nn; t++) {
+    const double *v = q + 5 * t;
+    const double p = (c->cfg.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0]);
+    sp += p;
+    se += v[4];
+    st += p / v[0];
+  }
+  c->dc.p_ref = sp / nn;
+  c->dc.e_ref = se / nn;
+  c->dc.t_ref = st / nn;
+  c->dc.h_ref = c->dc.e_ref + c->dc.p_ref;
+  c->have_refs = true;
+  invalidate_graphs(c);
+}
+
 int cb_upload_state(cb_ctx *c, const double *q) {
   if (!c || !q) return CB_E_ARG;
+  if (c->cfg.precision == CB_MIXED && !c->have_refs) set_reference_state(c, q);
   c->cur = 0;
   c->uc = -1;
   int e = upload_planes(c, q, 5, PT_Q0, false);

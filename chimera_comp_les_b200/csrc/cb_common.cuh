@@ -28,6 +28,8 @@ struct DevCfg {
   double inv_ren;       // 1./ren
   double inv_ren_half;  // 1./ren*0.5
   double gm1;           // gamma-1.0
+  // mixed form: reference state subtracted before FP32 rounding
+  double p_ref, e_ref, t_ref, h_ref;  // h_ref = e_ref + p_ref
 };
 
 struct DevFields {
@@ -39,6 +41,9 @@ struct DevFields {
   const double *nvert;
   const double *nut;
   const double *delta2;    // LES filter width squared, pow(pow(1/aj,1/3),2), per node
+  const float *met32[3][3];  // mixed form: FP32 copies of the metrics
+  const float *delta2_32;    // mixed form: FP32 copy of delta2
+  const double *gcl[3];      // mixed form: per-node metric divergence sum_d dh_d (FP64)
   double *rhs[5];          // formRHS output (rhs mode only)
   unsigned *status;        // sticky status word
 };

@@ -1,0 +1,19 @@
+// Host launchers of the stage kernel, one per translation unit: the FP64
+// parity form is compiled without FMA contraction (cb_api.cu), the mixed form
+// with it (cb_mixed.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "cb_common.cuh"
+
+namespace cb {
+
+cudaError_t set_stage_attrs_mixed();
+cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt,
+                               int kchunk, bool les, bool visc, bool rhs_mode, cudaStream_t s);
+// FP32 metric copies, FP32 filter width and the FP64 metric divergence
+// (sum over directions of h(+1/2) - h(-1/2)) for the mixed form.
+cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, float *const *met32,
+                              float *delta2_32, double *const *gcl, int grid, cudaStream_t s);
+
+}  // namespace cb

@@ -1,0 +1,82 @@
+// Mixed-precision form of the stage kernel (FP32 flux arithmetic, FP64 state,
+// EOS and RK combination).  Compiled with FMA contraction and fast FP32
+// division/sqrt; see cb_stage.cuh for the shift of the reference state.
+#include "cb_launch.h"
+#include "cb_stage.cuh"
+
+namespace cb {
+
+namespace {
+template <bool LES, bool VISC, bool RHSM>
+cudaError_t attr1() {
+  return cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)STAGE_SMEM_BYTES_MIXED);
+}
+template <bool LES, bool VISC, bool RHSM>
+void launch1(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt, int kchunk,
+             cudaStream_t s) {
+  const int nkin = c.mz - 2;
+  dim3 grid((c.mx - 2 + SBX - 1) / SBX, (c.my - 2 + SBY - 1) / SBY, (nkin + kchunk - 1) / kchunk);
+  stage_kernel<float, true, LES, VISC, RHSM><<<grid, SNT, STAGE_SMEM_BYTES_MIXED, s>>>(c, F, istage, alfa, beta, adt, kchunk);
+}
+
+__global__ void mixed_prep_kernel(const DevCfg c, const double *const *met, const double *delta2, float *const *met32,
+                                  float *delta2_32, double *const *gcl) {
+  const long long total = (long long)c.px * c.py * c.pz;
+  const long long nx = c.px, ny = c.py;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    for (int q = 0; q < 9; q++) met32[q][t] = (float)met[q][t];
+    delta2_32[t] = (float)delta2[t];
+    const int i = (int)(t % nx) - 2, j = (int)((t / nx) % ny) - 2, k = (int)(t / (nx * ny)) - 2;
+    const bool interior = i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2;
+    for (int a = 0; a < 3; a++) {
+      double s = 0.;
+      if (interior) {
+        for (int d = 0; d < 3; d++) {
+          const long long sd = gstride(c, d);
+          const double *m = met[3 * d + a];
+          const double hp = 0.5 * (m[t] + m[t + sd]), hm = 0.5 * (m[t - sd] + m[t]);
+          s += hp - hm;
+        }
+      }
+      gcl[a][t] = s;
+    }
+  }
+}
+}  // namespace
+
+cudaError_t set_stage_attrs_mixed() {
+  cudaError_t e;
+  if ((e = attr1<true, true, false>()) != cudaSuccess) return e;
+  if ((e = attr1<true, false, false>()) != cudaSuccess) return e;
+  if ((e = attr1<false, true, false>()) != cudaSuccess) return e;
+  if ((e = attr1<false, false, false>()) != cudaSuccess) return e;
+  if ((e = attr1<true, true, true>()) != cudaSuccess) return e;
+  if ((e = attr1<true, false, true>()) != cudaSuccess) return e;
+  if ((e = attr1<false, true, true>()) != cudaSuccess) return e;
+  return attr1<false, false, true>();
+}
+
+cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt,
+                               int kchunk, bool les, bool visc, bool rhs_mode, cudaStream_t s) {
+  if (rhs_mode) {
+    if (les && visc) launch1<true, true, true>(c, F, istage, alfa, beta, adt, kchunk, s);
+    else if (les) launch1<true, false, true>(c, F, istage, alfa, beta, adt, kchunk, s);
+    else if (visc) launch1<false, true, true>(c, F, istage, alfa, beta, adt, kchunk, s);
+    else launch1<false, false, true>(c, F, istage, alfa, beta, adt, kchunk, s);
+  } else {
+    if (les && visc) launch1<true, true, false>(c, F, istage, alfa, beta, adt, kchunk, s);
+    else if (les) launch1<true, false, false>(c, F, istage, alfa, beta, adt, kchunk, s);
+    else if (visc) launch1<false, true, false>(c, F, istage, alfa, beta, adt, kchunk, s);
+    else launch1<false, false, false>(c, F, istage, alfa, beta, adt, kchunk, s);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, float *const *met32,
+                              float *delta2_32, double *const *gcl, int grid, cudaStream_t s) {
+  mixed_prep_kernel<<<grid, 256, 0, s>>>(c, met, delta2, met32, delta2_32, gcl);
+  return cudaGetLastError();
+}
+
+}  // namespace cb

@@ -54,7 +54,7 @@ NaDevice g_dev[64];
 
 template <bool LES, bool VISC>
 cudaError_t na_attr() {
-  return cudaFuncSetAttribute(stage_kernel<LES, VISC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)STAGE_SMEM_BYTES);
 }
 
@@ -62,7 +62,7 @@ template <bool LES, bool VISC>
 void na_launch_rhs(const DevCfg &dc, const DevFields &F, int kchunk, cudaStream_t s) {
   const int nkin = dc.mz - 2;
   dim3 grid((dc.mx - 2 + SBX - 1) / SBX, (dc.my - 2 + SBY - 1) / SBY, (nkin + kchunk - 1) / kchunk);
-  stage_kernel<LES, VISC, true><<<grid, SNT, STAGE_SMEM_BYTES, s>>>(dc, F, 0, 0., 0., 0., kchunk);
+  stage_kernel<double, false, LES, VISC, true><<<grid, SNT, STAGE_SMEM_BYTES, s>>>(dc, F, 0, 0., 0., 0., kchunk);
 }
 
 int na_fail(int code, const char *msg) {

@@ -1,5 +1,5 @@
 // Fused stage kernel: formRHS (inviscid + viscous + SGS face fluxes, flux
-// difference, MultAj) followed by the SSP-RK stage combination, FP64.
+// difference, MultAj) followed by the SSP-RK stage combination.
 //
 // Reference arithmetic restated (rhs.c):
 //   formConvection      2570-3224   (non-LES upwind: first order / MUSCL / WENO3, Rusanov)
@@ -8,14 +8,24 @@
 //   MultAj / formRHS    4575-4736
 //   RungeKutta          solvers.c:232-271 (stage combination)
 //
-// Execution shape (B200): a block owns a BX x BY column of interior nodes and
+// Two forms share this code, selected by the flux type R:
+//   R = double, MIX = false : the FP64 parity form, the reference's IEEE operation order.
+//   R = float,  MIX = true  : the mixed form.  The state, the EOS and the RK combination
+//     stay FP64; reconstruction, Riemann/central fluxes, viscous and SGS terms run in FP32.
+//     FP64 -> FP32 rounding would erase the low-Mach pressure signal (p ~ 100, dp ~ 0.06),
+//     so the FP64 EOS delivers p' = p - p_ref, rhoE' = rhoE - E_ref, T' = T - T_ref and the
+//     FP32 fluxes carry only fluctuations.  The constant part p_ref*h of every momentum
+//     face flux is restored exactly in FP64 through the per-node metric divergence
+//     gcl = sum_d (h_d(+1/2) - h_d(-1/2)); the constant part H_ref = E_ref + p_ref of the
+//     energy flux is carried in FP32 (its error is relative to H_ref * dU).
+//
+// Execution shape (B200): a block owns a SBX x SBY column of interior nodes and
 // marches along k through a chunk of planes.  A ring of four node planes
 // (k-1 .. k+2, each with a two-node halo in i and j) lives in shared memory
 // holding the conserved state and the derived p, u, v, w, T=p/rho, so every
 // division of the EOS / CalcUCat happens once per node.  Each face flux is
-// computed exactly once: i- and j-faces of the current plane go to shared
-// memory, the k-face k+1/2 stays in registers and becomes k-1/2 of the next
-// plane.  Metrics, nvert and nu_t are read through the read-only cache.
+// computed exactly once per plane.  Metrics, nvert and nu_t are read through
+// the read-only cache.
 #pragma once
 #include "cb_common.cuh"
 
@@ -23,7 +33,6 @@ namespace cb {
 
 constexpr int NF = 10;  // fields per node in the plane ring
 enum { F_RHO = 0, F_RU, F_RV, F_RW, F_RE, F_P, F_U, F_V, F_W, F_T };
-constexpr int NG = 13;  // per face: Fconv[0..4], Fvisc[5..9], LES stress part A[10..12]
 
 constexpr double BLANKWALL = 2.9;
 constexpr double BLANK = 0.1;
@@ -31,19 +40,43 @@ constexpr double SOLID = 0.5;
 constexpr double INNERBLANK = 7.;
 constexpr double GAMMA_CONV = 1.4;  // formConvection[LES] fix gamma = 1.4 (rhs.c:2596, 3257)
 
+// face buffer width: FP64 keeps conv (5), visc (5), LES stress (3) apart to
+// difference them in the reference's order; the mixed form stores visc-conv.
+template <bool MIX>
+struct FaceWidth {
+  static constexpr int NG = MIX ? 8 : 13;
+  static constexpr int VOFF = MIX ? 0 : 5;   // visc offset
+  static constexpr int AOFF = MIX ? 5 : 10;  // LES stress offset
+};
+
 template <int BX, int BY>
 struct TileShape {
   static constexpr int PX = BX + 4, PY = BY + 4, PN = PX * PY;
   static constexpr int NXF = (BX + 1) * BY;
   static constexpr int NYF = BX * (BY + 1);
-  static constexpr size_t smem_bytes = sizeof(double) * ((size_t)4 * NF * PN + (size_t)NG * (NXF + NYF));
 };
 
 // Selections by a runtime direction d without dynamic indexing (which would
 // place the indexed array in local memory).
-__device__ __forceinline__ const double *met_ptr(const DevFields &F, int d, int q) {
+template <typename R>
+__device__ __forceinline__ const R *met_ptr(const DevFields &F, int d, int q);
+template <>
+__device__ __forceinline__ const double *met_ptr<double>(const DevFields &F, int d, int q) {
   return d == 0 ? F.met[0][q] : (d == 1 ? F.met[1][q] : F.met[2][q]);
 }
+template <>
+__device__ __forceinline__ const float *met_ptr<float>(const DevFields &F, int d, int q) {
+  return d == 0 ? F.met32[0][q] : (d == 1 ? F.met32[1][q] : F.met32[2][q]);
+}
+template <typename R>
+__device__ __forceinline__ const R *met_ptr_e(const DevFields &F, int e, int q);
+template <>
+__device__ __forceinline__ const double *met_ptr_e<double>(const DevFields &F, int e, int q) { return F.met[e][q]; }
+template <>
+__device__ __forceinline__ const float *met_ptr_e<float>(const DevFields &F, int e, int q) { return F.met32[e][q]; }
+template <typename R>
+__device__ __forceinline__ R ldr(const R *p) { return __ldg(p); }
+
 __device__ __forceinline__ int bc_lo(const DevCfg &c, int d) { return d == 0 ? c.bctype[0] : (d == 1 ? c.bctype[2] : c.bctype[4]); }
 __device__ __forceinline__ int bc_hi(const DevCfg &c, int d) { return d == 0 ? c.bctype[1] : (d == 1 ? c.bctype[3] : c.bctype[5]); }
 
@@ -58,97 +91,107 @@ __device__ __forceinline__ NRef nshift(NRef n, int d, int s) {
   return n;
 }
 
-template <int BX, int BY>
+template <typename R, int BX, int BY>
 struct Ring {
-  double *pl;
+  R *pl;
   int slot[4];
-  __device__ __forceinline__ double get(int f, NRef n) const {
+  __device__ __forceinline__ R get(int f, NRef n) const {
     return pl[((slot[n.r + 1] * NF + f) * TileShape<BX, BY>::PY + n.y) * TileShape<BX, BY>::PX + n.x];
-  }
-  __device__ __forceinline__ double *ptr(int s, int f) const {
-    return pl + (size_t)(s * NF + f) * TileShape<BX, BY>::PN;
   }
 };
 
 // ---------------------------------------------------------------- recon --
-__device__ __forceinline__ double d_sgn(double a) { return (a >= 0) ? ((a == 0) ? 0. : 1.) : -1.; }
-__device__ __forceinline__ double d_minmod(double a, double b) {
-  if (a * b < 0) return 0.;
-  double fa = fabs(a), fb = fabs(b);
-  return d_sgn(a) * ((fa < fb) ? fa : fb);
+template <typename R>
+__device__ __forceinline__ R r_sgn(R a) { return (a >= R(0)) ? ((a == R(0)) ? R(0.) : R(1.)) : R(-1.); }
+template <typename R>
+__device__ __forceinline__ R r_minmod(R a, R b) {
+  if (a * b < R(0)) return R(0.);
+  R fa = fabs(a), fb = fabs(b);
+  return r_sgn(a) * ((fa < fb) ? fa : fb);
 }
-__device__ __forceinline__ double muscl_l(double qm, double q0, double qp) { return q0 + 0.5 * d_minmod(qp - q0, q0 - qm); }
-__device__ __forceinline__ double muscl_r(double qm, double q0, double qp) { return q0 - 0.5 * d_minmod(qp - q0, q0 - qm); }
-__device__ __forceinline__ double weno3_l(double qm, double q0, double qp) {
-  const double d0 = 0.6666667, d1 = 0.3333333, eps = 1e-6;  // rhs.c:2386 (truncated weights)
-  double r0 = 0.5 * q0 + 0.5 * qp, r1 = -0.5 * qm + 1.5 * q0;
-  double b0 = (qp - q0) * (qp - q0), b1 = (qm - q0) * (qm - q0);
-  double a0 = d0 / ((eps + b0) * (eps + b0)), a1 = d1 / ((eps + b1) * (eps + b1));
-  double as = a0 + a1;
+template <typename R>
+__device__ __forceinline__ R muscl_l(R qm, R q0, R qp) { return q0 + R(0.5) * r_minmod(qp - q0, q0 - qm); }
+template <typename R>
+__device__ __forceinline__ R muscl_r(R qm, R q0, R qp) { return q0 - R(0.5) * r_minmod(qp - q0, q0 - qm); }
+template <typename R>
+__device__ __forceinline__ R weno3_l(R qm, R q0, R qp) {
+  const R d0 = R(0.6666667), d1 = R(0.3333333), eps = R(1e-6);  // rhs.c:2386 (truncated weights)
+  R r0 = R(0.5) * q0 + R(0.5) * qp, r1 = R(-0.5) * qm + R(1.5) * q0;
+  R b0 = (qp - q0) * (qp - q0), b1 = (qm - q0) * (qm - q0);
+  R a0 = d0 / ((eps + b0) * (eps + b0)), a1 = d1 / ((eps + b1) * (eps + b1));
+  R as = a0 + a1;
   return (a0 / as) * r0 + (a1 / as) * r1;
 }
-__device__ __forceinline__ double weno3_r(double qm, double q0, double qp) {
-  const double d0 = 0.6666667, d1 = 0.3333333, eps = 1e-6;
-  double r0 = 1.5 * q0 - 0.5 * qp, r1 = 0.5 * qm + 0.5 * q0;
-  double b0 = (qp - q0) * (qp - q0), b1 = (qm - q0) * (qm - q0);
-  double a0 = d0 / ((eps + b0) * (eps + b0)), a1 = d1 / ((eps + b1) * (eps + b1));
-  double as = a0 + a1;
+template <typename R>
+__device__ __forceinline__ R weno3_r(R qm, R q0, R qp) {
+  const R d0 = R(0.6666667), d1 = R(0.3333333), eps = R(1e-6);
+  R r0 = R(1.5) * q0 - R(0.5) * qp, r1 = R(0.5) * qm + R(0.5) * q0;
+  R b0 = (qp - q0) * (qp - q0), b1 = (qm - q0) * (qm - q0);
+  R a0 = d0 / ((eps + b0) * (eps + b0)), a1 = d1 / ((eps + b1) * (eps + b1));
+  R as = a0 + a1;
   return (a0 / as) * r0 + (a1 / as) * r1;
 }
-__device__ __forceinline__ double eno_r(double qm, double q0, double qp, int k) {
-  if (k == 2) return 0.5 * q0 + 0.5 * qp;
-  return -qm * 0.1666666666666666 + q0 * 0.8333333333333333 + qp * 0.3333333333333333;
+template <typename R>
+__device__ __forceinline__ R eno_r(R qm, R q0, R qp, int k) {
+  if (k == 2) return R(0.5) * q0 + R(0.5) * qp;
+  return -qm * R(0.1666666666666666) + q0 * R(0.8333333333333333) + qp * R(0.3333333333333333);
 }
-__device__ __forceinline__ double eno_l(double qm, double q0, double qp, int k) {
-  if (k == 2) return 0.5 * q0 + 0.5 * qm;
-  return qm * 0.3333333333333333 + q0 * 0.8333333333333333 - qp * 0.1666666666666666;
+template <typename R>
+__device__ __forceinline__ R eno_l(R qm, R q0, R qp, int k) {
+  if (k == 2) return R(0.5) * q0 + R(0.5) * qm;
+  return qm * R(0.3333333333333333) + q0 * R(0.8333333333333333) - qp * R(0.1666666666666666);
 }
 
 // Rusanov flux on reconstructed states (rhs.c:2769-2810), same operation
-// order as the reference (divisions, no reciprocal reuse).
-__device__ __forceinline__ void rusanov(const double QL[5], const double QR[5], double pL, double pR,
-                                        const double h[3], bool use_qr_for_l, bool r_from_l, double F[5]) {
-  double uconL = use_qr_for_l ? (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]))
-                              : (h[0] * (QL[1] / QL[0]) + h[1] * (QL[2] / QL[0]) + h[2] * (QL[3] / QL[0]));
-  double uconR = r_from_l ? uconL : (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
-  double gii = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
-  double cL = GAMMA_CONV * pL / QL[0], cR = GAMMA_CONV * pR / QR[0];
-  double saL = fabs(uconL) + sqrt(fabs(cL) * gii);
-  double saR = fabs(uconR) + sqrt(fabs(cR) * gii);
-  double SA = (saL < saR) ? saR : saL;
-  F[0] = 0.5 * (QL[0] * uconL + QR[0] * uconR) - 0.5 * SA * (QR[0] - QL[0]);
+// order as the reference (divisions, no reciprocal reuse).  In the mixed form
+// pL/pR are p - p_ref (the sound speed adds p_ref back) and Uf returns the
+// face velocity measure 0.5*(uconL + uconR) that multiplies H_ref.
+template <typename R, bool MIX>
+__device__ __forceinline__ void rusanov(const R QL[5], const R QR[5], R pL, R pR, const R h[3], bool use_qr_for_l,
+                                        bool r_from_l, R pref, R F[5], R &Uf) {
+  R uconL = use_qr_for_l ? (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]))
+                         : (h[0] * (QL[1] / QL[0]) + h[1] * (QL[2] / QL[0]) + h[2] * (QL[3] / QL[0]));
+  R uconR = r_from_l ? uconL : (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
+  R gii = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+  R cL = R(GAMMA_CONV) * (MIX ? pL + pref : pL) / QL[0], cR = R(GAMMA_CONV) * (MIX ? pR + pref : pR) / QR[0];
+  R saL = fabs(uconL) + sqrt(fabs(cL) * gii);
+  R saR = fabs(uconR) + sqrt(fabs(cR) * gii);
+  R SA = (saL < saR) ? saR : saL;
+  F[0] = R(0.5) * (QL[0] * uconL + QR[0] * uconR) - R(0.5) * SA * (QR[0] - QL[0]);
 #pragma unroll
   for (int a = 0; a < 3; a++)
-    F[1 + a] = 0.5 * ((QL[1 + a] * uconL + QR[1 + a] * uconR) + (pL * h[a] + pR * h[a])) - 0.5 * SA * (QR[1 + a] - QL[1 + a]);
-  F[4] = 0.5 * ((pL + QL[4]) * uconL + (pR + QR[4]) * uconR) - 0.5 * SA * (QR[4] - QL[4]);
+    F[1 + a] = R(0.5) * ((QL[1 + a] * uconL + QR[1 + a] * uconR) + (pL * h[a] + pR * h[a])) - R(0.5) * SA * (QR[1 + a] - QL[1 + a]);
+  F[4] = R(0.5) * ((pL + QL[4]) * uconL + (pR + QR[4]) * uconR) - R(0.5) * SA * (QR[4] - QL[4]);
+  Uf = MIX ? R(0.5) * (uconL + uconR) : R(0);
 }
 
 // ------------------------------------------------------- inviscid face ----
 // Face between node A (tile ref a, global (gi,gj,gk)) and A + e_d.
-template <bool LES, int BX, int BY>
-__device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, const Ring<BX, BY> &R, int d, NRef a,
-                                          int gi, int gj, int gk, double Fc[5]) {
+template <typename R, bool MIX, bool LES, int BX, int BY>
+__device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, int d, NRef a,
+                                          int gi, int gj, int gk, R Fc[5]) {
   const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d);
   const int pos = d == 0 ? gi : (d == 1 ? gj : gk);
   const int m = d == 0 ? c.mx : (d == 1 ? c.my : c.mz);
   const double nvm = ldg(F.nvert + g0 - sd), nv0 = ldg(F.nvert + g0), nv1 = ldg(F.nvert + g0 + sd),
                nv2 = ldg(F.nvert + g0 + 2 * sd);
-  const double *met[3] = {met_ptr(F, d, 0), met_ptr(F, d, 1), met_ptr(F, d, 2)};
-  double h[3];
+  const R *met[3] = {met_ptr<R>(F, d, 0), met_ptr<R>(F, d, 1), met_ptr<R>(F, d, 2)};
+  R h[3];
 #pragma unroll
-  for (int q = 0; q < 3; q++) h[q] = 0.5 * (ldg(met[q] + g0) + ldg(met[q] + g0 + sd));
+  for (int q = 0; q < 3; q++) h[q] = R(0.5) * (ldr(met[q] + g0) + ldr(met[q] + g0 + sd));
+  const R pref = R(c.p_ref), href = R(c.h_ref);
 
   // stencil values along d: s=0..3 -> node offsets -1..2
-  double Q[4][5], P[4];
+  R Q[4][5], P[4];
 #pragma unroll
   for (int s = 0; s < 4; s++) {
     NRef n = nshift(a, d, s - 1);
 #pragma unroll
-    for (int q = 0; q < 5; q++) Q[s][q] = R.get(F_RHO + q, n);
-    P[s] = R.get(F_P, n);
+    for (int q = 0; q < 5; q++) Q[s][q] = Rg.get(F_RHO + q, n);
+    P[s] = Rg.get(F_P, n);
   }
 
-  double QL[5], QR[5], pL, pR;
+  R QL[5], QR[5], pL, pR;
   const int fo = c.fluxorder;
   bool first;
   if (LES) {
@@ -212,86 +255,91 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
       pR = weno3_r(P[1], P[2], P[3]);
     }
   }
-  double Fw[5];
+  R Fw[5], Ufw;
   if (LES) {
-    rusanov(QL, QR, pL, pR, h, false, false, Fw);
+    rusanov<R, MIX>(QL, QR, pL, pR, h, false, false, pref, Fw, Ufw);
   } else {
     const bool use_qr_l = (pos == m - 2 && bc_hi(c, d) == 1);
     const bool r_from_l = (pos == 0 && bc_lo(c, d) == 1);
-    rusanov(QL, QR, pL, pR, h, use_qr_l, r_from_l, Fw);
+    rusanov<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, Fw, Ufw);
   }
   if (!LES) {
 #pragma unroll
     for (int q = 0; q < 5; q++) Fc[q] = Fw[q];
+    if (MIX) Fc[4] += href * Ufw;
     return;
   }
 
   // central flux (rhs.c:3483-3547) and blend
-  double Fcen[5];
+  R Fcen[5], Ufc;
   bool four = false;
   if (pos > 0 && pos < m - 2) {
     double nsum = (d == 0) ? nv0 + nv1 + nv2 + nvm : nvm + nv0 + nv1 + nv2;
     four = nsum < 2.9;
   }
   if (four && (c.central == 2 || c.central == 3)) {
-    double U[4], EP[4];
+    R U[4], EP[4];
 #pragma unroll
     for (int s = 0; s < 4; s++) {
       const long long gs = g0 + (s - 1) * sd;
-      U[s] = 1. / Q[s][0] * (ldg(met[0] + gs) * Q[s][1] + ldg(met[1] + gs) * Q[s][2] + ldg(met[2] + gs) * Q[s][3]);
+      U[s] = R(1.) / Q[s][0] * (ldr(met[0] + gs) * Q[s][1] + ldr(met[1] + gs) * Q[s][2] + ldr(met[2] + gs) * Q[s][3]);
       EP[s] = P[s] + Q[s][4];
     }
-    const double fp4 = 1.0 / 12.0 * (-P[0] + 7 * P[1] + 7 * P[2] - P[3]);
+    const R fp4 = R(1.0) / R(12.0) * (-P[0] + R(7) * P[1] + R(7) * P[2] - P[3]);
     if (c.central == 2) {
-#define CB_FP2(A0, A1, A2, A3) ((A1 + A2) * (U[1] + U[2]) / 3.0 - 1. / 24. * (A0 * U[0] + A0 * U[2] + A1 * U[1] + A1 * U[3] + A2 * U[2] + A2 * U[0] + A3 * U[1] + A3 * U[3]))
+#define CB_FP2(A0, A1, A2, A3) ((A1 + A2) * (U[1] + U[2]) / R(3.0) - R(1.) / R(24.) * (A0 * U[0] + A0 * U[2] + A1 * U[1] + A1 * U[3] + A2 * U[2] + A2 * U[0] + A3 * U[1] + A3 * U[3]))
       Fcen[0] = CB_FP2(Q[0][0], Q[1][0], Q[2][0], Q[3][0]);
       Fcen[1] = CB_FP2(Q[0][1], Q[1][1], Q[2][1], Q[3][1]) + fp4 * h[0];
       Fcen[2] = CB_FP2(Q[0][2], Q[1][2], Q[2][2], Q[3][2]) + fp4 * h[1];
       Fcen[3] = CB_FP2(Q[0][3], Q[1][3], Q[2][3], Q[3][3]) + fp4 * h[2];
       Fcen[4] = CB_FP2(EP[0], EP[1], EP[2], EP[3]);
+      Ufc = MIX ? CB_FP2(R(1), R(1), R(1), R(1)) : R(0);
 #undef CB_FP2
     } else {
-#define CB_FP1(A0, A1, A2, A3) (1.0 / 12.0 * (-A0 * U[0] + 7 * A1 * U[1] + 7 * A2 * U[2] - A3 * U[3]))
+#define CB_FP1(A0, A1, A2, A3) (R(1.0) / R(12.0) * (-A0 * U[0] + R(7) * A1 * U[1] + R(7) * A2 * U[2] - A3 * U[3]))
       Fcen[0] = CB_FP1(Q[0][0], Q[1][0], Q[2][0], Q[3][0]);
       Fcen[1] = CB_FP1(Q[0][1], Q[1][1], Q[2][1], Q[3][1]) + fp4 * h[0];
       Fcen[2] = CB_FP1(Q[0][2], Q[1][2], Q[2][2], Q[3][2]) + fp4 * h[1];
       Fcen[3] = CB_FP1(Q[0][3], Q[1][3], Q[2][3], Q[3][3]) + fp4 * h[2];
       Fcen[4] = CB_FP1(EP[0], EP[1], EP[2], EP[3]);
+      Ufc = MIX ? CB_FP1(R(1), R(1), R(1), R(1)) : R(0);
 #undef CB_FP1
     }
   } else {
-    const double rc = 0.5 * (Q[1][0] + Q[2][0]), uc = 0.5 * (Q[1][1] + Q[2][1]), vc = 0.5 * (Q[1][2] + Q[2][2]);
-    const double wc = 0.5 * (Q[1][3] + Q[2][3]), ec = 0.5 * (Q[1][4] + Q[2][4]);
-    const double Uc = (h[0] * uc + h[1] * vc + h[2] * wc) / rc;
-    const double pa = 0.5 * (P[1] + P[2]);
+    const R rc = R(0.5) * (Q[1][0] + Q[2][0]), uc = R(0.5) * (Q[1][1] + Q[2][1]), vc = R(0.5) * (Q[1][2] + Q[2][2]);
+    const R wc = R(0.5) * (Q[1][3] + Q[2][3]), ec = R(0.5) * (Q[1][4] + Q[2][4]);
+    const R Uc = (h[0] * uc + h[1] * vc + h[2] * wc) / rc;
+    const R pa = R(0.5) * (P[1] + P[2]);
     Fcen[0] = rc * Uc;
     Fcen[1] = uc * Uc + pa * h[0];
     Fcen[2] = vc * Uc + pa * h[1];
     Fcen[3] = wc * Uc + pa * h[2];
     Fcen[4] = Uc * (ec + pa);
+    Ufc = MIX ? Uc : R(0);
   }
-  const double sigma = sigma_at(c, d, gi, gj, gk);
+  const R sigma = R(sigma_at(c, d, gi, gj, gk));
 #pragma unroll
-  for (int q = 0; q < 5; q++) Fc[q] = Fw[q] * (1.0 - sigma) + Fcen[q] * sigma;
+  for (int q = 0; q < 5; q++) Fc[q] = Fw[q] * (R(1.0) - sigma) + Fcen[q] * sigma;
+  if (MIX) Fc[4] += href * (Ufw * (R(1.0) - sigma) + Ufc * sigma);
 }
 
 // -------------------------------------------------------- viscous face ----
 __device__ __forceinline__ bool blocked(double v) { return v > SOLID && v < INNERBLANK; }
 
-template <bool LES, int BX, int BY>
-__device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, const Ring<BX, BY> &R, int d, NRef a,
-                                          int gi, int gj, int gk, double Fv[5], double A[3]) {
+template <typename R, bool MIX, bool LES, int BX, int BY>
+__device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, int d, NRef a,
+                                          int gi, int gj, int gk, R Fv[5], R A[3]) {
   const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d), g1 = g0 + sd;
   const int pos = d == 0 ? gi : (d == 1 ? gj : gk);
   const int m = d == 0 ? c.mx : (d == 1 ? c.my : c.mz);
   const NRef b = nshift(a, d, 1);
   // D[f][e]: derivative of (u, v, w, T) along computational direction e
-  double D[4][3];
+  R D[4][3];
 #pragma unroll
   for (int e = 0; e < 3; e++) {
     if (e == d) {
 #pragma unroll
-      for (int f = 0; f < 4; f++) D[f][e] = R.get(F_U + f, b) - R.get(F_U + f, a);
+      for (int f = 0; f < 4; f++) D[f][e] = Rg.get(F_U + f, b) - Rg.get(F_U + f, a);
       continue;
     }
     const long long te = gstride(c, e);
@@ -303,59 +351,59 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
       const int fi = F_U + f;
       if (plus_blocked) {
         if (f == 3 && d == 0 && e == 2)  // quirk: dpdz typo rhs.c:1544-1545
-          D[f][e] = (R.get(fi, b) + R.get(fi, a) - R.get(fi, bm) - R.get(fi, a)) * 0.5;
+          D[f][e] = (Rg.get(fi, b) + Rg.get(fi, a) - Rg.get(fi, bm) - Rg.get(fi, a)) * R(0.5);
         else
-          D[f][e] = (R.get(fi, b) + R.get(fi, a) - R.get(fi, bm) - R.get(fi, am)) * 0.5;
+          D[f][e] = (Rg.get(fi, b) + Rg.get(fi, a) - Rg.get(fi, bm) - Rg.get(fi, am)) * R(0.5);
       } else if (minus_blocked) {
-        D[f][e] = (R.get(fi, bp) + R.get(fi, ap) - R.get(fi, b) - R.get(fi, a)) * 0.5;
+        D[f][e] = (Rg.get(fi, bp) + Rg.get(fi, ap) - Rg.get(fi, b) - Rg.get(fi, a)) * R(0.5);
       } else {
-        D[f][e] = (R.get(fi, bp) + R.get(fi, ap) - R.get(fi, bm) - R.get(fi, am)) * 0.25;
+        D[f][e] = (Rg.get(fi, bp) + Rg.get(fi, ap) - Rg.get(fi, bm) - Rg.get(fi, am)) * R(0.25);
       }
     }
   }
-  const double dudc = D[0][0], dude = D[0][1], dudz = D[0][2];
-  const double dvdc = D[1][0], dvde = D[1][1], dvdz = D[1][2];
-  const double dwdc = D[2][0], dwde = D[2][1], dwdz = D[2][2];
-  const double dpdc = D[3][0], dpde = D[3][1], dpdz = D[3][2];
+  const R dudc = D[0][0], dude = D[0][1], dudz = D[0][2];
+  const R dvdc = D[1][0], dvde = D[1][1], dvdz = D[1][2];
+  const R dwdc = D[2][0], dwde = D[2][1], dwdz = D[2][2];
+  const R dpdc = D[3][0], dpde = D[3][1], dpdz = D[3][2];
 
-  double mh[3][3];
+  R mh[3][3];
 #pragma unroll
   for (int e = 0; e < 3; e++)
 #pragma unroll
-    for (int q = 0; q < 3; q++) mh[e][q] = 0.5 * (ldg(F.met[e][q] + g0) + ldg(F.met[e][q] + g1));
-  const double md0 = d == 0 ? mh[0][0] : (d == 1 ? mh[1][0] : mh[2][0]);
-  const double md1 = d == 0 ? mh[0][1] : (d == 1 ? mh[1][1] : mh[2][1]);
-  const double md2 = d == 0 ? mh[0][2] : (d == 1 ? mh[1][2] : mh[2][2]);
-  const double csi0 = mh[0][0], csi1 = mh[0][1], csi2 = mh[0][2];
-  const double eta0 = mh[1][0], eta1 = mh[1][1], eta2 = mh[1][2];
-  const double zet0 = mh[2][0], zet1 = mh[2][1], zet2 = mh[2][2];
-  const double g11 = csi0 * md0 + csi1 * md1 + csi2 * md2;
-  const double g21 = eta0 * md0 + eta1 * md1 + eta2 * md2;
-  const double g31 = zet0 * md0 + zet1 * md1 + zet2 * md2;
+    for (int q = 0; q < 3; q++) mh[e][q] = R(0.5) * (ldr(met_ptr_e<R>(F, e, q) + g0) + ldr(met_ptr_e<R>(F, e, q) + g1));
+  const R md0 = d == 0 ? mh[0][0] : (d == 1 ? mh[1][0] : mh[2][0]);
+  const R md1 = d == 0 ? mh[0][1] : (d == 1 ? mh[1][1] : mh[2][1]);
+  const R md2 = d == 0 ? mh[0][2] : (d == 1 ? mh[1][2] : mh[2][2]);
+  const R csi0 = mh[0][0], csi1 = mh[0][1], csi2 = mh[0][2];
+  const R eta0 = mh[1][0], eta1 = mh[1][1], eta2 = mh[1][2];
+  const R zet0 = mh[2][0], zet1 = mh[2][1], zet2 = mh[2][2];
+  const R g11 = csi0 * md0 + csi1 * md1 + csi2 * md2;
+  const R g21 = eta0 * md0 + eta1 * md1 + eta2 * md2;
+  const R g31 = zet0 * md0 + zet1 * md1 + zet2 * md2;
 
-  const double r11 = dudc * csi0 + dude * eta0 + dudz * zet0;
-  const double r21 = dvdc * csi0 + dvde * eta0 + dvdz * zet0;
-  const double r31 = dwdc * csi0 + dwde * eta0 + dwdz * zet0;
-  const double r12 = dudc * csi1 + dude * eta1 + dudz * zet1;
-  const double r22 = dvdc * csi1 + dvde * eta1 + dvdz * zet1;
-  const double r32 = dwdc * csi1 + dwde * eta1 + dwdz * zet1;
-  const double r13 = dudc * csi2 + dude * eta2 + dudz * zet2;
-  const double r23 = dvdc * csi2 + dvde * eta2 + dvdz * zet2;
-  const double r33 = dwdc * csi2 + dwde * eta2 + dwdz * zet2;
+  const R r11 = dudc * csi0 + dude * eta0 + dudz * zet0;
+  const R r21 = dvdc * csi0 + dvde * eta0 + dvdz * zet0;
+  const R r31 = dwdc * csi0 + dwde * eta0 + dwdz * zet0;
+  const R r12 = dudc * csi1 + dude * eta1 + dudz * zet1;
+  const R r22 = dvdc * csi1 + dvde * eta1 + dvdz * zet1;
+  const R r32 = dwdc * csi1 + dwde * eta1 + dwdz * zet1;
+  const R r13 = dudc * csi2 + dude * eta2 + dudz * zet2;
+  const R r23 = dvdc * csi2 + dvde * eta2 + dvdz * zet2;
+  const R r33 = dwdc * csi2 + dwde * eta2 + dwdz * zet2;
 
-  const double ajc = 0.5 * (ldg(F.aj + g0) + ldg(F.aj + g1));
-  double nu = c.inv_ren;  // 1./ren (evaluated once on the host, same value)
+  const R ajc = R(0.5) * (R(ldg(F.aj + g0)) + R(ldg(F.aj + g1)));
+  R nu = R(c.inv_ren);  // 1./ren (evaluated once on the host, same value)
   if (LES) {
     // quirk: eta/zeta faces average rho over i and i+1 (rhs.c:1835, 2034)
-    const double rhs_rho = (d == 0) ? R.get(F_RHO, b) : R.get(F_RHO, nshift(a, 0, 1));
-    nu = c.inv_ren_half * (R.get(F_RHO, a) + rhs_rho);  // (1./ren*0.5)*(...)
+    const R rhs_rho = (d == 0) ? Rg.get(F_RHO, b) : Rg.get(F_RHO, nshift(a, 0, 1));
+    nu = R(c.inv_ren_half) * (Rg.get(F_RHO, a) + rhs_rho);  // (1./ren*0.5)*(...)
   }
-  const double div = 2. / 3. * (dudc * csi0 + dude * eta0 + dudz * zet0 + dvdc * csi1 + dvde * eta1 + dvdz * zet1 +
-                                dwdc * csi2 + dwde * eta2 + dwdz * zet2);
-  const double tu = g11 * dudc + g21 * dude + g31 * dudz + r11 * md0 + r21 * md1 + r31 * md2;
-  const double tv = g11 * dvdc + g21 * dvde + g31 * dvdz + r12 * md0 + r22 * md1 + r32 * md2;
-  const double tw = g11 * dwdc + g21 * dwde + g31 * dwdz + r13 * md0 + r23 * md1 + r33 * md2;
-  Fv[0] = 0.;
+  const R div = R(2.) / R(3.) * (dudc * csi0 + dude * eta0 + dudz * zet0 + dvdc * csi1 + dvde * eta1 + dvdz * zet1 +
+                                 dwdc * csi2 + dwde * eta2 + dwdz * zet2);
+  const R tu = g11 * dudc + g21 * dude + g31 * dudz + r11 * md0 + r21 * md1 + r31 * md2;
+  const R tv = g11 * dvdc + g21 * dvde + g31 * dvdz + r12 * md0 + r22 * md1 + r32 * md2;
+  const R tw = g11 * dwdc + g21 * dwde + g31 * dwdz + r13 * md0 + r23 * md1 + r33 * md2;
+  Fv[0] = R(0.);
   Fv[1] = tu * ajc * (nu);
   Fv[2] = tv * ajc * (nu);
   Fv[3] = tw * ajc * (nu);
@@ -363,38 +411,38 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   Fv[2] -= div * md1 * ajc * nu;
   Fv[3] -= div * md2 * ajc * nu;
 
-  double uh[3];
+  R uh[3];
   if (pos == 0 && bc_lo(c, d) == 1) {
 #pragma unroll
-    for (int q = 0; q < 3; q++) uh[q] = R.get(F_U + q, a);
+    for (int q = 0; q < 3; q++) uh[q] = Rg.get(F_U + q, a);
   } else if (pos == m - 2 && bc_hi(c, d) == 1) {
 #pragma unroll
-    for (int q = 0; q < 3; q++) uh[q] = R.get(F_U + q, b);
+    for (int q = 0; q < 3; q++) uh[q] = Rg.get(F_U + q, b);
   } else {
 #pragma unroll
-    for (int q = 0; q < 3; q++) uh[q] = 0.5 * (R.get(F_U + q, b) + R.get(F_U + q, a));
+    for (int q = 0; q < 3; q++) uh[q] = R(0.5) * (Rg.get(F_U + q, b) + Rg.get(F_U + q, a));
   }
-  const double gm = c.gamma;
+  const R gm = R(c.gamma);
   Fv[4] = (Fv[1] * uh[0] + Fv[2] * uh[1] + Fv[3] * uh[2]) +
-          (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (gm * nu / c.pr / c.gm1);
+          (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (gm * nu / R(c.pr) / R(c.gm1));
 
-  A[0] = A[1] = A[2] = 0.;
+  A[0] = A[1] = A[2] = R(0.);
   if (LES) {  // rhs.c:1677-1710
-    const double sa = sigma_at(c, d, gi, gj, gk);
+    const R sa = R(sigma_at(c, d, gi, gj, gk));
     const int bi = gi + (d == 0), bj = gj + (d == 1), bk = gk + (d == 2);
-    const double sb = sigma_at(c, d, bi, bj, bk);
-    double nut = 0.5 * (ldg(F.nut + g0) * sa + ldg(F.nut + g1) * sb);
-    const double rho_c = 0.5 * (R.get(F_RHO, a) + R.get(F_RHO, b));
-    const double sigma_c = 0.5 * (sa + sb);
-    if ((bc_lo(c, d) == 1 && pos == 0) || (bc_hi(c, d) == 1 && pos == m - 2)) nut = 0;
-    const double tx = (tu - div * md0) * ajc * (nut * rho_c);
-    const double ty = (tv - div * md1) * ajc * (nut * rho_c);
-    const double tz = (tw - div * md2) * ajc * (nut * rho_c);
-    const double S2 = .5 * ((r11 - div) * (r11 - div) + r12 * r12 + r13 * r13 + r21 * r21 + (r22 - div) * (r22 - div) +
-                            r23 * r23 + r31 * r31 + r32 * r32 + (r33 - div) * (r33 - div));
+    const R sb = R(sigma_at(c, d, bi, bj, bk));
+    R nut = R(0.5) * (R(ldg(F.nut + g0)) * sa + R(ldg(F.nut + g1)) * sb);
+    const R rho_c = R(0.5) * (Rg.get(F_RHO, a) + Rg.get(F_RHO, b));
+    const R sigma_c = R(0.5) * (sa + sb);
+    if ((bc_lo(c, d) == 1 && pos == 0) || (bc_hi(c, d) == 1 && pos == m - 2)) nut = R(0);
+    const R tx = (tu - div * md0) * ajc * (nut * rho_c);
+    const R ty = (tv - div * md1) * ajc * (nut * rho_c);
+    const R tz = (tw - div * md2) * ajc * (nut * rho_c);
+    const R S2 = R(.5) * ((r11 - div) * (r11 - div) + r12 * r12 + r13 * r13 + r21 * r21 + (r22 - div) * (r22 - div) +
+                          r23 * r23 + r31 * r31 + r32 * r32 + (r33 - div) * (r33 - div));
     // pow(pow(1/aj, 1/3), 2) of the left node, precomputed once per node
-    const double pf = ldg(F.delta2 + g0);
-    const double sgs = -S2 * pf * c.ci * 2.0 / 3.0;
+    const R pf = MIX ? R(ldr(F.delta2_32 + g0)) : R(ldg(F.delta2 + g0));
+    const R sgs = -S2 * pf * R(c.ci) * R(2.0) / R(3.0);
     A[0] = tx + sgs * md0 * rho_c * sigma_c;
     A[1] = ty + sgs * md1 * rho_c * sigma_c;
     A[2] = tz + sgs * md2 * rho_c * sigma_c;
@@ -415,10 +463,17 @@ using STile = TileShape<SBX, SBY>;
 constexpr int S_NXF = STile::NXF;  // 231
 constexpr int S_NYF = STile::NYF;  // 256
 constexpr int S_NZF = SBX * SBY;   // 224
-constexpr size_t STAGE_SMEM_BYTES =
-    sizeof(double) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF) + (size_t)5 * STile::PN);
+template <typename R, bool MIX>
+struct StageSmem {
+  static constexpr int NG = FaceWidth<MIX>::NG;
+  static constexpr size_t bytes = sizeof(R) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF)) +
+                                  sizeof(double) * (size_t)5 * STile::PN;
+};
+constexpr size_t STAGE_SMEM_BYTES = StageSmem<double, false>::bytes;
+constexpr size_t STAGE_SMEM_BYTES_MIXED = StageSmem<float, true>::bytes;
 static_assert(S_NXF <= 256 && S_NYF <= 256 && S_NZF <= 224, "face schedule segments");
 static_assert(STAGE_SMEM_BYTES <= 232448, "shared memory budget of one block");
+static_assert(2 * (STAGE_SMEM_BYTES_MIXED + 1024) <= 233472, "mixed form: two blocks per SM");
 
 __device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc, bool valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
@@ -428,17 +483,19 @@ __device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc, bool val
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <bool LES, bool VISC, bool RHS_MODE>
-__global__ void __launch_bounds__(SNT, 1)
+template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE>
+__global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
-  extern __shared__ double smem[];
-  Ring<BX, BY> R;
-  R.pl = smem;
-  double *gxb = smem + (size_t)4 * NF * PN;  // [NG][S_NXF]
-  double *gyb = gxb + (size_t)NG * S_NXF;    // [NG][S_NYF]
-  double *gzb = gyb + (size_t)NG * S_NYF;    // [NG][S_NZF]
-  double *stg = gzb + (size_t)NG * S_NZF;    // [5][PN] raw Q of the next plane
+  constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
+  extern __shared__ double smem_d[];
+  double *stg = smem_d;  // [5][PN] raw FP64 Q of the next plane
+  R *smem = reinterpret_cast<R *>(smem_d + (size_t)5 * PN);
+  Ring<R, BX, BY> Rg;
+  Rg.pl = smem;
+  R *gxb = smem + (size_t)4 * NF * PN;  // [NG][S_NXF]
+  R *gyb = gxb + (size_t)NG * S_NXF;    // [NG][S_NYF]
+  R *gzb = gyb + (size_t)NG * S_NYF;    // [NG][S_NZF]
 
   const int tid = threadIdx.x;
   const int i0 = 1 + blockIdx.x * BX, j0 = 1 + blockIdx.y * BY;
@@ -461,7 +518,8 @@ __global__ void __launch_bounds__(SNT, 1)
     }
     cp_async_commit();
   };
-  // staging -> ring slot s with the derived p, u, v, w, T (EqOfState rhs.c:4850, CalcUCat rhs.c:1349)
+  // staging -> ring slot s with the derived p, u, v, w, T (EqOfState rhs.c:4850,
+  // CalcUCat rhs.c:1349), all in FP64; the mixed form stores shifted FP32 values
   auto derive = [&](int s) {
     for (int idx = tid; idx < PN; idx += NT) {
       double v[NF];
@@ -474,13 +532,18 @@ __global__ void __launch_bounds__(SNT, 1)
         v[F_V] = v[2] / r;
         v[F_W] = v[3] / r;
         v[F_T] = v[F_P] / r;
+        if (MIX) {
+          v[F_RE] -= c.e_ref;
+          v[F_P] -= c.p_ref;
+          v[F_T] -= c.t_ref;
+        }
       } else {
 #pragma unroll
         for (int q = 5; q < NF; q++) v[q] = 0.0;
       }
-      double *base = R.pl + (size_t)s * NF * PN + idx;
+      R *base = Rg.pl + (size_t)s * NF * PN + idx;
 #pragma unroll
-      for (int q = 0; q < NF; q++) base[(size_t)q * PN] = v[q];
+      for (int q = 0; q < NF; q++) base[(size_t)q * PN] = R(v[q]);
     }
   };
   auto load_plane_sync = [&](int kk, int s) {
@@ -498,7 +561,7 @@ __global__ void __launch_bounds__(SNT, 1)
       const int v = r * NT + tid;
       int d, u, fi, fj;
       NRef a;
-      double *dst;
+      R *dst;
       int nslot;
       if (v < 256) {
         d = 0; u = v;
@@ -521,18 +584,28 @@ __global__ void __launch_bounds__(SNT, 1)
         a = NRef{0, fy + 2, fx + 2};
         dst = gzb; nslot = S_NZF;
       }
-      double G[NG];
+      R G[NG];
       if (fi <= c.mx - 2 && fj <= c.my - 2) {
-        conv_face<LES, BX, BY>(c, F, R, d, a, fi, fj, k, G);
+        R Fc[5], Fv[5], A[3];
+        conv_face<R, MIX, LES, BX, BY>(c, F, Rg, d, a, fi, fj, k, Fc);
         if (VISC) {
-          visc_face<LES, BX, BY>(c, F, R, d, a, fi, fj, k, G + 5, G + 10);
+          visc_face<R, MIX, LES, BX, BY>(c, F, Rg, d, a, fi, fj, k, Fv, A);
         } else {
 #pragma unroll
-          for (int q = 5; q < NG; q++) G[q] = 0.;
+          for (int q = 0; q < 5; q++) Fv[q] = R(0.);
+          A[0] = A[1] = A[2] = R(0.);
         }
+        if (MIX) {
+#pragma unroll
+          for (int q = 0; q < 5; q++) G[q] = Fv[q] - Fc[q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < 5; q++) { G[q] = Fc[q]; G[VOFF + q] = Fv[q]; }
+        }
+        G[AOFF] = A[0]; G[AOFF + 1] = A[1]; G[AOFF + 2] = A[2];
       } else {
 #pragma unroll
-        for (int q = 0; q < NG; q++) G[q] = 0.;
+        for (int q = 0; q < NG; q++) G[q] = R(0.);
       }
 #pragma unroll
       for (int q = 0; q < NG; q++) dst[(size_t)q * nslot + u] = G[q];
@@ -540,28 +613,28 @@ __global__ void __launch_bounds__(SNT, 1)
   };
 
   // prologue: planes kb-2 .. kb+1 in slots 0..3, k-face kb-1/2, then kb+2
-  R.slot[0] = 0; R.slot[1] = 1; R.slot[2] = 2; R.slot[3] = 3;
+  Rg.slot[0] = 0; Rg.slot[1] = 1; Rg.slot[2] = 2; Rg.slot[3] = 3;
   load_plane_sync(kb - 2, 0);
   load_plane_sync(kb - 1, 1);
   load_plane_sync(kb, 2);
   load_plane_sync(kb + 1, 3);
   faces(kb - 1, true);  // r = 0 -> plane kb-1
   __syncthreads();
-  double Gzp[NG];  // k-face k-1/2 of the node this thread updates
+  R Gzp[NG];  // k-face k-1/2 of the node this thread updates
 #pragma unroll
-  for (int q = 0; q < NG; q++) Gzp[q] = uact ? gzb[(size_t)q * S_NZF + tid] : 0.;
+  for (int q = 0; q < NG; q++) Gzp[q] = uact ? gzb[(size_t)q * S_NZF + tid] : R(0.);
   __syncthreads();
   load_plane_sync(kb + 2, 0);
   int base = 1;  // slot of plane k-1
 
   for (int k = kb; k < ke; k++) {
-    R.slot[0] = base & 3; R.slot[1] = (base + 1) & 3; R.slot[2] = (base + 2) & 3; R.slot[3] = (base + 3) & 3;
+    Rg.slot[0] = base & 3; Rg.slot[1] = (base + 1) & 3; Rg.slot[2] = (base + 2) & 3; Rg.slot[3] = (base + 3) & 3;
     const bool more = k + 1 < ke;
     if (more) issue_stage(k + 3);  // overlaps the face computation
     faces(k, false);
     // the only plane k-1 value the update needs, read before that slot is refilled
     const NRef n{0, uty + 2, utx + 2};
-    const double rho_km1 = (LES && VISC && uact) ? R.get(F_RHO, nshift(n, 2, -1)) : 0.;
+    const R rho_km1 = (LES && VISC && uact) ? Rg.get(F_RHO, nshift(n, 2, -1)) : R(0.);
     cp_async_wait_all();
     __syncthreads();
 
@@ -572,46 +645,62 @@ __global__ void __launch_bounds__(SNT, 1)
       const int fyu = (uty + 1) * BX + utx, fyd = uty * BX + utx;  // j+1/2, j-1/2
       const int fz = tid;                                          // k+1/2 (k-1/2 in Gzp)
       // flux differences in the reference's order (rhs.c:3159-3205, 2123-2151):
-      // ((((F_i - F_i-1) + F_j) - F_j-1) + F_k) - F_k-1, conv and visc apart
+      // ((((F_i - F_i-1) + F_j) - F_j-1) + F_k) - F_k-1
       auto fdiff = [&](int q) {
         return gxb[(size_t)q * S_NXF + fxr] - gxb[(size_t)q * S_NXF + fxl] + gyb[(size_t)q * S_NYF + fyu] -
                gyb[(size_t)q * S_NYF + fyd] + gzb[(size_t)q * S_NZF + fz] - Gzp[q];
       };
-      double conv[5], visc[5];
+      // LES energy term (rhs.c:2153-2197): u . sum of rho_face * stress differences
+      auto les_energy = [&]() -> R {
+        const R r0 = Rg.get(F_RHO, n);
+        const R rL = (r0 + Rg.get(F_RHO, nshift(n, 0, -1))) * R(0.5), rR = (Rg.get(F_RHO, nshift(n, 0, 1)) + r0) * R(0.5);
+        const R rD = (r0 + Rg.get(F_RHO, nshift(n, 1, -1))) * R(0.5), rU = (Rg.get(F_RHO, nshift(n, 1, 1)) + r0) * R(0.5);
+        const R rB = (r0 + rho_km1) * R(0.5), rF = (Rg.get(F_RHO, nshift(n, 2, 1)) + r0) * R(0.5);
+        R e = R(0.);
 #pragma unroll
-      for (int q = 0; q < 5; q++) conv[q] = (nv < BLANK) ? fdiff(q) : 0.;
-      visc[0] = 0.;
-#pragma unroll
-      for (int q = 1; q < 5; q++) visc[q] = VISC ? fdiff(5 + q) : 0.;
-      if (LES) {
-        if (nv < BLANK && c.ratio != 0.0) {  // channel forcing terms (rhs.c:4226-4235); exact no-op at ratio 0
-          const double ajn = ldg(F.aj + g);
-          conv[3] = conv[3] - c.ratio / ajn * R.get(F_RHO, n) / c.dt;
-          conv[4] = conv[4] - c.ratio / ajn * R.get(F_RW, n) / c.dt;
+        for (int q = 0; q < 3; q++) {
+          const int a = AOFF + q;
+          const R t = rR * gxb[(size_t)a * S_NXF + fxr] - rL * gxb[(size_t)a * S_NXF + fxl] +
+                      rU * gyb[(size_t)a * S_NYF + fyu] - rD * gyb[(size_t)a * S_NYF + fyd] +
+                      rF * gzb[(size_t)a * S_NZF + fz] - rB * Gzp[a];
+          e = (q == 0) ? Rg.get(F_U + q, n) * t : e + Rg.get(F_U + q, n) * t;
         }
-        if (VISC && ugj > 2 && ugj < c.my - 2 && nv < 0.5) {  // rhs.c:2153-2197
-          const double r0 = R.get(F_RHO, n);
-          const double rL = (r0 + R.get(F_RHO, nshift(n, 0, -1))) * 0.5, rR = (R.get(F_RHO, nshift(n, 0, 1)) + r0) * 0.5;
-          const double rD = (r0 + R.get(F_RHO, nshift(n, 1, -1))) * 0.5, rU = (R.get(F_RHO, nshift(n, 1, 1)) + r0) * 0.5;
-          const double rB = (r0 + rho_km1) * 0.5, rF = (R.get(F_RHO, nshift(n, 2, 1)) + r0) * 0.5;
-          double e = 0.;
-#pragma unroll
-          for (int q = 0; q < 3; q++) {
-            const int a = 10 + q;
-            const double t = rR * gxb[(size_t)a * S_NXF + fxr] - rL * gxb[(size_t)a * S_NXF + fxl] +
-                             rU * gyb[(size_t)a * S_NYF + fyu] - rD * gyb[(size_t)a * S_NYF + fyd] +
-                             rF * gzb[(size_t)a * S_NZF + fz] - rB * Gzp[a];
-            e = (q == 0) ? R.get(F_U + q, n) * t : e + R.get(F_U + q, n) * t;
-          }
-          visc[4] += e;
-        }
-      }
-      const double aj = ldg(F.aj + g);
+        return e;
+      };
+      const bool les_e = LES && VISC && ugj > 2 && ugj < c.my - 2 && nv < 0.5;
       double rhs[5];
+      if (MIX) {
+        // G = visc - conv' (FP32); the p_ref * h part of conv is p_ref * gcl (FP64)
+        R d4[5];
 #pragma unroll
-      for (int q = 0; q < 5; q++) {
-        rhs[q] = visc[q] - conv[q];                  // VecWAXPY(Rhs, -1, Conv, Visc)
-        rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;     // MultAj
+        for (int q = 0; q < 5; q++) d4[q] = fdiff(q);
+        if (les_e) d4[4] += les_energy();
+        const double aj = ldg(F.aj + g);
+        rhs[0] = (double)d4[0];
+#pragma unroll
+        for (int q = 1; q < 4; q++) rhs[q] = (double)d4[q] - c.p_ref * ldg(F.gcl[q - 1] + g);
+        rhs[4] = (double)d4[4];
+#pragma unroll
+        for (int q = 0; q < 5; q++) rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;
+      } else {
+        R conv[5], visc[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) conv[q] = (nv < BLANK) ? fdiff(q) : R(0.);
+        visc[0] = R(0.);
+#pragma unroll
+        for (int q = 1; q < 5; q++) visc[q] = VISC ? fdiff(VOFF + q) : R(0.);
+        if (LES && nv < BLANK && c.ratio != 0.0) {  // channel forcing (rhs.c:4226-4235); exact no-op at ratio 0
+          const double ajn = ldg(F.aj + g);
+          conv[3] = conv[3] - c.ratio / ajn * Rg.get(F_RHO, n) / c.dt;
+          conv[4] = conv[4] - c.ratio / ajn * Rg.get(F_RW, n) / c.dt;
+        }
+        if (les_e) visc[4] += les_energy();
+        const double aj = ldg(F.aj + g);
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+          rhs[q] = visc[q] - conv[q];                 // VecWAXPY(Rhs, -1, Conv, Visc)
+          rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;    // MultAj
+        }
       }
       if (RHS_MODE) {
 #pragma unroll
@@ -621,8 +710,9 @@ __global__ void __launch_bounds__(SNT, 1)
 #pragma unroll
         for (int q = 0; q < 5; q++) {
           const double qo = ldg(F.qold[q] + g);
-          // solvers.c:257 (VecWAXPY) and 269 (VecAXPBYPCZ)
-          out[q] = (istage == 0) ? qo + adt * rhs[q] : beta * qo + adt * rhs[q] + alfa * R.get(F_RHO + q, n);
+          const double qi = MIX ? ldg(F.q[q] + g) : (double)Rg.get(F_RHO + q, n);
+          // solvers.c:257 (VecWAXPY) and 269 (VecAXPBYPCZ), FP64 in every form
+          out[q] = (istage == 0) ? qo + adt * rhs[q] : beta * qo + adt * rhs[q] + alfa * qi;
           F.qout[q][g] = out[q];
         }
         const double p = (c.gamma - 1) * (out[4] - 0.5 * (out[1] * out[1] + out[2] * out[2] + out[3] * out[3]) / out[0]);
