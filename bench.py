@@ -267,6 +267,80 @@ def _accuracy(fp64, mixed, q0):
             "ke": [h[0] for h in hist["fp64"]], "checkpoints_every": ACC_STEPS // 4}
 
 
+def _batch_timed(bt, steps, warmup, per_block, local):
+    import torch
+    stream = torch.cuda.ExternalStream(bt.stream, device=f"cuda:{local}")
+    bt.RungeKutta(max(warmup, 3), per_block=per_block)  # captures the step graphs of this mode
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    bt.RungeKutta(steps, per_block=per_block, sync=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    bt.sync()
+    return e0.elapsed_time(e1)
+
+
+def run_batched(args, local):
+    """Uneven multi-block set (24 blocks, sizes drawn from 32..160 x 32..128 x
+    32..96 unique points, metric distortion 0.03, von Karman turbulence k_peak 4,
+    Mt 0.3, 2-node overlap halos from a seeded donor permutation): the
+    persistent work-queue launch against one launch per block, both forms,
+    and the mixed-vs-FP64 error after ACC_STEPS steps."""
+    from chimera_comp_les_b200 import batch as B
+    from chimera_comp_les_b200 import diagnostics as D
+    from chimera_comp_les_b200 import workloads as W
+    mb = W.multiblock_set(seed=2024, nblocks=24)
+    # half upwind (sigma 0.5): the donor halos put jumps at every block face, on
+    # which the purely central blend (sigma 1) of the headline loses positivity
+    opts = dict(CFG, s_x=0.5, s_y=0.5, s_z=0.5)
+    opts["dt"] = mb["dt"]
+    maps = B.halo_maps_donor(mb["dims"], mb["perm"])
+    out = {"workload": "24 uneven curvilinear blocks (unique points per direction drawn from 32..160 x 32..128 x "
+                       "32..96, seed 2024), random smooth metric distortion 0.03, decaying isotropic turbulence "
+                       "(von Karman, k_peak 4, Mt 0.3), 2-node overlap halos gathered from a seeded donor "
+                       "permutation; LES scheme and RK3 as the headline but sigma 0.5 (half upwind), dt from CFL 0.4",
+           "blocks": len(mb["dims"]), "dt": mb["dt"]}
+    final, hist = {}, {}
+    for prec in ("mixed", "fp64"):
+        bt = B.Batch(mb["dims"], precision=prec, device=local, **opts)
+        for k in range(len(mb["dims"])):
+            bt.FormMetrics(k, mb["coords"][k])
+            bt.SetInitialCondition(k, mb["q"][k])
+        bt.set_halo_maps(maps)
+        kc, tune_ms = bt.autotune()
+        interior, stages = bt.interior_nodes, opts["fluxorder"]
+        r = {"kchunk": kc, "autotune_stage_ms": tune_ms, "work_items": bt.work_items}
+        for name, pb in (("persistent", False), ("per_block", True)):
+            ms = _batch_timed(bt, args.steps, args.warmup, pb, local)
+            r[name] = {"value": interior * stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps}
+        r["persistent_vs_per_block"] = r["persistent"]["value"] / r["per_block"]["value"]
+        out[prec] = r
+        out["interior_nodes"] = interior
+        # accuracy run from the initial state
+        for k in range(len(mb["dims"])):
+            bt.SetInitialCondition(k, mb["q"][k])
+        mets = [bt.metrics(k) for k in range(len(mb["dims"]))]
+        ke = []
+        for c in range(5):
+            if c:
+                bt.RungeKutta(ACC_STEPS // 4)
+            qs = [bt.Q(k) for k in range(len(mb["dims"]))]
+            ke.append(sum(D.kinetic_energy(q, m[3]) for q, m in zip(qs, mets)))
+        en = sum(D.enstrophy(q, *m) for q, m in zip(qs, mets))
+        hist[prec] = (ke, en)
+        final[prec] = np.concatenate([q[1:-1, 1:-1, 1:-1].reshape(-1, 5) for q in qs])
+        bt.close()
+    l2, linf = D.field_errors(final["mixed"], final["fp64"])
+    out["speedup_mixed_vs_fp64_persistent"] = out["mixed"]["persistent"]["value"] / out["fp64"]["persistent"]["value"]
+    out["mixed_vs_fp64_error"] = {
+        "steps": ACC_STEPS, "rel_l2": l2, "rel_linf": linf,
+        "ke_history_max_rel_dev": max(abs(a - b) / abs(b) for a, b in zip(hist["mixed"][0], hist["fp64"][0])),
+        "enstrophy_final_rel_dev": abs(hist["mixed"][1] - hist["fp64"][1]) / abs(hist["fp64"][1]),
+    }
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import ctypes
     import torch
@@ -325,6 +399,8 @@ def run_ours(args, ws, rank, local):
     if not np.isfinite(q_out).all():
         raise RuntimeError("non-finite state after end-to-end steps")
 
+    batched = run_batched(args, local) if (ws == 1 and not args.no_batched) else None
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import cpu_baseline as cb
@@ -355,6 +431,7 @@ def run_ours(args, ws, rank, local):
             other: {k: v for k, v in forms[other].items() if k != "clocks"},
             "speedup_mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"],
             "mixed_vs_fp64_error": acc,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     for b in blocks.values():
@@ -370,6 +447,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
                     help="form reported as the headline value (both are measured)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the multi-block batched measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

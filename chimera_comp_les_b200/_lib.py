@@ -64,6 +64,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = C.c_int
+    lib.cb_cfl_dt.argtypes = [P, C.c_double, D, D]
+    lib.cb_cfl_dt.restype = C.c_int
     lib.cb_rhs_noalloc.argtypes = [C.POINTER(CbConfig), P, P, P, P, P, P]
     lib.cb_rhs_noalloc.restype = C.c_int
     lib.cb_stream.argtypes = [P]
@@ -76,6 +78,31 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.cb_launches_per_step.restype = C.c_int
     lib.cb_last_error.argtypes = [P]
     lib.cb_last_error.restype = C.c_char_p
+    # batched multi-block form
+    I = C.c_int
+    IP = C.POINTER(C.c_int)
+    lib.cb_batch_create.argtypes = [C.POINTER(CbConfig), I, IP, C.POINTER(P)]
+    lib.cb_batch_create.restype = I
+    lib.cb_batch_destroy.argtypes = [P]
+    lib.cb_batch_destroy.restype = None
+    lib.cb_batch_last_error.argtypes = [P]
+    lib.cb_batch_last_error.restype = C.c_char_p
+    lib.cb_batch_interior_nodes.argtypes = [P]
+    lib.cb_batch_interior_nodes.restype = C.c_longlong
+    lib.cb_batch_stream.argtypes = [P]
+    lib.cb_batch_stream.restype = P
+    lib.cb_batch_work_items.argtypes = [P]
+    lib.cb_batch_work_items.restype = I
+    for name, args in [
+        ("cb_batch_set_grid", [P, I, D]), ("cb_batch_set_nvert", [P, I, D]),
+        ("cb_batch_upload_state", [P, I, D]), ("cb_batch_download_state", [P, I, D]),
+        ("cb_batch_get_metrics", [P, I, D, D, D, D]),
+        ("cb_batch_set_halo_map", [P, I, C.c_longlong, IP]), ("cb_batch_halo_periodic", [P]),
+        ("cb_batch_rk_step", [P, I, I]), ("cb_batch_sync", [P]), ("cb_batch_autotune", [P, IP, D]),
+    ]:
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = I
     _lib = lib
     return lib
 

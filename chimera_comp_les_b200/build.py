@@ -21,6 +21,7 @@ MIXED_FLAGS = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]
 SOURCES = [
     (os.path.join(PKG_DIR, "csrc", "cb_api.cu"), FP64_FLAGS),
     (os.path.join(PKG_DIR, "csrc", "cb_noalloc.cu"), FP64_FLAGS),
+    (os.path.join(PKG_DIR, "csrc", "cb_batch.cu"), FP64_FLAGS),
     (os.path.join(PKG_DIR, "csrc", "cb_mixed.cu"), MIXED_FLAGS),
 ]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

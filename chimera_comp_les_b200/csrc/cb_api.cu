@@ -582,6 +582,25 @@ int cb_rhs(cb_ctx *c, int istage, double *rhs) {
   return CB_OK;
 }
 
+int cb_cfl_dt(cb_ctx *c, double cfl, double *dt, double *lambda_max) {
+  if (!c || !dt || !(cfl > 0)) return CB_E_ARG;
+  if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set");
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(c->staging);  // staging is free between calls
+  CB_CUDA(c, cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->stream));
+  const long long work = (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2);
+  spectral_radius_kernel<<<grid_for(c, work), 256, 0, c->stream>>>(
+      c->dc, (const double *const *)(c->ptab + 5 * c->cur), (const double *const *)(c->ptab + PT_MET), c->aj, c->nvert, d);
+  CB_CUDA(c, cudaGetLastError());
+  unsigned long long bits = 0;
+  CB_CUDA(c, cudaMemcpyAsync(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  double lam;
+  std::memcpy(&lam, &bits, sizeof(lam));
+  if (lambda_max) *lambda_max = lam;
+  *dt = lam > 0 ? cfl / lam : 0.0;
+  return CB_OK;
+}
+
 int cb_calc_ucat(cb_ctx *c) {
   if (!c) return CB_E_ARG;
   if (!c->have_state) return fail(c, CB_E_STATE, "no state");

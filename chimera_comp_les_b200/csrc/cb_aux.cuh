@@ -208,3 +208,50 @@ static __global__ void eos_pack_kernel(const DevCfg c, const double *const *q, d
 }
 
 }  // namespace cb
+
+namespace cb {
+
+// ------------------------------------------------------------------- CFL --
+// Largest inviscid spectral radius over the interior nodes,
+//   lambda = aj * sum_d ( |m_d . u| + c |m_d| ),  c^2 = gamma p / rho,
+// with m_d the contravariant area vectors (csi, eta, zet carry 1/J), so that
+// dt = CFL / lambda_max.  The reference keeps dt fixed (-dt, init.c:94) and its
+// Spectral (rhs.c:4739-4814) is an unused incompressible estimate; this is the
+// compressible one the time-step controller needs.  Max per warp by shuffles,
+// per block through shared memory, one atomicMax per block on the bit pattern
+// of the (non-negative) double.
+static __global__ void spectral_radius_kernel(const DevCfg c, const double *const *q, const double *const *met,
+                                              const double *aj, const double *nvert, unsigned long long *out) {
+  const long long nx = c.mx - 2, ny = c.my - 2, nz = c.mz - 2, total = nx * ny * nz;
+  double lmax = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / (nx * ny));
+    const long long n = gidx(c, i, j, k);
+    if (ldg(nvert + n) >= 0.1) continue;  // solid and interface nodes carry no RHS (rhs.c:4610)
+    const double r = ldg(q[0] + n), u = ldg(q[1] + n) / r, v = ldg(q[2] + n) / r, w = ldg(q[3] + n) / r;
+    const double p = (c.gamma - 1) * (ldg(q[4] + n) - 0.5 * r * (u * u + v * v + w * w));
+    const double cs = sqrt(fabs(c.gamma * p / r));
+    double lam = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const double mx = ldg(met[3 * d] + n), my = ldg(met[3 * d + 1] + n), mz = ldg(met[3 * d + 2] + n);
+      lam += fabs(mx * u + my * v + mz * w) + cs * sqrt(mx * mx + my * my + mz * mz);
+    }
+    lam *= ldg(aj + n);
+    lmax = fmax(lmax, lam);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
+  __shared__ double wmax[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) wmax[warp] = lmax;
+  __syncthreads();
+  if (warp == 0) {
+    double m = lane < (int)(blockDim.x >> 5) ? wmax[lane] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));  // order-preserving for m >= 0
+  }
+}
+
+}  // namespace cb

@@ -1,0 +1,793 @@
+// Batched multi-block form: many curvilinear blocks of uneven sizes resident
+// on one GPU and advanced together.
+//
+// Layout: every field is ONE contiguous array over all blocks' padded node
+// boxes (block b at offset off[b]), so a node is addressed by a single global
+// offset valid in every field and every state buffer.  That lets one gather
+// table describe all inter-block halo copies:
+//   entry = (dst offset, src offset, source buffer)
+// where the source buffer is the stage output (a donor's freshly updated
+// interior) or the stage input (the reference's periodic FormBCS, which reads
+// the not-yet-refreshed lQ, rhs.c:1107-1227).
+//
+// Per RK stage: ONE persistent stage launch over a largest-first list of work
+// items (block, tile column, k-chunk) taken from a device counter, then one
+// gather launch.  The eddy viscosity runs once per step per block.  A whole
+// step is captured as a CUDA graph per buffer-rotation state.  The k-chunk of
+// the work items is chosen by timing candidates (cb_batch_autotune).  For
+// comparison the same step can run with one stage launch per block.
+//
+// The reference advances its blocks one after another without coupling
+// (solvers.c:246); the gather is new.  With the self-periodic map
+// (cb_batch_halo_periodic) every block reproduces the single-block path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/chimera_b200.h"
+#include "cb_aux.cuh"
+#include "cb_common.cuh"
+#include "cb_launch.h"
+#include "cb_stage.cuh"
+
+using namespace cb;
+
+namespace {
+
+// gather: dst[e] <- (from_in[e] ? qin : qout)[src[e]] for the 5 state fields
+__global__ void halo_gather_kernel(const long long *__restrict__ dst, const long long *__restrict__ src,
+                                   const unsigned char *__restrict__ from_in, long long n, DevFields F) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long d = dst[e], s = src[e];
+    const bool fin = from_in[e] != 0;
+#pragma unroll
+    for (int q = 0; q < 5; q++) F.qout[q][d] = fin ? F.q[q][s] : F.qout[q][s];
+  }
+}
+
+// single-field gather within one array: dst[e] <- f[src[e]] (plain periodic
+// wrap / DMGlobalToLocal across blocks: the eddy viscosity and the initial state)
+__global__ void plane_gather_kernel(const long long *__restrict__ dst, const long long *__restrict__ src, long long n,
+                                    double *f) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    f[dst[e]] = f[src[e]];
+}
+
+struct BlockHost {
+  int mx, my, mz;
+  DevCfg dc;
+  long long off;        // offset of the block's padded box in every field array
+  int tiles_x, tiles_y;
+  bool have_grid = false, have_state = false;
+};
+
+}  // namespace
+
+struct cb_batch {
+  cb_config cfg{};
+  int nb = 0;
+  int dev = 0, sms = 148;
+  cudaStream_t stream = nullptr;
+  std::vector<BlockHost> blk;
+  long long total = 0;  // padded nodes over all blocks
+  // fields (each `total` long): 3 x 5 state, 9 metrics, aj, nvert, nut, delta2
+  double *arena = nullptr;
+  double *qb[3][5] = {};
+  double *met[3][3] = {};
+  double *aj = nullptr, *nvert = nullptr, *nut = nullptr, *delta2 = nullptr;
+  void *arena_mixed = nullptr;
+  float *met32[3][3] = {};
+  float *delta2_32 = nullptr;
+  double *gcl[3] = {};
+  double *staging = nullptr;  // AoS host transfer buffer, sized for the largest block
+  double **ptab = nullptr;    // per-block pointer tables for the set-up kernels
+  float **ptab32 = nullptr;
+  // batched launch data
+  BatchBlock *d_tables = nullptr;  // [27][nb] indexed by (in, old, out) buffer triple
+  int2 *d_items = nullptr;
+  int nitems = 0;
+  unsigned *d_counter = nullptr;
+  unsigned *status = nullptr;
+  int kchunk = 16;
+  // stage halo map (FormBCS + wrap across blocks) and plain wrap map
+  long long nhalo = 0, nwrap = 0;
+  long long *d_hdst = nullptr, *d_hsrc = nullptr, *d_wdst = nullptr, *d_wsrc = nullptr;
+  unsigned char *d_hin = nullptr;
+  bool ghosts_dirty = false;  // uploaded state still carries per-block ghosts
+  // stepping
+  int cur = 0, uc = -1;
+  cudaGraphExec_t graphs[2][3][4] = {};
+  bool have_refs = false;
+  std::string err;
+};
+
+static int bfail(cb_batch *b, int code, const std::string &m) {
+  if (b) b->err = m;
+  return code;
+}
+#define BCUDA(b, call)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return bfail(b, CB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+static int bgrid(const cb_batch *b, long long work) {
+  long long g = (work + 255) / 256, cap = (long long)b->sms * 8;
+  return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+static void destroy_graphs(cb_batch *b) {
+  for (auto &m : b->graphs)
+    for (auto &r : m)
+      for (auto &g : r)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+// Pointers of one block (all fields at the block's offset) for a buffer triple.
+static DevFields block_fields(const cb_batch *b, int blk, int in, int old, int out) {
+  const long long o = b->blk[blk].off;
+  DevFields F{};
+  for (int q = 0; q < 5; q++) {
+    F.q[q] = b->qb[in][q] + o;
+    F.qold[q] = b->qb[old][q] + o;
+    F.qout[q] = out >= 0 ? b->qb[out][q] + o : nullptr;
+    F.rhs[q] = nullptr;
+  }
+  for (int e = 0; e < 3; e++)
+    for (int q = 0; q < 3; q++) {
+      F.met[e][q] = b->met[e][q] + o;
+      F.met32[e][q] = b->met32[e][q] ? b->met32[e][q] + o : nullptr;
+    }
+  F.aj = b->aj + o;
+  F.nvert = b->nvert + o;
+  F.nut = b->nut + o;
+  F.delta2 = b->delta2 + o;
+  F.delta2_32 = b->delta2_32 ? b->delta2_32 + o : nullptr;
+  for (int a = 0; a < 3; a++) F.gcl[a] = b->gcl[a] ? b->gcl[a] + o : nullptr;
+  F.status = b->status;
+  return F;
+}
+
+// Builds the 27 (in, old, out) tables and the largest-first item list.
+static int build_tables(cb_batch *b) {
+  std::vector<BatchBlock> h((size_t)27 * b->nb);
+  for (int in = 0; in < 3; in++)
+    for (int old = 0; old < 3; old++)
+      for (int out = 0; out < 3; out++)
+        for (int k = 0; k < b->nb; k++) {
+          BatchBlock &t = h[(size_t)(in * 9 + old * 3 + out) * b->nb + k];
+          const BlockHost &bh = b->blk[k];
+          t.c = bh.dc;
+          t.F = block_fields(b, k, in, old, out);
+          t.tiles_x = bh.tiles_x;
+          t.tiles_y = bh.tiles_y;
+          t.kchunk = b->kchunk;
+          t.nchunks = (bh.mz - 2 + b->kchunk - 1) / b->kchunk;
+          t.first_item = 0;
+        }
+  // items: (block, local index), ordered by descending estimated cost
+  struct It { int blk, loc; long long cost; };
+  std::vector<It> items;
+  for (int k = 0; k < b->nb; k++) {
+    const BlockHost &bh = b->blk[k];
+    const int nch = (bh.mz - 2 + b->kchunk - 1) / b->kchunk;
+    for (int z = 0; z < nch; z++)
+      for (int y = 0; y < bh.tiles_y; y++)
+        for (int x = 0; x < bh.tiles_x; x++) {
+          const int nxn = std::min(SBX, bh.mx - 2 - x * SBX), nyn = std::min(SBY, bh.my - 2 - y * SBY);
+          const int nzn = std::min(b->kchunk, bh.mz - 2 - z * b->kchunk);
+          // interior nodes plus the 3-plane prologue of each chunk
+          items.push_back({k, (z * bh.tiles_y + y) * bh.tiles_x + x, (long long)nxn * nyn * (nzn + 3)});
+        }
+  }
+  std::stable_sort(items.begin(), items.end(), [](const It &a, const It &c) { return a.cost > c.cost; });
+  std::vector<int2> hi(items.size());
+  for (size_t i = 0; i < items.size(); i++) hi[i] = make_int2(items[i].blk, items[i].loc);
+  if (b->d_items) cudaFree(b->d_items);
+  b->d_items = nullptr;
+  b->nitems = (int)hi.size();
+  BCUDA(b, cudaMalloc(&b->d_items, sizeof(int2) * hi.size()));
+  BCUDA(b, cudaMemcpy(b->d_items, hi.data(), sizeof(int2) * hi.size(), cudaMemcpyHostToDevice));
+  if (!b->d_tables) BCUDA(b, cudaMalloc(&b->d_tables, sizeof(BatchBlock) * h.size()));
+  BCUDA(b, cudaMemcpy(b->d_tables, h.data(), sizeof(BatchBlock) * h.size(), cudaMemcpyHostToDevice));
+  destroy_graphs(b);
+  return CB_OK;
+}
+
+static int block_ptab(cb_batch *b, int k) {
+  // per-block pointer table for the set-up kernels (planes of block k)
+  const long long o = b->blk[k].off;
+  double *h[64] = {};
+  for (int s = 0; s < 3; s++)
+    for (int q = 0; q < 5; q++) h[5 * s + q] = b->qb[s][q] + o;
+  for (int e = 0; e < 3; e++)
+    for (int q = 0; q < 3; q++) h[15 + 3 * e + q] = b->met[e][q] + o;
+  h[24] = b->aj + o;  // 15..24: 9 metrics + aj contiguous for the ghost fill
+  h[25] = b->nvert + o;
+  h[26] = b->nut + o;
+  for (int a = 0; a < 3; a++) h[27 + a] = b->gcl[a] ? b->gcl[a] + o : nullptr;
+  BCUDA(b, cudaMemcpyAsync(b->ptab, h, sizeof(h), cudaMemcpyHostToDevice, b->stream));
+  if (b->ptab32) {
+    float *h32[16] = {};
+    for (int e = 0; e < 3; e++)
+      for (int q = 0; q < 3; q++) h32[3 * e + q] = b->met32[e][q] + o;
+    h32[9] = b->delta2_32 + o;
+    BCUDA(b, cudaMemcpyAsync(b->ptab32, h32, sizeof(h32), cudaMemcpyHostToDevice, b->stream));
+  }
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  return CB_OK;
+}
+
+extern "C" {
+
+int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch **out) {
+  if (!cfg || !dims || !out || nblocks < 1) return CB_E_ARG;
+  *out = nullptr;
+  cb_batch *b = new cb_batch();
+  b->cfg = *cfg;
+  b->nb = nblocks;
+  auto bail = [&](int code, const char *m) {
+    fprintf(stderr, "chimera_b200: cb_batch_create: %s\n", m);
+    cb_batch_destroy(b);
+    return code;
+  };
+  if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
+      (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED))
+    return bail(CB_E_UNSUPPORTED, "option combination not built");
+  b->dev = cfg->device;
+  if (cudaSetDevice(b->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice");
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->dev);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(CB_E_CUDA, "stream");
+  long long off = 0;
+  size_t maxnn = 0;
+  for (int k = 0; k < nblocks; k++) {
+    BlockHost bh;
+    bh.mx = dims[3 * k]; bh.my = dims[3 * k + 1]; bh.mz = dims[3 * k + 2];
+    if (bh.mx < 6 || bh.my < 6 || bh.mz < 6) return bail(CB_E_ARG, "every block needs at least 6 nodes per direction");
+    DevCfg &d = bh.dc;
+    d.mx = bh.mx; d.my = bh.my; d.mz = bh.mz;
+    d.px = ((bh.mx + 4 + 15) / 16) * 16;
+    d.py = bh.my + 4;
+    d.pz = bh.mz + 4;
+    d.plane = (long long)d.px * d.py * d.pz;
+    for (int s = 0; s < 6; s++) d.bctype[s] = 7;  // block faces are interfaces: full-order stencils into the halo
+    d.les = cfg->les; d.inviscid = cfg->inviscid; d.fluxorder = cfg->fluxorder; d.eno_order = cfg->eno_order;
+    d.central = cfg->central; d.isothermal = cfg->isothermal;
+    d.s_x = cfg->s_x; d.s_y = cfg->s_y; d.s_z = cfg->s_z;
+    d.ren = cfg->ren; d.ma = cfg->ma; d.pr = cfg->pr; d.gamma = cfg->gamma; d.dt = cfg->dt; d.st = cfg->st;
+    d.cs_const = cfg->cs_const; d.ci = cfg->ci; d.ratio = cfg->ratio;
+    d.inv_ren = 1. / cfg->ren;
+    d.inv_ren_half = 1. / cfg->ren * 0.5;
+    d.gm1 = cfg->gamma - 1.0;
+    bh.off = off;
+    off += (d.plane + 31) / 32 * 32;  // 256-byte aligned block starts
+    bh.tiles_x = (bh.mx - 2 + SBX - 1) / SBX;
+    bh.tiles_y = (bh.my - 2 + SBY - 1) / SBY;
+    maxnn = std::max(maxnn, (size_t)bh.mx * bh.my * bh.mz);
+    b->blk.push_back(bh);
+  }
+  b->total = off;
+  const size_t bytes = sizeof(double) * (size_t)b->total * 28;
+  if (cudaMalloc(&b->arena, bytes) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc arena");
+  cudaMemsetAsync(b->arena, 0, bytes, b->stream);
+  int p = 0;
+  for (int s = 0; s < 3; s++)
+    for (int q = 0; q < 5; q++) b->qb[s][q] = b->arena + (size_t)b->total * (p++);
+  for (int e = 0; e < 3; e++)
+    for (int q = 0; q < 3; q++) b->met[e][q] = b->arena + (size_t)b->total * (p++);
+  b->aj = b->arena + (size_t)b->total * (p++);
+  b->nvert = b->arena + (size_t)b->total * (p++);
+  b->nut = b->arena + (size_t)b->total * (p++);
+  b->delta2 = b->arena + (size_t)b->total * (p++);
+  if (cfg->precision == CB_MIXED) {
+    const size_t mb = sizeof(float) * (size_t)b->total * 10 + sizeof(double) * (size_t)b->total * 3;
+    if (cudaMalloc(&b->arena_mixed, mb) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc mixed");
+    cudaMemsetAsync(b->arena_mixed, 0, mb, b->stream);
+    float *f = (float *)b->arena_mixed;
+    for (int e = 0; e < 3; e++)
+      for (int q = 0; q < 3; q++) b->met32[e][q] = f + (size_t)b->total * (3 * e + q);
+    b->delta2_32 = f + (size_t)b->total * 9;
+    double *g = (double *)(f + (size_t)b->total * 10);
+    for (int a = 0; a < 3; a++) b->gcl[a] = g + (size_t)b->total * a;
+    if (cudaMalloc(&b->ptab32, sizeof(float *) * 16) != cudaSuccess) return bail(CB_E_CUDA, "ptab32");
+    if (set_stage_attrs_mixed() != cudaSuccess || set_batched_attrs_mixed() != cudaSuccess)
+      return bail(CB_E_CUDA, "mixed kernel attributes");
+  }
+  if (cudaFuncSetAttribute(stage_batched_kernel<double, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(stage_batched_kernel<double, false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(stage_batched_kernel<double, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(stage_batched_kernel<double, false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(stage_kernel<double, false, true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(stage_kernel<double, false, true, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(stage_kernel<double, false, false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(stage_kernel<double, false, false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)STAGE_SMEM_BYTES) != cudaSuccess)
+    return bail(CB_E_CUDA, "kernel attributes");
+  if (cudaMalloc(&b->staging, sizeof(double) * 5 * maxnn) != cudaSuccess) return bail(CB_E_CUDA, "staging");
+  if (cudaMalloc(&b->ptab, sizeof(double *) * 64) != cudaSuccess) return bail(CB_E_CUDA, "ptab");
+  if (cudaMalloc(&b->d_counter, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "counter");
+  if (cudaMalloc(&b->status, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "status");
+  cudaMemsetAsync(b->status, 0, sizeof(unsigned), b->stream);
+  if (build_tables(b)) return bail(CB_E_CUDA, b->err.c_str());
+  *out = b;
+  return CB_OK;
+}
+
+void cb_batch_destroy(cb_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  destroy_graphs(b);
+  void *ptrs[] = {b->arena, b->arena_mixed, b->staging, b->ptab, b->ptab32, b->d_tables, b->d_items, b->d_counter,
+                  b->status, b->d_hdst, b->d_hsrc, b->d_hin, b->d_wdst, b->d_wsrc};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+const char *cb_batch_last_error(const cb_batch *b) { return b ? b->err.c_str() : "null batch"; }
+long long cb_batch_interior_nodes(const cb_batch *b) {
+  long long s = 0;
+  if (b)
+    for (auto &bh : b->blk) s += (long long)(bh.mx - 2) * (bh.my - 2) * (bh.mz - 2);
+  return s;
+}
+void *cb_batch_stream(cb_batch *b) { return b ? (void *)b->stream : nullptr; }
+int cb_batch_work_items(const cb_batch *b) { return b ? b->nitems : 0; }
+
+static int check_block(cb_batch *b, int k) {
+  if (!b || k < 0 || k >= b->nb) return CB_E_ARG;
+  return CB_OK;
+}
+
+int cb_batch_set_grid(cb_batch *b, int k, const double *coor) {
+  if (check_block(b, k) || !coor) return CB_E_ARG;
+  BlockHost &bh = b->blk[k];
+  const DevCfg &d = bh.dc;
+  const size_t nn = (size_t)bh.mx * bh.my * bh.mz;
+  if (block_ptab(b, k)) return CB_E_CUDA;
+  BCUDA(b, cudaMemcpyAsync(b->staging, coor, sizeof(double) * 3 * nn, cudaMemcpyHostToDevice, b->stream));
+  // coordinates into the block's state buffer 2 (scratch until a state is uploaded)
+  unpack_kernel<<<bgrid(b, (long long)nn), 256, 0, b->stream>>>(d, b->staging, 3, b->ptab + 10);
+  metrics_interior_kernel<<<bgrid(b, (long long)nn), 256, 0, b->stream>>>(d, (const double *const *)(b->ptab + 10),
+                                                                           b->ptab + 15, b->aj + bh.off);
+  for (int f = 0; f < 6; f++)
+    metrics_boundary_kernel<<<bgrid(b, (long long)nn / 4 + 1), 256, 0, b->stream>>>(d, b->ptab + 15, b->aj + bh.off, f);
+  const long long all = (long long)(bh.mx + 4) * (bh.my + 4) * (bh.mz + 4);
+  ghost_fill_kernel<<<bgrid(b, all), 256, 0, b->stream>>>(d, b->ptab + 15, 10);
+  delta2_kernel<<<bgrid(b, d.plane), 256, 0, b->stream>>>(d, b->aj + bh.off, b->delta2 + bh.off);
+  BCUDA(b, cudaGetLastError());
+  if (b->cfg.precision == CB_MIXED)
+    BCUDA(b, launch_mixed_prep(d, (const double *const *)(b->ptab + 15), b->delta2 + bh.off, b->ptab32,
+                               b->delta2_32 + bh.off, b->ptab + 27, bgrid(b, d.plane), b->stream));
+  for (int q = 0; q < 3; q++) BCUDA(b, cudaMemsetAsync(b->qb[2][q] + bh.off, 0, sizeof(double) * d.plane, b->stream));
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  bh.have_grid = true;
+  if (b->cur == 2) bh.have_state = false;  // the coordinates went through the block's current state buffer
+  return CB_OK;
+}
+
+int cb_batch_set_nvert(cb_batch *b, int k, const double *nvert) {
+  if (check_block(b, k) || !nvert) return CB_E_ARG;
+  BlockHost &bh = b->blk[k];
+  const size_t nn = (size_t)bh.mx * bh.my * bh.mz;
+  if (block_ptab(b, k)) return CB_E_CUDA;
+  BCUDA(b, cudaMemcpyAsync(b->staging, nvert, sizeof(double) * nn, cudaMemcpyHostToDevice, b->stream));
+  unpack_kernel<<<bgrid(b, (long long)nn), 256, 0, b->stream>>>(bh.dc, b->staging, 1, b->ptab + 25);
+  const long long all = (long long)(bh.mx + 4) * (bh.my + 4) * (bh.mz + 4);
+  ghost_fill_kernel<<<bgrid(b, all), 256, 0, b->stream>>>(bh.dc, b->ptab + 25, 1);
+  BCUDA(b, cudaGetLastError());
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  return CB_OK;
+}
+
+// State of block k (5 per node, AoS) into the CURRENT buffer, ghosts by
+// periodic wrap (the halo gather replaces them at every stage).  Resets the
+// velocity record of the eddy viscosity, as cb_upload_state does.
+int cb_batch_upload_state(cb_batch *b, int k, const double *q) {
+  if (check_block(b, k) || !q) return CB_E_ARG;
+  BlockHost &bh = b->blk[k];
+  const size_t nn = (size_t)bh.mx * bh.my * bh.mz;
+  if (b->cfg.precision == CB_MIXED && !b->have_refs) {
+    double sp = 0, se = 0, st = 0;
+    for (size_t t = 0; t < nn; t++) {
+      const double *v = q + 5 * t;
+      const double pp = (b->cfg.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0]);
+      sp += pp; se += v[4]; st += pp / v[0];
+    }
+    for (auto &x : b->blk) {
+      x.dc.p_ref = sp / nn; x.dc.e_ref = se / nn; x.dc.t_ref = st / nn; x.dc.h_ref = x.dc.e_ref + x.dc.p_ref;
+    }
+    b->have_refs = true;
+    if (build_tables(b)) return CB_E_CUDA;
+  }
+  if (block_ptab(b, k)) return CB_E_CUDA;
+  BCUDA(b, cudaMemcpyAsync(b->staging, q, sizeof(double) * 5 * nn, cudaMemcpyHostToDevice, b->stream));
+  unpack_kernel<<<bgrid(b, (long long)nn), 256, 0, b->stream>>>(bh.dc, b->staging, 5, b->ptab + 5 * b->cur);
+  const long long all = (long long)(bh.mx + 4) * (bh.my + 4) * (bh.mz + 4);
+  ghost_fill_kernel<<<bgrid(b, all), 256, 0, b->stream>>>(bh.dc, b->ptab + 5 * b->cur, 5);
+  BCUDA(b, cudaGetLastError());
+  BCUDA(b, cudaMemsetAsync(b->nut + bh.off, 0, sizeof(double) * bh.dc.plane, b->stream));
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  b->uc = -1;
+  b->ghosts_dirty = true;
+  bh.have_state = true;
+  return CB_OK;
+}
+
+int cb_batch_download_state(cb_batch *b, int k, double *q) {
+  if (check_block(b, k) || !q) return CB_E_ARG;
+  BlockHost &bh = b->blk[k];
+  const size_t nn = (size_t)bh.mx * bh.my * bh.mz;
+  if (block_ptab(b, k)) return CB_E_CUDA;
+  pack_kernel<<<bgrid(b, (long long)nn), 256, 0, b->stream>>>(bh.dc, (const double *const *)(b->ptab + 5 * b->cur), 5,
+                                                               b->staging);
+  BCUDA(b, cudaGetLastError());
+  BCUDA(b, cudaMemcpyAsync(q, b->staging, sizeof(double) * 5 * nn, cudaMemcpyDeviceToHost, b->stream));
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  return CB_OK;
+}
+
+static bool interior_node(const BlockHost &bh, int i, int j, int k) {
+  return i >= 1 && i <= bh.mx - 2 && j >= 1 && j <= bh.my - 2 && k >= 1 && k <= bh.mz - 2;
+}
+
+// Metrics of block k as resident (csi, eta, zet: 3 per node; aj: 1), natural AoS.
+int cb_batch_get_metrics(cb_batch *b, int k, double *csi, double *eta, double *zet, double *aj) {
+  if (check_block(b, k) || !csi || !eta || !zet || !aj) return CB_E_ARG;
+  BlockHost &bh = b->blk[k];
+  if (!bh.have_grid) return bfail(b, CB_E_STATE, "no grid");
+  const size_t nn = (size_t)bh.mx * bh.my * bh.mz;
+  if (block_ptab(b, k)) return CB_E_CUDA;
+  double *dst[4] = {csi, eta, zet, aj};
+  for (int e = 0; e < 4; e++) {
+    const int nc = e < 3 ? 3 : 1;
+    pack_kernel<<<bgrid(b, (long long)nn), 256, 0, b->stream>>>(bh.dc, (const double *const *)(b->ptab + 15 + 3 * e), nc,
+                                                                 b->staging);
+    BCUDA(b, cudaGetLastError());
+    BCUDA(b, cudaMemcpyAsync(dst[e], b->staging, sizeof(double) * nc * nn, cudaMemcpyDeviceToHost, b->stream));
+    BCUDA(b, cudaStreamSynchronize(b->stream));
+  }
+  return CB_OK;
+}
+
+// Halo maps: n entries of 9 ints (dst block, di, dj, dk, src block, si, sj, sk,
+// from_stage_input), node indices in -2..m+1.
+//   kind CB_HALO_STAGE: applied after every stage; the source is read from the
+//     stage output (must then be an interior node) or, with from_stage_input,
+//     from the stage input (any node).
+//   kind CB_HALO_WRAP: plain wrap (DMGlobalToLocal across blocks), applied to
+//     the eddy viscosity every step and once to the uploaded state; the last
+//     int is ignored and no source may also be a destination.
+// Destinations must be non-interior nodes, each at most once per map.
+int cb_batch_set_halo_map(cb_batch *b, int kind, long long n, const int *e) {
+  if (!b || n < 0 || (n && !e) || (kind != CB_HALO_STAGE && kind != CB_HALO_WRAP)) return CB_E_ARG;
+  std::vector<long long> hd((size_t)n), hs((size_t)n);
+  std::vector<unsigned char> hin((size_t)n);
+  for (long long t = 0; t < n; t++) {
+    const int *r = e + 9 * t;
+    if (r[0] < 0 || r[0] >= b->nb || r[4] < 0 || r[4] >= b->nb) return bfail(b, CB_E_ARG, "halo map: block index");
+    const BlockHost &db = b->blk[r[0]], &sb = b->blk[r[4]];
+    if (r[1] < -2 || r[1] > db.mx + 1 || r[2] < -2 || r[2] > db.my + 1 || r[3] < -2 || r[3] > db.mz + 1 ||
+        r[5] < -2 || r[5] > sb.mx + 1 || r[6] < -2 || r[6] > sb.my + 1 || r[7] < -2 || r[7] > sb.mz + 1)
+      return bfail(b, CB_E_ARG, "halo map: node outside the padded box");
+    if (interior_node(db, r[1], r[2], r[3])) return bfail(b, CB_E_ARG, "halo map: destination is an interior node");
+    const bool fin = kind == CB_HALO_STAGE && r[8] != 0;
+    if (kind == CB_HALO_STAGE && !fin && !interior_node(sb, r[5], r[6], r[7]))
+      return bfail(b, CB_E_ARG, "halo map: stage-output source is not an interior node");
+    hd[t] = db.off + gidx(db.dc, r[1], r[2], r[3]);
+    hs[t] = sb.off + gidx(sb.dc, r[5], r[6], r[7]);
+    hin[t] = fin ? 1 : 0;
+  }
+  std::vector<long long> sd(hd);
+  std::sort(sd.begin(), sd.end());
+  if (std::adjacent_find(sd.begin(), sd.end()) != sd.end()) return bfail(b, CB_E_ARG, "halo map: duplicate destination");
+  if (kind == CB_HALO_WRAP)
+    for (long long t = 0; t < n; t++)
+      if (std::binary_search(sd.begin(), sd.end(), hs[t]))
+        return bfail(b, CB_E_ARG, "halo map: wrap source is also a destination");
+  long long **pd = kind == CB_HALO_STAGE ? &b->d_hdst : &b->d_wdst;
+  long long **ps = kind == CB_HALO_STAGE ? &b->d_hsrc : &b->d_wsrc;
+  if (*pd) cudaFree(*pd);
+  if (*ps) cudaFree(*ps);
+  *pd = *ps = nullptr;
+  if (kind == CB_HALO_STAGE) {
+    if (b->d_hin) cudaFree(b->d_hin);
+    b->d_hin = nullptr;
+    b->nhalo = n;
+  } else {
+    b->nwrap = n;
+  }
+  if (n) {
+    BCUDA(b, cudaMalloc(pd, sizeof(long long) * n));
+    BCUDA(b, cudaMalloc(ps, sizeof(long long) * n));
+    BCUDA(b, cudaMemcpy(*pd, hd.data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
+    BCUDA(b, cudaMemcpy(*ps, hs.data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
+    if (kind == CB_HALO_STAGE) {
+      BCUDA(b, cudaMalloc(&b->d_hin, n));
+      BCUDA(b, cudaMemcpy(b->d_hin, hin.data(), n, cudaMemcpyHostToDevice));
+    }
+  }
+  if (kind == CB_HALO_WRAP) b->ghosts_dirty = true;
+  destroy_graphs(b);
+  return CB_OK;
+}
+
+// Self-periodic maps: every block wraps onto itself exactly as the
+// single-block periodic path (FormBCS stale copy, rhs.c:1107-1227, then
+// DMGlobalToLocal), so each block evolves as it would alone.
+int cb_batch_halo_periodic(cb_batch *b) {
+  if (!b) return CB_E_ARG;
+  std::vector<int> st, wr;
+  auto wrapi = [](int x, int m) { return x < 0 ? x + m : (x >= m ? x - m : x); };
+  for (int k = 0; k < b->nb; k++) {
+    const BlockHost &bh = b->blk[k];
+    for (int kk = -2; kk <= bh.mz + 1; kk++)
+      for (int j = -2; j <= bh.my + 1; j++)
+        for (int i = -2; i <= bh.mx + 1; i++) {
+          if (interior_node(bh, i, j, kk)) continue;
+          const int oi = wrapi(i, bh.mx), oj = wrapi(j, bh.my), ok = wrapi(kk, bh.mz);
+          // stage map: the device rule of the single-block path (bc_source)
+          int si = oi, sj = oj, sk = ok, fin = 0;
+          const bool bnd = !interior_node(bh, oi, oj, ok);
+          if (bnd) {
+            fin = 1;
+            if (ok == 0) sk = ok - 2;
+            else if (ok == bh.mz - 1) sk = ok + 2;
+            else if (oj == 0) sj = oj - 2;
+            else if (oj == bh.my - 1) sj = oj + 2;
+            else if (oi == 0) si = oi - 2;
+            else si = oi + 2;
+          }
+          const int r[9] = {k, i, j, kk, k, si, sj, sk, fin};
+          st.insert(st.end(), r, r + 9);
+          // wrap map: ghosts take their owned image; owned nodes keep their value
+          const bool ghost = i != oi || j != oj || kk != ok;
+          if (ghost) {
+            const int w[9] = {k, i, j, kk, k, oi, oj, ok, 0};
+            wr.insert(wr.end(), w, w + 9);
+          }
+        }
+  }
+  int rc = cb_batch_set_halo_map(b, CB_HALO_STAGE, (long long)(st.size() / 9), st.data());
+  if (rc) return rc;
+  return cb_batch_set_halo_map(b, CB_HALO_WRAP, (long long)(wr.size() / 9), wr.data());
+}
+
+// Applies the wrap map to the current state (after uploads).
+static int fill_ghosts(cb_batch *b) {
+  if (b->nwrap) {
+    for (int q = 0; q < 5; q++)
+      plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, b->qb[b->cur][q]);
+    BCUDA(b, cudaGetLastError());
+  }
+  b->ghosts_dirty = false;
+  return CB_OK;
+}
+
+static void rk_ab(const cb_batch *b, int s, double *alfa, double *beta) {
+  double a[3] = {1., 1 / 4., 2 / 3.}, bb[3] = {1., 3 / 4., 1 / 3.};  // solvers.c:233-234
+  if (b->cfg.fluxorder < 3) { a[1] = 1 / 2.; bb[1] = 1 / 2.; }
+  *alfa = a[s];
+  *beta = bb[s];
+}
+
+// One step: eddy viscosity per block, then per stage one stage launch
+// (persistent over all blocks, or one per block) and one halo gather.
+static int enqueue_batch_step(cb_batch *b, int per_block) {
+  const bool les = b->cfg.les != 0, visc = b->cfg.inviscid == 0, mixed = b->cfg.precision == CB_MIXED;
+  if (les && visc) {
+    // Compute_eddy_viscosity_LES per block from the recorded state; the
+    // pointer arrays are the q and met members of the block's (uc, uc, uc)
+    // table entry in device memory
+    const int u = b->uc < 0 ? 0 : b->uc;
+    for (int k = 0; k < b->nb; k++) {
+      const BlockHost &bh = b->blk[k];
+      const long long o = bh.off;
+      const long long work = (long long)(bh.mx - 2) * (bh.my - 2) * (bh.mz - 2);
+      const char *ent = reinterpret_cast<const char *>(b->d_tables + (size_t)(u * 13) * b->nb + k);
+      const double *const *qu = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
+      const double *const *mt = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, met));
+      eddy_viscosity_kernel<<<bgrid(b, work), 256, 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
+                                                                   b->delta2 + o, b->nvert + o, b->nut + o);
+    }
+    if (b->nwrap) {
+      plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, b->nut);
+    } else {
+      for (int k = 0; k < b->nb; k++) {
+        const BlockHost &bh = b->blk[k];
+        const long long all = (long long)(bh.mx + 4) * (bh.my + 4) * (bh.mz + 4);
+        // a one-entry pointer table: the nut plane of block k sits in the table's nut member
+        const char *ent = reinterpret_cast<const char *>(b->d_tables + k);
+        double *const *np = reinterpret_cast<double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, nut));
+        ghost_fill_kernel<<<bgrid(b, all), 256, 0, b->stream>>>(bh.dc, np, 1);
+      }
+    }
+    BCUDA(b, cudaGetLastError());
+  }
+  const int ns = b->cfg.fluxorder;
+  const int old = b->cur, A = (b->cur + 1) % 3, B = (b->cur + 2) % 3;
+  int in = b->cur;
+  for (int s = 0; s < ns; s++) {
+    const int out = (s % 2 == 0) ? A : B;
+    double alfa, beta;
+    rk_ab(b, s, &alfa, &beta);
+    const double adt = alfa * b->cfg.dt * b->cfg.st;
+    const BatchBlock *tab = b->d_tables + (size_t)(in * 9 + old * 3 + out) * b->nb;
+    if (!per_block) {
+      BCUDA(b, cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream));
+      const int ctas = b->sms * (mixed ? 2 : 1);
+      if (mixed) {
+        BCUDA(b, launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, les, visc, ctas,
+                                      b->stream));
+      } else {
+        if (les && visc)
+          stage_batched_kernel<double, false, true, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+        else if (les)
+          stage_batched_kernel<double, false, true, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+        else if (visc)
+          stage_batched_kernel<double, false, false, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+        else
+          stage_batched_kernel<double, false, false, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+      }
+    } else {
+      for (int k = 0; k < b->nb; k++) {
+        const BlockHost &bh = b->blk[k];
+        const DevFields F = block_fields(b, k, in, old, out);
+        const int nk = bh.mz - 2;
+        // per-block k-chunk for whole waves of one CTA per SM
+        const int tiles = bh.tiles_x * bh.tiles_y;
+        int kc = nk;
+        double best = 1e30;
+        for (int cand = 4; cand <= nk; cand++) {
+          const long long blocks = (long long)tiles * ((nk + cand - 1) / cand);
+          const double cost = (double)((blocks + b->sms - 1) / b->sms) * (cand + 3.0);
+          if (cost < best) { best = cost; kc = cand; }
+        }
+        if (mixed) {
+          BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, b->stream));
+        } else {
+          dim3 grid(bh.tiles_x, bh.tiles_y, (nk + kc - 1) / kc);
+          if (les && visc)
+            stage_kernel<double, false, true, true, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
+          else if (les)
+            stage_kernel<double, false, true, false, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
+          else if (visc)
+            stage_kernel<double, false, false, true, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
+          else
+            stage_kernel<double, false, false, false, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
+        }
+      }
+    }
+    BCUDA(b, cudaGetLastError());
+    if (b->nhalo) {
+      DevFields G{};
+      for (int q = 0; q < 5; q++) { G.q[q] = b->qb[in][q]; G.qout[q] = b->qb[out][q]; }
+      halo_gather_kernel<<<bgrid(b, b->nhalo), 256, 0, b->stream>>>(b->d_hdst, b->d_hsrc, b->d_hin, b->nhalo, G);
+      BCUDA(b, cudaGetLastError());
+    }
+    if (visc) b->uc = in;
+    in = out;
+  }
+  b->cur = in;
+  return CB_OK;
+}
+
+// mode 0: one persistent stage launch over all blocks; 1: one launch per block.
+// Steps are captured once per rotation state and replayed as CUDA graphs.
+int cb_batch_rk_step(cb_batch *b, int nsteps, int mode) {
+  if (!b || nsteps < 0 || (mode != 0 && mode != 1)) return CB_E_ARG;
+  for (auto &bh : b->blk)
+    if (!bh.have_grid || !bh.have_state) return bfail(b, CB_E_STATE, "every block needs a grid and a state");
+  if (!b->nhalo) return bfail(b, CB_E_STATE, "no halo map (cb_batch_set_halo_map / cb_batch_halo_periodic)");
+  if (b->ghosts_dirty && fill_ghosts(b)) return CB_E_CUDA;
+  for (int n = 0; n < nsteps; n++) {
+    cudaGraphExec_t &g = b->graphs[mode][b->cur][b->uc + 1];
+    if (!g) {
+      cudaGraph_t graph;
+      const int cur0 = b->cur, uc0 = b->uc;
+      BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      int e = enqueue_batch_step(b, mode);
+      cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+      if (e) return e;
+      if (ce != cudaSuccess) return bfail(b, CB_E_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&g, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return bfail(b, CB_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(ce));
+      b->cur = cur0;
+      b->uc = uc0;
+    }
+    BCUDA(b, cudaGraphLaunch(g, b->stream));
+    // bookkeeping of the rotation (as enqueue_batch_step)
+    const int A = (b->cur + 1) % 3, B = (b->cur + 2) % 3;
+    int in = b->cur;
+    for (int s = 0; s < b->cfg.fluxorder; s++) {
+      if (!b->cfg.inviscid) b->uc = in;
+      in = (s % 2 == 0) ? A : B;
+    }
+    b->cur = in;
+  }
+  return CB_OK;
+}
+
+int cb_batch_sync(cb_batch *b) {
+  if (!b) return CB_E_ARG;
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  unsigned st = 0;
+  BCUDA(b, cudaMemcpy(&st, b->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (st) {
+    BCUDA(b, cudaMemset(b->status, 0, sizeof(unsigned)));
+    return bfail(b, CB_E_NONFINITE, "device status: non-finite state or rho/p <= 0");
+  }
+  return CB_OK;
+}
+
+// Autotuner: times one stage launch of the persistent form for each candidate
+// k-chunk (largest-first item list rebuilt each time) and keeps the fastest.
+// The state is not advanced: the timed launches write a scratch buffer pair.
+int cb_batch_autotune(cb_batch *b, int *best_kchunk, double *best_ms) {
+  if (!b) return CB_E_ARG;
+  for (auto &bh : b->blk)
+    if (!bh.have_grid || !bh.have_state) return bfail(b, CB_E_STATE, "every block needs a grid and a state");
+  const int cands[] = {6, 8, 12, 16, 24, 32, 48};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const bool les = b->cfg.les != 0, visc = b->cfg.inviscid == 0, mixed = b->cfg.precision == CB_MIXED;
+  int best = b->kchunk;
+  double bms = 1e30;
+  // the timed launches write a buffer that holds neither the state nor the
+  // recorded velocity field of the next eddy-viscosity evaluation
+  const int in = b->cur;
+  int out = (b->cur + 1) % 3;
+  if (out == b->uc) out = (b->cur + 2) % 3;
+  for (int kc : cands) {
+    b->kchunk = kc;
+    if (build_tables(b)) return CB_E_CUDA;
+    const BatchBlock *tab = b->d_tables + (size_t)(in * 9 + in * 3 + out) * b->nb;
+    float tot = 0.f;
+    for (int rep = 0; rep < 3; rep++) {
+      cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream);
+      cudaEventRecord(e0, b->stream);
+      const int ctas = b->sms * (mixed ? 2 : 1);
+      if (mixed) {
+        launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, les, visc, ctas, b->stream);
+      } else if (les && visc) {
+        stage_batched_kernel<double, false, true, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0);
+      } else if (les) {
+        stage_batched_kernel<double, false, true, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0);
+      } else if (visc) {
+        stage_batched_kernel<double, false, false, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0);
+      } else {
+        stage_batched_kernel<double, false, false, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0);
+      }
+      cudaEventRecord(e1, b->stream);
+      BCUDA(b, cudaEventSynchronize(e1));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep) tot += ms;  // first launch warms caches
+    }
+    const double avg = tot / 2.0;
+    if (avg < bms) { bms = avg; best = kc; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->kchunk = best;
+  if (build_tables(b)) return CB_E_CUDA;
+  if (best_kchunk) *best_kchunk = best;
+  if (best_ms) *best_ms = bms;
+  return CB_OK;
+}
+
+}  // extern "C"

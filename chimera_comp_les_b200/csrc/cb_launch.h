@@ -16,4 +16,10 @@ cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, 
 cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, float *const *met32,
                               float *delta2_32, double *const *gcl, int grid, cudaStream_t s);
 
+// Persistent batched stage kernel of the mixed form (multi-block work queue).
+struct BatchBlock;
+cudaError_t set_batched_attrs_mixed();
+cudaError_t launch_batched_mixed(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int istage,
+                                 double alfa, double beta, double adt, bool les, bool visc, int ctas, cudaStream_t s);
+
 }  // namespace cb

@@ -73,6 +73,36 @@ cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, 
   return cudaGetLastError();
 }
 
+namespace {
+template <bool LES, bool VISC>
+cudaError_t battr1() {
+  return cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)STAGE_SMEM_BYTES_MIXED);
+}
+}  // namespace
+
+cudaError_t set_batched_attrs_mixed() {
+  cudaError_t e;
+  if ((e = battr1<true, true>()) != cudaSuccess) return e;
+  if ((e = battr1<true, false>()) != cudaSuccess) return e;
+  if ((e = battr1<false, true>()) != cudaSuccess) return e;
+  return battr1<false, false>();
+}
+
+cudaError_t launch_batched_mixed(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int istage,
+                                 double alfa, double beta, double adt, bool les, bool visc, int ctas, cudaStream_t s) {
+  const size_t sm = STAGE_SMEM_BYTES_MIXED;
+  if (les && visc)
+    stage_batched_kernel<float, true, true, true><<<ctas, SNT, sm, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
+  else if (les)
+    stage_batched_kernel<float, true, true, false><<<ctas, SNT, sm, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
+  else if (visc)
+    stage_batched_kernel<float, true, false, true><<<ctas, SNT, sm, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
+  else
+    stage_batched_kernel<float, true, false, false><<<ctas, SNT, sm, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, float *const *met32,
                               float *delta2_32, double *const *gcl, int grid, cudaStream_t s) {
   mixed_prep_kernel<<<grid, 256, 0, s>>>(c, met, delta2, met32, delta2_32, gcl);

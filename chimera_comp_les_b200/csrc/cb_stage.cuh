@@ -483,12 +483,12 @@ __device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc, bool val
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// One tile (tile column bxi, byi, k-chunk bzi) of one block: the whole k march.
 template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE>
-__global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
-    stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
+__device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, int bxi, int byi, int bzi, int istage,
+                                           double alfa, double beta, double adt, int kchunk, double *smem_d) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
   constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
-  extern __shared__ double smem_d[];
   double *stg = smem_d;  // [5][PN] raw FP64 Q of the next plane
   R *smem = reinterpret_cast<R *>(smem_d + (size_t)5 * PN);
   Ring<R, BX, BY> Rg;
@@ -498,8 +498,8 @@ __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
   R *gzb = gyb + (size_t)NG * S_NYF;    // [NG][S_NZF]
 
   const int tid = threadIdx.x;
-  const int i0 = 1 + blockIdx.x * BX, j0 = 1 + blockIdx.y * BY;
-  const int kb = 1 + blockIdx.z * kchunk;
+  const int i0 = 1 + bxi * BX, j0 = 1 + byi * BY;
+  const int kb = 1 + bzi * kchunk;
   const int ke = min(c.mz - 1, kb + kchunk);  // exclusive
   // node updated by this thread (threads 224..255 only load and compute faces)
   const int utx = tid % BX, uty = tid / BX;
@@ -728,6 +728,49 @@ __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     if (more) derive(base & 3);  // plane k+3 into the slot of plane k-1
     base++;
     __syncthreads();
+  }
+}
+
+template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE>
+__global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
+    stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
+  extern __shared__ double smem_d[];
+  stage_tile<R, MIX, LES, VISC, RHS_MODE>(c, F, blockIdx.x, blockIdx.y, blockIdx.z, istage, alfa, beta, adt, kchunk,
+                                          smem_d);
+}
+
+// ------------------------------------------------------- batched form ----
+// Several blocks of uneven sizes advanced by ONE persistent launch: every CTA
+// takes work items (block, tile column, k-chunk) from a device counter until
+// the list is exhausted (a bounded loop, no waiting on other CTAs).  Items are
+// listed largest-first by the host so the tail of the launch is short.
+struct BatchBlock {
+  DevCfg c;
+  DevFields F;
+  int tiles_x, tiles_y, nchunks, kchunk;
+  long long first_item;  // index of this block's first item in the global list
+};
+
+template <typename R, bool MIX, bool LES, bool VISC>
+__global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
+    stage_batched_kernel(const BatchBlock *__restrict__ blocks, const int2 *__restrict__ items, int nitems,
+                         unsigned *__restrict__ counter, int istage, double alfa, double beta, double adt) {
+  extern __shared__ double smem_d[];
+  __shared__ BatchBlock bb;
+  __shared__ int item;
+  for (;;) {
+    if (threadIdx.x == 0) item = (int)atomicAdd(counter, 1u);
+    __syncthreads();
+    const int it = item;
+    if (it >= nitems) break;
+    const int2 ib = items[it];  // (block, local item index)
+    if (threadIdx.x == 0) bb = blocks[ib.x];
+    __syncthreads();
+    const int txy = bb.tiles_x * bb.tiles_y;
+    const int bzi = ib.y / txy, rem = ib.y - bzi * txy;
+    const int byi = rem / bb.tiles_x, bxi = rem - byi * bb.tiles_x;
+    stage_tile<R, MIX, LES, VISC, false>(bb.c, bb.F, bxi, byi, bzi, istage, alfa, beta, adt, bb.kchunk, smem_d);
+    __syncthreads();  // bb and item are rewritten by the next iteration
   }
 }
 

@@ -55,3 +55,20 @@ def field_errors(a: np.ndarray, ref: np.ndarray):
         l2.append(float(np.linalg.norm(d)) / nr if nr else float(np.linalg.norm(d)))
         linf.append(float(np.abs(d).max()) / mr if mr else float(np.abs(d).max()))
     return l2, linf
+
+
+def spectral_radius_max(q: np.ndarray, csi, eta, zet, aj, nvert, gamma: float = 1.4) -> float:
+    """Host twin of the device CFL reduction: max over interior fluid nodes of
+    aj * sum_d (|m_d . u| + c |m_d|)."""
+    s = (slice(1, -1),) * 3
+    r = q[s + (0,)]
+    u, v, w = (q[s + (a,)] / r for a in (1, 2, 3))
+    p = (gamma - 1) * (q[s + (4,)] - 0.5 * r * (u * u + v * v + w * w))
+    c = np.sqrt(np.abs(gamma * p / r))
+    lam = np.zeros_like(r)
+    for m in (csi, eta, zet):
+        mx, my, mz = m[s + (0,)], m[s + (1,)], m[s + (2,)]
+        lam += np.abs(mx * u + my * v + mz * w) + c * np.sqrt(mx * mx + my * my + mz * mz)
+    lam *= aj[s]
+    lam[nvert[s] >= 0.1] = 0.0
+    return float(lam.max())

@@ -137,6 +137,12 @@ class Block:
         self._check(self.lib.cb_rhs(self._ctx, istage, dptr(out)))
         return out
 
+    def cfl_dt(self, cfl: float):
+        """(dt, lambda_max) for the CFL number `cfl` on the current state."""
+        dt, lam = C.c_double(), C.c_double()
+        self._check(self.lib.cb_cfl_dt(self._ctx, float(cfl), C.byref(dt), C.byref(lam)))
+        return dt.value, lam.value
+
     def CalcUCat(self):
         self._check(self.lib.cb_calc_ucat(self._ctx))
 

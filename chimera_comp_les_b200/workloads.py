@@ -90,3 +90,104 @@ def random_smooth_state(shape, seed: int, gamma: float = 1.4, amp: float = 0.05,
         fields.append(f)
     rho, u, v, w, p = fields
     return conserved(rho, u, v, w, p, gamma)
+
+
+def distorted_periodic_grid(n, length, amp: float, seed: int, modes: int = 3) -> np.ndarray:
+    """Periodic box (n, length as in ``periodic_grid``) whose nodes are moved
+    by a seeded smooth random field: every coordinate gets a sum of `modes`
+    periodic sine modes (wavenumbers 1..2 per direction, random phases) scaled
+    so the largest displacement is `amp`."""
+    ns = (n, n, n) if np.isscalar(n) else tuple(int(x) for x in n)
+    ls = (length, length, length) if np.isscalar(length) else tuple(length)
+    g = periodic_grid(ns, ls, 0.0)
+    rng = np.random.default_rng(seed)
+    xi = [2 * math.pi * (np.arange(ns[d] + 2) - 1.0) / ns[d] for d in range(3)]
+    z, y, x = np.meshgrid(xi[2], xi[1], xi[0], indexing="ij")
+    out = g.copy()
+    for c in range(3):
+        f = np.zeros_like(x)
+        for _ in range(modes):
+            kx, ky, kz = rng.integers(0, 3, size=3)
+            if kx == ky == kz == 0:
+                kx = 1
+            f += rng.uniform(-1, 1) * np.sin(kx * x + ky * y + kz * z + rng.uniform(0, 2 * math.pi))
+        m = np.abs(f).max()
+        if m > 0:
+            out[..., c] += amp * f / m
+    return np.ascontiguousarray(out)
+
+
+def _spectrum(kind: str, k: np.ndarray, k_peak: float) -> np.ndarray:
+    if kind == "von_karman":  # E ~ (k/kp)^4 / (1 + (k/kp)^2)^(17/6)
+        r = k / k_peak
+        return r ** 4 / (1.0 + r * r) ** (17.0 / 6.0)
+    if kind == "passot_pouquet":  # E ~ (k/k0)^4 exp(-2 (k/k0)^2)
+        r = k / k_peak
+        return r ** 4 * np.exp(-2.0 * r * r)
+    raise ValueError(kind)
+
+
+def isotropic_turbulence(n, seed: int, k_peak: float = 4.0, mach_t: float = 0.3, spectrum: str = "von_karman",
+                         gamma: float = 1.4, u_rms: float | None = None) -> np.ndarray:
+    """Solenoidal random velocity field with energy spectrum `spectrum` peaking
+    near k_peak (integer wavenumbers of a 2*pi box) and random phases from
+    `seed`, on rho = 1, p = 1/gamma (sound speed 1).  The field is scaled so
+    sqrt(<u.u>) = mach_t (or, with u_rms given, so each component has that rms,
+    and mach_t is ignored).  n: unique points (nx, ny, nz); returns the state on
+    the DMDA nodes (nz+2, ny+2, nx+2, 5) with the periodic images."""
+    nx, ny, nz = (n, n, n) if np.isscalar(n) else tuple(int(x) for x in n)
+    rng = np.random.default_rng(seed)
+    kx, ky, kz = (np.fft.fftfreq(m, 1.0 / m) for m in (nx, ny, nz))
+    KZ, KY, KX = np.meshgrid(kz, ky, kx, indexing="ij")
+    k2 = KX * KX + KY * KY + KZ * KZ
+    k = np.sqrt(k2)
+    amp = np.zeros_like(k)
+    # no Nyquist modes (their -k is the same coefficient, which breaks the projection)
+    nz_ = (k > 0) & (2 * np.abs(KX) < nx) & (2 * np.abs(KY) < ny) & (2 * np.abs(KZ) < nz)
+    amp[nz_] = np.sqrt(_spectrum(spectrum, k[nz_], k_peak) / (4 * math.pi * k2[nz_]))
+    uh = [amp * (rng.standard_normal(k.shape) + 1j * rng.standard_normal(k.shape)) for _ in range(3)]
+    kdu = KX * uh[0] + KY * uh[1] + KZ * uh[2]
+    inv = np.zeros_like(k)
+    inv[nz_] = 1.0 / k2[nz_]
+    uh = [uh[0] - KX * kdu * inv, uh[1] - KY * kdu * inv, uh[2] - KZ * kdu * inv]
+    u = [np.real(np.fft.ifftn(a)) for a in uh]
+    if u_rms is not None:
+        s = u_rms / math.sqrt(np.mean((u[0] ** 2 + u[1] ** 2 + u[2] ** 2) / 3.0))
+    else:
+        s = mach_t / math.sqrt(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2))
+    u = [a * s for a in u]
+    iz, iy, ix = ((np.arange(m + 2) - 1) % m for m in (nz, ny, nx))
+    u = [a[np.ix_(iz, iy, ix)] for a in u]
+    rho = np.ones_like(u[0])
+    p = np.full_like(u[0], 1.0 / gamma)
+    return conserved(rho, u[0], u[1], u[2], p, gamma)
+
+
+def multiblock_set(seed: int = 2024, nblocks: int = 24, ranges=((32, 160), (32, 128), (32, 96)), amp: float = 0.03,
+                   k_peak: float = 4.0, mach_t: float = 0.3, gamma: float = 1.4, cfl: float = 0.4):
+    """Uneven multi-block set: block sizes (unique points per direction) drawn
+    uniformly from `ranges`, each block a [0, 2*pi]^3 box with a seeded smooth
+    metric distortion of amplitude `amp` carrying decaying isotropic turbulence
+    (von Karman spectrum, k_peak, turbulent Mach mach_t), and a seeded donor
+    permutation without fixed points for the 2-node overlap halo.
+
+    Returns dict(dims=[(mx, my, mz)] DMDA node counts, coords=[...], q=[...],
+    perm=[...], dt=...) with dt from the CFL estimate
+    cfl / max_b sum_d (max|u| + c) * N_d / (2*pi) * 1.2."""
+    rng = np.random.default_rng(seed)
+    uniq = [tuple(int(rng.integers(lo, hi + 1)) for lo, hi in ranges) for _ in range(nblocks)]
+    while True:
+        perm = rng.permutation(nblocks)
+        if nblocks == 1 or not (perm == np.arange(nblocks)).any():
+            break
+    coords, qs = [], []
+    lam = 0.0
+    for b, n in enumerate(uniq):
+        coords.append(distorted_periodic_grid(n, 2 * math.pi, amp, seed=seed * 1000 + 2 * b))
+        q = isotropic_turbulence(n, seed * 1000 + 2 * b + 1, k_peak=k_peak, mach_t=mach_t, gamma=gamma)
+        qs.append(q)
+        umax = float(np.abs(q[..., 1:4] / q[..., :1]).max())
+        lam = max(lam, sum((umax + 1.0) * n[d] / (2 * math.pi) for d in range(3)) * 1.2)
+    dt = math.floor(cfl / lam * 1e5) / 1e5
+    return dict(dims=[(n[0] + 2, n[1] + 2, n[2] + 2) for n in uniq], coords=coords, q=qs,
+                perm=[int(x) for x in perm], dt=dt)

@@ -126,6 +126,14 @@ int cb_get_nut(cb_ctx *ctx, double *nut);
  * the context's stream; returns after enqueueing. */
 int cb_rk_step(cb_ctx *ctx, int nsteps);
 
+/* Time step from the CFL condition on the current state: dt = cfl / lambda_max,
+ * lambda = aj * sum_d (|m_d . u| + c |m_d|) the largest inviscid spectral radius
+ * over interior fluid nodes (warp-shuffle max reduction on the device).  No
+ * counterpart in the reference, which runs a fixed -dt (init.c:94); its
+ * Spectral (rhs.c:4739) is an unused incompressible estimate.  Does not change
+ * the context's dt; synchronises. */
+int cb_cfl_dt(cb_ctx *ctx, double cfl, double *dt, double *lambda_max);
+
 /* Waits for the context's stream and checks the device status word
  * (CB_E_NONFINITE when a NaN/Inf or non-positive rho/p was produced). */
 int cb_sync(cb_ctx *ctx);
@@ -176,6 +184,58 @@ int cb_abi_version(void);
 #define CB_NOALLOC_MAX_PLANE 98304LL
 int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const double *d_q, const double *d_nvert,
                    const double *d_nut, double *d_rhs, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Batched multi-block form.  Replaces the per-block loop of the reference's
+ * time step (solvers.c:246, `for (bi = 0; bi < block_number; bi++)` around
+ * RungeKutta) with one context holding every block resident on the GPU.
+ * Per RK stage: ONE persistent stage launch whose CTAs take (block, tile,
+ * k-chunk) work items, largest first, from a device counter, then one
+ * on-device gather that fills every block's boundary and ghost nodes from a
+ * halo map.  A whole step runs as a CUDA graph.  Blocks share the cb_config
+ * (bctype is ignored: block faces are interfaces filled by the halo map);
+ * their sizes may differ.
+ *
+ * Per block k: cb_batch_set_grid (coordinates, 3 per node, AoS, as
+ * cb_set_grid), cb_batch_set_nvert (optional; default 0), cb_batch_upload_state
+ * (5 per node).  Then a halo map (cb_batch_halo_periodic for independent
+ * periodic blocks, each of which then evolves exactly as it would alone in a
+ * cb_ctx), cb_batch_rk_step, cb_batch_sync, cb_batch_download_state. */
+typedef struct cb_batch cb_batch;
+/* dims: 3 ints (mx, my, mz) per block, each >= 6 */
+int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch **out);
+void cb_batch_destroy(cb_batch *b);
+const char *cb_batch_last_error(const cb_batch *b);
+long long cb_batch_interior_nodes(const cb_batch *b);
+void *cb_batch_stream(cb_batch *b);
+int cb_batch_work_items(const cb_batch *b);
+int cb_batch_set_grid(cb_batch *b, int block, const double *coor);
+int cb_batch_set_nvert(cb_batch *b, int block, const double *nvert);
+int cb_batch_upload_state(cb_batch *b, int block, const double *q);
+int cb_batch_download_state(cb_batch *b, int block, double *q);
+/* metrics of a block as resident (csi, eta, zet 3 per node, aj 1), AoS */
+int cb_batch_get_metrics(cb_batch *b, int block, double *csi, double *eta, double *zet, double *aj);
+/* Halo maps: n entries of 9 ints (dst block, di, dj, dk, src block, si, sj,
+ * sk, from_stage_input), node indices -2..m+1.  CB_HALO_STAGE runs after every
+ * stage: the source is the stage output (then it must be an interior node) or,
+ * with from_stage_input, the stage input (the reference's FormBCS reads the
+ * not-yet-refreshed local vector, rhs.c:1107-1227).  CB_HALO_WRAP (the last
+ * int ignored) is a plain copy within one buffer (DMGlobalToLocal across
+ * blocks): applied to the eddy viscosity each step and once to the uploaded
+ * state before the first step.  Destinations are non-interior nodes, each at
+ * most once per map; wrap sources may not be destinations.  CB_E_ARG on a
+ * violation. */
+#define CB_HALO_STAGE 0
+#define CB_HALO_WRAP 1
+int cb_batch_set_halo_map(cb_batch *b, int kind, long long n, const int *entries);
+int cb_batch_halo_periodic(cb_batch *b);
+/* mode 0: one persistent stage launch over all blocks per stage; mode 1: one
+ * stage launch per block (for comparison).  Asynchronous. */
+int cb_batch_rk_step(cb_batch *b, int nsteps, int mode);
+int cb_batch_sync(cb_batch *b);
+/* Times one persistent stage launch per candidate k-chunk of the work items
+ * and keeps the fastest.  The state is not advanced. */
+int cb_batch_autotune(cb_batch *b, int *best_kchunk, double *best_ms);
 
 #ifdef __cplusplus
 }
