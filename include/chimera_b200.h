@@ -19,7 +19,9 @@
  *     not thread-safe (one context per host thread, as the reference runs one
  *     rank per process).
  *   - No function allocates device memory except cb_create, cb_rhs (first
- *     call: its output planes) and cb_capture_graph (graph instantiation).
+ *     call: its output planes), cb_capture_graph (graph instantiation) and,
+ *     in the batched form, cb_batch_create, cb_batch_set_halo_map and
+ *     cb_batch_autotune (item lists, maps, graphs).
  */
 #ifndef CHIMERA_B200_H
 #define CHIMERA_B200_H
