@@ -350,6 +350,7 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.inv_ren = 1. / cfg->ren;
   d.inv_ren_half = 1. / cfg->ren * 0.5;
   d.gm1 = cfg->gamma - 1.0;
+  d.nvq = 1;  // nvert starts zero
   c->plane = (size_t)d.plane;
   // planes: 15 state + 9 metrics + aj + nvert + nut + LES filter width = 28
   const int nplanes = 28;
@@ -506,6 +507,11 @@ int cb_set_nvert(cb_ctx *c, const double *nvert) {
   int e = upload_planes(c, nvert, 1, PT_MISC + 1, false);
   if (e) return e;
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int q = nvert_codes_exact(nvert, (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz);
+  if (q != c->dc.nvq) {
+    c->dc.nvq = q;
+    invalidate_graphs(c);  // the graphs carry the config by value
+  }
   return CB_OK;
 }
 

@@ -263,6 +263,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.inv_ren = 1. / cfg->ren;
     d.inv_ren_half = 1. / cfg->ren * 0.5;
     d.gm1 = cfg->gamma - 1.0;
+    d.nvq = 1;  // nvert starts zero
     bh.off = off;
     off += (d.plane + 31) / 32 * 32;  // 256-byte aligned block starts
     bh.tiles_x = (bh.mx - 2 + SBX - 1) / SBX;
@@ -389,6 +390,11 @@ int cb_batch_set_nvert(cb_batch *b, int k, const double *nvert) {
   ghost_fill_kernel<<<bgrid(b, all), 256, 0, b->stream>>>(bh.dc, b->ptab + 25, 1);
   BCUDA(b, cudaGetLastError());
   BCUDA(b, cudaStreamSynchronize(b->stream));
+  const int q = nvert_codes_exact(nvert, nn);
+  if (q != bh.dc.nvq) {
+    bh.dc.nvq = q;
+    if (build_tables(b)) return CB_E_CUDA;  // tables and graphs carry the config
+  }
   return CB_OK;
 }
 

@@ -30,7 +30,19 @@ struct DevCfg {
   double gm1;           // gamma-1.0
   // mixed form: reference state subtracted before FP32 rounding
   double p_ref, e_ref, t_ref, h_ref;  // h_ref = e_ref + p_ref
+  // 1: every nvert value is k/4 with 0 <= k <= 255, so the stage kernel keeps
+  // nvert as one exact byte per node in shared memory; 0: read from global
+  int nvq;
 };
+
+// Host check of an nvert array for the byte code of DevCfg::nvq.
+inline int nvert_codes_exact(const double *nv, size_t n) {
+  for (size_t t = 0; t < n; t++) {
+    const double c = nv[t] * 4.0;
+    if (!(c >= 0.0 && c <= 255.0) || c != (double)(long long)c) return 0;
+  }
+  return 1;
+}
 
 struct DevFields {
   const double *q[5];      // stage input (ghosted)

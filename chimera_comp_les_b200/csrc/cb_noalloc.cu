@@ -102,6 +102,7 @@ extern "C" int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const 
   d.inv_ren = 1. / cfg->ren;
   d.inv_ren_half = 1. / cfg->ren * 0.5;
   d.gm1 = cfg->gamma - 1.0;
+  d.nvq = 0;  // nvert is a caller-owned device array: read it from global memory
 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return na_fail(CB_E_CUDA, "no current CUDA device");

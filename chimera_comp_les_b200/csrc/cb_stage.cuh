@@ -94,11 +94,24 @@ __device__ __forceinline__ NRef nshift(NRef n, int d, int s) {
 template <typename R, int BX, int BY>
 struct Ring {
   R *pl;
-  int slot[4];
+  const unsigned char *nvc;  // [4][PN] nvert * 4 (exact when DevCfg::nvq)
+  int sb;  // slot of relative plane r is (sb + r + 1) & 3: a rotation, no table
+  __device__ __forceinline__ int slot(int r) const { return (sb + r + 1) & 3; }
   __device__ __forceinline__ R get(int f, NRef n) const {
-    return pl[((slot[n.r + 1] * NF + f) * TileShape<BX, BY>::PY + n.y) * TileShape<BX, BY>::PX + n.x];
+    return pl[((slot(n.r) * NF + f) * TileShape<BX, BY>::PY + n.y) * TileShape<BX, BY>::PX + n.x];
+  }
+  __device__ __forceinline__ double nv(NRef n) const {
+    return 0.25 * (double)nvc[(slot(n.r) * TileShape<BX, BY>::PY + n.y) * TileShape<BX, BY>::PX + n.x];
   }
 };
+
+// nvert of a ring node: from shared memory when the byte code is exact, else
+// from global memory at g
+template <typename R, int BX, int BY>
+__device__ __forceinline__ double nvert_at(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef n,
+                                           long long g) {
+  return c.nvq ? Rg.nv(n) : ldg(F.nvert + g);
+}
 
 // ---------------------------------------------------------------- recon --
 template <typename R>
@@ -173,8 +186,8 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d);
   const int pos = d == 0 ? gi : (d == 1 ? gj : gk);
   const int m = d == 0 ? c.mx : (d == 1 ? c.my : c.mz);
-  const double nvm = ldg(F.nvert + g0 - sd), nv0 = ldg(F.nvert + g0), nv1 = ldg(F.nvert + g0 + sd),
-               nv2 = ldg(F.nvert + g0 + 2 * sd);
+  const double nvm = nvert_at(c, F, Rg, nshift(a, d, -1), g0 - sd), nv0 = nvert_at(c, F, Rg, a, g0),
+               nv1 = nvert_at(c, F, Rg, nshift(a, d, 1), g0 + sd), nv2 = nvert_at(c, F, Rg, nshift(a, d, 2), g0 + 2 * sd);
   const R *met[3] = {met_ptr<R>(F, d, 0), met_ptr<R>(F, d, 1), met_ptr<R>(F, d, 2)};
   R h[3];
 #pragma unroll
@@ -343,9 +356,9 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
       continue;
     }
     const long long te = gstride(c, e);
-    const bool plus_blocked = blocked(ldg(F.nvert + g0 + te)) || blocked(ldg(F.nvert + g1 + te));
-    const bool minus_blocked = blocked(ldg(F.nvert + g0 - te)) || blocked(ldg(F.nvert + g1 - te));
     const NRef ap = nshift(a, e, 1), am = nshift(a, e, -1), bp = nshift(b, e, 1), bm = nshift(b, e, -1);
+    const bool plus_blocked = blocked(nvert_at(c, F, Rg, ap, g0 + te)) || blocked(nvert_at(c, F, Rg, bp, g1 + te));
+    const bool minus_blocked = blocked(nvert_at(c, F, Rg, am, g0 - te)) || blocked(nvert_at(c, F, Rg, bm, g1 - te));
 #pragma unroll
     for (int f = 0; f < 4; f++) {
       const int fi = F_U + f;
@@ -466,8 +479,10 @@ constexpr int S_NZF = SBX * SBY;   // 224
 template <typename R, bool MIX>
 struct StageSmem {
   static constexpr int NG = FaceWidth<MIX>::NG;
+  // ring + face buffers, FP64 staging of the next plane (5 state fields + nvert),
+  // nvert byte ring [4][PN]
   static constexpr size_t bytes = sizeof(R) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF)) +
-                                  sizeof(double) * (size_t)5 * STile::PN;
+                                  sizeof(double) * (size_t)6 * STile::PN + (size_t)4 * STile::PN;
 };
 constexpr size_t STAGE_SMEM_BYTES = StageSmem<double, false>::bytes;
 constexpr size_t STAGE_SMEM_BYTES_MIXED = StageSmem<float, true>::bytes;
@@ -489,13 +504,16 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
                                            double alfa, double beta, double adt, int kchunk, double *smem_d) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
   constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
-  double *stg = smem_d;  // [5][PN] raw FP64 Q of the next plane
-  R *smem = reinterpret_cast<R *>(smem_d + (size_t)5 * PN);
+  double *stg = smem_d;  // [6][PN] raw FP64 Q and nvert of the next plane
+  R *smem = reinterpret_cast<R *>(smem_d + (size_t)6 * PN);
   Ring<R, BX, BY> Rg;
   Rg.pl = smem;
   R *gxb = smem + (size_t)4 * NF * PN;  // [NG][S_NXF]
   R *gyb = gxb + (size_t)NG * S_NXF;    // [NG][S_NYF]
   R *gzb = gyb + (size_t)NG * S_NYF;    // [NG][S_NZF]
+  unsigned char *nvc = reinterpret_cast<unsigned char *>(gzb + (size_t)NG * S_NZF);  // [4][PN]
+  Rg.nvc = nvc;
+  const int nstg = c.nvq ? 6 : 5;  // staged fields per plane
 
   const int tid = threadIdx.x;
   const int i0 = 1 + bxi * BX, j0 = 1 + byi * BY;
@@ -508,12 +526,13 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 
   // async copy of the raw state of plane kk (with its halo) into the staging buffer
   auto issue_stage = [&](int kk) {
-    for (int e = tid; e < 5 * PN; e += NT) {
+    for (int e = tid; e < nstg * PN; e += NT) {
       const int q = e / PN, idx = e - q * PN;
       const int lx = idx % PX, ly = idx / PX;
       const int xi = i0 - 2 + lx, yj = j0 - 2 + ly;
       const bool ok = xi <= c.mx + 1 && yj <= c.my + 1 && kk >= -2 && kk <= c.mz + 1;
-      const double *src = ok ? F.q[q] + gidx(c, xi, yj, kk) : F.q[q];
+      const double *base = q < 5 ? F.q[q] : F.nvert;
+      const double *src = ok ? base + gidx(c, xi, yj, kk) : base;
       cp_async8(stg + e, src, ok);
     }
     cp_async_commit();
@@ -544,6 +563,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       R *base = Rg.pl + (size_t)s * NF * PN + idx;
 #pragma unroll
       for (int q = 0; q < NF; q++) base[(size_t)q * PN] = R(v[q]);
+      if (nstg == 6) nvc[s * PN + idx] = (unsigned char)(stg[5 * PN + idx] * 4.0);
     }
   };
   auto load_plane_sync = [&](int kk, int s) {
@@ -613,7 +633,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   };
 
   // prologue: planes kb-2 .. kb+1 in slots 0..3, k-face kb-1/2, then kb+2
-  Rg.slot[0] = 0; Rg.slot[1] = 1; Rg.slot[2] = 2; Rg.slot[3] = 3;
+  Rg.sb = 0;
   load_plane_sync(kb - 2, 0);
   load_plane_sync(kb - 1, 1);
   load_plane_sync(kb, 2);
@@ -628,7 +648,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   int base = 1;  // slot of plane k-1
 
   for (int k = kb; k < ke; k++) {
-    Rg.slot[0] = base & 3; Rg.slot[1] = (base + 1) & 3; Rg.slot[2] = (base + 2) & 3; Rg.slot[3] = (base + 3) & 3;
+    Rg.sb = base;
     const bool more = k + 1 < ke;
     if (more) issue_stage(k + 3);  // overlaps the face computation
     faces(k, false);
@@ -640,7 +660,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 
     if (uact) {
       const long long g = gidx(c, ugi, ugj, k);
-      const double nv = ldg(F.nvert + g);
+      const double nv = nvert_at(c, F, Rg, n, g);
       const int fxr = uty * (BX + 1) + utx + 1, fxl = fxr - 1;   // i+1/2, i-1/2
       const int fyu = (uty + 1) * BX + utx, fyd = uty * BX + utx;  // j+1/2, j-1/2
       const int fz = tid;                                          // k+1/2 (k-1/2 in Gzp)

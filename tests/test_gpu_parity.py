@@ -65,19 +65,28 @@ ORACLE_CASES = [
     ("les_visc_weno_mask", (33, 17, 23), dict(les=1, inviscid=0, fluxorder=3, s_x=0.2, s_y=0.5, s_z=0.9, ren=500., ma=0.3, pr=0.71, dt=0.002), True),
     ("std_visc_weno_mask", (35, 41, 20), dict(les=0, inviscid=0, fluxorder=3, ren=500., ma=0.3, pr=0.71, dt=0.002), True),
     ("std_inv_muscl", (40, 12, 31), dict(les=0, inviscid=1, fluxorder=2, dt=0.002), False),
+    # nvert values that are not multiples of 1/4: the kernel reads nvert from
+    # global memory instead of its shared-memory byte code
+    ("les_visc_weno_mask_offgrid", (33, 17, 23), dict(les=1, inviscid=0, fluxorder=3, ren=500., ma=0.3, pr=0.71, dt=0.002), "offgrid"),
+    ("std_visc_weno_mask_offgrid", (35, 21, 20), dict(les=0, inviscid=0, fluxorder=3, ren=500., ma=0.3, pr=0.71, dt=0.002), "offgrid"),
+    # multiples of 1/4 around every threshold (0.1, 0.5, 2.9, 7): byte-code path
+    ("les_visc_weno_mask_quarters", (33, 17, 23), dict(les=1, inviscid=0, fluxorder=3, ren=500., ma=0.3, pr=0.71, dt=0.002), "quarters"),
 ]
 
 
-def _mask(shape, seed):
+def _mask(shape, seed, kind=True):
+    """Three spheres: band 1 / solid 3 (the reference's IBM encoding), or with
+    "offgrid" values 0.3 / 0.6 / 2.95 / 7.3 and "quarters" 0.25 / 0.75 / 3.0 / 7.25."""
     rng = np.random.default_rng(seed)
     mz, my, mx = shape
     z, y, x = np.meshgrid(np.arange(mz), np.arange(my), np.arange(mx), indexing="ij")
+    vals = {True: (1.0, 1.0, 3.0, 3.0), "offgrid": (0.3, 0.6, 2.95, 7.3), "quarters": (0.25, 0.75, 3.0, 7.25)}[kind]
     nv = np.zeros(shape)
     for _ in range(3):
         c = rng.uniform(4, np.array([mx, my, mz]) - 4)
         r = np.sqrt((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2)
-        nv[r < 3.0] = np.maximum(nv[r < 3.0], 1.0)
-        nv[r < 1.9] = 3.0
+        for rad, v in zip((3.2, 2.6, 1.9, 1.2), vals):
+            nv[r < rad] = np.maximum(nv[r < rad], v)
     return nv
 
 
@@ -87,7 +96,7 @@ def test_rhs_and_steps_match_oracle(name, n, kw, mask):
     shape = coords.shape[:3]
     cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, **kw)
     q = W.random_smooth_state(shape, seed=11)
-    nv = _mask(shape, 5) if mask else np.zeros(shape)
+    nv = _mask(shape, 5, mask) if mask else np.zeros(shape)
     ref = oracle_run(cfg, coords, q, nv, steps=2)
     with _setup(cfg, coords, q, nv) as b:
         if cfg.les and not cfg.inviscid:
