@@ -46,12 +46,11 @@ struct cb_ctx {
   double *met[3][3] = {};
   double *aj = nullptr, *nvert = nullptr, *nut = nullptr, *delta2 = nullptr;
   double *rhsb[5] = {};
-  // mixed form: FP32 metric copies, FP32 filter width, FP64 metric divergence
+  // mixed form: FP32 metric vectors (with filter width and aj), FP64 metric divergence
   void *arena_mixed = nullptr;
-  float *met32[3][3] = {};
-  float *delta2_32 = nullptr;
+  float4 *met4[3] = {};
   double *gcl[3] = {};
-  float **ptab32 = nullptr;
+  float4 **ptab4 = nullptr;
   bool have_refs = false;
   double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
   double **ptab = nullptr;    // device pointer tables
@@ -107,9 +106,7 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
   F.nvert = c->nvert;
   F.nut = c->nut;
   F.delta2 = c->delta2;
-  for (int e = 0; e < 3; e++)
-    for (int q = 0; q < 3; q++) F.met32[e][q] = c->met32[e][q];
-  F.delta2_32 = c->delta2_32;
+  for (int e = 0; e < 3; e++) F.met4[e] = c->met4[e];
   for (int a = 0; a < 3; a++) F.gcl[a] = c->gcl[a];
   F.status = c->status;
   return F;
@@ -278,13 +275,7 @@ static int fill_ptab(cb_ctx *c) {
   h[PT_MISC + 11] = c->aj;
   for (int a = 0; a < 3; a++) h[PT_GCL + a] = c->gcl[a];
   CB_CUDA(c, cudaMemcpyAsync(c->ptab, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
-  if (c->ptab32) {
-    float *h32[16] = {};
-    for (int e = 0; e < 3; e++)
-      for (int q = 0; q < 3; q++) h32[3 * e + q] = c->met32[e][q];
-    h32[9] = c->delta2_32;
-    CB_CUDA(c, cudaMemcpyAsync(c->ptab32, h32, sizeof(h32), cudaMemcpyHostToDevice, c->stream));
-  }
+  if (c->ptab4) CB_CUDA(c, cudaMemcpyAsync(c->ptab4, c->met4, sizeof(c->met4), cudaMemcpyHostToDevice, c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
   return CB_OK;
 }
@@ -369,16 +360,14 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   const size_t nn = (size_t)cfg->mx * cfg->my * cfg->mz;
   if (cudaMalloc(&c->staging, sizeof(double) * 5 * nn) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc staging");
   if (cfg->precision == CB_MIXED) {
-    const size_t mbytes = sizeof(float) * c->plane * 10 + sizeof(double) * c->plane * 3;
+    const size_t mbytes = sizeof(float4) * c->plane * 3 + sizeof(double) * c->plane * 3;
     if (cudaMalloc(&c->arena_mixed, mbytes) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc mixed planes");
     if (cudaMemsetAsync(c->arena_mixed, 0, mbytes, c->stream) != cudaSuccess) return bail(CB_E_CUDA, "memset");
-    float *f = (float *)c->arena_mixed;
-    for (int e = 0; e < 3; e++)
-      for (int q = 0; q < 3; q++) c->met32[e][q] = f + c->plane * (3 * e + q);
-    c->delta2_32 = f + c->plane * 9;
-    double *g = (double *)(f + c->plane * 10);
+    float4 *f = (float4 *)c->arena_mixed;
+    for (int e = 0; e < 3; e++) c->met4[e] = f + c->plane * e;
+    double *g = (double *)(f + c->plane * 3);
     for (int a = 0; a < 3; a++) c->gcl[a] = g + c->plane * a;
-    if (cudaMalloc(&c->ptab32, sizeof(float *) * 16) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab32");
+    if (cudaMalloc(&c->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab4");
   }
   if (cudaMalloc(&c->ptab, sizeof(double *) * PT_N) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab");
   if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc status");
@@ -410,7 +399,7 @@ void cb_destroy(cb_ctx *c) {
   if (c->arena) cudaFree(c->arena);
   if (c->staging) cudaFree(c->staging);
   if (c->arena_mixed) cudaFree(c->arena_mixed);
-  if (c->ptab32) cudaFree(c->ptab32);
+  if (c->ptab4) cudaFree(c->ptab4);
   if (c->ptab) cudaFree(c->ptab);
   if (c->status) cudaFree(c->status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -457,7 +446,7 @@ int cb_set_grid(cb_ctx *c, const double *coor) {
   delta2_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->aj, c->delta2);
   CB_CUDA(c, cudaGetLastError());
   if (c->cfg.precision == CB_MIXED)
-    CB_CUDA(c, launch_mixed_prep(c->dc, (const double *const *)(c->ptab + PT_MET), c->delta2, c->ptab32, c->delta2_32,
+    CB_CUDA(c, launch_mixed_prep(c->dc, (const double *const *)(c->ptab + PT_MET), c->delta2, c->aj, c->ptab4,
                                  c->ptab + PT_GCL, grid_for(c, (long long)c->plane), c->stream));
   // scrub buffer 2 (coordinates) so later ghost reads see zeros until written
   for (int q = 0; q < 3; q++) CB_CUDA(c, cudaMemsetAsync(X[q], 0, sizeof(double) * c->plane, c->stream));
@@ -478,7 +467,7 @@ int cb_set_metrics(cb_ctx *c, const double *csi, const double *eta, const double
   delta2_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->aj, c->delta2);
   CB_CUDA(c, cudaGetLastError());
   if (c->cfg.precision == CB_MIXED)
-    CB_CUDA(c, launch_mixed_prep(c->dc, (const double *const *)(c->ptab + PT_MET), c->delta2, c->ptab32, c->delta2_32,
+    CB_CUDA(c, launch_mixed_prep(c->dc, (const double *const *)(c->ptab + PT_MET), c->delta2, c->aj, c->ptab4,
                                  c->ptab + PT_GCL, grid_for(c, (long long)c->plane), c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_grid = true;

@@ -80,12 +80,11 @@ struct cb_batch {
   double *met[3][3] = {};
   double *aj = nullptr, *nvert = nullptr, *nut = nullptr, *delta2 = nullptr;
   void *arena_mixed = nullptr;
-  float *met32[3][3] = {};
-  float *delta2_32 = nullptr;
+  float4 *met4[3] = {};
   double *gcl[3] = {};
   double *staging = nullptr;  // AoS host transfer buffer, sized for the largest block
   double **ptab = nullptr;    // per-block pointer tables for the set-up kernels
-  float **ptab32 = nullptr;
+  float4 **ptab4 = nullptr;
   // batched launch data
   BatchBlock *d_tables = nullptr;  // [27][nb] indexed by (in, old, out) buffer triple
   int2 *d_items = nullptr;
@@ -137,16 +136,14 @@ static DevFields block_fields(const cb_batch *b, int blk, int in, int old, int o
     F.qout[q] = out >= 0 ? b->qb[out][q] + o : nullptr;
     F.rhs[q] = nullptr;
   }
-  for (int e = 0; e < 3; e++)
-    for (int q = 0; q < 3; q++) {
-      F.met[e][q] = b->met[e][q] + o;
-      F.met32[e][q] = b->met32[e][q] ? b->met32[e][q] + o : nullptr;
-    }
+  for (int e = 0; e < 3; e++) {
+    for (int q = 0; q < 3; q++) F.met[e][q] = b->met[e][q] + o;
+    F.met4[e] = b->met4[e] ? b->met4[e] + o : nullptr;
+  }
   F.aj = b->aj + o;
   F.nvert = b->nvert + o;
   F.nut = b->nut + o;
   F.delta2 = b->delta2 + o;
-  F.delta2_32 = b->delta2_32 ? b->delta2_32 + o : nullptr;
   for (int a = 0; a < 3; a++) F.gcl[a] = b->gcl[a] ? b->gcl[a] + o : nullptr;
   F.status = b->status;
   return F;
@@ -211,12 +208,9 @@ static int block_ptab(cb_batch *b, int k) {
   h[26] = b->nut + o;
   for (int a = 0; a < 3; a++) h[27 + a] = b->gcl[a] ? b->gcl[a] + o : nullptr;
   BCUDA(b, cudaMemcpyAsync(b->ptab, h, sizeof(h), cudaMemcpyHostToDevice, b->stream));
-  if (b->ptab32) {
-    float *h32[16] = {};
-    for (int e = 0; e < 3; e++)
-      for (int q = 0; q < 3; q++) h32[3 * e + q] = b->met32[e][q] + o;
-    h32[9] = b->delta2_32 + o;
-    BCUDA(b, cudaMemcpyAsync(b->ptab32, h32, sizeof(h32), cudaMemcpyHostToDevice, b->stream));
+  if (b->ptab4) {
+    float4 *h4[3] = {b->met4[0] + o, b->met4[1] + o, b->met4[2] + o};
+    BCUDA(b, cudaMemcpyAsync(b->ptab4, h4, sizeof(h4), cudaMemcpyHostToDevice, b->stream));
   }
   BCUDA(b, cudaStreamSynchronize(b->stream));
   return CB_OK;
@@ -285,16 +279,14 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
   b->nut = b->arena + (size_t)b->total * (p++);
   b->delta2 = b->arena + (size_t)b->total * (p++);
   if (cfg->precision == CB_MIXED) {
-    const size_t mb = sizeof(float) * (size_t)b->total * 10 + sizeof(double) * (size_t)b->total * 3;
+    const size_t mb = sizeof(float4) * (size_t)b->total * 3 + sizeof(double) * (size_t)b->total * 3;
     if (cudaMalloc(&b->arena_mixed, mb) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc mixed");
     cudaMemsetAsync(b->arena_mixed, 0, mb, b->stream);
-    float *f = (float *)b->arena_mixed;
-    for (int e = 0; e < 3; e++)
-      for (int q = 0; q < 3; q++) b->met32[e][q] = f + (size_t)b->total * (3 * e + q);
-    b->delta2_32 = f + (size_t)b->total * 9;
-    double *g = (double *)(f + (size_t)b->total * 10);
+    float4 *f = (float4 *)b->arena_mixed;
+    for (int e = 0; e < 3; e++) b->met4[e] = f + (size_t)b->total * e;
+    double *g = (double *)(f + (size_t)b->total * 3);
     for (int a = 0; a < 3; a++) b->gcl[a] = g + (size_t)b->total * a;
-    if (cudaMalloc(&b->ptab32, sizeof(float *) * 16) != cudaSuccess) return bail(CB_E_CUDA, "ptab32");
+    if (cudaMalloc(&b->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "ptab4");
     if (set_stage_attrs_mixed() != cudaSuccess || set_batched_attrs_mixed() != cudaSuccess)
       return bail(CB_E_CUDA, "mixed kernel attributes");
   }
@@ -329,7 +321,7 @@ void cb_batch_destroy(cb_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
   destroy_graphs(b);
-  void *ptrs[] = {b->arena, b->arena_mixed, b->staging, b->ptab, b->ptab32, b->d_tables, b->d_items, b->d_counter,
+  void *ptrs[] = {b->arena, b->arena_mixed, b->staging, b->ptab, b->ptab4, b->d_tables, b->d_items, b->d_counter,
                   b->status, b->d_hdst, b->d_hsrc, b->d_hin, b->d_wdst, b->d_wsrc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -370,8 +362,8 @@ int cb_batch_set_grid(cb_batch *b, int k, const double *coor) {
   delta2_kernel<<<bgrid(b, d.plane), 256, 0, b->stream>>>(d, b->aj + bh.off, b->delta2 + bh.off);
   BCUDA(b, cudaGetLastError());
   if (b->cfg.precision == CB_MIXED)
-    BCUDA(b, launch_mixed_prep(d, (const double *const *)(b->ptab + 15), b->delta2 + bh.off, b->ptab32,
-                               b->delta2_32 + bh.off, b->ptab + 27, bgrid(b, d.plane), b->stream));
+    BCUDA(b, launch_mixed_prep(d, (const double *const *)(b->ptab + 15), b->delta2 + bh.off, b->aj + bh.off, b->ptab4,
+                               b->ptab + 27, bgrid(b, d.plane), b->stream));
   for (int q = 0; q < 3; q++) BCUDA(b, cudaMemsetAsync(b->qb[2][q] + bh.off, 0, sizeof(double) * d.plane, b->stream));
   BCUDA(b, cudaStreamSynchronize(b->stream));
   bh.have_grid = true;

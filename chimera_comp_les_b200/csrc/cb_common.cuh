@@ -53,8 +53,9 @@ struct DevFields {
   const double *nvert;
   const double *nut;
   const double *delta2;    // LES filter width squared, pow(pow(1/aj,1/3),2), per node
-  const float *met32[3][3];  // mixed form: FP32 copies of the metrics
-  const float *delta2_32;    // mixed form: FP32 copy of delta2
+  // mixed form: FP32 metric vectors, one 16-byte load per node and direction;
+  // w carries the FP32 filter width (csi), aj (eta), 0 (zet)
+  const float4 *met4[3];
   const double *gcl[3];      // mixed form: per-node metric divergence sum_d dh_d (FP64)
   double *rhs[5];          // formRHS output (rhs mode only)
   unsigned *status;        // sticky status word

@@ -20,13 +20,14 @@ void launch1(const DevCfg &c, const DevFields &F, int istage, double alfa, doubl
   stage_kernel<float, true, LES, VISC, RHSM><<<grid, SNT, STAGE_SMEM_BYTES_MIXED, s>>>(c, F, istage, alfa, beta, adt, kchunk);
 }
 
-__global__ void mixed_prep_kernel(const DevCfg c, const double *const *met, const double *delta2, float *const *met32,
-                                  float *delta2_32, double *const *gcl) {
+__global__ void mixed_prep_kernel(const DevCfg c, const double *const *met, const double *delta2, const double *aj,
+                                  float4 *const *met4, double *const *gcl) {
   const long long total = (long long)c.px * c.py * c.pz;
   const long long nx = c.px, ny = c.py;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    for (int q = 0; q < 9; q++) met32[q][t] = (float)met[q][t];
-    delta2_32[t] = (float)delta2[t];
+    const float w[3] = {(float)delta2[t], (float)aj[t], 0.f};
+    for (int e = 0; e < 3; e++)
+      met4[e][t] = make_float4((float)met[3 * e][t], (float)met[3 * e + 1][t], (float)met[3 * e + 2][t], w[e]);
     const int i = (int)(t % nx) - 2, j = (int)((t / nx) % ny) - 2, k = (int)(t / (nx * ny)) - 2;
     const bool interior = i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2;
     for (int a = 0; a < 3; a++) {
@@ -103,9 +104,9 @@ cudaError_t launch_batched_mixed(const BatchBlock *tab, const int2 *items, int n
   return cudaGetLastError();
 }
 
-cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, float *const *met32,
-                              float *delta2_32, double *const *gcl, int grid, cudaStream_t s) {
-  mixed_prep_kernel<<<grid, 256, 0, s>>>(c, met, delta2, met32, delta2_32, gcl);
+cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, const double *aj,
+                              float4 *const *met4, double *const *gcl, int grid, cudaStream_t s) {
+  mixed_prep_kernel<<<grid, 256, 0, s>>>(c, met, delta2, aj, met4, gcl);
   return cudaGetLastError();
 }
 

@@ -64,18 +64,30 @@ template <>
 __device__ __forceinline__ const double *met_ptr<double>(const DevFields &F, int d, int q) {
   return d == 0 ? F.met[0][q] : (d == 1 ? F.met[1][q] : F.met[2][q]);
 }
-template <>
-__device__ __forceinline__ const float *met_ptr<float>(const DevFields &F, int d, int q) {
-  return d == 0 ? F.met32[0][q] : (d == 1 ? F.met32[1][q] : F.met32[2][q]);
-}
-template <typename R>
-__device__ __forceinline__ const R *met_ptr_e(const DevFields &F, int e, int q);
-template <>
-__device__ __forceinline__ const double *met_ptr_e<double>(const DevFields &F, int e, int q) { return F.met[e][q]; }
-template <>
-__device__ __forceinline__ const float *met_ptr_e<float>(const DevFields &F, int e, int q) { return F.met32[e][q]; }
+
 template <typename R>
 __device__ __forceinline__ R ldr(const R *p) { return __ldg(p); }
+
+// Metric vector of direction e at node g in the form's arithmetic type; w is
+// the mixed form's companion value (FP32 filter width for e = 0, aj for e = 1).
+template <typename R>
+struct MetV {
+  R x, y, z, w;
+};
+template <typename R, bool MIX>
+__device__ __forceinline__ MetV<R> met_load(const DevFields &F, int e, long long g) {
+  MetV<R> r;
+  if constexpr (MIX) {
+    const float4 v = __ldg((e == 0 ? F.met4[0] : (e == 1 ? F.met4[1] : F.met4[2])) + g);
+    r.x = v.x; r.y = v.y; r.z = v.z; r.w = v.w;
+  } else {
+    r.x = ldg(met_ptr<double>(F, e, 0) + g);
+    r.y = ldg(met_ptr<double>(F, e, 1) + g);
+    r.z = ldg(met_ptr<double>(F, e, 2) + g);
+    r.w = 0.;
+  }
+  return r;
+}
 
 __device__ __forceinline__ int bc_lo(const DevCfg &c, int d) { return d == 0 ? c.bctype[0] : (d == 1 ? c.bctype[2] : c.bctype[4]); }
 __device__ __forceinline__ int bc_hi(const DevCfg &c, int d) { return d == 0 ? c.bctype[1] : (d == 1 ? c.bctype[3] : c.bctype[5]); }
@@ -192,10 +204,11 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   const int m = d == 0 ? c.mx : (d == 1 ? c.my : c.mz);
   const double nvm = nvert_at(c, F, Rg, nshift(a, d, -1), g0 - sd), nv0 = nvert_at(c, F, Rg, a, g0),
                nv1 = nvert_at(c, F, Rg, nshift(a, d, 1), g0 + sd), nv2 = nvert_at(c, F, Rg, nshift(a, d, 2), g0 + 2 * sd);
-  const R *met[3] = {met_ptr<R>(F, d, 0), met_ptr<R>(F, d, 1), met_ptr<R>(F, d, 2)};
+  const MetV<R> m0 = met_load<R, MIX>(F, d, g0), m1 = met_load<R, MIX>(F, d, g0 + sd);
   R h[3];
-#pragma unroll
-  for (int q = 0; q < 3; q++) h[q] = R(0.5) * (ldr(met[q] + g0) + ldr(met[q] + g0 + sd));
+  h[0] = R(0.5) * (m0.x + m1.x);
+  h[1] = R(0.5) * (m0.y + m1.y);
+  h[2] = R(0.5) * (m0.z + m1.z);
   const R pref = R(c.p_ref), href = R(c.h_ref);
 
   // stencil values along d: s=0..3 -> node offsets -1..2
@@ -298,8 +311,8 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
     R U[4], EP[4];
 #pragma unroll
     for (int s = 0; s < 4; s++) {
-      const long long gs = g0 + (s - 1) * sd;
-      U[s] = R(1.) / Q[s][0] * (ldr(met[0] + gs) * Q[s][1] + ldr(met[1] + gs) * Q[s][2] + ldr(met[2] + gs) * Q[s][3]);
+      const MetV<R> ms = s == 1 ? m0 : (s == 2 ? m1 : met_load<R, MIX>(F, d, g0 + (s - 1) * sd));
+      U[s] = R(1.) / Q[s][0] * (ms.x * Q[s][1] + ms.y * Q[s][2] + ms.z * Q[s][3]);
       EP[s] = P[s] + Q[s][4];
     }
     const R fp4 = R(1.0) / R(12.0) * (-P[0] + R(7) * P[1] + R(7) * P[2] - P[3]);
@@ -385,10 +398,15 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   const R dpdc = D[3][0], dpde = D[3][1], dpdz = D[3][2];
 
   R mh[3][3];
+  R w0[2], w1[2];  // mixed form: filter width and aj at g0 / g1
 #pragma unroll
-  for (int e = 0; e < 3; e++)
-#pragma unroll
-    for (int q = 0; q < 3; q++) mh[e][q] = R(0.5) * (ldr(met_ptr_e<R>(F, e, q) + g0) + ldr(met_ptr_e<R>(F, e, q) + g1));
+  for (int e = 0; e < 3; e++) {
+    const MetV<R> p0 = met_load<R, MIX>(F, e, g0), p1 = met_load<R, MIX>(F, e, g1);
+    mh[e][0] = R(0.5) * (p0.x + p1.x);
+    mh[e][1] = R(0.5) * (p0.y + p1.y);
+    mh[e][2] = R(0.5) * (p0.z + p1.z);
+    if (e < 2) { w0[e] = p0.w; w1[e] = p1.w; }
+  }
   const R md0 = d == 0 ? mh[0][0] : (d == 1 ? mh[1][0] : mh[2][0]);
   const R md1 = d == 0 ? mh[0][1] : (d == 1 ? mh[1][1] : mh[2][1]);
   const R md2 = d == 0 ? mh[0][2] : (d == 1 ? mh[1][2] : mh[2][2]);
@@ -409,7 +427,7 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   const R r23 = dvdc * csi2 + dvde * eta2 + dvdz * zet2;
   const R r33 = dwdc * csi2 + dwde * eta2 + dwdz * zet2;
 
-  const R ajc = R(0.5) * (R(ldg(F.aj + g0)) + R(ldg(F.aj + g1)));
+  const R ajc = MIX ? R(0.5) * (w0[1] + w1[1]) : R(0.5) * (R(ldg(F.aj + g0)) + R(ldg(F.aj + g1)));
   R nu = R(c.inv_ren);  // 1./ren (evaluated once on the host, same value)
   if (LES) {
     // quirk: eta/zeta faces average rho over i and i+1 (rhs.c:1835, 2034)
@@ -459,7 +477,7 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
     const R S2 = R(.5) * ((r11 - div) * (r11 - div) + r12 * r12 + r13 * r13 + r21 * r21 + (r22 - div) * (r22 - div) +
                           r23 * r23 + r31 * r31 + r32 * r32 + (r33 - div) * (r33 - div));
     // pow(pow(1/aj, 1/3), 2) of the left node, precomputed once per node
-    const R pf = MIX ? R(ldr(F.delta2_32 + g0)) : R(ldg(F.delta2 + g0));
+    const R pf = MIX ? w0[0] : R(ldg(F.delta2 + g0));
     const R sgs = -S2 * pf * R(c.ci) * R(2.0) / R(3.0);
     A[0] = tx + sgs * md0 * rho_c * sigma_c;
     A[1] = ty + sgs * md1 * rho_c * sigma_c;
