@@ -213,8 +213,7 @@ static int nut_update(cb_ctx *c) {
   }
   {
     TimedScope ts(c, false);
-    const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
-    ghost_fill_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->ptab + PT_NUT, 1);
+    ghost_fill_kernel<<<grid_for(c, shell_count(c->dc)), 256, 0, c->stream>>>(c->dc, c->ptab + PT_NUT, 1);
   }
   CB_CUDA(c, cudaGetLastError());
   return CB_OK;
@@ -237,7 +236,7 @@ static int enqueue_step(cb_ctx *c) {
   const int old = c->cur;
   const int A = (c->cur + 1) % 3, B = (c->cur + 2) % 3;
   int in = c->cur;
-  const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
+  const long long shell = shell_count(c->dc);
   for (int s = 0; s < ns; s++) {
     const int out = (s % 2 == 0) ? A : B;
     double alfa, beta;
@@ -250,7 +249,7 @@ static int enqueue_step(cb_ctx *c) {
     }
     {
       TimedScope ts(c, false);
-      bc_periodic_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, F);
+      bc_periodic_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, F);
     }
     CB_CUDA(c, cudaGetLastError());
     if (!c->cfg.inviscid) c->uc = in;  // CalcUCat inside formRHS keeps the stage input

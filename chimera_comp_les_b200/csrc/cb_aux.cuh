@@ -30,12 +30,47 @@ __device__ __forceinline__ void bc_source(const DevCfg &c, int i, int j, int k, 
   else si = oi + 2;  // oi == mx-1
 }
 
+// The non-interior nodes of the padded box (three layers on each side: two
+// ghost layers and the boundary layer), enumerated without the interior: six
+// full planes, then per middle plane six full rows and six side nodes per
+// middle row.
+__host__ __device__ __forceinline__ long long shell_count(const DevCfg &c) {
+  const long long NX = c.mx + 4, NY = c.my + 4;
+  return 6 * NX * NY + (long long)(c.mz - 2) * (6 * NX + 6 * (c.my - 2));
+}
+__device__ __forceinline__ void shell_node(const DevCfg &c, long long t, int &i, int &j, int &k) {
+  const long long NX = c.mx + 4, NY = c.my + 4, NZ = c.mz + 4, A = NX * NY, Pm = 6 * NX + 6 * (c.my - 2);
+  long long I, J, K;
+  if (t < 6 * A) {
+    const long long p = t / A, r = t - p * A;
+    K = p < 3 ? p : NZ - 6 + p;
+    J = r / NX;
+    I = r - J * NX;
+  } else {
+    const long long t2 = t - 6 * A;
+    K = 3 + t2 / Pm;
+    const long long r = t2 - (K - 3) * Pm;
+    if (r < 6 * NX) {
+      const long long q = r / NX;
+      J = q < 3 ? q : NY - 6 + q;
+      I = r - q * NX;
+    } else {
+      const long long r2 = r - 6 * NX, cc = r2 % 6;
+      J = 3 + r2 / 6;
+      I = cc < 3 ? cc : NX - 6 + cc;
+    }
+  }
+  i = (int)I - 2;
+  j = (int)J - 2;
+  k = (int)K - 2;
+}
+
 // Writes every non-interior node (boundary layer + both ghost layers) of qout.
 static __global__ void bc_periodic_kernel(const DevCfg c, DevFields F) {
-  const long long nx = c.mx + 4, ny = c.my + 4, nz = c.mz + 4, total = nx * ny * nz;
+  const long long total = shell_count(c);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % nx) - 2, j = (int)((t / nx) % ny) - 2, k = (int)(t / (nx * ny)) - 2;
-    if (i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2) continue;
+    int i, j, k;
+    shell_node(c, t, i, j, k);
     int si, sj, sk;
     bool from_in;
     bc_source(c, i, j, k, si, sj, sk, from_in);
@@ -47,9 +82,10 @@ static __global__ void bc_periodic_kernel(const DevCfg c, DevFields F) {
 
 // Ghost layers of periodic planes from their owned images (DMGlobalToLocal).
 static __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, int nplanes) {
-  const long long nx = c.mx + 4, ny = c.my + 4, nz = c.mz + 4, total = nx * ny * nz;
+  const long long total = shell_count(c);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % nx) - 2, j = (int)((t / nx) % ny) - 2, k = (int)(t / (nx * ny)) - 2;
+    int i, j, k;
+    shell_node(c, t, i, j, k);
     const bool gi = i < 0 || i >= c.mx, gj = j < 0 || j >= c.my, gk = k < 0 || k >= c.mz;
     if (!(gi || gj || gk)) continue;
     const bool pi = c.bctype[0] == 7, pj = c.bctype[2] == 7, pk = c.bctype[4] == 7;
