@@ -438,6 +438,118 @@ def run_ours(args, ws, rank, local):
         b.close()
 
 
+# ------------------------------------------------------- sharded (N > 1) --
+def run_sharded(args, ws, rank, local):
+    """k-slab decomposition of one periodic TGV box of 128 x 128 x 128N unique
+    nodes over N GPUs, one 128^3 slab (DMDA 130^3) per rank: every RK stage
+    exchanges the slabs' two-node halos (and the eddy viscosity's once per
+    step) with the neighbours through NCCL point-to-point on the library's
+    stream.  Weak scaling: per-GPU work equals the N = 1 workload."""
+    import torch
+
+    from chimera_comp_les_b200 import batch as B
+    from chimera_comp_les_b200 import sharded as S
+    from chimera_comp_les_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    n = N_UNIQUE
+    gn = (n, n, n * ws)
+    glen = (2 * math.pi, 2 * math.pi, 2 * math.pi * ws)
+    M = (n + 2, n + 2, n * ws + 2)
+    parts = B.decompose(M, [[n], [n], [n] * ws])
+    rob = S.slab_ranks(len(parts), ws)
+    near = {(rank - 1) % ws, rank, (rank + 1) % ws}
+    st, wr = B.halo_maps_decomposed(M, parts, only=near)
+    plan = S.exchange_plan(st, wr, rob, rank)
+    (b,) = plan.blocks
+    off, d = parts[b]
+    coords = W.periodic_grid_slab(gn, glen, 0.05, off[2], d[2])
+    q0 = W.tgv_state(coords, gamma=CFG["gamma"], ma=CFG["ma"])
+    prec = args.precision
+    bt = B.Batch([d], precision=prec, device=local, **CFG)
+    bt.FormMetrics(0, coords)
+    bt.SetInitialCondition(0, q0)
+    sh = S.Shard(bt, plan, torch.device("cuda", local))
+    tr = S.DistTransport()
+    S.fill_ghosts_all([sh], tr)
+    S.step_all([sh], tr, max(args.warmup, 3))
+    stream = torch.cuda.ExternalStream(bt.stream, device=f"cuda:{local}")
+    sampler = ClockSampler(gpu_identifier(local)) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    S.step_all([sh], tr, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = sampler.stop() if sampler else None
+    bt.sync()
+    ms = max_over_ranks(e0.elapsed_time(e1), ws, local)
+    interior, stages = bt.interior_nodes, CFG["fluxorder"]
+    # stage phases alone (stage kernel + local halo gather + pack), on the library stream
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(stages)]
+    for s_, (a, c) in enumerate(ev):
+        if s_ == 0 and CFG["les"]:
+            S._run_phase([sh], tr, S.CB_PHASE_NUT, 0, B.HALO_WRAP, 1, False)
+        a.record(stream)
+        bt.phase(S.CB_PHASE_STAGE, s_)
+        c.record(stream)
+        tr.exchange([sh], B.HALO_STAGE, 5)
+        bt.phase_unpack(S.CB_PHASE_STAGE)
+    torch.cuda.synchronize()
+    kms = max_over_ranks(sum(a.elapsed_time(c) for a, c in ev) / stages, ws, local)
+    # end to end through the public API with host buffers: upload, ghost exchange, one step, download
+    q_host = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    q_host[...] = q0
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier(ws)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        bt.SetInitialCondition(0, q_host)
+        S.fill_ghosts_all([sh], tr)
+        S.step_all([sh], tr, 1)
+        q_out = bt.Q(0)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), ws, local)
+    if not np.isfinite(q_out).all():
+        raise RuntimeError("non-finite state after end-to-end steps")
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        achieved = B_ALG[prec] * interior / (kms / 1e3) / 1e9
+        cfg = workload_config(n)
+        cfg.update({"workload": cfg["workload"].replace(f"{n}^3 (DMDA {n + 2}^3)",
+                                                        f"{n}x{n}x{n * ws} box in {ws} k-slabs of {n}^3 (DMDA {n + 2}^3 each)"),
+                    "parallelism": f"k-slabs over {ws} GPUs, 2-node halo exchange per stage (NCCL send/recv)",
+                    "precision_form": prec, "interior_nodes": interior * ws})
+        line = {
+            "metric": METRIC, "value": ws * interior * stages * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32-flux/f64-state" if prec == "mixed" else "f64", "data": "synthetic", "config": cfg,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic(prec),
+                         "kernel": f"stage phase ({prec} form: persistent stage kernel + local halo gather + pack)",
+                         "kernel_avg_ms": kms, "bytes_per_cell": B_ALG[prec],
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "clocks": clocks,
+            "e2e": {"value": ws * interior * stages * e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(q0.nbytes) * ws, "d2h_bytes_per_step": int(q0.nbytes) * ws},
+            "gpu_launches": (stages * 4 + 3) * args.steps,
+            "cpu_baseline": None,
+            "exchange_entries_per_stage": {"send": int(len(plan.stage.send)), "recv": int(len(plan.stage.recv))},
+        }
+        print(json.dumps(line), flush=True)
+    bt.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -448,13 +560,19 @@ def main():
                     help="form reported as the headline value (both are measured)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the multi-block batched measurement")
+    ap.add_argument("--layout", default="auto", choices=["auto", "replicas", "slabs"],
+                    help="N GPUs: one TGV box split in k-slabs with halo exchange (default for N > 1), "
+                         "or independent replicas")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_setup()
     try:
+        layout = args.layout if args.layout != "auto" else ("slabs" if ws > 1 else "replicas")
         if args.impl == "reference":
             run_reference(args, ws, rank)
+        elif layout == "slabs":
+            run_sharded(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

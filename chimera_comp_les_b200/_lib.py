@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(_PKG, "libchimera_b200.so")
 
 CB_OK, CB_E_ARG, CB_E_CUDA, CB_E_STATE, CB_E_NONFINITE, CB_E_UNSUPPORTED = 0, 1, 2, 3, 4, 5
 CB_FP64, CB_MIXED = 0, 1
+CB_PHASE_STATE, CB_PHASE_NUT, CB_PHASE_STAGE = 0, 1, 2
 
 
 class CbConfig(C.Structure):
@@ -99,6 +100,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         ("cb_batch_get_metrics", [P, I, D, D, D, D]),
         ("cb_batch_set_halo_map", [P, I, C.c_longlong, IP]), ("cb_batch_halo_periodic", [P]),
         ("cb_batch_rk_step", [P, I, I]), ("cb_batch_sync", [P]), ("cb_batch_autotune", [P, IP, D]),
+        ("cb_batch_set_exchange", [P, I, C.c_longlong, IP, P, C.c_longlong, IP, P]),
+        ("cb_batch_phase", [P, I, I, I]), ("cb_batch_phase_unpack", [P, I]),
     ]:
         f = getattr(lib, name)
         f.argtypes = args

@@ -106,13 +106,14 @@ def decompose(gdims: Tuple[int, int, int], cuts: Sequence[Sequence[int]]):
     return parts
 
 
-def halo_maps_decomposed(gdims: Tuple[int, int, int], parts):
+def halo_maps_decomposed(gdims: Tuple[int, int, int], parts, only=None):
     """Maps under which the sub-blocks `parts` (from ``decompose``) evolve as
     the undivided periodic box: every non-interior node takes what the
     single-block rule gives at its global position, read from the block that
     owns the source node as interior (stage output), or, for a stale-input
     source (a global ghost node), from the block owning the nearest interior
-    node, in whose padded box it lies."""
+    node, in whose padded box it lies.  `only`: destination blocks to list
+    (default all) -- a process needs its own blocks and their neighbours."""
     M = np.array(gdims)
     offs = np.array([p[0] for p in parts])
     dims = np.array([p[1] for p in parts])
@@ -134,6 +135,8 @@ def halo_maps_decomposed(gdims: Tuple[int, int, int], parts):
 
     st, wr = [], []
     for b, (off, d) in enumerate(parts):
+        if only is not None and b not in only:
+            continue
         i, j, k, non = _padded_nodes(d)
         i, j, k = i[non], j[non], k[non]
         gi, gj, gk = i + off[0], j + off[1], k + off[2]
@@ -287,6 +290,23 @@ class Batch:
         stage, wrap = maps
         self.set_halo_map(HALO_STAGE, stage)
         self.set_halo_map(HALO_WRAP, wrap)
+
+    def set_exchange(self, kind: int, send: np.ndarray, d_send: int, recv: np.ndarray, d_recv: int):
+        """Cross-process exchange lists (see cb_batch_set_exchange): send rows of
+        5 (stage) or 4 (wrap) ints, recv rows of 4 ints; d_send / d_recv device
+        pointers of caller-owned buffers (5 doubles per entry)."""
+        sw = 5 if kind == HALO_STAGE else 4
+        s = np.ascontiguousarray(send, dtype=np.int32).reshape(-1, sw)
+        r = np.ascontiguousarray(recv, dtype=np.int32).reshape(-1, 4)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        self._check(self.lib.cb_batch_set_exchange(self._b, int(kind), s.shape[0], ip(s), C.c_void_p(d_send or None),
+                                                   r.shape[0], ip(r), C.c_void_p(d_recv or None)))
+
+    def phase(self, phase: int, stage: int = 0, per_block: bool = False):
+        self._check(self.lib.cb_batch_phase(self._b, int(phase), int(stage), 1 if per_block else 0))
+
+    def phase_unpack(self, phase: int):
+        self._check(self.lib.cb_batch_phase_unpack(self._b, int(phase)))
 
     def halo_periodic(self):
         self._check(self.lib.cb_batch_halo_periodic(self._b))

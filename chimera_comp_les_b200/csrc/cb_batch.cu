@@ -57,6 +57,39 @@ __global__ void plane_gather_kernel(const long long *__restrict__ dst, const lon
     f[dst[e]] = f[src[e]];
 }
 
+// Cross-process halo exchange: pack the values this process owes its peers
+// into a caller-owned device buffer (entry-major, nf values per entry) and
+// scatter the values received from them.
+struct FieldSet {
+  const double *in[5];
+  const double *out[5];
+};
+struct OutSet {
+  double *a[5];
+};
+__global__ void xpack_kernel(const long long *__restrict__ src, const unsigned char *__restrict__ fin, long long n, int nf,
+                             FieldSet fs, double *__restrict__ buf) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long sidx = src[e];
+    const bool from_in = fin != nullptr && fin[e] != 0;
+    for (int f = 0; f < nf; f++) buf[e * nf + f] = from_in ? fs.in[f][sidx] : fs.out[f][sidx];
+  }
+}
+__global__ void xunpack_kernel(const long long *__restrict__ dst, long long n, int nf, OutSet os,
+                               const double *__restrict__ buf) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long d = dst[e];
+    for (int f = 0; f < nf; f++) os.a[f][d] = buf[e * nf + f];
+  }
+}
+
+struct Xchg {
+  long long nsend = 0, nrecv = 0;
+  long long *d_src = nullptr, *d_dst = nullptr;
+  unsigned char *d_fin = nullptr;
+  double *d_send = nullptr, *d_recv = nullptr;  // caller-owned
+};
+
 struct BlockHost {
   int mx, my, mz;
   DevCfg dc;
@@ -97,6 +130,9 @@ struct cb_batch {
   long long *d_hdst = nullptr, *d_hsrc = nullptr, *d_wdst = nullptr, *d_wsrc = nullptr;
   unsigned char *d_hin = nullptr;
   bool ghosts_dirty = false;  // uploaded state still carries per-block ghosts
+  // cross-process exchange (stage values, wrap values) and the phase state
+  Xchg xs, xw;
+  int xcur0 = -1, xnext = 0, xin = -1, xout = -1;
   // stepping
   int cur = 0, uc = -1;
   cudaGraphExec_t graphs[2][3][4] = {};
@@ -322,7 +358,8 @@ void cb_batch_destroy(cb_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   destroy_graphs(b);
   void *ptrs[] = {b->arena, b->arena_mixed, b->staging, b->ptab, b->ptab4, b->d_tables, b->d_items, b->d_counter,
-                  b->status, b->d_hdst, b->d_hsrc, b->d_hin, b->d_wdst, b->d_wsrc};
+                  b->status, b->d_hdst, b->d_hsrc, b->d_hin, b->d_wdst, b->d_wsrc,
+                  b->xs.d_src, b->xs.d_dst, b->xs.d_fin, b->xw.d_src, b->xw.d_dst, b->xw.d_fin};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -583,102 +620,122 @@ static void rk_ab(const cb_batch *b, int s, double *alfa, double *beta) {
 
 // One step: eddy viscosity per block, then per stage one stage launch
 // (persistent over all blocks, or one per block) and one halo gather.
-static int enqueue_batch_step(cb_batch *b, int per_block) {
-  const bool les = b->cfg.les != 0, visc = b->cfg.inviscid == 0, mixed = b->cfg.precision == CB_MIXED;
-  if (les && visc) {
-    // Compute_eddy_viscosity_LES per block from the recorded state; the
-    // pointer arrays are the q and met members of the block's (uc, uc, uc)
-    // table entry in device memory
-    const int u = b->uc < 0 ? 0 : b->uc;
+static int enqueue_nut(cb_batch *b) {
+  // Compute_eddy_viscosity_LES per block from the recorded state; the
+  // pointer arrays are the q and met members of the block's (uc, uc, uc)
+  // table entry in device memory
+  const int u = b->uc < 0 ? 0 : b->uc;
+  for (int k = 0; k < b->nb; k++) {
+    const BlockHost &bh = b->blk[k];
+    const long long o = bh.off;
+    const long long work = (long long)(bh.mx - 2) * (bh.my - 2) * (bh.mz - 2);
+    const char *ent = reinterpret_cast<const char *>(b->d_tables + (size_t)(u * 13) * b->nb + k);
+    const double *const *qu = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
+    const double *const *mt = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, met));
+    eddy_viscosity_kernel<<<bgrid(b, work), 256, 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
+                                                                 b->delta2 + o, b->nvert + o, b->nut + o);
+  }
+  if (b->nwrap || b->xw.nsend || b->xw.nrecv) {
+    if (b->nwrap) plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, b->nut);
+  } else {
     for (int k = 0; k < b->nb; k++) {
       const BlockHost &bh = b->blk[k];
-      const long long o = bh.off;
-      const long long work = (long long)(bh.mx - 2) * (bh.my - 2) * (bh.mz - 2);
-      const char *ent = reinterpret_cast<const char *>(b->d_tables + (size_t)(u * 13) * b->nb + k);
-      const double *const *qu = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
-      const double *const *mt = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, met));
-      eddy_viscosity_kernel<<<bgrid(b, work), 256, 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
-                                                                   b->delta2 + o, b->nvert + o, b->nut + o);
+      // a one-entry pointer table: the nut plane of block k sits in the table's nut member
+      const char *ent = reinterpret_cast<const char *>(b->d_tables + k);
+      double *const *np = reinterpret_cast<double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, nut));
+      ghost_fill_kernel<<<bgrid(b, shell_count(bh.dc)), 256, 0, b->stream>>>(bh.dc, np, 1);
     }
-    if (b->nwrap) {
-      plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, b->nut);
-    } else {
-      for (int k = 0; k < b->nb; k++) {
-        const BlockHost &bh = b->blk[k];
-        const long long all = (long long)(bh.mx + 4) * (bh.my + 4) * (bh.mz + 4);
-        // a one-entry pointer table: the nut plane of block k sits in the table's nut member
-        const char *ent = reinterpret_cast<const char *>(b->d_tables + k);
-        double *const *np = reinterpret_cast<double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, nut));
-        ghost_fill_kernel<<<bgrid(b, all), 256, 0, b->stream>>>(bh.dc, np, 1);
-      }
-    }
-    BCUDA(b, cudaGetLastError());
   }
-  const int ns = b->cfg.fluxorder;
-  const int old = b->cur, A = (b->cur + 1) % 3, B = (b->cur + 2) % 3;
-  int in = b->cur;
-  for (int s = 0; s < ns; s++) {
-    const int out = (s % 2 == 0) ? A : B;
-    double alfa, beta;
-    rk_ab(b, s, &alfa, &beta);
-    const double adt = alfa * b->cfg.dt * b->cfg.st;
-    const BatchBlock *tab = b->d_tables + (size_t)(in * 9 + old * 3 + out) * b->nb;
-    if (!per_block) {
-      BCUDA(b, cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream));
-      const int ctas = b->sms * (mixed ? 2 : 1);
+  BCUDA(b, cudaGetLastError());
+  return CB_OK;
+}
+
+// Stage s of the step that started from buffer `old`: the stage kernel over
+// all blocks (persistent or one launch per block), then the local halo gather.
+static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int out) {
+  const bool les = b->cfg.les != 0, visc = b->cfg.inviscid == 0, mixed = b->cfg.precision == CB_MIXED;
+  double alfa, beta;
+  rk_ab(b, s, &alfa, &beta);
+  const double adt = alfa * b->cfg.dt * b->cfg.st;
+  const BatchBlock *tab = b->d_tables + (size_t)(in * 9 + old * 3 + out) * b->nb;
+  if (!per_block) {
+    BCUDA(b, cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream));
+    const int ctas = b->sms * (mixed ? 2 : 1);
+    if (mixed) {
+      BCUDA(b, launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, les, visc, ctas,
+                                    b->stream));
+    } else {
+      if (les && visc)
+        stage_batched_kernel<double, false, true, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+      else if (les)
+        stage_batched_kernel<double, false, true, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+      else if (visc)
+        stage_batched_kernel<double, false, false, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+      else
+        stage_batched_kernel<double, false, false, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+    }
+  } else {
+    for (int k = 0; k < b->nb; k++) {
+      const BlockHost &bh = b->blk[k];
+      const DevFields F = block_fields(b, k, in, old, out);
+      const int nk = bh.mz - 2;
+      // per-block k-chunk for whole waves of one CTA per SM
+      const int tiles = bh.tiles_x * bh.tiles_y;
+      int kc = nk;
+      double best = 1e30;
+      for (int cand = 4; cand <= nk; cand++) {
+        const long long blocks = (long long)tiles * ((nk + cand - 1) / cand);
+        const double cost = (double)((blocks + b->sms - 1) / b->sms) * (cand + 3.0);
+        if (cost < best) { best = cost; kc = cand; }
+      }
       if (mixed) {
-        BCUDA(b, launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, les, visc, ctas,
-                                      b->stream));
+        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, b->stream));
       } else {
+        dim3 grid(bh.tiles_x, bh.tiles_y, (nk + kc - 1) / kc);
         if (les && visc)
-          stage_batched_kernel<double, false, true, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+          stage_kernel<double, false, true, true, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
         else if (les)
-          stage_batched_kernel<double, false, true, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+          stage_kernel<double, false, true, false, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
         else if (visc)
-          stage_batched_kernel<double, false, false, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+          stage_kernel<double, false, false, true, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
         else
-          stage_batched_kernel<double, false, false, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
-      }
-    } else {
-      for (int k = 0; k < b->nb; k++) {
-        const BlockHost &bh = b->blk[k];
-        const DevFields F = block_fields(b, k, in, old, out);
-        const int nk = bh.mz - 2;
-        // per-block k-chunk for whole waves of one CTA per SM
-        const int tiles = bh.tiles_x * bh.tiles_y;
-        int kc = nk;
-        double best = 1e30;
-        for (int cand = 4; cand <= nk; cand++) {
-          const long long blocks = (long long)tiles * ((nk + cand - 1) / cand);
-          const double cost = (double)((blocks + b->sms - 1) / b->sms) * (cand + 3.0);
-          if (cost < best) { best = cost; kc = cand; }
-        }
-        if (mixed) {
-          BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, b->stream));
-        } else {
-          dim3 grid(bh.tiles_x, bh.tiles_y, (nk + kc - 1) / kc);
-          if (les && visc)
-            stage_kernel<double, false, true, true, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
-          else if (les)
-            stage_kernel<double, false, true, false, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
-          else if (visc)
-            stage_kernel<double, false, false, true, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
-          else
-            stage_kernel<double, false, false, false, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
-        }
+          stage_kernel<double, false, false, false, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
       }
     }
-    BCUDA(b, cudaGetLastError());
-    if (b->nhalo) {
-      DevFields G{};
-      for (int q = 0; q < 5; q++) { G.q[q] = b->qb[in][q]; G.qout[q] = b->qb[out][q]; }
-      halo_gather_kernel<<<bgrid(b, b->nhalo), 256, 0, b->stream>>>(b->d_hdst, b->d_hsrc, b->d_hin, b->nhalo, G);
-      BCUDA(b, cudaGetLastError());
-    }
-    if (visc) b->uc = in;
-    in = out;
   }
-  b->cur = in;
+  BCUDA(b, cudaGetLastError());
+  if (b->nhalo) {
+    DevFields G{};
+    for (int q = 0; q < 5; q++) { G.q[q] = b->qb[in][q]; G.qout[q] = b->qb[out][q]; }
+    halo_gather_kernel<<<bgrid(b, b->nhalo), 256, 0, b->stream>>>(b->d_hdst, b->d_hsrc, b->d_hin, b->nhalo, G);
+    BCUDA(b, cudaGetLastError());
+  }
+  return CB_OK;
+}
+
+// Buffers of stage s when the step starts from buffer cur0.
+static void stage_buffers(int cur0, int s, int *in, int *out) {
+  const int A = (cur0 + 1) % 3, B = (cur0 + 2) % 3;
+  *out = (s % 2 == 0) ? A : B;
+  *in = s == 0 ? cur0 : (((s - 1) % 2 == 0) ? A : B);
+}
+
+// One step: eddy viscosity per block, then per stage one stage launch
+// (persistent over all blocks, or one per block) and one halo gather.
+static int enqueue_batch_step(cb_batch *b, int per_block) {
+  if (b->cfg.les && !b->cfg.inviscid) {
+    int e = enqueue_nut(b);
+    if (e) return e;
+  }
+  const int ns = b->cfg.fluxorder, old = b->cur;
+  int in = b->cur, out = b->cur;
+  for (int s = 0; s < ns; s++) {
+    stage_buffers(old, s, &in, &out);
+    int e = enqueue_stage(b, s, per_block, in, old, out);
+    if (e) return e;
+    if (!b->cfg.inviscid) b->uc = in;
+  }
+  b->cur = out;
   return CB_OK;
 }
 
@@ -689,6 +746,8 @@ int cb_batch_rk_step(cb_batch *b, int nsteps, int mode) {
   for (auto &bh : b->blk)
     if (!bh.have_grid || !bh.have_state) return bfail(b, CB_E_STATE, "every block needs a grid and a state");
   if (!b->nhalo) return bfail(b, CB_E_STATE, "no halo map (cb_batch_set_halo_map / cb_batch_halo_periodic)");
+  if (b->xs.nsend || b->xs.nrecv || b->xw.nsend || b->xw.nrecv)
+    return bfail(b, CB_E_STATE, "a batch with a cross-process exchange steps through cb_batch_phase");
   if (b->ghosts_dirty && fill_ghosts(b)) return CB_E_CUDA;
   for (int n = 0; n < nsteps; n++) {
     cudaGraphExec_t &g = b->graphs[mode][b->cur][b->uc + 1];
@@ -715,6 +774,162 @@ int cb_batch_rk_step(cb_batch *b, int nsteps, int mode) {
       in = (s % 2 == 0) ? A : B;
     }
     b->cur = in;
+  }
+  return CB_OK;
+}
+
+// Exchange lists of a batch that holds part of a domain whose other parts
+// live in other processes.  kind CB_HALO_STAGE: nsend entries of 5 ints
+// (block, i, j, k, from_stage_input), nrecv entries of 4 ints (block, i, j, k);
+// kind CB_HALO_WRAP: both 4 ints.  d_send / d_recv: caller-owned device
+// buffers of 5 doubles per entry.
+int cb_batch_set_exchange(cb_batch *b, int kind, long long nsend, const int *send, double *d_send, long long nrecv,
+                          const int *recv, double *d_recv) {
+  if (!b || (kind != CB_HALO_STAGE && kind != CB_HALO_WRAP) || nsend < 0 || nrecv < 0 || (nsend && (!send || !d_send)) ||
+      (nrecv && (!recv || !d_recv)))
+    return CB_E_ARG;
+  const int sw = kind == CB_HALO_STAGE ? 5 : 4;
+  std::vector<long long> hs((size_t)nsend), hd((size_t)nrecv);
+  std::vector<unsigned char> hf((size_t)nsend);
+  auto in_box = [&](const BlockHost &bh, int i, int j, int k) {
+    return i >= -2 && i <= bh.mx + 1 && j >= -2 && j <= bh.my + 1 && k >= -2 && k <= bh.mz + 1;
+  };
+  for (long long t = 0; t < nsend; t++) {
+    const int *r = send + sw * t;
+    if (r[0] < 0 || r[0] >= b->nb) return bfail(b, CB_E_ARG, "exchange: block index");
+    const BlockHost &bh = b->blk[r[0]];
+    if (!in_box(bh, r[1], r[2], r[3])) return bfail(b, CB_E_ARG, "exchange: node outside the padded box");
+    const bool fin = kind == CB_HALO_STAGE && r[4] != 0;
+    if (kind == CB_HALO_STAGE && !fin && !interior_node(bh, r[1], r[2], r[3]))
+      return bfail(b, CB_E_ARG, "exchange: stage-output source is not an interior node");
+    hs[t] = bh.off + gidx(bh.dc, r[1], r[2], r[3]);
+    hf[t] = fin ? 1 : 0;
+  }
+  for (long long t = 0; t < nrecv; t++) {
+    const int *r = recv + 4 * t;
+    if (r[0] < 0 || r[0] >= b->nb) return bfail(b, CB_E_ARG, "exchange: block index");
+    const BlockHost &bh = b->blk[r[0]];
+    if (!in_box(bh, r[1], r[2], r[3])) return bfail(b, CB_E_ARG, "exchange: node outside the padded box");
+    if (interior_node(bh, r[1], r[2], r[3])) return bfail(b, CB_E_ARG, "exchange: destination is an interior node");
+    hd[t] = bh.off + gidx(bh.dc, r[1], r[2], r[3]);
+  }
+  std::vector<long long> sd(hd);
+  std::sort(sd.begin(), sd.end());
+  if (std::adjacent_find(sd.begin(), sd.end()) != sd.end()) return bfail(b, CB_E_ARG, "exchange: duplicate destination");
+  Xchg &x = kind == CB_HALO_STAGE ? b->xs : b->xw;
+  if (x.d_src) cudaFree(x.d_src);
+  if (x.d_dst) cudaFree(x.d_dst);
+  if (x.d_fin) cudaFree(x.d_fin);
+  x = Xchg();
+  x.nsend = nsend;
+  x.nrecv = nrecv;
+  x.d_send = d_send;
+  x.d_recv = d_recv;
+  if (nsend) {
+    BCUDA(b, cudaMalloc(&x.d_src, sizeof(long long) * nsend));
+    BCUDA(b, cudaMemcpy(x.d_src, hs.data(), sizeof(long long) * nsend, cudaMemcpyHostToDevice));
+    if (kind == CB_HALO_STAGE) {
+      BCUDA(b, cudaMalloc(&x.d_fin, nsend));
+      BCUDA(b, cudaMemcpy(x.d_fin, hf.data(), nsend, cudaMemcpyHostToDevice));
+    }
+  }
+  if (nrecv) {
+    BCUDA(b, cudaMalloc(&x.d_dst, sizeof(long long) * nrecv));
+    BCUDA(b, cudaMemcpy(x.d_dst, hd.data(), sizeof(long long) * nrecv, cudaMemcpyHostToDevice));
+  }
+  destroy_graphs(b);
+  return CB_OK;
+}
+
+static FieldSet field_set(const double *const *in, const double *const *out, int nf) {
+  FieldSet fs{};
+  for (int f = 0; f < nf; f++) { fs.in[f] = in ? in[f] : nullptr; fs.out[f] = out[f]; }
+  return fs;
+}
+
+// Enqueues one phase of a step with a cross-process exchange and packs what
+// this process sends; the caller then exchanges the buffers (all on the
+// batch's stream) and calls cb_batch_phase_unpack.  Phases:
+//   CB_PHASE_STATE  once after the uploads: wrap map on the state, pack of the
+//                   state's wrap values (5 per entry)
+//   CB_PHASE_NUT    each step with LES: eddy viscosity, wrap map, pack (1 per entry)
+//   CB_PHASE_STAGE  stage `stage` (0, 1, ... in order): stage kernel, stage
+//                   map, pack of the stage values (5 per entry)
+int cb_batch_phase(cb_batch *b, int phase, int stage, int mode) {
+  if (!b || (mode != 0 && mode != 1)) return CB_E_ARG;
+  for (auto &bh : b->blk)
+    if (!bh.have_grid || !bh.have_state) return bfail(b, CB_E_STATE, "every block needs a grid and a state");
+  if (phase == CB_PHASE_STATE) {
+    if (fill_ghosts(b)) return CB_E_CUDA;
+    if (b->xw.nsend) {
+      const double *qs[5];
+      for (int q = 0; q < 5; q++) qs[q] = b->qb[b->cur][q];
+      xpack_kernel<<<bgrid(b, b->xw.nsend), 256, 0, b->stream>>>(b->xw.d_src, nullptr, b->xw.nsend, 5,
+                                                                  field_set(nullptr, qs, 5), b->xw.d_send);
+    }
+  } else if (phase == CB_PHASE_NUT) {
+    if (!(b->cfg.les && !b->cfg.inviscid)) return bfail(b, CB_E_STATE, "no eddy viscosity without les and viscosity");
+    if (b->ghosts_dirty) return bfail(b, CB_E_STATE, "run CB_PHASE_STATE after uploads");
+    int e = enqueue_nut(b);
+    if (e) return e;
+    if (b->xw.nsend) {
+      const double *ns[1] = {b->nut};
+      xpack_kernel<<<bgrid(b, b->xw.nsend), 256, 0, b->stream>>>(b->xw.d_src, nullptr, b->xw.nsend, 1,
+                                                                  field_set(nullptr, ns, 1), b->xw.d_send);
+    }
+  } else if (phase == CB_PHASE_STAGE) {
+    if (b->ghosts_dirty) return bfail(b, CB_E_STATE, "run CB_PHASE_STATE after uploads");
+    if (stage != b->xnext || stage < 0 || stage >= b->cfg.fluxorder) return bfail(b, CB_E_STATE, "stages must run in order");
+    if (stage == 0) b->xcur0 = b->cur;
+    int in, out;
+    stage_buffers(b->xcur0, stage, &in, &out);
+    int e = enqueue_stage(b, stage, mode, in, b->xcur0, out);
+    if (e) return e;
+    if (b->xs.nsend) {
+      const double *qi[5], *qo[5];
+      for (int q = 0; q < 5; q++) { qi[q] = b->qb[in][q]; qo[q] = b->qb[out][q]; }
+      xpack_kernel<<<bgrid(b, b->xs.nsend), 256, 0, b->stream>>>(b->xs.d_src, b->xs.d_fin, b->xs.nsend, 5,
+                                                                  field_set(qi, qo, 5), b->xs.d_send);
+    }
+    b->xin = in;
+    b->xout = out;
+  } else {
+    return CB_E_ARG;
+  }
+  BCUDA(b, cudaGetLastError());
+  return CB_OK;
+}
+
+int cb_batch_phase_unpack(cb_batch *b, int phase) {
+  if (!b) return CB_E_ARG;
+  OutSet os{};
+  int nf = 5;
+  const Xchg *x = &b->xw;
+  if (phase == CB_PHASE_STATE) {
+    for (int q = 0; q < 5; q++) os.a[q] = b->qb[b->cur][q];
+  } else if (phase == CB_PHASE_NUT) {
+    os.a[0] = b->nut;
+    nf = 1;
+  } else if (phase == CB_PHASE_STAGE) {
+    if (b->xout < 0) return bfail(b, CB_E_STATE, "no stage to unpack");
+    for (int q = 0; q < 5; q++) os.a[q] = b->qb[b->xout][q];
+    x = &b->xs;
+  } else {
+    return CB_E_ARG;
+  }
+  if (x->nrecv)
+    xunpack_kernel<<<bgrid(b, x->nrecv), 256, 0, b->stream>>>(x->d_dst, x->nrecv, nf, os, x->d_recv);
+  BCUDA(b, cudaGetLastError());
+  if (phase == CB_PHASE_STAGE) {
+    if (!b->cfg.inviscid) b->uc = b->xin;
+    const int s = b->xnext;
+    b->xnext = s + 1;
+    if (b->xnext == b->cfg.fluxorder) {  // step complete
+      b->cur = b->xout;
+      b->xnext = 0;
+      b->xcur0 = -1;
+    }
+    b->xout = -1;
   }
   return CB_OK;
 }

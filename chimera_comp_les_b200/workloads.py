@@ -34,6 +34,20 @@ def periodic_grid(n, length, amp: float = 0.0) -> np.ndarray:
     return np.ascontiguousarray(np.stack([x, y, z], axis=-1))
 
 
+def periodic_grid_slab(n, length, amp: float, k0: int, mz: int) -> np.ndarray:
+    """Nodes k0 .. k0+mz-1 (global DMDA k index) of ``periodic_grid(n, length,
+    amp)``, without building the whole box."""
+    ns = tuple(n)
+    ls = tuple(length)
+    ax = [(np.arange(ns[d] + 2) - 1.0) * (ls[d] / ns[d]) for d in range(3)]
+    z, y, x = np.meshgrid(ax[2][k0:k0 + mz], ax[1], ax[0], indexing="ij")
+    if amp:
+        sx, sy, sz = (2 * math.pi * x / ls[0], 2 * math.pi * y / ls[1], 2 * math.pi * z / ls[2])
+        x, y, z = (x + amp * np.sin(sy) * np.sin(sz), y + amp * np.sin(sz) * np.sin(sx),
+                   z + amp * np.sin(sx) * np.sin(sy))
+    return np.ascontiguousarray(np.stack([x, y, z], axis=-1))
+
+
 def conserved(rho, u, v, w, p, gamma: float) -> np.ndarray:
     e = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
     return np.ascontiguousarray(np.stack([rho, rho * u, rho * v, rho * w, e], axis=-1))

@@ -235,6 +235,26 @@ int cb_batch_halo_periodic(cb_batch *b);
  * stage launch per block (for comparison).  Asynchronous. */
 int cb_batch_rk_step(cb_batch *b, int nsteps, int mode);
 int cb_batch_sync(cb_batch *b);
+/* Cross-process exchange (one process per GPU, each holding part of a
+ * decomposed domain; the reference exchanges its DMDA ghosts with MPI inside
+ * DMGlobalToLocal, init.c:156).  Halo entries whose source node lives in
+ * another process are split into what this process sends (kind
+ * CB_HALO_STAGE: 5 ints block,i,j,k,from_stage_input; CB_HALO_WRAP: 4 ints)
+ * and what it receives (4 ints, destination nodes).  d_send / d_recv are
+ * caller-owned device buffers of 5 doubles per entry, packed entry-major.
+ * With an exchange the batch steps through phases: cb_batch_phase enqueues
+ * the local work and packs d_send; the caller moves the buffers between
+ * processes (e.g. NCCL send/recv) ordered on cb_batch_stream; then
+ * cb_batch_phase_unpack scatters d_recv.  Per step: CB_PHASE_NUT (LES only),
+ * then CB_PHASE_STAGE for stages 0..fluxorder-1; once after the uploads
+ * CB_PHASE_STATE.  cb_batch_rk_step refuses such a batch (CB_E_STATE). */
+#define CB_PHASE_STATE 0
+#define CB_PHASE_NUT 1
+#define CB_PHASE_STAGE 2
+int cb_batch_set_exchange(cb_batch *b, int kind, long long nsend, const int *send, double *d_send, long long nrecv,
+                          const int *recv, double *d_recv);
+int cb_batch_phase(cb_batch *b, int phase, int stage, int mode);
+int cb_batch_phase_unpack(cb_batch *b, int phase);
 /* Times one persistent stage launch per candidate k-chunk of the work items
  * and keeps the fastest.  The state is not advanced. */
 int cb_batch_autotune(cb_batch *b, int *best_kchunk, double *best_ms);
