@@ -211,6 +211,7 @@ def _block(precision, local, coords, q0, nv):
     blk.FormMetrics(coords)
     blk.set_nvert(nv)
     blk.SetInitialCondition(q0)
+    blk.kchunk, _ = blk.autotune()  # k-chunk of the stage kernel by measurement
     return blk
 
 
@@ -365,7 +366,7 @@ def run_ours(args, ws, rank, local):
         achieved = B_ALG[prec] * interior / (kms / 1e3) / 1e9
         forms[prec] = {"value": ws * interior * stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
                        "clocks": clocks, "kernel_avg_ms": kms, "achieved_gbs": achieved,
-                       "launches_per_step": blk.launches_per_step}
+                       "launches_per_step": blk.launches_per_step, "kchunk_autotuned": blk.kchunk}
     head = forms[args.precision]
     acc = _accuracy(blocks["fp64"], blocks["mixed"], q0) if rank == 0 else None
 
@@ -436,6 +437,58 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
     for b in blocks.values():
         b.close()
+
+
+# ------------------------------------------------------------ size sweep --
+def run_sweep(args, local):
+    """Decaying compressible isotropic turbulence on a periodic [0, 2*pi]^3
+    Cartesian box at 128^3 .. 512^3 (Passot-Pouquet spectrum, k0 4, u_rms 1,
+    Mt 0.4, seed 5; rho 1, uniform p): per size and form cell-updates/s per
+    stage, stage-kernel HBM GB/s, and the mixed-vs-FP64 per-field error after
+    ACC_STEPS steps.  The reference's LES scheme (WENO3 + Rusanov blended with
+    the central flux at sigma 0.5, CS 0.03 = 0.17^2), SSP-RK3, dt from CFL 0.4.
+    One JSON line per size (not the contract line)."""
+    import torch
+
+    from chimera_comp_les_b200 import Block
+    from chimera_comp_les_b200 import diagnostics as D
+    from chimera_comp_les_b200 import workloads as W
+    torch.cuda.set_device(local)
+    peak, peak_kind = measured_peaks()
+    for n in [int(x) for x in args.sweep.split(",")]:
+        coords = W.periodic_grid(n, 2 * math.pi, amp=0.0)
+        q0 = W.isotropic_turbulence(n, 5, k_peak=4.0, mach_t=0.4, spectrum="passot_pouquet", u_rms=1.0)
+        r = q0[..., 0]
+        c = np.sqrt(1.4 * 0.4 * (q0[..., 4] - 0.5 * (q0[..., 1] ** 2 + q0[..., 2] ** 2 + q0[..., 3] ** 2) / r) / r)
+        lam = sum(float((np.abs(q0[..., 1 + a] / r) + c).max()) for a in range(3)) * n / (2 * math.pi)
+        dt = math.floor(0.4 / lam * 1e6) / 1e6
+        opts = dict(CFG, s_x=0.5, s_y=0.5, s_z=0.5, ren=10000.0, ma=0.4, dt=dt)
+        nv = np.zeros(coords.shape[:3])
+        out = {"sweep": "isotropic turbulence", "n": n, "grid": [n + 2] * 3, "dt": dt}
+        final = {}
+        for prec in ("fp64", "mixed"):
+            blk = Block(n + 2, n + 2, n + 2, precision=prec, device=local, **opts)
+            blk.FormMetrics(coords)
+            blk.set_nvert(nv)
+            blk.SetInitialCondition(q0)
+            kc, _ = blk.autotune()
+            steps = args.steps
+            ms, _ = _timed(blk, steps, args.warmup, 1, local)
+            kms = _kernel_ms(blk, 5)
+            interior = blk.interior_nodes
+            out[prec] = {"value": interior * blk.stages * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                         "kernel_avg_ms": kms, "achieved_gbs": B_ALG[prec] * interior / (kms / 1e3) / 1e9,
+                         "kchunk_autotuned": kc}
+            blk.SetInitialCondition(q0)
+            blk.RungeKutta(ACC_STEPS)
+            final[prec] = blk.Q()
+            blk.close()
+        l2, linf = D.field_errors(final["mixed"], final["fp64"])
+        out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+        out["mixed_vs_fp64_error"] = {"steps": ACC_STEPS, "rel_l2": l2, "rel_linf": linf}
+        out["peak_gbs"] = peak
+        out["peak_source"] = peak_kind
+        print(json.dumps(out), flush=True)
 
 
 # ------------------------------------------------------- sharded (N > 1) --
@@ -560,6 +613,8 @@ def main():
                     help="form reported as the headline value (both are measured)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the multi-block batched measurement")
+    ap.add_argument("--sweep", default="", help="comma-separated sizes, e.g. 128,256,384,512: isotropic-turbulence "
+                                                  "size sweep, one JSON line per size instead of the bench line")
     ap.add_argument("--layout", default="auto", choices=["auto", "replicas", "slabs"],
                     help="N GPUs: one TGV box split in k-slabs with halo exchange (default for N > 1), "
                          "or independent replicas")
@@ -571,6 +626,8 @@ def main():
         layout = args.layout if args.layout != "auto" else ("slabs" if ws > 1 else "replicas")
         if args.impl == "reference":
             run_reference(args, ws, rank)
+        elif args.sweep:
+            run_sweep(args, local)
         elif layout == "slabs":
             run_sharded(args, ws, rank, local)
         else:

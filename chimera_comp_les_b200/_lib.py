@@ -65,6 +65,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = C.c_int
+    lib.cb_autotune.argtypes = [P, C.c_int, C.POINTER(C.c_int), D, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.cb_autotune.restype = C.c_int
     lib.cb_cfl_dt.argtypes = [P, C.c_double, D, D]
     lib.cb_cfl_dt.restype = C.c_int
     lib.cb_rhs_noalloc.argtypes = [C.POINTER(CbConfig), P, P, P, P, P, P]

@@ -372,16 +372,19 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc status");
   cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream);
   if (fill_ptab(c)) return bail(CB_E_CUDA, "pointer table");
-  // k-chunk: aim for a whole number of waves of one block per SM
+  // k-chunk: whole waves of the resident blocks (1 per SM in the FP64 form,
+  // 2 in the mixed form); a chunk's prologue costs about one plane.  The
+  // autotuner (cb_autotune) refines this by measurement.
   {
     const int tiles = ((cfg->mx - 2 + BX - 1) / BX) * ((cfg->my - 2 + BY - 1) / BY);
     const int nk = cfg->mz - 2;
+    const int slots = c->sms * (cfg->precision == CB_MIXED ? 2 : 1);
     double best = 1e30;
     for (int kc = 4; kc <= nk; kc++) {
       const int chunks = (nk + kc - 1) / kc;
       const long long blocks = (long long)tiles * chunks;
-      const long long waves = (blocks + c->sms - 1) / c->sms;
-      const double cost = (double)waves * (kc + 3.0);  // ~3 extra plane loads per chunk prologue
+      const long long waves = (blocks + slots - 1) / slots;
+      const double cost = (double)waves * (kc + 1.0);
       if (cost < best) { best = cost; c->kchunk = kc; }
     }
   }
@@ -661,6 +664,64 @@ int cb_rk_step(cb_ctx *c, int nsteps) {
     int e = enqueue_step(c);
     if (e) return e;
   }
+  return CB_OK;
+}
+
+// Autotuner of the stage kernel's k-chunk (planes per block along k): times
+// one stage launch per candidate on the current state, writing a buffer that
+// holds neither the state nor the recorded velocity field, and keeps the
+// fastest.  ncand = 0: every k-chunk from 4 to mz-2 that changes the number
+// of chunks.  ms_out (optional, ncand entries or the default count) receives
+// the average time of each candidate; *best the chosen k-chunk.
+int cb_autotune(cb_ctx *c, int ncand, const int *cand, double *ms_out, int *nout, int *best) {
+  if (!c || ncand < 0 || (ncand && !cand)) return CB_E_ARG;
+  if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set");
+  std::vector<int> cs;
+  const int nk = c->dc.mz - 2;
+  if (ncand) {
+    for (int t = 0; t < ncand; t++)
+      if (cand[t] < 1) return fail(c, CB_E_ARG, "k-chunk candidates must be positive");
+    cs.assign(cand, cand + ncand);
+  } else {
+    int last = -1;
+    for (int kc = nk; kc >= 4; kc--) {
+      const int ch = (nk + kc - 1) / kc;
+      if (ch != last) { cs.push_back(kc); last = ch; }
+    }
+  }
+  const int in = c->cur;
+  int out = (c->cur + 1) % 3;
+  if (out == c->uc) out = (c->cur + 2) % 3;
+  DevFields F = fields_for(c, in, in, out);
+  cudaEvent_t e0, e1;
+  CB_CUDA(c, cudaEventCreate(&e0));
+  CB_CUDA(c, cudaEventCreate(&e1));
+  const int keep = c->kchunk;
+  double bms = 1e30;
+  int bkc = keep;
+  for (size_t t = 0; t < cs.size(); t++) {
+    c->kchunk = cs[t];
+    float tot = 0.f;
+    for (int rep = 0; rep < 3; rep++) {
+      cudaEventRecord(e0, c->stream);
+      cudaError_t ce = launch_stage(c, F, 1, 1.0, 1.0, 0.0, false);
+      cudaEventRecord(e1, c->stream);
+      if (ce != cudaSuccess) { c->kchunk = keep; return fail(c, CB_E_CUDA, cudaGetErrorString(ce)); }
+      CB_CUDA(c, cudaEventSynchronize(e1));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep) tot += ms;  // the first launch warms the caches
+    }
+    const double avg = tot / 2.0;
+    if (ms_out && (!nout || (int)t < *nout)) ms_out[t] = avg;
+    if (avg < bms) { bms = avg; bkc = cs[t]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (nout) *nout = (int)cs.size();
+  c->kchunk = bkc;
+  if (best) *best = bkc;
+  invalidate_graphs(c);  // the graphs carry the launch shape
   return CB_OK;
 }
 

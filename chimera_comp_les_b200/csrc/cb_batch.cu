@@ -679,13 +679,15 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
       const BlockHost &bh = b->blk[k];
       const DevFields F = block_fields(b, k, in, old, out);
       const int nk = bh.mz - 2;
-      // per-block k-chunk for whole waves of one CTA per SM
+      // per-block k-chunk for whole waves of the resident CTAs (the
+      // single-block context's rule)
       const int tiles = bh.tiles_x * bh.tiles_y;
+      const int slots = b->sms * (mixed ? 2 : 1);
       int kc = nk;
       double best = 1e30;
       for (int cand = 4; cand <= nk; cand++) {
         const long long blocks = (long long)tiles * ((nk + cand - 1) / cand);
-        const double cost = (double)((blocks + b->sms - 1) / b->sms) * (cand + 3.0);
+        const double cost = (double)((blocks + slots - 1) / slots) * (cand + 1.0);
         if (cost < best) { best = cost; kc = cand; }
       }
       if (mixed) {

@@ -143,6 +143,26 @@ class Block:
         self._check(self.lib.cb_cfl_dt(self._ctx, float(cfl), C.byref(dt), C.byref(lam)))
         return dt.value, lam.value
 
+    def autotune(self, candidates=None):
+        """Time the stage kernel per k-chunk candidate and keep the fastest.
+        Returns (best k-chunk, {k-chunk: ms})."""
+        cand = list(candidates or [])
+        ca = (C.c_int * max(len(cand), 1))(*cand)
+        cap = max(len(cand), self.shape[0])
+        ms = (C.c_double * cap)()
+        nout, best = C.c_int(cap), C.c_int()
+        self._check(self.lib.cb_autotune(self._ctx, len(cand), ca, ms, C.byref(nout), C.byref(best)))
+        if cand:
+            keys = cand
+        else:
+            nk, keys, last = self.shape[0] - 2, [], -1
+            for kc in range(nk, 3, -1):
+                ch = -(-nk // kc)
+                if ch != last:
+                    keys.append(kc)
+                    last = ch
+        return best.value, {k: ms[i] for i, k in enumerate(keys[:nout.value])}
+
     def CalcUCat(self):
         self._check(self.lib.cb_calc_ucat(self._ctx))
 

@@ -145,10 +145,11 @@ def isotropic_turbulence(n, seed: int, k_peak: float = 4.0, mach_t: float = 0.3,
                          gamma: float = 1.4, u_rms: float | None = None) -> np.ndarray:
     """Solenoidal random velocity field with energy spectrum `spectrum` peaking
     near k_peak (integer wavenumbers of a 2*pi box) and random phases from
-    `seed`, on rho = 1, p = 1/gamma (sound speed 1).  The field is scaled so
-    sqrt(<u.u>) = mach_t (or, with u_rms given, so each component has that rms,
-    and mach_t is ignored).  n: unique points (nx, ny, nz); returns the state on
-    the DMDA nodes (nz+2, ny+2, nx+2, 5) with the periodic images."""
+    `seed`, on rho = 1 and a uniform pressure.  Without u_rms: sound speed 1
+    (p = 1/gamma) and the field scaled so sqrt(<u.u>) = mach_t.  With u_rms:
+    each component has that rms and p is set so sqrt(<u.u>) / c = mach_t.
+    n: unique points (nx, ny, nz); returns the state on the DMDA nodes
+    (nz+2, ny+2, nx+2, 5) with the periodic images."""
     nx, ny, nz = (n, n, n) if np.isscalar(n) else tuple(int(x) for x in n)
     rng = np.random.default_rng(seed)
     kx, ky, kz = (np.fft.fftfreq(m, 1.0 / m) for m in (nx, ny, nz))
@@ -170,10 +171,11 @@ def isotropic_turbulence(n, seed: int, k_peak: float = 4.0, mach_t: float = 0.3,
     else:
         s = mach_t / math.sqrt(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2))
     u = [a * s for a in u]
+    c = math.sqrt(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2)) / mach_t if u_rms is not None else 1.0
     iz, iy, ix = ((np.arange(m + 2) - 1) % m for m in (nz, ny, nx))
     u = [a[np.ix_(iz, iy, ix)] for a in u]
     rho = np.ones_like(u[0])
-    p = np.full_like(u[0], 1.0 / gamma)
+    p = np.full_like(u[0], c * c / gamma)
     return conserved(rho, u[0], u[1], u[2], p, gamma)
 
 

@@ -136,6 +136,14 @@ int cb_rk_step(cb_ctx *ctx, int nsteps);
  * the context's dt; synchronises. */
 int cb_cfl_dt(cb_ctx *ctx, double cfl, double *dt, double *lambda_max);
 
+/* Autotuner of the stage kernel's k-chunk (planes per thread block along k):
+ * times one stage launch per candidate on the current state (ncand = 0: every
+ * k-chunk from 4 to mz-2 that changes the chunk count) and keeps the fastest.
+ * ms_out/nout (optional): per-candidate milliseconds (*nout in: capacity,
+ * out: candidates timed).  Does not advance the state.  No counterpart in the
+ * reference (CPU loops have no launch shape). */
+int cb_autotune(cb_ctx *ctx, int ncand, const int *cand, double *ms_out, int *nout, int *best_kchunk);
+
 /* Waits for the context's stream and checks the device status word
  * (CB_E_NONFINITE when a NaN/Inf or non-positive rho/p was produced). */
 int cb_sync(cb_ctx *ctx);

@@ -168,3 +168,26 @@ def test_nonfinite_state_reports_status_not_fault():
 def test_unsupported_options_fail_loudly():
     with pytest.raises(ChimeraError):
         gpu_block(O.Config(mx=12, my=12, mz=12, bctype=(1, 1, 7, 7, 7, 7)))
+
+
+def test_autotune_changes_launch_shape_not_results():
+    """cb_autotune picks the k-chunk by timing; the state it leaves and every
+    later step are bit-for-bit those of the untuned context."""
+    n = (40, 30, 36)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=1, inviscid=0, fluxorder=3, ren=1600., ma=0.1,
+                   pr=0.71, dt=0.002)
+    q = W.random_smooth_state(shape, seed=3)
+    nv = np.zeros(shape)
+    with _setup(cfg, coords, q, nv) as b:
+        b.RungeKutta(2)
+        want = b.Q()
+    with _setup(cfg, coords, q, nv) as b:
+        b.RungeKutta(1)
+        before = b.Q()
+        best, times = b.autotune()
+        assert best in times and all(t > 0 for t in times.values())
+        assert np.array_equal(b.Q(), before)
+        b.RungeKutta(1)
+        assert np.array_equal(b.Q(), want)
