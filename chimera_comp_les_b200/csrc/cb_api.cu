@@ -51,6 +51,9 @@ struct cb_ctx {
   float4 *met4[3] = {};
   double *gcl[3] = {};
   float4 **ptab4 = nullptr;
+  // shock sensor: final hybrid weights (a) and the pass buffer (b)
+  double *sig_arena = nullptr;
+  double *sig_a[3] = {}, *sig_b[3] = {};
   bool have_refs = false;
   double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
   double **ptab = nullptr;    // device pointer tables
@@ -82,7 +85,8 @@ static int fail(cb_ctx *c, int code, const std::string &msg) {
   } while (0)
 
 // device pointer tables inside ctx->ptab
-enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27, PT_NUT = 32, PT_MISC = 33, PT_GCL = 48, PT_N = 56 };
+enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27, PT_NUT = 32, PT_MISC = 33, PT_GCL = 48,
+       PT_SIGA = 56, PT_SIGB = 59, PT_N = 64 };
 
 static int grid_for(const cb_ctx *c, long long work, int block = 256) {
   long long b = (work + block - 1) / block;
@@ -107,6 +111,7 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
   F.nut = c->nut;
   F.delta2 = c->delta2;
   for (int e = 0; e < 3; e++) F.met4[e] = c->met4[e];
+  for (int a = 0; a < 3; a++) F.sig[a] = c->sig_a[a];
   for (int a = 0; a < 3; a++) F.gcl[a] = c->gcl[a];
   F.status = c->status;
   return F;
@@ -202,6 +207,23 @@ static void harvest_timing(cb_ctx *c) {
   c->ev_pairs_other.clear();
 }
 
+// Hybrid weights of the shock sensor from the stage input `in` (istage 0 of
+// formConvectionLES): three passes, each followed by the DMGlobalToLocal wrap.
+static int sigma_update(cb_ctx *c, int in) {
+  if (!c->dc.calc_sigma) return CB_OK;
+  TimedScope ts(c, false);
+  const int g = grid_for(c, (long long)c->plane);
+  const long long sh = shell_count(c->dc);
+  sigma_sensor_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * in), c->ptab + PT_SIGA);
+  ghost_fill_kernel<<<grid_for(c, sh), 256, 0, c->stream>>>(c->dc, c->ptab + PT_SIGA, 3);
+  sigma_filter_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_SIGA), c->ptab + PT_SIGB);
+  ghost_fill_kernel<<<grid_for(c, sh), 256, 0, c->stream>>>(c->dc, c->ptab + PT_SIGB, 3);
+  sigma_post_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_SIGB), c->ptab + PT_SIGA);
+  ghost_fill_kernel<<<grid_for(c, sh), 256, 0, c->stream>>>(c->dc, c->ptab + PT_SIGA, 3);
+  CB_CUDA(c, cudaGetLastError());
+  return CB_OK;
+}
+
 static int nut_update(cb_ctx *c) {
   // Compute_eddy_viscosity_LES from the recorded state (or zero velocity).
   const long long work = (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2);
@@ -243,6 +265,10 @@ static int enqueue_step(cb_ctx *c) {
     rk_coeffs(c, s, &alfa, &beta);
     const double adt = alfa * c->cfg.dt * c->cfg.st;
     DevFields F = fields_for(c, in, old, out);
+    if (s == 0) {
+      int e = sigma_update(c, in);
+      if (e) return e;
+    }
     {
       TimedScope ts(c, true);
       CB_CUDA(c, launch_stage(c, F, s, alfa, beta, adt, false));
@@ -273,6 +299,7 @@ static int fill_ptab(cb_ctx *c) {
     for (int q = 0; q < 3; q++) h[PT_MISC + 2 + 3 * e + q] = c->met[e][q];
   h[PT_MISC + 11] = c->aj;
   for (int a = 0; a < 3; a++) h[PT_GCL + a] = c->gcl[a];
+  for (int a = 0; a < 3; a++) { h[PT_SIGA + a] = c->sig_a[a]; h[PT_SIGB + a] = c->sig_b[a]; }
   CB_CUDA(c, cudaMemcpyAsync(c->ptab, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   if (c->ptab4) CB_CUDA(c, cudaMemcpyAsync(c->ptab4, c->met4, sizeof(c->met4), cudaMemcpyHostToDevice, c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -299,6 +326,9 @@ void cb_config_default(cb_config *cfg, int mx, int my, int mz) {
   cfg->cs_const = 0.03; cfg->ci = 0.06; cfg->ratio = 0.;
   cfg->precision = CB_FP64;
   cfg->device = 0;
+  cfg->calc_sigma = 0;
+  cfg->s_x_min = cfg->s_y_min = cfg->s_z_min = 0.;
+  cfg->sigma_thrsh = 0.00001;  // rhs.c:3322
 }
 
 int cb_create(const cb_config *cfg, cb_ctx **out) {
@@ -341,6 +371,9 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.inv_ren_half = 1. / cfg->ren * 0.5;
   d.gm1 = cfg->gamma - 1.0;
   d.nvq = 1;  // nvert starts zero
+  d.calc_sigma = (cfg->les && cfg->calc_sigma) ? 1 : 0;
+  d.s_x_min = cfg->s_x_min; d.s_y_min = cfg->s_y_min; d.s_z_min = cfg->s_z_min;
+  d.ks = cfg->sigma_thrsh;
   c->plane = (size_t)d.plane;
   // planes: 15 state + 9 metrics + aj + nvert + nut + LES filter width = 28
   const int nplanes = 28;
@@ -367,6 +400,15 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
     double *g = (double *)(f + c->plane * 3);
     for (int a = 0; a < 3; a++) c->gcl[a] = g + c->plane * a;
     if (cudaMalloc(&c->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab4");
+  }
+  if (c->dc.calc_sigma) {
+    const size_t sb = sizeof(double) * c->plane * 6;
+    if (cudaMalloc(&c->sig_arena, sb) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc sensor planes");
+    if (cudaMemsetAsync(c->sig_arena, 0, sb, c->stream) != cudaSuccess) return bail(CB_E_CUDA, "memset");
+    for (int a = 0; a < 3; a++) {
+      c->sig_a[a] = c->sig_arena + c->plane * a;
+      c->sig_b[a] = c->sig_arena + c->plane * (3 + a);
+    }
   }
   if (cudaMalloc(&c->ptab, sizeof(double *) * PT_N) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab");
   if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc status");
@@ -402,6 +444,7 @@ void cb_destroy(cb_ctx *c) {
   if (c->staging) cudaFree(c->staging);
   if (c->arena_mixed) cudaFree(c->arena_mixed);
   if (c->ptab4) cudaFree(c->ptab4);
+  if (c->sig_arena) cudaFree(c->sig_arena);
   if (c->ptab) cudaFree(c->ptab);
   if (c->status) cudaFree(c->status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -416,7 +459,7 @@ long long cb_interior_nodes(const cb_ctx *c) {
 int cb_stages(const cb_ctx *c) { return c ? c->cfg.fluxorder : 0; }
 int cb_launches_per_step(const cb_ctx *c) {
   if (!c) return 0;
-  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + 2 * c->cfg.fluxorder;
+  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + 2 * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0);
 }
 
 static int upload_planes(cb_ctx *c, const double *host, int nc, int pt_first, bool pinned_hint) {
@@ -569,6 +612,10 @@ int cb_rhs(cb_ctx *c, int istage, double *rhs) {
   double alfa, beta;
   rk_coeffs(c, istage < 0 ? 0 : (istage > 2 ? 2 : istage), &alfa, &beta);
   DevFields F = fields_for(c, c->cur, c->cur, -1);
+  if (istage == 0) {
+    int e = sigma_update(c, c->cur);
+    if (e) return e;
+  }
   CB_CUDA(c, launch_stage(c, F, istage, alfa, beta, 0.0, true));
   if (!c->cfg.inviscid) c->uc = c->cur;
   const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;

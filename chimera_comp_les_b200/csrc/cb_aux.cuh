@@ -132,6 +132,95 @@ static __global__ void eddy_viscosity_kernel(const DevCfg c, const double *const
   }
 }
 
+// ------------------------------------------------------------ shock sensor --
+// Hybrid weights with -calc_sigma (formConvectionLES at istage 0,
+// rhs.c:3328-3433; compute_ri / sigma_cent rhs.c:2334-2358).  Three passes
+// with a ghost fill between them, as the reference's DMGlobalToLocal calls:
+// raw ramp per direction, product filter of neighbour square roots,
+// curvature rule with y = z = min(y, z).  Boundary nodes keep (s_x, s_y, s_z).
+__device__ __forceinline__ double sensor_ri(double fR, double f0, double fL, double ks) {
+  const double dfL = fL - f0, dfR = f0 - fR;
+  return (fabs(2 * dfL * dfR) + ks) / (dfL * dfL + dfR * dfR + ks);
+}
+__device__ __forceinline__ double sensor_ramp(double fL, double f0, double fR, double fRR, double ks) {
+  const double rL = sensor_ri(fL, f0, fR, ks), rR = sensor_ri(f0, fR, fRR, ks);
+  const double r = (rR < rL) ? rR : rL;
+  const double rd = 0.5;
+  const double rmax = (rd < r) ? r : rd;
+  return 0.5 + 0.5 * tanh(3.0 * (r - rd) / rmax) / tanh(3.0);
+}
+__device__ __forceinline__ double eos_node(const DevCfg &c, const double *const *q, long long n) {
+  const double r = q[0][n];
+  return r != 0.0 ? (c.gamma - 1) * (q[4][n] - 0.5 * (q[1][n] * q[1][n] + q[2][n] * q[2][n] + q[3][n] * q[3][n]) / r)
+                  : 0.0;
+}
+__device__ __forceinline__ double pmin(double a, double b) { return (a < b) ? a : b; }
+__device__ __forceinline__ double pmax(double a, double b) { return (a < b) ? b : a; }
+
+// pass 1: every node (s_x, s_y, s_z); interior nodes the clipped ramp of p
+static __global__ void sigma_sensor_kernel(const DevCfg c, const double *const *q, double *const *sig) {
+  const long long total = (long long)c.px * c.py * c.pz;
+  const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % c.px) - 2, j = (int)((t / c.px) % c.py) - 2, k = (int)(t / sk) - 2;
+    double sx = c.s_x, sy = c.s_y, sz = c.s_z;
+    if (i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2) {
+      const long long n = t;
+      const double p0 = eos_node(c, q, n);
+      if (i < c.mx - 4 && i > 2)
+        sx = sensor_ramp(eos_node(c, q, n - si), p0, eos_node(c, q, n + si), eos_node(c, q, n + 2 * si), c.ks);
+      sx = pmax(c.s_x_min, pmin(c.s_x, sx));
+      if (c.bctype[4] == 7 || (k < c.mz - 4 && k > 4))
+        sz = sensor_ramp(eos_node(c, q, n - sk), p0, eos_node(c, q, n + sk), eos_node(c, q, n + 2 * sk), c.ks);
+      sz = pmax(c.s_z_min, pmin(c.s_z, sz));
+      if (j < c.my - 4 && j > 4)
+        sy = sensor_ramp(eos_node(c, q, n - sj), p0, eos_node(c, q, n + sj), eos_node(c, q, n + 2 * sj), c.ks);
+      sy = pmax(c.s_y_min, pmin(c.s_y, sy));
+    }
+    sig[0][t] = sx;
+    sig[1][t] = sy;
+    sig[2][t] = sz;
+  }
+}
+
+// pass 2 (ls: ghosted pass-1 planes): interior nodes times
+// sqrt(ls[j-1] ls) sqrt(ls[k-1] ls[k+1]) sqrt(ls[i-1] ls[i+1]); others copied
+static __global__ void sigma_filter_kernel(const DevCfg c, const double *const *ls, double *const *sig) {
+  const long long total = (long long)c.px * c.py * c.pz;
+  const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % c.px) - 2, j = (int)((t / c.px) % c.py) - 2, k = (int)(t / sk) - 2;
+    const bool inner = i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double *l = ls[a];
+      double v = l[t];
+      if (inner) v *= sqrt(l[t - sj] * l[t]) * sqrt(l[t - sk] * l[t + sk]) * sqrt(l[t - si] * l[t + si]);
+      sig[a][t] = v;
+    }
+  }
+}
+
+// pass 3 (ls: ghosted pass-2 planes): curvature rule, then y = z = min(z, y)
+static __global__ void sigma_post_kernel(const DevCfg c, const double *const *ls, double *const *sig) {
+  const long long total = (long long)c.px * c.py * c.pz;
+  const long long sj = c.px, sk = (long long)c.px * c.py;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % c.px) - 2, j = (int)((t / c.px) % c.py) - 2, k = (int)(t / sk) - 2;
+    double x = ls[0][t], y = ls[1][t], z = ls[2][t];
+    if (i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2) {
+      const double *ly = ls[1], *lz = ls[2];
+      if (j < c.my - 4 && j > 4 && ly[t - sj] + ly[t + sj] - 2. * ly[t] < 0.0) y = (ly[t - sj] * ly[t] * ly[t]);
+      if (k < c.mz - 4 && k > 4 && lz[t - sk] + lz[t + sk] - 2. * lz[t] < 0.0) z = (lz[t - sk] * lz[t + sk] * lz[t]);
+      z = pmin(z, y);
+      y = z;
+    }
+    sig[0][t] = x;
+    sig[1][t] = y;
+    sig[2][t] = z;
+  }
+}
+
 // LES filter width squared per node, pow(pow(1/aj, 1/3), 2.0) -- the value
 // formViscous (rhs.c:1694-1696) and Compute_eddy_viscosity_LES (les.c:1560-1561)
 // recompute at every use; aj is fixed after FormMetrics, so once per grid.

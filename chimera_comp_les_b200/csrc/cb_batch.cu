@@ -266,7 +266,8 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     return code;
   };
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
-      (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED))
+      (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
+      (cfg->les && cfg->calc_sigma))
     return bail(CB_E_UNSUPPORTED, "option combination not built");
   b->dev = cfg->device;
   if (cudaSetDevice(b->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice");
@@ -275,7 +276,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
   long long off = 0;
   size_t maxnn = 0;
   for (int k = 0; k < nblocks; k++) {
-    BlockHost bh;
+    BlockHost bh{};
     bh.mx = dims[3 * k]; bh.my = dims[3 * k + 1]; bh.mz = dims[3 * k + 2];
     if (bh.mx < 6 || bh.my < 6 || bh.mz < 6) return bail(CB_E_ARG, "every block needs at least 6 nodes per direction");
     DevCfg &d = bh.dc;
@@ -294,6 +295,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.inv_ren_half = 1. / cfg->ren * 0.5;
     d.gm1 = cfg->gamma - 1.0;
     d.nvq = 1;  // nvert starts zero
+    d.calc_sigma = 0;  // the shock sensor is built for single-block contexts
     bh.off = off;
     off += (d.plane + 31) / 32 * 32;  // 256-byte aligned block starts
     bh.tiles_x = (bh.mx - 2 + SBX - 1) / SBX;

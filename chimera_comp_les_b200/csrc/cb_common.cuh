@@ -33,6 +33,9 @@ struct DevCfg {
   // 1: every nvert value is k/4 with 0 <= k <= 255, so the stage kernel keeps
   // nvert as one exact byte per node in shared memory; 0: read from global
   int nvq;
+  // LES shock sensor (rhs.c:3333-3433): hybrid weights from per-node planes
+  int calc_sigma;
+  double s_x_min, s_y_min, s_z_min, ks;
 };
 
 // Host check of an nvert array for the byte code of DevCfg::nvq.
@@ -57,6 +60,7 @@ struct DevFields {
   // w carries the FP32 filter width (csi), aj (eta), 0 (zet)
   const float4 *met4[3];
   const double *gcl[3];      // mixed form: per-node metric divergence sum_d dh_d (FP64)
+  const double *sig[3];    // hybrid weights per node (only with the shock sensor)
   double *rhs[5];          // formRHS output (rhs mode only)
   unsigned *status;        // sticky status word
 };
@@ -71,10 +75,12 @@ __host__ __device__ __forceinline__ long long gstride(const DevCfg &c, int d) {
 
 __device__ __forceinline__ double ldg(const double *p) { return __ldg(p); }
 
-// Hybrid weight sigma of direction d at node (i,j,k) when the shock sensor is
-// off (rhs.c:3322-3441): every node starts at (s_x, s_y, s_z); interior nodes
-// then take y = z = min(z, y).  Ghost nodes carry the wrap-around image.
-__device__ __forceinline__ double sigma_at(const DevCfg &c, int d, int i, int j, int k) {
+// Hybrid weight sigma of direction d at node (i,j,k): from the sensor's
+// planes when it is on; otherwise (rhs.c:3322-3441) every node starts at
+// (s_x, s_y, s_z) and interior nodes then take y = z = min(z, y).  Ghost
+// nodes carry the wrap-around image.
+__device__ __forceinline__ double sigma_at(const DevCfg &c, const DevFields &F, int d, int i, int j, int k) {
+  if (c.calc_sigma) return ldg((d == 0 ? F.sig[0] : (d == 1 ? F.sig[1] : F.sig[2])) + gidx(c, i, j, k));
   if (d == 0) return c.s_x;
   // wrap ghost indices to their owned image (periodic directions only reach ghosts)
   int ii = i < 0 ? i + c.mx : (i >= c.mx ? i - c.mx : i);

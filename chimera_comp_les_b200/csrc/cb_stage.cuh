@@ -347,7 +347,7 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
     Fcen[4] = Uc * (ec + pa);
     Ufc = MIX ? Uc : R(0);
   }
-  const R sigma = R(sigma_at(c, d, gi, gj, gk));
+  const R sigma = R(sigma_at(c, F, d, gi, gj, gk));
 #pragma unroll
   for (int q = 0; q < 5; q++) Fc[q] = Fw[q] * (R(1.0) - sigma) + Fcen[q] * sigma;
   if (MIX) Fc[4] += href * (Ufw * (R(1.0) - sigma) + Ufc * sigma);
@@ -464,9 +464,9 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
 
   A[0] = A[1] = A[2] = R(0.);
   if (LES) {  // rhs.c:1677-1710
-    const R sa = R(sigma_at(c, d, gi, gj, gk));
+    const R sa = R(sigma_at(c, F, d, gi, gj, gk));
     const int bi = gi + (d == 0), bj = gj + (d == 1), bk = gk + (d == 2);
-    const R sb = R(sigma_at(c, d, bi, bj, bk));
+    const R sb = R(sigma_at(c, F, d, bi, bj, bk));
     R nut = R(0.5) * (R(ldg(F.nut + g0)) * sa + R(ldg(F.nut + g1)) * sb);
     const R rho_c = R(0.5) * (Rg.get(F_RHO, a) + Rg.get(F_RHO, b));
     const R sigma_c = R(0.5) * (sa + sb);

@@ -32,6 +32,8 @@ _OPT_MAP = {
     "-ENOorder": ("eno_order", int), "-central": ("central", int), "-isothermal": ("isothermal", int),
     "-s_x": ("s_x", float), "-s_y": ("s_y", float), "-s_z": ("s_z", float), "-ren": ("ren", float),
     "-Ma": ("ma", float), "-Pr": ("pr", float), "-gamma": ("gamma", float), "-dt": ("dt", float),
+    "-calc_sigma": ("calc_sigma", int), "-s_x_min": ("s_x_min", float), "-s_y_min": ("s_y_min", float),
+    "-s_z_min": ("s_z_min", float), "-sigma_thrsh": ("sigma_thrsh", float),
 }
 
 
@@ -50,14 +52,16 @@ class Block:
                  isothermal: int = 0, s_x: float = 1.0, s_y: float = 1.0, s_z: float = 1.0,
                  ren: float = 3000.0, ma: float = 2.81, pr: float = 0.72, gamma: float = 1.4,
                  dt: float = 0.01, st: float = 1.0, cs_const: float = 0.03, ci: float = 0.06,
-                 ratio: float = 0.0, precision: str = "fp64", device: int = 0):
+                 ratio: float = 0.0, precision: str = "fp64", device: int = 0, calc_sigma: int = 0,
+                 s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5):
         self.lib = _lib.load()
         cfg = CbConfig()
         self.lib.cb_config_default(C.byref(cfg), mx, my, mz)
         cfg.bctype = (C.c_int * 6)(*bctype)
         for k, v in dict(les=les, inviscid=inviscid, fluxorder=fluxorder, eno_order=eno_order, central=central,
                          isothermal=isothermal, s_x=s_x, s_y=s_y, s_z=s_z, ren=ren, ma=ma, pr=pr, gamma=gamma,
-                         dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device).items():
+                         dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device, calc_sigma=calc_sigma,
+                         s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh).items():
             setattr(cfg, k, v)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]
         self.cfg = cfg

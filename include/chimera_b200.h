@@ -69,6 +69,9 @@ typedef struct {
   double ratio;         /* channel forcing ratio (0 unless channel/wavy) */
   int precision;        /* CB_FP64 or CB_MIXED */
   int device;           /* CUDA device ordinal */
+  int calc_sigma;       /* -calc_sigma: pressure shock sensor for the hybrid weights (rhs.c:3333-3411) */
+  double s_x_min, s_y_min, s_z_min; /* -s_x_min/-s_y_min/-s_z_min: lower bounds of the sensor (default 0) */
+  double sigma_thrsh;   /* -sigma_thrsh: ks of the smoothness ratio (rhs.c:3323, default 1e-5) */
 } cb_config;
 
 /* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */

@@ -61,6 +61,11 @@ class Config:
     cs_const: float = 0.03
     ci: float = 0.06
     ratio: float = 0.0
+    calc_sigma: int = 0
+    s_x_min: float = 0.0
+    s_y_min: float = 0.0
+    s_z_min: float = 0.0
+    sigma_thrsh: float = 1e-5
 
     def ref_options(self) -> str:
         o = [
@@ -71,7 +76,9 @@ class Config:
             ("-ren", repr(float(self.ren))), ("-Ma", repr(float(self.ma))),
             ("-Pr", repr(float(self.pr))), ("-gamma", repr(float(self.gamma))),
             ("-dt", repr(float(self.dt))), ("-visT", 0), ("-twoD", 0), ("-TwoD", 0),
-            ("-calc_sigma", 0),
+            ("-calc_sigma", self.calc_sigma), ("-s_x_min", repr(float(self.s_x_min))),
+            ("-s_y_min", repr(float(self.s_y_min))), ("-s_z_min", repr(float(self.s_z_min))),
+            ("-sigma_thrsh", repr(float(self.sigma_thrsh))),
         ]
         return " ".join(f"{k} {v}" for k, v in o)
 
@@ -92,7 +99,8 @@ class _CCfg(C.Structure):
         ("s_x", C.c_double), ("s_y", C.c_double), ("s_z", C.c_double),
         ("ren", C.c_double), ("ma", C.c_double), ("pr", C.c_double), ("gamma", C.c_double),
         ("dt", C.c_double), ("st", C.c_double), ("cs_const", C.c_double), ("ci", C.c_double),
-        ("ratio", C.c_double),
+        ("ratio", C.c_double), ("calc_sigma", C.c_int),
+        ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double), ("sigma_thrsh", C.c_double),
     ]
 
 
@@ -166,6 +174,7 @@ class Oracle:
         L.cbo_metrics.argtypes = [C.c_void_p, PP, PP, PP, PP, D]
         L.cbo_eos.argtypes = [C.c_void_p, PP, D]
         L.cbo_sigma.argtypes = [C.c_void_p, PP]
+        L.cbo_sigma_sensor.argtypes = [C.c_void_p, PP, PP]
         L.cbo_rhs.argtypes = [C.c_void_p, PP, PP, PP, PP, D, D, D, PP, PP]
         L.cbo_rhs.restype = C.c_int
         L.cbo_eddy_viscosity.argtypes = [C.c_void_p, PP, PP, PP, PP, D, D, D]
@@ -195,9 +204,16 @@ class Oracle:
         self.lib.cbo_eos(self._cp, _ptrs(list(q)), _dp(p[0]))
         return p
 
-    def sigma(self) -> np.ndarray:
+    def sigma(self, q: Optional[np.ndarray] = None) -> np.ndarray:
+        """Hybrid weights at istage 0: constant (sensor off) or from the ghosted
+        stage state q with -calc_sigma 1."""
         s = self.zeros(3)
-        self.lib.cbo_sigma(self._cp, _ptrs(list(s)))
+        if self.cfg.calc_sigma:
+            if q is None:
+                raise ValueError("the shock sensor needs the stage state")
+            self.lib.cbo_sigma_sensor(self._cp, _ptrs(list(q)), _ptrs(list(s)))
+        else:
+            self.lib.cbo_sigma(self._cp, _ptrs(list(s)))
         return s
 
     def eddy_viscosity(self, qu: Optional[np.ndarray], met, nvert: np.ndarray, nut: np.ndarray):

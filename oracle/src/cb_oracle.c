@@ -213,6 +213,96 @@ void cbo_sigma(const cbo_config *c, double *const sig[3]) {
   for (int a = 0; a < 3; a++) cbo_fill_ghosts(c, sig[a]);
 }
 
+/* compute_ri / sigma_cent (rhs.c:2334-2358): smoothness ratio of two
+ * neighbouring differences and the tanh ramp from it. */
+static double compute_ri(double fR, double f0, double fL, double ks) {
+  double dfL = fL - f0, dfR = f0 - fR;
+  return (fabs(2 * dfL * dfR) + ks) / (dfL * dfL + dfR * dfR + ks);
+}
+static double sigma_cent(double fL, double f0, double fR, double fRR, double ks) {
+  double rL = compute_ri(fL, f0, fR, ks), rR = compute_ri(f0, fR, fRR, ks);
+  double r = (rR < rL) ? rR : rL;       /* PetscMin(rR, rL) */
+  double rd = 0.5;
+  double rmax = (rd < r) ? r : rd;      /* PetscMax(rd, r) */
+  return 0.5 + 0.5 * tanh(3.0 * (r - rd) / rmax) / tanh(3.0);
+}
+#define PMIN(a, b) (((a) < (b)) ? (a) : (b))
+#define PMAX(a, b) (((a) < (b)) ? (b) : (a))
+
+/* Hybrid weights with the sensor on (rhs.c:3328-3433): per interior node the
+ * ramp of the pressure smoothness along each direction (x for 2 < i < mx-4,
+ * y for 4 < j < my-4, z everywhere in a periodic k), clipped to
+ * [s_min, s]; a product filter of square roots of neighbour pairs; then the
+ * curvature rule and y = z = min(y, z).  Boundary nodes keep (s_x, s_y, s_z). */
+void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *const sig[3]) {
+  geom G = mkgeom(c);
+  double *p = (double *)malloc(G.n * sizeof(double));
+  double *ls[3];
+  for (int a = 0; a < 3; a++) ls[a] = (double *)malloc(G.n * sizeof(double));
+  cbo_eos(c, q, p);
+  const double ks = c->sigma_thrsh;
+  const ptrdiff_t si = 1, sj = G.m[0] + 4, sk = (ptrdiff_t)(G.m[0] + 4) * (G.m[1] + 4);
+  const int mx = G.m[0], my = G.m[1], mz = G.m[2];
+  for (size_t n = 0; n < G.n; n++) { sig[0][n] = c->s_x; sig[1][n] = c->s_y; sig[2][n] = c->s_z; }
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        ptrdiff_t n = IX(&G, i, j, k);
+        if (i < mx - 4 && i > 2) sig[0][n] = sigma_cent(p[n - si], p[n], p[n + si], p[n + 2 * si], ks);
+        sig[0][n] = PMIN(c->s_x, sig[0][n]);
+        sig[0][n] = PMAX(c->s_x_min, sig[0][n]);
+      }
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        ptrdiff_t n = IX(&G, i, j, k);
+        if (c->bctype[4] == 7 || (k < mz - 4 && k > 4))
+          sig[2][n] = sigma_cent(p[n - sk], p[n], p[n + sk], p[n + 2 * sk], ks);
+        sig[2][n] = PMIN(c->s_z, sig[2][n]);
+        sig[2][n] = PMAX(c->s_z_min, sig[2][n]);
+      }
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        ptrdiff_t n = IX(&G, i, j, k);
+        if (j < my - 4 && j > 4) sig[1][n] = sigma_cent(p[n - sj], p[n], p[n + sj], p[n + 2 * sj], ks);
+        sig[1][n] = PMIN(c->s_y, sig[1][n]);
+        sig[1][n] = PMAX(c->s_y_min, sig[1][n]);
+      }
+  /* filter with the ghosted copy (rhs.c:3382-3407) */
+  for (int a = 0; a < 3; a++) {
+    memcpy(ls[a], sig[a], G.n * sizeof(double));
+    cbo_fill_ghosts(c, ls[a]);
+  }
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        ptrdiff_t n = IX(&G, i, j, k);
+        for (int a = 0; a < 3; a++)
+          sig[a][n] *= sqrt(ls[a][n - sj] * ls[a][n]) * sqrt(ls[a][n - sk] * ls[a][n + sk]) *
+                       sqrt(ls[a][n - si] * ls[a][n + si]);
+      }
+  /* curvature rule and y = z = min (rhs.c:3415-3433) */
+  for (int a = 0; a < 3; a++) {
+    memcpy(ls[a], sig[a], G.n * sizeof(double));
+    cbo_fill_ghosts(c, ls[a]);
+  }
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        ptrdiff_t n = IX(&G, i, j, k);
+        if (j < my - 4 && j > 4 && ls[1][n - sj] + ls[1][n + sj] - 2. * ls[1][n] < 0.0)
+          sig[1][n] = (ls[1][n - sj] * ls[1][n] * ls[1][n]);
+        if (k < mz - 4 && k > 4 && ls[2][n - sk] + ls[2][n + sk] - 2. * ls[2][n] < 0.0)
+          sig[2][n] = (ls[2][n - sk] * ls[2][n + sk] * ls[2][n]);
+        sig[2][n] = PMIN(sig[2][n], sig[1][n]);
+        sig[1][n] = sig[2][n];
+      }
+  for (int a = 0; a < 3; a++) cbo_fill_ghosts(c, sig[a]);
+  free(p);
+  for (int a = 0; a < 3; a++) free(ls[a]);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Reconstructions  (rhs.c:2256-2307, 2359-2461, 2498-2568)                  */
 /* ------------------------------------------------------------------------ */
@@ -815,12 +905,13 @@ int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const
   double *rhs[5], *qn[5], *sig[3];
   for (int a = 0; a < 5; a++) { rhs[a] = buf + G.n * a; qn[a] = buf + G.n * (5 + a); }
   for (int a = 0; a < 3; a++) sig[a] = buf + G.n * (10 + a);
-  if (c->les) cbo_sigma(c, sig);
+  if (c->les && !c->calc_sigma) cbo_sigma(c, sig);
   int err = 0;
   for (int step = 0; step < nsteps && !err; step++) {
     if (c->les && !c->inviscid)
       cbo_eddy_viscosity(c, *have_uc ? (const double *const *)quc : NULL, csi, eta, zet, aj, nvert, nut);
     for (int s = 0; s < ns && !err; s++) {
+      if (c->les && c->calc_sigma && s == 0) cbo_sigma_sensor(c, (const double *const *)q, sig); /* istage 0 */
       err = cbo_rhs(c, (const double *const *)q, csi, eta, zet, aj, nvert, nut, (const double *const *)sig, rhs);
       if (err) break;
       if (!c->inviscid) { /* CalcUCat inside formRHS keeps this stage's input */

@@ -34,6 +34,9 @@ typedef struct {
   double cs_const;         /* constant Smagorinsky coefficient (CS field value) */
   double ci;               /* Yoshizawa constant CI */
   double ratio;            /* channel forcing ratio (0 unless channel/wavy) */
+  int calc_sigma;          /* -calc_sigma: pressure shock sensor for the hybrid weights */
+  double s_x_min, s_y_min, s_z_min; /* -s_x_min/-s_y_min/-s_z_min: lower bounds of the sensor */
+  double sigma_thrsh;      /* -sigma_thrsh: ks of the smoothness ratio (default 1e-5) */
 } cbo_config;
 
 /* Fill the two ghost layers of each periodic direction of one padded plane
@@ -51,6 +54,10 @@ void cbo_eos(const cbo_config *c, const double *const q[5], double *p);
 /* Hybrid weights field (3 planes) as formConvectionLES sets it at istage 0
  * when the sensor is off. */
 void cbo_sigma(const cbo_config *c, double *const sig[3]);
+
+/* Hybrid weights with the pressure shock sensor (-calc_sigma 1), as
+ * formConvectionLES sets them at istage 0 from the ghosted stage state q. */
+void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *const sig[3]);
 
 /* formRHS: q = ghosted stage state, nut/sig may be NULL when les == 0.
  * rhs: 5 padded planes; interior nodes written, every other node zeroed. */

@@ -33,7 +33,7 @@ def oracle_run(cfg, coords, q, nvert, steps=0):
     met = ora.metrics(O.to_padded(cfg, coords))
     nvp = ora.fill_ghosts(O.to_padded(cfg, nvert))
     st = ora.initial_state(q)
-    sig = ora.sigma() if cfg.les else None
+    sig = ora.sigma(st["q"]) if cfg.les else None
     nut = ora.zeros(1)
     out = {"metrics": {k: O.from_padded(v) for k, v in met.items()}}
     if cfg.les and not cfg.inviscid:
@@ -53,7 +53,8 @@ def gpu_block(cfg, precision="fp64"):
                  fluxorder=cfg.fluxorder, eno_order=cfg.eno_order, central=cfg.central,
                  isothermal=cfg.isothermal, s_x=cfg.s_x, s_y=cfg.s_y, s_z=cfg.s_z, ren=cfg.ren, ma=cfg.ma,
                  pr=cfg.pr, gamma=cfg.gamma, dt=cfg.dt, st=cfg.st, cs_const=cfg.cs_const, ci=cfg.ci,
-                 ratio=cfg.ratio, precision=precision)
+                 ratio=cfg.ratio, precision=precision, calc_sigma=cfg.calc_sigma, s_x_min=cfg.s_x_min,
+                 s_y_min=cfg.s_y_min, s_z_min=cfg.s_z_min, sigma_thrsh=cfg.sigma_thrsh)
 
 
 def per_field_rel_l2(a, b):

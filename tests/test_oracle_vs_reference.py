@@ -59,3 +59,53 @@ def test_restatement_bitexact_vs_reference(les, inv, fo, mask):
     st = ora.initial_state(q)
     ora.steps(2, st, met, nvp)
     assert np.array_equal(O.from_padded(st["q"]), ref2.Q())
+
+
+def _state_with_jump(shape, seed):
+    """Smooth random state plus a pressure/density step, so the shock sensor
+    ramps between its bounds (rhs.c:2334-2358)."""
+    q = W.random_smooth_state(shape, seed=seed)
+    mz, my, mx = shape
+    z, y, x = np.meshgrid(np.arange(mz), np.arange(my), np.arange(mx), indexing="ij")
+    jump = (x + 0.7 * y + 0.4 * z) > 0.55 * (mx + my + mz) * 0.6
+    q[..., 0] = np.where(jump, 1.6 * q[..., 0], q[..., 0])
+    q[..., 4] = np.where(jump, 1.9 * q[..., 4], q[..., 4])
+    return q
+
+
+@pytest.mark.parametrize("inv,smin", [(0, (0.0, 0.0, 0.0)), (1, (0.2, 0.1, 0.3))])
+def test_shock_sensor_restatement_bitexact_vs_reference(inv, smin):
+    n = (17, 16, 15)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=1, inviscid=inv, fluxorder=3, s_x=0.9, s_y=0.8,
+                   s_z=1.0, ren=250., ma=0.3, pr=0.71, dt=0.002, calc_sigma=1, s_x_min=smin[0], s_y_min=smin[1],
+                   s_z_min=smin[2])
+    q = _state_with_jump(shape, 5)
+    nv = np.zeros(shape)
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q)
+    ora = O.Oracle(cfg)
+    met = ora.metrics(O.to_padded(cfg, coords))
+    nvp = ora.fill_ghosts(O.to_padded(cfg, nv))
+    st = ora.initial_state(q)
+    nut = ora.zeros(1)
+    if not inv:
+        ref.calc_ucat()
+        ref.eddy_viscosity()
+        ora.eddy_viscosity(st["q"], met, nvp, nut)
+    r_ref = ref.rhs(0)
+    sig = ora.sigma(st["q"])
+    s_ref = O.local_to_padded(cfg, ref.local("lsigma", 3), 3)
+    assert np.array_equal(sig, s_ref)
+    assert sig[0].min() < 0.9 * cfg.s_x  # the ramp fired somewhere
+    r_ora = O.from_padded(ora.rhs(st["q"], met, nvp, nut, sig))
+    assert np.array_equal(r_ora, r_ref)
+    ref2 = O.RefOracle(cfg, coords)
+    ref2.set_nvert(nv)
+    ref2.set_state(q)
+    ref2.steps(2)
+    st = ora.initial_state(q)
+    ora.steps(2, st, met, nvp)
+    assert np.array_equal(O.from_padded(st["q"]), ref2.Q())
