@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -58,6 +59,7 @@ struct cb_ctx {
   double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
   double **ptab = nullptr;    // device pointer tables
   unsigned *status = nullptr;
+  bool fully_periodic = true;  // every face bctype 7: one fused periodic BC kernel
   int cur = 0;                // buffer with the current Q (== Qold between steps)
   int uc = -1;                // buffer of the last CalcUCat state, -1: none
   bool have_grid = false, have_state = false;
@@ -275,7 +277,18 @@ static int enqueue_step(cb_ctx *c) {
     }
     {
       TimedScope ts(c, false);
-      bc_periodic_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, F);
+      if (c->fully_periodic) {
+        bc_periodic_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, F);
+      } else {  // FormBCS with boundary codes (rhs.c:477-1227)
+        bc_combine_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, F, s, alfa, beta, adt);
+        const long long face = (long long)std::max(c->dc.mx, c->dc.my) * std::max(c->dc.my, c->dc.mz);
+        for (int dir = 0; dir < 3; dir++)
+          bc_face_kernel<<<grid_for(c, face), 256, 0, c->stream>>>(c->dc, F, dir, alfa);
+        for (int dir = 0; dir < 3; dir++)
+          if (c->dc.bctype[2 * dir] == 7)
+            bc_periodic_dir_kernel<<<grid_for(c, face), 256, 0, c->stream>>>(c->dc, F, dir);
+        ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, c->ptab + 5 * out, 5);
+      }
     }
     CB_CUDA(c, cudaGetLastError());
     if (!c->cfg.inviscid) c->uc = in;  // CalcUCat inside formRHS keeps the stage input
@@ -342,8 +355,18 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
     return code;
   };
   if (cfg->mx < 5 || cfg->my < 5 || cfg->mz < 5) return bail(CB_E_ARG, "grid must have at least 5 nodes per direction");
-  for (int b = 0; b < 6; b++)
-    if (cfg->bctype[b] != 7) return bail(CB_E_UNSUPPORTED, "only fully periodic blocks (bctype 7) are built");
+  {
+    const int *bc = cfg->bctype;
+    for (int d = 0; d < 3; d++)
+      if ((bc[2 * d] == 7) != (bc[2 * d + 1] == 7))
+        return bail(CB_E_UNSUPPORTED, "a periodic direction needs bctype 7 on both faces");
+    if (bc[4] == 52 || bc[4] == 47)
+      return bail(CB_E_UNSUPPORTED, "boundary codes 52 and 47 (profile inlets from the coordinates) are not built");
+    if ((bc[2] == 1 || bc[3] == 1) && cfg->isothermal == 2)
+      return bail(CB_E_UNSUPPORTED, "the characteristic isothermal wall (isothermal 2) is not built");
+    c->fully_periodic = true;
+    for (int b = 0; b < 6; b++) c->fully_periodic = c->fully_periodic && bc[b] == 7;
+  }
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3) return bail(CB_E_ARG, "fluxorder must be 1, 2 or 3");
   if (cfg->eno_order != 2 && cfg->eno_order != 3) return bail(CB_E_ARG, "ENOorder must be 2 or 3");
   if (cfg->les != 0 && cfg->les != 1) return bail(CB_E_UNSUPPORTED, "only les 0 or 1 (constant Smagorinsky) is built");
@@ -459,7 +482,12 @@ long long cb_interior_nodes(const cb_ctx *c) {
 int cb_stages(const cb_ctx *c) { return c ? c->cfg.fluxorder : 0; }
 int cb_launches_per_step(const cb_ctx *c) {
   if (!c) return 0;
-  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + 2 * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0);
+  int per_stage = 2;
+  if (!c->fully_periodic) {
+    per_stage = 1 + 1 + 3 + 1;
+    for (int d = 0; d < 3; d++) per_stage += c->cfg.bctype[2 * d] == 7;
+  }
+  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0);
 }
 
 static int upload_planes(cb_ctx *c, const double *host, int nc, int pt_first, bool pinned_hint) {

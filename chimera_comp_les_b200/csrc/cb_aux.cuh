@@ -80,6 +80,214 @@ static __global__ void bc_periodic_kernel(const DevCfg c, DevFields F) {
   }
 }
 
+// ------------------------------------------------ non-periodic FormBCS --
+// Blocks with boundary codes other than 7 (FormBCS rhs.c:477-1227), after the
+// stage kernel has updated the interior: (1) the RK update of the boundary
+// layer itself (the reference combines the whole global vector; Rhs is zero
+// there), (2) the face codes in the reference's order i, j, k, (3) the
+// periodic copies of the periodic directions from the stale stage input,
+// (4) the ghost wrap.  Pressures are the stage input's EOS (lP before
+// EqOfState refreshes it).
+
+// (1) owned non-interior nodes: istage 0 Qold + adt*0, else beta Qold + adt*0 + alfa Qin
+static __global__ void bc_combine_kernel(const DevCfg c, DevFields F, int istage, double alfa, double beta, double adt) {
+  const long long total = shell_count(c);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    shell_node(c, t, i, j, k);
+    if (i < 0 || i >= c.mx || j < 0 || j >= c.my || k < 0 || k >= c.mz) continue;
+    const long long n = gidx(c, i, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      const double qo = F.qold[q][n];
+      F.qout[q][n] = (istage == 0) ? qo + adt * 0.0 : beta * qo + adt * 0.0 + alfa * F.q[q][n];
+    }
+  }
+}
+
+__device__ __forceinline__ double lp_at(const DevCfg &c, const DevFields &F, long long n) {
+  const double r = F.q[0][n];
+  return r != 0.0 ? (c.gamma - 1) * (F.q[4][n] - 0.5 * (F.q[1][n] * F.q[1][n] + F.q[2][n] * F.q[2][n] + F.q[3][n] * F.q[3][n]) / r)
+                  : 0.0;
+}
+
+// (2) one direction's two faces; a thread per face node (lo and hi, as the
+// reference's loop body)
+static __global__ void bc_face_kernel(const DevCfg c, DevFields F, int dir, double alfa) {
+  double *const *q = F.qout;
+  const int *bc = c.bctype;
+  const double g = c.gamma, Ma = c.ma;
+  const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
+  int na, nb, a0 = 0;
+  if (dir == 0) { na = c.my; nb = c.mz; }
+  else if (dir == 1) { na = c.mx; nb = c.mz; }
+  else { na = c.mx; a0 = (bc[2] == 1) ? 1 : 0; nb = ((bc[3] == 1) ? c.my - 1 : c.my) - a0; }
+  const long long total = (long long)na * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t % na), b = (int)(t / na);
+    if (dir == 0) {  // rhs.c:601-636: j = a, k = b
+      long long n = gidx(c, 0, a, b);
+      if (bc[0] == 3) {
+        q[0][n] = q[0][n + si]; q[1][n] = 0.; q[2][n] = q[2][n + si]; q[3][n] = q[3][n + si]; q[4][n] = q[4][n + si];
+      } else if (bc[0] == 51) {
+        q[0][n] = 0.445; q[1][n] = 0.311; q[2][n] = 0.; q[3][n] = 0.; q[4][n] = 8.928;
+      }
+      n = gidx(c, c.mx - 1, a, b);
+      if (bc[1] == 3) {
+        q[0][n] = q[0][n - si]; q[1][n] = 0.; q[2][n] = q[2][n - si]; q[3][n] = q[3][n - si]; q[4][n] = q[4][n - si];
+      } else if (bc[0] == 51) {  // the high-i Lax state is keyed on bctype[0] (rhs.c:627)
+        q[0][n] = 0.5; q[1][n] = 0.; q[2][n] = 0.; q[3][n] = 0.; q[4][n] = 1.4275;
+      }
+    } else if (dir == 1) {  // rhs.c:639-835: i = a, k = b
+      long long n = gidx(c, a, 0, b);
+      if (bc[2] == 3) {
+        q[0][n] = q[0][n + sj]; q[1][n] = q[1][n + sj]; q[2][n] = 0.; q[3][n] = q[3][n + sj]; q[4][n] = q[4][n + sj];
+      } else if (bc[2] == 10) {
+        q[0][n] = q[0][n + sj]; q[1][n] = 0.; q[2][n] = q[2][n + sj]; q[3][n] = q[3][n + sj]; q[4][n] = q[4][n + sj];
+      } else if (bc[2] == 1) {
+        q[1][n] = 0.0; q[2][n] = 0.0; q[3][n] = 0.0;
+        const double lpn = lp_at(c, F, n + sj);
+        q[0][n] = lpn * (g * Ma * Ma);
+        q[4][n] = lpn / (g - 1);
+      }
+      n = gidx(c, a, c.my - 1, b);
+      if (bc[3] == 3) {
+        q[0][n] = q[0][n - sj]; q[1][n] = q[1][n - sj]; q[2][n] = 0.; q[3][n] = q[3][n - sj]; q[4][n] = q[4][n - sj];
+      } else if (bc[3] == 10) {
+        q[0][n] = q[0][n - sj]; q[1][n] = 0.; q[2][n] = q[2][n - sj]; q[3][n] = q[3][n - sj]; q[4][n] = q[4][n - sj];
+      } else if (bc[3] == 1) {
+        q[1][n] = 0.0; q[2][n] = 0.0; q[3][n] = 0.0;
+        if (c.isothermal == 1) q[0][n] = lp_at(c, F, n) * (g * Ma * Ma);
+        else q[0][n] = q[0][n - sj];
+        q[4][n] = lp_at(c, F, n - sj) / (g - 1.0);
+      }
+    } else {  // rhs.c:840-1087: i = a, j = a0 + b
+      const int j = a0 + b;
+      long long n = gidx(c, a, j, 0);
+      if (bc[4] == 3) {
+        q[0][n] = q[0][n + sk]; q[1][n] = q[1][n + sk]; q[2][n] = q[2][n + sk]; q[3][n] = 0.; q[4][n] = q[4][n + sk];
+      } else if (bc[4] == 55) {  // u = Ma, rho = gamma (rhs.c:837)
+        const double rho = g, u = Ma;
+        q[0][n] = rho; q[3][n] = rho * u; q[4][n] = 0.5 * rho * u * u + 1. / (g - 1.);
+      } else if (bc[4] == 44) {
+        q[0][n] = q[0][n + sk]; q[1][n] = 0.; q[2][n] = 0.; q[3][n] = q[3][n + sk]; q[4][n] = q[4][n + sk];
+      } else if (bc[4] == 45) {
+        q[0][n] = 1.; q[3][n] = 1.; q[4][n] = .5 + 1. / (Ma * Ma * g * (g - 1.));
+      } else if (bc[4] == 51) {
+        q[0][n] = 0.445; q[3][n] = 0.311; q[4][n] = 8.928;
+      } else if (bc[4] == 10) {
+        q[0][n] = 1.; q[1][n] = 0.; q[2][n] = 0.; q[3][n] = 1.; q[4][n] = 1. / 0.4 + 0.5;
+      }
+      n = gidx(c, a, j, c.mz - 1);
+      const long long m1 = n - sk, m2 = n - 2 * sk;
+      if (bc[5] == 3) {
+        q[0][n] = q[0][m1]; q[1][n] = q[1][m1]; q[2][n] = q[2][m1]; q[3][n] = 0.; q[4][n] = q[4][m1];
+      } else if (bc[5] == 44) {
+        q[0][n] = q[0][m1]; q[1][n] = 0.; q[2][n] = 0.; q[3][n] = q[3][m1]; q[4][n] = q[4][m1];
+      } else if (bc[5] == 45) {
+        q[0][n] = q[0][m1]; q[1][n] = q[1][m1]; q[2][n] = q[2][m1]; q[3][n] = q[3][m1]; q[4][n] = q[4][m1];
+      } else if (bc[5] == 49) {  // characteristic (rhs.c:1003-1042)
+        double Vn, Rplus, Rminus, sv, pOverrho, pp;
+        const double lp1 = lp_at(c, F, m1);
+        Vn = q[3][m1] / q[0][m1];
+        double a_sound = sqrt(g * lp1 / q[0][m1]);
+        const double lambda1 = Vn + a_sound, lambda2 = Vn - a_sound;
+        if (Vn < 0.) {
+          if (lambda1 < 0) {
+            q[1][n] = 0.; q[2][n] = 0.;
+            Rplus = Vn + 2 / Ma / (g - 1.);
+            Rminus = Vn - 2 / Ma / (g - 1.);
+            sv = 1. / (Ma * Ma * g);
+          } else {
+            Rplus = Vn + 2 * a_sound / (g - 1.);
+            Rminus = Vn - 2 / Ma / (g - 1.);
+            q[1][n] = 0.; q[2][n] = 0.;
+            sv = 1. / (Ma * Ma * g);
+          }
+        } else {
+          if (lambda2 >= 0) {
+            Rplus = Vn + 2 * a_sound / (g - 1.);
+            Rminus = Vn - 2 * a_sound / (g - 1.);
+            q[1][n] = q[1][m1];
+            q[2][n] = q[0][m1];  // rhoV takes rho (rhs.c:1022)
+            sv = lp1 / pow(q[0][m1], g);
+          } else {
+            Rminus = Vn - 2 / Ma / (g - 1.);
+            Rplus = Vn + 2 * a_sound / (g - 1.);
+            q[1][n] = q[1][m1]; q[2][n] = q[2][m1];
+            sv = lp1 / pow(q[0][m1], g);
+          }
+        }
+        Vn = 0.5 * (Rplus + Rminus);
+        a_sound = 0.25 * (g - 1.) * (Rplus - Rminus);
+        pOverrho = a_sound * a_sound / (g);
+        q[0][n] = pow(pOverrho / sv, 1. / (g - 2.));  // gamma-2 (rhs.c:1036)
+        q[3][n] = q[0][n] * Vn;
+        pp = pOverrho * q[0][n];
+        q[4][n] = pp / (g - 1.) + 0.5 * (q[1][n] * q[1][n] + q[2][n] * q[2][n] + q[3][n] * q[3][n]) * q[0][n];
+      } else if (bc[5] == 51) {
+        q[0][n] = 0.5; q[1][n] = 0.; q[2][n] = 0.; q[3][n] = 0.; q[4][n] = 1.4275;
+      } else if (bc[5] == 10) {
+        q[0][n] = 1.; q[1][n] = 0.; q[2][n] = 0.; q[3][n] = 1.; q[4][n] = 1 / 0.4 + 0.5;
+      } else if (bc[5] == 8) {  // subsonic non-reflecting outflow (rhs.c:1056-1086)
+        const double *const *lq = F.q;
+        const double lpn = lp_at(c, F, n), lp1 = lp_at(c, F, m1), lp2 = lp_at(c, F, m2);
+        const double a_sound = sqrt(g * lp1 / lq[0][m1]);
+        const double AA = q[3][m1] / q[0][m1];
+        const double Lam0 = AA - a_sound, Lam4 = AA + a_sound;
+        (void)Lam0;
+        const double L0 = 0;
+        const double L1 = AA * F.aj[m1] * F.met[2][2][m1] * (a_sound * a_sound * (lq[0][m1] - lq[0][m2]) - (lpn - lp1));
+        const double L2 = AA * F.aj[m1] * F.met[2][2][m1] * (lq[1][m1] / q[0][m1] - lq[1][m2] / q[0][m1]);
+        const double L3 = AA * F.aj[m1] * F.met[2][2][m1] * (lq[2][m1] / q[0][m1] - lq[2][m2] / q[0][m2]);
+        const double L4 = Lam4 * F.aj[m1] * F.met[2][2][m1] *
+                          ((lp1 - lp2) + q[0][m1] * a_sound * (lq[3][m1] / q[0][m1] - lq[3][m2] / q[0][m2]));
+        (void)L2; (void)L3;
+        const double d0 = 1. / (a_sound * a_sound) * (L1 + 0.5 * (L4 + L0));
+        const double d1 = 0.5 * (L0 + L4);
+        const double d2 = 0.5 / (q[0][m1] * a_sound) * (L4 - L0);
+        q[0][n] = F.qold[0][n] - c.dt * alfa * d0;
+        q[4][n] = F.qold[4][n] - c.dt * alfa *
+                                     (0.5 * d0 * (lq[3][m1] / q[0][m1] * lq[3][m1] / q[0][m1]) + d1 / (g - 1.) +
+                                      lq[3][m1] * d2);
+        q[3][n] = F.qold[3][n] - c.dt * alfa * (lq[3][m1] / q[0][m1] * d0 + q[0][m1] * d2);
+      }
+    }
+  }
+}
+
+// (3) periodic copies of one periodic direction with the reference's guards
+// (i faces: 0 < k, 0 < j; j faces: j = 0 for k > 0, j = my-1 for 0 < k < mz-1;
+// k faces unguarded), from the stale ghosted stage input.
+static __global__ void bc_periodic_dir_kernel(const DevCfg c, DevFields F, int dir) {
+  int na, nb;
+  if (dir == 0) { na = c.my; nb = c.mz; }
+  else if (dir == 1) { na = c.mx; nb = c.mz; }
+  else { na = c.mx; nb = c.my; }
+  const long long s = gstride(c, dir);
+  const long long total = (long long)na * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t % na), b = (int)(t / na);
+    long long lo, hi;
+    bool do_lo = true, do_hi = true;
+    if (dir == 0) {
+      lo = gidx(c, 0, a, b); hi = gidx(c, c.mx - 1, a, b);
+      do_lo = do_hi = (a > 0 && b > 0);
+    } else if (dir == 1) {
+      lo = gidx(c, a, 0, b); hi = gidx(c, a, c.my - 1, b);
+      do_lo = b > 0;
+      do_hi = b > 0 && b < c.mz - 1;
+    } else {
+      lo = gidx(c, a, b, 0); hi = gidx(c, a, b, c.mz - 1);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      if (do_lo) F.qout[q][lo] = F.q[q][lo - 2 * s];
+      if (do_hi) F.qout[q][hi] = F.q[q][hi + 2 * s];
+    }
+  }
+}
+
 // Ghost layers of periodic planes from their owned images (DMGlobalToLocal).
 static __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, int nplanes) {
   const long long total = shell_count(c);

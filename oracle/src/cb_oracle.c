@@ -893,6 +893,218 @@ int cbo_bc_periodic(const cbo_config *c, const double *const qin[5], double *con
 }
 
 /* ------------------------------------------------------------------------ */
+/* FormBCS  (rhs.c:477-1227)                                                 */
+/* q: the stage output, every node already combined by the RK update; lq:    */
+/* the stale ghosted stage input (its pressure lp from the EOS); qold: the   */
+/* step's initial state.  Face order i, j, k, then the periodic copies, then */
+/* the wrap of periodic directions (DMGlobalToLocal).  Codes: i 3, 51; j 3,   */
+/* 10, 1 (isothermal 0/1); k-lo 3, 55, 44, 45, 51, 10; k-hi 3, 44, 45, 49,   */
+/* 51, 10, 8; 7 periodic; any other code leaves the face as the RK update    */
+/* left it, as in the reference.  Not restated (returns 5): k-lo 52 and 47   */
+/* (they read the coordinates and the step index) and the characteristic    */
+/* isothermal wall (isothermal 2 with a j wall).                             */
+/* ------------------------------------------------------------------------ */
+int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], const double *const qold[5],
+                const double *const zet[3], const double *aj, double *const q[5]) {
+  geom G = mkgeom(c);
+  const int mx = G.m[0], my = G.m[1], mz = G.m[2];
+  const int *bc = c->bctype;
+  if (bc[4] == 52 || bc[4] == 47) return 5;
+  if ((bc[2] == 1 || bc[3] == 1) && c->isothermal == 2) return 5;
+  if ((bc[0] == 7) != (bc[1] == 7) || (bc[2] == 7) != (bc[3] == 7) || (bc[4] == 7) != (bc[5] == 7)) return 5;
+  const ptrdiff_t si = G.s[0], sj = G.s[1], sk = G.s[2];
+  const double g = c->gamma, Ma = c->ma;
+  double *lp = (double *)malloc(G.n * sizeof(double));
+  cbo_eos(c, lq, lp);
+#define RO(n) q[0][n]
+#define RU(n) q[1][n]
+#define RV(n) q[2][n]
+#define RW(n) q[3][n]
+#define RE(n) q[4][n]
+  /* i BC (rhs.c:601-636) */
+  for (int k = 0; k < mz; k++)
+    for (int j = 0; j < my; j++) {
+      ptrdiff_t n = IX(&G, 0, j, k);
+      if (bc[0] == 3) {
+        RO(n) = RO(n + si); RU(n) = 0.; RV(n) = RV(n + si); RW(n) = RW(n + si); RE(n) = RE(n + si);
+      } else if (bc[0] == 51) {
+        RO(n) = 0.445; RU(n) = 0.311; RV(n) = 0.; RW(n) = 0.; RE(n) = 8.928;
+      }
+      n = IX(&G, mx - 1, j, k);
+      if (bc[1] == 3) {
+        RO(n) = RO(n - si); RU(n) = 0.; RV(n) = RV(n - si); RW(n) = RW(n - si); RE(n) = RE(n - si);
+      } else if (bc[0] == 51) { /* quirk: the high-i Lax state is keyed on bctype[0] (rhs.c:627) */
+        RO(n) = 0.5; RU(n) = 0.; RV(n) = 0.; RW(n) = 0.; RE(n) = 1.4275;
+      }
+    }
+  /* j BC (rhs.c:639-835) */
+  for (int k = 0; k < mz; k++)
+    for (int i = 0; i < mx; i++) {
+      ptrdiff_t n = IX(&G, i, 0, k);
+      if (bc[2] == 3) {
+        RO(n) = RO(n + sj); RU(n) = RU(n + sj); RV(n) = 0.; RW(n) = RW(n + sj); RE(n) = RE(n + sj);
+      } else if (bc[2] == 10) {
+        RO(n) = RO(n + sj); RU(n) = 0.; RV(n) = RV(n + sj); RW(n) = RW(n + sj); RE(n) = RE(n + sj);
+      } else if (bc[2] == 1) {
+        RU(n) = 0.0; RV(n) = 0.0; RW(n) = 0.0;
+        lp[n] = lp[n + sj];
+        RO(n) = lp[n] * (g * Ma * Ma);
+        RE(n) = lp[n] / (g - 1);
+      }
+      n = IX(&G, i, my - 1, k);
+      if (bc[3] == 3) {
+        RO(n) = RO(n - sj); RU(n) = RU(n - sj); RV(n) = 0.; RW(n) = RW(n - sj); RE(n) = RE(n - sj);
+      } else if (bc[3] == 10) {
+        RO(n) = RO(n - sj); RU(n) = 0.; RV(n) = RV(n - sj); RW(n) = RW(n - sj); RE(n) = RE(n - sj);
+      } else if (bc[3] == 1) {
+        RU(n) = 0.0; RV(n) = 0.0; RW(n) = 0.0;
+        if (c->isothermal == 1) {
+          RO(n) = lp[n] * (g * Ma * Ma);
+          lp[n] = lp[n - sj];
+        } else {
+          RO(n) = RO(n - sj);
+          lp[n] = lp[n - sj];
+        }
+        RE(n) = lp[n] / (g - 1.0);
+      }
+    }
+  /* k BC (rhs.c:840-1087) */
+  const int ls = (bc[2] == 1) ? 1 : 0, le = (bc[3] == 1) ? my - 1 : my;
+  const double u55 = Ma, rho55 = g;
+  for (int j = ls; j < le; j++)
+    for (int i = 0; i < mx; i++) {
+      ptrdiff_t n = IX(&G, i, j, 0);
+      if (bc[4] == 3) {
+        RO(n) = RO(n + sk); RU(n) = RU(n + sk); RV(n) = RV(n + sk); RW(n) = 0.; RE(n) = RE(n + sk);
+      } else if (bc[4] == 55) {
+        RO(n) = rho55; RW(n) = rho55 * u55; RE(n) = 0.5 * rho55 * u55 * u55 + 1. / (g - 1.);
+      } else if (bc[4] == 44) {
+        RO(n) = RO(n + sk); RU(n) = 0.; RV(n) = 0.; RW(n) = RW(n + sk); RE(n) = RE(n + sk);
+      } else if (bc[4] == 45) {
+        RO(n) = 1.; RW(n) = 1.; RE(n) = .5 + 1. / (Ma * Ma * g * (g - 1.));
+      } else if (bc[4] == 51) {
+        RO(n) = 0.445; RW(n) = 0.311; RE(n) = 8.928;
+      } else if (bc[4] == 10) {
+        RO(n) = 1.; RU(n) = 0.; RV(n) = 0.; RW(n) = 1.; RE(n) = 1. / 0.4 + 0.5;
+      }
+      n = IX(&G, i, j, mz - 1);
+      const ptrdiff_t m1 = n - sk, m2 = n - 2 * sk;
+      if (bc[5] == 3) {
+        RO(n) = RO(m1); RU(n) = RU(m1); RV(n) = RV(m1); RW(n) = 0.; RE(n) = RE(m1);
+      } else if (bc[5] == 44) {
+        RO(n) = RO(m1); RU(n) = 0.; RV(n) = 0.; RW(n) = RW(m1); RE(n) = RE(m1);
+      } else if (bc[5] == 45) {
+        RO(n) = RO(m1); RU(n) = RU(m1); RV(n) = RV(m1); RW(n) = RW(m1); RE(n) = RE(m1);
+      } else if (bc[5] == 49) { /* characteristic (rhs.c:1003-1042) */
+        double Vn, Rplus, Rminus, lambda1, lambda2, sv, pOverrho, pp, a_sound;
+        Vn = RW(m1) / RO(m1);
+        a_sound = sqrt(g * lp[m1] / RO(m1));
+        lambda1 = Vn + a_sound;
+        lambda2 = Vn - a_sound;
+        if (Vn < 0.) {
+          if (lambda1 < 0) {
+            RU(n) = 0.; RV(n) = 0.;
+            Rplus = Vn + 2 / Ma / (g - 1.);
+            Rminus = Vn - 2 / Ma / (g - 1.);
+            sv = 1. / (Ma * Ma * g);
+          } else {
+            Rplus = Vn + 2 * a_sound / (g - 1.);
+            Rminus = Vn - 2 / Ma / (g - 1.);
+            RU(n) = 0.; RV(n) = 0.;
+            sv = 1. / (Ma * Ma * g);
+          }
+        } else {
+          if (lambda2 >= 0) {
+            Rplus = Vn + 2 * a_sound / (g - 1.);
+            Rminus = Vn - 2 * a_sound / (g - 1.);
+            RU(n) = RU(m1);
+            RV(n) = RO(m1); /* quirk: rhoV takes rho (rhs.c:1022) */
+            sv = lp[m1] / pow(RO(m1), g);
+          } else {
+            Rminus = Vn - 2 / Ma / (g - 1.);
+            Rplus = Vn + 2 * a_sound / (g - 1.);
+            RU(n) = RU(m1); RV(n) = RV(m1);
+            sv = lp[m1] / pow(RO(m1), g);
+          }
+        }
+        Vn = 0.5 * (Rplus + Rminus);
+        a_sound = 0.25 * (g - 1.) * (Rplus - Rminus);
+        pOverrho = a_sound * a_sound / (g);
+        RO(n) = pow(pOverrho / sv, 1. / (g - 2.)); /* quirk: gamma-2 (rhs.c:1036) */
+        RW(n) = RO(n) * Vn;
+        pp = pOverrho * RO(n);
+        RE(n) = pp / (g - 1.) + 0.5 * (RU(n) * RU(n) + RV(n) * RV(n) + RW(n) * RW(n)) * RO(n);
+      } else if (bc[5] == 51) {
+        RO(n) = 0.5; RU(n) = 0.; RV(n) = 0.; RW(n) = 0.; RE(n) = 1.4275;
+      } else if (bc[5] == 10) {
+        RO(n) = 1.; RU(n) = 0.; RV(n) = 0.; RW(n) = 1.; RE(n) = 1 / 0.4 + 0.5;
+      } else if (bc[5] == 8) { /* subsonic non-reflecting outflow (rhs.c:1056-1086) */
+        double L[5], Lambda[5], d[5], a_sound, AA;
+        a_sound = sqrt(g * lp[m1] / lq[0][m1]);
+        AA = RW(m1) / RO(m1);
+        Lambda[0] = AA - a_sound;
+        Lambda[1] = AA; Lambda[2] = AA; Lambda[3] = AA;
+        Lambda[4] = AA + a_sound;
+        L[0] = 0;
+        L[1] = Lambda[1] * aj[m1] * zet[2][m1] * (a_sound * a_sound * (lq[0][m1] - lq[0][m2]) - (lp[n] - lp[m1]));
+        L[2] = Lambda[2] * aj[m1] * zet[2][m1] * (lq[1][m1] / RO(m1) - lq[1][m2] / RO(m1)); /* TwoD 0 */
+        L[3] = Lambda[3] * aj[m1] * zet[2][m1] * (lq[2][m1] / RO(m1) - lq[2][m2] / RO(m2));
+        L[4] = Lambda[4] * aj[m1] * zet[2][m1] *
+               ((lp[m1] - lp[m2]) + RO(m1) * a_sound * (lq[3][m1] / RO(m1) - lq[3][m2] / RO(m2)));
+        d[0] = 1. / (a_sound * a_sound) * (L[1] + 0.5 * (L[4] + L[0]));
+        d[1] = 0.5 * (L[0] + L[4]);
+        d[2] = 0.5 / (RO(m1) * a_sound) * (L[4] - L[0]);
+        d[3] = L[2];
+        d[4] = L[3];
+        RO(n) = qold[0][n] - c->dt * alfa * d[0];
+        RE(n) = qold[4][n] - c->dt * alfa *
+                                 (0.5 * d[0] * (lq[3][m1] / RO(m1) * lq[3][m1] / RO(m1)) + d[1] / (g - 1.) +
+                                  lq[3][m1] * d[2]);
+        RW(n) = qold[3][n] - c->dt * alfa * (lq[3][m1] / RO(m1) * d[0] + RO(m1) * d[2]);
+      }
+    }
+#undef RO
+#undef RU
+#undef RV
+#undef RW
+#undef RE
+  free(lp);
+  /* periodic copies (rhs.c:1107-1227) */
+  if (bc[0] == 7 || bc[1] == 7) {
+    for (int k = 1; k < mz; k++)
+      for (int j = 1; j < my; j++) {
+        ptrdiff_t n = IX(&G, 0, j, k);
+        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n - 2 * si];
+        n = IX(&G, mx - 1, j, k);
+        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n + 2 * si];
+      }
+  }
+  if (bc[2] == 7 || bc[3] == 7) {
+    for (int k = 1; k < mz; k++)
+      for (int i = 0; i < mx; i++) {
+        ptrdiff_t n = IX(&G, i, 0, k);
+        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n - 2 * sj];
+      }
+    for (int k = 1; k < mz - 1; k++)
+      for (int i = 0; i < mx; i++) {
+        ptrdiff_t n = IX(&G, i, my - 1, k);
+        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n + 2 * sj];
+      }
+  }
+  if (bc[4] == 7 || bc[5] == 7) {
+    for (int j = 0; j < my; j++)
+      for (int i = 0; i < mx; i++) {
+        ptrdiff_t n = IX(&G, i, j, 0);
+        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n - 2 * sk];
+        n = IX(&G, i, j, mz - 1);
+        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n + 2 * sk];
+      }
+  }
+  for (int a = 0; a < 5; a++) cbo_fill_ghosts(c, q[a]);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Time steps  (main.c:900-974 -> Flow_Solver solvers.c:13-64 -> RungeKutta)  */
 /* ------------------------------------------------------------------------ */
 int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const qold[5],
@@ -919,7 +1131,11 @@ int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const
         *have_uc = 1;
       }
       cbo_rk_combine(c, s, (const double *const *)qold, (const double *const *)q, (const double *const *)rhs, qn);
-      err = cbo_bc_periodic(c, (const double *const *)q, qn);
+      {
+        double al[3] = {1., 1 / 4., 2 / 3.};
+        if (c->fluxorder < 3) al[1] = 1 / 2.;
+        err = cbo_formbcs(c, al[s], (const double *const *)q, (const double *const *)qold, zet, aj, qn);
+      }
       for (int a = 0; a < 5; a++) memcpy(q[a], qn[a], G.n * sizeof(double));
     }
     for (int a = 0; a < 5; a++) memcpy(qold[a], q[a], G.n * sizeof(double));

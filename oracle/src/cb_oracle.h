@@ -81,6 +81,13 @@ void cbo_rk_combine(const cbo_config *c, int istage, const double *const qold[5]
  * input qin, then DMGlobalToLocal of qout. */
 int cbo_bc_periodic(const cbo_config *c, const double *const qin[5], double *const qout[5]);
 
+/* FormBCS: boundary nodes of q (the RK-combined stage output) from the
+ * boundary codes, the periodic copies from the stale ghosted stage input lq,
+ * then the ghost wrap; alfa: the stage's RK coefficient.  Returns 5 for the
+ * codes that are not restated. */
+int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], const double *const qold[5],
+                const double *const zet[3], const double *aj, double *const q[5]);
+
 /* Full time steps (Flow_Solver + main loop): q (ghosted, in/out), qold,
  * quc (ghosted state of the last CalcUCat; in/out), have_uc (in/out flag),
  * nut (in/out).  Scratch buffers are allocated inside. */

@@ -1,0 +1,51 @@
+"""Non-periodic boundary codes on the GPU (FormBCS rhs.c:477-1227 and the wall
+branches of formConvection / formViscous): RHS and RK steps against the oracle
+restatement, which is bit-exact against the reference
+(tests/test_oracle_vs_reference.py::test_formbcs_restatement_bitexact_vs_reference)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from _common import RTOL_L2, gpu_block, oracle_run, per_field_rel_l2
+from chimera_comp_les_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+BC = [(3, 3, 1, 1, 45, 44), (7, 7, 1, 1, 7, 7), (3, 3, 3, 3, 55, 45), (51, 51, 10, 10, 51, 51),
+      (3, 3, 1, 1, 44, 49), (7, 7, 3, 3, 45, 8), (1, 1, 1, 1, 44, 45)]
+
+
+@pytest.mark.parametrize("bct", BC)
+@pytest.mark.parametrize("les,iso,fo", [(0, 0, 3), (1, 1, 3), (0, 1, 2)])
+def test_boundary_codes_match_oracle(bct, les, iso, fo):
+    n = (35, 17, 23)  # several tiles in i and j, partial tiles
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, bctype=bct, les=les, inviscid=0, fluxorder=fo,
+                   isothermal=iso, s_x=0.4 if les else 1.0, s_y=0.7, s_z=0.9, ren=250., ma=0.3, pr=0.71, dt=0.002)
+    q = W.random_smooth_state(shape, seed=9, periodic=False)
+    nv = np.zeros(shape)
+    ref = oracle_run(cfg, coords, q, nv, steps=3)
+    with gpu_block(cfg) as b:
+        b.FormMetrics(coords)
+        b.set_nvert(nv)
+        b.SetInitialCondition(q)
+        if cfg.les:
+            b.CalcUCat()
+            b.Compute_eddy_viscosity_LES()
+            assert O.rel_l2(b.nu_t(), ref["nut"]) <= RTOL_L2
+        rhs = b.formRHS(0)
+    assert max(per_field_rel_l2(rhs, ref["rhs"])) <= RTOL_L2
+    with gpu_block(cfg) as b:
+        b.FormMetrics(coords)
+        b.set_nvert(nv)
+        b.SetInitialCondition(q)
+        b.RungeKutta(3)
+        got = b.Q()
+    assert max(per_field_rel_l2(got, ref["q_steps"])) <= RTOL_L2
+    with gpu_block(cfg, precision="mixed") as b:
+        b.FormMetrics(coords)
+        b.set_nvert(nv)
+        b.SetInitialCondition(q)
+        b.RungeKutta(3)
+        assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= 1e-5

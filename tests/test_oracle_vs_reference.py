@@ -109,3 +109,30 @@ def test_shock_sensor_restatement_bitexact_vs_reference(inv, smin):
     st = ora.initial_state(q)
     ora.steps(2, st, met, nvp)
     assert np.array_equal(O.from_padded(st["q"]), ref2.Q())
+
+
+BC_CASES = [(3, 3, 1, 1, 45, 44), (7, 7, 1, 1, 7, 7), (3, 3, 3, 3, 55, 45), (51, 51, 10, 10, 51, 51),
+            (3, 3, 1, 1, 44, 49), (7, 7, 3, 3, 45, 8), (1, 1, 1, 1, 44, 45)]
+
+
+@pytest.mark.parametrize("bct", BC_CASES)
+@pytest.mark.parametrize("les,iso", [(0, 0), (1, 1)])
+def test_formbcs_restatement_bitexact_vs_reference(bct, les, iso):
+    """Non-periodic boundary codes (FormBCS rhs.c:477-1227): two RK steps."""
+    n = (12, 13, 11)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, bctype=bct, les=les, inviscid=0, fluxorder=3,
+                   isothermal=iso, s_x=0.4 if les else 1.0, s_y=0.7, s_z=0.9, ren=250., ma=0.3, pr=0.71, dt=0.002)
+    q = W.random_smooth_state(shape, seed=9, periodic=False)
+    nv = np.zeros(shape)
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q)
+    ref.steps(2)
+    ora = O.Oracle(cfg)
+    met = ora.metrics(O.to_padded(cfg, coords))
+    nvp = ora.fill_ghosts(O.to_padded(cfg, nv))
+    st = ora.initial_state(q)
+    ora.steps(2, st, met, nvp)
+    assert np.array_equal(O.from_padded(st["q"]), ref.Q())
