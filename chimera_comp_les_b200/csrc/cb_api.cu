@@ -231,7 +231,7 @@ static int nut_update(cb_ctx *c) {
   const long long work = (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2);
   {
     TimedScope ts(c, false);
-    eddy_viscosity_kernel<<<grid_for(c, work), 256, 0, c->stream>>>(
+    eddy_viscosity_kernel<<<eddy_grid(c->dc), dim3(EDDY_BX, EDDY_BY), 0, c->stream>>>(
         c->dc, c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr,
         (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvert, c->nut);
   }
@@ -394,6 +394,7 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.inv_ren_half = 1. / cfg->ren * 0.5;
   d.gm1 = cfg->gamma - 1.0;
   d.nvq = 1;  // nvert starts zero
+  if (shell_count(d) >= (1LL << 31)) return bail(CB_E_ARG, "grid too large for 32-bit boundary indexing");
   d.calc_sigma = (cfg->les && cfg->calc_sigma) ? 1 : 0;
   d.s_x_min = cfg->s_x_min; d.s_y_min = cfg->s_y_min; d.s_z_min = cfg->s_z_min;
   d.ks = cfg->sigma_thrsh;

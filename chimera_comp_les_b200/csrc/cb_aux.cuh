@@ -38,24 +38,27 @@ __host__ __device__ __forceinline__ long long shell_count(const DevCfg &c) {
   const long long NX = c.mx + 4, NY = c.my + 4;
   return 6 * NX * NY + (long long)(c.mz - 2) * (6 * NX + 6 * (c.my - 2));
 }
-__device__ __forceinline__ void shell_node(const DevCfg &c, long long t, int &i, int &j, int &k) {
-  const long long NX = c.mx + 4, NY = c.my + 4, NZ = c.mz + 4, A = NX * NY, Pm = 6 * NX + 6 * (c.my - 2);
-  long long I, J, K;
+// 32-bit index arithmetic (a shell count below 2^31 is checked on the host):
+// 64-bit division costs far more than the copy it addresses.
+__device__ __forceinline__ void shell_node(const DevCfg &c, long long t64, int &i, int &j, int &k) {
+  const unsigned t = (unsigned)t64;
+  const unsigned NX = c.mx + 4, NY = c.my + 4, NZ = c.mz + 4, A = NX * NY, Pm = 6 * NX + 6 * (c.my - 2);
+  unsigned I, J, K;
   if (t < 6 * A) {
-    const long long p = t / A, r = t - p * A;
+    const unsigned p = t / A, r = t - p * A;
     K = p < 3 ? p : NZ - 6 + p;
     J = r / NX;
     I = r - J * NX;
   } else {
-    const long long t2 = t - 6 * A;
+    const unsigned t2 = t - 6 * A;
     K = 3 + t2 / Pm;
-    const long long r = t2 - (K - 3) * Pm;
+    const unsigned r = t2 - (K - 3) * Pm;
     if (r < 6 * NX) {
-      const long long q = r / NX;
+      const unsigned q = r / NX;
       J = q < 3 ? q : NY - 6 + q;
       I = r - q * NX;
     } else {
-      const long long r2 = r - 6 * NX, cc = r2 % 6;
+      const unsigned r2 = r - 6 * NX, cc = r2 % 6;
       J = 3 + r2 / 6;
       I = cc < 3 ? cc : NX - 6 + cc;
     }
@@ -306,14 +309,18 @@ static __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, 
 // Compute_eddy_viscosity_LES (les.c:1523-1567) with constant CS
 // (les.c:135-150): interior nodes only; velocity from the recorded state qu
 // (nullptr: zero velocity before the first CalcUCat).
-static __global__ void eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met,
-                                      const double *aj, const double *delta2, const double *nvert, double *nut) {
-  const long long nx = c.mx - 2, ny = c.my - 2, nz = c.mz - 2, total = nx * ny * nz;
+// Launched on a 3-D grid (EDDY_BX x EDDY_BY threads per block, one block
+// row per k plane): no index division.
+constexpr int EDDY_BX = 32, EDDY_BY = 8;
+static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
+    eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met, const double *aj,
+                          const double *delta2, const double *nvert, double *nut) {
   const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / (nx * ny));
+  const int i = 1 + blockIdx.x * EDDY_BX + threadIdx.x, j = 1 + blockIdx.y * EDDY_BY + threadIdx.y, k = 1 + blockIdx.z;
+  if (i > c.mx - 2 || j > c.my - 2) return;
+  {
     const long long n = gidx(c, i, j, k);
-    if (ldg(nvert + n) > 0.1) { nut[n] = 0.; continue; }
+    if (ldg(nvert + n) > 0.1) { nut[n] = 0.; return; }
     double dd[3][3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -338,6 +345,9 @@ static __global__ void eddy_viscosity_kernel(const DevCfg c, const double *const
                                     Syz * Syz + Szz * Szz));
     nut[n] = c.cs_const * ldg(delta2 + n) * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
   }
+}
+static inline dim3 eddy_grid(const DevCfg &c) {
+  return dim3((c.mx - 2 + EDDY_BX - 1) / EDDY_BX, (c.my - 2 + EDDY_BY - 1) / EDDY_BY, c.mz - 2);
 }
 
 // ------------------------------------------------------------ shock sensor --

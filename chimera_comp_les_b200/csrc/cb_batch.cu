@@ -296,6 +296,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.gm1 = cfg->gamma - 1.0;
     d.nvq = 1;  // nvert starts zero
     d.calc_sigma = 0;  // the shock sensor is built for single-block contexts
+    if (shell_count(d) >= (1LL << 31)) return bail(CB_E_ARG, "block too large for 32-bit boundary indexing");
     bh.off = off;
     off += (d.plane + 31) / 32 * 32;  // 256-byte aligned block starts
     bh.tiles_x = (bh.mx - 2 + SBX - 1) / SBX;
@@ -634,7 +635,7 @@ static int enqueue_nut(cb_batch *b) {
     const char *ent = reinterpret_cast<const char *>(b->d_tables + (size_t)(u * 13) * b->nb + k);
     const double *const *qu = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
     const double *const *mt = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, met));
-    eddy_viscosity_kernel<<<bgrid(b, work), 256, 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
+    eddy_viscosity_kernel<<<eddy_grid(bh.dc), dim3(EDDY_BX, EDDY_BY), 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
                                                                  b->delta2 + o, b->nvert + o, b->nut + o);
   }
   if (b->nwrap || b->xw.nsend || b->xw.nrecv) {
