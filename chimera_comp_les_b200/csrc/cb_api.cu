@@ -231,9 +231,10 @@ static int nut_update(cb_ctx *c) {
   const long long work = (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2);
   {
     TimedScope ts(c, false);
-    eddy_viscosity_kernel<<<eddy_grid(c->dc), dim3(EDDY_BX, EDDY_BY), 0, c->stream>>>(
+    const int ekc = eddy_kchunk(c->dc, c->sms);
+    eddy_viscosity_kernel<<<eddy_grid(c->dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, c->stream>>>(
         c->dc, c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr,
-        (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvert, c->nut);
+        (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvert, c->nut, ekc);
   }
   {
     TimedScope ts(c, false);

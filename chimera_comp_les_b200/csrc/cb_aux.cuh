@@ -309,45 +309,87 @@ static __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, 
 // Compute_eddy_viscosity_LES (les.c:1523-1567) with constant CS
 // (les.c:135-150): interior nodes only; velocity from the recorded state qu
 // (nullptr: zero velocity before the first CalcUCat).
-// Launched on a 3-D grid (EDDY_BX x EDDY_BY threads per block, one block
-// row per k plane): no index division.
-constexpr int EDDY_BX = 32, EDDY_BY = 8;
+// A block owns an EDDY_BX x EDDY_BY column of interior nodes and marches
+// along k through a chunk of planes; the velocity u = rhoU / rho of three
+// planes (k-1, k, k+1, with a one-node halo in i and j) sits in shared
+// memory, so each node's three divisions happen once instead of at each of
+// its six neighbours (the same IEEE quotients the reference forms there).
+constexpr int EDDY_BX = 32, EDDY_BY = 8, EDDY_PX = EDDY_BX + 2, EDDY_PN = EDDY_PX * (EDDY_BY + 2);
 static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
     eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met, const double *aj,
-                          const double *delta2, const double *nvert, double *nut) {
-  const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
-  const int i = 1 + blockIdx.x * EDDY_BX + threadIdx.x, j = 1 + blockIdx.y * EDDY_BY + threadIdx.y, k = 1 + blockIdx.z;
-  if (i > c.mx - 2 || j > c.my - 2) return;
-  {
-    const long long n = gidx(c, i, j, k);
-    if (ldg(nvert + n) > 0.1) { nut[n] = 0.; return; }
-    double dd[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      if (!qu) { dd[a][0] = dd[a][1] = dd[a][2] = 0.; continue; }
-      const double *r = qu[0], *m = qu[1 + a];
-      dd[a][0] = (ldg(m + n + si) / ldg(r + n + si) - ldg(m + n - si) / ldg(r + n - si)) * 0.5;
-      dd[a][1] = (ldg(m + n + sj) / ldg(r + n + sj) - ldg(m + n - sj) / ldg(r + n - sj)) * 0.5;
-      dd[a][2] = (ldg(m + n + sk) / ldg(r + n + sk) - ldg(m + n - sk) / ldg(r + n - sk)) * 0.5;
+                          const double *delta2, const double *nvert, double *nut, int kchunk) {
+  __shared__ double us[3][3][EDDY_PN];  // [slot][component][node]
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * EDDY_BX + tx;
+  const int i0 = 1 + blockIdx.x * EDDY_BX, j0 = 1 + blockIdx.y * EDDY_BY;
+  const int kb = 1 + blockIdx.z * kchunk, ke = min(c.mz - 1, kb + kchunk);
+  const int i = i0 + tx, j = j0 + ty;
+  const bool act = i <= c.mx - 2 && j <= c.my - 2;
+  // velocity of plane kk into slot s (halo entries beyond the owned nodes are never read)
+  auto load = [&](int kk, int s) {
+    for (int e = tid; e < EDDY_PN; e += EDDY_BX * EDDY_BY) {
+      const int lx = e % EDDY_PX, ly = e / EDDY_PX;
+      const int xi = i0 - 1 + lx, yj = j0 - 1 + ly;
+      double u0 = 0., u1 = 0., u2 = 0.;
+      if (qu && xi <= c.mx - 1 && yj <= c.my - 1) {
+        const long long n = gidx(c, xi, yj, kk);
+        const double r = ldg(qu[0] + n);
+        u0 = ldg(qu[1] + n) / r;
+        u1 = ldg(qu[2] + n) / r;
+        u2 = ldg(qu[3] + n) / r;
+      }
+      us[s][0][e] = u0;
+      us[s][1][e] = u1;
+      us[s][2][e] = u2;
     }
-    const double ajc = ldg(aj + n);
-    double g[3][3];
+  };
+  load(kb - 1, (kb - 1) % 3);
+  load(kb, kb % 3);
+  const int e0 = (ty + 1) * EDDY_PX + tx + 1;
+  for (int k = kb; k < ke; k++) {
+    load(k + 1, (k + 1) % 3);
+    __syncthreads();
+    if (act) {
+      const long long n = gidx(c, i, j, k);
+      if (ldg(nvert + n) > 0.1) {
+        nut[n] = 0.;
+      } else {
+        const int sm = (k - 1) % 3, s0 = k % 3, sp = (k + 1) % 3;
+        double dd[3][3];
 #pragma unroll
-    for (int a = 0; a < 3; a++)
+        for (int a = 0; a < 3; a++) {
+          dd[a][0] = (us[s0][a][e0 + 1] - us[s0][a][e0 - 1]) * 0.5;
+          dd[a][1] = (us[s0][a][e0 + EDDY_PX] - us[s0][a][e0 - EDDY_PX]) * 0.5;
+          dd[a][2] = (us[sp][a][e0] - us[sm][a][e0]) * 0.5;
+        }
+        const double ajc = ldg(aj + n);
+        double g[3][3];
 #pragma unroll
-      for (int x = 0; x < 3; x++)
-        g[a][x] = (dd[a][0] * ldg(met[0 * 3 + x] + n) + dd[a][1] * ldg(met[1 * 3 + x] + n) + dd[a][2] * ldg(met[2 * 3 + x] + n)) * ajc;
-    const double Sdd = 2. / 3. * (g[0][0] + g[1][1] + g[2][2]);
-    const double Sxx = 0.5 * (g[0][0] + g[0][0]) - Sdd, Sxy = 0.5 * (g[0][1] + g[1][0]), Sxz = 0.5 * (g[0][2] + g[2][0]);
-    const double Syy = 0.5 * (g[1][1] + g[1][1]) - Sdd, Syz = 0.5 * (g[1][2] + g[2][1]);
-    const double Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
-    const double Sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Sxy * Sxy + Syy * Syy + Syz * Syz + Sxz * Sxz +
-                                    Syz * Syz + Szz * Szz));
-    nut[n] = c.cs_const * ldg(delta2 + n) * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int x = 0; x < 3; x++)
+            g[a][x] = (dd[a][0] * ldg(met[0 * 3 + x] + n) + dd[a][1] * ldg(met[1 * 3 + x] + n) +
+                       dd[a][2] * ldg(met[2 * 3 + x] + n)) * ajc;
+        const double Sdd = 2. / 3. * (g[0][0] + g[1][1] + g[2][2]);
+        const double Sxx = 0.5 * (g[0][0] + g[0][0]) - Sdd, Sxy = 0.5 * (g[0][1] + g[1][0]), Sxz = 0.5 * (g[0][2] + g[2][0]);
+        const double Syy = 0.5 * (g[1][1] + g[1][1]) - Sdd, Syz = 0.5 * (g[1][2] + g[2][1]);
+        const double Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
+        const double Sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Sxy * Sxy + Syy * Syy + Syz * Syz +
+                                        Sxz * Sxz + Syz * Syz + Szz * Szz));
+        nut[n] = c.cs_const * ldg(delta2 + n) * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
+      }
+    }
+    __syncthreads();  // the slot of plane k-1 is refilled next
   }
 }
-static inline dim3 eddy_grid(const DevCfg &c) {
-  return dim3((c.mx - 2 + EDDY_BX - 1) / EDDY_BX, (c.my - 2 + EDDY_BY - 1) / EDDY_BY, c.mz - 2);
+// k-chunk of the eddy-viscosity march: short chunks (many blocks, a short
+// tail wave); a chunk re-reads two velocity planes, a quarter of its q loads
+static inline int eddy_kchunk(const DevCfg &c, int sms) {
+  (void)sms;
+  const int nk = c.mz - 2;
+  return nk < 8 ? nk : 8;
+}
+static inline dim3 eddy_grid(const DevCfg &c, int kchunk) {
+  return dim3((c.mx - 2 + EDDY_BX - 1) / EDDY_BX, (c.my - 2 + EDDY_BY - 1) / EDDY_BY, (c.mz - 2 + kchunk - 1) / kchunk);
 }
 
 // ------------------------------------------------------------ shock sensor --
