@@ -403,10 +403,28 @@ def run_ours(args, ws, rank, local):
     batched = run_batched(args, local) if (ws == 1 and not args.no_batched) else None
 
     cpu = None
+    vs_oracle = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import cpu_baseline as cb
         r = cb.run(n, steps=1, warmup=0, cfgkw=CFG)
         cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
+        # the same CPU leg, as the checker: one full-size step of the oracle
+        # against one step of each GPU form from the same state
+        import oracle as O
+        from chimera_comp_les_b200 import diagnostics as D
+        ocfg = O.Config(mx=n + 2, my=n + 2, mz=n + 2, **{k: v for k, v in CFG.items()})
+        ora = O.Oracle(ocfg)
+        met = ora.metrics(O.to_padded(ocfg, coords))
+        nvp = ora.fill_ghosts(O.to_padded(ocfg, nv))
+        st = ora.initial_state(q0)
+        ora.steps(1, st, met, nvp)
+        q_ora = O.from_padded(st["q"])
+        vs_oracle = {"steps": 1, "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]}
+        for prec, blk in blocks.items():
+            blk.SetInitialCondition(q0)
+            blk.RungeKutta(1)
+            l2, linf = D.field_errors(blk.Q(), q_ora)
+            vs_oracle[prec] = {"rel_l2": l2, "rel_linf": linf}
 
     if rank == 0:
         cfg = workload_config(n)
@@ -433,6 +451,7 @@ def run_ours(args, ws, rank, local):
             "speedup_mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"],
             "mixed_vs_fp64_error": acc,
             "batched": batched,
+            "vs_oracle": vs_oracle,
         }
         print(json.dumps(line), flush=True)
     for b in blocks.values():

@@ -121,7 +121,10 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t set_stage_attr() {
-  return cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 0>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STAGE_SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)STAGE_SMEM_BYTES);
 }
 
@@ -141,7 +144,7 @@ static cudaError_t set_stage_attrs() {
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt) {
-  auto kern = stage_kernel<double, false, LES, VISC, RHSM>;
+  auto kern = c->dc.flux == 1 ? stage_kernel<double, false, LES, VISC, RHSM, 1> : stage_kernel<double, false, LES, VISC, RHSM, 0>;
   const int nkin = c->dc.mz - 2;
   dim3 grid((c->dc.mx - 2 + BX - 1) / BX, (c->dc.my - 2 + BY - 1) / BY, (nkin + c->kchunk - 1) / c->kchunk);
   kern<<<grid, SNT, STAGE_SMEM_BYTES, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
@@ -151,7 +154,8 @@ static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, dou
 static cudaError_t launch_stage(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt, bool rhs_mode) {
   const bool les = c->cfg.les != 0, visc = c->cfg.inviscid == 0;
   if (c->cfg.precision == CB_MIXED)
-    return launch_stage_mixed(c->dc, F, istage, alfa, beta, adt, c->kchunk, les, visc, rhs_mode, c->stream);
+    return launch_stage_mixed(c->dc, F, istage, alfa, beta, adt, c->kchunk, les, visc, rhs_mode, c->dc.flux == 1,
+                              c->stream);
   if (rhs_mode) {
     if (les && visc) return launch_stage_t<true, true, true>(c, F, istage, alfa, beta, adt);
     if (les) return launch_stage_t<true, false, true>(c, F, istage, alfa, beta, adt);
@@ -372,6 +376,7 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   if (cfg->eno_order != 2 && cfg->eno_order != 3) return bail(CB_E_ARG, "ENOorder must be 2 or 3");
   if (cfg->les != 0 && cfg->les != 1) return bail(CB_E_UNSUPPORTED, "only les 0 or 1 (constant Smagorinsky) is built");
   if (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) return bail(CB_E_ARG, "precision must be CB_FP64 or CB_MIXED");
+  if (cfg->flux != 0 && cfg->flux != 1) return bail(CB_E_ARG, "flux must be 0 (Rusanov) or 1 (Roe)");
   c->dev = cfg->device;
   if (cudaSetDevice(c->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice failed");
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
@@ -399,6 +404,7 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.calc_sigma = (cfg->les && cfg->calc_sigma) ? 1 : 0;
   d.s_x_min = cfg->s_x_min; d.s_y_min = cfg->s_y_min; d.s_z_min = cfg->s_z_min;
   d.ks = cfg->sigma_thrsh;
+  d.flux = cfg->flux;
   c->plane = (size_t)d.plane;
   // planes: 15 state + 9 metrics + aj + nvert + nut + LES filter width = 28
   const int nplanes = 28;

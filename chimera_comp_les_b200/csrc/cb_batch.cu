@@ -267,7 +267,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
   };
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
       (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
-      (cfg->les && cfg->calc_sigma))
+      (cfg->les && cfg->calc_sigma) || cfg->flux != 0)
     return bail(CB_E_UNSUPPORTED, "option combination not built");
   b->dev = cfg->device;
   if (cudaSetDevice(b->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice");
@@ -296,6 +296,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.gm1 = cfg->gamma - 1.0;
     d.nvq = 1;  // nvert starts zero
     d.calc_sigma = 0;  // the shock sensor is built for single-block contexts
+    d.flux = 0;  // the Roe flux is built for single-block contexts
     if (shell_count(d) >= (1LL << 31)) return bail(CB_E_ARG, "block too large for 32-bit boundary indexing");
     bh.off = off;
     off += (d.plane + 31) / 32 * 32;  // 256-byte aligned block starts
@@ -695,7 +696,7 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
         if (cost < best) { best = cost; kc = cand; }
       }
       if (mixed) {
-        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, b->stream));
+        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, false, b->stream));
       } else {
         dim3 grid(bh.tiles_x, bh.tiles_y, (nk + kc - 1) / kc);
         if (les && visc)

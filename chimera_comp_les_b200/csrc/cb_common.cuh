@@ -36,6 +36,7 @@ struct DevCfg {
   // LES shock sensor (rhs.c:3333-3433): hybrid weights from per-node planes
   int calc_sigma;
   double s_x_min, s_y_min, s_z_min, ks;
+  int flux;  // 0 Rusanov (the reference's), 1 Roe with Harten's entropy fix
 };
 
 // Host check of an nvert array for the byte code of DevCfg::nvq.

@@ -79,7 +79,7 @@ extern "C" int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const 
   for (int b = 0; b < 6; b++)
     if (cfg->bctype[b] != 7) return na_fail(CB_E_UNSUPPORTED, "only fully periodic blocks (bctype 7) are built");
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
-      (cfg->les != 0 && cfg->les != 1) || cfg->precision != CB_FP64 || (cfg->les && cfg->calc_sigma))
+      (cfg->les != 0 && cfg->les != 1) || cfg->precision != CB_FP64 || (cfg->les && cfg->calc_sigma) || cfg->flux != 0)
     return na_fail(CB_E_UNSUPPORTED, "option combination not built");
   DevCfg d{};
   d.mx = cfg->mx; d.my = cfg->my; d.mz = cfg->mz;
@@ -103,6 +103,7 @@ extern "C" int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const 
   d.inv_ren_half = 1. / cfg->ren * 0.5;
   d.gm1 = cfg->gamma - 1.0;
   d.nvq = 0;  // nvert is a caller-owned device array: read it from global memory
+  d.flux = 0;
 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return na_fail(CB_E_CUDA, "no current CUDA device");

@@ -190,12 +190,60 @@ __device__ __forceinline__ void rusanov(const R QL[5], const R QR[5], R pL, R pR
   Uf = MIX ? R(0.5) * (uconL + uconR) : R(0);
 }
 
+// Roe's approximate Riemann solver with Harten's entropy fix (no counterpart
+// in the reference; Roe, J. Comput. Phys. 43 (1981); Harten, J. Comput.
+// Phys. 49 (1983)): the central part is the Rusanov flux's average of the
+// two physical fluxes; the dissipation is |h| |A~| (QR - QL) of the
+// Roe-averaged Jacobian along n = h/|h|, acoustic speeds below 0.1 c~
+// smoothed to (l^2 + delta^2) / (2 delta).  Mixed form: the enthalpy adds
+// back H_ref; pressure and energy differences are shift-free.
+template <typename R, bool MIX>
+__device__ __forceinline__ void roe(const R QL[5], const R QR[5], R pL, R pR, const R h[3], bool use_qr_for_l,
+                                    bool r_from_l, R pref, R href, R F[5], R &Uf) {
+  R uconL = use_qr_for_l ? (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]))
+                         : (h[0] * (QL[1] / QL[0]) + h[1] * (QL[2] / QL[0]) + h[2] * (QL[3] / QL[0]));
+  R uconR = r_from_l ? uconL : (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
+  (void)pref;
+  const R g = R(GAMMA_CONV);
+  const R area = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+  const R nx = h[0] / area, ny = h[1] / area, nz = h[2] / area;
+  const R sl = sqrt(QL[0]), sr = sqrt(QR[0]), wl = sl / (sl + sr), wr = sr / (sl + sr);
+  const R uL = QL[1] / QL[0], vL = QL[2] / QL[0], zL = QL[3] / QL[0];
+  const R uR = QR[1] / QR[0], vR = QR[2] / QR[0], zR = QR[3] / QR[0];
+  const R HL = (MIX ? (QL[4] + pL + href) : (QL[4] + pL)) / QL[0];
+  const R HR = (MIX ? (QR[4] + pR + href) : (QR[4] + pR)) / QR[0];
+  const R rt = sl * sr, ut = wl * uL + wr * uR, vt = wl * vL + wr * vR, zt = wl * zL + wr * zR;
+  const R Ht = wl * HL + wr * HR, q2 = ut * ut + vt * vt + zt * zt;
+  const R c2 = (g - R(1.0)) * (Ht - R(0.5) * q2), ct = sqrt(fabs(c2));
+  const R Unt = ut * nx + vt * ny + zt * nz;
+  const R dp = pR - pL, dr = QR[0] - QL[0];
+  const R du = uR - uL, dv = vR - vL, dz = zR - zL, dUn = du * nx + dv * ny + dz * nz;
+  const R a1 = (dp - rt * ct * dUn) / (R(2.0) * c2), a2 = dr - dp / c2, a3 = (dp + rt * ct * dUn) / (R(2.0) * c2);
+  R l1 = fabs(Unt - ct), l2 = fabs(Unt), l3 = fabs(Unt + ct);
+  const R delta = R(0.1) * ct;
+  if (l1 < delta) l1 = (l1 * l1 + delta * delta) / (R(2.0) * delta);
+  if (l3 < delta) l3 = (l3 * l3 + delta * delta) / (R(2.0) * delta);
+  const R s1 = l1 * a1, s2 = l2 * a2, s3 = l3 * a3, ss = l2 * rt;
+  R D[5];
+  D[0] = s1 + s2 + s3;
+  D[1] = s1 * (ut - ct * nx) + s2 * ut + s3 * (ut + ct * nx) + ss * (du - dUn * nx);
+  D[2] = s1 * (vt - ct * ny) + s2 * vt + s3 * (vt + ct * ny) + ss * (dv - dUn * ny);
+  D[3] = s1 * (zt - ct * nz) + s2 * zt + s3 * (zt + ct * nz) + ss * (dz - dUn * nz);
+  D[4] = s1 * (Ht - Unt * ct) + s2 * R(0.5) * q2 + s3 * (Ht + Unt * ct) + ss * (ut * du + vt * dv + zt * dz - Unt * dUn);
+  F[0] = R(0.5) * (QL[0] * uconL + QR[0] * uconR) - R(0.5) * area * D[0];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    F[1 + a] = R(0.5) * ((QL[1 + a] * uconL + QR[1 + a] * uconR) + (pL * h[a] + pR * h[a])) - R(0.5) * area * D[1 + a];
+  F[4] = R(0.5) * ((pL + QL[4]) * uconL + (pR + QR[4]) * uconR) - R(0.5) * area * D[4];
+  Uf = MIX ? R(0.5) * (uconL + uconR) : R(0);
+}
+
 // ------------------------------------------------------- inviscid face ----
 // Face between node A (tile ref a, global (gi,gj,gk)) and A + e_d.
 // DIR >= 0: the face direction as a compile-time constant, so every stencil
 // shift, stride and metric selection folds into fixed offsets; DIR = -1: the
 // direction is the runtime argument drt (one copy of the code for all three).
-template <typename R, bool MIX, bool LES, int BX, int BY, int DIR>
+template <typename R, bool MIX, bool LES, int BX, int BY, int DIR, int FLUX = 0>
 __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a,
                                           int gi, int gj, int gk, int drt, R Fc[5]) {
   const int d = DIR >= 0 ? DIR : drt;
@@ -287,11 +335,13 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   }
   R Fw[5], Ufw;
   if (LES) {
-    rusanov<R, MIX>(QL, QR, pL, pR, h, false, false, pref, Fw, Ufw);
+    if (FLUX == 1) roe<R, MIX>(QL, QR, pL, pR, h, false, false, pref, href, Fw, Ufw);
+    else rusanov<R, MIX>(QL, QR, pL, pR, h, false, false, pref, Fw, Ufw);
   } else {
     const bool use_qr_l = (pos == m - 2 && bc_hi(c, d) == 1);
     const bool r_from_l = (pos == 0 && bc_lo(c, d) == 1);
-    rusanov<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, Fw, Ufw);
+    if (FLUX == 1) roe<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, href, Fw, Ufw);
+    else rusanov<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, Fw, Ufw);
   }
   if (!LES) {
 #pragma unroll
@@ -490,12 +540,12 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
 
 // Everything one face contributes: the FP64 form keeps conv, visc and the LES
 // stress apart (G[0..4], G[5..9], G[10..12]), the mixed form stores visc - conv.
-template <typename R, bool MIX, bool LES, bool VISC, int BX, int BY, int DIR>
+template <typename R, bool MIX, bool LES, bool VISC, int BX, int BY, int DIR, int FLUX = 0>
 __device__ __forceinline__ void face_flux(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a, int fi,
                                           int fj, int k, int drt, R *G) {
   constexpr int VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
   R Fc[5], Fv[5], A[3];
-  conv_face<R, MIX, LES, BX, BY, DIR>(c, F, Rg, a, fi, fj, k, drt, Fc);
+  conv_face<R, MIX, LES, BX, BY, DIR, FLUX>(c, F, Rg, a, fi, fj, k, drt, Fc);
   if (VISC) {
     visc_face<R, MIX, LES, BX, BY, DIR>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
   } else {
@@ -542,7 +592,7 @@ static_assert(2 * (STAGE_SMEM_BYTES_MIXED + 1024) <= 233472, "mixed form: two bl
 // k-faces, for the prologue).  A function rather than a lambda so that it is
 // always inlined: an outlined call would copy the kernel parameters to local
 // memory.
-template <typename R, bool MIX, bool LES, bool VISC, bool ZONLY>
+template <typename R, bool MIX, bool LES, bool VISC, bool ZONLY, int FLUX = 0>
 __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F, const Ring<R, SBX, SBY> &Rg, int i0,
                                             int j0, int k, R *gxb, R *gyb, R *gzb) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, NG = FaceWidth<MIX>::NG;
@@ -580,13 +630,13 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
       if (MIX) {
         // one instantiation per direction (d is warp-uniform): 16 % faster
         // for the FP32 arithmetic of the mixed form
-        if (d == 0) face_flux<R, MIX, LES, VISC, BX, BY, 0>(c, F, Rg, a, fi, fj, k, d, G);
-        else if (d == 1) face_flux<R, MIX, LES, VISC, BX, BY, 1>(c, F, Rg, a, fi, fj, k, d, G);
-        else face_flux<R, MIX, LES, VISC, BX, BY, 2>(c, F, Rg, a, fi, fj, k, d, G);
+        if (d == 0) face_flux<R, MIX, LES, VISC, BX, BY, 0, FLUX>(c, F, Rg, a, fi, fj, k, d, G);
+        else if (d == 1) face_flux<R, MIX, LES, VISC, BX, BY, 1, FLUX>(c, F, Rg, a, fi, fj, k, d, G);
+        else face_flux<R, MIX, LES, VISC, BX, BY, 2, FLUX>(c, F, Rg, a, fi, fj, k, d, G);
       } else {
         // one copy for all directions: the FP64 form at 255 registers runs
         // 12 % slower with three
-        face_flux<R, MIX, LES, VISC, BX, BY, -1>(c, F, Rg, a, fi, fj, k, d, G);
+        face_flux<R, MIX, LES, VISC, BX, BY, -1, FLUX>(c, F, Rg, a, fi, fj, k, d, G);
       }
     } else {
 #pragma unroll
@@ -606,7 +656,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // One tile (tile column bxi, byi, k-chunk bzi) of one block: the whole k march.
-template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE>
+template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0>
 __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, int bxi, int byi, int bzi, int istage,
                                            double alfa, double beta, double adt, int kchunk, double *smem_d) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
@@ -689,7 +739,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   load_plane_sync(kb - 1, 1);
   load_plane_sync(kb, 2);
   load_plane_sync(kb + 1, 3);
-  plane_faces<R, MIX, LES, VISC, true>(c, F, Rg, i0, j0, kb - 1, gxb, gyb, gzb);  // k-face kb-1/2
+  plane_faces<R, MIX, LES, VISC, true, FLUX>(c, F, Rg, i0, j0, kb - 1, gxb, gyb, gzb);  // k-face kb-1/2
   __syncthreads();
   R Gzp[NG];  // k-face k-1/2 of the node this thread updates
 #pragma unroll
@@ -702,7 +752,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
     Rg.sb = base;
     const bool more = k + 1 < ke;
     if (more) issue_stage(k + 3);  // overlaps the face computation
-    plane_faces<R, MIX, LES, VISC, false>(c, F, Rg, i0, j0, k, gxb, gyb, gzb);
+    plane_faces<R, MIX, LES, VISC, false, FLUX>(c, F, Rg, i0, j0, k, gxb, gyb, gzb);
     // the only plane k-1 value the update needs, read before that slot is refilled
     const NRef n{0, uty + 2, utx + 2};
     const R rho_km1 = (LES && VISC && uact) ? Rg.get(F_RHO, nshift(n, 2, -1)) : R(0.);
@@ -802,11 +852,11 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   }
 }
 
-template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE>
+template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0>
 __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
   extern __shared__ double smem_d[];
-  stage_tile<R, MIX, LES, VISC, RHS_MODE>(c, F, blockIdx.x, blockIdx.y, blockIdx.z, istage, alfa, beta, adt, kchunk,
+  stage_tile<R, MIX, LES, VISC, RHS_MODE, FLUX>(c, F, blockIdx.x, blockIdx.y, blockIdx.z, istage, alfa, beta, adt, kchunk,
                                           smem_d);
 }
 

@@ -53,7 +53,8 @@ class Block:
                  ren: float = 3000.0, ma: float = 2.81, pr: float = 0.72, gamma: float = 1.4,
                  dt: float = 0.01, st: float = 1.0, cs_const: float = 0.03, ci: float = 0.06,
                  ratio: float = 0.0, precision: str = "fp64", device: int = 0, calc_sigma: int = 0,
-                 s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5):
+                 s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5,
+                 flux: str = "rusanov"):
         self.lib = _lib.load()
         cfg = CbConfig()
         self.lib.cb_config_default(C.byref(cfg), mx, my, mz)
@@ -63,6 +64,7 @@ class Block:
                          dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device, calc_sigma=calc_sigma,
                          s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh).items():
             setattr(cfg, k, v)
+        cfg.flux = {"rusanov": 0, "roe": 1}[flux] if isinstance(flux, str) else int(flux)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]
         self.cfg = cfg
         self.shape = (mz, my, mx)

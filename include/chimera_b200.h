@@ -72,6 +72,8 @@ typedef struct {
   int calc_sigma;       /* -calc_sigma: pressure shock sensor for the hybrid weights (rhs.c:3333-3411) */
   double s_x_min, s_y_min, s_z_min; /* -s_x_min/-s_y_min/-s_z_min: lower bounds of the sensor (default 0) */
   double sigma_thrsh;   /* -sigma_thrsh: ks of the smoothness ratio (rhs.c:3323, default 1e-5) */
+  int flux;             /* upwind flux: 0 Rusanov (the reference's, default), 1 Roe with Harten's
+                           entropy fix (no counterpart in the reference) */
 } cb_config;
 
 /* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */

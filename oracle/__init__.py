@@ -66,6 +66,7 @@ class Config:
     s_y_min: float = 0.0
     s_z_min: float = 0.0
     sigma_thrsh: float = 1e-5
+    flux: int = 0  # 0 Rusanov (the reference's), 1 Roe (no reference counterpart)
 
     def ref_options(self) -> str:
         o = [
@@ -101,6 +102,7 @@ class _CCfg(C.Structure):
         ("dt", C.c_double), ("st", C.c_double), ("cs_const", C.c_double), ("ci", C.c_double),
         ("ratio", C.c_double), ("calc_sigma", C.c_int),
         ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double), ("sigma_thrsh", C.c_double),
+        ("flux", C.c_int),
     ]
 
 
@@ -270,6 +272,8 @@ class RefOracle:
     per process (the reference keeps its state in globals)."""
 
     def __init__(self, cfg: Config, coords_nat: np.ndarray, optimized: bool = False):
+        if cfg.flux != 0:
+            raise ValueError("the reference has no Roe flux (flux 1); check it against the restatement")
         self.cfg = cfg
         self.lib = C.CDLL(build_ref(optimized=optimized))
         L = self.lib

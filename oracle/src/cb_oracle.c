@@ -365,6 +365,56 @@ static void rusanov(const double QL[5], const double QR[5], double pL, double pR
   F[4] = 0.5 * ((pL + QL[4]) * uconL + (pR + QR[4]) * uconR) - 0.5 * SA * (QR[4] - QL[4]);
 }
 
+/* Roe's approximate Riemann solver (P. L. Roe, J. Comput. Phys. 43, 1981)
+ * on a curvilinear face with area vector h: the central part is the same
+ * average of the two physical fluxes as the Rusanov flux above; the
+ * dissipation is |A~|(QR - QL) of the Roe-averaged Jacobian along n = h/|h|,
+ * scaled by |h|, with Harten's entropy fix on the acoustic waves
+ * (A. Harten, J. Comput. Phys. 49, 1983): |l| < delta -> (l^2 + delta^2) /
+ * (2 delta), delta = 0.1 c~.  gamma is the flux code's 1.4.  No counterpart
+ * in the reference. */
+static void roe(const double QL[5], const double QR[5], double pL, double pR, const double h[3],
+                int use_qr_for_l, int ucon_r_from_l, double F[5]) {
+  double uconL, uconR;
+  if (use_qr_for_l)
+    uconL = (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
+  else
+    uconL = (h[0] * (QL[1] / QL[0]) + h[1] * (QL[2] / QL[0]) + h[2] * (QL[3] / QL[0]));
+  if (ucon_r_from_l)
+    uconR = uconL;
+  else
+    uconR = (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
+  const double g = GAMMA_CONV;
+  const double area = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+  const double nx = h[0] / area, ny = h[1] / area, nz = h[2] / area;
+  const double sl = sqrt(QL[0]), sr = sqrt(QR[0]), wl = sl / (sl + sr), wr = sr / (sl + sr);
+  const double uL = QL[1] / QL[0], vL = QL[2] / QL[0], zL = QL[3] / QL[0];
+  const double uR = QR[1] / QR[0], vR = QR[2] / QR[0], zR = QR[3] / QR[0];
+  const double HL = (QL[4] + pL) / QL[0], HR = (QR[4] + pR) / QR[0];
+  const double rt = sl * sr, ut = wl * uL + wr * uR, vt = wl * vL + wr * vR, zt = wl * zL + wr * zR;
+  const double Ht = wl * HL + wr * HR, q2 = ut * ut + vt * vt + zt * zt;
+  const double c2 = (g - 1.0) * (Ht - 0.5 * q2), ct = sqrt(fabs(c2));
+  const double Unt = ut * nx + vt * ny + zt * nz;
+  const double dp = pR - pL, dr = QR[0] - QL[0];
+  const double du = uR - uL, dv = vR - vL, dz = zR - zL, dUn = du * nx + dv * ny + dz * nz;
+  const double a1 = (dp - rt * ct * dUn) / (2.0 * c2), a2 = dr - dp / c2, a3 = (dp + rt * ct * dUn) / (2.0 * c2);
+  double l1 = fabs(Unt - ct), l2 = fabs(Unt), l3 = fabs(Unt + ct);
+  const double delta = 0.1 * ct;
+  if (l1 < delta) l1 = (l1 * l1 + delta * delta) / (2.0 * delta);
+  if (l3 < delta) l3 = (l3 * l3 + delta * delta) / (2.0 * delta);
+  const double s1 = l1 * a1, s2 = l2 * a2, s3 = l3 * a3, ss = l2 * rt;
+  double D[5];
+  D[0] = s1 + s2 + s3;
+  D[1] = s1 * (ut - ct * nx) + s2 * ut + s3 * (ut + ct * nx) + ss * (du - dUn * nx);
+  D[2] = s1 * (vt - ct * ny) + s2 * vt + s3 * (vt + ct * ny) + ss * (dv - dUn * ny);
+  D[3] = s1 * (zt - ct * nz) + s2 * zt + s3 * (zt + ct * nz) + ss * (dz - dUn * nz);
+  D[4] = s1 * (Ht - Unt * ct) + s2 * 0.5 * q2 + s3 * (Ht + Unt * ct) + ss * (ut * du + vt * dv + zt * dz - Unt * dUn);
+  F[0] = 0.5 * (QL[0] * uconL + QR[0] * uconR) - 0.5 * area * D[0];
+  for (int a = 0; a < 3; a++)
+    F[1 + a] = 0.5 * ((QL[1 + a] * uconL + QR[1 + a] * uconR) + (pL * h[a] + pR * h[a])) - 0.5 * area * D[1 + a];
+  F[4] = 0.5 * ((pL + QL[4]) * uconL + (pR + QR[4]) * uconR) - 0.5 * area * D[4];
+}
+
 typedef struct {
   const cbo_config *c;
   geom G;
@@ -458,7 +508,8 @@ static void conv_face_std(const ctx_t *C, int d, int i, int j, int k, double F[5
   face_metric(C, d, n0, h);
   int use_qr_l = (pos == m - 2 && c->bctype[2 * d + 1] == 1);
   int r_from_l = (pos == 0 && c->bctype[2 * d] == 1);
-  rusanov(QL, QR, pL, pR, h, use_qr_l, r_from_l, F);
+  if (c->flux == 1) roe(QL, QR, pL, pR, h, use_qr_l, r_from_l, F);
+  else rusanov(QL, QR, pL, pR, h, use_qr_l, r_from_l, F);
 }
 
 /* formConvectionLES face flux (rhs.c:3466-3705 and its eta/zeta copies). */
@@ -543,7 +594,8 @@ static void conv_face_les(const ctx_t *C, int d, int i, int j, int k, const doub
     recon_weno(C, d, pos, n0, el, er, 0, QL, QR, &pL, &pR);
   }
   double Fw[5];
-  rusanov(QL, QR, pL, pR, h, 0, 0, Fw);
+  if (c->flux == 1) roe(QL, QR, pL, pR, h, 0, 0, Fw);
+  else rusanov(QL, QR, pL, pR, h, 0, 0, Fw);
   for (int a = 0; a < 5; a++) F[a] = Fw[a] * (1.0 - sigma) + Fc[a] * sigma;
 }
 

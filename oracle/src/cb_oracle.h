@@ -37,6 +37,7 @@ typedef struct {
   int calc_sigma;          /* -calc_sigma: pressure shock sensor for the hybrid weights */
   double s_x_min, s_y_min, s_z_min; /* -s_x_min/-s_y_min/-s_z_min: lower bounds of the sensor */
   double sigma_thrsh;      /* -sigma_thrsh: ks of the smoothness ratio (default 1e-5) */
+  int flux;                /* upwind flux: 0 Rusanov (the reference's), 1 Roe with Harten's entropy fix */
 } cbo_config;
 
 /* Fill the two ghost layers of each periodic direction of one padded plane

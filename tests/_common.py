@@ -54,7 +54,7 @@ def gpu_block(cfg, precision="fp64"):
                  isothermal=cfg.isothermal, s_x=cfg.s_x, s_y=cfg.s_y, s_z=cfg.s_z, ren=cfg.ren, ma=cfg.ma,
                  pr=cfg.pr, gamma=cfg.gamma, dt=cfg.dt, st=cfg.st, cs_const=cfg.cs_const, ci=cfg.ci,
                  ratio=cfg.ratio, precision=precision, calc_sigma=cfg.calc_sigma, s_x_min=cfg.s_x_min,
-                 s_y_min=cfg.s_y_min, s_z_min=cfg.s_z_min, sigma_thrsh=cfg.sigma_thrsh)
+                 s_y_min=cfg.s_y_min, s_z_min=cfg.s_z_min, sigma_thrsh=cfg.sigma_thrsh, flux=cfg.flux)
 
 
 def per_field_rel_l2(a, b):
