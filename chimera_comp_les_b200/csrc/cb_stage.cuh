@@ -613,6 +613,7 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
       if (u >= S_NXF) continue;
     } else if (v < 512) {
       d = 1; u = v - 256;
+      if (u >= S_NYF) continue;  // (exactly full for the 32 x 7 tile)
       const int fx = u % BX, fy = u / BX;
       fi = i0 + fx; fj = j0 - 1 + fy;
       a = NRef{0, fy + 1, fx + 2};
