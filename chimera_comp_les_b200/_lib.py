@@ -8,12 +8,25 @@ from __future__ import annotations
 import ctypes as C
 import os
 
+import numpy as np
+
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libchimera_b200.so")
 
 CB_OK, CB_E_ARG, CB_E_CUDA, CB_E_STATE, CB_E_NONFINITE, CB_E_UNSUPPORTED = 0, 1, 2, 3, 4, 5
 CB_FP64, CB_MIXED = 0, 1
 CB_PHASE_STATE, CB_PHASE_NUT, CB_PHASE_STAGE = 0, 1, 2
+CB_IBM_MAX_BODIES = 16
+
+# cb_ibm_info: one entry of an immersed body's interpolation list (the IBMInfo
+# fields ibm_interpolation_advanced reads), 144 bytes.
+IBM_INFO_DTYPE = np.dtype([
+    ("ni", "<i4"), ("nj", "<i4"), ("nk", "<i4"), ("cell", "<i4"),
+    ("i1", "<i4"), ("j1", "<i4"), ("k1", "<i4"), ("i2", "<i4"), ("j2", "<i4"), ("k2", "<i4"),
+    ("i3", "<i4"), ("j3", "<i4"), ("k3", "<i4"), ("pad", "<i4"),
+    ("cr1", "<f8"), ("cr2", "<f8"), ("cr3", "<f8"), ("cs1", "<f8"), ("cs2", "<f8"), ("cs3", "<f8"),
+    ("d_s", "<f8"), ("d_i", "<f8"), ("pmin", "<f8", (3,)),
+])
 
 
 class CbConfig(C.Structure):
@@ -83,6 +96,16 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.cb_launches_per_step.restype = C.c_int
     lib.cb_last_error.argtypes = [P]
     lib.cb_last_error.restype = C.c_char_p
+    # immersed bodies
+    for name, args in [
+        ("cb_ibm_set_surface", [P, C.c_int, C.c_int, C.c_int, P, P, P, D, D, D]),
+        ("cb_ibm_set_velocity", [P, C.c_int, D, D]), ("cb_ibm_set_list", [P, C.c_int, C.c_int, P, D]),
+        ("cb_ibm_count", [P, C.c_int]), ("cb_ibm_set_options", [P, C.c_int, C.c_int]),
+        ("cb_ibm_interpolate", [P, C.c_int, C.c_int]),
+    ]:
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
     # batched multi-block form
     I = C.c_int
     IP = C.POINTER(C.c_int)

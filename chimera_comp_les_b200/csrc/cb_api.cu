@@ -15,11 +15,13 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/chimera_b200.h"
 #include "cb_aux.cuh"
 #include "cb_common.cuh"
+#include "cb_ibm.cuh"
 #include "cb_launch.h"
 #include "cb_stage.cuh"
 
@@ -31,6 +33,24 @@ constexpr int BX = SBX, BY = SBY;
 
 struct GraphSlot {
   cudaGraphExec_t exec = nullptr;
+};
+
+// One immersed body: its surface (IBMNodes) and interpolation list (IBMList)
+// in device memory.
+struct IbmBody {
+  int n_v = 0, n_elmt = 0, n = 0;
+  void *surf = nullptr;  // nf (3 per element), u, uold (3 per vertex), tri (3 per element)
+  void *list = nullptr;  // node, donors, weights, sweep output
+  double *nf = nullptr, *u = nullptr, *uold = nullptr;
+  int *tri = nullptr;
+  int4 *node = nullptr;
+  long long *don = nullptr;
+  double *w = nullptr, *out = nullptr;
+  IbmDev dev() const {
+    IbmDev d;
+    d.n = n; d.node = node; d.don = don; d.w = w; d.tri = tri; d.nf = nf; d.u = u; d.uold = uold; d.out = out;
+    return d;
+  }
 };
 
 }  // namespace
@@ -66,6 +86,10 @@ struct cb_ctx {
   int kchunk = 16;
   GraphSlot graphs[3][4];
   bool use_graphs = true;
+  // immersed bodies: interpolation after the stages, then FormBCS(user, 0)
+  IbmBody ibm[CB_IBM_MAX_BODIES];
+  double *spare = nullptr;  // 5 planes: the state FormBCS(user, 0) reads as lQ
+  int ibm_twoD = 0, ibm_wallfunction = 0;
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, int>> ev_pairs_rhs, ev_pairs_other;
@@ -255,6 +279,50 @@ static void rk_coeffs(const cb_ctx *c, int s, double *alfa, double *beta) {
   *beta = b[s];
 }
 
+static bool ibm_active(const cb_ctx *c) {
+  for (const auto &b : c->ibm)
+    if (b.n > 0) return true;
+  return false;
+}
+
+// Five sweeps of ibm_interpolation_advanced for one body on the current state.
+static int ibm_sweeps(cb_ctx *c, const IbmBody &b, int add_dundt) {
+  const IbmDev d = b.dev();
+  const int g = grid_for(c, b.n);
+  const int slip = (c->cfg.inviscid || c->ibm_wallfunction == 3) ? 1 : 0;  // ibm_iso.c:2721
+  const int iso1 = c->cfg.isothermal == 1 ? 1 : 0;
+  for (int s = 0; s < IBM_SWEEPS; s++) {
+    ibm_interp_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), d, add_dundt,
+                                                c->ibm_twoD, slip, iso1);
+    ibm_scatter_kernel<<<g, 256, 0, c->stream>>>(c->dc, c->ptab + 5 * c->cur, d);
+  }
+  CB_CUDA(c, cudaGetLastError());
+  return CB_OK;
+}
+
+// FormBCS(user, 0) after the interpolation (solvers.c:286): the boundary of
+// the current state from a snapshot of it (the reference's lQ), Qold from
+// buffer `old`, then the ghost wrap FormBCS ends with (rhs.c:1305-1308).
+static int formbcs_zero(cb_ctx *c, int old) {
+  CB_CUDA(c, cudaMemcpyAsync(c->spare, c->qb[c->cur][0], sizeof(double) * 5 * c->plane, cudaMemcpyDeviceToDevice,
+                             c->stream));
+  DevFields F = fields_for(c, c->cur, old, c->cur);
+  for (int q = 0; q < 5; q++) F.q[q] = c->spare + c->plane * q;
+  const long long shell = shell_count(c->dc);
+  if (c->fully_periodic) {
+    bc_periodic_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, F);
+  } else {
+    const long long face = (long long)std::max(c->dc.mx, c->dc.my) * std::max(c->dc.my, c->dc.mz);
+    for (int dir = 0; dir < 3; dir++) bc_face_kernel<<<grid_for(c, face), 256, 0, c->stream>>>(c->dc, F, dir, 0.0);
+    for (int dir = 0; dir < 3; dir++)
+      if (c->dc.bctype[2 * dir] == 7)
+        bc_periodic_dir_kernel<<<grid_for(c, face), 256, 0, c->stream>>>(c->dc, F, dir);
+    ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, c->ptab + 5 * c->cur, 5);
+  }
+  CB_CUDA(c, cudaGetLastError());
+  return CB_OK;
+}
+
 // Enqueue one time step (no graph).
 static int enqueue_step(cb_ctx *c) {
   if (c->cfg.les && !c->cfg.inviscid) {
@@ -300,6 +368,16 @@ static int enqueue_step(cb_ctx *c) {
     in = out;
   }
   c->cur = in;
+  if (ibm_active(c)) {  // solvers.c:282-288
+    TimedScope ts(c, false);
+    for (const auto &b : c->ibm)
+      if (b.n > 0) {
+        int e = ibm_sweeps(c, b, 1);
+        if (e) return e;
+      }
+    int e = formbcs_zero(c, old);
+    if (e) return e;
+  }
   return CB_OK;
 }
 
@@ -476,6 +554,11 @@ void cb_destroy(cb_ctx *c) {
   if (c->arena_mixed) cudaFree(c->arena_mixed);
   if (c->ptab4) cudaFree(c->ptab4);
   if (c->sig_arena) cudaFree(c->sig_arena);
+  for (auto &b : c->ibm) {
+    if (b.surf) cudaFree(b.surf);
+    if (b.list) cudaFree(b.list);
+  }
+  if (c->spare) cudaFree(c->spare);
   if (c->ptab) cudaFree(c->ptab);
   if (c->status) cudaFree(c->status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -495,7 +578,12 @@ int cb_launches_per_step(const cb_ctx *c) {
     per_stage = 1 + 1 + 3 + 1;
     for (int d = 0; d < 3; d++) per_stage += c->cfg.bctype[2 * d] == 7;
   }
-  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0);
+  int ib = 0;
+  if (ibm_active(c)) {
+    for (const auto &b : c->ibm) ib += b.n > 0 ? 2 * IBM_SWEEPS : 0;
+    ib += c->fully_periodic ? 1 : per_stage - 2;  // FormBCS(user, 0): no stage kernel, no RK combine
+  }
+  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0) + ib;
 }
 
 static int upload_planes(cb_ctx *c, const double *host, int nc, int pt_first, bool pinned_hint) {
@@ -812,6 +900,165 @@ int cb_capture_graph(cb_ctx *c) {
   if (!c) return CB_E_ARG;
   if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set");
   c->use_graphs = true;
+  return CB_OK;
+}
+
+// ------------------------------------------------------ immersed boundary --
+static int ibm_body(cb_ctx *c, int ibi, IbmBody **b) {
+  if (!c) return CB_E_ARG;
+  if (ibi < 0 || ibi >= CB_IBM_MAX_BODIES) return fail(c, CB_E_ARG, "body index out of range");
+  *b = &c->ibm[ibi];
+  return CB_OK;
+}
+
+static void ibm_drop_list(IbmBody &b) {
+  if (b.list) cudaFree(b.list);
+  b.list = nullptr;
+  b.node = nullptr; b.don = nullptr; b.w = nullptr; b.out = nullptr;
+  b.n = 0;
+}
+
+int cb_ibm_set_surface(cb_ctx *c, int ibi, int n_v, int n_elmt, const int *nv1, const int *nv2, const int *nv3,
+                       const double *nf_x, const double *nf_y, const double *nf_z) {
+  IbmBody *b;
+  int e = ibm_body(c, ibi, &b);
+  if (e) return e;
+  if (n_v < 1 || n_elmt < 1 || !nv1 || !nv2 || !nv3 || !nf_x || !nf_y || !nf_z)
+    return fail(c, CB_E_ARG, "surface needs n_v, n_elmt >= 1 and all arrays");
+  std::vector<int> tri(3 * (size_t)n_elmt);
+  std::vector<double> h(3 * (size_t)n_elmt + 6 * (size_t)n_v, 0.0);
+  for (int t = 0; t < n_elmt; t++) {
+    const int v[3] = {nv1[t], nv2[t], nv3[t]};
+    for (int a = 0; a < 3; a++) {
+      if (v[a] < 0 || v[a] >= n_v) return fail(c, CB_E_ARG, "element vertex index out of range");
+      tri[3 * (size_t)t + a] = v[a];
+    }
+    h[3 * (size_t)t] = nf_x[t]; h[3 * (size_t)t + 1] = nf_y[t]; h[3 * (size_t)t + 2] = nf_z[t];
+  }
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));  // graphs in flight may read the old arrays
+  ibm_drop_list(*b);
+  if (b->surf) cudaFree(b->surf);
+  b->surf = nullptr;
+  const size_t nd = h.size();
+  CB_CUDA(c, cudaMalloc(&b->surf, sizeof(double) * nd + sizeof(int) * tri.size()));
+  b->nf = (double *)b->surf;
+  b->u = b->nf + 3 * (size_t)n_elmt;
+  b->uold = b->u + 3 * (size_t)n_v;
+  b->tri = (int *)(b->nf + nd);
+  b->n_v = n_v;
+  b->n_elmt = n_elmt;
+  CB_CUDA(c, cudaMemcpyAsync(b->nf, h.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaMemcpyAsync(b->tri, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  invalidate_graphs(c);
+  return CB_OK;
+}
+
+int cb_ibm_set_velocity(cb_ctx *c, int ibi, const double *u, const double *uold) {
+  IbmBody *b;
+  int e = ibm_body(c, ibi, &b);
+  if (e) return e;
+  if (!u || !uold) return CB_E_ARG;
+  if (!b->surf) return fail(c, CB_E_STATE, "set the body's surface first");
+  // stream-ordered: steps enqueued before this call read the previous values
+  CB_CUDA(c, cudaMemcpyAsync(b->u, u, sizeof(double) * 3 * b->n_v, cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaMemcpyAsync(b->uold, uold, sizeof(double) * 3 * b->n_v, cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const double *coor) {
+  IbmBody *b;
+  int e = ibm_body(c, ibi, &b);
+  if (e) return e;
+  if (n < 0 || (n > 0 && (!list || !coor))) return CB_E_ARG;
+  if (n > 0 && !b->surf) return fail(c, CB_E_STATE, "set the body's surface first");
+  if (n > 0 && c->cfg.isothermal == 2)
+    return fail(c, CB_E_UNSUPPORTED, "the characteristic isothermal IB wall (isothermal 2) is not built");
+  const int m[3] = {c->cfg.mx, c->cfg.my, c->cfg.mz};
+  const bool per[3] = {c->cfg.bctype[0] == 7, c->cfg.bctype[2] == 7, c->cfg.bctype[4] == 7};
+  // a node listed twice keeps its last entry
+  std::unordered_map<long long, int> last;
+  for (int t = 0; t < n; t++) {
+    const cb_ibm_info &f = list[t];
+    const int nd[3] = {f.ni, f.nj, f.nk};
+    for (int d = 0; d < 3; d++)
+      if (nd[d] < 0 || nd[d] >= m[d]) return fail(c, CB_E_ARG, "interface node outside the block");
+    const int dn[9] = {f.i1, f.j1, f.k1, f.i2, f.j2, f.k2, f.i3, f.j3, f.k3};
+    for (int a = 0; a < 9; a++) {
+      const int d = a % 3, lo = per[d] ? -2 : 0, hi = per[d] ? m[d] + 1 : m[d] - 1;
+      if (dn[a] < lo || dn[a] > hi) return fail(c, CB_E_ARG, "donor node outside the ghosted block");
+    }
+    if (f.cell < -1 || f.cell >= b->n_elmt) return fail(c, CB_E_ARG, "surface element index out of range");
+    last[((long long)f.nk * m[1] + f.nj) * m[0] + f.ni] = t;
+  }
+  std::vector<int> keep;
+  keep.reserve(last.size());
+  for (int t = 0; t < n; t++) {
+    const cb_ibm_info &f = list[t];
+    if (last[((long long)f.nk * m[1] + f.nj) * m[0] + f.ni] == t) keep.push_back(t);
+  }
+  const int nk = (int)keep.size();
+  std::vector<int4> node(nk);
+  std::vector<long long> don(3 * (size_t)nk);
+  std::vector<double> w((size_t)IBM_NW * nk);
+  for (int t = 0; t < nk; t++) {
+    const cb_ibm_info &f = list[keep[t]];
+    node[t] = make_int4(f.ni, f.nj, f.nk, f.cell);
+    don[3 * (size_t)t] = gidx(c->dc, f.i1, f.j1, f.k1);
+    don[3 * (size_t)t + 1] = gidx(c->dc, f.i2, f.j2, f.k2);
+    don[3 * (size_t)t + 2] = gidx(c->dc, f.i3, f.j3, f.k3);
+    const double *x = coor + 3 * (((size_t)f.nk * m[1] + f.nj) * m[0] + f.ni);
+    const double v[IBM_NW] = {f.cr1, f.cr2, f.cr3, f.cs1, f.cs2, f.cs3, f.d_s, f.d_s + f.d_i,
+                              x[0] - f.pmin[0], x[1] - f.pmin[1], x[2] - f.pmin[2]};  // ibm_iso.c:2653, 2662-2664
+    for (int a = 0; a < IBM_NW; a++) w[(size_t)a * nk + t] = v[a];
+  }
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  ibm_drop_list(*b);
+  invalidate_graphs(c);
+  if (nk == 0) return CB_OK;
+  if (!c->spare) CB_CUDA(c, cudaMalloc(&c->spare, sizeof(double) * 5 * c->plane));
+  const size_t bytes = sizeof(int4) * nk + sizeof(long long) * 3 * nk + sizeof(double) * (IBM_NW + 5) * nk;
+  CB_CUDA(c, cudaMalloc(&b->list, bytes));
+  b->node = (int4 *)b->list;
+  b->don = (long long *)(b->node + nk);
+  b->w = (double *)(b->don + 3 * (size_t)nk);
+  b->out = b->w + (size_t)IBM_NW * nk;
+  b->n = nk;
+  CB_CUDA(c, cudaMemcpyAsync(b->node, node.data(), sizeof(int4) * nk, cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaMemcpyAsync(b->don, don.data(), sizeof(long long) * don.size(), cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaMemcpyAsync(b->w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_ibm_count(const cb_ctx *c, int ibi) {
+  if (!c || ibi < 0 || ibi >= CB_IBM_MAX_BODIES) return -1;
+  return c->ibm[ibi].n;
+}
+
+int cb_ibm_set_options(cb_ctx *c, int twoD, int wallfunction) {
+  if (!c) return CB_E_ARG;
+  if (twoD < 0 || twoD > 3) return fail(c, CB_E_ARG, "twoD must be 0..3");
+  if (wallfunction == 1 || wallfunction == 2)
+    return fail(c, CB_E_UNSUPPORTED, "log-law wall functions (wallfunction 1/2) are not built");
+  if (wallfunction != 0 && wallfunction != 3) return fail(c, CB_E_ARG, "wallfunction must be 0 or 3");
+  c->ibm_twoD = twoD;
+  c->ibm_wallfunction = wallfunction;
+  invalidate_graphs(c);
+  return CB_OK;
+}
+
+int cb_ibm_interpolate(cb_ctx *c, int ibi, int add_dundt) {
+  IbmBody *b;
+  int e = ibm_body(c, ibi, &b);
+  if (e) return e;
+  if (!c->have_state) return fail(c, CB_E_STATE, "no state uploaded");
+  if (b->n > 0) {
+    e = ibm_sweeps(c, *b, add_dundt ? 1 : 0);
+    if (e) return e;
+  }
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
   return CB_OK;
 }
 

@@ -12,6 +12,13 @@ AoS order (mz, my, mx, ncomp):
   Compute_eddy_viscosity_LES()       les.c:1477       (cb_eddy_viscosity)
   RungeKutta(nsteps) / Flow_Solver   solvers.c:13,223 (cb_rk_step)
   EqOfState()                        rhs.c:4820       (pressure download)
+  ibm_interpolation_advanced(ibi)    ibm_iso.c:2572   (cb_ibm_interpolate)
+
+Immersed bodies: ``set_ibm_surface`` / ``set_ibm_velocity`` / ``set_ibm_list``
+hand over what the reference's host search built (IBMNodes and
+user->ibmlist[ibi]); every ``RungeKutta`` step then interpolates each body
+after the stages and applies FormBCS(user, 0) on the device
+(solvers.c:282-288).
 
 Options may be given as the reference's command-line flags via
 ``Block.from_options``.
@@ -137,6 +144,38 @@ class Block:
         self._check(self.lib.cb_sync(self._ctx))
 
     upload_state = SetInitialCondition
+
+    # ------------------------------------------------------ immersed bodies --
+    def set_ibm_surface(self, ibi: int, surface: dict):
+        """IBMNodes of body ibi: nv1, nv2, nv3 (vertex indices per triangle),
+        nf_x, nf_y, nf_z (unit normals) and x (for the vertex count)."""
+        tri = [np.ascontiguousarray(surface[k], dtype=np.int32) for k in ("nv1", "nv2", "nv3")]
+        nf = [np.ascontiguousarray(surface[k], dtype=np.float64) for k in ("nf_x", "nf_y", "nf_z")]
+        n_v = int(surface["n_v"]) if "n_v" in surface else len(surface["x"])
+        self._check(self.lib.cb_ibm_set_surface(self._ctx, ibi, n_v, len(tri[0]), *[t.ctypes.data for t in tri],
+                                                *[dptr(a) for a in nf]))
+
+    def set_ibm_velocity(self, ibi: int, u: np.ndarray, uold: np.ndarray):
+        """Vertex velocities ibm->u and ibm->uold, shape (n_v, 3)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        uold = np.ascontiguousarray(uold, dtype=np.float64)
+        self._check(self.lib.cb_ibm_set_velocity(self._ctx, ibi, dptr(u), dptr(uold)))
+
+    def set_ibm_list(self, ibi: int, info: np.ndarray, coor: np.ndarray):
+        """Interpolation list of body ibi (structured array of _lib.IBM_INFO_DTYPE,
+        in the reference's list order) and the node coordinates."""
+        a = np.ascontiguousarray(info, dtype=_lib.IBM_INFO_DTYPE)
+        c = _f64(coor, self.shape + (3,))
+        self._check(self.lib.cb_ibm_set_list(self._ctx, ibi, a.size, a.ctypes.data if a.size else None, dptr(c)))
+
+    def ibm_count(self, ibi: int) -> int:
+        return int(self.lib.cb_ibm_count(self._ctx, ibi))
+
+    def set_ibm_options(self, twoD: int = 0, wallfunction: int = 0):
+        self._check(self.lib.cb_ibm_set_options(self._ctx, twoD, wallfunction))
+
+    def ibm_interpolation_advanced(self, ibi: int = 0, Add_dUndt: int = 1):
+        self._check(self.lib.cb_ibm_interpolate(self._ctx, ibi, Add_dUndt))
 
     def formRHS(self, istage: int = 0) -> np.ndarray:
         out = np.empty(self.shape + (5,))

@@ -207,3 +207,45 @@ def multiblock_set(seed: int = 2024, nblocks: int = 24, ranges=((32, 160), (32, 
     dt = math.floor(cfl / lam * 1e5) / 1e5
     return dict(dims=[(n[0] + 2, n[1] + 2, n[2] + 2) for n in uniq], coords=coords, q=qs,
                 perm=[int(x) for x in perm], dt=dt)
+
+
+def sphere_surface(radius: float, center=(0.0, 0.0, 0.0), subdiv: int = 3):
+    """Triangulated sphere (a subdivided icosahedron projected onto the
+    sphere), in the arrays of the reference's IBM surface (IBMNodes,
+    variables.h:91-118): vertex coordinates x, y, z (n_v each), triangles
+    nv1, nv2, nv3 (n_elmt each, counter-clockwise seen from outside), and the
+    unit normals nf_x, nf_y, nf_z of each triangle, (p2 - p1) x (p3 - p1)
+    normalised, pointing out of the body (ibm_read_ucd
+    forms them the same way, ibm_io.c:1718-1732)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    v = [np.array(p, dtype=np.float64) / np.linalg.norm(p) for p in verts]
+    for _ in range(subdiv):
+        mid = {}
+
+        def midpoint(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                m = v[a] + v[b]
+                v.append(m / np.linalg.norm(m))
+                mid[key] = len(v) - 1
+            return mid[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    P = np.array(v) * radius + np.asarray(center, dtype=np.float64)
+    tri = np.array(faces, dtype=np.int32)
+    d12 = P[tri[:, 1]] - P[tri[:, 0]]
+    d13 = P[tri[:, 2]] - P[tri[:, 0]]
+    n = np.cross(d12, d13)
+    n /= np.linalg.norm(n, axis=1)[:, None]
+    return {"x": P[:, 0].copy(), "y": P[:, 1].copy(), "z": P[:, 2].copy(),
+            "nv1": tri[:, 0].copy(), "nv2": tri[:, 1].copy(), "nv3": tri[:, 2].copy(),
+            "nf_x": n[:, 0].copy(), "nf_y": n[:, 1].copy(), "nf_z": n[:, 2].copy()}

@@ -19,7 +19,8 @@
  *     not thread-safe (one context per host thread, as the reference runs one
  *     rank per process).
  *   - No function allocates device memory except cb_create, cb_rhs (first
- *     call: its output planes), cb_capture_graph (graph instantiation) and,
+ *     call: its output planes), cb_capture_graph (graph instantiation),
+ *     cb_ibm_set_surface and cb_ibm_set_list (immersed-body arrays) and,
  *     in the batched form, cb_batch_create, cb_batch_set_halo_map and
  *     cb_batch_autotune (item lists, maps, graphs).
  */
@@ -148,6 +149,54 @@ int cb_cfl_dt(cb_ctx *ctx, double cfl, double *dt, double *lambda_max);
  * out: candidates timed).  Does not advance the state.  No counterpart in the
  * reference (CPU loops have no launch shape). */
 int cb_autotune(cb_ctx *ctx, int ncand, const int *cand, double *ms_out, int *nout, int *best_kchunk);
+
+/* ---- immersed boundary (ibm_interpolation_advanced, ibm_iso.c:2572-2880) ----
+ *
+ * The reference's host search (ibm_search_advanced, ibm_iso.c:87) stays on
+ * the host: it sets nvert (pass it with cb_set_nvert) and builds one
+ * interpolation list per body (user->ibmlist[ibi]).  Hand each list and the
+ * body's surface to the context; every cb_rk_step then runs, after the RK
+ * stages, the interpolation of each body in order (Add_dUndt = 1) and
+ * FormBCS(user, 0), as RungeKutta does when -imm is set
+ * (solvers.c:282-288), without a host round trip.
+ *
+ * One list entry: the IBMInfo fields the interpolation reads
+ * (variables.h:50-89), same layout as the oracle's cbo_ibm_info. */
+typedef struct {
+  int ni, nj, nk;           /* the interface node (natural indices, 0 <= n < m) */
+  int cell;                 /* surface element of the interception point, -1: none */
+  int i1, j1, k1, i2, j2, k2, i3, j3, k3; /* donor nodes */
+  int pad;                  /* unused (aligns the doubles) */
+  double cr1, cr2, cr3;     /* donor weights */
+  double cs1, cs2, cs3;     /* weights of the element's vertices at the interception point */
+  double d_s, d_i;          /* node -> surface and surface -> donor point distances */
+  double pmin[3];           /* interception point */
+} cb_ibm_info;
+
+#define CB_IBM_MAX_BODIES 16
+
+/* IBMNodes of body ibi (variables.h:91-118): triangles nv1..nv3 (vertex
+ * indices) and unit normals nf_x..nf_z of each of the n_elmt elements;
+ * vertex velocities start at zero (ibm_read_ucd, ibm_io.c:1643-1653).
+ * Replaces the body's surface and drops its list.  Allocates. */
+int cb_ibm_set_surface(cb_ctx *ctx, int ibi, int n_v, int n_elmt, const int *nv1, const int *nv2, const int *nv3,
+                       const double *nf_x, const double *nf_y, const double *nf_z);
+/* Vertex velocities ibm->u and ibm->uold (n_v x (x,y,z) each, Cmpnts). */
+int cb_ibm_set_velocity(cb_ctx *ctx, int ibi, const double *u, const double *uold);
+/* The interpolation list of body ibi in the order the reference walks it
+ * (IBMList head first), with coor the node coordinates passed to
+ * cb_set_grid.  A node listed twice keeps its last entry (the later write
+ * wins in the reference).  n = 0 removes the body's list.  Allocates. */
+int cb_ibm_set_list(cb_ctx *ctx, int ibi, int n, const cb_ibm_info *list, const double *coor);
+/* Entries of body ibi's list after duplicate nodes were dropped. */
+int cb_ibm_count(const cb_ctx *ctx, int ibi);
+/* -twoD (0, or 1/2/3: drop x/y/z from the normal and the velocity) and
+ * -wallfunction (0: noslip unless -inv, 3: freeslip; 1 and 2, the log-law wall
+ * functions, return CB_E_UNSUPPORTED). */
+int cb_ibm_set_options(cb_ctx *ctx, int twoD, int wallfunction);
+/* One call of ibm_interpolation_advanced(user, ibm, ibi, Add_dUndt) on the
+ * current state: five sweeps, each ending with the ghost update. */
+int cb_ibm_interpolate(cb_ctx *ctx, int ibi, int add_dundt);
 
 /* Waits for the context's stream and checks the device status word
  * (CB_E_NONFINITE when a NaN/Inf or non-positive rho/p was produced). */

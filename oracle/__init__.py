@@ -67,6 +67,9 @@ class Config:
     s_z_min: float = 0.0
     sigma_thrsh: float = 1e-5
     flux: int = 0  # 0 Rusanov (the reference's), 1 Roe (no reference counterpart)
+    immersed: int = 0      # -imm: run the IB interpolation after the stages (solvers.c:282-288)
+    wallfunction: int = 0  # -wallfunction: 0 noslip, 3 freeslip at IB nodes
+    twoD: int = 0          # -twoD: 1/2/3 drops x/y/z from the IB normal and velocity
 
     def ref_options(self) -> str:
         o = [
@@ -76,7 +79,8 @@ class Config:
             ("-s_y", repr(float(self.s_y))), ("-s_z", repr(float(self.s_z))),
             ("-ren", repr(float(self.ren))), ("-Ma", repr(float(self.ma))),
             ("-Pr", repr(float(self.pr))), ("-gamma", repr(float(self.gamma))),
-            ("-dt", repr(float(self.dt))), ("-visT", 0), ("-twoD", 0), ("-TwoD", 0),
+            ("-dt", repr(float(self.dt))), ("-visT", 0), ("-twoD", self.twoD), ("-TwoD", 0),
+            ("-imm", self.immersed), ("-wallfunction", self.wallfunction),
             ("-calc_sigma", self.calc_sigma), ("-s_x_min", repr(float(self.s_x_min))),
             ("-s_y_min", repr(float(self.s_y_min))), ("-s_z_min", repr(float(self.s_z_min))),
             ("-sigma_thrsh", repr(float(self.sigma_thrsh))),
@@ -184,6 +188,15 @@ class Oracle:
         L.cbo_steps.restype = C.c_int
         L.cbo_bc_periodic.argtypes = [C.c_void_p, PP, PP]
         L.cbo_bc_periodic.restype = C.c_int
+        L.cbo_formbcs.argtypes = [C.c_void_p, C.c_double, PP, PP, PP, D, PP]
+        L.cbo_formbcs.restype = C.c_int
+        L.cbo_ibm_interpolate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, PP, PP, D, C.c_int,
+                                          C.c_int, C.c_int]
+        L.cbo_ibm_interpolate.restype = C.c_int
+        L.cbo_steps_ibm.argtypes = [C.c_void_p, C.c_int, PP, PP, PP, C.POINTER(C.c_int), D, PP, PP, PP, D, D,
+                                    C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, PP, D, C.POINTER(C.c_int),
+                                    C.c_int, C.c_int]
+        L.cbo_steps_ibm.restype = C.c_int
         self._cp = C.byref(self.c)
 
     def zeros(self, nc: int) -> np.ndarray:
@@ -251,6 +264,110 @@ class Oracle:
     def initial_state(self, q_nat: np.ndarray) -> dict:
         q = self.fill_ghosts(to_padded(self.cfg, q_nat))
         return {"q": q, "qold": q.copy(), "quc": np.zeros_like(q), "have_uc": 0, "nut": self.zeros(1)}
+
+    def formbcs(self, alfa: float, lq: np.ndarray, qold: np.ndarray, met, q: np.ndarray) -> np.ndarray:
+        """FormBCS(user, alfa) on q (padded 5, in/out) from the ghosted lq."""
+        e = self.lib.cbo_formbcs(self._cp, alfa, _ptrs(list(lq)), _ptrs(list(qold)), _ptrs(list(met["zet"])),
+                                 _dp(met["aj"][0]), _ptrs(list(q)))
+        if e:
+            raise RuntimeError(f"cbo_formbcs failed with status {e}")
+        return q
+
+    def ibm_interpolate(self, surface: "IbmSurface", info: np.ndarray, coor_pad: np.ndarray, q: np.ndarray,
+                        p: np.ndarray, add_dundt: int = 1) -> None:
+        """ibm_interpolation_advanced on q (padded 5) and p (padded 1), in place."""
+        info = np.ascontiguousarray(info, dtype=IBM_INFO_DTYPE)
+        e = self.lib.cbo_ibm_interpolate(self._cp, C.byref(surface.c), info.size, info.ctypes.data,
+                                         _ptrs(list(coor_pad)), _ptrs(list(q)), _dp(p[0]), add_dundt,
+                                         self.cfg.twoD, self.cfg.wallfunction)
+        if e:
+            raise RuntimeError(f"cbo_ibm_interpolate failed with status {e}")
+
+    def steps_immersed(self, nsteps: int, state: dict, met, nvert: np.ndarray, surface, info,
+                       coor_pad: np.ndarray) -> dict:
+        """Time steps with immersed bodies (cbo_steps_ibm): surface / info are
+        one body's IbmSurface and list, or equal-length sequences of them.
+        state as for steps() plus "lp" (padded 1: the pressure the reference
+        carries in P / lP) and "lp_valid", both updated in place."""
+        surfs = list(surface) if isinstance(surface, (list, tuple)) else [surface]
+        infos = list(info) if isinstance(info, (list, tuple)) else [info]
+        infos = [np.ascontiguousarray(a, dtype=IBM_INFO_DTYPE) for a in infos]
+        nb = len(surfs)
+        sarr = (_CSurf * nb)(*[s.c for s in surfs])
+        nl = (C.c_int * nb)(*[a.size for a in infos])
+        lp = (C.c_void_p * nb)(*[a.ctypes.data for a in infos])
+        if "lp" not in state:
+            state["lp"] = self.zeros(1)
+            state["lp_valid"] = 0
+        hu = C.c_int(int(state["have_uc"]))
+        lv = C.c_int(int(state["lp_valid"]))
+        e = self.lib.cbo_steps_ibm(self._cp, nsteps, _ptrs(list(state["q"])), _ptrs(list(state["qold"])),
+                                   _ptrs(list(state["quc"])), C.byref(hu), _dp(state["nut"][0]),
+                                   _ptrs(list(met["csi"])), _ptrs(list(met["eta"])), _ptrs(list(met["zet"])),
+                                   _dp(met["aj"][0]), _dp(nvert[0]), nb, sarr, nl, lp, _ptrs(list(coor_pad)),
+                                   _dp(state["lp"][0]), C.byref(lv), self.cfg.twoD, self.cfg.wallfunction)
+        if e:
+            raise RuntimeError(f"cbo_steps_ibm failed with status {e}")
+        state["have_uc"] = hu.value
+        state["lp_valid"] = lv.value
+        return state
+
+
+# ------------------------------------------------------ immersed boundary --
+# One entry of the interpolation list: cbo_ibm_info (oracle/src/cb_oracle.h),
+# the IBMInfo fields the interpolation reads (variables.h:50-89).
+IBM_INFO_DTYPE = np.dtype([
+    ("ni", "<i4"), ("nj", "<i4"), ("nk", "<i4"), ("cell", "<i4"),
+    ("i1", "<i4"), ("j1", "<i4"), ("k1", "<i4"), ("i2", "<i4"), ("j2", "<i4"), ("k2", "<i4"),
+    ("i3", "<i4"), ("j3", "<i4"), ("k3", "<i4"), ("pad", "<i4"),
+    ("cr1", "<f8"), ("cr2", "<f8"), ("cr3", "<f8"), ("cs1", "<f8"), ("cs2", "<f8"), ("cs3", "<f8"),
+    ("d_s", "<f8"), ("d_i", "<f8"), ("pmin", "<f8", (3,)),
+])
+_IBM_INTS = ("ni", "nj", "nk", "cell", "i1", "j1", "k1", "i2", "j2", "k2", "i3", "j3", "k3")
+_IBM_REALS = ("cr1", "cr2", "cr3", "cs1", "cs2", "cs3", "d_s", "d_i")
+
+
+def ibm_info_from_flat(iv: np.ndarray, rv: np.ndarray) -> np.ndarray:
+    """13 ints + 11 doubles per entry (the reference driver's layout) -> list."""
+    n = iv.size // 13
+    iv, rv = iv.reshape(n, 13), rv.reshape(n, 11)
+    out = np.zeros(n, dtype=IBM_INFO_DTYPE)
+    for a, f in enumerate(_IBM_INTS):
+        out[f] = iv[:, a]
+    for a, f in enumerate(_IBM_REALS):
+        out[f] = rv[:, a]
+    out["pmin"] = rv[:, 8:11]
+    return out
+
+
+def ibm_info_to_flat(info: np.ndarray):
+    iv = np.stack([info[f] for f in _IBM_INTS], axis=1).astype(np.int32)
+    rv = np.concatenate([np.stack([info[f] for f in _IBM_REALS], axis=1), info["pmin"]], axis=1)
+    return np.ascontiguousarray(iv), np.ascontiguousarray(rv, dtype=np.float64)
+
+
+class _CSurf(C.Structure):
+    _fields_ = [("n_v", C.c_int), ("n_elmt", C.c_int), ("nv1", C.c_void_p), ("nv2", C.c_void_p),
+                ("nv3", C.c_void_p), ("nf_x", C.c_void_p), ("nf_y", C.c_void_p), ("nf_z", C.c_void_p),
+                ("u", C.c_void_p), ("uold", C.c_void_p)]
+
+
+class IbmSurface:
+    """cbo_ibm_surface over numpy arrays (kept alive here): a dict with x, y, z,
+    nv1..nv3, nf_x..nf_z (workloads.sphere_surface) and vertex velocities
+    u, uold of shape (n_v, 3) (zero when absent)."""
+
+    def __init__(self, s: dict, u: Optional[np.ndarray] = None, uold: Optional[np.ndarray] = None):
+        self.a = {k: np.ascontiguousarray(s[k], dtype=np.int32) for k in ("nv1", "nv2", "nv3")}
+        self.a.update({k: np.ascontiguousarray(s[k], dtype=np.float64) for k in ("nf_x", "nf_y", "nf_z")})
+        n_v = len(s["x"])
+        self.a["u"] = np.ascontiguousarray(np.zeros((n_v, 3)) if u is None else u, dtype=np.float64)
+        self.a["uold"] = np.ascontiguousarray(np.zeros((n_v, 3)) if uold is None else uold, dtype=np.float64)
+        c = _CSurf()
+        c.n_v, c.n_elmt = n_v, len(s["nv1"])
+        for k, v in self.a.items():
+            setattr(c, k, v.ctypes.data)
+        self.c = c
 
 
 # ------------------------------------------------------ shim-built reference --
@@ -343,6 +460,50 @@ class RefOracle:
         out = np.zeros(gz * gy * gx * nc)
         getattr(self.lib, f"ref_get_{which}")(_dp(out))
         return out.reshape(gz, gy, gx, nc)
+
+    def ibm_setup(self, s: dict):
+        """One immersed body (ibi 0) from a surface dict (workloads.sphere_surface)."""
+        L = self.lib
+        self._surf = {k: np.ascontiguousarray(s[k], dtype=np.float64) for k in ("x", "y", "z", "nf_x", "nf_y", "nf_z")}
+        self._surf.update({k: np.ascontiguousarray(s[k], dtype=np.int32) for k in ("nv1", "nv2", "nv3")})
+        a = self._surf
+        e = L.ref_ibm_setup(len(a["x"]), len(a["nv1"]), *(C.c_void_p(a[k].ctypes.data) for k in (
+            "x", "y", "z", "nv1", "nv2", "nv3", "nf_x", "nf_y", "nf_z")))
+        if e:
+            raise RuntimeError(f"ref_ibm_setup failed ({e})")
+
+    def ibm_set_velocity(self, u: np.ndarray, uold: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        uold = np.ascontiguousarray(uold, dtype=np.float64)
+        self.lib.ref_ibm_set_velocity(C.c_void_p(u.ctypes.data), C.c_void_p(uold.ctypes.data))
+
+    def ibm_search(self):
+        """ibm_search_advanced: returns (nvert natural, interpolation list)."""
+        L = self.lib
+        if L.ref_ibm_search():
+            raise RuntimeError("ref_ibm_search failed")
+        nv = np.zeros(self.nnodes)
+        L.ref_get_nvert(_dp(nv))
+        return nv.reshape(self.cfg.mz, self.cfg.my, self.cfg.mx), self.ibm_list()
+
+    def ibm_list(self) -> np.ndarray:
+        L = self.lib
+        n = L.ref_ibm_list_count()
+        iv, rv = np.zeros(13 * n, dtype=np.int32), np.zeros(11 * n)
+        L.ref_ibm_list_get(C.c_void_p(iv.ctypes.data), C.c_void_p(rv.ctypes.data))
+        return ibm_info_from_flat(iv, rv)
+
+    def ibm_set_list(self, info: np.ndarray):
+        iv, rv = ibm_info_to_flat(info)
+        self.lib.ref_ibm_list_set(info.size, C.c_void_p(iv.ctypes.data), C.c_void_p(rv.ctypes.data))
+
+    def ibm_interpolate(self, add_dundt: int = 1):
+        if self.lib.ref_ibm_interpolate(add_dundt):
+            raise RuntimeError("ref_ibm_interpolate failed")
+
+    def formbcs(self, alfa: float):
+        self.lib.ref_formbcs.argtypes = [C.c_double]
+        return self.lib.ref_formbcs(alfa)
 
     def metrics_local(self):
         gz, gy, gx = self.ldims

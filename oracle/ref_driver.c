@@ -1,6 +1,7 @@
 /*
  * Driver that runs the reference's own hot-path source (rhs.c, les.c,
- * metrics.c, solvers.c, compiled UNMODIFIED against the serial PETSc shim)
+ * metrics.c, solvers.c, and the immersed boundary's ibm_iso.c, compgeom.c,
+ * variables.c, wallfunction.c, compiled UNMODIFIED against the serial PETSc shim)
  * behind a small C-ABI, so tests can pin the oracle restatement and the CUDA
  * path against the reference's actual arithmetic.
  *
@@ -19,7 +20,8 @@
  * EqOfState (rhs.c:4820), CalcUCat (rhs.c:1322), formRHS (rhs.c:4703),
  * FormBCS (rhs.c:477), Compute_Smagorinsky_Constant_1 (les.c:135),
  * Compute_eddy_viscosity_LES (les.c:1477), RungeKutta (solvers.c:223),
- * Flow_Solver (solvers.c:13).
+ * Flow_Solver (solvers.c:13), ibm_search_advanced (ibm_iso.c:87),
+ * ibm_interpolation_advanced (ibm_iso.c:2572).
  */
 #include "variables.h"
 
@@ -51,6 +53,7 @@ PetscInt i_homo_filter = 0, j_homo_filter = 0, k_homo_filter = 0;
 PetscInt channel = 0;
 PetscInt block_number = 1;
 PetscReal max_cs = 0.5;
+PetscInt thin = 0;  /* main.c:45, read by ibm_search_advanced */
 
 /* ---- reference entry points (prototypes live only under __cplusplus) ---- */
 PetscErrorCode FormMetrics(UserCtx *user);
@@ -62,6 +65,11 @@ void Compute_Smagorinsky_Constant_1(UserCtx *user);
 void Compute_eddy_viscosity_LES(UserCtx *user);
 PetscErrorCode RungeKutta(UserCtx *user, IBMNodes *ibm, FSInfo *fsi);
 PetscErrorCode Flow_Solver(UserMG *usermg, IBMNodes *ibm, FSInfo *fsi);
+PetscErrorCode ibm_search_advanced(UserCtx *user, IBMNodes *ibm, PetscInt ibi);
+PetscErrorCode ibm_interpolation_advanced(UserCtx *user, IBMNodes *ibm, PetscInt ibi, PetscInt Add_dUndt);
+void InitIBMList(IBMList *ilist);
+void AddIBMNode(IBMList *ilist, IBMInfo ibm_intp);
+void DestroyIBMList(IBMList *ilist);
 
 /* ---- stubs for subsystems outside the hot path (IBM, FSI, output) ---- */
 PetscErrorCode Q_P_Binary_Output(UserCtx *u) { (void)u; return 0; }
@@ -72,17 +80,16 @@ PetscErrorCode Elmt_Move_FSI_TRANSpROT_quarternion() { return 0; }
 PetscErrorCode calc_ibm_normal() { return 0; }
 PetscErrorCode Elmt_Move_FSI_TRANS() { return 0; }
 PetscErrorCode Set_ibm_velocity_to_fsi() { return 0; }
-PetscErrorCode ibm_search_advanced() { return 0; }
 PetscErrorCode ibm_surface_VTKOut() { return 0; }
 PetscErrorCode FSI_position_Output() { return 0; }
 PetscErrorCode FSI_DATA_Output() { return 0; }
-PetscErrorCode ibm_interpolation_advanced() { return 0; }
 
 /* ---- driver state ---- */
 static UserCtx *U = NULL;
 static UserMG MG;
 static MGCtx MGC;
 static PetscInt g_ti = 0;
+static IBMNodes *IBM = NULL;  /* one immersed body (ibi 0) */
 
 static void read_globals_from_options(void) {
   /* main.c:716-801 (subset that the hot path reads) */
@@ -96,18 +103,36 @@ static void read_globals_from_options(void) {
   PetscOptionsGetInt(NULL, NULL, "-central", &central, NULL);
   PetscOptionsGetInt(NULL, NULL, "-channel", &channel, NULL);
   PetscOptionsGetInt(NULL, NULL, "-calc_sigma", &calc_sigma, NULL);
+  PetscOptionsGetInt(NULL, NULL, "-wallfunction", &wallfunction, NULL);
+  PetscOptionsGetInt(NULL, NULL, "-thin", &thin, NULL);
 }
 
 static void reset_globals(void) {
   tistart = 0; rstart_flg = PETSC_FALSE; immersed = 0; wavy = 0; isothermal = 0;
   calc_sigma = 0; invicid = 0; TwoD = 0; central = 2; les = 0; rans = 0; channel = 0;
+  wallfunction = 0; thin = 0;
+}
+
+static void ibm_free(void) {
+  if (U && U->ibmlist) {
+    DestroyIBMList(&U->ibmlist[0]);
+    free(U->ibmlist);
+    U->ibmlist = NULL;
+  }
+  if (!IBM) return;
+  void *arrs[] = {IBM->x_bp, IBM->y_bp, IBM->z_bp, IBM->nv1, IBM->nv2, IBM->nv3, IBM->nf_x, IBM->nf_y,
+                  IBM->nf_z, IBM->u, IBM->uold, IBM->urm1};
+  for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); i++) free(arrs[i]);
+  free(IBM);
+  IBM = NULL;
 }
 
 static void destroy_user(void) {
+  ibm_free();
   if (!U) return;
   Vec *vs[] = {&U->Q, &U->Qold, &U->Rhs, &U->lQ, &U->lQold, &U->Ucat, &U->Nvert, &U->P, &U->Nvert_o,
                &U->lCsi, &U->lEta, &U->lZet, &U->lUcat, &U->lAj, &U->lNvert, &U->lP, &U->lNvert_o,
-               &U->lBeta, &U->Sigma, &U->lSigma, &U->lNu_t, &U->Nu_t, &U->lCS, &U->CS, &U->lBBeta};
+               &U->lBeta, &U->Sigma, &U->lSigma, &U->lNu_t, &U->Nu_t, &U->lCS, &U->CS, &U->lBBeta, &U->lUstar};
   for (size_t i = 0; i < sizeof(vs) / sizeof(vs[0]); i++) VecDestroy(vs[i]);
   DMDestroy(&U->cda);
   DMDestroy(&U->da);
@@ -197,6 +222,7 @@ int ref_setup(int mx, int my, int mz, const int *bctype, const double *coords, c
   }
   VecDuplicate(U->lAj, &U->lP);
   VecDuplicate(U->lAj, &U->lNvert_o);
+  if (wallfunction) VecDuplicate(U->lAj, &U->lUstar); /* ibm_iso.c:2635 */
 
   /* init.c:45-103 FormInitialize */
   VecSet(U->Nvert, 0.); VecSet(U->lNvert, 0.);
@@ -287,7 +313,7 @@ int ref_steps(int nsteps) {
   if (!U) return 1;
   for (int n = 0; n < nsteps; n++) {
     U->ti = g_ti;
-    Flow_Solver(&MG, NULL, NULL);
+    Flow_Solver(&MG, immersed ? IBM : NULL, NULL);
     VecCopy(U->Q, U->Qold);
     DMGlobalToLocalBegin(U->cda, U->Qold, INSERT_VALUES, U->lQold);
     DMGlobalToLocalEnd(U->cda, U->Qold, INSERT_VALUES, U->lQold);
@@ -327,3 +353,108 @@ int ref_get_metrics(double *lcsi, double *leta, double *lzet, double *laj) {
   return 0;
 }
 void ref_destroy(void) { destroy_user(); }
+
+/* ---- immersed boundary: one body, ibi 0 (main.c:813-858 sets up the same
+ * objects: a calloc'ed IBMNodes, user->ibmlist with InitIBMList, the surface
+ * as ibm_read_ucd leaves it, zero surface velocity) ---- */
+int ref_ibm_setup(int n_v, int n_elmt, const double *x, const double *y, const double *z, const int *nv1,
+                  const int *nv2, const int *nv3, const double *nf_x, const double *nf_y, const double *nf_z) {
+  if (!U) return 1;
+  ibm_free();
+  IBM = (IBMNodes *)calloc(1, sizeof(IBMNodes));
+  IBM->n_v = n_v;
+  IBM->n_elmt = n_elmt;
+  IBM->x_bp = malloc(sizeof(double) * n_v); memcpy(IBM->x_bp, x, sizeof(double) * n_v);
+  IBM->y_bp = malloc(sizeof(double) * n_v); memcpy(IBM->y_bp, y, sizeof(double) * n_v);
+  IBM->z_bp = malloc(sizeof(double) * n_v); memcpy(IBM->z_bp, z, sizeof(double) * n_v);
+  IBM->nv1 = malloc(sizeof(PetscInt) * n_elmt); memcpy(IBM->nv1, nv1, sizeof(PetscInt) * n_elmt);
+  IBM->nv2 = malloc(sizeof(PetscInt) * n_elmt); memcpy(IBM->nv2, nv2, sizeof(PetscInt) * n_elmt);
+  IBM->nv3 = malloc(sizeof(PetscInt) * n_elmt); memcpy(IBM->nv3, nv3, sizeof(PetscInt) * n_elmt);
+  IBM->nf_x = malloc(sizeof(double) * n_elmt); memcpy(IBM->nf_x, nf_x, sizeof(double) * n_elmt);
+  IBM->nf_y = malloc(sizeof(double) * n_elmt); memcpy(IBM->nf_y, nf_y, sizeof(double) * n_elmt);
+  IBM->nf_z = malloc(sizeof(double) * n_elmt); memcpy(IBM->nf_z, nf_z, sizeof(double) * n_elmt);
+  IBM->u = calloc(n_v, sizeof(Cmpnts));
+  IBM->uold = calloc(n_v, sizeof(Cmpnts));
+  IBM->urm1 = calloc(n_v, sizeof(Cmpnts));
+  U->ibmlist = (IBMList *)malloc(sizeof(IBMList));
+  InitIBMList(&U->ibmlist[0]);
+  return 0;
+}
+
+/* Surface velocity of the current and the previous step (n_v x,y,z each). */
+int ref_ibm_set_velocity(const double *u, const double *uold) {
+  if (!IBM) return 1;
+  memcpy(IBM->u, u, sizeof(Cmpnts) * IBM->n_v);
+  memcpy(IBM->uold, uold, sizeof(Cmpnts) * IBM->n_v);
+  return 0;
+}
+
+/* ibm_search_advanced (ibm_iso.c:87): nvert and the interpolation list. */
+int ref_ibm_search(void) {
+  if (!U || !IBM) return 1;
+  DestroyIBMList(&U->ibmlist[0]);
+  InitIBMList(&U->ibmlist[0]);
+  return ibm_search_advanced(U, IBM, 0);
+}
+
+int ref_get_nvert(double *out) { return U ? copy_out(U->Nvert, out) : 1; }
+
+int ref_ibm_list_count(void) {
+  if (!U || !U->ibmlist) return -1;
+  int n = 0;
+  for (IBMListNode *c = U->ibmlist[0].head; c; c = c->next) n++;
+  return n;
+}
+
+/* The list in traversal order; per entry 13 ints (ni nj nk cell i1 j1 k1 i2 j2
+ * k2 i3 j3 k3) and 11 doubles (cr1 cr2 cr3 cs1 cs2 cs3 d_s d_i pmin.x pmin.y
+ * pmin.z). */
+int ref_ibm_list_get(int *iv, double *rv) {
+  if (!U || !U->ibmlist) return 1;
+  int n = 0;
+  for (IBMListNode *c = U->ibmlist[0].head; c; c = c->next, n++) {
+    const IBMInfo *b = &c->ibm_intp;
+    int *a = iv + 13 * n;
+    double *r = rv + 11 * n;
+    a[0] = b->ni; a[1] = b->nj; a[2] = b->nk; a[3] = b->cell;
+    a[4] = b->i1; a[5] = b->j1; a[6] = b->k1; a[7] = b->i2; a[8] = b->j2; a[9] = b->k2;
+    a[10] = b->i3; a[11] = b->j3; a[12] = b->k3;
+    r[0] = b->cr1; r[1] = b->cr2; r[2] = b->cr3; r[3] = b->cs1; r[4] = b->cs2; r[5] = b->cs3;
+    r[6] = b->d_s; r[7] = b->d_i; r[8] = b->pmin.x; r[9] = b->pmin.y; r[10] = b->pmin.z;
+  }
+  return 0;
+}
+
+/* Replace the list (same per-entry layout as ref_ibm_list_get, traversal
+ * order kept: AddIBMNode prepends, so entries are added last to first). */
+int ref_ibm_list_set(int n, const int *iv, const double *rv) {
+  if (!U || !U->ibmlist) return 1;
+  DestroyIBMList(&U->ibmlist[0]);
+  InitIBMList(&U->ibmlist[0]);
+  for (int e = n - 1; e >= 0; e--) {
+    IBMInfo b;
+    memset(&b, 0, sizeof(b));
+    const int *a = iv + 13 * e;
+    const double *r = rv + 11 * e;
+    b.ni = a[0]; b.nj = a[1]; b.nk = a[2]; b.cell = a[3];
+    b.i1 = a[4]; b.j1 = a[5]; b.k1 = a[6]; b.i2 = a[7]; b.j2 = a[8]; b.k2 = a[9];
+    b.i3 = a[10]; b.j3 = a[11]; b.k3 = a[12];
+    b.cr1 = r[0]; b.cr2 = r[1]; b.cr3 = r[2]; b.cs1 = r[3]; b.cs2 = r[4]; b.cs3 = r[5];
+    b.d_s = r[6]; b.d_i = r[7]; b.pmin.x = r[8]; b.pmin.y = r[9]; b.pmin.z = r[10];
+    AddIBMNode(&U->ibmlist[0], b);
+  }
+  return 0;
+}
+
+/* ibm_interpolation_advanced (ibm_iso.c:2572) on the current Q/lQ/P/lP. */
+int ref_ibm_interpolate(int add_dundt) {
+  if (!U || !IBM) return 1;
+  U->ti = g_ti;
+  return ibm_interpolation_advanced(U, IBM, 0, add_dundt);
+}
+
+/* FormBCS(user, alfa) (rhs.c:477) on the current Q from lQ. */
+int ref_formbcs(double alfa) {
+  if (!U) return 1;
+  return FormBCS(U, alfa);
+}

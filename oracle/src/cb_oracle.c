@@ -727,16 +727,18 @@ static void visc_face(const ctx_t *C, const visc_t *V, int d, int i, int j, int 
 /* ------------------------------------------------------------------------ */
 /* formRHS  (rhs.c:4703-4736) with MultAj (rhs.c:4575-4701)                  */
 /* ------------------------------------------------------------------------ */
-int cbo_rhs(const cbo_config *c, const double *const q[5], const double *const csi[3],
-            const double *const eta[3], const double *const zet[3], const double *aj,
-            const double *nvert, const double *nut, const double *const sig[3],
-            double *const rhs[5]) {
+/* lp_in: the local pressure lP the reference reads (NULL: EqOfState of q). */
+static int rhs_impl(const cbo_config *c, const double *const q[5], const double *lp_in, const double *const csi[3],
+                    const double *const eta[3], const double *const zet[3], const double *aj,
+                    const double *nvert, const double *nut, const double *const sig[3],
+                    double *const rhs[5]) {
   geom G = mkgeom(c);
   const int mx = G.m[0], my = G.m[1], mz = G.m[2];
   if (mx < 5 || my < 5 || mz < 5) return 3;
   if (c->les && (!nut || !sig)) return 4;
   double *p = (double *)malloc(G.n * sizeof(double));
-  cbo_eos(c, q, p);
+  if (lp_in) memcpy(p, lp_in, G.n * sizeof(double));
+  else cbo_eos(c, q, p);
   ctx_t C;
   C.c = c; C.G = G; C.q = q; C.p = p; C.nv = nvert;
   C.met[0] = csi; C.met[1] = eta; C.met[2] = zet;
@@ -835,6 +837,20 @@ int cbo_rhs(const cbo_config *c, const double *const q[5], const double *const c
   free(buf);
   free(p);
   return 0;
+}
+
+int cbo_rhs(const cbo_config *c, const double *const q[5], const double *const csi[3],
+            const double *const eta[3], const double *const zet[3], const double *aj,
+            const double *nvert, const double *nut, const double *const sig[3],
+            double *const rhs[5]) {
+  return rhs_impl(c, q, NULL, csi, eta, zet, aj, nvert, nut, sig, rhs);
+}
+
+int cbo_rhs_lp(const cbo_config *c, const double *const q[5], const double *lp, const double *const csi[3],
+               const double *const eta[3], const double *const zet[3], const double *aj,
+               const double *nvert, const double *nut, const double *const sig[3],
+               double *const rhs[5]) {
+  return rhs_impl(c, q, lp, csi, eta, zet, aj, nvert, nut, sig, rhs);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -956,8 +972,11 @@ int cbo_bc_periodic(const cbo_config *c, const double *const qin[5], double *con
 /* (they read the coordinates and the step index) and the characteristic    */
 /* isothermal wall (isothermal 2 with a j wall).                             */
 /* ------------------------------------------------------------------------ */
-int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], const double *const qold[5],
-                const double *const zet[3], const double *aj, double *const q[5]) {
+/* lp_in: the local pressure lP (NULL: EqOfState of lq); p (may be NULL): the
+ * global P, which receives the periodic copies and then the ghost wrap. */
+static int formbcs_impl(const cbo_config *c, double alfa, const double *const lq[5], const double *lp_in,
+                        const double *const qold[5], const double *const zet[3], const double *aj,
+                        double *const q[5], double *p) {
   geom G = mkgeom(c);
   const int mx = G.m[0], my = G.m[1], mz = G.m[2];
   const int *bc = c->bctype;
@@ -967,7 +986,8 @@ int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], con
   const ptrdiff_t si = G.s[0], sj = G.s[1], sk = G.s[2];
   const double g = c->gamma, Ma = c->ma;
   double *lp = (double *)malloc(G.n * sizeof(double));
-  cbo_eos(c, lq, lp);
+  if (lp_in) memcpy(lp, lp_in, G.n * sizeof(double));
+  else cbo_eos(c, lq, lp);
 #define RO(n) q[0][n]
 #define RU(n) q[1][n]
 #define RV(n) q[2][n]
@@ -1120,40 +1140,59 @@ int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], con
 #undef RV
 #undef RW
 #undef RE
-  free(lp);
-  /* periodic copies (rhs.c:1107-1227) */
+  /* periodic copies (rhs.c:1107-1227), of Q and P alike, from lQ and the
+   * local pressure as the face codes left it */
+#define PCOPY(n, src)                                           \
+  do {                                                          \
+    for (int a = 0; a < 5; a++) q[a][n] = lq[a][src];           \
+    if (p) p[n] = lp[src];                                      \
+  } while (0)
   if (bc[0] == 7 || bc[1] == 7) {
     for (int k = 1; k < mz; k++)
       for (int j = 1; j < my; j++) {
         ptrdiff_t n = IX(&G, 0, j, k);
-        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n - 2 * si];
+        PCOPY(n, n - 2 * si);
         n = IX(&G, mx - 1, j, k);
-        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n + 2 * si];
+        PCOPY(n, n + 2 * si);
       }
   }
   if (bc[2] == 7 || bc[3] == 7) {
     for (int k = 1; k < mz; k++)
       for (int i = 0; i < mx; i++) {
         ptrdiff_t n = IX(&G, i, 0, k);
-        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n - 2 * sj];
+        PCOPY(n, n - 2 * sj);
       }
     for (int k = 1; k < mz - 1; k++)
       for (int i = 0; i < mx; i++) {
         ptrdiff_t n = IX(&G, i, my - 1, k);
-        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n + 2 * sj];
+        PCOPY(n, n + 2 * sj);
       }
   }
   if (bc[4] == 7 || bc[5] == 7) {
     for (int j = 0; j < my; j++)
       for (int i = 0; i < mx; i++) {
         ptrdiff_t n = IX(&G, i, j, 0);
-        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n - 2 * sk];
+        PCOPY(n, n - 2 * sk);
         n = IX(&G, i, j, mz - 1);
-        for (int a = 0; a < 5; a++) q[a][n] = lq[a][n + 2 * sk];
+        PCOPY(n, n + 2 * sk);
       }
   }
+#undef PCOPY
+  free(lp);
   for (int a = 0; a < 5; a++) cbo_fill_ghosts(c, q[a]);
+  if (p) cbo_fill_ghosts(c, p);
   return 0;
+}
+
+int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], const double *const qold[5],
+                const double *const zet[3], const double *aj, double *const q[5]) {
+  return formbcs_impl(c, alfa, lq, NULL, qold, zet, aj, q, NULL);
+}
+
+int cbo_formbcs_lp(const cbo_config *c, double alfa, const double *const lq[5], const double *lp,
+                   const double *const qold[5], const double *const zet[3], const double *aj, double *const q[5],
+                   double *p) {
+  return formbcs_impl(c, alfa, lq, lp, qold, zet, aj, q, p);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1190,6 +1229,148 @@ int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const
       }
       for (int a = 0; a < 5; a++) memcpy(q[a], qn[a], G.n * sizeof(double));
     }
+    for (int a = 0; a < 5; a++) memcpy(qold[a], q[a], G.n * sizeof(double));
+  }
+  free(buf);
+  return err;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Immersed-boundary interpolation (ibm_interpolation_advanced,              */
+/* ibm_iso.c:2572-2880) with the wall models noslip / freeslip                */
+/* (wallfunction.c:12-48)                                                     */
+/* ------------------------------------------------------------------------ */
+#define IBM_SWEEPS 5 /* itr_tmp, ibm_iso.c:2616 */
+
+/* Surface velocity at the interception point: the element's three vertex
+ * values weighted by cs1..cs3 (ibm_iso.c:2680-2690). */
+static void ibm_surface_u(const cbo_ibm_surface *s, const double *u, int cell, const cbo_ibm_info *b, double U[3]) {
+  const int a = s->nv1[cell], m = s->nv2[cell], z = s->nv3[cell];
+  for (int d = 0; d < 3; d++) U[d] = u[3 * a + d] * b->cs1 + u[3 * m + d] * b->cs2 + u[3 * z + d] * b->cs3;
+}
+
+int cbo_ibm_interpolate(const cbo_config *c, const cbo_ibm_surface *s, int n, const cbo_ibm_info *list,
+                        const double *const coor[3], double *const q[5], double *p, int add_dundt, int twoD,
+                        int wallfunction) {
+  if (c->isothermal == 2 || wallfunction == 1 || wallfunction == 2) return 5; /* not restated */
+  geom G = mkgeom(c);
+  double *buf = (double *)malloc(G.n * 6 * sizeof(double));
+  double *lq[5], *lp = buf + G.n * 5;
+  for (int a = 0; a < 5; a++) lq[a] = buf + G.n * a;
+  const double gm2 = c->gamma * c->ma * c->ma;
+  const int slip = c->inviscid || wallfunction == 3; /* ibm_iso.c:2721 */
+  for (int sweep = 0; sweep < IBM_SWEEPS; sweep++) {
+    /* the sweep reads the local vectors lQ / lP and writes the global Q / P */
+    for (int a = 0; a < 5; a++) memcpy(lq[a], q[a], G.n * sizeof(double));
+    memcpy(lp, p, G.n * sizeof(double));
+    for (int e = 0; e < n; e++) {
+      const cbo_ibm_info *b = &list[e];
+      const ptrdiff_t o = IX(&G, b->ni, b->nj, b->nk);
+      const ptrdiff_t d1 = IX(&G, b->i1, b->j1, b->k1), d2 = IX(&G, b->i2, b->j2, b->k2),
+                      d3 = IX(&G, b->i3, b->j3, b->k3);
+      const double sb = b->d_s, sc = sb + b->d_i;
+      const double sk1 = b->cr1, sk2 = b->cr2, sk3 = b->cr3;
+      /* direction from the interception point to the node (ibm_iso.c:2662-2681) */
+      double nfx = twoD == 1 ? 0. : coor[0][o] - b->pmin[0];
+      double nfy = twoD == 2 ? 0. : coor[1][o] - b->pmin[1];
+      double nfz = twoD == 3 ? 0. : coor[2][o] - b->pmin[2];
+      const double dr = sqrt(nfx * nfx + nfy * nfy + nfz * nfz);
+      if (dr < 0.000000001) {
+        if (b->cell >= 0) { nfx = s->nf_x[b->cell]; nfy = s->nf_y[b->cell]; nfz = s->nf_z[b->cell]; }
+        else { nfx = 0.; nfy = 0.; nfz = 0.; }
+      } else {
+        nfx = nfx / dr; nfy = nfy / dr; nfz = nfz / dr;
+      }
+      double Ua[3] = {0., 0., 0.}, Ua_n = 0., Ua_nold = 0.;
+      if (b->cell >= 0) {
+        ibm_surface_u(s, s->uold, b->cell, b, Ua);
+        Ua_nold = Ua[0] * nfx + Ua[1] * nfy + Ua[2] * nfz;
+        ibm_surface_u(s, s->u, b->cell, b, Ua);
+        Ua_n = Ua[0] * nfx + Ua[1] * nfy + Ua[2] * nfz;
+      }
+      /* velocity at the donor point (ibm_iso.c:2704-2706) */
+      double Uc[3];
+      for (int d = 0; d < 3; d++)
+        Uc[d] = lq[1 + d][d1] / lq[0][d1] * sk1 + lq[1 + d][d2] / lq[0][d2] * sk2 + lq[1 + d][d3] / lq[0][d3] * sk3;
+      double Ub[3];
+      if (slip) { /* freeslip: normal part linear in the distance, tangential part of the donor */
+        const double Uan = Ua[0] * nfx + Ua[1] * nfy + Ua[2] * nfz;
+        const double Ucn = Uc[0] * nfx + Uc[1] * nfy + Uc[2] * nfz;
+        const double Ubn = Uan + (Ucn - Uan) * sb / sc;
+        const double nv[3] = {nfx, nfy, nfz};
+        for (int d = 0; d < 3; d++) Ub[d] = (Uc[d] - Ucn * nv[d]) + Ubn * nv[d];
+      } else { /* noslip: linear between the wall velocity and the donor */
+        for (int d = 0; d < 3; d++) Ub[d] = sb / sc * (Uc[d] - Ua[d]) + Ua[d];
+      }
+      double pb = lp[d1] * sk1 + lp[d2] * sk2 + lp[d3] * sk3;
+      if (twoD == 1) Ub[0] = 0.;
+      if (twoD == 2) Ub[1] = 0.;
+      if (twoD == 3) Ub[2] = 0.;
+      double rho;
+      if (c->isothermal == 1) rho = pb * gm2 / 1.0; /* wall temperature Tb = 1 (ibm_iso.c:2795-2803) */
+      else rho = lq[0][d1] * sk1 + lq[0][d2] * sk2 + lq[0][d3] * sk3; /* d rho / dn = 0 */
+      if (add_dundt) pb += rho * (Ua_n - Ua_nold) / c->dt * (sc - sb);
+      const double ru = rho * Ub[0], rv = rho * Ub[1], rw = rho * Ub[2];
+      q[0][o] = rho; q[1][o] = ru; q[2][o] = rv; q[3][o] = rw;
+      q[4][o] = pb / (c->gamma - 1) + 0.5 * (ru * ru + rv * rv + rw * rw) / rho;
+      p[o] = pb;
+    }
+    /* DMGlobalToLocal of Q and P after each sweep */
+    for (int a = 0; a < 5; a++) cbo_fill_ghosts(c, q[a]);
+    cbo_fill_ghosts(c, p);
+  }
+  free(buf);
+  return 0;
+}
+
+/* Time steps with immersed bodies (RungeKutta with -imm, solvers.c:245-288):
+ * the stages as in cbo_steps, EqOfState, the interpolation of each body
+ * (Add_dUndt = 1), then FormBCS(user, 0), which copies Q and P across the
+ * periodic boundaries and ends with their ghost wrap.  No EqOfState follows,
+ * so the next step's first stage reads the pressure lp carried from here
+ * (*lp_valid set) instead of the EqOfState of its input. */
+int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *const qold[5],
+                  double *const quc[5], int *have_uc, double *nut, const double *const csi[3],
+                  const double *const eta[3], const double *const zet[3], const double *aj,
+                  const double *nvert, int nbodies, const cbo_ibm_surface *surf, const int *nlist,
+                  const cbo_ibm_info *const *lists, const double *const coor[3], double *lp, int *lp_valid,
+                  int twoD, int wallfunction) {
+  if (c->calc_sigma) return 5; /* the sensor with a carried pressure is not restated */
+  geom G = mkgeom(c);
+  int ns = cbo_nstages(c);
+  double *buf = (double *)calloc(G.n * 19, sizeof(double));
+  double *rhs[5], *qn[5], *sig[3], *lq[5], *lpc = buf + G.n * 18;
+  for (int a = 0; a < 5; a++) { rhs[a] = buf + G.n * a; qn[a] = buf + G.n * (5 + a); lq[a] = buf + G.n * (13 + a); }
+  for (int a = 0; a < 3; a++) sig[a] = buf + G.n * (10 + a);
+  if (c->les) cbo_sigma(c, sig);
+  double al[3] = {1., 1 / 4., 2 / 3.};
+  if (c->fluxorder < 3) al[1] = 1 / 2.;
+  int err = 0;
+  for (int step = 0; step < nsteps && !err; step++) {
+    if (c->les && !c->inviscid)
+      cbo_eddy_viscosity(c, *have_uc ? (const double *const *)quc : NULL, csi, eta, zet, aj, nvert, nut);
+    for (int s = 0; s < ns && !err; s++) {
+      const double *lps = (s == 0 && *lp_valid) ? lp : NULL;
+      err = rhs_impl(c, (const double *const *)q, lps, csi, eta, zet, aj, nvert, nut, (const double *const *)sig,
+                     rhs);
+      if (err) break;
+      if (!c->inviscid) {
+        for (int a = 0; a < 5; a++) memcpy(quc[a], q[a], G.n * sizeof(double));
+        *have_uc = 1;
+      }
+      cbo_rk_combine(c, s, (const double *const *)qold, (const double *const *)q, (const double *const *)rhs, qn);
+      err = formbcs_impl(c, al[s], (const double *const *)q, lps, (const double *const *)qold, zet, aj, qn, NULL);
+      for (int a = 0; a < 5; a++) memcpy(q[a], qn[a], G.n * sizeof(double));
+    }
+    if (err) break;
+    cbo_eos(c, (const double *const *)q, lp); /* EqOfState after the last stage (solvers.c:279) */
+    for (int b = 0; b < nbodies && !err; b++)
+      if (nlist[b] > 0) err = cbo_ibm_interpolate(c, &surf[b], nlist[b], lists[b], coor, q, lp, 1, twoD, wallfunction);
+    if (err) break;
+    for (int a = 0; a < 5; a++) memcpy(lq[a], q[a], G.n * sizeof(double));
+    memcpy(lpc, lp, G.n * sizeof(double));
+    err = formbcs_impl(c, 0.0, (const double *const *)lq, lpc, (const double *const *)qold, zet, aj, q, lp);
+    *lp_valid = 1;
     for (int a = 0; a < 5; a++) memcpy(qold[a], q[a], G.n * sizeof(double));
   }
   free(buf);

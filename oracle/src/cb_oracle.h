@@ -97,6 +97,61 @@ int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const
               const double *const eta[3], const double *const zet[3], const double *aj,
               const double *nvert);
 
+/* One entry of the immersed-boundary interpolation list (IBMInfo,
+ * variables.h:50-89): the interface node, the surface element of its
+ * interception point (-1: none), three donor nodes with weights cr, the
+ * element's vertex weights cs, the distances node -> surface (d_s) and
+ * surface -> donor point (d_i), and the interception point pmin. */
+typedef struct {
+  int ni, nj, nk, cell;
+  int i1, j1, k1, i2, j2, k2, i3, j3, k3;
+  int pad;
+  double cr1, cr2, cr3, cs1, cs2, cs3, d_s, d_i, pmin[3];
+} cbo_ibm_info;
+
+/* The surface arrays of one body the interpolation reads (IBMNodes,
+ * variables.h:91-118): triangles, their normals, the vertex velocities of
+ * this and the previous step (x, y, z per vertex). */
+typedef struct {
+  int n_v, n_elmt;
+  const int *nv1, *nv2, *nv3;
+  const double *nf_x, *nf_y, *nf_z;
+  const double *u, *uold;
+} cbo_ibm_surface;
+
+/* ibm_interpolation_advanced (ibm_iso.c:2572-2880): five Jacobi sweeps over
+ * the list; q (ghosted, in/out) serves as both Q and lQ, p (ghosted, in/out)
+ * as P and lP, coor the node coordinates (3 padded planes).  Returns 5 for
+ * the variants that are not restated (wall functions 1/2, isothermal 2). */
+int cbo_ibm_interpolate(const cbo_config *c, const cbo_ibm_surface *s, int n, const cbo_ibm_info *list,
+                        const double *const coor[3], double *const q[5], double *p, int add_dundt, int twoD,
+                        int wallfunction);
+
+/* formRHS / FormBCS reading the local pressure lp (padded) the reference
+ * carries in lP instead of the EqOfState of the stage input; cbo_formbcs_lp
+ * also copies P (p, in/out; may be NULL) across periodic boundaries from lp
+ * and wraps its ghosts, as FormBCS does (rhs.c:1107-1227, 1305-1308). */
+int cbo_rhs_lp(const cbo_config *c, const double *const q[5], const double *lp, const double *const csi[3],
+               const double *const eta[3], const double *const zet[3], const double *aj,
+               const double *nvert, const double *nut, const double *const sig[3],
+               double *const rhs[5]);
+int cbo_formbcs_lp(const cbo_config *c, double alfa, const double *const lq[5], const double *lp,
+                   const double *const qold[5], const double *const zet[3], const double *aj, double *const q[5],
+                   double *p);
+
+/* Time steps with immersed bodies (RungeKutta with -imm): the stages, the
+ * interpolation of each of the nbodies bodies (surf[b], lists[b] with
+ * nlist[b] entries), then FormBCS(user, 0).  lp (padded, in/out) is the
+ * pressure the reference keeps in P / lP; *lp_valid (in/out) says whether
+ * the first stage reads it (set after an immersed step) or the EqOfState of
+ * its input.  Returns 5 with the shock sensor (not restated here). */
+int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *const qold[5],
+                  double *const quc[5], int *have_uc, double *nut, const double *const csi[3],
+                  const double *const eta[3], const double *const zet[3], const double *aj,
+                  const double *nvert, int nbodies, const cbo_ibm_surface *surf, const int *nlist,
+                  const cbo_ibm_info *const *lists, const double *const coor[3], double *lp, int *lp_valid,
+                  int twoD, int wallfunction);
+
 /* Number of RK stages the reference runs for this config (= fluxorder). */
 int cbo_nstages(const cbo_config *c);
 
