@@ -84,11 +84,14 @@ struct cb_ctx {
   int uc = -1;                // buffer of the last CalcUCat state, -1: none
   bool have_grid = false, have_state = false;
   int kchunk = 16;
-  GraphSlot graphs[3][4];
+  GraphSlot graphs[3][4][2];  // [cur][uc + 1][p_carry]
   bool use_graphs = true;
   // immersed bodies: interpolation after the stages, then FormBCS(user, 0)
   IbmBody ibm[CB_IBM_MAX_BODIES];
-  double *spare = nullptr;  // 5 planes: the state FormBCS(user, 0) reads as lQ
+  double *ibm_arena = nullptr;  // 7 planes: spare (5) and psnap (1), the Q and P FormBCS reads, and pl
+  double *spare = nullptr, *psnap = nullptr;
+  double *pl = nullptr;  // the reference's P / lP after an immersed step
+  bool p_carry = false;  // pl holds lP of the current state (no EqOfState since the interpolation)
   int ibm_twoD = 0, ibm_wallfunction = 0;
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -112,7 +115,7 @@ static int fail(cb_ctx *c, int code, const std::string &msg) {
 
 // device pointer tables inside ctx->ptab
 enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27, PT_NUT = 32, PT_MISC = 33, PT_GCL = 48,
-       PT_SIGA = 56, PT_SIGB = 59, PT_N = 64 };
+       PT_SIGA = 56, PT_SIGB = 59, PT_PL = 64, PT_N = 65 };
 
 static int grid_for(const cb_ctx *c, long long work, int block = 256) {
   long long b = (work + block - 1) / block;
@@ -292,32 +295,48 @@ static int ibm_sweeps(cb_ctx *c, const IbmBody &b, int add_dundt) {
   const int slip = (c->cfg.inviscid || c->ibm_wallfunction == 3) ? 1 : 0;  // ibm_iso.c:2721
   const int iso1 = c->cfg.isothermal == 1 ? 1 : 0;
   for (int s = 0; s < IBM_SWEEPS; s++) {
-    ibm_interp_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), d, add_dundt,
-                                                c->ibm_twoD, slip, iso1);
-    ibm_scatter_kernel<<<g, 256, 0, c->stream>>>(c->dc, c->ptab + 5 * c->cur, d);
+    ibm_interp_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), c->pl, d,
+                                                add_dundt, c->ibm_twoD, slip, iso1);
+    ibm_scatter_kernel<<<g, 256, 0, c->stream>>>(c->dc, c->ptab + 5 * c->cur, c->pl, d);
   }
   CB_CUDA(c, cudaGetLastError());
   return CB_OK;
 }
 
+// EqOfState of the current state into the pressure plane (solvers.c:279).
+static int eos_to_plane(cb_ctx *c) {
+  eos_plane_kernel<<<grid_for(c, (long long)c->plane), 256, 0, c->stream>>>(
+      c->dc, (const double *const *)(c->ptab + 5 * c->cur), c->pl);
+  CB_CUDA(c, cudaGetLastError());
+  return CB_OK;
+}
+
 // FormBCS(user, 0) after the interpolation (solvers.c:286): the boundary of
-// the current state from a snapshot of it (the reference's lQ), Qold from
-// buffer `old`, then the ghost wrap FormBCS ends with (rhs.c:1305-1308).
+// the current state from a snapshot of it and of the pressure plane (the
+// reference's lQ and lP), Qold from buffer `old`; the periodic copies move P
+// with Q; then the ghost wrap of both that FormBCS ends with
+// (rhs.c:1305-1308).  No EqOfState follows: the pressure plane is carried.
 static int formbcs_zero(cb_ctx *c, int old) {
   CB_CUDA(c, cudaMemcpyAsync(c->spare, c->qb[c->cur][0], sizeof(double) * 5 * c->plane, cudaMemcpyDeviceToDevice,
                              c->stream));
+  CB_CUDA(c, cudaMemcpyAsync(c->psnap, c->pl, sizeof(double) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
   DevFields F = fields_for(c, c->cur, old, c->cur);
   for (int q = 0; q < 5; q++) F.q[q] = c->spare + c->plane * q;
+  F.pin = c->psnap;
   const long long shell = shell_count(c->dc);
   if (c->fully_periodic) {
     bc_periodic_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, F);
+    bc_periodic_p_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, c->psnap, c->pl);
   } else {
     const long long face = (long long)std::max(c->dc.mx, c->dc.my) * std::max(c->dc.my, c->dc.mz);
     for (int dir = 0; dir < 3; dir++) bc_face_kernel<<<grid_for(c, face), 256, 0, c->stream>>>(c->dc, F, dir, 0.0);
     for (int dir = 0; dir < 3; dir++)
-      if (c->dc.bctype[2 * dir] == 7)
+      if (c->dc.bctype[2 * dir] == 7) {
         bc_periodic_dir_kernel<<<grid_for(c, face), 256, 0, c->stream>>>(c->dc, F, dir);
+        bc_periodic_dir_p_kernel<<<grid_for(c, face), 256, 0, c->stream>>>(c->dc, c->psnap, c->pl, dir);
+      }
     ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, c->ptab + 5 * c->cur, 5);
+    ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, c->ptab + PT_PL, 1);
   }
   CB_CUDA(c, cudaGetLastError());
   return CB_OK;
@@ -340,6 +359,7 @@ static int enqueue_step(cb_ctx *c) {
     rk_coeffs(c, s, &alfa, &beta);
     const double adt = alfa * c->cfg.dt * c->cfg.st;
     DevFields F = fields_for(c, in, old, out);
+    if (s == 0 && c->p_carry) F.pin = c->pl;  // lP carried from the interpolation of the previous step
     if (s == 0) {
       int e = sigma_update(c, in);
       if (e) return e;
@@ -368,15 +388,19 @@ static int enqueue_step(cb_ctx *c) {
     in = out;
   }
   c->cur = in;
-  if (ibm_active(c)) {  // solvers.c:282-288
+  c->p_carry = false;
+  if (ibm_active(c)) {  // solvers.c:279-288
     TimedScope ts(c, false);
+    int e = eos_to_plane(c);
+    if (e) return e;
     for (const auto &b : c->ibm)
       if (b.n > 0) {
-        int e = ibm_sweeps(c, b, 1);
+        e = ibm_sweeps(c, b, 1);
         if (e) return e;
       }
-    int e = formbcs_zero(c, old);
+    e = formbcs_zero(c, old);
     if (e) return e;
+    c->p_carry = true;
   }
   return CB_OK;
 }
@@ -396,6 +420,7 @@ static int fill_ptab(cb_ctx *c) {
   h[PT_MISC + 11] = c->aj;
   for (int a = 0; a < 3; a++) h[PT_GCL + a] = c->gcl[a];
   for (int a = 0; a < 3; a++) { h[PT_SIGA + a] = c->sig_a[a]; h[PT_SIGB + a] = c->sig_b[a]; }
+  h[PT_PL] = c->pl;
   CB_CUDA(c, cudaMemcpyAsync(c->ptab, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   if (c->ptab4) CB_CUDA(c, cudaMemcpyAsync(c->ptab4, c->met4, sizeof(c->met4), cudaMemcpyHostToDevice, c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -404,8 +429,9 @@ static int fill_ptab(cb_ctx *c) {
 
 static void invalidate_graphs(cb_ctx *c) {
   for (auto &row : c->graphs)
-    for (auto &g : row)
-      if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
+    for (auto &col : row)
+      for (auto &g : col)
+        if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
 }
 
 extern "C" {
@@ -558,7 +584,7 @@ void cb_destroy(cb_ctx *c) {
     if (b.surf) cudaFree(b.surf);
     if (b.list) cudaFree(b.list);
   }
-  if (c->spare) cudaFree(c->spare);
+  if (c->ibm_arena) cudaFree(c->ibm_arena);
   if (c->ptab) cudaFree(c->ptab);
   if (c->status) cudaFree(c->status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -580,8 +606,12 @@ int cb_launches_per_step(const cb_ctx *c) {
   }
   int ib = 0;
   if (ibm_active(c)) {
+    ib += 1;  // EqOfState into the pressure plane
     for (const auto &b : c->ibm) ib += b.n > 0 ? 2 * IBM_SWEEPS : 0;
-    ib += c->fully_periodic ? 1 : per_stage - 2;  // FormBCS(user, 0): no stage kernel, no RK combine
+    // FormBCS(user, 0): no stage kernel, no RK combine; P copies and ghost wrap beside Q's
+    int nper = 0;
+    for (int d = 0; d < 3; d++) nper += c->cfg.bctype[2 * d] == 7;
+    ib += c->fully_periodic ? 2 : per_stage - 2 + nper + 1;
   }
   return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0) + ib;
 }
@@ -698,6 +728,7 @@ int cb_upload_state(cb_ctx *c, const double *q) {
   if (c->cfg.precision == CB_MIXED && !c->have_refs) set_reference_state(c, q);
   c->cur = 0;
   c->uc = -1;
+  c->p_carry = false;
   int e = upload_planes(c, q, 5, PT_Q0, false);
   if (e) return e;
   CB_CUDA(c, cudaMemsetAsync(c->nut, 0, sizeof(double) * c->plane, c->stream));
@@ -714,7 +745,11 @@ int cb_download_state(cb_ctx *c, double *q, double *p) {
   CB_CUDA(c, cudaMemcpyAsync(q, c->staging, sizeof(double) * 5 * nn, cudaMemcpyDeviceToHost, c->stream));
   if (p) {
     CB_CUDA(c, cudaStreamSynchronize(c->stream));
-    eos_pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), c->staging);
+    if (c->p_carry)  // P as the interpolation and FormBCS(user, 0) left it
+      pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_PL), 1,
+                                                                      c->staging);
+    else
+      eos_pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), c->staging);
     CB_CUDA(c, cudaGetLastError());
     CB_CUDA(c, cudaMemcpyAsync(p, c->staging, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
   }
@@ -736,6 +771,7 @@ int cb_rhs(cb_ctx *c, int istage, double *rhs) {
   double alfa, beta;
   rk_coeffs(c, istage < 0 ? 0 : (istage > 2 ? 2 : istage), &alfa, &beta);
   DevFields F = fields_for(c, c->cur, c->cur, -1);
+  if (c->p_carry) F.pin = c->pl;
   if (istage == 0) {
     int e = sigma_update(c, c->cur);
     if (e) return e;
@@ -801,7 +837,7 @@ int cb_rk_step(cb_ctx *c, int nsteps) {
   if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set before cb_rk_step");
   for (int n = 0; n < nsteps; n++) {
     const int ucslot = c->uc + 1;  // 0: none, 1..3: buffer
-    GraphSlot &g = c->graphs[c->cur][ucslot];
+    GraphSlot &g = c->graphs[c->cur][ucslot][c->p_carry ? 1 : 0];
     if (c->use_graphs && !c->timing && g.exec) {
       const int ns = c->cfg.fluxorder;
       CB_CUDA(c, cudaGraphLaunch(g.exec, c->stream));
@@ -814,6 +850,7 @@ int cb_rk_step(cb_ctx *c, int nsteps) {
         in = out;
       }
       c->cur = in;
+      c->p_carry = ibm_active(c);
       continue;
     }
     if (c->use_graphs && !c->timing) {
@@ -975,6 +1012,8 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
   if (n > 0 && !b->surf) return fail(c, CB_E_STATE, "set the body's surface first");
   if (n > 0 && c->cfg.isothermal == 2)
     return fail(c, CB_E_UNSUPPORTED, "the characteristic isothermal IB wall (isothermal 2) is not built");
+  if (n > 0 && c->dc.calc_sigma)
+    return fail(c, CB_E_UNSUPPORTED, "the shock sensor with immersed bodies is not built");
   const int m[3] = {c->cfg.mx, c->cfg.my, c->cfg.mz};
   const bool per[3] = {c->cfg.bctype[0] == 7, c->cfg.bctype[2] == 7, c->cfg.bctype[4] == 7};
   // a node listed twice keeps its last entry
@@ -1017,8 +1056,16 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
   ibm_drop_list(*b);
   invalidate_graphs(c);
   if (nk == 0) return CB_OK;
-  if (!c->spare) CB_CUDA(c, cudaMalloc(&c->spare, sizeof(double) * 5 * c->plane));
-  const size_t bytes = sizeof(int4) * nk + sizeof(long long) * 3 * nk + sizeof(double) * (IBM_NW + 5) * nk;
+  if (!c->ibm_arena) {
+    CB_CUDA(c, cudaMalloc(&c->ibm_arena, sizeof(double) * 7 * c->plane));
+    CB_CUDA(c, cudaMemsetAsync(c->ibm_arena, 0, sizeof(double) * 7 * c->plane, c->stream));
+    c->spare = c->ibm_arena;
+    c->psnap = c->ibm_arena + 5 * c->plane;
+    c->pl = c->ibm_arena + 6 * c->plane;
+    int fe = fill_ptab(c);
+    if (fe) return fe;
+  }
+  const size_t bytes = sizeof(int4) * nk + sizeof(long long) * 3 * nk + sizeof(double) * (IBM_NW + 6) * nk;
   CB_CUDA(c, cudaMalloc(&b->list, bytes));
   b->node = (int4 *)b->list;
   b->don = (long long *)(b->node + nk);
@@ -1055,8 +1102,13 @@ int cb_ibm_interpolate(cb_ctx *c, int ibi, int add_dundt) {
   if (e) return e;
   if (!c->have_state) return fail(c, CB_E_STATE, "no state uploaded");
   if (b->n > 0) {
+    if (!c->p_carry) {  // P is the EqOfState of the state until an interpolation writes it
+      e = eos_to_plane(c);
+      if (e) return e;
+    }
     e = ibm_sweeps(c, *b, add_dundt ? 1 : 0);
     if (e) return e;
+    c->p_carry = true;
   }
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
   return CB_OK;

@@ -109,6 +109,7 @@ static __global__ void bc_combine_kernel(const DevCfg c, DevFields F, int istage
 }
 
 __device__ __forceinline__ double lp_at(const DevCfg &c, const DevFields &F, long long n) {
+  if (F.pin) return F.pin[n];  // the pressure carried in lP
   const double r = F.q[0][n];
   return r != 0.0 ? (c.gamma - 1) * (F.q[4][n] - 0.5 * (F.q[1][n] * F.q[1][n] + F.q[2][n] * F.q[2][n] + F.q[3][n] * F.q[3][n]) / r)
                   : 0.0;
@@ -288,6 +289,60 @@ static __global__ void bc_periodic_dir_kernel(const DevCfg c, DevFields F, int d
       if (do_lo) F.qout[q][lo] = F.q[q][lo - 2 * s];
       if (do_hi) F.qout[q][hi] = F.q[q][hi + 2 * s];
     }
+  }
+}
+
+// The pressure's periodic copies in FormBCS (rhs.c:1107-1227 copy P from lP
+// beside Q from lQ): fully periodic, the final value source of bc_source;
+// `psnap` is P before the copies.
+static __global__ void bc_periodic_p_kernel(const DevCfg c, const double *psnap, double *P) {
+  const long long total = shell_count(c);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    shell_node(c, t, i, j, k);
+    int si, sj, sk;
+    bool from_in;
+    bc_source(c, i, j, k, si, sj, sk, from_in);
+    const long long g = gidx(c, i, j, k), s = gidx(c, si, sj, sk);
+    P[g] = from_in ? psnap[s] : P[s];
+  }
+}
+
+// One periodic direction's pressure copies with the guards of
+// bc_periodic_dir_kernel.
+static __global__ void bc_periodic_dir_p_kernel(const DevCfg c, const double *psnap, double *P, int dir) {
+  int na, nb;
+  if (dir == 0) { na = c.my; nb = c.mz; }
+  else if (dir == 1) { na = c.mx; nb = c.mz; }
+  else { na = c.mx; nb = c.my; }
+  const long long s = gstride(c, dir);
+  const long long total = (long long)na * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t % na), b = (int)(t / na);
+    long long lo, hi;
+    bool do_lo = true, do_hi = true;
+    if (dir == 0) {
+      lo = gidx(c, 0, a, b); hi = gidx(c, c.mx - 1, a, b);
+      do_lo = do_hi = (a > 0 && b > 0);
+    } else if (dir == 1) {
+      lo = gidx(c, a, 0, b); hi = gidx(c, a, c.my - 1, b);
+      do_lo = b > 0;
+      do_hi = b > 0 && b < c.mz - 1;
+    } else {
+      lo = gidx(c, a, b, 0); hi = gidx(c, a, b, c.mz - 1);
+    }
+    if (do_lo) P[lo] = psnap[lo - 2 * s];
+    if (do_hi) P[hi] = psnap[hi + 2 * s];
+  }
+}
+
+// EqOfState (rhs.c:4820-4862) on every node of the padded box; rho = 0
+// (unused padding) gives 0.
+static __global__ void eos_plane_kernel(const DevCfg c, const double *const *q, double *P) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < c.plane; t += (long long)gridDim.x * blockDim.x) {
+    const double r = q[0][t];
+    P[t] = r != 0.0 ? (c.gamma - 1) * (q[4][t] - 0.5 * (q[1][t] * q[1][t] + q[2][t] * q[2][t] + q[3][t] * q[3][t]) / r)
+                    : 0.0;
   }
 }
 

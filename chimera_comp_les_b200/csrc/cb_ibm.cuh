@@ -10,9 +10,9 @@
 // compact buffer; the second launch stores them at the node and at its
 // periodic ghost images.  Five sweeps (itr_tmp, ibm_iso.c:2616).
 //
-// Donor pressures are the equation of state of the donor's conserved values
-// (EqOfState, rhs.c:4850); the reference keeps the interpolated pressure of an
-// interface node in P, whose EOS image differs from it by rounding only.
+// Pressures live in a plane P holding the reference's P / lP: the EqOfState
+// after the last stage, overwritten at interface nodes (and their ghost
+// images) by each sweep's interpolated pressure, which donors read.
 #pragma once
 #include "cb_common.cuh"
 
@@ -31,19 +31,14 @@ struct IbmDev {
   const int *tri;         // nv1, nv2, nv3 of each element
   const double *nf;       // element normals, 3 per element
   const double *u, *uold; // vertex velocities of this and the previous step, 3 per vertex
-  double *out;            // 5 x n: the sweep's conserved values
+  double *out;            // 6 x n: the sweep's conserved values and pressure
 };
-
-__device__ __forceinline__ double ibm_eos(const DevCfg &c, const double *const *q, long long g) {
-  const double r = q[0][g];
-  return (c.gamma - 1) * (q[4][g] - 0.5 * (q[1][g] * q[1][g] + q[2][g] * q[2][g] + q[3][g] * q[3][g]) / r);
-}
 
 // One sweep over the list: new Q of every interface node from the state q.
 // slip: freeslip (inviscid or wallfunction 3), else noslip; iso1: isothermal
 // wall with Tb = 1 (rho = p gamma Ma^2), else d rho / dn = 0.
-static __global__ void __launch_bounds__(256) ibm_interp_kernel(const DevCfg c, const double *const *q, IbmDev b,
-                                                                 int add_dundt, int twoD, int slip, int iso1) {
+static __global__ void __launch_bounds__(256) ibm_interp_kernel(const DevCfg c, const double *const *q, const double *P,
+                                                                 IbmDev b, int add_dundt, int twoD, int slip, int iso1) {
   const int n = b.n;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     const int cell = b.node[e].w;
@@ -90,7 +85,7 @@ static __global__ void __launch_bounds__(256) ibm_interp_kernel(const DevCfg c, 
 #pragma unroll
       for (int d = 0; d < 3; d++) Ub[d] = sb / sc * (Uc[d] - Ua[d]) + Ua[d];
     }
-    double pb = ibm_eos(c, q, d1) * sk1 + ibm_eos(c, q, d2) * sk2 + ibm_eos(c, q, d3) * sk3;
+    double pb = P[d1] * sk1 + P[d2] * sk2 + P[d3] * sk3;  // ibm_iso.c:2737-2741
     if (twoD == 1) Ub[0] = 0.;
     if (twoD == 2) Ub[1] = 0.;
     if (twoD == 3) Ub[2] = 0.;
@@ -104,21 +99,23 @@ static __global__ void __launch_bounds__(256) ibm_interp_kernel(const DevCfg c, 
     b.out[2 * n + e] = rv;
     b.out[3 * n + e] = rw;
     b.out[4 * n + e] = pb / (c.gamma - 1) + 0.5 * (ru * ru + rv * rv + rw * rw) / rho;
+    b.out[5 * n + e] = pb;
   }
 }
 
-// Store the sweep's values at each interface node and at every ghost image of
-// it in the periodic directions (the DMGlobalToLocal that ends a sweep).
-static __global__ void __launch_bounds__(256) ibm_scatter_kernel(const DevCfg c, double *const *q, IbmDev b) {
+// Store the sweep's values (Q and P) at each interface node and at every ghost
+// image of it in the periodic directions (the DMGlobalToLocal of Q and P that
+// ends a sweep).
+static __global__ void __launch_bounds__(256) ibm_scatter_kernel(const DevCfg c, double *const *q, double *P, IbmDev b) {
   const int n = b.n;
   const bool per[3] = {c.bctype[0] == 7, c.bctype[2] == 7, c.bctype[4] == 7};
   const int m[3] = {c.mx, c.my, c.mz};
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     const int4 nd = b.node[e];
     const int x[3] = {nd.x, nd.y, nd.z};
-    double v[5];
+    double v[6];
 #pragma unroll
-    for (int f = 0; f < 5; f++) v[f] = b.out[f * n + e];
+    for (int f = 0; f < 6; f++) v[f] = b.out[f * n + e];
     for (int a = -1; a <= 1; a++)
       for (int bb = -1; bb <= 1; bb++)
         for (int cc = -1; cc <= 1; cc++) {
@@ -135,6 +132,7 @@ static __global__ void __launch_bounds__(256) ibm_scatter_kernel(const DevCfg c,
           const long long g = gidx(c, y[0], y[1], y[2]);
 #pragma unroll
           for (int f = 0; f < 5; f++) q[f][g] = v[f];
+          P[g] = v[5];
         }
   }
 }

@@ -577,10 +577,12 @@ constexpr int S_NZF = SBX * SBY;   // 224
 template <typename R, bool MIX>
 struct StageSmem {
   static constexpr int NG = FaceWidth<MIX>::NG;
-  // ring + face buffers, FP64 staging of the next plane (5 state fields + nvert),
-  // nvert byte ring [4][PN]
+  // FP64 staging fields per plane: 5 state fields + nvert, and in the FP64 form
+  // the carried pressure
+  static constexpr int NSTG = MIX ? 6 : 7;
+  // ring + face buffers, FP64 staging of the next plane, nvert byte ring [4][PN]
   static constexpr size_t bytes = sizeof(R) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF)) +
-                                  sizeof(double) * (size_t)6 * STile::PN + (size_t)4 * STile::PN;
+                                  sizeof(double) * (size_t)NSTG * STile::PN + (size_t)4 * STile::PN;
 };
 constexpr size_t STAGE_SMEM_BYTES = StageSmem<double, false>::bytes;
 constexpr size_t STAGE_SMEM_BYTES_MIXED = StageSmem<float, true>::bytes;
@@ -662,8 +664,9 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
                                            double alfa, double beta, double adt, int kchunk, double *smem_d) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
   constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
-  double *stg = smem_d;  // [6][PN] raw FP64 Q and nvert of the next plane
-  R *smem = reinterpret_cast<R *>(smem_d + (size_t)6 * PN);
+  constexpr int NSTG = StageSmem<R, MIX>::NSTG;
+  double *stg = smem_d;  // [NSTG][PN] raw FP64 Q, nvert and carried pressure of the next plane
+  R *smem = reinterpret_cast<R *>(smem_d + (size_t)NSTG * PN);
   Ring<R, BX, BY> Rg;
   Rg.pl = smem;
   R *gxb = smem + (size_t)4 * NF * PN;  // [NG][S_NXF]
@@ -671,7 +674,10 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   R *gzb = gyb + (size_t)NG * S_NYF;    // [NG][S_NZF]
   unsigned char *nvc = reinterpret_cast<unsigned char *>(gzb + (size_t)NG * S_NZF);  // [4][PN]
   Rg.nvc = nvc;
-  const int nstg = c.nvq ? 6 : 5;  // staged fields per plane
+  // staged fields per plane: Q, then nvert (byte-exact codes), then lP (carried pressure)
+  const bool pst = !MIX && F.pin != nullptr;
+  const int pslot = c.nvq ? 6 : 5;
+  const int nstg = pslot + (pst ? 1 : 0);
 
   const int tid = threadIdx.x;
   const int i0 = 1 + bxi * BX, j0 = 1 + byi * BY;
@@ -691,7 +697,8 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       const bool ok = xi <= c.mx + 1 && yj <= c.my + 1 && kk >= -2 && kk <= c.mz + 1;
       // field pointer by selects (a dynamic index into the parameter struct
       // would copy the whole struct to local memory)
-      const double *base = q == 0 ? F.q[0] : q == 1 ? F.q[1] : q == 2 ? F.q[2] : q == 3 ? F.q[3] : q == 4 ? F.q[4] : F.nvert;
+      const double *base = q == 0 ? F.q[0] : q == 1 ? F.q[1] : q == 2 ? F.q[2] : q == 3 ? F.q[3] : q == 4 ? F.q[4]
+                           : q == pslot ? F.pin : F.nvert;
       const double *src = ok ? base + gidx(c, xi, yj, kk) : base;
       cp_async8(stg + e, src, ok);
     }
@@ -706,7 +713,8 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       for (int q = 0; q < 5; q++) v[q] = stg[q * PN + idx];
       if (v[0] != 0.0) {
         const double r = v[0];
-        v[F_P] = (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / r);
+        v[F_P] = pst ? stg[pslot * PN + idx]
+                     : (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / r);
         v[F_U] = v[1] / r;
         v[F_V] = v[2] / r;
         v[F_W] = v[3] / r;
@@ -723,7 +731,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       R *base = Rg.pl + (size_t)s * NF * PN + idx;
 #pragma unroll
       for (int q = 0; q < NF; q++) base[(size_t)q * PN] = R(v[q]);
-      if (nstg == 6) nvc[s * PN + idx] = (unsigned char)(stg[5 * PN + idx] * 4.0);
+      if (c.nvq) nvc[s * PN + idx] = (unsigned char)(stg[5 * PN + idx] * 4.0);
     }
   };
   auto load_plane_sync = [&](int kk, int s) {

@@ -71,8 +71,9 @@ def make(name, spec):
     surf = W.sphere_surface(1.6, ctr, 3)
     n_v = len(surf["x"])
     rng = np.random.default_rng(seed)
-    u = rng.normal(size=(n_v, 3)) * 0.05
-    uold = u + rng.normal(size=(n_v, 3)) * 0.01
+    # a slowly accelerating surface: d(Un)/dt = O(0.1), pressures stay positive
+    u = rng.normal(size=(n_v, 3)) * 0.02
+    uold = u + rng.normal(size=(n_v, 3)) * 2e-4
     q = W.random_smooth_state(shape, seed=seed)
 
     scfg = O.Config(**{**cfg.__dict__, **(list_kw or {})})

@@ -1,0 +1,189 @@
+"""GPU parity of the immersed-boundary path (cb_ibm_*): the interpolation
+(ibm_interpolation_advanced, ibm_iso.c:2572-2880) and immersed time steps
+(RungeKutta with -imm, solvers.c:245-288) against the reference's outputs
+(tests/golden/ibm, made by the reference's own search and interpolation) and
+against the oracle restatement.
+
+Bar (FP64 form): per conserved field, relative L2 <= 1e-12 (RTOL_L2)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from chimera_comp_les_b200 import ChimeraError
+from chimera_comp_les_b200 import workloads as W
+
+from _common import (RTOL_L2, gpu_block, gpu_ibm_block, ibm_golden_names, load_ibm_golden, per_field_rel_l2,
+                     synthetic_ibm_list)
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ibm_golden_names()
+
+
+def _fixture_block(name, precision="fp64"):
+    cfg, meta, g, info, surf = load_ibm_golden(name)
+    b = gpu_ibm_block(cfg, g["coords"], g["nvert"], g["q"], surf, info, g["u"], g["uold"], precision)
+    return cfg, meta, g, info, b
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_interpolation_matches_reference(name):
+    cfg, meta, g, info, b = _fixture_block(name)
+    with b:
+        assert b.ibm_count(0) == info.size
+        b.ibm_interpolation_advanced(0, 1)
+        q = b.Q()
+        p = b.EqOfState()
+    k, j, i = info["nk"], info["nj"], info["ni"]
+    assert max(per_field_rel_l2(q[k, j, i], g["q_interp"])) <= RTOL_L2
+    assert O.rel_l2(p[k, j, i], g["p_interp"]) <= RTOL_L2
+    rest = np.ones(q.shape[:3], dtype=bool)
+    rest[k, j, i] = False
+    assert np.array_equal(q[rest], g["q"][rest])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_immersed_steps_match_reference(name):
+    cfg, meta, g, info, b = _fixture_block(name)
+    with b:
+        b.RungeKutta(meta["steps"])
+        q = b.Q()
+    errs = per_field_rel_l2(q, g["q_steps"])
+    assert max(errs) <= RTOL_L2, errs
+
+
+def _synthetic_case(seed=5, n=(37, 29, 33), **kw):
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    shape = coords.shape[:3]
+    base = dict(les=1, inviscid=0, fluxorder=3, ren=500., ma=0.3, pr=0.71, dt=0.002, isothermal=1)
+    base.update(kw)
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, immersed=1, **base)
+    surf = W.sphere_surface(2.0, coords[shape[0] // 2, shape[1] // 2, shape[2] // 2], 2)
+    info = synthetic_ibm_list(cfg, coords, len(surf["nv1"]), seed=seed, radius=6.0)
+    rng = np.random.default_rng(seed)
+    u = rng.normal(size=(len(surf["x"]), 3)) * 0.02
+    uold = u * 0.99
+    q = W.random_smooth_state(shape, seed=seed)
+    nv = np.zeros(shape)
+    nv[info["nk"], info["nj"], info["ni"]] = 1.0
+    return cfg, coords, q, nv, surf, info, u, uold
+
+
+SYN = [
+    ("les_noslip_periodic", {}),
+    ("inviscid_iso0_kflow", dict(les=0, inviscid=1, isothermal=0, bctype=(7, 7, 7, 7, 45, 45))),
+    ("visc_wf3_walls", dict(les=0, wallfunction=3, bctype=(7, 7, 3, 3, 44, 44))),
+]
+
+
+@pytest.mark.parametrize("name,kw", SYN, ids=[s[0] for s in SYN])
+def test_synthetic_list_steps_match_oracle(name, kw):
+    """Duplicate nodes (the later entry wins), donors that are interface nodes
+    (sweeps chain), the element-normal fallback, a moving surface; several
+    tiles and k-chunks."""
+    cfg, coords, q, nv, surf, info, u, uold = _synthetic_case(**kw)
+    o = O.Oracle(cfg)
+    met = o.metrics(o.fill_ghosts(O.to_padded(cfg, coords)))
+    st = o.initial_state(q)
+    o.steps_immersed(3, st, met, o.fill_ghosts(O.to_padded(cfg, nv)), O.IbmSurface(surf, u, uold), info,
+                     O.to_padded(cfg, coords))
+    with gpu_ibm_block(cfg, coords, nv, q, surf, info, u, uold) as b:
+        assert b.ibm_count(0) == len({(a, c, d) for a, c, d in zip(info["ni"], info["nj"], info["nk"])})
+        b.RungeKutta(3)
+        qd = b.Q()
+        pd = b.EqOfState()
+    assert max(per_field_rel_l2(qd, O.from_padded(st["q"]))) <= RTOL_L2
+    assert O.rel_l2(pd, O.from_padded(st["lp"])[..., 0]) <= RTOL_L2
+
+
+def test_two_bodies_in_order():
+    cfg, coords, q, nv, surf, info, u, uold = _synthetic_case(seed=9)
+    half = info.size // 2
+    lists = [info[:half], info[half:]]
+    o = O.Oracle(cfg)
+    met = o.metrics(o.fill_ghosts(O.to_padded(cfg, coords)))
+    st = o.initial_state(q)
+    surfs = [O.IbmSurface(surf, u, uold), O.IbmSurface(surf, -u, -uold)]
+    o.steps_immersed(2, st, met, o.fill_ghosts(O.to_padded(cfg, nv)), surfs, lists, O.to_padded(cfg, coords))
+    with gpu_block(cfg) as b:
+        b.FormMetrics(coords)
+        b.set_nvert(nv)
+        b.SetInitialCondition(q)
+        for ibi, (lst, sgn) in enumerate(zip(lists, (1, -1))):
+            b.set_ibm_surface(ibi, surf)
+            b.set_ibm_velocity(ibi, sgn * u, sgn * uold)
+            b.set_ibm_list(ibi, lst, coords)
+        b.RungeKutta(2)
+        qd = b.Q()
+    assert max(per_field_rel_l2(qd, O.from_padded(st["q"]))) <= RTOL_L2
+
+
+def test_graph_replay_equals_eager_with_bodies():
+    cfg, coords, q, nv, surf, info, u, uold = _synthetic_case(seed=3, n=(30, 22, 26))
+    with gpu_ibm_block(cfg, coords, nv, q, surf, info, u, uold) as b:
+        b.RungeKutta(5)
+        qa = b.Q()
+    with gpu_ibm_block(cfg, coords, nv, q, surf, info, u, uold) as b:
+        b.timing(True)
+        b.RungeKutta(5)
+        qb = b.Q()
+    assert np.array_equal(qa, qb)
+
+
+def test_mixed_form_with_bodies_tracks_fp64():
+    cfg, coords, q, nv, surf, info, u, uold = _synthetic_case(seed=4, n=(40, 32, 36))
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with gpu_ibm_block(cfg, coords, nv, q, surf, info, u, uold, precision=prec) as b:
+            b.RungeKutta(20)
+            out[prec] = b.Q()
+    assert max(per_field_rel_l2(out["mixed"], out["fp64"])) <= 1e-5
+
+
+def test_removing_the_list_restores_plain_steps():
+    cfg, coords, q, nv, surf, info, u, uold = _synthetic_case(seed=6, n=(24, 20, 22))
+    with gpu_block(cfg) as b:
+        b.FormMetrics(coords)
+        b.set_nvert(nv)
+        b.SetInitialCondition(q)
+        b.RungeKutta(2)
+        want = b.Q()
+    with gpu_ibm_block(cfg, coords, nv, q, surf, info, u, uold) as b:
+        b.set_ibm_list(0, info[:0], coords)
+        assert b.ibm_count(0) == 0
+        b.RungeKutta(2)
+        assert np.array_equal(b.Q(), want)
+
+
+def test_invalid_lists_and_options_fail_loudly():
+    cfg, coords, q, nv, surf, info, u, uold = _synthetic_case(seed=2, n=(20, 18, 16))
+    with gpu_block(cfg) as b:
+        b.FormMetrics(coords)
+        b.SetInitialCondition(q)
+        with pytest.raises(ChimeraError) as ei:
+            b.set_ibm_list(0, info, coords)  # no surface yet
+        assert ei.value.code == 3
+        b.set_ibm_surface(0, surf)
+        bad = info.copy()
+        bad[3]["i2"] = cfg.mx + 5
+        with pytest.raises(ChimeraError) as ei:
+            b.set_ibm_list(0, bad, coords)
+        assert ei.value.code == 1
+        bad = info.copy()
+        bad[0]["cell"] = len(surf["nv1"])
+        with pytest.raises(ChimeraError):
+            b.set_ibm_list(0, bad, coords)
+        for wf in (1, 2):
+            with pytest.raises(ChimeraError) as ei:
+                b.set_ibm_options(0, wf)
+            assert ei.value.code == 5
+        with pytest.raises(ChimeraError):
+            b.set_ibm_surface(16, surf)  # body index out of range (CB_IBM_MAX_BODIES)
+    cfg2 = O.Config(**{**cfg.__dict__, "isothermal": 2})
+    with gpu_block(cfg2) as b:
+        b.FormMetrics(coords)
+        b.SetInitialCondition(q)
+        b.set_ibm_surface(0, surf)
+        with pytest.raises(ChimeraError) as ei:
+            b.set_ibm_list(0, info, coords)
+        assert ei.value.code == 5
