@@ -510,6 +510,96 @@ def run_sweep(args, local):
         print(json.dumps(out), flush=True)
 
 
+# -------------------------------------------------------- sphere (IB) --
+# algorithmic bytes of one interpolation sweep per list entry: node 16, donor
+# offsets 24, weights 88, three donors' Q and P 144, the element's vertex
+# velocities now and one step back 144 and its vertex indices 12, the new Q
+# and P written 48, then read 48 and stored at the node 48
+B_IBM_ENTRY = 16 + 24 + 88 + 144 + 144 + 12 + 48 + 48 + 48
+SPHERE_OPTS = dict(les=1, inviscid=0, fluxorder=3, eno_order=2, central=2, s_x=1.0, s_y=1.0, s_z=1.0, ren=300.0,
+                   ma=0.3, pr=0.71, gamma=1.4, dt=1e-3, cs_const=0.1, isothermal=0, flux="roe")
+
+
+def run_sphere(args, local):
+    """Flow past a stationary sphere with the immersed boundary on the device:
+    DMDA 192 x 192 x 256 (i, j across, k streamwise on [-5, 15] D), nodes
+    clustered toward the sphere (spacing 0.01 D there), slip walls in i and j,
+    inflow / outflow 45 in k, Re 300, Ma 0.3, WENO3 with the Roe flux,
+    Smagorinsky CS 0.1, dt 1e-3; uniform stream plus seeded 1e-3 white noise.
+    The interpolation list comes from workloads.sphere_ibm_list (an analytic
+    stand-in for the reference's host search).  Per form: cell-updates/s per
+    stage with the interpolation in every step, the interpolation's share of
+    the step, one interpolation's device time, and the host round trip
+    (download + upload of Q) a host-side interpolation would add per step.
+    One JSON line (not the contract line)."""
+    import torch
+
+    from chimera_comp_les_b200 import Block
+    from chimera_comp_les_b200 import diagnostics as D
+    from chimera_comp_les_b200 import workloads as W
+    torch.cuda.set_device(local)
+    n = tuple(int(x) for x in args.sphere_n.split(","))
+    t0 = time.perf_counter()
+    case = W.sphere_case(n=n)
+    build_s = time.perf_counter() - t0
+    info = case["info"]
+    out = {"workload": f"sphere D=1, DMDA {n[0]}x{n[1]}x{n[2]}, clustered to 0.01 D, slip i/j, inflow/outflow 45 in k, "
+                       "Re 300 Ma 0.3, WENO3 + Roe, Smagorinsky CS 0.1, SSP-RK3, dt 1e-3",
+           "interface_nodes": int(info.size), "list_build_s": build_s, "unit": UNIT}
+    final = {}
+    peak, peak_kind = measured_peaks()
+    for prec in ("fp64", "mixed"):
+        blk = Block(n[0], n[1], n[2], bctype=case["bctype"], precision=prec, device=local, **SPHERE_OPTS)
+        blk.FormMetrics(case["coords"])
+        blk.set_nvert(case["nvert"])
+        blk.SetInitialCondition(case["q"])
+        blk.set_ibm_surface(0, case["surface"])
+        blk.set_ibm_list(0, info, case["coords"])
+        kc, _ = blk.autotune()
+        steps = args.steps
+        ms_ib, clocks = _timed(blk, steps, args.warmup, 1, local, sample_clocks=(prec == "mixed"))
+        # one interpolation (five sweeps), device time on the library's stream
+        stream = torch.cuda.ExternalStream(blk.stream, device=f"cuda:{local}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(10):
+            blk.ibm_interpolation_advanced(0, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        interp_ms = e0.elapsed_time(e1) / 10
+        # host round trip per step a host-side interpolation would need
+        qh = np.empty(blk.shape + (5,))
+        t1 = time.perf_counter()
+        for _ in range(3):
+            blk.download(qh)
+            blk.SetInitialCondition(qh)
+        rt_ms = (time.perf_counter() - t1) / 3 * 1e3
+        # the same steps without the list
+        blk.set_ibm_list(0, info[:0], case["coords"])
+        ms_plain, _ = _timed(blk, steps, args.warmup, 1, local)
+        interior = blk.interior_nodes
+        out[prec] = {"value": interior * blk.stages * steps / (ms_ib / 1e3), "ms_per_step": ms_ib / steps,
+                     "ms_per_step_without_ib": ms_plain / steps,
+                     "ib_ms_per_step": (ms_ib - ms_plain) / steps,
+                     "ib_share_of_step": (ms_ib - ms_plain) / ms_ib,
+                     "interpolation_ms": interp_ms,
+                     "sweep_gbs": B_IBM_ENTRY * info.size * 5 / (interp_ms / 1e3) / 1e9,
+                     "host_roundtrip_ms_per_step": rt_ms, "kchunk_autotuned": kc}
+        if clocks:
+            out["clocks"] = clocks
+        blk.set_ibm_list(0, info, case["coords"])
+        blk.SetInitialCondition(case["q"])
+        blk.RungeKutta(args.sphere_acc_steps)
+        final[prec] = blk.Q()
+        blk.close()
+    l2, linf = D.field_errors(final["mixed"], final["fp64"])
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["mixed_vs_fp64_error"] = {"steps": args.sphere_acc_steps, "rel_l2": l2, "rel_linf": linf}
+    out["peak_gbs"] = peak
+    out["peak_source"] = peak_kind
+    print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------------- sharded (N > 1) --
 def run_sharded(args, ws, rank, local):
     """k-slab decomposition of one periodic TGV box of 128 x 128 x 128N unique
@@ -634,6 +724,10 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the multi-block batched measurement")
     ap.add_argument("--sweep", default="", help="comma-separated sizes, e.g. 128,256,384,512: isotropic-turbulence "
                                                   "size sweep, one JSON line per size instead of the bench line")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "sphere"],
+                    help="sphere: flow past a sphere with the device immersed boundary, one JSON line of its own")
+    ap.add_argument("--sphere-n", default="192,192,256", help="DMDA node counts mx,my,mz of the sphere workload")
+    ap.add_argument("--sphere-acc-steps", type=int, default=50, help="steps of the sphere's mixed-vs-FP64 comparison")
     ap.add_argument("--layout", default="auto", choices=["auto", "replicas", "slabs"],
                     help="N GPUs: one TGV box split in k-slabs with halo exchange (default for N > 1), "
                          "or independent replicas")
@@ -647,6 +741,8 @@ def main():
             run_reference(args, ws, rank)
         elif args.sweep:
             run_sweep(args, local)
+        elif args.workload == "sphere":
+            run_sphere(args, local)
         elif layout == "slabs":
             run_sharded(args, ws, rank, local)
         else:

@@ -115,7 +115,7 @@ static int fail(cb_ctx *c, int code, const std::string &msg) {
 
 // device pointer tables inside ctx->ptab
 enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27, PT_NUT = 32, PT_MISC = 33, PT_GCL = 48,
-       PT_SIGA = 56, PT_SIGB = 59, PT_PL = 64, PT_N = 65 };
+       PT_SIGA = 56, PT_SIGB = 59, PT_PL = 64, PT_SNAP = 65, PT_N = 71 };
 
 static int grid_for(const cb_ctx *c, long long work, int block = 256) {
   long long b = (work + block - 1) / block;
@@ -317,9 +317,19 @@ static int eos_to_plane(cb_ctx *c) {
 // with Q; then the ghost wrap of both that FormBCS ends with
 // (rhs.c:1305-1308).  No EqOfState follows: the pressure plane is carried.
 static int formbcs_zero(cb_ctx *c, int old) {
-  CB_CUDA(c, cudaMemcpyAsync(c->spare, c->qb[c->cur][0], sizeof(double) * 5 * c->plane, cudaMemcpyDeviceToDevice,
-                             c->stream));
-  CB_CUDA(c, cudaMemcpyAsync(c->psnap, c->pl, sizeof(double) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
+  // snapshot of Q and P within five layers of the faces: FormBCS reads its lQ / lP
+  // at most two nodes beyond the boundary layer, on either side
+  if (std::min(c->dc.mx, std::min(c->dc.my, c->dc.mz)) >= 6) {
+    const long long thick = thick_shell_count(c->dc, 5);
+    thick_shell_copy_kernel<<<grid_for(c, thick), 256, 0, c->stream>>>(
+        c->dc, 5, (const double *const *)(c->ptab + 5 * c->cur), c->ptab + PT_SNAP, 5);
+    thick_shell_copy_kernel<<<grid_for(c, thick), 256, 0, c->stream>>>(
+        c->dc, 5, (const double *const *)(c->ptab + PT_PL), c->ptab + PT_SNAP + 5, 1);
+  } else {  // every node lies within five layers of a face
+    CB_CUDA(c, cudaMemcpyAsync(c->spare, c->qb[c->cur][0], sizeof(double) * 5 * c->plane, cudaMemcpyDeviceToDevice,
+                               c->stream));
+    CB_CUDA(c, cudaMemcpyAsync(c->psnap, c->pl, sizeof(double) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
+  }
   DevFields F = fields_for(c, c->cur, old, c->cur);
   for (int q = 0; q < 5; q++) F.q[q] = c->spare + c->plane * q;
   F.pin = c->psnap;
@@ -421,6 +431,8 @@ static int fill_ptab(cb_ctx *c) {
   for (int a = 0; a < 3; a++) h[PT_GCL + a] = c->gcl[a];
   for (int a = 0; a < 3; a++) { h[PT_SIGA + a] = c->sig_a[a]; h[PT_SIGB + a] = c->sig_b[a]; }
   h[PT_PL] = c->pl;
+  for (int q = 0; q < 5; q++) h[PT_SNAP + q] = c->spare ? c->spare + c->plane * q : nullptr;
+  h[PT_SNAP + 5] = c->psnap;
   CB_CUDA(c, cudaMemcpyAsync(c->ptab, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   if (c->ptab4) CB_CUDA(c, cudaMemcpyAsync(c->ptab4, c->met4, sizeof(c->met4), cudaMemcpyHostToDevice, c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -504,7 +516,8 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.inv_ren_half = 1. / cfg->ren * 0.5;
   d.gm1 = cfg->gamma - 1.0;
   d.nvq = 1;  // nvert starts zero
-  if (shell_count(d) >= (1LL << 31)) return bail(CB_E_ARG, "grid too large for 32-bit boundary indexing");
+  if ((long long)(cfg->mx + 4) * (cfg->my + 4) * (cfg->mz + 4) >= (1LL << 31))
+    return bail(CB_E_ARG, "grid too large for 32-bit boundary indexing");
   d.calc_sigma = (cfg->les && cfg->calc_sigma) ? 1 : 0;
   d.s_x_min = cfg->s_x_min; d.s_y_min = cfg->s_y_min; d.s_z_min = cfg->s_z_min;
   d.ks = cfg->sigma_thrsh;
@@ -611,6 +624,7 @@ int cb_launches_per_step(const cb_ctx *c) {
     // FormBCS(user, 0): no stage kernel, no RK combine; P copies and ghost wrap beside Q's
     int nper = 0;
     for (int d = 0; d < 3; d++) nper += c->cfg.bctype[2 * d] == 7;
+    if (std::min(c->dc.mx, std::min(c->dc.my, c->dc.mz)) >= 6) ib += 2;  // the snapshots of Q and P near the faces
     ib += c->fully_periodic ? 2 : per_stage - 2 + nper + 1;
   }
   return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0) + ib;

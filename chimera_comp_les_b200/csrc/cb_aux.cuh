@@ -68,6 +68,54 @@ __device__ __forceinline__ void shell_node(const DevCfg &c, long long t64, int &
   k = (int)K - 2;
 }
 
+// The nodes of the padded box within L layers of its faces (the two ghost
+// layers, the boundary layer and L - 3 interior layers), enumerated as
+// shell_node does for L = 3.
+__host__ __device__ __forceinline__ long long thick_shell_count(const DevCfg &c, int L) {
+  const long long NX = c.mx + 4, NY = c.my + 4, NZ = c.mz + 4;
+  return 2LL * L * NX * NY + (NZ - 2LL * L) * (2LL * L * NX + 2LL * L * (NY - 2LL * L));
+}
+__host__ __device__ __forceinline__ void thick_shell_node(const DevCfg &c, int L, long long t64, int &i, int &j, int &k) {
+  const unsigned t = (unsigned)t64;
+  const unsigned L2 = 2u * L, NX = c.mx + 4, NY = c.my + 4, NZ = c.mz + 4, A = NX * NY, Pm = L2 * NX + L2 * (NY - L2);
+  unsigned I, J, K;
+  if (t < L2 * A) {
+    const unsigned p = t / A, r = t - p * A;
+    K = p < (unsigned)L ? p : NZ - L2 + p;
+    J = r / NX;
+    I = r - J * NX;
+  } else {
+    const unsigned t2 = t - L2 * A;
+    K = L + t2 / Pm;
+    const unsigned r = t2 - (K - L) * Pm;
+    if (r < L2 * NX) {
+      const unsigned q = r / NX;
+      J = q < (unsigned)L ? q : NY - L2 + q;
+      I = r - q * NX;
+    } else {
+      const unsigned r2 = r - L2 * NX, cc = r2 % L2;
+      J = L + r2 / L2;
+      I = cc < (unsigned)L ? cc : NX - L2 + cc;
+    }
+  }
+  i = (int)I - 2;
+  j = (int)J - 2;
+  k = (int)K - 2;
+}
+
+// Copy of the planes' nodes within L layers of the faces (the part of a state
+// FormBCS reads: periodic images two nodes across, face codes two nodes in).
+static __global__ void thick_shell_copy_kernel(const DevCfg c, int L, const double *const *src, double *const *dst,
+                                               int nplanes) {
+  const long long total = thick_shell_count(c, L);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    thick_shell_node(c, L, t, i, j, k);
+    const long long g = gidx(c, i, j, k);
+    for (int p = 0; p < nplanes; p++) dst[p][g] = src[p][g];
+  }
+}
+
 // Writes every non-interior node (boundary layer + both ghost layers) of qout.
 static __global__ void bc_periodic_kernel(const DevCfg c, DevFields F) {
   const long long total = shell_count(c);

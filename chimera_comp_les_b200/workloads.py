@@ -249,3 +249,158 @@ def sphere_surface(radius: float, center=(0.0, 0.0, 0.0), subdiv: int = 3):
     return {"x": P[:, 0].copy(), "y": P[:, 1].copy(), "z": P[:, 2].copy(),
             "nv1": tri[:, 0].copy(), "nv2": tri[:, 1].copy(), "nv3": tri[:, 2].copy(),
             "nf_x": n[:, 0].copy(), "nf_y": n[:, 1].copy(), "nf_z": n[:, 2].copy()}
+
+
+# ------------------------------------------------------------ sphere flow --
+def clustered_axis(n: int, a: float, b: float, h_min: float, x0: float = 0.0) -> np.ndarray:
+    """n node positions on [a, b] clustered at x0 by a hyperbolic-sine map,
+    x(s) = x0 + A sinh(beta (s - s0)), s uniform on [0, 1], with the spacing at
+    x0 equal to h_min (A beta = h_min (n - 1))."""
+    if not (a < x0 < b) or h_min * (n - 1) >= (b - a):
+        raise ValueError("clustered_axis: x0 must lie inside (a, b) and h_min be below the uniform spacing")
+    ga = h_min * (n - 1)
+
+    def s0_for(beta):  # x(0) = a, x(1) = b fix s0 for a given beta
+        lo, hi = 0.0, 1.0
+        for _ in range(200):
+            s0 = 0.5 * (lo + hi)
+            r = math.sinh(beta * (1 - s0)) / math.sinh(beta * s0)
+            if r > (b - x0) / (x0 - a):
+                lo = s0
+            else:
+                hi = s0
+        return 0.5 * (lo + hi)
+
+    def span(beta):  # b - a produced by (beta, s0(beta)) at the given centre spacing
+        s0 = s0_for(beta)
+        A = ga / beta
+        return A * (math.sinh(beta * (1 - s0)) + math.sinh(beta * s0)), s0
+
+    lo, hi = 1e-6, 60.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if span(mid)[0] < (b - a):
+            lo = mid
+        else:
+            hi = mid
+    beta = 0.5 * (lo + hi)
+    s0 = s0_for(beta)
+    s = np.arange(n) / (n - 1.0)
+    x = x0 + (ga / beta) * np.sinh(beta * (s - s0))
+    x[0], x[-1] = a, b
+    return x
+
+
+def sphere_case(n=(192, 192, 256), diameter: float = 1.0, h_min: float = 0.01, ma: float = 0.3,
+                gamma: float = 1.4, noise: float = 1e-3, seed: int = 3, subdiv: int = 4):
+    """Flow past a stationary sphere: streamwise k on [-5, 15] D, i and j on
+    [-6, 6] D, nodes clustered toward the sphere at the origin (spacing h_min D
+    there); n = DMDA node counts (mx, my, mz).  The sphere marks nvert in the
+    reference's encoding (ibm_iso.c:765-766): 3 inside, 1 on interface nodes
+    (outside, with an inside node among their 26 neighbours), 0 in the fluid.
+    State: uniform stream rho = 1, w = 1, p = 1/(gamma Ma^2) (the inflow of
+    bctype 45, rhs.c:889-892) plus seeded white noise of amplitude `noise` on
+    the three velocity components.  Returns coords, q, nvert, the surface
+    (sphere_surface) and the interpolation list (sphere_ibm_list)."""
+    mx, my, mz = n
+    D = diameter
+    xs = clustered_axis(mx, -6 * D, 6 * D, h_min * D)
+    ys = clustered_axis(my, -6 * D, 6 * D, h_min * D)
+    zs = clustered_axis(mz, -5 * D, 15 * D, h_min * D)
+    z, y, x = np.meshgrid(zs, ys, xs, indexing="ij")
+    coords = np.ascontiguousarray(np.stack([x, y, z], axis=-1))
+    r = np.sqrt(x * x + y * y + z * z)
+    inside = r < 0.5 * D
+    near = np.zeros_like(inside)
+    ii = np.argwhere(inside)
+    for dk in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for di in (-1, 0, 1):
+                k = np.clip(ii[:, 0] + dk, 0, mz - 1)
+                j = np.clip(ii[:, 1] + dj, 0, my - 1)
+                i = np.clip(ii[:, 2] + di, 0, mx - 1)
+                near[k, j, i] = True
+    nvert = np.zeros((mz, my, mx))
+    nvert[near & ~inside] = 1.0
+    nvert[inside] = 3.0
+    rng = np.random.default_rng(seed)
+    u = noise * rng.standard_normal((mz, my, mx))
+    v = noise * rng.standard_normal((mz, my, mx))
+    w = 1.0 + noise * rng.standard_normal((mz, my, mx))
+    rho = np.ones((mz, my, mx))
+    p = np.full((mz, my, mx), 1.0 / (gamma * ma * ma))
+    q = conserved(rho, u, v, w, p, gamma)
+    surf = sphere_surface(0.5 * D, (0.0, 0.0, 0.0), subdiv)
+    info = sphere_ibm_list(coords, nvert, (0.0, 0.0, 0.0), 0.5 * D, surf)
+    return {"coords": coords, "q": q, "nvert": nvert, "surface": surf, "info": info,
+            "bctype": (3, 3, 3, 3, 45, 45)}
+
+
+IBM_LIST_FIELDS = [
+    ("ni", "<i4"), ("nj", "<i4"), ("nk", "<i4"), ("cell", "<i4"),
+    ("i1", "<i4"), ("j1", "<i4"), ("k1", "<i4"), ("i2", "<i4"), ("j2", "<i4"), ("k2", "<i4"),
+    ("i3", "<i4"), ("j3", "<i4"), ("k3", "<i4"), ("pad", "<i4"),
+    ("cr1", "<f8"), ("cr2", "<f8"), ("cr3", "<f8"), ("cs1", "<f8"), ("cs2", "<f8"), ("cs3", "<f8"),
+    ("d_s", "<f8"), ("d_i", "<f8"), ("pmin", "<f8", (3,)),
+]
+
+
+def sphere_ibm_list(coords: np.ndarray, nvert: np.ndarray, center, radius: float, surf: dict) -> np.ndarray:
+    """An interpolation list for an analytic sphere, in the entry layout of
+    cb_ibm_info.  A stand-in for the reference's ray-casting search
+    (ibm_search_advanced, which stays on the host): for every interface node
+    (nvert 1) the interception point pmin is the nearest point of the sphere,
+    d_s the distance to it, the donor point lies one local grid spacing d_i
+    further out along the normal, and its three nearest fluid nodes (nvert 0)
+    within two nodes carry inverse-distance weights.  The surface element is
+    the triangle whose centroid is nearest to pmin, with equal vertex weights."""
+    c = np.asarray(center, dtype=np.float64)
+    nodes = np.argwhere(nvert == 1.0)  # (k, j, i)
+    mz, my, mx = nvert.shape
+    X = coords[nodes[:, 0], nodes[:, 1], nodes[:, 2]]
+    d = X - c
+    r = np.linalg.norm(d, axis=1)
+    nrm = d / r[:, None]
+    pmin = c + radius * nrm
+    d_s = r - radius
+    # local spacing: the shortest edge to a neighbour along i, j, k
+    h = np.full(len(nodes), np.inf)
+    for ax, lim in ((2, mx), (1, my), (0, mz)):
+        for s in (-1, 1):
+            nb = nodes.copy()
+            nb[:, ax] = np.clip(nb[:, ax] + s, 0, lim - 1)
+            e = np.linalg.norm(coords[nb[:, 0], nb[:, 1], nb[:, 2]] - X, axis=1)
+            h = np.minimum(h, np.where(e > 0, e, np.inf))
+    xd = X + nrm * h[:, None]
+    offs = np.array([(a, b, cc) for a in range(-2, 3) for b in range(-2, 3) for cc in range(-2, 3)])
+    cand = nodes[:, None, :] + offs[None, :, :]
+    lim = np.array([mz, my, mx])
+    valid = np.all((cand >= 0) & (cand < lim), axis=2)
+    cc_ = np.clip(cand, 0, lim - 1)
+    fluid = valid & (nvert[cc_[..., 0], cc_[..., 1], cc_[..., 2]] == 0.0)
+    dist = np.linalg.norm(coords[cc_[..., 0], cc_[..., 1], cc_[..., 2]] - xd[:, None, :], axis=2)
+    dist = np.where(fluid, dist, np.inf)
+    pick = np.argsort(dist, axis=1)[:, :3]
+    dd = np.take_along_axis(dist, pick, axis=1)
+    if not np.all(np.isfinite(dd)):
+        raise ValueError("sphere_ibm_list: an interface node has fewer than three fluid nodes within two nodes")
+    wgt = 1.0 / np.maximum(dd, 1e-12)
+    wgt /= wgt.sum(axis=1, keepdims=True)
+    don = np.take_along_axis(cand, pick[:, :, None], axis=1)  # (n, 3, (k, j, i))
+    # nearest surface element by centroid, in chunks
+    P = np.stack([surf["x"], surf["y"], surf["z"]], 1)
+    cen = (P[surf["nv1"]] + P[surf["nv2"]] + P[surf["nv3"]]) / 3.0
+    cell = np.empty(len(nodes), dtype=np.int32)
+    for a in range(0, len(nodes), 4096):
+        dc = np.linalg.norm(pmin[a:a + 4096, None, :] - cen[None, :, :], axis=2)
+        cell[a:a + 4096] = np.argmin(dc, axis=1)
+    out = np.zeros(len(nodes), dtype=np.dtype(IBM_LIST_FIELDS))
+    out["nk"], out["nj"], out["ni"] = nodes[:, 0], nodes[:, 1], nodes[:, 2]
+    out["cell"] = cell
+    for t, (a, b, cc) in enumerate((("i1", "j1", "k1"), ("i2", "j2", "k2"), ("i3", "j3", "k3"))):
+        out[cc], out[b], out[a] = don[:, t, 0], don[:, t, 1], don[:, t, 2]
+    out["cr1"], out["cr2"], out["cr3"] = wgt[:, 0], wgt[:, 1], wgt[:, 2]
+    out["cs1"] = out["cs2"] = out["cs3"] = 1.0 / 3.0
+    out["d_s"], out["d_i"] = d_s, h
+    out["pmin"] = pmin
+    return out

@@ -187,3 +187,25 @@ def test_invalid_lists_and_options_fail_loudly():
         with pytest.raises(ChimeraError) as ei:
             b.set_ibm_list(0, info, coords)
         assert ei.value.code == 5
+
+
+def test_sphere_workload_small_matches_oracle():
+    """The sphere workload (clustered grid, slip walls, inflow/outflow 45,
+    Roe flux, analytic interpolation list) at 40 x 36 x 48 nodes: three
+    immersed steps against the oracle in both the FP64 and mixed forms."""
+    n = (40, 36, 48)
+    case = W.sphere_case(n=n, h_min=0.05)
+    cfg = O.Config(mx=n[0], my=n[1], mz=n[2], bctype=case["bctype"], les=1, inviscid=0, fluxorder=3, ren=300.,
+                   ma=0.3, pr=0.71, dt=1e-3, cs_const=0.1, isothermal=0, flux=1, immersed=1)
+    o = O.Oracle(cfg)
+    met = o.metrics(O.to_padded(cfg, case["coords"]))
+    st = o.initial_state(case["q"])
+    o.steps_immersed(3, st, met, o.fill_ghosts(O.to_padded(cfg, case["nvert"])), O.IbmSurface(case["surface"]),
+                     case["info"], O.to_padded(cfg, case["coords"]))
+    want = O.from_padded(st["q"])
+    for prec, tol in (("fp64", RTOL_L2), ("mixed", 1e-5)):
+        with gpu_ibm_block(cfg, case["coords"], case["nvert"], case["q"], case["surface"], case["info"],
+                           precision=prec) as b:
+            b.RungeKutta(3)
+            errs = per_field_rel_l2(b.Q(), want)
+        assert max(errs) <= tol, (prec, errs)
