@@ -45,3 +45,32 @@ def test_padded_roundtrip():
     cfg = O.Config(mx=7, my=8, mz=9)
     a = np.random.default_rng(0).standard_normal((9, 8, 7, 5))
     assert np.array_equal(O.from_padded(O.to_padded(cfg, a)), a)
+
+
+def test_clustered_axis_spacing():
+    x = W.clustered_axis(192, -6.0, 6.0, 0.01)
+    dx = np.diff(x)
+    assert x[0] == -6.0 and x[-1] == 6.0 and np.all(dx > 0)
+    assert abs(dx.min() - 0.01) < 1e-4 and abs(x[np.argmin(dx)]) < 0.02
+    z = W.clustered_axis(256, -5.0, 15.0, 0.01)
+    assert abs(np.diff(z).min() - 0.01) < 1e-4 and abs(z[np.argmin(np.diff(z))]) < 0.02
+
+
+def test_sphere_case_list_is_consistent():
+    n = (40, 36, 48)
+    c = W.sphere_case(n=n, h_min=0.05)
+    nv, info, coords = c["nvert"], c["info"], c["coords"]
+    assert nv.shape == (48, 36, 40)
+    k, j, i = info["nk"], info["nj"], info["ni"]
+    assert np.all(nv[k, j, i] == 1.0) and info.size == int((nv == 1.0).sum())
+    assert len(set(zip(i, j, k))) == info.size
+    r = np.linalg.norm(coords[nv == 3.0], axis=1)
+    assert np.all(r < 0.5)
+    assert np.allclose(np.linalg.norm(info["pmin"], axis=1), 0.5)
+    w = np.stack([info["cr1"], info["cr2"], info["cr3"]], 1)
+    assert np.all(w > 0) and np.allclose(w.sum(1), 1.0)
+    for a, b, cc in (("i1", "j1", "k1"), ("i2", "j2", "k2"), ("i3", "j3", "k3")):
+        assert np.all(np.abs(info[a] - i) <= 2) and np.all(np.abs(info[b] - j) <= 2) and np.all(np.abs(info[cc] - k) <= 2)
+        assert np.all(nv[info[cc], info[b], info[a]] == 0.0)
+    assert np.all(info["d_s"] > 0) and np.all(info["d_i"] > 0)
+    assert info["cell"].min() >= 0 and info["cell"].max() < len(c["surface"]["nv1"])
