@@ -39,7 +39,7 @@ class CbConfig(C.Structure):
         ("dt", C.c_double), ("st", C.c_double), ("cs_const", C.c_double), ("ci", C.c_double),
         ("ratio", C.c_double), ("precision", C.c_int), ("device", C.c_int),
         ("calc_sigma", C.c_int), ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double),
-        ("sigma_thrsh", C.c_double), ("flux", C.c_int),
+        ("sigma_thrsh", C.c_double), ("flux", C.c_int), ("max_cs", C.c_double),
     ]
 
 
@@ -72,7 +72,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     for name, args in [
         ("cb_set_grid", [P, D]), ("cb_set_metrics", [P, D, D, D, D]), ("cb_get_metrics", [P, D, D, D, D]), ("cb_set_nvert", [P, D]),
         ("cb_upload_state", [P, D]), ("cb_download_state", [P, D, D]), ("cb_rhs", [P, C.c_int, D]),
-        ("cb_calc_ucat", [P]), ("cb_eddy_viscosity", [P]), ("cb_get_nut", [P, D]),
+        ("cb_calc_ucat", [P]), ("cb_eddy_viscosity", [P]), ("cb_get_nut", [P, D]), ("cb_get_cs", [P, D]),
         ("cb_rk_step", [P, C.c_int]), ("cb_sync", [P]), ("cb_capture_graph", [P]),
         ("cb_timing_enable", [P, C.c_int]),
         ("cb_timing_read", [P, D, C.POINTER(C.c_int), D, C.POINTER(C.c_int)]),

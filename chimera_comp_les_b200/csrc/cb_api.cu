@@ -21,6 +21,7 @@
 #include "../../include/chimera_b200.h"
 #include "cb_aux.cuh"
 #include "cb_common.cuh"
+#include "cb_dyn.cuh"
 #include "cb_ibm.cuh"
 #include "cb_launch.h"
 #include "cb_stage.cuh"
@@ -75,6 +76,8 @@ struct cb_ctx {
   // shock sensor: final hybrid weights (a) and the pass buffer (b)
   double *sig_arena = nullptr;
   double *sig_a[3] = {}, *sig_b[3] = {};
+  // dynamic Smagorinsky: velocity gradients (9), |S|, LM, MM, CS, lCS
+  double *dyn_arena = nullptr;
   bool have_refs = false;
   double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
   double **ptab = nullptr;    // device pointer tables
@@ -115,7 +118,8 @@ static int fail(cb_ctx *c, int code, const std::string &msg) {
 
 // device pointer tables inside ctx->ptab
 enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27, PT_NUT = 32, PT_MISC = 33, PT_GCL = 48,
-       PT_SIGA = 56, PT_SIGB = 59, PT_PL = 64, PT_SNAP = 65, PT_N = 71 };
+       PT_SIGA = 56, PT_SIGB = 59, PT_PL = 64, PT_SNAP = 65, PT_DYN = 71, PT_N = 85 };
+// PT_DYN + 0..8: du/dx .. dw/dz, 9: |S|, 10: LM, 11: MM, 12: CS, 13: lCS
 
 static int grid_for(const cb_ctx *c, long long work, int block = 256) {
   long long b = (work + block - 1) / block;
@@ -257,15 +261,52 @@ static int sigma_update(cb_ctx *c, int in) {
   return CB_OK;
 }
 
+// Compute_Smagorinsky_Constant_1 with -les 2 (les.c:151-1472) into the CS
+// plane, from the current state and the recorded CalcUCat state.
+static int dynamic_cs(cb_ctx *c) {
+  TimedScope ts(c, false);
+  const double *const *q = (const double *const *)(c->ptab + 5 * c->cur);
+  const double *const *qu = c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr;
+  double *const *D = c->ptab + PT_DYN;
+  double *base = c->dyn_arena;
+  double *Sabs = base + 9 * c->plane, *LM = base + 10 * c->plane, *MM = base + 11 * c->plane;
+  double *CS = base + 12 * c->plane, *CT = base + 13 * c->plane;
+  const int gp = grid_for(c, (long long)c->plane);
+  const long long shell = shell_count(c->dc);
+  const long long faces = (long long)(c->dc.my - 2) * (c->dc.mz - 2) + (long long)(c->dc.mx - 2) * (c->dc.mz - 2) +
+                          (long long)(c->dc.mx - 2) * (c->dc.my - 2);
+  dyn_grad_kernel<<<gp, 256, 0, c->stream>>>(c->dc, q, qu, (const double *const *)(c->ptab + PT_MET), c->aj,
+                                             c->nvert, D, Sabs);
+  ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D, 10);  // DMLocalToLocal
+  dyn_copy_kernel<<<grid_for(c, faces), 256, 0, c->stream>>>(c->dc, D, 9);
+  dyn_lm_kernel<<<gp, 256, 0, c->stream>>>(c->dc, q, qu, c->aj, c->nvert, (const double *const *)D, Sabs, LM, MM);
+  ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D + 10, 2);
+  dyn_cs_kernel<<<grid_for(c, (long long)c->dc.mx * c->dc.my * c->dc.mz), 256, 0, c->stream>>>(
+      c->dc, c->nvert, LM, MM, CS, c->cfg.max_cs);
+  CB_CUDA(c, cudaMemcpyAsync(CT, CS, sizeof(double) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
+  ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D + 13, 1);  // DMGlobalToLocal
+  dyn_copy_kernel<<<grid_for(c, faces), 256, 0, c->stream>>>(c->dc, D + 13, 1);
+  dyn_avg_kernel<<<grid_for(c, (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2)), 256, 0, c->stream>>>(
+      c->dc, c->aj, c->nvert, CT, CS);
+  CB_CUDA(c, cudaGetLastError());
+  return CB_OK;
+}
+
 static int nut_update(cb_ctx *c) {
   // Compute_eddy_viscosity_LES from the recorded state (or zero velocity).
   const long long work = (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2);
+  const bool dyn = c->cfg.les == 2;
+  if (dyn) {
+    int e = dynamic_cs(c);
+    if (e) return e;
+  }
   {
     TimedScope ts(c, false);
     const int ekc = eddy_kchunk(c->dc, c->sms);
     eddy_viscosity_kernel<<<eddy_grid(c->dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, c->stream>>>(
         c->dc, c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr,
-        (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvert, c->nut, ekc);
+        (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvert, c->nut, ekc,
+        dyn ? (const double *const *)(c->ptab + 5 * c->cur) : nullptr, dyn ? c->dyn_arena + 12 * c->plane : nullptr);
   }
   {
     TimedScope ts(c, false);
@@ -433,6 +474,7 @@ static int fill_ptab(cb_ctx *c) {
   h[PT_PL] = c->pl;
   for (int q = 0; q < 5; q++) h[PT_SNAP + q] = c->spare ? c->spare + c->plane * q : nullptr;
   h[PT_SNAP + 5] = c->psnap;
+  for (int a = 0; a < 14; a++) h[PT_DYN + a] = c->dyn_arena ? c->dyn_arena + c->plane * a : nullptr;
   CB_CUDA(c, cudaMemcpyAsync(c->ptab, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   if (c->ptab4) CB_CUDA(c, cudaMemcpyAsync(c->ptab4, c->met4, sizeof(c->met4), cudaMemcpyHostToDevice, c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -463,6 +505,7 @@ void cb_config_default(cb_config *cfg, int mx, int my, int mz) {
   cfg->calc_sigma = 0;
   cfg->s_x_min = cfg->s_y_min = cfg->s_z_min = 0.;
   cfg->sigma_thrsh = 0.00001;  // rhs.c:3322
+  cfg->max_cs = 0.05;          // les.c:151
 }
 
 int cb_create(const cb_config *cfg, cb_ctx **out) {
@@ -490,7 +533,9 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   }
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3) return bail(CB_E_ARG, "fluxorder must be 1, 2 or 3");
   if (cfg->eno_order != 2 && cfg->eno_order != 3) return bail(CB_E_ARG, "ENOorder must be 2 or 3");
-  if (cfg->les != 0 && cfg->les != 1) return bail(CB_E_UNSUPPORTED, "only les 0 or 1 (constant Smagorinsky) is built");
+  if (cfg->les < 0 || cfg->les > 2)
+    return bail(CB_E_UNSUPPORTED, "only les 0, 1 (constant Smagorinsky) and 2 (dynamic, box test filter) are built");
+  if (cfg->les == 2 && !(cfg->max_cs >= 0.0)) return bail(CB_E_ARG, "max_cs must be >= 0");
   if (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) return bail(CB_E_ARG, "precision must be CB_FP64 or CB_MIXED");
   if (cfg->flux != 0 && cfg->flux != 1) return bail(CB_E_ARG, "flux must be 0 (Rusanov) or 1 (Roe)");
   c->dev = cfg->device;
@@ -549,6 +594,11 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
     for (int a = 0; a < 3; a++) c->gcl[a] = g + c->plane * a;
     if (cudaMalloc(&c->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab4");
   }
+  if (cfg->les == 2) {
+    const size_t db = sizeof(double) * c->plane * 14;
+    if (cudaMalloc(&c->dyn_arena, db) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc dynamic-model planes");
+    if (cudaMemsetAsync(c->dyn_arena, 0, db, c->stream) != cudaSuccess) return bail(CB_E_CUDA, "memset");
+  }
   if (c->dc.calc_sigma) {
     const size_t sb = sizeof(double) * c->plane * 6;
     if (cudaMalloc(&c->sig_arena, sb) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc sensor planes");
@@ -593,6 +643,7 @@ void cb_destroy(cb_ctx *c) {
   if (c->arena_mixed) cudaFree(c->arena_mixed);
   if (c->ptab4) cudaFree(c->ptab4);
   if (c->sig_arena) cudaFree(c->sig_arena);
+  if (c->dyn_arena) cudaFree(c->dyn_arena);
   for (auto &b : c->ibm) {
     if (b.surf) cudaFree(b.surf);
     if (b.list) cudaFree(b.list);
@@ -627,7 +678,8 @@ int cb_launches_per_step(const cb_ctx *c) {
     if (std::min(c->dc.mx, std::min(c->dc.my, c->dc.mz)) >= 6) ib += 2;  // the snapshots of Q and P near the faces
     ib += c->fully_periodic ? 2 : per_stage - 2 + nper + 1;
   }
-  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0) + ib;
+  const int dyn = (c->cfg.les == 2 && !c->cfg.inviscid) ? 9 : 0;  // the dynamic model's kernels
+  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + dyn + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0) + ib;
 }
 
 static int upload_planes(cb_ctx *c, const double *host, int nc, int pt_first, bool pinned_hint) {
@@ -829,7 +881,7 @@ int cb_calc_ucat(cb_ctx *c) {
 int cb_eddy_viscosity(cb_ctx *c) {
   if (!c) return CB_E_ARG;
   if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set");
-  if (!c->cfg.les) return fail(c, CB_E_ARG, "eddy viscosity needs les = 1");
+  if (!c->cfg.les) return fail(c, CB_E_ARG, "eddy viscosity needs les = 1 or 2");
   int e = nut_update(c);
   if (e) return e;
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -842,6 +894,18 @@ int cb_get_nut(cb_ctx *c, double *nut) {
   pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_NUT), 1, c->staging);
   CB_CUDA(c, cudaGetLastError());
   CB_CUDA(c, cudaMemcpyAsync(nut, c->staging, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_get_cs(cb_ctx *c, double *cs) {
+  if (!c || !cs) return CB_E_ARG;
+  if (!c->dyn_arena) return fail(c, CB_E_STATE, "the coefficient plane exists with les = 2 only");
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_DYN + 12), 1,
+                                                                  c->staging);
+  CB_CUDA(c, cudaGetLastError());
+  CB_CUDA(c, cudaMemcpyAsync(cs, c->staging, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
   return CB_OK;
 }
@@ -1028,6 +1092,8 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
     return fail(c, CB_E_UNSUPPORTED, "the characteristic isothermal IB wall (isothermal 2) is not built");
   if (n > 0 && c->dc.calc_sigma)
     return fail(c, CB_E_UNSUPPORTED, "the shock sensor with immersed bodies is not built");
+  if (n > 0 && c->cfg.les == 2)
+    return fail(c, CB_E_UNSUPPORTED, "the dynamic Smagorinsky model with immersed bodies is not built");
   const int m[3] = {c->cfg.mx, c->cfg.my, c->cfg.mz};
   const bool per[3] = {c->cfg.bctype[0] == 7, c->cfg.bctype[2] == 7, c->cfg.bctype[4] == 7};
   // a node listed twice keeps its last entry

@@ -410,8 +410,9 @@ static __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, 
 }
 
 // Compute_eddy_viscosity_LES (les.c:1523-1567) with constant CS
-// (les.c:135-150): interior nodes only; velocity from the recorded state qu
-// (nullptr: zero velocity before the first CalcUCat).
+// (les.c:135-150) or, with csp, the dynamic model's CS per node: interior
+// nodes only; velocity from the recorded state qu (nullptr: zero velocity
+// before the first CalcUCat) or, with qn, as the dynamic model left lUcat.
 // A block owns an EDDY_BX x EDDY_BY column of interior nodes and marches
 // along k through a chunk of planes; the velocity u = rhoU / rho of three
 // planes (k-1, k, k+1, with a one-node halo in i and j) sits in shared
@@ -420,7 +421,8 @@ static __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, 
 constexpr int EDDY_BX = 32, EDDY_BY = 8, EDDY_PX = EDDY_BX + 2, EDDY_PN = EDDY_PX * (EDDY_BY + 2);
 static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
     eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met, const double *aj,
-                          const double *delta2, const double *nvert, double *nut, int kchunk) {
+                          const double *delta2, const double *nvert, double *nut, int kchunk,
+                          const double *const *qn = nullptr, const double *csp = nullptr) {
   __shared__ double us[3][3][EDDY_PN];  // [slot][component][node]
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * EDDY_BX + tx;
   const int i0 = 1 + blockIdx.x * EDDY_BX, j0 = 1 + blockIdx.y * EDDY_BY;
@@ -433,12 +435,20 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
       const int lx = e % EDDY_PX, ly = e / EDDY_PX;
       const int xi = i0 - 1 + lx, yj = j0 - 1 + ly;
       double u0 = 0., u1 = 0., u2 = 0.;
-      if (qu && xi <= c.mx - 1 && yj <= c.my - 1) {
+      if (xi <= c.mx - 1 && yj <= c.my - 1) {
         const long long n = gidx(c, xi, yj, kk);
-        const double r = ldg(qu[0] + n);
-        u0 = ldg(qu[1] + n) / r;
-        u1 = ldg(qu[2] + n) / r;
-        u2 = ldg(qu[3] + n) / r;
+        // after the dynamic model (qn set) lUcat holds the current state's
+        // velocity at interior nodes with nvert <= 1.1 (les.c:234-238)
+        const double *const *src = qu;
+        if (qn && xi >= 1 && xi <= c.mx - 2 && yj >= 1 && yj <= c.my - 2 && kk >= 1 && kk <= c.mz - 2 &&
+            ldg(nvert + n) <= 1.1)
+          src = qn;
+        if (src) {
+          const double r = ldg(src[0] + n);
+          u0 = ldg(src[1] + n) / r;
+          u1 = ldg(src[2] + n) / r;
+          u2 = ldg(src[3] + n) / r;
+        }
       }
       us[s][0][e] = u0;
       us[s][1][e] = u1;
@@ -478,7 +488,7 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
         const double Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
         const double Sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Sxy * Sxy + Syy * Syy + Syz * Syz +
                                         Sxz * Sxz + Syz * Syz + Szz * Szz));
-        nut[n] = c.cs_const * ldg(delta2 + n) * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
+        nut[n] = (csp ? ldg(csp + n) : c.cs_const) * ldg(delta2 + n) * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
       }
     }
     __syncthreads();  // the slot of plane k-1 is refilled next

@@ -1,0 +1,257 @@
+// Dynamic Smagorinsky model (Compute_Smagorinsky_Constant_1 with -les 2,
+// les.c:151-1472, the default 3-D box test filter with local averaging):
+// Germano's identity with a 3x3x3 test filter, the least-squares ratio
+// LM / MM averaged over 27 nodes, clipping, and a 1/aj-weighted 27-node mean
+// of the coefficient.  Runs once per step before the eddy viscosity, all in
+// FP64 on the ghosted current state.
+//
+// The reference overwrites lUcat in place in its first loop (les.c:234-238):
+// a node's velocity becomes rhoU/rho of the current state once the loop has
+// reached it (interior nodes with nvert <= 1.1), so that loop's central
+// differences see the new value at the i-1, j-1, k-1 neighbours and the value
+// of the last CalcUCat (the state `qu`) at the +1 neighbours; everything
+// after it sees the new value at every such node.  dyn_u reproduces that.
+#pragma once
+#include "cb_common.cuh"
+
+namespace cb {
+
+constexpr double DYN_EPS = 0.000001;  // les.c:8
+
+__device__ __forceinline__ bool dyn_interior(const DevCfg &c, int i, int j, int k) {
+  return i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2;
+}
+
+__device__ __forceinline__ double dyn_u(const DevCfg &c, const double *const *q, const double *const *qu,
+                                        const double *nvert, int a, int i, int j, int k, bool reached) {
+  const long long m = gidx(c, i, j, k);
+  if (reached && dyn_interior(c, i, j, k) && nvert[m] <= 1.1) return q[1 + a][m] / q[0][m];
+  return qu ? qu[1 + a][m] / qu[0][m] : 0.0;
+}
+
+__device__ __forceinline__ void dyn_node(const DevCfg &c, long long t, int &i, int &j, int &k) {
+  const unsigned u = (unsigned)t, px = (unsigned)c.px, py = (unsigned)c.py;
+  const unsigned row = u / px;
+  i = (int)(u - row * px) - 2;
+  j = (int)(row % py) - 2;
+  k = (int)(row / py) - 2;
+}
+
+// (1) velocity gradients (du/dx .. dw/dz) and |S| at interior nodes with
+// nvert <= 1.1 (les.c:234-284); zero on every other node of the padded box.
+static __global__ void dyn_grad_kernel(const DevCfg c, const double *const *q, const double *const *qu,
+                                       const double *const *met, const double *aj, const double *nvert,
+                                       double *const *A, double *Sabs) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < c.plane; t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    dyn_node(c, t, i, j, k);
+    double g[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
+    double sabs = 0.;
+    if (i <= c.mx + 1 && j <= c.my + 1 && dyn_interior(c, i, j, k) && nvert[t] <= 1.1) {
+      double d[3][3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        d[a][0] = (dyn_u(c, q, qu, nvert, a, i + 1, j, k, false) - dyn_u(c, q, qu, nvert, a, i - 1, j, k, true)) * 0.5;
+        d[a][1] = (dyn_u(c, q, qu, nvert, a, i, j + 1, k, false) - dyn_u(c, q, qu, nvert, a, i, j - 1, k, true)) * 0.5;
+        d[a][2] = (dyn_u(c, q, qu, nvert, a, i, j, k + 1, false) - dyn_u(c, q, qu, nvert, a, i, j, k - 1, true)) * 0.5;
+      }
+      const double ajc = aj[t];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int x = 0; x < 3; x++)
+          g[a][x] = (d[a][0] * met[0 * 3 + x][t] + d[a][1] * met[1 * 3 + x][t] + d[a][2] * met[2 * 3 + x][t]) * ajc;
+      const double Sdd = 2. / 3. * (g[0][0] + g[1][1] + g[2][2]);
+      const double Sxx = 0.5 * (g[0][0] + g[0][0]) - Sdd, Sxy = 0.5 * (g[0][1] + g[1][0]), Sxz = 0.5 * (g[0][2] + g[2][0]);
+      const double Syy = 0.5 * (g[1][1] + g[1][1]) - Sdd, Syz = 0.5 * (g[1][2] + g[2][1]);
+      const double Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
+      sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Sxy * Sxy + Syy * Syy + Syz * Syz + Sxz * Sxz + Syz * Syz +
+                         Szz * Szz));
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int x = 0; x < 3; x++) A[3 * a + x][t] = g[a][x];
+    Sabs[t] = sabs;
+  }
+}
+
+// Boundary nodes of the periodic directions from two nodes across, over the
+// interior ranges of the other two directions (les.c:287-353, 1217-1271);
+// the three faces' node sets are disjoint.
+static __global__ void dyn_copy_kernel(const DevCfg c, double *const *f, int nplanes) {
+  const long long ni = (long long)(c.my - 2) * (c.mz - 2), nj = (long long)(c.mx - 2) * (c.mz - 2),
+                  nk = (long long)(c.mx - 2) * (c.my - 2);
+  const long long total = ni + nj + nk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int dir;
+    long long r = t;
+    int a, b;
+    if (r < ni) { dir = 0; a = 1 + (int)(r % (c.my - 2)); b = 1 + (int)(r / (c.my - 2)); }
+    else if ((r -= ni) < nj) { dir = 1; a = 1 + (int)(r % (c.mx - 2)); b = 1 + (int)(r / (c.mx - 2)); }
+    else { r -= nj; dir = 2; a = 1 + (int)(r % (c.mx - 2)); b = 1 + (int)(r / (c.mx - 2)); }
+    if (c.bctype[2 * dir] != 7 && c.bctype[2 * dir + 1] != 7) continue;
+    long long lo, hi;
+    if (dir == 0) { lo = gidx(c, 0, a, b); hi = gidx(c, c.mx - 1, a, b); }
+    else if (dir == 1) { lo = gidx(c, a, 0, b); hi = gidx(c, a, c.my - 1, b); }
+    else { lo = gidx(c, a, b, 0); hi = gidx(c, a, b, c.mz - 1); }
+    const long long s = gstride(c, dir);
+    for (int p = 0; p < nplanes; p++) {
+      f[p][lo] = f[p][lo - 2 * s];
+      f[p][hi] = f[p][hi + 2 * s];
+    }
+  }
+}
+
+// (2) LM and MM of Germano's identity at interior nodes with nvert <= 1.1
+// (les.c:442-792): the test-filtered products of the 27 nodes around, with
+// weights 1/(|r|+1)/(|q|+1)/(|p|+1), accumulated in the reference's k, j, i
+// order; zero on every other node.  The pressure-velocity terms (beta) feed
+// nothing downstream and are not formed.
+static __global__ void dyn_lm_kernel(const DevCfg c, const double *const *q, const double *const *qu,
+                                     const double *aj, const double *nvert, const double *const *A,
+                                     const double *Sabs, double *LM, double *MM) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < c.plane; t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    dyn_node(c, t, i, j, k);
+    double lm = 0., mm = 0.;
+    if (i <= c.mx + 1 && j <= c.my + 1 && dyn_interior(c, i, j, k) && nvert[t] <= 1.1) {
+      // filtered: rho, rhou, rhov, rhow, rhouu, rhouv, rhouw, rhovv, rhovw, rhoww,
+      // S11 S12 S13 S22 S23 S33, and |S| rho S of the same six
+      double f[22];
+#pragma unroll
+      for (int x = 0; x < 22; x++) f[x] = 0.;
+      double ws = 0.;
+      double Sc[6] = {0., 0., 0., 0., 0., 0.};
+      for (int R = 0; R < 3; R++)
+        for (int Q = 0; Q < 3; Q++)
+          for (int P = 0; P < 3; P++) {
+            const int II = i + P - 1, JJ = j + Q - 1, KK = k + R - 1;
+            const long long m = gidx(c, II, JJ, KK);
+            const double w = 1. / (fabs(R - 1.0) + 1) * 1. / (fabs(Q - 1.0) + 1) * 1. / (fabs(P - 1.0) + 1);
+            const double u = dyn_u(c, q, qu, nvert, 0, II, JJ, KK, true);
+            const double v = dyn_u(c, q, qu, nvert, 1, II, JJ, KK, true);
+            const double ww = dyn_u(c, q, qu, nvert, 2, II, JJ, KK, true);
+            const double rho = q[0][m], ru = q[1][m], rv = q[2][m], rw = q[3][m];
+            const double S6[6] = {0.5 * (A[0][m] + A[0][m]), 0.5 * (A[1][m] + A[3][m]), 0.5 * (A[2][m] + A[6][m]),
+                                  0.5 * (A[4][m] + A[4][m]), 0.5 * (A[5][m] + A[7][m]), 0.5 * (A[8][m] + A[8][m])};
+            const double sm = Sabs[m];
+            const double val[10] = {rho, ru, rv, rw, ru * u, ru * v, ru * ww, rv * v, rv * ww, rw * ww};
+#pragma unroll
+            for (int x = 0; x < 10; x++) f[x] += w * val[x];
+#pragma unroll
+            for (int x = 0; x < 6; x++) {
+              f[10 + x] += w * S6[x];
+              f[16 + x] += w * (S6[x] * sm * rho);
+            }
+            ws += w;
+            if (R == 1 && Q == 1 && P == 1) {
+#pragma unroll
+              for (int x = 0; x < 6; x++) Sc[x] = S6[x];
+            }
+          }
+      const double _rho = f[0] / ws, _rhou = f[1] / ws, _rhov = f[2] / ws, _rhow = f[3] / ws;
+      // symmetric 3x3 from the six distinct entries: (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+      const int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+      double Lij[3][3], Sh[3][3], SSh[3][3], Sx[3][3];
+      const double fr[3] = {_rhou, _rhov, _rhow};
+      const int prod[3][3] = {{4, 5, 6}, {5, 7, 8}, {6, 8, 9}};
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          Lij[a][b] = f[prod[a][b]] / ws - fr[a] * fr[b] / _rho;
+          Sh[a][b] = f[10 + sym[a][b]] / ws;
+          SSh[a][b] = f[16 + sym[a][b]] / ws;
+          Sx[a][b] = Sc[sym[a][b]];
+        }
+      double S_hat = 0;
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) S_hat += pow(Sh[a][b], 2.);
+      S_hat = sqrt(2 * S_hat);
+      const double filter = pow(1. / aj[t], 1. / 3.);
+      const double test_filter = 2.0 * filter;
+      double L_cat = 0.0, M_cat = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          M_cat += -2.0 * _rho * pow(test_filter, 2.) * S_hat * (Sh[a][b] * Sx[a][b] - 0.33 * Sh[a][a] * Sx[b][b]) +
+                   2.0 * pow(filter, 2.) * (SSh[a][b] * Sx[a][b] - 0.33 * SSh[a][a] * Sx[b][b]);
+          L_cat += Lij[a][b] * Sx[a][b] - 0.33 * Sx[a][a] * Lij[b][b];
+        }
+      lm = L_cat;
+      mm = M_cat;
+    }
+    LM[t] = lm;
+    MM[t] = mm;
+  }
+}
+
+// (3) Cs from the 27-node means of LM and MM at interior nodes
+// (les.c:905-925), then the clipping of every owned node (les.c:1124-1137,
+// whose face tests compare !bctype with 7 and never hold); boundary nodes keep
+// their previous value through it.
+static __global__ void dyn_cs_kernel(const DevCfg c, const double *nvert, const double *LM, const double *MM,
+                                     double *cs, double max_cs) {
+  const long long total = (long long)c.mx * c.my * c.mz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const unsigned u = (unsigned)t;
+    const int i = (int)(u % (unsigned)c.mx), j = (int)((u / (unsigned)c.mx) % (unsigned)c.my),
+              k = (int)(u / ((unsigned)c.mx * (unsigned)c.my));
+    const long long n = gidx(c, i, j, k);
+    const double nv = nvert[n];
+    double v = cs[n];
+    if (dyn_interior(c, i, j, k)) {
+      if (nv > 1.1) {
+        v = 0;
+      } else {
+        double lm = 0.0, mm = 0.0;
+        for (int R = 0; R < 3; R++)
+          for (int Q = 0; Q < 3; Q++)
+            for (int P = 0; P < 3; P++) {
+              const long long m = gidx(c, i + P - 1, j + Q - 1, k + R - 1);
+              lm += LM[m] / 27.0;
+              mm += MM[m] / 27.0;
+            }
+        const double C = lm / (mm + DYN_EPS);
+        v = (C < 0.0001) ? 0.0001 : C;
+      }
+    }
+    if (nv > 1.1 && nv < 7.) {
+      v = 0.0;
+    } else {
+      if (nv > 0.1 && nv < 1.1) v = (0.01 < v) ? v : 0.01;
+      const double tt = (v < 0.000) ? 0.000 : v;
+      v = (tt < max_cs) ? tt : max_cs;
+    }
+    cs[n] = v;
+  }
+}
+
+// (4) the 1/aj-weighted mean of lCS (ct) over the 27 nodes around interior
+// nodes with nvert < 0.1 (les.c:1302-1333).
+static __global__ void dyn_avg_kernel(const DevCfg c, const double *aj, const double *nvert, const double *ct,
+                                      double *cs) {
+  const long long total = (long long)(c.mx - 2) * (c.my - 2) * (c.mz - 2);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const unsigned u = (unsigned)t, nx = (unsigned)(c.mx - 2), ny = (unsigned)(c.my - 2);
+    const int i = 1 + (int)(u % nx), j = 1 + (int)((u / nx) % ny), k = 1 + (int)(u / (nx * ny));
+    const long long n = gidx(c, i, j, k);
+    if (!(nvert[n] < 0.1)) continue;
+    double vs = 0.0, ws = 0.0;
+    for (int R = 0; R < 3; R++)
+      for (int Q = 0; Q < 3; Q++)
+        for (int P = 0; P < 3; P++) {
+          const long long m = gidx(c, i + P - 1, j + Q - 1, k + R - 1);
+          const double w = 1. / aj[m];
+          vs += w * ct[m];
+          ws += w;
+        }
+    cs[n] = vs / ws;
+  }
+}
+
+}  // namespace cb

@@ -40,7 +40,7 @@ _OPT_MAP = {
     "-s_x": ("s_x", float), "-s_y": ("s_y", float), "-s_z": ("s_z", float), "-ren": ("ren", float),
     "-Ma": ("ma", float), "-Pr": ("pr", float), "-gamma": ("gamma", float), "-dt": ("dt", float),
     "-calc_sigma": ("calc_sigma", int), "-s_x_min": ("s_x_min", float), "-s_y_min": ("s_y_min", float),
-    "-s_z_min": ("s_z_min", float), "-sigma_thrsh": ("sigma_thrsh", float),
+    "-s_z_min": ("s_z_min", float), "-sigma_thrsh": ("sigma_thrsh", float), "-max_cs": ("max_cs", float),
 }
 
 
@@ -61,7 +61,7 @@ class Block:
                  dt: float = 0.01, st: float = 1.0, cs_const: float = 0.03, ci: float = 0.06,
                  ratio: float = 0.0, precision: str = "fp64", device: int = 0, calc_sigma: int = 0,
                  s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5,
-                 flux: str = "rusanov"):
+                 flux: str = "rusanov", max_cs: float = 0.05):
         self.lib = _lib.load()
         cfg = CbConfig()
         self.lib.cb_config_default(C.byref(cfg), mx, my, mz)
@@ -69,7 +69,8 @@ class Block:
         for k, v in dict(les=les, inviscid=inviscid, fluxorder=fluxorder, eno_order=eno_order, central=central,
                          isothermal=isothermal, s_x=s_x, s_y=s_y, s_z=s_z, ren=ren, ma=ma, pr=pr, gamma=gamma,
                          dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device, calc_sigma=calc_sigma,
-                         s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh).items():
+                         s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh,
+                         max_cs=max_cs).items():
             setattr(cfg, k, v)
         cfg.flux = {"rusanov": 0, "roe": 1}[flux] if isinstance(flux, str) else int(flux)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]
@@ -213,6 +214,12 @@ class Block:
 
     def Compute_eddy_viscosity_LES(self):
         self._check(self.lib.cb_eddy_viscosity(self._ctx))
+
+    def CS(self) -> np.ndarray:
+        """The dynamic Smagorinsky coefficient user->CS (-les 2)."""
+        out = np.empty(self.shape)
+        self._check(self.lib.cb_get_cs(self._ctx, dptr(out)))
+        return out
 
     def nu_t(self) -> np.ndarray:
         out = np.empty(self.shape)

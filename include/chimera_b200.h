@@ -52,7 +52,8 @@ extern "C" {
 typedef struct {
   int mx, my, mz;       /* -im/-jm/-km (DMDA node counts) */
   int bctype[6];        /* bcs.dat: i-lo,i-hi,j-lo,j-hi,k-lo,k-hi; 7 = periodic */
-  int les;              /* -les     : 0 off, 1 constant Smagorinsky */
+  int les;              /* -les     : 0 off, 1 constant Smagorinsky, 2 dynamic Smagorinsky (single-block
+                           contexts; Compute_Smagorinsky_Constant_1, les.c:151-1472) */
   int inviscid;         /* -inv     : 1 skips formViscous */
   int fluxorder;        /* -fluxorder: 1 first order, 2 MUSCL-minmod, 3 WENO3; also the RK stage count */
   int eno_order;        /* -ENOorder: 2 or 3 */
@@ -75,6 +76,8 @@ typedef struct {
   double sigma_thrsh;   /* -sigma_thrsh: ks of the smoothness ratio (rhs.c:3323, default 1e-5) */
   int flux;             /* upwind flux: 0 Rusanov (the reference's, default), 1 Roe with Harten's
                            entropy fix (no counterpart in the reference) */
+  double max_cs;        /* -max_cs: upper clip of the dynamic Smagorinsky coefficient (-les 2;
+                           les.c:151, default 0.05) */
 } cb_config;
 
 /* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */
@@ -122,11 +125,16 @@ int cb_rhs(cb_ctx *ctx, int istage, double *rhs);
 int cb_calc_ucat(cb_ctx *ctx);
 
 /* Compute_Smagorinsky_Constant_1 + Compute_eddy_viscosity_LES
- * (les.c:135-150, 1477-1661) from the recorded velocity field. */
+ * (les.c:135-1472, 1477-1661) from the recorded velocity field and, with
+ * -les 2, the dynamic model on the current state. */
 int cb_eddy_viscosity(cb_ctx *ctx);
 
 /* Eddy viscosity Nu_t (1 double per node, global order). */
 int cb_get_nut(cb_ctx *ctx, double *nut);
+
+/* The dynamic model's coefficient user->CS (1 double per node, global order;
+ * -les 2 only). */
+int cb_get_cs(cb_ctx *ctx, double *cs);
 
 /* nsteps physical time steps: per step Flow_Solver (solvers.c:13-64: LES
  * eddy viscosity, then RungeKutta solvers.c:223-294 with FormBCS and

@@ -67,6 +67,7 @@ class Config:
     s_z_min: float = 0.0
     sigma_thrsh: float = 1e-5
     flux: int = 0  # 0 Rusanov (the reference's), 1 Roe (no reference counterpart)
+    max_cs: float = 0.05  # -max_cs: clip of the dynamic Smagorinsky coefficient (les.c:151)
     immersed: int = 0      # -imm: run the IB interpolation after the stages (solvers.c:282-288)
     wallfunction: int = 0  # -wallfunction: 0 noslip, 3 freeslip at IB nodes
     twoD: int = 0          # -twoD: 1/2/3 drops x/y/z from the IB normal and velocity
@@ -80,7 +81,7 @@ class Config:
             ("-ren", repr(float(self.ren))), ("-Ma", repr(float(self.ma))),
             ("-Pr", repr(float(self.pr))), ("-gamma", repr(float(self.gamma))),
             ("-dt", repr(float(self.dt))), ("-visT", 0), ("-twoD", self.twoD), ("-TwoD", 0),
-            ("-imm", self.immersed), ("-wallfunction", self.wallfunction),
+            ("-imm", self.immersed), ("-wallfunction", self.wallfunction), ("-max_cs", repr(float(self.max_cs))),
             ("-calc_sigma", self.calc_sigma), ("-s_x_min", repr(float(self.s_x_min))),
             ("-s_y_min", repr(float(self.s_y_min))), ("-s_z_min", repr(float(self.s_z_min))),
             ("-sigma_thrsh", repr(float(self.sigma_thrsh))),
@@ -106,7 +107,7 @@ class _CCfg(C.Structure):
         ("dt", C.c_double), ("st", C.c_double), ("cs_const", C.c_double), ("ci", C.c_double),
         ("ratio", C.c_double), ("calc_sigma", C.c_int),
         ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double), ("sigma_thrsh", C.c_double),
-        ("flux", C.c_int),
+        ("flux", C.c_int), ("max_cs", C.c_double),
     ]
 
 
@@ -197,6 +198,9 @@ class Oracle:
                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, PP, D, C.POINTER(C.c_int),
                                     C.c_int, C.c_int]
         L.cbo_steps_ibm.restype = C.c_int
+        L.cbo_dynamic_smagorinsky.argtypes = [C.c_void_p, PP, PP, D, PP, PP, PP, D, D, D]
+        L.cbo_dynamic_smagorinsky.restype = C.c_int
+        L.cbo_eddy_viscosity_dyn.argtypes = [C.c_void_p, PP, PP, PP, PP, PP, D, D, D, D]
         self._cp = C.byref(self.c)
 
     def zeros(self, nc: int) -> np.ndarray:
@@ -264,6 +268,27 @@ class Oracle:
     def initial_state(self, q_nat: np.ndarray) -> dict:
         q = self.fill_ghosts(to_padded(self.cfg, q_nat))
         return {"q": q, "qold": q.copy(), "quc": np.zeros_like(q), "have_uc": 0, "nut": self.zeros(1)}
+
+    def dynamic_smagorinsky(self, q: np.ndarray, quc: Optional[np.ndarray], met, nvert: np.ndarray,
+                            cs: Optional[np.ndarray] = None, lp: Optional[np.ndarray] = None) -> np.ndarray:
+        """Compute_Smagorinsky_Constant_1 with -les 2: Cs (padded 1) from the
+        ghosted state q and the last CalcUCat state quc (None: zero velocity);
+        lp defaults to the EqOfState of q."""
+        cs = self.zeros(1) if cs is None else cs
+        lp = self.eos(q) if lp is None else lp
+        e = self.lib.cbo_dynamic_smagorinsky(self._cp, _ptrs(list(q)), _ptrs(list(quc)) if quc is not None else None,
+                                             _dp(lp[0]), _ptrs(list(met["csi"])), _ptrs(list(met["eta"])),
+                                             _ptrs(list(met["zet"])), _dp(met["aj"][0]), _dp(nvert[0]), _dp(cs[0]))
+        if e:
+            raise RuntimeError(f"cbo_dynamic_smagorinsky failed with status {e}")
+        return cs
+
+    def eddy_viscosity_dyn(self, q: np.ndarray, quc: Optional[np.ndarray], met, nvert: np.ndarray, cs: np.ndarray,
+                           nut: np.ndarray) -> np.ndarray:
+        self.lib.cbo_eddy_viscosity_dyn(self._cp, _ptrs(list(q)), _ptrs(list(quc)) if quc is not None else None,
+                                        _ptrs(list(met["csi"])), _ptrs(list(met["eta"])), _ptrs(list(met["zet"])),
+                                        _dp(met["aj"][0]), _dp(nvert[0]), _dp(cs[0]), _dp(nut[0]))
+        return nut
 
     def formbcs(self, alfa: float, lq: np.ndarray, qold: np.ndarray, met, q: np.ndarray) -> np.ndarray:
         """FormBCS(user, alfa) on q (padded 5, in/out) from the ghosted lq."""
@@ -453,6 +478,11 @@ class RefOracle:
     def nut(self) -> np.ndarray:
         out = np.zeros(self.nnodes)
         self.lib.ref_get_nut(_dp(out))
+        return out.reshape(self.cfg.mz, self.cfg.my, self.cfg.mx)
+
+    def cs(self) -> np.ndarray:
+        out = np.zeros(self.nnodes)
+        self.lib.ref_get_cs(_dp(out))
         return out.reshape(self.cfg.mz, self.cfg.my, self.cfg.mx)
 
     def local(self, which: str, nc: int) -> np.ndarray:

@@ -393,7 +393,13 @@ PetscErrorCode DMDAVecGetArray(DM dm, Vec v, void *array) {
   return 0;
 }
 
-PetscErrorCode DMDAVecRestoreArray(DM dm, Vec v, void *array) { (void)dm; (void)v; if (array) *(void **)array = NULL; return 0; }
+/* PETSc 3.12's DMDAVecRestoreArray (VecRestoreArray3d) frees the row-pointer
+ * table but leaves the caller's pointer as it was; les.c:417-419 reads csi,
+ * eta and zet after restoring them (les.c:400-402) and works only because the
+ * freed table still holds valid rows.  The shim keeps its table alive with the
+ * Vec, so leaving the pointer as it was reproduces that behaviour without a
+ * use after free. */
+PetscErrorCode DMDAVecRestoreArray(DM dm, Vec v, void *array) { (void)dm; (void)v; (void)array; return 0; }
 
 static inline PetscInt wrap(PetscInt i, PetscInt M) { i %= M; return i < 0 ? i + M : i; }
 

@@ -341,6 +341,7 @@ int ref_get_P(double *out) { return U ? copy_out(U->P, out) : 1; }
 int ref_get_lQ(double *out) { return U ? copy_out(U->lQ, out) : 1; }
 int ref_get_lP(double *out) { return U ? copy_out(U->lP, out) : 1; }
 int ref_get_nut(double *out) { return U ? copy_out(U->Nu_t, out) : 1; }
+int ref_get_cs(double *out) { return U && U->CS ? copy_out(U->CS, out) : 1; }
 int ref_get_lnut(double *out) { return U ? copy_out(U->lNu_t, out) : 1; }
 int ref_get_lsigma(double *out) { return U ? copy_out(U->lSigma, out) : 1; }
 int ref_get_lucat(double *out) { return U ? copy_out(U->lUcat, out) : 1; }

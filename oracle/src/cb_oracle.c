@@ -1204,14 +1204,19 @@ int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const
               const double *nvert) {
   geom G = mkgeom(c);
   int ns = cbo_nstages(c);
-  double *buf = (double *)calloc(G.n * 13, sizeof(double));
-  double *rhs[5], *qn[5], *sig[3];
+  double *buf = (double *)calloc(G.n * 15, sizeof(double));
+  double *rhs[5], *qn[5], *sig[3], *pbuf = buf + G.n * 13, *csbuf = buf + G.n * 14;
   for (int a = 0; a < 5; a++) { rhs[a] = buf + G.n * a; qn[a] = buf + G.n * (5 + a); }
   for (int a = 0; a < 3; a++) sig[a] = buf + G.n * (10 + a);
   if (c->les && !c->calc_sigma) cbo_sigma(c, sig);
   int err = 0;
   for (int step = 0; step < nsteps && !err; step++) {
-    if (c->les && !c->inviscid)
+    if (c->les == 2 && !c->inviscid) { /* Compute_Smagorinsky_Constant_1 -les 2, then the eddy viscosity */
+      const double *const *qu = *have_uc ? (const double *const *)quc : NULL;
+      cbo_eos(c, (const double *const *)q, pbuf);
+      cbo_dynamic_smagorinsky(c, (const double *const *)q, qu, pbuf, csi, eta, zet, aj, nvert, csbuf);
+      cbo_eddy_viscosity_dyn(c, (const double *const *)q, qu, csi, eta, zet, aj, nvert, csbuf, nut);
+    } else if (c->les && !c->inviscid)
       cbo_eddy_viscosity(c, *have_uc ? (const double *const *)quc : NULL, csi, eta, zet, aj, nvert, nut);
     for (int s = 0; s < ns && !err; s++) {
       if (c->les && c->calc_sigma && s == 0) cbo_sigma_sensor(c, (const double *const *)q, sig); /* istage 0 */
@@ -1336,6 +1341,7 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
                   const cbo_ibm_info *const *lists, const double *const coor[3], double *lp, int *lp_valid,
                   int twoD, int wallfunction) {
   if (c->calc_sigma) return 5; /* the sensor with a carried pressure is not restated */
+  if (c->les == 2) return 5;   /* nor the dynamic model's reading of it */
   geom G = mkgeom(c);
   int ns = cbo_nstages(c);
   double *buf = (double *)calloc(G.n * 19, sizeof(double));
@@ -1375,4 +1381,271 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
   }
   free(buf);
   return err;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dynamic Smagorinsky  (Compute_Smagorinsky_Constant_1 with -les 2,          */
+/* les.c:135-1472: the default 3-D box test filter, local averaging)          */
+/* ------------------------------------------------------------------------ */
+#define DYN_EPS 0.000001 /* les.c:8 */
+
+static int interior(const geom *G, int i, int j, int k) {
+  return i >= 1 && i <= G->m[0] - 2 && j >= 1 && j <= G->m[1] - 2 && k >= 1 && k <= G->m[2] - 2;
+}
+
+/* integrate_testfilter (les.c:80-132): sum w*val and w in k, j, i order */
+static double itf(const double val[27], const double w[27]) {
+  double vs = 0.0, ws = 0.0;
+  for (int t = 0; t < 27; t++) { vs += w[t] * val[t]; ws += w[t]; }
+  return vs / ws;
+}
+
+/* boundary copies from two nodes across of the periodic directions over the
+ * interior ranges of the other two (les.c:287-353, 1217-1271) */
+static void dyn_periodic_copies(const cbo_config *c, const geom *G, double *f) {
+  const int mx = G->m[0], my = G->m[1], mz = G->m[2];
+  const int *bc = c->bctype;
+  if (bc[0] == 7 || bc[1] == 7)
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++) {
+        f[IX(G, 0, j, k)] = f[IX(G, -2, j, k)];
+        f[IX(G, mx - 1, j, k)] = f[IX(G, mx + 1, j, k)];
+      }
+  if (bc[2] == 7 || bc[3] == 7)
+    for (int k = 1; k < mz - 1; k++)
+      for (int i = 1; i < mx - 1; i++) {
+        f[IX(G, i, 0, k)] = f[IX(G, i, -2, k)];
+        f[IX(G, i, my - 1, k)] = f[IX(G, i, my + 1, k)];
+      }
+  if (bc[4] == 7 || bc[5] == 7)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        f[IX(G, i, j, 0)] = f[IX(G, i, j, -2)];
+        f[IX(G, i, j, mz - 1)] = f[IX(G, i, j, mz + 1)];
+      }
+}
+
+/* Velocity component a the reference's lUcat holds at node m once the first
+ * loop of the dynamic model has overwritten it in place: rhoU/rho of the
+ * current state q at interior nodes with nvert <= 1.1 (a node the loop has
+ * reached, when `reached` restricts it), else the value CalcUCat left from
+ * quc (zero before any CalcUCat). */
+static double dyn_u(const geom *G, const double *const q[5], const double *const quc[5], const double *nvert, int a,
+                    int i, int j, int k, int reached) {
+  const ptrdiff_t m = IX(G, i, j, k);
+  if (reached && interior(G, i, j, k) && nvert[m] <= 1.1) return q[1 + a][m] / q[0][m];
+  return quc ? quc[1 + a][m] / quc[0][m] : 0.0;
+}
+
+int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const double *const quc[5],
+                            const double *lp, const double *const csi[3], const double *const eta[3],
+                            const double *const zet[3], const double *aj, const double *nvert, double *cs) {
+  const double max_cs = c->max_cs;
+  geom G = mkgeom(c);
+  const int mx = G.m[0], my = G.m[1], mz = G.m[2];
+  if (c->les != 2) return 5;
+  double *buf = (double *)calloc(G.n * 13, sizeof(double));
+  double *A[9], *Sabs = buf + 9 * G.n, *LM = buf + 10 * G.n, *MM = buf + 11 * G.n, *ct = buf + 12 * G.n;
+  for (int a = 0; a < 9; a++) A[a] = buf + a * G.n; /* du_dx du_dy du_dz dv_dx .. dw_dz */
+  /* (1) velocity gradients and |S| at interior nodes (les.c:234-284), the
+   * velocity overwritten in loop order: the -1 neighbours are already new */
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        const ptrdiff_t n = IX(&G, i, j, k);
+        if (nvert[n] > 1.1) continue;
+        double d[3][3];
+        for (int a = 0; a < 3; a++) {
+          d[a][0] = (dyn_u(&G, q, quc, nvert, a, i + 1, j, k, 0) - dyn_u(&G, q, quc, nvert, a, i - 1, j, k, 1)) * 0.5;
+          d[a][2] = (dyn_u(&G, q, quc, nvert, a, i, j, k + 1, 0) - dyn_u(&G, q, quc, nvert, a, i, j, k - 1, 1)) * 0.5;
+          d[a][1] = (dyn_u(&G, q, quc, nvert, a, i, j + 1, k, 0) - dyn_u(&G, q, quc, nvert, a, i, j - 1, k, 1)) * 0.5;
+        }
+        const double ajc = aj[n];
+        const double c0 = csi[0][n], c1 = csi[1][n], c2 = csi[2][n];
+        const double e0 = eta[0][n], e1 = eta[1][n], e2 = eta[2][n];
+        const double z0 = zet[0][n], z1 = zet[1][n], z2 = zet[2][n];
+        double g[3][3];
+        for (int a = 0; a < 3; a++) {
+          g[a][0] = (d[a][0] * c0 + d[a][1] * e0 + d[a][2] * z0) * ajc;
+          g[a][1] = (d[a][0] * c1 + d[a][1] * e1 + d[a][2] * z1) * ajc;
+          g[a][2] = (d[a][0] * c2 + d[a][1] * e2 + d[a][2] * z2) * ajc;
+        }
+        const double Sdd = 2. / 3. * (g[0][0] + g[1][1] + g[2][2]);
+        const double Sxx = 0.5 * (g[0][0] + g[0][0]) - Sdd, Sxy = 0.5 * (g[0][1] + g[1][0]), Sxz = 0.5 * (g[0][2] + g[2][0]);
+        const double Syx = Sxy, Syy = 0.5 * (g[1][1] + g[1][1]) - Sdd, Syz = 0.5 * (g[1][2] + g[2][1]);
+        const double Szx = Sxz, Szy = Syz, Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
+        Sabs[n] = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Syx * Syx + Syy * Syy + Syz * Syz + Szx * Szx +
+                              Szy * Szy + Szz * Szz));
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++) A[3 * a + b][n] = g[a][b];
+      }
+  /* DMLocalToLocal of the gradients and |S|, then the gradients' periodic copies */
+  for (int a = 0; a < 9; a++) cbo_fill_ghosts(c, A[a]);
+  cbo_fill_ghosts(c, Sabs);
+  for (int a = 0; a < 9; a++) dyn_periodic_copies(c, &G, A[a]);
+  /* (2) Germano identity with the 3x3x3 box test filter (les.c:442-792) */
+  double w[27];
+  for (int R = 0; R < 3; R++)
+    for (int Q = 0; Q < 3; Q++)
+      for (int P = 0; P < 3; P++)
+        w[(R * 3 + Q) * 3 + P] = 1. / (fabs(R - 1.0) + 1) * 1. / (fabs(Q - 1.0) + 1) * 1. / (fabs(P - 1.0) + 1);
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        const ptrdiff_t n = IX(&G, i, j, k);
+        if (nvert[n] > 1.1) { LM[n] = MM[n] = 0; continue; }
+        double u[27], v[27], ww[27], rho[27], ru[27], rv[27], rw[27], ruu[27], ruv[27], ruw[27], rvv[27], rvw[27],
+            rww[27], S[9][27], SS[9][27], pu[27], pv[27], pw[27], pp[27];
+        for (int R = 0; R < 3; R++)
+          for (int Q = 0; Q < 3; Q++)
+            for (int P = 0; P < 3; P++) {
+              const int t = (R * 3 + Q) * 3 + P;
+              const int II = i + P - 1, JJ = j + Q - 1, KK = k + R - 1;
+              const ptrdiff_t m = IX(&G, II, JJ, KK);
+              u[t] = dyn_u(&G, q, quc, nvert, 0, II, JJ, KK, 1);
+              v[t] = dyn_u(&G, q, quc, nvert, 1, II, JJ, KK, 1);
+              ww[t] = dyn_u(&G, q, quc, nvert, 2, II, JJ, KK, 1);
+              ru[t] = q[1][m]; rv[t] = q[2][m]; rw[t] = q[3][m]; rho[t] = q[0][m];
+              ruu[t] = ru[t] * u[t]; ruv[t] = ru[t] * v[t]; ruw[t] = ru[t] * ww[t];
+              rvv[t] = rv[t] * v[t]; rvw[t] = rv[t] * ww[t]; rww[t] = rw[t] * ww[t];
+              const double du_dx = A[0][m], du_dy = A[1][m], du_dz = A[2][m];
+              const double dv_dx = A[3][m], dv_dy = A[4][m], dv_dz = A[5][m];
+              const double dw_dx = A[6][m], dw_dy = A[7][m], dw_dz = A[8][m];
+              const double Sxx = 0.5 * (du_dx + du_dx), Sxy = 0.5 * (du_dy + dv_dx), Sxz = 0.5 * (du_dz + dw_dx);
+              const double Syy = 0.5 * (dv_dy + dv_dy), Syz = 0.5 * (dv_dz + dw_dy);
+              const double Szz = 0.5 * (dw_dz + dw_dz);
+              const double s9[9] = {Sxx, Sxy, Sxz, Sxy, Syy, Syz, Sxz, Syz, Szz};
+              for (int a = 0; a < 9; a++) {
+                S[a][t] = s9[a];
+                SS[a][t] = s9[a] * Sabs[m] * rho[t];
+              }
+              pu[t] = u[t] * lp[m]; pv[t] = v[t] * lp[m]; pw[t] = ww[t] * lp[m]; pp[t] = lp[m];
+            }
+        (void)pu; (void)pv; (void)pw; (void)pp; /* beta (les.c:578-581) feeds nothing downstream */
+        const double filter = pow(1. / aj[n], 1. / 3.);
+        const double test_filter = 2.0 * filter;
+        const double _rho = itf(rho, w), _rhou = itf(ru, w), _rhov = itf(rv, w), _rhow = itf(rw, w);
+        double Lij[3][3];
+        Lij[0][0] = itf(ruu, w) - _rhou * _rhou / _rho;
+        Lij[0][1] = itf(ruv, w) - _rhou * _rhov / _rho;
+        Lij[0][2] = itf(ruw, w) - _rhou * _rhow / _rho;
+        Lij[1][0] = itf(ruv, w) - _rhov * _rhou / _rho;
+        Lij[1][1] = itf(rvv, w) - _rhov * _rhov / _rho;
+        Lij[1][2] = itf(rvw, w) - _rhov * _rhow / _rho;
+        Lij[2][0] = itf(ruw, w) - _rhow * _rhou / _rho;
+        Lij[2][1] = itf(rvw, w) - _rhow * _rhov / _rho;
+        Lij[2][2] = itf(rww, w) - _rhow * _rhow / _rho;
+        double Sxyz[3][3], Sh[3][3], SSh[3][3];
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++) {
+            Sxyz[a][b] = S[3 * a + b][13];
+            Sh[a][b] = itf(S[3 * a + b], w);
+            SSh[a][b] = itf(SS[3 * a + b], w);
+          }
+        double S_hat = 0;
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++) S_hat += pow(Sh[a][b], 2.);
+        S_hat = sqrt(2 * S_hat);
+        double L_cat = 0.0, M_cat = 0.0;
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++) {
+            M_cat += -2.0 * _rho * pow(test_filter, 2.) * S_hat * (Sh[a][b] * Sxyz[a][b] - 0.33 * Sh[a][a] * Sxyz[b][b]) +
+                     2.0 * pow(filter, 2.) * (SSh[a][b] * Sxyz[a][b] - 0.33 * SSh[a][a] * Sxyz[b][b]);
+            L_cat += Lij[a][b] * Sxyz[a][b] - 0.33 * Sxyz[a][a] * Lij[b][b];
+          }
+        LM[n] = L_cat;
+        MM[n] = M_cat;
+      }
+  cbo_fill_ghosts(c, LM);
+  cbo_fill_ghosts(c, MM);
+  /* (3) Cs from the 27-node mean of LM and MM (les.c:905-925) */
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        const ptrdiff_t n = IX(&G, i, j, k);
+        if (nvert[n] > 1.1) { cs[n] = 0; continue; }
+        double lm = 0.0, mm = 0.0; /* integrate_t (les.c:66-78) */
+        for (int R = 0; R < 3; R++)
+          for (int Q = 0; Q < 3; Q++)
+            for (int P = 0; P < 3; P++) {
+              const ptrdiff_t m = IX(&G, i + P - 1, j + Q - 1, k + R - 1);
+              lm += LM[m] / 27.0;
+              mm += MM[m] / 27.0;
+            }
+        const double C = lm / (mm + DYN_EPS);
+        cs[n] = (C < 0.0001) ? 0.0001 : C;
+      }
+  /* (4) clipping on every owned node (les.c:1124-1137; its face tests compare
+   * !bctype with 7 and never hold) */
+  for (int k = 0; k < mz; k++)
+    for (int j = 0; j < my; j++)
+      for (int i = 0; i < mx; i++) {
+        const ptrdiff_t n = IX(&G, i, j, k);
+        if (nvert[n] > 1.1 && nvert[n] < 7.) { cs[n] = 0.0; continue; }
+        if (nvert[n] > 0.1 && nvert[n] < 1.1) cs[n] = (0.01 < cs[n]) ? cs[n] : 0.01; /* PetscMax(0.01, Cs) */
+        const double t = (cs[n] < 0.000) ? 0.000 : cs[n];
+        cs[n] = (t < max_cs) ? t : max_cs;
+      }
+  /* (5) lCS with its periodic copies, then the 1/aj-weighted mean over the
+   * 27 nodes around fluid interior nodes (les.c:1207-1333) */
+  memcpy(ct, cs, G.n * sizeof(double));
+  cbo_fill_ghosts(c, ct);
+  dyn_periodic_copies(c, &G, ct);
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        const ptrdiff_t n = IX(&G, i, j, k);
+        if (!(nvert[n] < 0.1)) continue;
+        double wt[27], C[27];
+        for (int R = 0; R < 3; R++)
+          for (int Q = 0; Q < 3; Q++)
+            for (int P = 0; P < 3; P++) {
+              const int t = (R * 3 + Q) * 3 + P;
+              const ptrdiff_t m = IX(&G, i + P - 1, j + Q - 1, k + R - 1);
+              wt[t] = 1. / aj[m];
+              C[t] = ct[m];
+            }
+        cs[n] = itf(C, wt);
+      }
+  free(buf);
+  return 0;
+}
+
+/* Compute_eddy_viscosity_LES (les.c:1523-1567) after the dynamic model: Cs
+ * per node, and the velocity the model left in lUcat (see dyn_u). */
+void cbo_eddy_viscosity_dyn(const cbo_config *c, const double *const q[5], const double *const quc[5],
+                            const double *const csi[3], const double *const eta[3], const double *const zet[3],
+                            const double *aj, const double *nvert, const double *cs, double *nut) {
+  geom G = mkgeom(c);
+  for (int k = 1; k < G.m[2] - 1; k++)
+    for (int j = 1; j < G.m[1] - 1; j++)
+      for (int i = 1; i < G.m[0] - 1; i++) {
+        const ptrdiff_t n = IX(&G, i, j, k);
+        if (nvert[n] > 0.1) { nut[n] = 0; continue; }
+        double d[3][3];
+        for (int a = 0; a < 3; a++) {
+          d[a][0] = (dyn_u(&G, q, quc, nvert, a, i + 1, j, k, 1) - dyn_u(&G, q, quc, nvert, a, i - 1, j, k, 1)) * 0.5;
+          d[a][1] = (dyn_u(&G, q, quc, nvert, a, i, j + 1, k, 1) - dyn_u(&G, q, quc, nvert, a, i, j - 1, k, 1)) * 0.5;
+          d[a][2] = (dyn_u(&G, q, quc, nvert, a, i, j, k + 1, 1) - dyn_u(&G, q, quc, nvert, a, i, j, k - 1, 1)) * 0.5;
+        }
+        const double ajc = aj[n];
+        const double c0 = csi[0][n], c1 = csi[1][n], c2 = csi[2][n];
+        const double e0 = eta[0][n], e1 = eta[1][n], e2 = eta[2][n];
+        const double z0 = zet[0][n], z1 = zet[1][n], z2 = zet[2][n];
+        double g[3][3];
+        for (int a = 0; a < 3; a++) {
+          g[a][0] = (d[a][0] * c0 + d[a][1] * e0 + d[a][2] * z0) * ajc;
+          g[a][1] = (d[a][0] * c1 + d[a][1] * e1 + d[a][2] * z1) * ajc;
+          g[a][2] = (d[a][0] * c2 + d[a][1] * e2 + d[a][2] * z2) * ajc;
+        }
+        const double Sdd = 2. / 3. * (g[0][0] + g[1][1] + g[2][2]);
+        const double Sxx = 0.5 * (g[0][0] + g[0][0]) - Sdd, Sxy = 0.5 * (g[0][1] + g[1][0]), Sxz = 0.5 * (g[0][2] + g[2][0]);
+        const double Syx = Sxy, Syy = 0.5 * (g[1][1] + g[1][1]) - Sdd, Syz = 0.5 * (g[1][2] + g[2][1]);
+        const double Szx = Sxz, Szy = Syz, Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
+        const double Sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Syx * Syx + Syy * Syy + Syz * Syz +
+                                        Szx * Szx + Szy * Szy + Szz * Szz));
+        const double filter = pow(1. / aj[n], 1. / 3.);
+        nut[n] = cs[n] * pow(filter, 2.0) * Sabs;
+      }
+  cbo_fill_ghosts(c, nut);
 }

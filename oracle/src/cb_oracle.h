@@ -38,6 +38,7 @@ typedef struct {
   double s_x_min, s_y_min, s_z_min; /* -s_x_min/-s_y_min/-s_z_min: lower bounds of the sensor */
   double sigma_thrsh;      /* -sigma_thrsh: ks of the smoothness ratio (default 1e-5) */
   int flux;                /* upwind flux: 0 Rusanov (the reference's), 1 Roe with Harten's entropy fix */
+  double max_cs;           /* -max_cs: upper clip of the dynamic Smagorinsky coefficient (default 0.05) */
 } cbo_config;
 
 /* Fill the two ghost layers of each periodic direction of one padded plane
@@ -151,6 +152,21 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
                   const double *nvert, int nbodies, const cbo_ibm_surface *surf, const int *nlist,
                   const cbo_ibm_info *const *lists, const double *const coor[3], double *lp, int *lp_valid,
                   int twoD, int wallfunction);
+
+/* Compute_Smagorinsky_Constant_1 with -les 2 (les.c:151-1472, the default
+ * 3-D box test filter with local averaging): Cs per node into cs (global CS,
+ * in/out: boundary nodes keep their value through the clipping) from the
+ * ghosted current state q, the state quc of the last CalcUCat (NULL: zero
+ * velocity) and the local pressure lp.  Returns 5 unless les == 2. */
+int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const double *const quc[5],
+                            const double *lp, const double *const csi[3], const double *const eta[3],
+                            const double *const zet[3], const double *aj, const double *nvert, double *cs);
+/* Compute_eddy_viscosity_LES after the dynamic model: Cs per node, and the
+ * velocity the model left in lUcat (q at interior nodes with nvert <= 1.1,
+ * quc elsewhere). */
+void cbo_eddy_viscosity_dyn(const cbo_config *c, const double *const q[5], const double *const quc[5],
+                            const double *const csi[3], const double *const eta[3], const double *const zet[3],
+                            const double *aj, const double *nvert, const double *cs, double *nut);
 
 /* Number of RK stages the reference runs for this config (= fluxorder). */
 int cbo_nstages(const cbo_config *c);

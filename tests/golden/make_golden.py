@@ -36,6 +36,8 @@ CASES = {
     "les_muscl_sigma1": ((11, 10, 9), 0.05, 3, dict(les=1, inviscid=0, fluxorder=2, ren=1600., ma=0.3, pr=0.71, dt=0.004), False, 3),
     "les_weno_blend": ((9, 10, 11), 0.05, 4, dict(les=1, inviscid=0, fluxorder=3, s_x=0.3, s_y=0.6, s_z=0.8, ren=400., ma=0.3, pr=0.71, dt=0.004), True, 2),
     "les_first_order_central3": ((10, 10, 10), 0.03, 5, dict(les=1, inviscid=0, fluxorder=1, central=3, eno_order=3, ren=300., ma=0.3, pr=0.71, dt=0.003), True, 2),
+    # dynamic Smagorinsky (Compute_Smagorinsky_Constant_1 with -les 2)
+    "les2_dynamic_weno_mask": ((11, 9, 10), 0.05, 6, dict(les=2, inviscid=0, fluxorder=3, ren=800., ma=0.3, pr=0.71, dt=0.003, max_cs=0.1), True, 3),
 }
 
 

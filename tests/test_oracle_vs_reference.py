@@ -136,3 +136,46 @@ def test_formbcs_restatement_bitexact_vs_reference(bct, les, iso):
     st = ora.initial_state(q)
     ora.steps(2, st, met, nvp)
     assert np.array_equal(O.from_padded(st["q"]), ref.Q())
+
+
+DYN_CASES = [
+    ((21, 17, 19), dict(fluxorder=3, ren=800.), False),
+    ((23, 19, 18), dict(fluxorder=2, ren=500., max_cs=0.2), True),
+]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference sources not present")
+@pytest.mark.parametrize("n,kw,mask", DYN_CASES)
+def test_dynamic_smagorinsky_restatement_bitexact_vs_reference(n, kw, mask):
+    """-les 2: Cs and nu_t when lUcat (CalcUCat of one state) differs from the
+    current state (the in-place velocity update of les.c:234-238), and three
+    full steps."""
+    from test_gpu_parity import _mask
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=2, inviscid=0, ma=0.3, pr=0.71, dt=0.002, **kw)
+    q1 = W.random_smooth_state(shape, seed=3)
+    q2 = W.random_smooth_state(shape, seed=4, amp=0.03)
+    nv = _mask(shape, 5, True) if mask else np.zeros(shape)
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q1)
+    ref.calc_ucat()
+    ref.set_state(q2)
+    ref.eddy_viscosity()
+    o = O.Oracle(cfg)
+    met = o.metrics(o.fill_ghosts(O.to_padded(cfg, coords)))
+    nvp = o.fill_ghosts(O.to_padded(cfg, nv))
+    qp1, qp2 = o.fill_ghosts(O.to_padded(cfg, q1)), o.fill_ghosts(O.to_padded(cfg, q2))
+    cs = o.dynamic_smagorinsky(qp2, qp1, met, nvp)
+    nut = o.eddy_viscosity_dyn(qp2, qp1, met, nvp, cs, o.zeros(1))
+    assert np.array_equal(O.from_padded(cs)[..., 0], ref.cs())
+    assert np.array_equal(O.from_padded(nut)[..., 0], ref.nut())
+    assert ref.cs().max() > 0.0
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q1)
+    ref.steps(3)
+    st = o.initial_state(q1)
+    o.steps(3, st, met, nvp)
+    assert np.array_equal(O.from_padded(st["q"]), ref.Q())
