@@ -279,7 +279,15 @@ static int dynamic_cs(cb_ctx *c) {
                                              c->nvert, D, Sabs);
   ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D, 10);  // DMLocalToLocal
   dyn_copy_kernel<<<grid_for(c, faces), 256, 0, c->stream>>>(c->dc, D, 9);
-  dyn_lm_kernel<<<gp, 256, 0, c->stream>>>(c->dc, q, qu, c->aj, c->nvert, (const double *const *)D, Sabs, LM, MM);
+  // LM / MM: zero on the whole box (the reference's VecSet), then the interior tiles
+  CB_CUDA(c, cudaMemsetAsync(LM, 0, sizeof(double) * 2 * c->plane, c->stream));
+  {
+    const int kc = std::min(8, c->dc.mz - 2);
+    const dim3 grid((c->dc.mx - 2 + DYN_BX - 1) / DYN_BX, (c->dc.my - 2 + DYN_BY - 1) / DYN_BY,
+                    (c->dc.mz - 2 + kc - 1) / kc);
+    dyn_lm_tiled_kernel<<<grid, dim3(DYN_BX, DYN_BY), DYN_LM_SMEM, c->stream>>>(
+        c->dc, q, qu, c->aj, c->nvert, (const double *const *)D, Sabs, LM, MM, kc);
+  }
   ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D + 10, 2);
   dyn_cs_kernel<<<grid_for(c, (long long)c->dc.mx * c->dc.my * c->dc.mz), 256, 0, c->stream>>>(
       c->dc, c->nvert, LM, MM, CS, c->cfg.max_cs);
@@ -595,6 +603,9 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
     if (cudaMalloc(&c->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab4");
   }
   if (cfg->les == 2) {
+    if (cudaFuncSetAttribute(dyn_lm_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DYN_LM_SMEM) !=
+        cudaSuccess)
+      return bail(CB_E_CUDA, "dynamic-model kernel attributes");
     const size_t db = sizeof(double) * c->plane * 14;
     if (cudaMalloc(&c->dyn_arena, db) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc dynamic-model planes");
     if (cudaMemsetAsync(c->dyn_arena, 0, db, c->stream) != cudaSuccess) return bail(CB_E_CUDA, "memset");

@@ -106,87 +106,128 @@ static __global__ void dyn_copy_kernel(const DevCfg c, double *const *f, int npl
 // (2) LM and MM of Germano's identity at interior nodes with nvert <= 1.1
 // (les.c:442-792): the test-filtered products of the 27 nodes around, with
 // weights 1/(|r|+1)/(|q|+1)/(|p|+1), accumulated in the reference's k, j, i
-// order; zero on every other node.  The pressure-velocity terms (beta) feed
-// nothing downstream and are not formed.
-static __global__ void dyn_lm_kernel(const DevCfg c, const double *const *q, const double *const *qu,
-                                     const double *aj, const double *nvert, const double *const *A,
-                                     const double *Sabs, double *LM, double *MM) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < c.plane; t += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    dyn_node(c, t, i, j, k);
-    double lm = 0., mm = 0.;
-    if (i <= c.mx + 1 && j <= c.my + 1 && dyn_interior(c, i, j, k) && nvert[t] <= 1.1) {
-      // filtered: rho, rhou, rhov, rhow, rhouu, rhouv, rhouw, rhovv, rhovw, rhoww,
-      // S11 S12 S13 S22 S23 S33, and |S| rho S of the same six
-      double f[22];
+// order (the caller zeroes every other node).  The pressure-velocity terms
+// (beta) feed nothing downstream and are not formed.  A block owns a
+// DYN_BX x DYN_BY column of interior nodes and marches along k through a
+// chunk of planes, keeping three planes (k-1, k, k+1, with a one-node halo in
+// i and j) of the per-node inputs in shared memory -- velocity as lUcat holds
+// it, rho, rhoU, rhoV, rhoW, the six distinct strain components and |S| -- so
+// each input is formed once per node instead of once per neighbour.
+constexpr int DYN_BX = 32, DYN_BY = 6, DYN_PX = DYN_BX + 2, DYN_PN = DYN_PX * (DYN_BY + 2), DYN_NF = 14;
+constexpr size_t DYN_LM_SMEM = sizeof(double) * 3 * DYN_NF * DYN_PN;
+static __global__ void __launch_bounds__(DYN_BX *DYN_BY)
+    dyn_lm_tiled_kernel(const DevCfg c, const double *const *q, const double *const *qu, const double *aj,
+                        const double *nvert, const double *const *A, const double *Sabs, double *LM, double *MM,
+                        int kchunk) {
+  extern __shared__ double dsm[];  // [slot][field][node]
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DYN_BX + tx;
+  const int i0 = 1 + blockIdx.x * DYN_BX, j0 = 1 + blockIdx.y * DYN_BY;
+  const int kb = 1 + blockIdx.z * kchunk, ke = min(c.mz - 1, kb + kchunk);
+  const int i = i0 + tx, j = j0 + ty;
+  const bool act = i <= c.mx - 2 && j <= c.my - 2;
+  auto load = [&](int kk, int s) {
+    double *base = dsm + (size_t)s * DYN_NF * DYN_PN;
+    for (int e = tid; e < DYN_PN; e += DYN_BX * DYN_BY) {
+      const int lx = e % DYN_PX, ly = e / DYN_PX;
+      const int xi = i0 - 1 + lx, yj = j0 - 1 + ly;
+      double v[DYN_NF];
 #pragma unroll
-      for (int x = 0; x < 22; x++) f[x] = 0.;
-      double ws = 0.;
-      double Sc[6] = {0., 0., 0., 0., 0., 0.};
-      for (int R = 0; R < 3; R++)
-        for (int Q = 0; Q < 3; Q++)
-          for (int P = 0; P < 3; P++) {
-            const int II = i + P - 1, JJ = j + Q - 1, KK = k + R - 1;
-            const long long m = gidx(c, II, JJ, KK);
-            const double w = 1. / (fabs(R - 1.0) + 1) * 1. / (fabs(Q - 1.0) + 1) * 1. / (fabs(P - 1.0) + 1);
-            const double u = dyn_u(c, q, qu, nvert, 0, II, JJ, KK, true);
-            const double v = dyn_u(c, q, qu, nvert, 1, II, JJ, KK, true);
-            const double ww = dyn_u(c, q, qu, nvert, 2, II, JJ, KK, true);
-            const double rho = q[0][m], ru = q[1][m], rv = q[2][m], rw = q[3][m];
-            const double S6[6] = {0.5 * (A[0][m] + A[0][m]), 0.5 * (A[1][m] + A[3][m]), 0.5 * (A[2][m] + A[6][m]),
-                                  0.5 * (A[4][m] + A[4][m]), 0.5 * (A[5][m] + A[7][m]), 0.5 * (A[8][m] + A[8][m])};
-            const double sm = Sabs[m];
-            const double val[10] = {rho, ru, rv, rw, ru * u, ru * v, ru * ww, rv * v, rv * ww, rw * ww};
+      for (int f = 0; f < DYN_NF; f++) v[f] = 0.;
+      if (xi <= c.mx - 1 && yj <= c.my - 1) {
+        const long long m = gidx(c, xi, yj, kk);
+        v[0] = dyn_u(c, q, qu, nvert, 0, xi, yj, kk, true);
+        v[1] = dyn_u(c, q, qu, nvert, 1, xi, yj, kk, true);
+        v[2] = dyn_u(c, q, qu, nvert, 2, xi, yj, kk, true);
+        v[3] = q[0][m]; v[4] = q[1][m]; v[5] = q[2][m]; v[6] = q[3][m];
+        v[7] = 0.5 * (A[0][m] + A[0][m]); v[8] = 0.5 * (A[1][m] + A[3][m]); v[9] = 0.5 * (A[2][m] + A[6][m]);
+        v[10] = 0.5 * (A[4][m] + A[4][m]); v[11] = 0.5 * (A[5][m] + A[7][m]); v[12] = 0.5 * (A[8][m] + A[8][m]);
+        v[13] = Sabs[m];
+      }
 #pragma unroll
-            for (int x = 0; x < 10; x++) f[x] += w * val[x];
-#pragma unroll
-            for (int x = 0; x < 6; x++) {
-              f[10 + x] += w * S6[x];
-              f[16 + x] += w * (S6[x] * sm * rho);
-            }
-            ws += w;
-            if (R == 1 && Q == 1 && P == 1) {
-#pragma unroll
-              for (int x = 0; x < 6; x++) Sc[x] = S6[x];
-            }
-          }
-      const double _rho = f[0] / ws, _rhou = f[1] / ws, _rhov = f[2] / ws, _rhow = f[3] / ws;
-      // symmetric 3x3 from the six distinct entries: (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
-      const int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-      double Lij[3][3], Sh[3][3], SSh[3][3], Sx[3][3];
-      const double fr[3] = {_rhou, _rhov, _rhow};
-      const int prod[3][3] = {{4, 5, 6}, {5, 7, 8}, {6, 8, 9}};
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-          Lij[a][b] = f[prod[a][b]] / ws - fr[a] * fr[b] / _rho;
-          Sh[a][b] = f[10 + sym[a][b]] / ws;
-          SSh[a][b] = f[16 + sym[a][b]] / ws;
-          Sx[a][b] = Sc[sym[a][b]];
-        }
-      double S_hat = 0;
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) S_hat += pow(Sh[a][b], 2.);
-      S_hat = sqrt(2 * S_hat);
-      const double filter = pow(1. / aj[t], 1. / 3.);
-      const double test_filter = 2.0 * filter;
-      double L_cat = 0.0, M_cat = 0.0;
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-          M_cat += -2.0 * _rho * pow(test_filter, 2.) * S_hat * (Sh[a][b] * Sx[a][b] - 0.33 * Sh[a][a] * Sx[b][b]) +
-                   2.0 * pow(filter, 2.) * (SSh[a][b] * Sx[a][b] - 0.33 * SSh[a][a] * Sx[b][b]);
-          L_cat += Lij[a][b] * Sx[a][b] - 0.33 * Sx[a][a] * Lij[b][b];
-        }
-      lm = L_cat;
-      mm = M_cat;
+      for (int f = 0; f < DYN_NF; f++) base[f * DYN_PN + e] = v[f];
     }
-    LM[t] = lm;
-    MM[t] = mm;
+  };
+  load(kb - 1, (kb - 1) % 3);
+  load(kb, kb % 3);
+  for (int k = kb; k < ke; k++) {
+    load(k + 1, (k + 1) % 3);
+    __syncthreads();
+    if (act) {
+      const long long n = gidx(c, i, j, k);
+      double lm = 0., mm = 0.;
+      if (nvert[n] <= 1.1) {
+        double f[22];
+#pragma unroll
+        for (int x = 0; x < 22; x++) f[x] = 0.;
+        double ws = 0.;
+        double Sc[6];
+        for (int R = 0; R < 3; R++) {
+          const double *pl = dsm + (size_t)((k + R - 1) % 3) * DYN_NF * DYN_PN;
+          for (int Q = 0; Q < 3; Q++)
+#pragma unroll
+            for (int P = 0; P < 3; P++) {
+              const int e = (ty + Q) * DYN_PX + tx + P;
+              const double w = 1. / (fabs(R - 1.0) + 1) * 1. / (fabs(Q - 1.0) + 1) * 1. / (fabs(P - 1.0) + 1);
+              const double u = pl[0 * DYN_PN + e], v = pl[1 * DYN_PN + e], ww = pl[2 * DYN_PN + e];
+              const double rho = pl[3 * DYN_PN + e], ru = pl[4 * DYN_PN + e], rv = pl[5 * DYN_PN + e],
+                           rw = pl[6 * DYN_PN + e];
+              const double sm = pl[13 * DYN_PN + e];
+              const double val[10] = {rho, ru, rv, rw, ru * u, ru * v, ru * ww, rv * v, rv * ww, rw * ww};
+#pragma unroll
+              for (int x = 0; x < 10; x++) f[x] += w * val[x];
+#pragma unroll
+              for (int x = 0; x < 6; x++) {
+                const double S = pl[(7 + x) * DYN_PN + e];
+                f[10 + x] += w * S;
+                f[16 + x] += w * (S * sm * rho);
+                if (R == 1 && Q == 1 && P == 1) Sc[x] = S;
+              }
+              ws += w;
+            }
+        }
+        // the weights sum to 8 exactly (powers of two), so dividing by the
+        // sum is the exact scaling by its reciprocal
+        const double rws = 1.0 / ws;
+        const double _rho = f[0] * rws, _rhou = f[1] * rws, _rhov = f[2] * rws, _rhow = f[3] * rws;
+        const int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+        const int prod[3][3] = {{4, 5, 6}, {5, 7, 8}, {6, 8, 9}};
+        const double fr[3] = {_rhou, _rhov, _rhow};
+        double Lij[3][3], Sh[3][3], SSh[3][3], Sx[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int b = 0; b < 3; b++) {
+            Lij[a][b] = f[prod[a][b]] * rws - fr[a] * fr[b] / _rho;
+            Sh[a][b] = f[10 + sym[a][b]] * rws;
+            SSh[a][b] = f[16 + sym[a][b]] * rws;
+            Sx[a][b] = Sc[sym[a][b]];
+          }
+        // pow(x, 2.) of the reference = x * x, the correctly rounded square
+        double S_hat = 0;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int b = 0; b < 3; b++) S_hat += Sh[a][b] * Sh[a][b];
+        S_hat = sqrt(2 * S_hat);
+        const double filter = pow(1. / aj[n], 1. / 3.);
+        const double test_filter = 2.0 * filter;
+        const double tf2 = test_filter * test_filter, f2 = filter * filter;
+        double L_cat = 0.0, M_cat = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int b = 0; b < 3; b++) {
+            M_cat += -2.0 * _rho * tf2 * S_hat * (Sh[a][b] * Sx[a][b] - 0.33 * Sh[a][a] * Sx[b][b]) +
+                     2.0 * f2 * (SSh[a][b] * Sx[a][b] - 0.33 * SSh[a][a] * Sx[b][b]);
+            L_cat += Lij[a][b] * Sx[a][b] - 0.33 * Sx[a][a] * Lij[b][b];
+          }
+        lm = L_cat;
+        mm = M_cat;
+      }
+      LM[n] = lm;
+      MM[n] = mm;
+    }
+    __syncthreads();  // the slot of plane k-1 is refilled next
   }
 }
 
