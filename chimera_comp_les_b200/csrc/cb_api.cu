@@ -514,6 +514,8 @@ void cb_config_default(cb_config *cfg, int mx, int my, int mz) {
   cfg->s_x_min = cfg->s_y_min = cfg->s_z_min = 0.;
   cfg->sigma_thrsh = 0.00001;  // rhs.c:3322
   cfg->max_cs = 0.05;          // les.c:151
+  cfg->twall = 1.;             // rhs.c:486
+  cfg->twod = 0;
 }
 
 int cb_create(const cb_config *cfg, cb_ctx **out) {
@@ -534,8 +536,6 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
         return bail(CB_E_UNSUPPORTED, "a periodic direction needs bctype 7 on both faces");
     if (bc[4] == 52 || bc[4] == 47)
       return bail(CB_E_UNSUPPORTED, "boundary codes 52 and 47 (profile inlets from the coordinates) are not built");
-    if ((bc[2] == 1 || bc[3] == 1) && cfg->isothermal == 2)
-      return bail(CB_E_UNSUPPORTED, "the characteristic isothermal wall (isothermal 2) is not built");
     c->fully_periodic = true;
     for (int b = 0; b < 6; b++) c->fully_periodic = c->fully_periodic && bc[b] == 7;
   }
@@ -575,6 +575,8 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.s_x_min = cfg->s_x_min; d.s_y_min = cfg->s_y_min; d.s_z_min = cfg->s_z_min;
   d.ks = cfg->sigma_thrsh;
   d.flux = cfg->flux;
+  d.twall = cfg->twall;
+  d.twod = cfg->twod;
   c->plane = (size_t)d.plane;
   // planes: 15 state + 9 metrics + aj + nvert + nut + LES filter width = 28
   const int nplanes = 28;

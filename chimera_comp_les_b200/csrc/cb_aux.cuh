@@ -198,9 +198,31 @@ static __global__ void bc_face_kernel(const DevCfg c, DevFields F, int dir, doub
         q[0][n] = q[0][n + sj]; q[1][n] = 0.; q[2][n] = q[2][n + sj]; q[3][n] = q[3][n + sj]; q[4][n] = q[4][n + sj];
       } else if (bc[2] == 1) {
         q[1][n] = 0.0; q[2][n] = 0.0; q[3][n] = 0.0;
-        const double lpn = lp_at(c, F, n + sj);
-        q[0][n] = lpn * (g * Ma * Ma);
-        q[4][n] = lpn / (g - 1);
+        if (c.isothermal == 2 && alfa != 0 && F.nvert[n] < 1.5) {
+          // characteristic isothermal wall (Poinsot & Lele), one pass (rhs.c:663-733, itr_tmp 1)
+          const double *const *lq = F.q;
+          const double ex = F.met[1][0][n], ey = F.met[1][1][n], ez = F.met[1][2][n];
+          const double a_sound = sqrt(c.twall / (Ma * Ma));
+          const double beta = sqrt(ey * ey + ex * ex + ez * ez);
+          const double L0 = -a_sound * beta;
+          if (!(b == 0 || b == c.mz - 1)) {
+            const long long n1 = n + sj, n2 = n + 2 * sj;
+            const double ajc = F.aj[n];
+            double L = L0 * ajc *
+                       ((-0.5 * lp_at(c, F, n2) + 2 * lp_at(c, F, n1) - 1.5 * lp_at(c, F, n)) -
+                        lq[0][n] * a_sound / beta *
+                            (ey * (-0.5 * lq[2][n2] / lq[0][n2] + 2. * lq[2][n1] / lq[0][n1] - 1.5 * lq[2][n] / lq[0][n]) +
+                             ez * (-0.5 * lq[3][n2] / lq[0][n2] + 2. * lq[3][n1] / lq[0][n1] - 1.5 * lq[3][n] / lq[0][n])));
+            if (c.twod != 1)
+              L -= L0 * ajc * lq[0][n] * a_sound / beta * ex *
+                   (-0.5 * lq[1][n2] / lq[0][n2] + 2. * lq[1][n1] / lq[0][n1] - 1.5 * lq[1][n] / lq[0][n]);
+            q[0][n] = F.qold[0][n] - c.dt * alfa * L / a_sound / a_sound;
+          }
+        } else {
+          const double lpn = lp_at(c, F, n + sj);
+          q[0][n] = lpn * (g * Ma * Ma);
+          q[4][n] = lpn / (g - 1);
+        }
       }
       n = gidx(c, a, c.my - 1, b);
       if (bc[3] == 3) {
@@ -209,9 +231,24 @@ static __global__ void bc_face_kernel(const DevCfg c, DevFields F, int dir, doub
         q[0][n] = q[0][n - sj]; q[1][n] = 0.; q[2][n] = q[2][n - sj]; q[3][n] = q[3][n - sj]; q[4][n] = q[4][n - sj];
       } else if (bc[3] == 1) {
         q[1][n] = 0.0; q[2][n] = 0.0; q[3][n] = 0.0;
-        if (c.isothermal == 1) q[0][n] = lp_at(c, F, n) * (g * Ma * Ma);
-        else q[0][n] = q[0][n - sj];
-        q[4][n] = lp_at(c, F, n - sj) / (g - 1.0);
+        if (c.isothermal == 2) {  // rhs.c:803-818
+          const double *const *lq = F.q;
+          const long long m1 = n - sj, m2 = n - 2 * sj;
+          const double lp1 = lp_at(c, F, m1);
+          const double a_sound = sqrt(g * lp1 / lq[0][m1]);
+          const double L0 = lq[2][m1] / lq[0][m1] - a_sound;
+          double L;
+          if (b == 0 || b == c.mz - 1 || L0 > 0.) L = 0.;
+          else
+            L = L0 * F.aj[m1] * F.met[1][1][m1] *
+                ((lp1 - lp_at(c, F, m2)) - lq[0][m1] * a_sound * (lq[2][n] / lq[0][n] - lq[2][m1] / lq[0][m1]));
+          q[0][n] = F.qold[0][n] - c.dt * alfa * L / a_sound / a_sound;
+          q[4][n] = q[0][n] * c.twall / (g * Ma * Ma) / (g - 1.0);
+        } else {
+          if (c.isothermal == 1) q[0][n] = lp_at(c, F, n) * (g * Ma * Ma);
+          else q[0][n] = q[0][n - sj];
+          q[4][n] = lp_at(c, F, n - sj) / (g - 1.0);
+        }
       }
     } else {  // rhs.c:840-1087: i = a, j = a0 + b
       const int j = a0 + b;

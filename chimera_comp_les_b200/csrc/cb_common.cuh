@@ -37,6 +37,8 @@ struct DevCfg {
   int calc_sigma;
   double s_x_min, s_y_min, s_z_min, ks;
   int flux;  // 0 Rusanov (the reference's), 1 Roe with Harten's entropy fix
+  double twall;  // -Twall of the characteristic isothermal wall
+  int twod;      // -twoD (1 drops that wall's x velocity term)
 };
 
 // Host check of an nvert array for the byte code of DevCfg::nvq.

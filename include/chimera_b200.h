@@ -78,6 +78,10 @@ typedef struct {
                            entropy fix (no counterpart in the reference) */
   double max_cs;        /* -max_cs: upper clip of the dynamic Smagorinsky coefficient (-les 2;
                            les.c:151, default 0.05) */
+  double twall;         /* -Twall: wall temperature of the characteristic isothermal wall
+                           (-isothermal 2 with j-wall code 1; rhs.c:486, default 1) */
+  int twod;             /* -twoD: 1 drops that wall's x-velocity term (rhs.c:724); the immersed
+                           boundary takes its own value from cb_ibm_set_options */
 } cb_config;
 
 /* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */

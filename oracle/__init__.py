@@ -68,6 +68,7 @@ class Config:
     sigma_thrsh: float = 1e-5
     flux: int = 0  # 0 Rusanov (the reference's), 1 Roe (no reference counterpart)
     max_cs: float = 0.05  # -max_cs: clip of the dynamic Smagorinsky coefficient (les.c:151)
+    twall: float = 1.0    # -Twall: characteristic isothermal wall temperature (rhs.c:486, 511)
     immersed: int = 0      # -imm: run the IB interpolation after the stages (solvers.c:282-288)
     wallfunction: int = 0  # -wallfunction: 0 noslip, 3 freeslip at IB nodes
     twoD: int = 0          # -twoD: 1/2/3 drops x/y/z from the IB normal and velocity
@@ -82,6 +83,7 @@ class Config:
             ("-Pr", repr(float(self.pr))), ("-gamma", repr(float(self.gamma))),
             ("-dt", repr(float(self.dt))), ("-visT", 0), ("-twoD", self.twoD), ("-TwoD", 0),
             ("-imm", self.immersed), ("-wallfunction", self.wallfunction), ("-max_cs", repr(float(self.max_cs))),
+            ("-Twall", repr(float(self.twall))),
             ("-calc_sigma", self.calc_sigma), ("-s_x_min", repr(float(self.s_x_min))),
             ("-s_y_min", repr(float(self.s_y_min))), ("-s_z_min", repr(float(self.s_z_min))),
             ("-sigma_thrsh", repr(float(self.sigma_thrsh))),
@@ -107,7 +109,7 @@ class _CCfg(C.Structure):
         ("dt", C.c_double), ("st", C.c_double), ("cs_const", C.c_double), ("ci", C.c_double),
         ("ratio", C.c_double), ("calc_sigma", C.c_int),
         ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double), ("sigma_thrsh", C.c_double),
-        ("flux", C.c_int), ("max_cs", C.c_double),
+        ("flux", C.c_int), ("max_cs", C.c_double), ("twall", C.c_double), ("twod", C.c_int),
     ]
 
 
@@ -116,6 +118,8 @@ def _ccfg(cfg: Config) -> _CCfg:
     for f, _ in _CCfg._fields_:
         if f == "bctype":
             c.bctype = (C.c_int * 6)(*cfg.bctype)
+        elif f == "twod":
+            c.twod = cfg.twoD
         else:
             setattr(c, f, getattr(cfg, f))
     return c
@@ -189,7 +193,7 @@ class Oracle:
         L.cbo_steps.restype = C.c_int
         L.cbo_bc_periodic.argtypes = [C.c_void_p, PP, PP]
         L.cbo_bc_periodic.restype = C.c_int
-        L.cbo_formbcs.argtypes = [C.c_void_p, C.c_double, PP, PP, PP, D, PP]
+        L.cbo_formbcs.argtypes = [C.c_void_p, C.c_double, PP, PP, PP, PP, D, D, PP]
         L.cbo_formbcs.restype = C.c_int
         L.cbo_ibm_interpolate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, PP, PP, D, C.c_int,
                                           C.c_int, C.c_int]
@@ -290,10 +294,12 @@ class Oracle:
                                         _dp(met["aj"][0]), _dp(nvert[0]), _dp(cs[0]), _dp(nut[0]))
         return nut
 
-    def formbcs(self, alfa: float, lq: np.ndarray, qold: np.ndarray, met, q: np.ndarray) -> np.ndarray:
+    def formbcs(self, alfa: float, lq: np.ndarray, qold: np.ndarray, met, q: np.ndarray,
+                nvert: Optional[np.ndarray] = None) -> np.ndarray:
         """FormBCS(user, alfa) on q (padded 5, in/out) from the ghosted lq."""
-        e = self.lib.cbo_formbcs(self._cp, alfa, _ptrs(list(lq)), _ptrs(list(qold)), _ptrs(list(met["zet"])),
-                                 _dp(met["aj"][0]), _ptrs(list(q)))
+        e = self.lib.cbo_formbcs(self._cp, alfa, _ptrs(list(lq)), _ptrs(list(qold)), _ptrs(list(met["eta"])),
+                                 _ptrs(list(met["zet"])), _dp(met["aj"][0]),
+                                 _dp(nvert[0]) if nvert is not None else None, _ptrs(list(q)))
         if e:
             raise RuntimeError(f"cbo_formbcs failed with status {e}")
         return q

@@ -974,14 +974,15 @@ int cbo_bc_periodic(const cbo_config *c, const double *const qin[5], double *con
 /* ------------------------------------------------------------------------ */
 /* lp_in: the local pressure lP (NULL: EqOfState of lq); p (may be NULL): the
  * global P, which receives the periodic copies and then the ghost wrap. */
+static int nvert_ok(const double *nv, ptrdiff_t n) { return !nv || nv[n] < 1.5; }
+
 static int formbcs_impl(const cbo_config *c, double alfa, const double *const lq[5], const double *lp_in,
-                        const double *const qold[5], const double *const zet[3], const double *aj,
-                        double *const q[5], double *p) {
+                        const double *const qold[5], const double *const eta[3], const double *const zet[3],
+                        const double *aj, const double *nvert_in, double *const q[5], double *p) {
   geom G = mkgeom(c);
   const int mx = G.m[0], my = G.m[1], mz = G.m[2];
   const int *bc = c->bctype;
   if (bc[4] == 52 || bc[4] == 47) return 5;
-  if ((bc[2] == 1 || bc[3] == 1) && c->isothermal == 2) return 5;
   if ((bc[0] == 7) != (bc[1] == 7) || (bc[2] == 7) != (bc[3] == 7) || (bc[4] == 7) != (bc[5] == 7)) return 5;
   const ptrdiff_t si = G.s[0], sj = G.s[1], sk = G.s[2];
   const double g = c->gamma, Ma = c->ma;
@@ -1019,9 +1020,29 @@ static int formbcs_impl(const cbo_config *c, double alfa, const double *const lq
         RO(n) = RO(n + sj); RU(n) = 0.; RV(n) = RV(n + sj); RW(n) = RW(n + sj); RE(n) = RE(n + sj);
       } else if (bc[2] == 1) {
         RU(n) = 0.0; RV(n) = 0.0; RW(n) = 0.0;
-        lp[n] = lp[n + sj];
-        RO(n) = lp[n] * (g * Ma * Ma);
-        RE(n) = lp[n] / (g - 1);
+        if (c->isothermal == 2 && alfa != 0 && nvert_ok(nvert_in, n)) {
+          /* characteristic isothermal wall (Poinsot & Lele), one pass (rhs.c:663-733, itr_tmp 1) */
+          const double a_sound = sqrt(c->twall / (Ma * Ma));
+          const double beta = sqrt(eta[1][n] * eta[1][n] + eta[0][n] * eta[0][n] + eta[2][n] * eta[2][n]);
+          const double L0 = -a_sound * beta;
+          if (!(k == 0 || k == mz - 1)) {
+            const ptrdiff_t n1 = n + sj, n2 = n + 2 * sj;
+            double L = L0 * aj[n] *
+                       ((-0.5 * lp[n2] + 2 * lp[n1] - 1.5 * lp[n]) -
+                        lq[0][n] * a_sound / beta *
+                            (eta[1][n] * (-0.5 * lq[2][n2] / lq[0][n2] + 2. * lq[2][n1] / lq[0][n1] - 1.5 * lq[2][n] / lq[0][n]) +
+                             eta[2][n] * (-0.5 * lq[3][n2] / lq[0][n2] + 2. * lq[3][n1] / lq[0][n1] - 1.5 * lq[3][n] / lq[0][n])));
+            if (c->twod != 1)
+              L -= L0 * aj[n] * lq[0][n] * a_sound / beta * eta[0][n] *
+                   (-0.5 * lq[1][n2] / lq[0][n2] + 2. * lq[1][n1] / lq[0][n1] - 1.5 * lq[1][n] / lq[0][n]);
+            RO(n) = qold[0][n] - c->dt * alfa * L / a_sound / a_sound;
+            lp[n] = RO(n) * c->twall / (g * Ma * Ma);
+          }
+        } else {
+          lp[n] = lp[n + sj];
+          RO(n) = lp[n] * (g * Ma * Ma);
+          RE(n) = lp[n] / (g - 1);
+        }
       }
       n = IX(&G, i, my - 1, k);
       if (bc[3] == 3) {
@@ -1030,7 +1051,18 @@ static int formbcs_impl(const cbo_config *c, double alfa, const double *const lq
         RO(n) = RO(n - sj); RU(n) = 0.; RV(n) = RV(n - sj); RW(n) = RW(n - sj); RE(n) = RE(n - sj);
       } else if (bc[3] == 1) {
         RU(n) = 0.0; RV(n) = 0.0; RW(n) = 0.0;
-        if (c->isothermal == 1) {
+        if (c->isothermal == 2) { /* rhs.c:803-818 */
+          const ptrdiff_t m1 = n - sj, m2 = n - 2 * sj;
+          const double a_sound = sqrt(g * lp[m1] / lq[0][m1]);
+          const double L0 = lq[2][m1] / lq[0][m1] - a_sound;
+          double L;
+          if (k == 0 || k == mz - 1 || L0 > 0.) L = 0.;
+          else
+            L = L0 * aj[m1] * eta[1][m1] *
+                ((lp[m1] - lp[m2]) - lq[0][m1] * a_sound * (lq[2][n] / lq[0][n] - lq[2][m1] / lq[0][m1]));
+          RO(n) = qold[0][n] - c->dt * alfa * L / a_sound / a_sound;
+          lp[n] = RO(n) * c->twall / (g * Ma * Ma);
+        } else if (c->isothermal == 1) {
           RO(n) = lp[n] * (g * Ma * Ma);
           lp[n] = lp[n - sj];
         } else {
@@ -1185,14 +1217,15 @@ static int formbcs_impl(const cbo_config *c, double alfa, const double *const lq
 }
 
 int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], const double *const qold[5],
-                const double *const zet[3], const double *aj, double *const q[5]) {
-  return formbcs_impl(c, alfa, lq, NULL, qold, zet, aj, q, NULL);
+                const double *const eta[3], const double *const zet[3], const double *aj, const double *nvert,
+                double *const q[5]) {
+  return formbcs_impl(c, alfa, lq, NULL, qold, eta, zet, aj, nvert, q, NULL);
 }
 
 int cbo_formbcs_lp(const cbo_config *c, double alfa, const double *const lq[5], const double *lp,
-                   const double *const qold[5], const double *const zet[3], const double *aj, double *const q[5],
-                   double *p) {
-  return formbcs_impl(c, alfa, lq, lp, qold, zet, aj, q, p);
+                   const double *const qold[5], const double *const eta[3], const double *const zet[3],
+                   const double *aj, const double *nvert, double *const q[5], double *p) {
+  return formbcs_impl(c, alfa, lq, lp, qold, eta, zet, aj, nvert, q, p);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1230,7 +1263,7 @@ int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const
       {
         double al[3] = {1., 1 / 4., 2 / 3.};
         if (c->fluxorder < 3) al[1] = 1 / 2.;
-        err = cbo_formbcs(c, al[s], (const double *const *)q, (const double *const *)qold, zet, aj, qn);
+        err = cbo_formbcs(c, al[s], (const double *const *)q, (const double *const *)qold, eta, zet, aj, nvert, qn);
       }
       for (int a = 0; a < 5; a++) memcpy(q[a], qn[a], G.n * sizeof(double));
     }
@@ -1365,7 +1398,8 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
         *have_uc = 1;
       }
       cbo_rk_combine(c, s, (const double *const *)qold, (const double *const *)q, (const double *const *)rhs, qn);
-      err = formbcs_impl(c, al[s], (const double *const *)q, lps, (const double *const *)qold, zet, aj, qn, NULL);
+      err = formbcs_impl(c, al[s], (const double *const *)q, lps, (const double *const *)qold, eta, zet, aj, nvert, qn,
+                         NULL);
       for (int a = 0; a < 5; a++) memcpy(q[a], qn[a], G.n * sizeof(double));
     }
     if (err) break;
@@ -1375,7 +1409,8 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
     if (err) break;
     for (int a = 0; a < 5; a++) memcpy(lq[a], q[a], G.n * sizeof(double));
     memcpy(lpc, lp, G.n * sizeof(double));
-    err = formbcs_impl(c, 0.0, (const double *const *)lq, lpc, (const double *const *)qold, zet, aj, q, lp);
+    err = formbcs_impl(c, 0.0, (const double *const *)lq, lpc, (const double *const *)qold, eta, zet, aj, nvert, q,
+                       lp);
     *lp_valid = 1;
     for (int a = 0; a < 5; a++) memcpy(qold[a], q[a], G.n * sizeof(double));
   }

@@ -39,6 +39,8 @@ typedef struct {
   double sigma_thrsh;      /* -sigma_thrsh: ks of the smoothness ratio (default 1e-5) */
   int flux;                /* upwind flux: 0 Rusanov (the reference's), 1 Roe with Harten's entropy fix */
   double max_cs;           /* -max_cs: upper clip of the dynamic Smagorinsky coefficient (default 0.05) */
+  double twall;            /* -Twall: wall temperature of the characteristic isothermal wall (default 1) */
+  int twod;                /* -twoD: 1 drops the x velocity term of that wall (and x in the IB) */
 } cbo_config;
 
 /* Fill the two ghost layers of each periodic direction of one padded plane
@@ -88,7 +90,8 @@ int cbo_bc_periodic(const cbo_config *c, const double *const qin[5], double *con
  * then the ghost wrap; alfa: the stage's RK coefficient.  Returns 5 for the
  * codes that are not restated. */
 int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], const double *const qold[5],
-                const double *const zet[3], const double *aj, double *const q[5]);
+                const double *const eta[3], const double *const zet[3], const double *aj, const double *nvert,
+                double *const q[5]);
 
 /* Full time steps (Flow_Solver + main loop): q (ghosted, in/out), qold,
  * quc (ghosted state of the last CalcUCat; in/out), have_uc (in/out flag),
@@ -137,8 +140,8 @@ int cbo_rhs_lp(const cbo_config *c, const double *const q[5], const double *lp, 
                const double *nvert, const double *nut, const double *const sig[3],
                double *const rhs[5]);
 int cbo_formbcs_lp(const cbo_config *c, double alfa, const double *const lq[5], const double *lp,
-                   const double *const qold[5], const double *const zet[3], const double *aj, double *const q[5],
-                   double *p);
+                   const double *const qold[5], const double *const eta[3], const double *const zet[3],
+                   const double *aj, const double *nvert, double *const q[5], double *p);
 
 /* Time steps with immersed bodies (RungeKutta with -imm): the stages, the
  * interpolation of each of the nbodies bodies (surf[b], lists[b] with

@@ -60,7 +60,7 @@ def gpu_block(cfg, precision="fp64"):
                  pr=cfg.pr, gamma=cfg.gamma, dt=cfg.dt, st=cfg.st, cs_const=cfg.cs_const, ci=cfg.ci,
                  ratio=cfg.ratio, precision=precision, calc_sigma=cfg.calc_sigma, s_x_min=cfg.s_x_min,
                  s_y_min=cfg.s_y_min, s_z_min=cfg.s_z_min, sigma_thrsh=cfg.sigma_thrsh, flux=cfg.flux,
-                 max_cs=cfg.max_cs)
+                 max_cs=cfg.max_cs, twall=cfg.twall, twod=cfg.twoD)
 
 
 def per_field_rel_l2(a, b):

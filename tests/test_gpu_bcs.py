@@ -49,3 +49,30 @@ def test_boundary_codes_match_oracle(bct, les, iso, fo):
         b.SetInitialCondition(q)
         b.RungeKutta(3)
         assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= 1e-5
+
+
+ISO2_BC = [(3, 3, 1, 1, 45, 44), (7, 7, 1, 1, 7, 7), (1, 1, 1, 1, 44, 45)]
+
+
+@pytest.mark.parametrize("bct", ISO2_BC)
+@pytest.mark.parametrize("les,twoD,twall", [(0, 0, 1.0), (1, 1, 1.2)])
+def test_characteristic_isothermal_walls_match_oracle(bct, les, twoD, twall):
+    """-isothermal 2 on the j walls (code 1): the characteristic wall of
+    Poinsot & Lele (rhs.c:663-733 low, 803-818 high), with -twoD and -Twall."""
+    n = (35, 17, 23)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, bctype=bct, les=les, inviscid=0, fluxorder=3,
+                   isothermal=2, twoD=twoD, twall=twall, s_x=0.4 if les else 1.0, s_y=0.7, s_z=0.9, ren=250.,
+                   ma=0.3, pr=0.71, dt=0.002)
+    q = W.random_smooth_state(shape, seed=9, periodic=False)
+    nv = np.zeros(shape)
+    ref = oracle_run(cfg, coords, q, nv, steps=3)
+    assert np.isfinite(ref["q_steps"]).all()
+    for prec, tol in (("fp64", RTOL_L2), ("mixed", 1e-5)):
+        with gpu_block(cfg, precision=prec) as b:
+            b.FormMetrics(coords)
+            b.set_nvert(nv)
+            b.SetInitialCondition(q)
+            b.RungeKutta(3)
+            assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= tol, prec

@@ -116,7 +116,7 @@ BC_CASES = [(3, 3, 1, 1, 45, 44), (7, 7, 1, 1, 7, 7), (3, 3, 3, 3, 55, 45), (51,
 
 
 @pytest.mark.parametrize("bct", BC_CASES)
-@pytest.mark.parametrize("les,iso", [(0, 0), (1, 1)])
+@pytest.mark.parametrize("les,iso", [(0, 0), (1, 1), (0, 2), (1, 2)])
 def test_formbcs_restatement_bitexact_vs_reference(bct, les, iso):
     """Non-periodic boundary codes (FormBCS rhs.c:477-1227): two RK steps."""
     n = (12, 13, 11)
@@ -135,7 +135,11 @@ def test_formbcs_restatement_bitexact_vs_reference(bct, les, iso):
     nvp = ora.fill_ghosts(O.to_padded(cfg, nv))
     st = ora.initial_state(q)
     ora.steps(2, st, met, nvp)
-    assert np.array_equal(O.from_padded(st["q"]), ref.Q())
+    # isothermal 2 with the characteristic outflow 49 drives this synthetic state
+    # non-finite in the reference itself; the restatement matches it NaN for NaN
+    assert np.array_equal(O.from_padded(st["q"]), ref.Q(), equal_nan=(iso == 2 and 49 in bct))
+    if not (iso == 2 and 49 in bct):
+        assert np.isfinite(ref.Q()).all()
 
 
 DYN_CASES = [
