@@ -83,6 +83,7 @@ struct cb_ctx {
   double **ptab = nullptr;    // device pointer tables
   unsigned *status = nullptr;
   bool fully_periodic = true;  // every face bctype 7: one fused periodic BC kernel
+  bool nv0 = true;             // nvert is zero everywhere: the stage kernel's no-IBM variant
   int cur = 0;                // buffer with the current Q (== Qold between steps)
   int uc = -1;                // buffer of the last CalcUCat state, -1: none
   bool have_grid = false, have_state = false;
@@ -152,11 +153,15 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t set_stage_attr() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 0>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STAGE_SMEM_BYTES);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)STAGE_SMEM_BYTES);
+  const int sm = (int)STAGE_SMEM_BYTES;
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 0>, attr, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 1>, attr, sm);
+  if constexpr (!RHSM) {  // the no-IBM variants of the time step
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 0, true>, attr, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 1, true>, attr, sm);
+  }
+  return e;
 }
 
 // Opt every stage-kernel variant into its dynamic shared memory on the
@@ -176,6 +181,10 @@ static cudaError_t set_stage_attrs() {
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt) {
   auto kern = c->dc.flux == 1 ? stage_kernel<double, false, LES, VISC, RHSM, 1> : stage_kernel<double, false, LES, VISC, RHSM, 0>;
+  if constexpr (!RHSM)
+    if (c->nv0)
+      kern = c->dc.flux == 1 ? stage_kernel<double, false, LES, VISC, RHSM, 1, true>
+                             : stage_kernel<double, false, LES, VISC, RHSM, 0, true>;
   const int nkin = c->dc.mz - 2;
   dim3 grid((c->dc.mx - 2 + BX - 1) / BX, (c->dc.my - 2 + BY - 1) / BY, (nkin + c->kchunk - 1) / c->kchunk);
   kern<<<grid, SNT, STAGE_SMEM_BYTES, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
@@ -186,7 +195,7 @@ static cudaError_t launch_stage(cb_ctx *c, const DevFields &F, int istage, doubl
   const bool les = c->cfg.les != 0, visc = c->cfg.inviscid == 0;
   if (c->cfg.precision == CB_MIXED)
     return launch_stage_mixed(c->dc, F, istage, alfa, beta, adt, c->kchunk, les, visc, rhs_mode, c->dc.flux == 1,
-                              c->stream);
+                              c->nv0 && !rhs_mode, c->stream);
   if (rhs_mode) {
     if (les && visc) return launch_stage_t<true, true, true>(c, F, istage, alfa, beta, adt);
     if (les) return launch_stage_t<true, false, true>(c, F, istage, alfa, beta, adt);
@@ -774,10 +783,14 @@ int cb_set_nvert(cb_ctx *c, const double *nvert) {
   int e = upload_planes(c, nvert, 1, PT_MISC + 1, false);
   if (e) return e;
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
-  const int q = nvert_codes_exact(nvert, (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz);
-  if (q != c->dc.nvq) {
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  const int q = nvert_codes_exact(nvert, nn);
+  bool zero = true;
+  for (size_t t = 0; t < nn && zero; t++) zero = nvert[t] == 0.0;
+  if (q != c->dc.nvq || zero != c->nv0) {
     c->dc.nvq = q;
-    invalidate_graphs(c);  // the graphs carry the config by value
+    c->nv0 = zero;
+    invalidate_graphs(c);  // the graphs carry the config and the kernel variant
   }
   return CB_OK;
 }

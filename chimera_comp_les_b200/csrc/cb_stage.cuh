@@ -124,6 +124,13 @@ __device__ __forceinline__ double nvert_at(const DevCfg &c, const DevFields &F, 
                                            long long g) {
   return c.nvq ? Rg.nv(n) : ldg(F.nvert + g);
 }
+// NV0: the block's nvert is zero everywhere (no immersed body), known on the
+// host, so every nvert test folds away at compile time
+template <bool NV0, typename R, int BX, int BY>
+__device__ __forceinline__ double nvert_v(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef n,
+                                          long long g) {
+  return NV0 ? 0.0 : nvert_at(c, F, Rg, n, g);
+}
 
 // ---------------------------------------------------------------- recon --
 template <typename R>
@@ -243,15 +250,16 @@ __device__ __forceinline__ void roe(const R QL[5], const R QR[5], R pL, R pR, co
 // DIR >= 0: the face direction as a compile-time constant, so every stencil
 // shift, stride and metric selection folds into fixed offsets; DIR = -1: the
 // direction is the runtime argument drt (one copy of the code for all three).
-template <typename R, bool MIX, bool LES, int BX, int BY, int DIR, int FLUX = 0>
+template <typename R, bool MIX, bool LES, int BX, int BY, int DIR, int FLUX = 0, bool NV0 = false>
 __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a,
                                           int gi, int gj, int gk, int drt, R Fc[5]) {
   const int d = DIR >= 0 ? DIR : drt;
   const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d);
   const int pos = d == 0 ? gi : (d == 1 ? gj : gk);
   const int m = d == 0 ? c.mx : (d == 1 ? c.my : c.mz);
-  const double nvm = nvert_at(c, F, Rg, nshift(a, d, -1), g0 - sd), nv0 = nvert_at(c, F, Rg, a, g0),
-               nv1 = nvert_at(c, F, Rg, nshift(a, d, 1), g0 + sd), nv2 = nvert_at(c, F, Rg, nshift(a, d, 2), g0 + 2 * sd);
+  const double nvm = nvert_v<NV0>(c, F, Rg, nshift(a, d, -1), g0 - sd), nv0 = nvert_v<NV0>(c, F, Rg, a, g0),
+               nv1 = nvert_v<NV0>(c, F, Rg, nshift(a, d, 1), g0 + sd),
+               nv2 = nvert_v<NV0>(c, F, Rg, nshift(a, d, 2), g0 + 2 * sd);
   const MetV<R> m0 = met_load<R, MIX>(F, d, g0), m1 = met_load<R, MIX>(F, d, g0 + sd);
   R h[3];
   h[0] = R(0.5) * (m0.x + m1.x);
@@ -273,7 +281,7 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   const int fo = c.fluxorder;
   bool first;
   if (LES) {
-    double nsum2 = (d == 2) ? nv0 + ldg(F.nvert + gidx(c, 1, gj, gk + 1)) : nv0 + nv1;  // quirk rhs.c:4046
+    double nsum2 = (d == 2) ? nv0 + (NV0 ? 0.0 : ldg(F.nvert + gidx(c, 1, gj, gk + 1))) : nv0 + nv1;  // quirk rhs.c:4046
     first = fo == 1 || ((pos == 0 || pos == m - 2) && bc_lo(c, d) != 7) || nsum2 > BLANKWALL;
   } else {
     first = fo == 1 || pos == 0 || pos == m - 2 || (nv0 + nv1) > BLANKWALL;
@@ -406,7 +414,7 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
 // -------------------------------------------------------- viscous face ----
 __device__ __forceinline__ bool blocked(double v) { return v > SOLID && v < INNERBLANK; }
 
-template <typename R, bool MIX, bool LES, int BX, int BY, int DIR>
+template <typename R, bool MIX, bool LES, int BX, int BY, int DIR, bool NV0 = false>
 __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a,
                                           int gi, int gj, int gk, int drt, R Fv[5], R A[3]) {
   const int d = DIR >= 0 ? DIR : drt;
@@ -425,8 +433,10 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
     }
     const long long te = gstride(c, e);
     const NRef ap = nshift(a, e, 1), am = nshift(a, e, -1), bp = nshift(b, e, 1), bm = nshift(b, e, -1);
-    const bool plus_blocked = blocked(nvert_at(c, F, Rg, ap, g0 + te)) || blocked(nvert_at(c, F, Rg, bp, g1 + te));
-    const bool minus_blocked = blocked(nvert_at(c, F, Rg, am, g0 - te)) || blocked(nvert_at(c, F, Rg, bm, g1 - te));
+    const bool plus_blocked =
+        blocked(nvert_v<NV0>(c, F, Rg, ap, g0 + te)) || blocked(nvert_v<NV0>(c, F, Rg, bp, g1 + te));
+    const bool minus_blocked =
+        blocked(nvert_v<NV0>(c, F, Rg, am, g0 - te)) || blocked(nvert_v<NV0>(c, F, Rg, bm, g1 - te));
 #pragma unroll
     for (int f = 0; f < 4; f++) {
       const int fi = F_U + f;
@@ -540,14 +550,14 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
 
 // Everything one face contributes: the FP64 form keeps conv, visc and the LES
 // stress apart (G[0..4], G[5..9], G[10..12]), the mixed form stores visc - conv.
-template <typename R, bool MIX, bool LES, bool VISC, int BX, int BY, int DIR, int FLUX = 0>
+template <typename R, bool MIX, bool LES, bool VISC, int BX, int BY, int DIR, int FLUX = 0, bool NV0 = false>
 __device__ __forceinline__ void face_flux(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a, int fi,
                                           int fj, int k, int drt, R *G) {
   constexpr int VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
   R Fc[5], Fv[5], A[3];
-  conv_face<R, MIX, LES, BX, BY, DIR, FLUX>(c, F, Rg, a, fi, fj, k, drt, Fc);
+  conv_face<R, MIX, LES, BX, BY, DIR, FLUX, NV0>(c, F, Rg, a, fi, fj, k, drt, Fc);
   if (VISC) {
-    visc_face<R, MIX, LES, BX, BY, DIR>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
+    visc_face<R, MIX, LES, BX, BY, DIR, NV0>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
   } else {
 #pragma unroll
     for (int q = 0; q < 5; q++) Fv[q] = R(0.);
@@ -594,7 +604,7 @@ static_assert(2 * (STAGE_SMEM_BYTES_MIXED + 1024) <= 233472, "mixed form: two bl
 // k-faces, for the prologue).  A function rather than a lambda so that it is
 // always inlined: an outlined call would copy the kernel parameters to local
 // memory.
-template <typename R, bool MIX, bool LES, bool VISC, bool ZONLY, int FLUX = 0>
+template <typename R, bool MIX, bool LES, bool VISC, bool ZONLY, int FLUX = 0, bool NV0 = false>
 __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F, const Ring<R, SBX, SBY> &Rg, int i0,
                                             int j0, int k, R *gxb, R *gyb, R *gzb) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, NG = FaceWidth<MIX>::NG;
@@ -633,13 +643,13 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
       if (MIX) {
         // one instantiation per direction (d is warp-uniform): 16 % faster
         // for the FP32 arithmetic of the mixed form
-        if (d == 0) face_flux<R, MIX, LES, VISC, BX, BY, 0, FLUX>(c, F, Rg, a, fi, fj, k, d, G);
-        else if (d == 1) face_flux<R, MIX, LES, VISC, BX, BY, 1, FLUX>(c, F, Rg, a, fi, fj, k, d, G);
-        else face_flux<R, MIX, LES, VISC, BX, BY, 2, FLUX>(c, F, Rg, a, fi, fj, k, d, G);
+        if (d == 0) face_flux<R, MIX, LES, VISC, BX, BY, 0, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, G);
+        else if (d == 1) face_flux<R, MIX, LES, VISC, BX, BY, 1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, G);
+        else face_flux<R, MIX, LES, VISC, BX, BY, 2, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, G);
       } else {
         // one copy for all directions: the FP64 form at 255 registers runs
         // 12 % slower with three
-        face_flux<R, MIX, LES, VISC, BX, BY, -1, FLUX>(c, F, Rg, a, fi, fj, k, d, G);
+        face_flux<R, MIX, LES, VISC, BX, BY, -1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, G);
       }
     } else {
 #pragma unroll
@@ -659,7 +669,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // One tile (tile column bxi, byi, k-chunk bzi) of one block: the whole k march.
-template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0>
+template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0, bool NV0 = false>
 __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, int bxi, int byi, int bzi, int istage,
                                            double alfa, double beta, double adt, int kchunk, double *smem_d) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
@@ -676,7 +686,8 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   Rg.nvc = nvc;
   // staged fields per plane: Q, then nvert (byte-exact codes), then lP (carried pressure)
   const bool pst = !MIX && F.pin != nullptr;
-  const int pslot = c.nvq ? 6 : 5;
+  const bool nvs = c.nvq && !NV0;
+  const int pslot = nvs ? 6 : 5;
   const int nstg = pslot + (pst ? 1 : 0);
 
   const int tid = threadIdx.x;
@@ -731,7 +742,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       R *base = Rg.pl + (size_t)s * NF * PN + idx;
 #pragma unroll
       for (int q = 0; q < NF; q++) base[(size_t)q * PN] = R(v[q]);
-      if (c.nvq) nvc[s * PN + idx] = (unsigned char)(stg[5 * PN + idx] * 4.0);
+      if (nvs) nvc[s * PN + idx] = (unsigned char)(stg[5 * PN + idx] * 4.0);
     }
   };
   auto load_plane_sync = [&](int kk, int s) {
@@ -748,7 +759,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   load_plane_sync(kb - 1, 1);
   load_plane_sync(kb, 2);
   load_plane_sync(kb + 1, 3);
-  plane_faces<R, MIX, LES, VISC, true, FLUX>(c, F, Rg, i0, j0, kb - 1, gxb, gyb, gzb);  // k-face kb-1/2
+  plane_faces<R, MIX, LES, VISC, true, FLUX, NV0>(c, F, Rg, i0, j0, kb - 1, gxb, gyb, gzb);  // k-face kb-1/2
   __syncthreads();
   R Gzp[NG];  // k-face k-1/2 of the node this thread updates
 #pragma unroll
@@ -761,7 +772,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
     Rg.sb = base;
     const bool more = k + 1 < ke;
     if (more) issue_stage(k + 3);  // overlaps the face computation
-    plane_faces<R, MIX, LES, VISC, false, FLUX>(c, F, Rg, i0, j0, k, gxb, gyb, gzb);
+    plane_faces<R, MIX, LES, VISC, false, FLUX, NV0>(c, F, Rg, i0, j0, k, gxb, gyb, gzb);
     // the only plane k-1 value the update needs, read before that slot is refilled
     const NRef n{0, uty + 2, utx + 2};
     const R rho_km1 = (LES && VISC && uact) ? Rg.get(F_RHO, nshift(n, 2, -1)) : R(0.);
@@ -770,7 +781,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 
     if (uact) {
       const long long g = gidx(c, ugi, ugj, k);
-      const double nv = nvert_at(c, F, Rg, n, g);
+      const double nv = nvert_v<NV0>(c, F, Rg, n, g);
       const int fxr = uty * (BX + 1) + utx + 1, fxl = fxr - 1;   // i+1/2, i-1/2
       const int fyu = (uty + 1) * BX + utx, fyd = uty * BX + utx;  // j+1/2, j-1/2
       const int fz = tid;                                          // k+1/2 (k-1/2 in Gzp)
@@ -861,12 +872,12 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   }
 }
 
-template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0>
+template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0, bool NV0 = false>
 __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
   extern __shared__ double smem_d[];
-  stage_tile<R, MIX, LES, VISC, RHS_MODE, FLUX>(c, F, blockIdx.x, blockIdx.y, blockIdx.z, istage, alfa, beta, adt, kchunk,
-                                          smem_d);
+  stage_tile<R, MIX, LES, VISC, RHS_MODE, FLUX, NV0>(c, F, blockIdx.x, blockIdx.y, blockIdx.z, istage, alfa, beta, adt,
+                                                    kchunk, smem_d);
 }
 
 // ------------------------------------------------------- batched form ----
