@@ -1118,8 +1118,6 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
     return fail(c, CB_E_UNSUPPORTED, "the characteristic isothermal IB wall (isothermal 2) is not built");
   if (n > 0 && c->dc.calc_sigma)
     return fail(c, CB_E_UNSUPPORTED, "the shock sensor with immersed bodies is not built");
-  if (n > 0 && c->cfg.les == 2)
-    return fail(c, CB_E_UNSUPPORTED, "the dynamic Smagorinsky model with immersed bodies is not built");
   const int m[3] = {c->cfg.mx, c->cfg.my, c->cfg.mz};
   const bool per[3] = {c->cfg.bctype[0] == 7, c->cfg.bctype[2] == 7, c->cfg.bctype[4] == 7};
   // a node listed twice keeps its last entry

@@ -89,6 +89,7 @@ __device__ __forceinline__ double ldg(const double *p) { return __ldg(p); }
 __device__ __forceinline__ double sigma_at(const DevCfg &c, const DevFields &F, int d, int i, int j, int k) {
   if (c.calc_sigma) return ldg((d == 0 ? F.sig[0] : (d == 1 ? F.sig[1] : F.sig[2])) + gidx(c, i, j, k));
   if (d == 0) return c.s_x;
+  if (c.s_y == c.s_z) return c.s_y;  // min(s_z, s_y) = s_y = s_z: the node's position does not matter
   // wrap ghost indices to their owned image (periodic directions only reach ghosts)
   int ii = i < 0 ? i + c.mx : (i >= c.mx ? i - c.mx : i);
   int jj = j < 0 ? j + c.my : (j >= c.my ? j - c.my : j);

@@ -1374,11 +1374,10 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
                   const cbo_ibm_info *const *lists, const double *const coor[3], double *lp, int *lp_valid,
                   int twoD, int wallfunction) {
   if (c->calc_sigma) return 5; /* the sensor with a carried pressure is not restated */
-  if (c->les == 2) return 5;   /* nor the dynamic model's reading of it */
   geom G = mkgeom(c);
   int ns = cbo_nstages(c);
-  double *buf = (double *)calloc(G.n * 19, sizeof(double));
-  double *rhs[5], *qn[5], *sig[3], *lq[5], *lpc = buf + G.n * 18;
+  double *buf = (double *)calloc(G.n * 20, sizeof(double));
+  double *rhs[5], *qn[5], *sig[3], *lq[5], *lpc = buf + G.n * 18, *csbuf = buf + G.n * 19;
   for (int a = 0; a < 5; a++) { rhs[a] = buf + G.n * a; qn[a] = buf + G.n * (5 + a); lq[a] = buf + G.n * (13 + a); }
   for (int a = 0; a < 3; a++) sig[a] = buf + G.n * (10 + a);
   if (c->les) cbo_sigma(c, sig);
@@ -1386,7 +1385,11 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
   if (c->fluxorder < 3) al[1] = 1 / 2.;
   int err = 0;
   for (int step = 0; step < nsteps && !err; step++) {
-    if (c->les && !c->inviscid)
+    if (c->les == 2 && !c->inviscid) { /* the dynamic model reads lP only for beta, which feeds nothing */
+      const double *const *qu = *have_uc ? (const double *const *)quc : NULL;
+      cbo_dynamic_smagorinsky(c, (const double *const *)q, qu, lp, csi, eta, zet, aj, nvert, csbuf);
+      cbo_eddy_viscosity_dyn(c, (const double *const *)q, qu, csi, eta, zet, aj, nvert, csbuf, nut);
+    } else if (c->les && !c->inviscid)
       cbo_eddy_viscosity(c, *have_uc ? (const double *const *)quc : NULL, csi, eta, zet, aj, nvert, nut);
     for (int s = 0; s < ns && !err; s++) {
       const double *lps = (s == 0 && *lp_valid) ? lp : NULL;

@@ -59,6 +59,9 @@ CASES = {
     # slip walls in j, outflow 44 in k, LES
     "sphere_les_walls44": (dict(les=1, inviscid=0, fluxorder=3, ren=400., ma=0.3, pr=0.71, dt=0.002, isothermal=1,
                                 bctype=(7, 7, 3, 3, 44, 44)), None, 6, 3),
+    # the dynamic Smagorinsky model (-les 2) around the body
+    "sphere_les2_dynamic": (dict(les=2, inviscid=0, fluxorder=3, ren=400., ma=0.3, pr=0.71, dt=0.002, isothermal=1,
+                                 max_cs=0.1), None, 7, 3),
 }
 
 

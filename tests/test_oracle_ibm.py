@@ -24,7 +24,7 @@ def _oracle_interp(cfg, g, info, surf):
 
 
 def test_fixtures_present():
-    assert len(NAMES) >= 6
+    assert len(NAMES) >= 7
 
 
 @pytest.mark.parametrize("name", NAMES)
