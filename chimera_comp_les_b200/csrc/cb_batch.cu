@@ -96,7 +96,52 @@ struct BlockHost {
   long long off;        // offset of the block's padded box in every field array
   int tiles_x, tiles_y;
   bool have_grid = false, have_state = false;
+  bool nvz = true;      // the block's nvert is zero everywhere
 };
+
+// FP64 stage launches of one (LES, VISC, no-IBM) variant: the persistent
+// work-queue kernel or one block's grid
+template <bool LES, bool VISC, bool NV0>
+void f64_batched(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int s, double alfa,
+                 double beta, double adt, int ctas, cudaStream_t st) {
+  stage_batched_kernel<double, false, LES, VISC, NV0><<<ctas, SNT, STAGE_SMEM_BYTES, st>>>(tab, items, nitems, counter, s,
+                                                                                          alfa, beta, adt);
+}
+template <bool LES, bool VISC, bool NV0>
+void f64_block(const DevCfg &dc, const DevFields &F, dim3 grid, int s, double alfa, double beta, double adt, int kc,
+               cudaStream_t st) {
+  stage_kernel<double, false, LES, VISC, false, 0, NV0><<<grid, SNT, STAGE_SMEM_BYTES, st>>>(dc, F, s, alfa, beta, adt, kc);
+}
+template <bool NV0>
+void f64_batched_any(bool les, bool visc, const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int s,
+                     double alfa, double beta, double adt, int ctas, cudaStream_t st) {
+  if (les && visc) f64_batched<true, true, NV0>(tab, items, nitems, counter, s, alfa, beta, adt, ctas, st);
+  else if (les) f64_batched<true, false, NV0>(tab, items, nitems, counter, s, alfa, beta, adt, ctas, st);
+  else if (visc) f64_batched<false, true, NV0>(tab, items, nitems, counter, s, alfa, beta, adt, ctas, st);
+  else f64_batched<false, false, NV0>(tab, items, nitems, counter, s, alfa, beta, adt, ctas, st);
+}
+template <bool NV0>
+void f64_block_any(bool les, bool visc, const DevCfg &dc, const DevFields &F, dim3 grid, int s, double alfa, double beta,
+                   double adt, int kc, cudaStream_t st) {
+  if (les && visc) f64_block<true, true, NV0>(dc, F, grid, s, alfa, beta, adt, kc, st);
+  else if (les) f64_block<true, false, NV0>(dc, F, grid, s, alfa, beta, adt, kc, st);
+  else if (visc) f64_block<false, true, NV0>(dc, F, grid, s, alfa, beta, adt, kc, st);
+  else f64_block<false, false, NV0>(dc, F, grid, s, alfa, beta, adt, kc, st);
+}
+template <bool NV0>
+cudaError_t f64_attrs() {
+  const int sm = (int)STAGE_SMEM_BYTES;
+  const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(stage_batched_kernel<double, false, true, true, NV0>, a, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_batched_kernel<double, false, true, false, NV0>, a, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_batched_kernel<double, false, false, true, NV0>, a, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_batched_kernel<double, false, false, false, NV0>, a, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, true, true, false, 0, NV0>, a, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, true, false, false, 0, NV0>, a, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, false, true, false, 0, NV0>, a, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, false, false, false, 0, NV0>, a, sm);
+  return e;
+}
 
 }  // namespace
 
@@ -139,6 +184,13 @@ struct cb_batch {
   bool have_refs = false;
   std::string err;
 };
+
+// every block's nvert is zero: the stage kernels' no-IBM variant
+static bool batch_nv0(const cb_batch *b) {
+  for (const auto &bh : b->blk)
+    if (!bh.nvz) return false;
+  return true;
+}
 
 static int bfail(cb_batch *b, int code, const std::string &m) {
   if (b) b->err = m;
@@ -330,23 +382,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     if (set_stage_attrs_mixed() != cudaSuccess || set_batched_attrs_mixed() != cudaSuccess)
       return bail(CB_E_CUDA, "mixed kernel attributes");
   }
-  if (cudaFuncSetAttribute(stage_batched_kernel<double, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(stage_batched_kernel<double, false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(stage_batched_kernel<double, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(stage_batched_kernel<double, false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(stage_kernel<double, false, true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(stage_kernel<double, false, true, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(stage_kernel<double, false, false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)STAGE_SMEM_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(stage_kernel<double, false, false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)STAGE_SMEM_BYTES) != cudaSuccess)
-    return bail(CB_E_CUDA, "kernel attributes");
+  if (f64_attrs<false>() != cudaSuccess || f64_attrs<true>() != cudaSuccess) return bail(CB_E_CUDA, "kernel attributes");
   if (cudaMalloc(&b->staging, sizeof(double) * 5 * maxnn) != cudaSuccess) return bail(CB_E_CUDA, "staging");
   if (cudaMalloc(&b->ptab, sizeof(double *) * 64) != cudaSuccess) return bail(CB_E_CUDA, "ptab");
   if (cudaMalloc(&b->d_counter, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "counter");
@@ -424,9 +460,13 @@ int cb_batch_set_nvert(cb_batch *b, int k, const double *nvert) {
   BCUDA(b, cudaGetLastError());
   BCUDA(b, cudaStreamSynchronize(b->stream));
   const int q = nvert_codes_exact(nvert, nn);
-  if (q != bh.dc.nvq) {
+  bool zero = true;
+  for (size_t t = 0; t < nn && zero; t++) zero = nvert[t] == 0.0;
+  const bool nv0_was = batch_nv0(b);
+  bh.nvz = zero;
+  if (q != bh.dc.nvq || batch_nv0(b) != nv0_was) {
     bh.dc.nvq = q;
-    if (build_tables(b)) return CB_E_CUDA;  // tables and graphs carry the config
+    if (build_tables(b)) return CB_E_CUDA;  // tables and graphs carry the config and the kernel variant
   }
   return CB_OK;
 }
@@ -666,18 +706,14 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
   if (!per_block) {
     BCUDA(b, cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream));
     const int ctas = b->sms * (mixed ? 2 : 1);
+    const bool nv0 = batch_nv0(b);
     if (mixed) {
-      BCUDA(b, launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, les, visc, ctas,
+      BCUDA(b, launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, les, visc, nv0, ctas,
                                     b->stream));
+    } else if (nv0) {
+      f64_batched_any<true>(les, visc, tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, ctas, b->stream);
     } else {
-      if (les && visc)
-        stage_batched_kernel<double, false, true, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
-      else if (les)
-        stage_batched_kernel<double, false, true, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
-      else if (visc)
-        stage_batched_kernel<double, false, false, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
-      else
-        stage_batched_kernel<double, false, false, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt);
+      f64_batched_any<false>(les, visc, tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, ctas, b->stream);
     }
   } else {
     for (int k = 0; k < b->nb; k++) {
@@ -696,17 +732,11 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
         if (cost < best) { best = cost; kc = cand; }
       }
       if (mixed) {
-        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, false, false, b->stream));
+        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, false, bh.nvz, b->stream));
       } else {
         dim3 grid(bh.tiles_x, bh.tiles_y, (nk + kc - 1) / kc);
-        if (les && visc)
-          stage_kernel<double, false, true, true, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
-        else if (les)
-          stage_kernel<double, false, true, false, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
-        else if (visc)
-          stage_kernel<double, false, false, true, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
-        else
-          stage_kernel<double, false, false, false, false><<<grid, SNT, STAGE_SMEM_BYTES, b->stream>>>(bh.dc, F, s, alfa, beta, adt, kc);
+        if (bh.nvz) f64_block_any<true>(les, visc, bh.dc, F, grid, s, alfa, beta, adt, kc, b->stream);
+        else f64_block_any<false>(les, visc, bh.dc, F, grid, s, alfa, beta, adt, kc, b->stream);
       }
     }
   }
@@ -981,16 +1011,13 @@ int cb_batch_autotune(cb_batch *b, int *best_kchunk, double *best_ms) {
       cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream);
       cudaEventRecord(e0, b->stream);
       const int ctas = b->sms * (mixed ? 2 : 1);
+      const bool nv0 = batch_nv0(b);
       if (mixed) {
-        launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, les, visc, ctas, b->stream);
-      } else if (les && visc) {
-        stage_batched_kernel<double, false, true, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0);
-      } else if (les) {
-        stage_batched_kernel<double, false, true, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0);
-      } else if (visc) {
-        stage_batched_kernel<double, false, false, true><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0);
+        launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, les, visc, nv0, ctas, b->stream);
+      } else if (nv0) {
+        f64_batched_any<true>(les, visc, tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, ctas, b->stream);
       } else {
-        stage_batched_kernel<double, false, false, false><<<ctas, SNT, STAGE_SMEM_BYTES, b->stream>>>(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0);
+        f64_batched_any<false>(les, visc, tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, ctas, b->stream);
       }
       cudaEventRecord(e1, b->stream);
       BCUDA(b, cudaEventSynchronize(e1));

@@ -21,6 +21,7 @@ cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const d
 struct BatchBlock;
 cudaError_t set_batched_attrs_mixed();
 cudaError_t launch_batched_mixed(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int istage,
-                                 double alfa, double beta, double adt, bool les, bool visc, int ctas, cudaStream_t s);
+                                 double alfa, double beta, double adt, bool les, bool visc, bool nv0, int ctas,
+                                 cudaStream_t s);
 
 }  // namespace cb

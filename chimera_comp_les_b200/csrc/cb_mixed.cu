@@ -87,8 +87,16 @@ cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, 
 namespace {
 template <bool LES, bool VISC>
 cudaError_t battr1() {
-  return cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)STAGE_SMEM_BYTES_MIXED);
+  const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC>, a, (int)STAGE_SMEM_BYTES_MIXED);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC, true>, a, (int)STAGE_SMEM_BYTES_MIXED);
+}
+template <bool LES, bool VISC>
+void blaunch1(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int istage, double alfa,
+              double beta, double adt, bool nv0, int ctas, cudaStream_t s) {
+  auto kern = nv0 ? stage_batched_kernel<float, true, LES, VISC, true> : stage_batched_kernel<float, true, LES, VISC, false>;
+  kern<<<ctas, SNT, STAGE_SMEM_BYTES_MIXED, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
 }
 }  // namespace
 
@@ -101,16 +109,12 @@ cudaError_t set_batched_attrs_mixed() {
 }
 
 cudaError_t launch_batched_mixed(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int istage,
-                                 double alfa, double beta, double adt, bool les, bool visc, int ctas, cudaStream_t s) {
-  const size_t sm = STAGE_SMEM_BYTES_MIXED;
-  if (les && visc)
-    stage_batched_kernel<float, true, true, true><<<ctas, SNT, sm, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
-  else if (les)
-    stage_batched_kernel<float, true, true, false><<<ctas, SNT, sm, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
-  else if (visc)
-    stage_batched_kernel<float, true, false, true><<<ctas, SNT, sm, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
-  else
-    stage_batched_kernel<float, true, false, false><<<ctas, SNT, sm, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
+                                 double alfa, double beta, double adt, bool les, bool visc, bool nv0, int ctas,
+                                 cudaStream_t s) {
+  if (les && visc) blaunch1<true, true>(tab, items, nitems, counter, istage, alfa, beta, adt, nv0, ctas, s);
+  else if (les) blaunch1<true, false>(tab, items, nitems, counter, istage, alfa, beta, adt, nv0, ctas, s);
+  else if (visc) blaunch1<false, true>(tab, items, nitems, counter, istage, alfa, beta, adt, nv0, ctas, s);
+  else blaunch1<false, false>(tab, items, nitems, counter, istage, alfa, beta, adt, nv0, ctas, s);
   return cudaGetLastError();
 }
 

@@ -892,7 +892,7 @@ struct BatchBlock {
   long long first_item;  // index of this block's first item in the global list
 };
 
-template <typename R, bool MIX, bool LES, bool VISC>
+template <typename R, bool MIX, bool LES, bool VISC, bool NV0 = false>
 __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     stage_batched_kernel(const BatchBlock *__restrict__ blocks, const int2 *__restrict__ items, int nitems,
                          unsigned *__restrict__ counter, int istage, double alfa, double beta, double adt) {
@@ -910,7 +910,7 @@ __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     const int txy = bb.tiles_x * bb.tiles_y;
     const int bzi = ib.y / txy, rem = ib.y - bzi * txy;
     const int byi = rem / bb.tiles_x, bxi = rem - byi * bb.tiles_x;
-    stage_tile<R, MIX, LES, VISC, false>(bb.c, bb.F, bxi, byi, bzi, istage, alfa, beta, adt, bb.kchunk, smem_d);
+    stage_tile<R, MIX, LES, VISC, false, 0, NV0>(bb.c, bb.F, bxi, byi, bzi, istage, alfa, beta, adt, bb.kchunk, smem_d);
     __syncthreads();  // bb and item are rewritten by the next iteration
   }
 }
