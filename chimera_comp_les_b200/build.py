@@ -56,11 +56,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB_PATH
     objdir = os.path.join(PKG_DIR, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
-    for src, flags in SOURCES:
+    objs, procs = [], []
+    for src, flags in SOURCES:  # the translation units compile in parallel
         obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
-        _run([NVCC] + NVCC_FLAGS + flags + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj, src], verbose)
+        cmd = [NVCC] + NVCC_FLAGS + flags + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj, src]
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
         objs.append(obj)
+    failed = None
+    for cmd, p in procs:
+        out, err = p.communicate()
+        if p.returncode != 0:
+            sys.stderr.write(out + err)
+            failed = failed or cmd
+        elif verbose:
+            sys.stderr.write(err)
+    if failed:
+        raise RuntimeError("nvcc failed building libchimera_b200.so: " + " ".join(failed))
     _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB_PATH] + objs, verbose)
     return LIB_PATH
 

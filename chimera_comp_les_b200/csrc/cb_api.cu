@@ -78,6 +78,7 @@ struct cb_ctx {
   double *sig_a[3] = {}, *sig_b[3] = {};
   // dynamic Smagorinsky: velocity gradients (9), |S|, LM, MM, CS, lCS
   double *dyn_arena = nullptr;
+  double dyn_tf_mult = 2.0;  // test-filter width over the filter width (les.c:598-601)
   bool have_refs = false;
   double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
   double **ptab = nullptr;    // device pointer tables
@@ -122,6 +123,10 @@ enum { PT_Q0 = 0, PT_Q1 = 5, PT_Q2 = 10, PT_MET = 15, PT_COOR = 24, PT_RHS = 27,
        PT_SIGA = 56, PT_SIGB = 59, PT_PL = 64, PT_SNAP = 65, PT_DYN = 71, PT_N = 85 };
 // PT_DYN + 0..8: du/dx .. dw/dz, 9: |S|, 10: LM, 11: MM, 12: CS, 13: lCS
 
+// -les values that run the dynamic model: >= 2 except 10 (les.c:134-146
+// single out 1 and 10; solvers.c:28 skips every model with 10)
+static bool les_dynamic(const cb_config &f) { return f.les >= 2 && f.les != 10; }
+
 static int grid_for(const cb_ctx *c, long long work, int block = 256) {
   long long b = (work + block - 1) / block;
   long long cap = (long long)c->sms * 8;
@@ -158,8 +163,7 @@ static cudaError_t set_stage_attr() {
   cudaError_t e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 0>, attr, sm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 1>, attr, sm);
   if constexpr (!RHSM) {  // the no-IBM variants of the time step
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 0, true>, attr, sm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 1, true>, attr, sm);
+    if (e == cudaSuccess) e = stage_nv0_attrs<double, false, LES, VISC>(sm);
   }
   return e;
 }
@@ -178,13 +182,23 @@ static cudaError_t set_stage_attrs() {
   return set_stage_attr<false, false, true>();
 }
 
+// Flux bits of the stage kernel: Roe, and with LES and the sensor off the
+// constant blend weight s_x = s_y = s_z when it is exactly 1 or 0.
+static int flux_bits(const cb_ctx *c) {
+  int fl = c->dc.flux == 1 ? FLUX_ROE : 0;
+  const cb_config &f = c->cfg;
+  if (f.les && !f.calc_sigma && f.s_x == f.s_y && f.s_y == f.s_z) {
+    if (f.s_x == 1.0) fl |= FLUX_SIGMA1;
+    else if (f.s_x == 0.0) fl |= FLUX_SIGMA0;
+  }
+  return fl;
+}
+
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt) {
   auto kern = c->dc.flux == 1 ? stage_kernel<double, false, LES, VISC, RHSM, 1> : stage_kernel<double, false, LES, VISC, RHSM, 0>;
   if constexpr (!RHSM)
-    if (c->nv0)
-      kern = c->dc.flux == 1 ? stage_kernel<double, false, LES, VISC, RHSM, 1, true>
-                             : stage_kernel<double, false, LES, VISC, RHSM, 0, true>;
+    if (c->nv0) kern = stage_nv0_kernel<double, false, LES, VISC>(flux_bits(c));
   const int nkin = c->dc.mz - 2;
   dim3 grid((c->dc.mx - 2 + BX - 1) / BX, (c->dc.my - 2 + BY - 1) / BY, (nkin + c->kchunk - 1) / c->kchunk);
   kern<<<grid, SNT, STAGE_SMEM_BYTES, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
@@ -194,7 +208,7 @@ static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, dou
 static cudaError_t launch_stage(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt, bool rhs_mode) {
   const bool les = c->cfg.les != 0, visc = c->cfg.inviscid == 0;
   if (c->cfg.precision == CB_MIXED)
-    return launch_stage_mixed(c->dc, F, istage, alfa, beta, adt, c->kchunk, les, visc, rhs_mode, c->dc.flux == 1,
+    return launch_stage_mixed(c->dc, F, istage, alfa, beta, adt, c->kchunk, les, visc, rhs_mode, flux_bits(c),
                               c->nv0 && !rhs_mode, c->stream);
   if (rhs_mode) {
     if (les && visc) return launch_stage_t<true, true, true>(c, F, istage, alfa, beta, adt);
@@ -295,11 +309,37 @@ static int dynamic_cs(cb_ctx *c) {
     const dim3 grid((c->dc.mx - 2 + DYN_BX - 1) / DYN_BX, (c->dc.my - 2 + DYN_BY - 1) / DYN_BY,
                     (c->dc.mz - 2 + kc - 1) / kc);
     dyn_lm_tiled_kernel<<<grid, dim3(DYN_BX, DYN_BY), DYN_LM_SMEM, c->stream>>>(
-        c->dc, q, qu, c->aj, c->nvert, (const double *const *)D, Sabs, LM, MM, kc);
+        c->dc, q, qu, c->aj, c->nvert, (const double *const *)D, Sabs, LM, MM, kc, c->dyn_tf_mult);
   }
   ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D + 10, 2);
-  dyn_cs_kernel<<<grid_for(c, (long long)c->dc.mx * c->dc.my * c->dc.mz), 256, 0, c->stream>>>(
-      c->dc, c->nvert, LM, MM, CS, c->cfg.max_cs);
+  const cb_config &f = c->cfg;
+  const bool homo = f.i_homo_filter || f.j_homo_filter || f.k_homo_filter;
+  const bool pointwise = homo || f.les == 3;  // les.c:916-922
+  const long long owned = (long long)c->dc.mx * c->dc.my * c->dc.mz;
+  dyn_cs_kernel<<<grid_for(c, owned), 256, 0, c->stream>>>(c->dc, c->nvert, LM, MM, CS, f.max_cs, pointwise ? 1 : 0,
+                                                          homo ? 0 : 1);
+  if (homo) {
+    // the reference's homogeneous branches in order; with all three filters
+    // the box value overwrites every node the plane means wrote
+    const bool box = f.i_homo_filter && f.j_homo_filter && f.k_homo_filter;
+    if (f.i_homo_filter && f.k_homo_filter && !box)
+      dyn_homo_plane_kernel<<<c->dc.my - 2, DYN_RED, 0, c->stream>>>(c->dc, c->nvert, LM, MM, CS);
+    if (f.i_homo_filter && !f.k_homo_filter)
+      dyn_homo_line_kernel<<<grid_for(c, (long long)(c->dc.my - 2) * (c->dc.mz - 2)), 256, 0, c->stream>>>(
+          c->dc, c->nvert, LM, MM, CS);
+    // CT is scratch here: 2 * nparts + 1 doubles of its plane
+    const int nparts = (int)std::max(1LL, std::min((long long)2 * c->sms, (long long)(c->plane - 1) / 2));
+    if (box) {
+      dyn_homo_box_partial_kernel<<<nparts, DYN_RED, 0, c->stream>>>(c->dc, LM, MM, CT);
+      dyn_homo_box_final_kernel<<<1, DYN_RED, 0, c->stream>>>(CT, nparts);
+    }
+    dyn_clip_kernel<<<grid_for(c, owned), 256, 0, c->stream>>>(c->dc, c->nvert, CS, f.max_cs,
+                                                              box ? CT + 2 * nparts : nullptr);
+  }
+  if (pointwise) {  // no final weighted mean (les.c:1302)
+    CB_CUDA(c, cudaGetLastError());
+    return CB_OK;
+  }
   CB_CUDA(c, cudaMemcpyAsync(CT, CS, sizeof(double) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
   ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D + 13, 1);  // DMGlobalToLocal
   dyn_copy_kernel<<<grid_for(c, faces), 256, 0, c->stream>>>(c->dc, D + 13, 1);
@@ -312,7 +352,11 @@ static int dynamic_cs(cb_ctx *c) {
 static int nut_update(cb_ctx *c) {
   // Compute_eddy_viscosity_LES from the recorded state (or zero velocity).
   const long long work = (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2);
-  const bool dyn = c->cfg.les == 2;
+  const bool dyn = les_dynamic(c->cfg);
+  if (c->cfg.les == 10) {  // Cs = 0 (les.c:134-137): nu_t stays zero
+    CB_CUDA(c, cudaMemsetAsync(c->nut, 0, sizeof(double) * c->plane, c->stream));
+    return CB_OK;
+  }
   if (dyn) {
     int e = dynamic_cs(c);
     if (e) return e;
@@ -412,7 +456,7 @@ static int formbcs_zero(cb_ctx *c, int old) {
 
 // Enqueue one time step (no graph).
 static int enqueue_step(cb_ctx *c) {
-  if (c->cfg.les && !c->cfg.inviscid) {
+  if (c->cfg.les && c->cfg.les != 10 && !c->cfg.inviscid) {  // solvers.c:28
     int e = nut_update(c);
     if (e) return e;
   }
@@ -550,9 +594,8 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   }
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3) return bail(CB_E_ARG, "fluxorder must be 1, 2 or 3");
   if (cfg->eno_order != 2 && cfg->eno_order != 3) return bail(CB_E_ARG, "ENOorder must be 2 or 3");
-  if (cfg->les < 0 || cfg->les > 2)
-    return bail(CB_E_UNSUPPORTED, "only les 0, 1 (constant Smagorinsky) and 2 (dynamic, box test filter) are built");
-  if (cfg->les == 2 && !(cfg->max_cs >= 0.0)) return bail(CB_E_ARG, "max_cs must be >= 0");
+  if (cfg->les < 0) return bail(CB_E_ARG, "les must be >= 0");
+  if (les_dynamic(*cfg) && !(cfg->max_cs >= 0.0)) return bail(CB_E_ARG, "max_cs must be >= 0");
   if (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) return bail(CB_E_ARG, "precision must be CB_FP64 or CB_MIXED");
   if (cfg->flux != 0 && cfg->flux != 1) return bail(CB_E_ARG, "flux must be 0 (Rusanov) or 1 (Roe)");
   c->dev = cfg->device;
@@ -613,7 +656,8 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
     for (int a = 0; a < 3; a++) c->gcl[a] = g + c->plane * a;
     if (cudaMalloc(&c->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab4");
   }
-  if (cfg->les == 2) {
+  if (les_dynamic(*cfg)) {
+    c->dyn_tf_mult = cfg->testfilter_ik ? pow(5.0, 1. / 3.) : 2.0;  // the host's pow, as the reference's
     if (cudaFuncSetAttribute(dyn_lm_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DYN_LM_SMEM) !=
         cudaSuccess)
       return bail(CB_E_CUDA, "dynamic-model kernel attributes");
@@ -700,8 +744,16 @@ int cb_launches_per_step(const cb_ctx *c) {
     if (std::min(c->dc.mx, std::min(c->dc.my, c->dc.mz)) >= 6) ib += 2;  // the snapshots of Q and P near the faces
     ib += c->fully_periodic ? 2 : per_stage - 2 + nper + 1;
   }
-  const int dyn = (c->cfg.les == 2 && !c->cfg.inviscid) ? 9 : 0;  // the dynamic model's kernels
-  return (c->cfg.les && !c->cfg.inviscid ? 2 : 0) + dyn + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0) + ib;
+  const cb_config &f = c->cfg;
+  const bool homo = f.i_homo_filter || f.j_homo_filter || f.k_homo_filter;
+  const bool box = f.i_homo_filter && f.j_homo_filter && f.k_homo_filter;
+  int dyn = 0;  // the dynamic model's kernels
+  if (les_dynamic(f) && !f.inviscid) {
+    dyn = (homo || f.les == 3) ? 6 : 9;
+    if (homo) dyn += 1 + (box ? 2 : (f.i_homo_filter ? 1 : 0));
+  }
+  const bool model = f.les && f.les != 10 && !f.inviscid;
+  return (model ? 2 : 0) + dyn + per_stage * c->cfg.fluxorder + (c->dc.calc_sigma ? 6 : 0) + ib;
 }
 
 static int upload_planes(cb_ctx *c, const double *host, int nc, int pt_first, bool pinned_hint) {
@@ -907,7 +959,7 @@ int cb_calc_ucat(cb_ctx *c) {
 int cb_eddy_viscosity(cb_ctx *c) {
   if (!c) return CB_E_ARG;
   if (!c->have_state || !c->have_grid) return fail(c, CB_E_STATE, "grid and state must be set");
-  if (!c->cfg.les) return fail(c, CB_E_ARG, "eddy viscosity needs les = 1 or 2");
+  if (!c->cfg.les) return fail(c, CB_E_ARG, "eddy viscosity needs les != 0");
   int e = nut_update(c);
   if (e) return e;
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -926,7 +978,7 @@ int cb_get_nut(cb_ctx *c, double *nut) {
 
 int cb_get_cs(cb_ctx *c, double *cs) {
   if (!c || !cs) return CB_E_ARG;
-  if (!c->dyn_arena) return fail(c, CB_E_STATE, "the coefficient plane exists with les = 2 only");
+  if (!c->dyn_arena) return fail(c, CB_E_STATE, "the coefficient plane exists with a dynamic les (>= 2, not 10) only");
   const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
   pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_DYN + 12), 1,
                                                                   c->staging);

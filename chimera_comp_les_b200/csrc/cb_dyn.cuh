@@ -1,9 +1,11 @@
-// Dynamic Smagorinsky model (Compute_Smagorinsky_Constant_1 with -les 2,
-// les.c:151-1472, the default 3-D box test filter with local averaging):
-// Germano's identity with a 3x3x3 test filter, the least-squares ratio
-// LM / MM averaged over 27 nodes, clipping, and a 1/aj-weighted 27-node mean
-// of the coefficient.  Runs once per step before the eddy viscosity, all in
-// FP64 on the ghosted current state.
+// Dynamic Smagorinsky model (Compute_Smagorinsky_Constant_1 with a dynamic
+// -les, les.c:151-1472, the 3-D box test filter): Germano's identity with a
+// 3x3x3 test filter, the least-squares ratio LM / MM averaged over 27 nodes,
+// clipping, and a 1/aj-weighted 27-node mean of the coefficient.  With -les 3
+// or a homogeneous filter LM / MM are taken node by node, the plane / line /
+// box means of -i/-j/-k_homo_filter replace them, and the final mean is
+// skipped.  Runs once per step before the eddy viscosity, all in FP64 on the
+// ghosted current state.
 //
 // The reference overwrites lUcat in place in its first loop (les.c:234-238):
 // a node's velocity becomes rhoU/rho of the current state once the loop has
@@ -118,7 +120,7 @@ constexpr size_t DYN_LM_SMEM = sizeof(double) * 3 * DYN_NF * DYN_PN;
 static __global__ void __launch_bounds__(DYN_BX *DYN_BY)
     dyn_lm_tiled_kernel(const DevCfg c, const double *const *q, const double *const *qu, const double *aj,
                         const double *nvert, const double *const *A, const double *Sabs, double *LM, double *MM,
-                        int kchunk) {
+                        int kchunk, double tf_mult) {
   extern __shared__ double dsm[];  // [slot][field][node]
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DYN_BX + tx;
   const int i0 = 1 + blockIdx.x * DYN_BX, j0 = 1 + blockIdx.y * DYN_BY;
@@ -210,7 +212,7 @@ static __global__ void __launch_bounds__(DYN_BX *DYN_BY)
           for (int b = 0; b < 3; b++) S_hat += Sh[a][b] * Sh[a][b];
         S_hat = sqrt(2 * S_hat);
         const double filter = pow(1. / aj[n], 1. / 3.);
-        const double test_filter = 2.0 * filter;
+        const double test_filter = tf_mult * filter;  // 2, or 5^(1/3) with -testfilter_ik (les.c:598-601)
         const double tf2 = test_filter * test_filter, f2 = filter * filter;
         double L_cat = 0.0, M_cat = 0.0;
 #pragma unroll
@@ -232,11 +234,19 @@ static __global__ void __launch_bounds__(DYN_BX *DYN_BY)
 }
 
 // (3) Cs from the 27-node means of LM and MM at interior nodes
-// (les.c:905-925), then the clipping of every owned node (les.c:1124-1137,
-// whose face tests compare !bctype with 7 and never hold); boundary nodes keep
-// their previous value through it.
+// (les.c:905-925), or from LM / MM of the node itself (pointwise: -les 3 or a
+// homogeneous filter), then, with clip, the clipping of every owned node
+// (les.c:1124-1137, whose face tests compare !bctype with 7 and never hold);
+// boundary nodes keep their previous value through it.
+__device__ __forceinline__ double dyn_clip(double v, double nv, double max_cs) {
+  if (nv > 1.1 && nv < 7.) return 0.0;
+  if (nv > 0.1 && nv < 1.1) v = (0.01 < v) ? v : 0.01;
+  const double tt = (v < 0.000) ? 0.000 : v;
+  return (tt < max_cs) ? tt : max_cs;
+}
+
 static __global__ void dyn_cs_kernel(const DevCfg c, const double *nvert, const double *LM, const double *MM,
-                                     double *cs, double max_cs) {
+                                     double *cs, double max_cs, int pointwise, int clip) {
   const long long total = (long long)c.mx * c.my * c.mz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const unsigned u = (unsigned)t;
@@ -250,25 +260,133 @@ static __global__ void dyn_cs_kernel(const DevCfg c, const double *nvert, const 
         v = 0;
       } else {
         double lm = 0.0, mm = 0.0;
-        for (int R = 0; R < 3; R++)
-          for (int Q = 0; Q < 3; Q++)
-            for (int P = 0; P < 3; P++) {
-              const long long m = gidx(c, i + P - 1, j + Q - 1, k + R - 1);
-              lm += LM[m] / 27.0;
-              mm += MM[m] / 27.0;
-            }
+        if (pointwise) {
+          lm = LM[n];
+          mm = MM[n];
+        } else {
+          for (int R = 0; R < 3; R++)
+            for (int Q = 0; Q < 3; Q++)
+              for (int P = 0; P < 3; P++) {
+                const long long m = gidx(c, i + P - 1, j + Q - 1, k + R - 1);
+                lm += LM[m] / 27.0;
+                mm += MM[m] / 27.0;
+              }
+        }
         const double C = lm / (mm + DYN_EPS);
         v = (C < 0.0001) ? 0.0001 : C;
       }
     }
-    if (nv > 1.1 && nv < 7.) {
-      v = 0.0;
-    } else {
-      if (nv > 0.1 && nv < 1.1) v = (0.01 < v) ? v : 0.01;
-      const double tt = (v < 0.000) ? 0.000 : v;
-      v = (tt < max_cs) ? tt : max_cs;
-    }
-    cs[n] = v;
+    cs[n] = clip ? dyn_clip(v, nv, max_cs) : v;
+  }
+}
+
+// Homogeneous averages of LM and MM (les.c:934-1115).  The reference sums in
+// k, j, i loop order on one rank; the i-line means here keep that order, the
+// plane and box sums are deterministic tree reductions (the same result on
+// every run, within a few ulps of the sequential sum).
+constexpr int DYN_RED = 256;
+
+// tree sum of one value per thread of a DYN_RED-thread block; every thread
+// gets the total
+__device__ __forceinline__ double dyn_block_sum(double v, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int x = 0; x < DYN_RED / 32; x++) t += red[x];
+  return t;
+}
+
+// -i_homo_filter with -k_homo_filter: one block per j plane sums LM, MM and
+// the count over its fluid (nvert < 0.1) interior nodes, then every interior
+// node of the plane gets 0.5 <LM> / (<MM> + eps)  (les.c:934-980).
+static __global__ void __launch_bounds__(DYN_RED) dyn_homo_plane_kernel(const DevCfg c, const double *nvert,
+                                                                        const double *LM, const double *MM,
+                                                                        double *cs) {
+  __shared__ double red[DYN_RED / 32];
+  const int j = 1 + blockIdx.x;
+  const int nx = c.mx - 2, nz = c.mz - 2;
+  const int cnt_all = nx * nz;
+  double lm = 0.0, mm = 0.0, cn = 0.0;
+  for (int t = threadIdx.x; t < cnt_all; t += DYN_RED) {
+    const int i = 1 + t % nx, k = 1 + t / nx;
+    const long long n = gidx(c, i, j, k);
+    if (nvert[n] < 0.1) { lm += LM[n]; mm += MM[n]; cn += 1.0; }
+  }
+  lm = dyn_block_sum(lm, red);
+  mm = dyn_block_sum(mm, red);
+  cn = dyn_block_sum(cn, red);
+  if (cn > 0.0) { lm /= cn; mm /= cn; }
+  const double v = 0.5 * lm / (mm + DYN_EPS);
+  for (int t = threadIdx.x; t < cnt_all; t += DYN_RED) {
+    const int i = 1 + t % nx, k = 1 + t / nx;
+    cs[gidx(c, i, j, k)] = v;
+  }
+}
+
+// -i_homo_filter without -k_homo_filter: one thread per (k, j) line sums
+// along i in the reference's order; fluid interior nodes of the line get
+// 0.5 <LM> / (<MM> + eps)  (les.c:984-1081).
+static __global__ void dyn_homo_line_kernel(const DevCfg c, const double *nvert, const double *LM, const double *MM,
+                                            double *cs) {
+  const int ny = c.my - 2, nz = c.mz - 2;
+  const int lines = ny * nz;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < lines; t += gridDim.x * blockDim.x) {
+    const int j = 1 + t % ny, k = 1 + t / ny;
+    const long long row = gidx(c, 0, j, k);
+    double lm = 0.0, mm = 0.0;
+    int cnt = 0;
+    for (int i = 1; i < c.mx - 1; i++)
+      if (nvert[row + i] < 0.1) { lm += LM[row + i]; mm += MM[row + i]; cnt++; }
+    if (cnt > 0) { lm /= (double)cnt; mm /= (double)cnt; }
+    const double v = 0.5 * lm / (mm + DYN_EPS);
+    for (int i = 1; i < c.mx - 1; i++)
+      if (nvert[row + i] < 0.1) cs[row + i] = v;
+  }
+}
+
+// -i/-j/-k_homo_filter together, first pass: per-block sums of LM and MM over
+// every interior node (no mask) into part[2 * block] (les.c:1087-1101).
+static __global__ void __launch_bounds__(DYN_RED) dyn_homo_box_partial_kernel(const DevCfg c, const double *LM,
+                                                                              const double *MM, double *part) {
+  __shared__ double red[DYN_RED / 32];
+  const long long nx = c.mx - 2, ny = c.my - 2, total = nx * ny * (c.mz - 2);
+  double lm = 0.0, mm = 0.0;
+  for (long long t = blockIdx.x * (long long)DYN_RED + threadIdx.x; t < total; t += (long long)gridDim.x * DYN_RED) {
+    const int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / (nx * ny));
+    const long long n = gidx(c, i, j, k);
+    lm += LM[n];
+    mm += MM[n];
+  }
+  lm = dyn_block_sum(lm, red);
+  mm = dyn_block_sum(mm, red);
+  if (threadIdx.x == 0) { part[2 * blockIdx.x] = lm; part[2 * blockIdx.x + 1] = mm; }
+}
+
+// second pass (one block): the box value sum LM / sum MM into part[2 * nparts]
+static __global__ void __launch_bounds__(DYN_RED) dyn_homo_box_final_kernel(double *part, int nparts) {
+  __shared__ double red[DYN_RED / 32];
+  double lm = 0.0, mm = 0.0;
+  for (int b = threadIdx.x; b < nparts; b += DYN_RED) { lm += part[2 * b]; mm += part[2 * b + 1]; }
+  lm = dyn_block_sum(lm, red);
+  mm = dyn_block_sum(mm, red);
+  if (threadIdx.x == 0) part[2 * nparts] = lm / mm;
+}
+
+// The clipping of every owned node (les.c:1124-1137) after the homogeneous
+// averages; with box, every owned node first takes the box value.
+static __global__ void dyn_clip_kernel(const DevCfg c, const double *nvert, double *cs, double max_cs,
+                                       const double *box) {
+  const long long total = (long long)c.mx * c.my * c.mz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const unsigned u = (unsigned)t;
+    const int i = (int)(u % (unsigned)c.mx), j = (int)((u / (unsigned)c.mx) % (unsigned)c.my),
+              k = (int)(u / ((unsigned)c.mx * (unsigned)c.my));
+    const long long n = gidx(c, i, j, k);
+    cs[n] = dyn_clip(box ? *box : cs[n], nvert[n], max_cs);
   }
 }
 

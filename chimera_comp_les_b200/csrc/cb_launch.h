@@ -9,9 +9,10 @@
 namespace cb {
 
 cudaError_t set_stage_attrs_mixed();
+// fl: flux bits (FLUX_ROE; the constant-sigma bits apply with nv0 only);
 // nv0: nvert is zero everywhere, the variant without any nvert test (time step only)
 cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt,
-                               int kchunk, bool les, bool visc, bool rhs_mode, bool roe, bool nv0, cudaStream_t s);
+                               int kchunk, bool les, bool visc, bool rhs_mode, int fl, bool nv0, cudaStream_t s);
 // FP32 metric vectors (w: filter width, aj, 0) and the FP64 metric divergence
 // (sum over directions of h(+1/2) - h(-1/2)) for the mixed form.
 cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, const double *aj,

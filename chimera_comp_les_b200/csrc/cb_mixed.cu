@@ -14,19 +14,19 @@ cudaError_t attr1() {
   cudaError_t e = cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM, 0>, attr, sm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM, 1>, attr, sm);
   if constexpr (!RHSM) {  // the no-IBM variants of the time step
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM, 0, true>, attr, sm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM, 1, true>, attr, sm);
+    if (e == cudaSuccess) e = stage_nv0_attrs<float, true, LES, VISC>(sm);
   }
   return e;
 }
 template <bool LES, bool VISC, bool RHSM>
 void launch1(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt, int kchunk,
-             bool roe, bool nv0, cudaStream_t s) {
+             int fl, bool nv0, cudaStream_t s) {
   const int nkin = c.mz - 2;
   dim3 grid((c.mx - 2 + SBX - 1) / SBX, (c.my - 2 + SBY - 1) / SBY, (nkin + kchunk - 1) / kchunk);
+  const bool roe = (fl & FLUX_ROE) != 0;
   auto kern = roe ? stage_kernel<float, true, LES, VISC, RHSM, 1> : stage_kernel<float, true, LES, VISC, RHSM, 0>;
   if constexpr (!RHSM)
-    if (nv0) kern = roe ? stage_kernel<float, true, LES, VISC, RHSM, 1, true> : stage_kernel<float, true, LES, VISC, RHSM, 0, true>;
+    if (nv0) kern = stage_nv0_kernel<float, true, LES, VISC>(fl);
   kern<<<grid, SNT, STAGE_SMEM_BYTES_MIXED, s>>>(c, F, istage, alfa, beta, adt, kchunk);
 }
 
@@ -69,17 +69,17 @@ cudaError_t set_stage_attrs_mixed() {
 }
 
 cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt,
-                               int kchunk, bool les, bool visc, bool rhs_mode, bool roe, bool nv0, cudaStream_t s) {
+                               int kchunk, bool les, bool visc, bool rhs_mode, int fl, bool nv0, cudaStream_t s) {
   if (rhs_mode) {
-    if (les && visc) launch1<true, true, true>(c, F, istage, alfa, beta, adt, kchunk, roe, false, s);
-    else if (les) launch1<true, false, true>(c, F, istage, alfa, beta, adt, kchunk, roe, false, s);
-    else if (visc) launch1<false, true, true>(c, F, istage, alfa, beta, adt, kchunk, roe, false, s);
-    else launch1<false, false, true>(c, F, istage, alfa, beta, adt, kchunk, roe, false, s);
+    if (les && visc) launch1<true, true, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, s);
+    else if (les) launch1<true, false, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, s);
+    else if (visc) launch1<false, true, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, s);
+    else launch1<false, false, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, s);
   } else {
-    if (les && visc) launch1<true, true, false>(c, F, istage, alfa, beta, adt, kchunk, roe, nv0, s);
-    else if (les) launch1<true, false, false>(c, F, istage, alfa, beta, adt, kchunk, roe, nv0, s);
-    else if (visc) launch1<false, true, false>(c, F, istage, alfa, beta, adt, kchunk, roe, nv0, s);
-    else launch1<false, false, false>(c, F, istage, alfa, beta, adt, kchunk, roe, nv0, s);
+    if (les && visc) launch1<true, true, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, s);
+    else if (les) launch1<true, false, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, s);
+    else if (visc) launch1<false, true, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, s);
+    else launch1<false, false, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, s);
   }
   return cudaGetLastError();
 }

@@ -250,6 +250,13 @@ __device__ __forceinline__ void roe(const R QL[5], const R QR[5], R pL, R pR, co
 // DIR >= 0: the face direction as a compile-time constant, so every stencil
 // shift, stride and metric selection folds into fixed offsets; DIR = -1: the
 // direction is the runtime argument drt (one copy of the code for all three).
+// FLUX bits: FLUX_ROE selects Roe's flux instead of Rusanov's.  With the
+// sensor off the LES blend weight is the option value s_x = s_y = s_z on
+// every face; the host sets FLUX_SIGMA1 when it is 1 and FLUX_SIGMA0 when it
+// is 0, and the face then skips the part the blend multiplies by exactly
+// zero: (1 - 1) * Fw + 1 * Fc = Fc and (1 - 0) * Fw + 0 * Fc = Fw for finite
+// fluxes (the sign of a zero flux aside), so the result is the reference's.
+constexpr int FLUX_ROE = 1, FLUX_SIGMA1 = 2, FLUX_SIGMA0 = 4;
 template <typename R, bool MIX, bool LES, int BX, int BY, int DIR, int FLUX = 0, bool NV0 = false>
 __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a,
                                           int gi, int gj, int gk, int drt, R Fc[5]) {
@@ -277,79 +284,86 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
     P[s] = Rg.get(F_P, n);
   }
 
-  R QL[5], QR[5], pL, pR;
-  const int fo = c.fluxorder;
-  bool first;
-  if (LES) {
-    double nsum2 = (d == 2) ? nv0 + (NV0 ? 0.0 : ldg(F.nvert + gidx(c, 1, gj, gk + 1))) : nv0 + nv1;  // quirk rhs.c:4046
-    first = fo == 1 || ((pos == 0 || pos == m - 2) && bc_lo(c, d) != 7) || nsum2 > BLANKWALL;
-  } else {
-    first = fo == 1 || pos == 0 || pos == m - 2 || (nv0 + nv1) > BLANKWALL;
-  }
-  int iso_case = 0;
-  if (!LES && d == 1 && c.isothermal) {
-    if (gj == 0 && c.bctype[2] == 1) iso_case = 1;           // rhs.c:2822
-    else if (gj == m - 2 && c.bctype[3] == 1) iso_case = 2;  // rhs.c:2828
-  }
-  if (iso_case == 1) {
+  constexpr bool ROE = (FLUX & FLUX_ROE) != 0;
+  constexpr bool CEN_ONLY = LES && (FLUX & FLUX_SIGMA1) != 0;
+  constexpr bool UPW_ONLY = LES && (FLUX & FLUX_SIGMA0) != 0;
+  R Fw[5], Ufw = R(0);
 #pragma unroll
-    for (int q = 0; q < 5; q++) QL[q] = QR[q] = Q[1][q];
-    pL = pR = P[1];
-  } else if (iso_case == 2) {
-#pragma unroll
-    for (int q = 0; q < 5; q++) QL[q] = QR[q] = Q[2][q];
-    pL = pR = P[2];
-  } else if (first) {
-#pragma unroll
-    for (int q = 0; q < 5; q++) { QL[q] = Q[1][q]; QR[q] = Q[2][q]; }
-    pL = P[1]; pR = P[2];
-  } else if (fo == 2 || (!LES && d > 0 && gj < 30 && gk < 7)) {  // quirk rhs.c:2840, 2997
-    const bool wm = nvm > BLANKWALL;  // qm = q[i+1] when i-1 is a wall
-    const bool wp = nv2 > BLANKWALL;  // qp = q[i] when i+2 is a wall
-#pragma unroll
-    for (int q = 0; q < 5; q++) {
-      QL[q] = muscl_l(wm ? Q[2][q] : Q[0][q], Q[1][q], Q[2][q]);
-      QR[q] = muscl_r(Q[1][q], Q[2][q], wp ? Q[1][q] : Q[3][q]);
-    }
-    pL = muscl_l(wm ? P[2] : P[0], P[1], P[2]);
-    pR = muscl_r(P[1], P[2], wp ? P[1] : P[3]);
-  } else {
-    const int ord = c.eno_order;
-    const bool el = nvm > BLANKWALL && (d != 0 || (gi + 2) < c.mx);
-    const bool er = nv2 > BLANKWALL;
-    if (el) {
-#pragma unroll
-      for (int q = 0; q < 5; q++) QL[q] = eno_l(Q[1][q], Q[2][q], Q[3][q], ord);
-      pL = eno_l(P[1], P[2], P[3], ord);
+  for (int q = 0; q < 5; q++) Fw[q] = R(0);
+  if constexpr (!CEN_ONLY) {  // reconstruction and the upwind flux
+    R QL[5], QR[5], pL, pR;
+    const int fo = c.fluxorder;
+    bool first;
+    if (LES) {
+      double nsum2 = (d == 2) ? nv0 + (NV0 ? 0.0 : ldg(F.nvert + gidx(c, 1, gj, gk + 1))) : nv0 + nv1;  // quirk rhs.c:4046
+      first = fo == 1 || ((pos == 0 || pos == m - 2) && bc_lo(c, d) != 7) || nsum2 > BLANKWALL;
     } else {
-#pragma unroll
-      for (int q = 0; q < 5; q++) QL[q] = weno3_l(Q[0][q], Q[1][q], Q[2][q]);
-      pL = weno3_l(P[0], P[1], P[2]);
-      if (!LES && d == 1 && gj == 1 && c.isothermal && c.bctype[2] == 1) {  // rhs.c:2926
-        QL[0] = eno_l(Q[1][0], Q[2][0], Q[3][0], ord);
-        QL[4] = eno_l(Q[1][4], Q[2][4], Q[3][4], ord);
+      first = fo == 1 || pos == 0 || pos == m - 2 || (nv0 + nv1) > BLANKWALL;
+    }
+    int iso_case = 0;
+    if (!LES && d == 1 && c.isothermal) {
+      if (gj == 0 && c.bctype[2] == 1) iso_case = 1;           // rhs.c:2822
+      else if (gj == m - 2 && c.bctype[3] == 1) iso_case = 2;  // rhs.c:2828
+    }
+    if (iso_case == 1) {
+  #pragma unroll
+      for (int q = 0; q < 5; q++) QL[q] = QR[q] = Q[1][q];
+      pL = pR = P[1];
+    } else if (iso_case == 2) {
+  #pragma unroll
+      for (int q = 0; q < 5; q++) QL[q] = QR[q] = Q[2][q];
+      pL = pR = P[2];
+    } else if (first) {
+  #pragma unroll
+      for (int q = 0; q < 5; q++) { QL[q] = Q[1][q]; QR[q] = Q[2][q]; }
+      pL = P[1]; pR = P[2];
+    } else if (fo == 2 || (!LES && d > 0 && gj < 30 && gk < 7)) {  // quirk rhs.c:2840, 2997
+      const bool wm = nvm > BLANKWALL;  // qm = q[i+1] when i-1 is a wall
+      const bool wp = nv2 > BLANKWALL;  // qp = q[i] when i+2 is a wall
+  #pragma unroll
+      for (int q = 0; q < 5; q++) {
+        QL[q] = muscl_l(wm ? Q[2][q] : Q[0][q], Q[1][q], Q[2][q]);
+        QR[q] = muscl_r(Q[1][q], Q[2][q], wp ? Q[1][q] : Q[3][q]);
+      }
+      pL = muscl_l(wm ? P[2] : P[0], P[1], P[2]);
+      pR = muscl_r(P[1], P[2], wp ? P[1] : P[3]);
+    } else {
+      const int ord = c.eno_order;
+      const bool el = nvm > BLANKWALL && (d != 0 || (gi + 2) < c.mx);
+      const bool er = nv2 > BLANKWALL;
+      if (el) {
+  #pragma unroll
+        for (int q = 0; q < 5; q++) QL[q] = eno_l(Q[1][q], Q[2][q], Q[3][q], ord);
         pL = eno_l(P[1], P[2], P[3], ord);
+      } else {
+  #pragma unroll
+        for (int q = 0; q < 5; q++) QL[q] = weno3_l(Q[0][q], Q[1][q], Q[2][q]);
+        pL = weno3_l(P[0], P[1], P[2]);
+        if (!LES && d == 1 && gj == 1 && c.isothermal && c.bctype[2] == 1) {  // rhs.c:2926
+          QL[0] = eno_l(Q[1][0], Q[2][0], Q[3][0], ord);
+          QL[4] = eno_l(Q[1][4], Q[2][4], Q[3][4], ord);
+          pL = eno_l(P[1], P[2], P[3], ord);
+        }
+      }
+      if (er) {
+  #pragma unroll
+        for (int q = 0; q < 5; q++) QR[q] = eno_r(Q[0][q], Q[1][q], Q[2][q], ord);
+        pR = eno_r(P[0], P[1], P[2], ord);
+      } else {
+  #pragma unroll
+        for (int q = 0; q < 5; q++) QR[q] = weno3_r(Q[1][q], Q[2][q], Q[3][q]);
+        pR = weno3_r(P[1], P[2], P[3]);
       }
     }
-    if (er) {
-#pragma unroll
-      for (int q = 0; q < 5; q++) QR[q] = eno_r(Q[0][q], Q[1][q], Q[2][q], ord);
-      pR = eno_r(P[0], P[1], P[2], ord);
+    if (LES) {
+      if (ROE) roe<R, MIX>(QL, QR, pL, pR, h, false, false, pref, href, Fw, Ufw);
+      else rusanov<R, MIX>(QL, QR, pL, pR, h, false, false, pref, Fw, Ufw);
     } else {
-#pragma unroll
-      for (int q = 0; q < 5; q++) QR[q] = weno3_r(Q[1][q], Q[2][q], Q[3][q]);
-      pR = weno3_r(P[1], P[2], P[3]);
+      const bool use_qr_l = (pos == m - 2 && bc_hi(c, d) == 1);
+      const bool r_from_l = (pos == 0 && bc_lo(c, d) == 1);
+      if (ROE) roe<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, href, Fw, Ufw);
+      else rusanov<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, Fw, Ufw);
     }
-  }
-  R Fw[5], Ufw;
-  if (LES) {
-    if (FLUX == 1) roe<R, MIX>(QL, QR, pL, pR, h, false, false, pref, href, Fw, Ufw);
-    else rusanov<R, MIX>(QL, QR, pL, pR, h, false, false, pref, Fw, Ufw);
-  } else {
-    const bool use_qr_l = (pos == m - 2 && bc_hi(c, d) == 1);
-    const bool r_from_l = (pos == 0 && bc_lo(c, d) == 1);
-    if (FLUX == 1) roe<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, href, Fw, Ufw);
-    else rusanov<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, Fw, Ufw);
   }
   if (!LES) {
 #pragma unroll
@@ -358,6 +372,12 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
     return;
   }
 
+  if constexpr (UPW_ONLY) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) Fc[q] = Fw[q];
+    if (MIX) Fc[4] += href * Ufw;
+    return;
+  }
   // central flux (rhs.c:3483-3547) and blend
   R Fcen[5], Ufc;
   bool four = false;
@@ -404,6 +424,12 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
     Fcen[3] = wc * Uc + pa * h[2];
     Fcen[4] = Uc * (ec + pa);
     Ufc = MIX ? Uc : R(0);
+  }
+  if constexpr (CEN_ONLY) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) Fc[q] = Fcen[q];
+    if (MIX) Fc[4] += href * Ufc;
+    return;
   }
   const R sigma = R(sigma_at(c, F, d, gi, gj, gk));
 #pragma unroll
@@ -878,6 +904,32 @@ __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
   extern __shared__ double smem_d[];
   stage_tile<R, MIX, LES, VISC, RHS_MODE, FLUX, NV0>(c, F, blockIdx.x, blockIdx.y, blockIdx.z, istage, alfa, beta, adt,
                                                     kchunk, smem_d);
+}
+
+// The time-step kernel without nvert (NV0) for FLUX bits fl: Roe, and with
+// LES the constant-sigma variants; fl outside them runs the general blend.
+using StageKern = void (*)(const DevCfg, const DevFields, int, double, double, double, int);
+template <typename R, bool MIX, bool LES, bool VISC>
+StageKern stage_nv0_kernel(int fl) {
+  if constexpr (LES) {
+    switch (fl) {
+      case 1: return stage_kernel<R, MIX, LES, VISC, false, 1, true>;
+      case 2: return stage_kernel<R, MIX, LES, VISC, false, 2, true>;
+      case 3: return stage_kernel<R, MIX, LES, VISC, false, 3, true>;
+      case 4: return stage_kernel<R, MIX, LES, VISC, false, 4, true>;
+      case 5: return stage_kernel<R, MIX, LES, VISC, false, 5, true>;
+      default: return stage_kernel<R, MIX, LES, VISC, false, 0, true>;
+    }
+  } else {
+    return (fl & FLUX_ROE) ? stage_kernel<R, MIX, LES, VISC, false, 1, true> : stage_kernel<R, MIX, LES, VISC, false, 0, true>;
+  }
+}
+template <typename R, bool MIX, bool LES, bool VISC>
+cudaError_t stage_nv0_attrs(int smem) {
+  cudaError_t e = cudaSuccess;
+  for (int fl = 0; fl < (LES ? 6 : 2) && e == cudaSuccess; fl++)
+    e = cudaFuncSetAttribute(stage_nv0_kernel<R, MIX, LES, VISC>(fl), cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return e;
 }
 
 // ------------------------------------------------------- batched form ----

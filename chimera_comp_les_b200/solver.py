@@ -41,7 +41,9 @@ _OPT_MAP = {
     "-Ma": ("ma", float), "-Pr": ("pr", float), "-gamma": ("gamma", float), "-dt": ("dt", float),
     "-calc_sigma": ("calc_sigma", int), "-s_x_min": ("s_x_min", float), "-s_y_min": ("s_y_min", float),
     "-s_z_min": ("s_z_min", float), "-sigma_thrsh": ("sigma_thrsh", float), "-max_cs": ("max_cs", float),
-    "-Twall": ("twall", float), "-twoD": ("twod", int),
+    "-Twall": ("twall", float), "-twoD": ("twod", int), "-i_homo_filter": ("i_homo_filter", int),
+    "-j_homo_filter": ("j_homo_filter", int), "-k_homo_filter": ("k_homo_filter", int),
+    "-testfilter_ik": ("testfilter_ik", int),
 }
 
 
@@ -62,7 +64,8 @@ class Block:
                  dt: float = 0.01, st: float = 1.0, cs_const: float = 0.03, ci: float = 0.06,
                  ratio: float = 0.0, precision: str = "fp64", device: int = 0, calc_sigma: int = 0,
                  s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5,
-                 flux: str = "rusanov", max_cs: float = 0.05, twall: float = 1.0, twod: int = 0):
+                 flux: str = "rusanov", max_cs: float = 0.05, twall: float = 1.0, twod: int = 0,
+                 i_homo_filter: int = 0, j_homo_filter: int = 0, k_homo_filter: int = 0, testfilter_ik: int = 0):
         self.lib = _lib.load()
         cfg = CbConfig()
         self.lib.cb_config_default(C.byref(cfg), mx, my, mz)
@@ -71,7 +74,9 @@ class Block:
                          isothermal=isothermal, s_x=s_x, s_y=s_y, s_z=s_z, ren=ren, ma=ma, pr=pr, gamma=gamma,
                          dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device, calc_sigma=calc_sigma,
                          s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh,
-                         max_cs=max_cs, twall=twall, twod=twod).items():
+                         max_cs=max_cs, twall=twall, twod=twod, i_homo_filter=i_homo_filter,
+                         j_homo_filter=j_homo_filter, k_homo_filter=k_homo_filter,
+                         testfilter_ik=testfilter_ik).items():
             setattr(cfg, k, v)
         cfg.flux = {"rusanov": 0, "roe": 1}[flux] if isinstance(flux, str) else int(flux)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]

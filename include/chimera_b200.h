@@ -52,8 +52,11 @@ extern "C" {
 typedef struct {
   int mx, my, mz;       /* -im/-jm/-km (DMDA node counts) */
   int bctype[6];        /* bcs.dat: i-lo,i-hi,j-lo,j-hi,k-lo,k-hi; 7 = periodic */
-  int les;              /* -les     : 0 off, 1 constant Smagorinsky, 2 dynamic Smagorinsky (single-block
-                           contexts; Compute_Smagorinsky_Constant_1, les.c:151-1472) */
+  int les;              /* -les     : 0 off, 1 constant Smagorinsky, 2 (and every other value but 3
+                           and 10) dynamic Smagorinsky with local averaging, 3 dynamic node by
+                           node, 10 the LES terms without a model (nu_t stays 0); the dynamic
+                           forms in single-block contexts only (Compute_Smagorinsky_Constant_1,
+                           les.c:134-1472; solvers.c:28) */
   int inviscid;         /* -inv     : 1 skips formViscous */
   int fluxorder;        /* -fluxorder: 1 first order, 2 MUSCL-minmod, 3 WENO3; also the RK stage count */
   int eno_order;        /* -ENOorder: 2 or 3 */
@@ -82,6 +85,12 @@ typedef struct {
                            (-isothermal 2 with j-wall code 1; rhs.c:486, default 1) */
   int twod;             /* -twoD: 1 drops that wall's x-velocity term (rhs.c:724); the immersed
                            boundary takes its own value from cb_ibm_set_options */
+  int i_homo_filter, j_homo_filter, k_homo_filter;
+                        /* -i/-j/-k_homo_filter: homogeneous averaging of the dynamic model's LM and
+                           MM (les.c:916-1115): i alone per (k, j) line, i and k per j plane, all
+                           three over the box; j or k alone only takes LM / MM node by node */
+  int testfilter_ik;    /* -testfilter_ik: test-filter width 5^(1/3) instead of 2 filter widths
+                           (les.c:598) */
 } cb_config;
 
 /* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */

@@ -72,6 +72,10 @@ class Config:
     immersed: int = 0      # -imm: run the IB interpolation after the stages (solvers.c:282-288)
     wallfunction: int = 0  # -wallfunction: 0 noslip, 3 freeslip at IB nodes
     twoD: int = 0          # -twoD: 1/2/3 drops x/y/z from the IB normal and velocity
+    i_homo_filter: int = 0  # -i/-j/-k_homo_filter: homogeneous averaging of the dynamic model (les.c:916-1115)
+    j_homo_filter: int = 0
+    k_homo_filter: int = 0
+    testfilter_ik: int = 0  # -testfilter_ik: test-filter width 5^(1/3) filter widths (les.c:598)
 
     def ref_options(self) -> str:
         o = [
@@ -87,6 +91,8 @@ class Config:
             ("-calc_sigma", self.calc_sigma), ("-s_x_min", repr(float(self.s_x_min))),
             ("-s_y_min", repr(float(self.s_y_min))), ("-s_z_min", repr(float(self.s_z_min))),
             ("-sigma_thrsh", repr(float(self.sigma_thrsh))),
+            ("-i_homo_filter", self.i_homo_filter), ("-j_homo_filter", self.j_homo_filter),
+            ("-k_homo_filter", self.k_homo_filter), ("-testfilter_ik", self.testfilter_ik),
         ]
         return " ".join(f"{k} {v}" for k, v in o)
 
@@ -110,6 +116,8 @@ class _CCfg(C.Structure):
         ("ratio", C.c_double), ("calc_sigma", C.c_int),
         ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double), ("sigma_thrsh", C.c_double),
         ("flux", C.c_int), ("max_cs", C.c_double), ("twall", C.c_double), ("twod", C.c_int),
+        ("i_homo_filter", C.c_int), ("j_homo_filter", C.c_int), ("k_homo_filter", C.c_int),
+        ("testfilter_ik", C.c_int),
     ]
 
 

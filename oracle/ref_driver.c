@@ -105,12 +105,19 @@ static void read_globals_from_options(void) {
   PetscOptionsGetInt(NULL, NULL, "-calc_sigma", &calc_sigma, NULL);
   PetscOptionsGetInt(NULL, NULL, "-wallfunction", &wallfunction, NULL);
   PetscOptionsGetInt(NULL, NULL, "-thin", &thin, NULL);
+  PetscOptionsGetInt(NULL, NULL, "-clark", &clark, NULL);
+  PetscOptionsGetInt(NULL, NULL, "-testfilter_ik", &testfilter_ik, NULL);
+  PetscOptionsGetInt(NULL, NULL, "-testfilter_1d", &testfilter_1d, NULL);
+  PetscOptionsGetInt(NULL, NULL, "-i_homo_filter", &i_homo_filter, NULL);
+  PetscOptionsGetInt(NULL, NULL, "-j_homo_filter", &j_homo_filter, NULL);
+  PetscOptionsGetInt(NULL, NULL, "-k_homo_filter", &k_homo_filter, NULL);
 }
 
 static void reset_globals(void) {
   tistart = 0; rstart_flg = PETSC_FALSE; immersed = 0; wavy = 0; isothermal = 0;
   calc_sigma = 0; invicid = 0; TwoD = 0; central = 2; les = 0; rans = 0; channel = 0;
-  wallfunction = 0; thin = 0;
+  wallfunction = 0; thin = 0; clark = 0; testfilter_ik = 0; testfilter_1d = 0;
+  i_homo_filter = 0; j_homo_filter = 0; k_homo_filter = 0;
 }
 
 static void ibm_free(void) {

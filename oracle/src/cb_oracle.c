@@ -1244,12 +1244,12 @@ int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const
   if (c->les && !c->calc_sigma) cbo_sigma(c, sig);
   int err = 0;
   for (int step = 0; step < nsteps && !err; step++) {
-    if (c->les == 2 && !c->inviscid) { /* Compute_Smagorinsky_Constant_1 -les 2, then the eddy viscosity */
+    if (cbo_les_dynamic(c) && !c->inviscid) { /* Compute_Smagorinsky_Constant_1 (dynamic), then the eddy viscosity */
       const double *const *qu = *have_uc ? (const double *const *)quc : NULL;
       cbo_eos(c, (const double *const *)q, pbuf);
       cbo_dynamic_smagorinsky(c, (const double *const *)q, qu, pbuf, csi, eta, zet, aj, nvert, csbuf);
       cbo_eddy_viscosity_dyn(c, (const double *const *)q, qu, csi, eta, zet, aj, nvert, csbuf, nut);
-    } else if (c->les && !c->inviscid)
+    } else if (c->les && c->les != 10 && !c->inviscid) /* solvers.c:28: no model at all with -les 10 */
       cbo_eddy_viscosity(c, *have_uc ? (const double *const *)quc : NULL, csi, eta, zet, aj, nvert, nut);
     for (int s = 0; s < ns && !err; s++) {
       if (c->les && c->calc_sigma && s == 0) cbo_sigma_sensor(c, (const double *const *)q, sig); /* istage 0 */
@@ -1385,11 +1385,11 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
   if (c->fluxorder < 3) al[1] = 1 / 2.;
   int err = 0;
   for (int step = 0; step < nsteps && !err; step++) {
-    if (c->les == 2 && !c->inviscid) { /* the dynamic model reads lP only for beta, which feeds nothing */
+    if (cbo_les_dynamic(c) && !c->inviscid) { /* the dynamic model reads lP only for beta, which feeds nothing */
       const double *const *qu = *have_uc ? (const double *const *)quc : NULL;
       cbo_dynamic_smagorinsky(c, (const double *const *)q, qu, lp, csi, eta, zet, aj, nvert, csbuf);
       cbo_eddy_viscosity_dyn(c, (const double *const *)q, qu, csi, eta, zet, aj, nvert, csbuf, nut);
-    } else if (c->les && !c->inviscid)
+    } else if (c->les && c->les != 10 && !c->inviscid) /* solvers.c:28: no model at all with -les 10 */
       cbo_eddy_viscosity(c, *have_uc ? (const double *const *)quc : NULL, csi, eta, zet, aj, nvert, nut);
     for (int s = 0; s < ns && !err; s++) {
       const double *lps = (s == 0 && *lp_valid) ? lp : NULL;
@@ -1475,13 +1475,78 @@ static double dyn_u(const geom *G, const double *const q[5], const double *const
   return quc ? quc[1 + a][m] / quc[0][m] : 0.0;
 }
 
+/* Homogeneous averaging of LM and MM before the clipping (les.c:934-1115), as
+ * one rank sums them: running sums in k, j, i loop order.
+ *  - i and k: per j plane over the fluid interior (nvert < 0.1) nodes; every
+ *    interior node of the plane gets 0.5 <LM> / (<MM> + eps);
+ *  - i without k: per (k, j) line along i, written at fluid interior nodes;
+ *  - i, j and k: afterwards, sum LM / sum MM over every interior node
+ *    (no mask, no eps, no 0.5) on every node of the box.
+ * The j- and k-only branches of the reference are commented out: those
+ * filters only make LM / MM pointwise. */
+static void dyn_homogeneous(const cbo_config *c, const geom *G, const double *nvert, const double *LM,
+                            const double *MM, double *cs) {
+  const int mx = G->m[0], my = G->m[1], mz = G->m[2];
+  if (c->i_homo_filter && c->k_homo_filter) {
+    double *lm = (double *)calloc((size_t)my * 2, sizeof(double)), *mm = lm + my;
+    int *cnt = (int *)calloc((size_t)my, sizeof(int));
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++)
+        for (int i = 1; i < mx - 1; i++) {
+          const ptrdiff_t n = IX(G, i, j, k);
+          if (nvert[n] < 0.1) { lm[j] += LM[n]; mm[j] += MM[n]; cnt[j]++; }
+        }
+    for (int j = 0; j < my; j++)
+      if (cnt[j] > 0) { lm[j] /= (double)cnt[j]; mm[j] /= (double)cnt[j]; }
+    for (int j = 1; j < my - 1; j++)
+      for (int k = 1; k < mz - 1; k++)
+        for (int i = 1; i < mx - 1; i++) cs[IX(G, i, j, k)] = 0.5 * lm[j] / (mm[j] + DYN_EPS);
+    free(lm);
+    free(cnt);
+  }
+  if (c->i_homo_filter && !c->k_homo_filter) {
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++) {
+        double lm = 0.0, mm = 0.0;
+        int cnt = 0;
+        for (int i = 1; i < mx - 1; i++) {
+          const ptrdiff_t n = IX(G, i, j, k);
+          if (nvert[n] < 0.1) { lm += LM[n]; mm += MM[n]; cnt++; }
+        }
+        if (cnt > 0) { lm /= (double)cnt; mm /= (double)cnt; }
+        for (int i = 1; i < mx - 1; i++) {
+          const ptrdiff_t n = IX(G, i, j, k);
+          if (nvert[n] < 0.1) cs[n] = 0.5 * lm / (mm + DYN_EPS);
+        }
+      }
+  }
+  if (c->i_homo_filter && c->j_homo_filter && c->k_homo_filter) {
+    double lm = 0.0, mm = 0.0;
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++)
+        for (int i = 1; i < mx - 1; i++) {
+          const ptrdiff_t n = IX(G, i, j, k);
+          mm += MM[n];
+          lm += LM[n];
+        }
+    for (int k = 0; k < mz; k++)
+      for (int j = 0; j < my; j++)
+        for (int i = 0; i < mx; i++) cs[IX(G, i, j, k)] = lm / mm;
+  }
+}
+
+int cbo_les_dynamic(const cbo_config *c) { return c->les >= 2 && c->les != 10; }
+
 int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const double *const quc[5],
                             const double *lp, const double *const csi[3], const double *const eta[3],
                             const double *const zet[3], const double *aj, const double *nvert, double *cs) {
   const double max_cs = c->max_cs;
   geom G = mkgeom(c);
   const int mx = G.m[0], my = G.m[1], mz = G.m[2];
-  if (c->les != 2) return 5;
+  if (!cbo_les_dynamic(c)) return 5;
+  /* -les 3 and the homogeneous filters take LM / MM node by node and skip
+   * the final 1/aj-weighted mean (les.c:916-922, 1302) */
+  const int pointwise = c->i_homo_filter || c->j_homo_filter || c->k_homo_filter || c->les == 3;
   double *buf = (double *)calloc(G.n * 13, sizeof(double));
   double *A[9], *Sabs = buf + 9 * G.n, *LM = buf + 10 * G.n, *MM = buf + 11 * G.n, *ct = buf + 12 * G.n;
   for (int a = 0; a < 9; a++) A[a] = buf + a * G.n; /* du_dx du_dy du_dz dv_dx .. dw_dz */
@@ -1561,7 +1626,7 @@ int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const
             }
         (void)pu; (void)pv; (void)pw; (void)pp; /* beta (les.c:578-581) feeds nothing downstream */
         const double filter = pow(1. / aj[n], 1. / 3.);
-        const double test_filter = 2.0 * filter;
+        const double test_filter = c->testfilter_ik ? pow(5.0, 1. / 3.) * filter : 2.0 * filter; /* les.c:598-601 */
         const double _rho = itf(rho, w), _rhou = itf(ru, w), _rhov = itf(rv, w), _rhow = itf(rw, w);
         double Lij[3][3];
         Lij[0][0] = itf(ruu, w) - _rhou * _rhou / _rho;
@@ -1603,16 +1668,22 @@ int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const
         const ptrdiff_t n = IX(&G, i, j, k);
         if (nvert[n] > 1.1) { cs[n] = 0; continue; }
         double lm = 0.0, mm = 0.0; /* integrate_t (les.c:66-78) */
-        for (int R = 0; R < 3; R++)
-          for (int Q = 0; Q < 3; Q++)
-            for (int P = 0; P < 3; P++) {
-              const ptrdiff_t m = IX(&G, i + P - 1, j + Q - 1, k + R - 1);
-              lm += LM[m] / 27.0;
-              mm += MM[m] / 27.0;
-            }
+        if (pointwise) {
+          lm = LM[n];
+          mm = MM[n];
+        } else {
+          for (int R = 0; R < 3; R++)
+            for (int Q = 0; Q < 3; Q++)
+              for (int P = 0; P < 3; P++) {
+                const ptrdiff_t m = IX(&G, i + P - 1, j + Q - 1, k + R - 1);
+                lm += LM[m] / 27.0;
+                mm += MM[m] / 27.0;
+              }
+        }
         const double C = lm / (mm + DYN_EPS);
         cs[n] = (C < 0.0001) ? 0.0001 : C;
       }
+  dyn_homogeneous(c, &G, nvert, LM, MM, cs);
   /* (4) clipping on every owned node (les.c:1124-1137; its face tests compare
    * !bctype with 7 and never hold) */
   for (int k = 0; k < mz; k++)
@@ -1626,6 +1697,10 @@ int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const
       }
   /* (5) lCS with its periodic copies, then the 1/aj-weighted mean over the
    * 27 nodes around fluid interior nodes (les.c:1207-1333) */
+  if (pointwise) {
+    free(buf);
+    return 0;
+  }
   memcpy(ct, cs, G.n * sizeof(double));
   cbo_fill_ghosts(c, ct);
   dyn_periodic_copies(c, &G, ct);

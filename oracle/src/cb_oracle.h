@@ -23,7 +23,8 @@ extern "C" {
 typedef struct {
   int mx, my, mz;          /* DMDA node counts including boundary nodes 0 and m-1 */
   int bctype[6];           /* bcs.dat codes, 7 = periodic */
-  int les;                 /* -les: 0 off, 1 constant Smagorinsky */
+  int les;                 /* -les: 0 off, 1 constant Smagorinsky, 3 dynamic node by node, 10 no model,
+                              other values dynamic with local averaging */
   int inviscid;            /* -inv */
   int fluxorder;           /* -fluxorder: 1 first order, 2 MUSCL, 3 WENO3 */
   int eno_order;           /* -ENOorder */
@@ -41,6 +42,9 @@ typedef struct {
   double max_cs;           /* -max_cs: upper clip of the dynamic Smagorinsky coefficient (default 0.05) */
   double twall;            /* -Twall: wall temperature of the characteristic isothermal wall (default 1) */
   int twod;                /* -twoD: 1 drops the x velocity term of that wall (and x in the IB) */
+  int i_homo_filter, j_homo_filter, k_homo_filter; /* -i/-j/-k_homo_filter: homogeneous averaging of the
+                              dynamic model's LM and MM (les.c:916-1115) */
+  int testfilter_ik;       /* -testfilter_ik: test-filter width 5^(1/3) instead of 2 filter widths (les.c:598) */
 } cbo_config;
 
 /* Fill the two ghost layers of each periodic direction of one padded plane
@@ -156,11 +160,17 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
                   const cbo_ibm_info *const *lists, const double *const coor[3], double *lp, int *lp_valid,
                   int twoD, int wallfunction);
 
-/* Compute_Smagorinsky_Constant_1 with -les 2 (les.c:151-1472, the default
- * 3-D box test filter with local averaging): Cs per node into cs (global CS,
- * in/out: boundary nodes keep their value through the clipping) from the
- * ghosted current state q, the state quc of the last CalcUCat (NULL: zero
- * velocity) and the local pressure lp.  Returns 5 unless les == 2. */
+/* The dynamic model runs: -les >= 2 except 10 (les.c:138-146 single out 1
+ * and 10; solvers.c:28 skips the model with 10). */
+int cbo_les_dynamic(const cbo_config *c);
+
+/* Compute_Smagorinsky_Constant_1 with a dynamic -les (les.c:151-1472, the
+ * 3-D box test filter; local 27-node averaging, or LM / MM node by node with
+ * -les 3 or a homogeneous filter, which also adds the plane / line / box
+ * averages of -i/-j/-k_homo_filter): Cs per node into cs (global CS, in/out:
+ * boundary nodes keep their value through the clipping) from the ghosted
+ * current state q, the state quc of the last CalcUCat (NULL: zero velocity)
+ * and the local pressure lp.  Returns 5 unless cbo_les_dynamic. */
 int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const double *const quc[5],
                             const double *lp, const double *const csi[3], const double *const eta[3],
                             const double *const zet[3], const double *aj, const double *nvert, double *cs);

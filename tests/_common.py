@@ -36,12 +36,12 @@ def oracle_run(cfg, coords, q, nvert, steps=0):
     sig = ora.sigma(st["q"]) if cfg.les else None
     nut = ora.zeros(1)
     out = {"metrics": {k: O.from_padded(v) for k, v in met.items()}}
-    if cfg.les == 2 and not cfg.inviscid:  # CalcUCat on the same state, then the dynamic model
+    if cfg.les >= 2 and cfg.les != 10 and not cfg.inviscid:  # CalcUCat on the same state, then the dynamic model
         cs = ora.dynamic_smagorinsky(st["q"], st["q"], met, nvp)
         ora.eddy_viscosity_dyn(st["q"], st["q"], met, nvp, cs, nut)
         out["nut"] = O.from_padded(nut)[..., 0]
         out["cs"] = O.from_padded(cs)[..., 0]
-    elif cfg.les and not cfg.inviscid:
+    elif cfg.les and cfg.les != 10 and not cfg.inviscid:
         ora.eddy_viscosity(st["q"], met, nvp, nut)
         out["nut"] = O.from_padded(nut)[..., 0]
     out["rhs"] = O.from_padded(ora.rhs(st["q"], met, nvp, nut, sig))
@@ -60,7 +60,8 @@ def gpu_block(cfg, precision="fp64"):
                  pr=cfg.pr, gamma=cfg.gamma, dt=cfg.dt, st=cfg.st, cs_const=cfg.cs_const, ci=cfg.ci,
                  ratio=cfg.ratio, precision=precision, calc_sigma=cfg.calc_sigma, s_x_min=cfg.s_x_min,
                  s_y_min=cfg.s_y_min, s_z_min=cfg.s_z_min, sigma_thrsh=cfg.sigma_thrsh, flux=cfg.flux,
-                 max_cs=cfg.max_cs, twall=cfg.twall, twod=cfg.twoD)
+                 max_cs=cfg.max_cs, twall=cfg.twall, twod=cfg.twoD, i_homo_filter=cfg.i_homo_filter,
+                 j_homo_filter=cfg.j_homo_filter, k_homo_filter=cfg.k_homo_filter, testfilter_ik=cfg.testfilter_ik)
 
 
 def per_field_rel_l2(a, b):

@@ -183,3 +183,80 @@ def test_dynamic_smagorinsky_restatement_bitexact_vs_reference(n, kw, mask):
     st = o.initial_state(q1)
     o.steps(3, st, met, nvp)
     assert np.array_equal(O.from_padded(st["q"]), ref.Q())
+
+
+DYN_VARIANTS = [
+    ("les3_pointwise", dict(les=3)),
+    ("testfilter_ik", dict(testfilter_ik=1)),
+    ("i_homo_lines", dict(i_homo_filter=1)),
+    ("ik_homo_planes", dict(i_homo_filter=1, k_homo_filter=1)),
+    ("ijk_homo_box", dict(i_homo_filter=1, j_homo_filter=1, k_homo_filter=1)),
+    ("j_homo_pointwise", dict(j_homo_filter=1)),
+    ("k_homo_ik_filter", dict(k_homo_filter=1, testfilter_ik=1)),
+    ("les7_as_local", dict(les=7)),
+]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference sources not present")
+@pytest.mark.parametrize("name,kw", DYN_VARIANTS, ids=[v[0] for v in DYN_VARIANTS])
+def test_dynamic_variants_restatement_bitexact_vs_reference(name, kw):
+    """The dynamic model's other forms: -les 3 and the homogeneous filters take
+    LM / MM node by node and skip the final weighted mean (les.c:916, 1302);
+    -i_homo_filter averages along i lines, with -k_homo_filter over j planes,
+    with all three over the box (les.c:934-1115); -testfilter_ik widens the
+    test filter (les.c:598); other -les values >= 2 run the default model."""
+    from test_gpu_parity import _mask
+    n = (17, 15, 16)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    shape = coords.shape[:3]
+    base = dict(les=2, inviscid=0, ma=0.3, pr=0.71, dt=0.002, fluxorder=3, ren=700., max_cs=0.3)
+    base.update(kw)
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, **base)
+    # a turbulent field: its plane and box means of LM are positive, so the
+    # homogeneous coefficients survive the clipping
+    q1 = W.isotropic_turbulence(n, seed=2, k_peak=3.0, mach_t=0.3)
+    q2 = W.isotropic_turbulence(n, seed=2, k_peak=3.0, mach_t=0.31)
+    nv = _mask(shape, 9, True)
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q1)
+    ref.calc_ucat()
+    ref.set_state(q2)
+    ref.eddy_viscosity()
+    o = O.Oracle(cfg)
+    met = o.metrics(o.fill_ghosts(O.to_padded(cfg, coords)))
+    nvp = o.fill_ghosts(O.to_padded(cfg, nv))
+    qp1, qp2 = o.fill_ghosts(O.to_padded(cfg, q1)), o.fill_ghosts(O.to_padded(cfg, q2))
+    cs = o.dynamic_smagorinsky(qp2, qp1, met, nvp)
+    nut = o.eddy_viscosity_dyn(qp2, qp1, met, nvp, cs, o.zeros(1))
+    assert np.array_equal(O.from_padded(cs)[..., 0], ref.cs())
+    assert np.array_equal(O.from_padded(nut)[..., 0], ref.nut())
+    assert ref.cs()[nv < 0.1].max() > 0.01  # above the band floor
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q1)
+    ref.steps(3)
+    st = o.initial_state(q1)
+    o.steps(3, st, met, nvp)
+    assert np.array_equal(O.from_padded(st["q"]), ref.Q())
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference sources not present")
+def test_les10_runs_without_a_model_bitexact_vs_reference():
+    """-les 10: the LES forms of the right-hand side with nu_t left at zero
+    (solvers.c:28 calls neither the coefficient nor the eddy viscosity)."""
+    n = (15, 13, 14)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=10, inviscid=0, ma=0.3, pr=0.71, dt=0.002,
+                   fluxorder=3, ren=700.)
+    q = W.random_smooth_state(coords.shape[:3], seed=8)
+    ref = O.RefOracle(cfg, coords)
+    ref.set_state(q)
+    ref.steps(3)
+    o = O.Oracle(cfg)
+    met = o.metrics(o.fill_ghosts(O.to_padded(cfg, coords)))
+    nvp = o.fill_ghosts(O.to_padded(cfg, np.zeros(coords.shape[:3])))
+    st = o.initial_state(q)
+    o.steps(3, st, met, nvp)
+    assert np.array_equal(O.from_padded(st["q"]), ref.Q())
+    assert not np.array_equal(ref.Q(), q)
