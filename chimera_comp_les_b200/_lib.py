@@ -131,6 +131,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         ("cb_batch_rk_step", [P, I, I]), ("cb_batch_sync", [P]), ("cb_batch_autotune", [P, IP, D]),
         ("cb_batch_set_exchange", [P, I, C.c_longlong, IP, P, C.c_longlong, IP, P]),
         ("cb_batch_phase", [P, I, I, I]), ("cb_batch_phase_unpack", [P, I]),
+        ("cb_batch_cfl_dt", [P, C.c_double, D, D]),
     ]:
         f = getattr(lib, name)
         f.argtypes = args

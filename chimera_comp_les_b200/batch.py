@@ -275,6 +275,12 @@ class Batch:
         self._check(self.lib.cb_batch_download_state(self._b, k, dptr(out)))
         return out
 
+    def cfl_dt(self, cfl: float):
+        """(dt, lambda_max) for the CFL number `cfl` over every block."""
+        dt, lam = C.c_double(), C.c_double()
+        self._check(self.lib.cb_batch_cfl_dt(self._b, float(cfl), C.byref(dt), C.byref(lam)))
+        return dt.value, lam.value
+
     def metrics(self, k: int):
         """(csi, eta, zet, aj) of block k as resident on the device."""
         csi, eta, zet = (np.empty(self.shape(k) + (3,)) for _ in range(3))

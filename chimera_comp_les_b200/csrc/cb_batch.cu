@@ -518,6 +518,34 @@ int cb_batch_download_state(cb_batch *b, int k, double *q) {
   return CB_OK;
 }
 
+// CFL time step over every block of the batch: the largest spectral radius
+// aj * sum_d (|m_d . u| + c |m_d|) over the fluid interior nodes of all blocks
+// (atomicMax into one device word), dt = cfl / lambda_max.
+int cb_batch_cfl_dt(cb_batch *b, double cfl, double *dt, double *lambda_max) {
+  if (!b || !dt || !(cfl > 0)) return CB_E_ARG;
+  for (const auto &bh : b->blk)
+    if (!bh.have_grid || !bh.have_state) return bfail(b, CB_E_STATE, "every block needs its grid and state");
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(b->staging);  // free between calls
+  BCUDA(b, cudaMemsetAsync(d, 0, sizeof(unsigned long long), b->stream));
+  for (int k = 0; k < b->nb; k++) {
+    const BlockHost &bh = b->blk[k];
+    if (block_ptab(b, k)) return CB_E_CUDA;  // stream-ordered after the previous block's launch
+    const long long work = (long long)(bh.mx - 2) * (bh.my - 2) * (bh.mz - 2);
+    spectral_radius_kernel<<<bgrid(b, work), 256, 0, b->stream>>>(
+        bh.dc, (const double *const *)(b->ptab + 5 * b->cur), (const double *const *)(b->ptab + 15), b->aj + bh.off,
+        b->nvert + bh.off, d);
+    BCUDA(b, cudaGetLastError());
+  }
+  unsigned long long bits = 0;
+  BCUDA(b, cudaMemcpyAsync(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost, b->stream));
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  double lam;
+  std::memcpy(&lam, &bits, sizeof(lam));
+  if (lambda_max) *lambda_max = lam;
+  *dt = lam > 0 ? cfl / lam : 0.0;
+  return CB_OK;
+}
+
 static bool interior_node(const BlockHost &bh, int i, int j, int k) {
   return i >= 1 && i <= bh.mx - 2 && j >= 1 && j <= bh.my - 2 && k >= 1 && k <= bh.mz - 2;
 }

@@ -181,6 +181,30 @@ class Shard:
         return self._buf[kind]
 
 
+def reduce_max(x: float, group=None) -> float:
+    """Max of one scalar over the processes of ``group`` (one all_reduce; NCCL
+    on a CUDA tensor, gloo on a CPU one); x itself outside torch.distributed."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(x)
+    on_gpu = dist.get_backend(group) == "nccl"
+    dev = torch.device("cuda", torch.cuda.current_device()) if on_gpu else torch.device("cpu")
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
+
+
+def cfl_dt(shards, cfl: float, group=None):
+    """CFL time step of the whole domain: the largest spectral radius of this
+    process's shards (``Batch.cfl_dt``), then the max over processes.  Every
+    process gets the same (dt, lambda_max).  No reference counterpart: the
+    reference steps with the fixed -dt (init.c:94)."""
+    lam = max(sh.batch.cfl_dt(cfl)[1] for sh in shards)
+    lam = reduce_max(lam, group)
+    return (cfl / lam if lam > 0 else 0.0), lam
+
+
 def _run_phase(shards, transport, phase, stage, kind, nf, per_block):
     for sh in shards:
         sh.batch.phase(phase, stage, per_block)

@@ -298,6 +298,11 @@ int cb_batch_set_grid(cb_batch *b, int block, const double *coor);
 int cb_batch_set_nvert(cb_batch *b, int block, const double *nvert);
 int cb_batch_upload_state(cb_batch *b, int block, const double *q);
 int cb_batch_download_state(cb_batch *b, int block, double *q);
+/* CFL time step over all blocks: dt = cfl / (largest spectral radius of any
+ * block, as cb_cfl_dt computes it per block).  No reference counterpart (the
+ * reference steps with the fixed -dt, init.c:94); the multi-process form
+ * reduces lambda_max across ranks (chimera_comp_les_b200.sharded.cfl_dt). */
+int cb_batch_cfl_dt(cb_batch *b, double cfl, double *dt, double *lambda_max);
 /* metrics of a block as resident (csi, eta, zet 3 per node, aj 1), AoS */
 int cb_batch_get_metrics(cb_batch *b, int block, double *csi, double *eta, double *zet, double *aj);
 /* Halo maps: n entries of 9 ints (dst block, di, dj, dk, src block, si, sj,

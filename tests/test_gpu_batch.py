@@ -197,3 +197,24 @@ def test_halo_map_errors():
         with pytest.raises(ChimeraError) as e:
             bt.set_halo_map(B.HALO_WRAP, bad)
         assert e.value.code == CB_E_ARG
+
+
+def test_batch_cfl_dt_is_the_max_over_blocks():
+    """cb_batch_cfl_dt over three blocks equals the largest single-block
+    cb_cfl_dt radius, before and after steps (the current state buffer)."""
+    from chimera_comp_les_b200 import Block
+    inputs = _inputs(DIMS, seed0=5)
+    with _batch(DIMS, inputs) as bt:
+        bt.halo_periodic()
+        for steps in (0, 2):
+            if steps:
+                bt.RungeKutta(steps)
+            dt, lam = bt.cfl_dt(0.4)
+            lams = []
+            for k, (d, (coords, _)) in enumerate(zip(DIMS, inputs)):
+                with Block(*d, **OPTS) as blk:
+                    blk.FormMetrics(coords)
+                    blk.SetInitialCondition(bt.Q(k))
+                    lams.append(blk.cfl_dt(0.4)[1])
+            assert lam == max(lams) and lam > 0
+            assert dt == 0.4 / lam

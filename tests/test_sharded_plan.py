@@ -150,3 +150,52 @@ def test_plan_counts_are_symmetric():
     # every destination of the global map lands exactly once: locally or received
     total = sum(len(p.stage.local) + len(p.stage.recv) for p in plans)
     assert total == len(st)
+
+
+class _StubBatch:
+    """Stands in for a Batch: its own largest spectral radius."""
+
+    def __init__(self, lam):
+        self.lam = lam
+
+    def cfl_dt(self, cfl):
+        return cfl / self.lam, self.lam
+
+
+class _StubShard:
+    def __init__(self, lam):
+        self.batch = _StubBatch(lam)
+
+
+def _cfl_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # rank r holds two shards; the global largest radius sits on the last rank
+        shards = [_StubShard(1.0 + rank), _StubShard(0.5 + 2.0 * rank)]
+        q.put((rank,) + S.cfl_dt(shards, 0.4))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_cfl_dt_takes_the_global_max(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_cfl_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=240) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    lam = max(1.0 + (world - 1), 0.5 + 2.0 * (world - 1))
+    for rank, dt, got in res:
+        assert got == lam and dt == 0.4 / lam, rank
+
+
+def test_cfl_dt_without_a_process_group():
+    dt, lam = S.cfl_dt([_StubShard(2.0), _StubShard(3.0)], 0.3)
+    assert lam == 3.0 and dt == 0.3 / 3.0
