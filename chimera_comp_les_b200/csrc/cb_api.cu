@@ -199,9 +199,8 @@ static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, dou
   auto kern = c->dc.flux == 1 ? stage_kernel<double, false, LES, VISC, RHSM, 1> : stage_kernel<double, false, LES, VISC, RHSM, 0>;
   if constexpr (!RHSM)
     if (c->nv0) kern = stage_nv0_kernel<double, false, LES, VISC>(flux_bits(c));
-  const int nkin = c->dc.mz - 2;
-  dim3 grid((c->dc.mx - 2 + BX - 1) / BX, (c->dc.my - 2 + BY - 1) / BY, (nkin + c->kchunk - 1) / c->kchunk);
-  kern<<<grid, SNT, STAGE_SMEM_BYTES, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
+  kern<<<stage_grid(c->dc, c->kchunk, c->sms), SNT, STAGE_SMEM_BYTES, c->stream>>>(c->dc, F, istage, alfa, beta, adt,
+                                                                                c->kchunk);
   return cudaGetLastError();
 }
 
@@ -209,7 +208,7 @@ static cudaError_t launch_stage(cb_ctx *c, const DevFields &F, int istage, doubl
   const bool les = c->cfg.les != 0, visc = c->cfg.inviscid == 0;
   if (c->cfg.precision == CB_MIXED)
     return launch_stage_mixed(c->dc, F, istage, alfa, beta, adt, c->kchunk, les, visc, rhs_mode, flux_bits(c),
-                              c->nv0 && !rhs_mode, c->stream);
+                              c->nv0 && !rhs_mode, 2 * c->sms, c->stream);
   if (rhs_mode) {
     if (les && visc) return launch_stage_t<true, true, true>(c, F, istage, alfa, beta, adt);
     if (les) return launch_stage_t<true, false, true>(c, F, istage, alfa, beta, adt);
@@ -1044,7 +1043,7 @@ int cb_autotune(cb_ctx *c, int ncand, const int *cand, double *ms_out, int *nout
   const int nk = c->dc.mz - 2;
   if (ncand) {
     for (int t = 0; t < ncand; t++)
-      if (cand[t] < 1) return fail(c, CB_E_ARG, "k-chunk candidates must be positive");
+      if (cand[t] < 0) return fail(c, CB_E_ARG, "k-chunk candidates must be >= 0 (0: balanced segments)");
     cs.assign(cand, cand + ncand);
   } else {
     int last = -1;
@@ -1052,6 +1051,7 @@ int cb_autotune(cb_ctx *c, int ncand, const int *cand, double *ms_out, int *nout
       const int ch = (nk + kc - 1) / kc;
       if (ch != last) { cs.push_back(kc); last = ch; }
     }
+    cs.push_back(0);  // balanced segments, one range per resident CTA
   }
   const int in = c->cur;
   int out = (c->cur + 1) % 3;

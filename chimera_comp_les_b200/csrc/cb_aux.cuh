@@ -531,12 +531,30 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
     __syncthreads();  // the slot of plane k-1 is refilled next
   }
 }
-// k-chunk of the eddy-viscosity march: short chunks (many blocks, a short
-// tail wave); a chunk re-reads two velocity planes, a quarter of its q loads
+// k-chunk of the eddy-viscosity march: the fewest whole waves of resident
+// blocks, each chunk paying two extra velocity planes (cost = waves x
+// (chunk + 2)); the result does not depend on it
 static inline int eddy_kchunk(const DevCfg &c, int sms) {
-  (void)sms;
+  static int resident = 0;  // blocks per SM, from the occupancy calculator once per process
+  if (resident == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, eddy_viscosity_kernel, EDDY_BX * EDDY_BY, 0) != cudaSuccess ||
+        nb < 1)
+      nb = 1;
+    resident = nb;
+  }
   const int nk = c.mz - 2;
-  return nk < 8 ? nk : 8;
+  if (nk <= 4) return nk < 1 ? 1 : nk;
+  const long long tiles = (long long)((c.mx - 2 + EDDY_BX - 1) / EDDY_BX) * ((c.my - 2 + EDDY_BY - 1) / EDDY_BY);
+  const long long slots = (long long)(sms > 0 ? sms : 1) * resident;
+  int best = nk;
+  double bc = 1e300;
+  for (int kc = 4; kc <= nk; kc++) {
+    const long long blocks = tiles * ((nk + kc - 1) / kc);
+    const double cost = (double)((blocks + slots - 1) / slots) * (kc + 2);
+    if (cost < bc) { bc = cost; best = kc; }
+  }
+  return best;
 }
 static inline dim3 eddy_grid(const DevCfg &c, int kchunk) {
   return dim3((c.mx - 2 + EDDY_BX - 1) / EDDY_BX, (c.my - 2 + EDDY_BY - 1) / EDDY_BY, (c.mz - 2 + kchunk - 1) / kchunk);

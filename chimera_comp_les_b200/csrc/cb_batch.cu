@@ -760,7 +760,7 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
         if (cost < best) { best = cost; kc = cand; }
       }
       if (mixed) {
-        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, 0, bh.nvz, b->stream));
+        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, 0, bh.nvz, 2 * b->sms, b->stream));
       } else {
         dim3 grid(bh.tiles_x, bh.tiles_y, (nk + kc - 1) / kc);
         if (bh.nvz) f64_block_any<true>(les, visc, bh.dc, F, grid, s, alfa, beta, adt, kc, b->stream);

@@ -66,9 +66,9 @@ struct DevFields {
   const double *sig[3];    // hybrid weights per node (only with the shock sensor)
   double *rhs[5];          // formRHS output (rhs mode only)
   unsigned *status;        // sticky status word
-  // FP64 form: the pressure lP to read instead of the EqOfState of q (the
-  // first stage after an immersed step, whose FormBCS(user, 0) is followed by
-  // no EqOfState); nullptr: EqOfState of q
+  // the pressure lP to read instead of the EqOfState of q (the first stage
+  // after an immersed step, whose FormBCS(user, 0) is followed by no
+  // EqOfState); nullptr: EqOfState of q
   const double *pin;
 };
 

@@ -5,14 +5,25 @@
 #include <cuda_runtime.h>
 
 #include "cb_common.cuh"
+#include "cb_stage.cuh"
 
 namespace cb {
 
 cudaError_t set_stage_attrs_mixed();
+// Grid of a stage-kernel launch: (tile columns in i, in j, k-chunks) for
+// kchunk > 0; `slots` CTAs (the resident ones) for the balanced segments of
+// kchunk == 0.
+inline dim3 stage_grid(const DevCfg &c, int kchunk, int slots) {
+  if (kchunk <= 0) return dim3((unsigned)slots);
+  return dim3((c.mx - 2 + SBX - 1) / SBX, (c.my - 2 + SBY - 1) / SBY, (c.mz - 2 + kchunk - 1) / kchunk);
+}
+
 // fl: flux bits (FLUX_ROE; the constant-sigma bits apply with nv0 only);
-// nv0: nvert is zero everywhere, the variant without any nvert test (time step only)
+// nv0: nvert is zero everywhere, the variant without any nvert test (time step
+// only); slots: CTAs of the balanced-segment shape (kchunk 0)
 cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt,
-                               int kchunk, bool les, bool visc, bool rhs_mode, int fl, bool nv0, cudaStream_t s);
+                               int kchunk, bool les, bool visc, bool rhs_mode, int fl, bool nv0, int slots,
+                               cudaStream_t s);
 // FP32 metric vectors (w: filter width, aj, 0) and the FP64 metric divergence
 // (sum over directions of h(+1/2) - h(-1/2)) for the mixed form.
 cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, const double *aj,

@@ -20,9 +20,8 @@ cudaError_t attr1() {
 }
 template <bool LES, bool VISC, bool RHSM>
 void launch1(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt, int kchunk,
-             int fl, bool nv0, cudaStream_t s) {
-  const int nkin = c.mz - 2;
-  dim3 grid((c.mx - 2 + SBX - 1) / SBX, (c.my - 2 + SBY - 1) / SBY, (nkin + kchunk - 1) / kchunk);
+             int fl, bool nv0, int slots, cudaStream_t s) {
+  const dim3 grid = stage_grid(c, kchunk, slots);
   const bool roe = (fl & FLUX_ROE) != 0;
   auto kern = roe ? stage_kernel<float, true, LES, VISC, RHSM, 1> : stage_kernel<float, true, LES, VISC, RHSM, 0>;
   if constexpr (!RHSM)
@@ -69,17 +68,18 @@ cudaError_t set_stage_attrs_mixed() {
 }
 
 cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt,
-                               int kchunk, bool les, bool visc, bool rhs_mode, int fl, bool nv0, cudaStream_t s) {
+                               int kchunk, bool les, bool visc, bool rhs_mode, int fl, bool nv0, int slots,
+                               cudaStream_t s) {
   if (rhs_mode) {
-    if (les && visc) launch1<true, true, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, s);
-    else if (les) launch1<true, false, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, s);
-    else if (visc) launch1<false, true, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, s);
-    else launch1<false, false, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, s);
+    if (les && visc) launch1<true, true, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, slots, s);
+    else if (les) launch1<true, false, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, slots, s);
+    else if (visc) launch1<false, true, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, slots, s);
+    else launch1<false, false, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, slots, s);
   } else {
-    if (les && visc) launch1<true, true, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, s);
-    else if (les) launch1<true, false, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, s);
-    else if (visc) launch1<false, true, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, s);
-    else launch1<false, false, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, s);
+    if (les && visc) launch1<true, true, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, slots, s);
+    else if (les) launch1<true, false, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, slots, s);
+    else if (visc) launch1<false, true, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, slots, s);
+    else launch1<false, false, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, slots, s);
   }
   return cudaGetLastError();
 }

@@ -613,9 +613,9 @@ constexpr int S_NZF = SBX * SBY;   // 224
 template <typename R, bool MIX>
 struct StageSmem {
   static constexpr int NG = FaceWidth<MIX>::NG;
-  // FP64 staging fields per plane: 5 state fields + nvert, and in the FP64 form
-  // the carried pressure
-  static constexpr int NSTG = MIX ? 6 : 7;
+  // FP64 staging fields per plane: 5 state fields, nvert, and the pressure
+  // carried from an immersed step's interpolation
+  static constexpr int NSTG = 7;
   // ring + face buffers, FP64 staging of the next plane, nvert byte ring [4][PN]
   static constexpr size_t bytes = sizeof(R) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF)) +
                                   sizeof(double) * (size_t)NSTG * STile::PN + (size_t)4 * STile::PN;
@@ -694,10 +694,11 @@ __device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc, bool val
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// One tile (tile column bxi, byi, k-chunk bzi) of one block: the whole k march.
+// One tile column (bxi, byi) of one block over the planes kb .. ke-1: the
+// whole k march, with its prologue.
 template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0, bool NV0 = false>
-__device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, int bxi, int byi, int bzi, int istage,
-                                           double alfa, double beta, double adt, int kchunk, double *smem_d) {
+__device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, int bxi, int byi, int kb, int ke,
+                                           int istage, double alfa, double beta, double adt, double *smem_d) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
   constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
   constexpr int NSTG = StageSmem<R, MIX>::NSTG;
@@ -711,15 +712,13 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   unsigned char *nvc = reinterpret_cast<unsigned char *>(gzb + (size_t)NG * S_NZF);  // [4][PN]
   Rg.nvc = nvc;
   // staged fields per plane: Q, then nvert (byte-exact codes), then lP (carried pressure)
-  const bool pst = !MIX && F.pin != nullptr;
+  const bool pst = F.pin != nullptr;
   const bool nvs = c.nvq && !NV0;
   const int pslot = nvs ? 6 : 5;
   const int nstg = pslot + (pst ? 1 : 0);
 
   const int tid = threadIdx.x;
   const int i0 = 1 + bxi * BX, j0 = 1 + byi * BY;
-  const int kb = 1 + bzi * kchunk;
-  const int ke = min(c.mz - 1, kb + kchunk);  // exclusive
   // node updated by this thread (threads 224..255 only load and compute faces)
   const int utx = tid % BX, uty = tid / BX;
   const int ugi = i0 + utx, ugj = j0 + uty;
@@ -898,12 +897,36 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   }
 }
 
+// kchunk > 0: grid (tiles_x, tiles_y, k-chunks), one tile column and chunk
+// per block.  kchunk == 0: balanced segments -- the tile columns' interior
+// planes laid end to end (column after column) and cut into gridDim.x equal
+// contiguous ranges, one per resident CTA; a CTA marches each column piece of
+// its range with its own prologue.  Every node gets the same arithmetic in
+// both shapes (a chunk start recomputes its first k-face from the same data).
 template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0, bool NV0 = false>
 __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
   extern __shared__ double smem_d[];
-  stage_tile<R, MIX, LES, VISC, RHS_MODE, FLUX, NV0>(c, F, blockIdx.x, blockIdx.y, blockIdx.z, istage, alfa, beta, adt,
-                                                    kchunk, smem_d);
+  const int nk = c.mz - 2, tiles_x = (c.mx - 2 + SBX - 1) / SBX;
+  long long s, e;  // range of (column, plane) units, column-major
+  if (kchunk > 0) {
+    const long long col = (long long)blockIdx.y * tiles_x + blockIdx.x;
+    const int k0 = blockIdx.z * kchunk;
+    s = col * nk + k0;
+    e = col * nk + min(nk, k0 + kchunk);
+  } else {
+    const long long total = (long long)tiles_x * ((c.my - 2 + SBY - 1) / SBY) * nk;
+    const long long per = (total + gridDim.x - 1) / gridDim.x;
+    s = min(total, (long long)blockIdx.x * per);
+    e = min(total, s + per);
+  }
+  while (s < e) {
+    const int col = (int)(s / nk), k0 = (int)(s - (long long)col * nk);
+    const int k1 = (int)min((long long)nk, k0 + (e - s));
+    stage_tile<R, MIX, LES, VISC, RHS_MODE, FLUX, NV0>(c, F, col % tiles_x, col / tiles_x, 1 + k0, 1 + k1, istage, alfa,
+                                                      beta, adt, smem_d);
+    s += k1 - k0;
+  }
 }
 
 // The time-step kernel without nvert (NV0) for FLUX bits fl: Roe, and with
@@ -962,7 +985,9 @@ __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     const int txy = bb.tiles_x * bb.tiles_y;
     const int bzi = ib.y / txy, rem = ib.y - bzi * txy;
     const int byi = rem / bb.tiles_x, bxi = rem - byi * bb.tiles_x;
-    stage_tile<R, MIX, LES, VISC, false, 0, NV0>(bb.c, bb.F, bxi, byi, bzi, istage, alfa, beta, adt, bb.kchunk, smem_d);
+    const int kb = 1 + bzi * bb.kchunk;
+    stage_tile<R, MIX, LES, VISC, false, 0, NV0>(bb.c, bb.F, bxi, byi, kb, min(bb.c.mz - 1, kb + bb.kchunk), istage, alfa,
+                                                beta, adt, smem_d);
     __syncthreads();  // bb and item are rewritten by the next iteration
   }
 }

@@ -196,11 +196,12 @@ class Block:
         return dt.value, lam.value
 
     def autotune(self, candidates=None):
-        """Time the stage kernel per k-chunk candidate and keep the fastest.
-        Returns (best k-chunk, {k-chunk: ms})."""
+        """Time the stage kernel per k-chunk candidate and keep the fastest
+        (k-chunk 0: balanced segments, one range of tile-column planes per
+        resident CTA).  Returns (best k-chunk, {k-chunk: ms})."""
         cand = list(candidates or [])
         ca = (C.c_int * max(len(cand), 1))(*cand)
-        cap = max(len(cand), self.shape[0])
+        cap = max(len(cand), self.shape[0] + 1)
         ms = (C.c_double * cap)()
         nout, best = C.c_int(cap), C.c_int()
         self._check(self.lib.cb_autotune(self._ctx, len(cand), ca, ms, C.byref(nout), C.byref(best)))
@@ -213,6 +214,7 @@ class Block:
                 if ch != last:
                     keys.append(kc)
                     last = ch
+            keys.append(0)  # balanced segments
         return best.value, {k: ms[i] for i, k in enumerate(keys[:nout.value])}
 
     def CalcUCat(self):

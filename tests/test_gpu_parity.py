@@ -192,3 +192,44 @@ def test_autotune_changes_launch_shape_not_results():
         assert np.array_equal(b.Q(), before)
         b.RungeKutta(1)
         assert np.array_equal(b.Q(), want)
+
+
+SEG_CASES = [
+    ("fp64_les_periodic", "fp64", dict(les=1, s_x=0.5, s_y=0.5, s_z=0.5), (40, 30, 36), False),
+    ("mixed_les_central", "mixed", dict(les=1), (37, 29, 33), False),
+    ("fp64_mask_walls", "fp64", dict(les=1, bctype=(7, 7, 3, 3, 44, 44)), (33, 26, 30), True),
+    ("mixed_inviscid_mask", "mixed", dict(les=0, inviscid=1), (35, 17, 41), True),
+]
+
+
+@pytest.mark.parametrize("name,prec,kw,n,mask", SEG_CASES, ids=[c[0] for c in SEG_CASES])
+def test_balanced_segments_equal_k_chunks(name, prec, kw, n, mask):
+    """k-chunk 0 (balanced segments: ranges of tile-column planes, pieces that
+    start mid-column and span columns) gives the results of the chunked grid:
+    bit for bit in the FP64 form; in the mixed form (FMA contraction) the
+    first k-face of a chunk comes from a second inlined copy of the face code,
+    whose FP32 rounding may differ in the last bit, so there the bar is 1e-7."""
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    shape = coords.shape[:3]
+    base = dict(inviscid=0, fluxorder=3, ren=900., ma=0.3, pr=0.71, dt=0.002)
+    base.update(kw)
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, **base)
+    q = W.isotropic_turbulence(n, seed=6, k_peak=3.0, mach_t=0.3)
+    nv = _mask(shape, 11, True) if mask else np.zeros(shape)
+    out = []
+    for cand in ([7], [0]):
+        with gpu_block(cfg, prec) as b:
+            b.FormMetrics(coords)
+            b.set_nvert(nv)
+            b.SetInitialCondition(q)
+            best, _ = b.autotune(cand)
+            assert best == cand[0]
+            rhs = b.formRHS(0)
+            b.RungeKutta(3)
+            out.append((rhs, b.Q()))
+    if prec == "fp64":
+        assert np.array_equal(out[0][0], out[1][0])
+        assert np.array_equal(out[0][1], out[1][1])
+    else:
+        assert max(per_field_rel_l2(out[0][0], out[1][0])) <= 1e-7
+        assert max(per_field_rel_l2(out[0][1], out[1][1])) <= 1e-7
