@@ -68,7 +68,7 @@ struct DevFields {
   unsigned *status;        // sticky status word
   // the pressure lP to read instead of the EqOfState of q (the first stage
   // after an immersed step, whose FormBCS(user, 0) is followed by no
-  // EqOfState); nullptr: EqOfState of q
+  // EqOfState; the FP64 stage kernel and FormBCS read it); nullptr: EqOfState of q
   const double *pin;
 };
 

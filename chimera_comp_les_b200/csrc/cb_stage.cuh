@@ -613,9 +613,11 @@ constexpr int S_NZF = SBX * SBY;   // 224
 template <typename R, bool MIX>
 struct StageSmem {
   static constexpr int NG = FaceWidth<MIX>::NG;
-  // FP64 staging fields per plane: 5 state fields, nvert, and the pressure
-  // carried from an immersed step's interpolation
-  static constexpr int NSTG = 7;
+  // FP64 staging fields per plane: 5 state fields + nvert, and in the FP64 form
+  // the pressure carried from an immersed step's interpolation (the mixed form
+  // keeps that shared memory as L1: the carried value differs from the EOS by
+  // <= 1e-12, inside its bar)
+  static constexpr int NSTG = MIX ? 6 : 7;
   // ring + face buffers, FP64 staging of the next plane, nvert byte ring [4][PN]
   static constexpr size_t bytes = sizeof(R) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF)) +
                                   sizeof(double) * (size_t)NSTG * STile::PN + (size_t)4 * STile::PN;
@@ -712,7 +714,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   unsigned char *nvc = reinterpret_cast<unsigned char *>(gzb + (size_t)NG * S_NZF);  // [4][PN]
   Rg.nvc = nvc;
   // staged fields per plane: Q, then nvert (byte-exact codes), then lP (carried pressure)
-  const bool pst = F.pin != nullptr;
+  const bool pst = !MIX && F.pin != nullptr;
   const bool nvs = c.nvq && !NV0;
   const int pslot = nvs ? 6 : 5;
   const int nstg = pslot + (pst ? 1 : 0);
