@@ -104,13 +104,13 @@ struct BlockHost {
 template <bool LES, bool VISC, bool NV0>
 void f64_batched(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int s, double alfa,
                  double beta, double adt, int ctas, cudaStream_t st) {
-  stage_batched_kernel<double, false, LES, VISC, NV0><<<ctas, SNT, STAGE_SMEM_BYTES, st>>>(tab, items, nitems, counter, s,
+  stage_batched_kernel<double, false, LES, VISC, NV0><<<ctas, SNT, stage_smem<double, false, NV0>(), st>>>(tab, items, nitems, counter, s,
                                                                                           alfa, beta, adt);
 }
 template <bool LES, bool VISC, bool NV0>
 void f64_block(const DevCfg &dc, const DevFields &F, dim3 grid, int s, double alfa, double beta, double adt, int kc,
                cudaStream_t st) {
-  stage_kernel<double, false, LES, VISC, false, 0, NV0><<<grid, SNT, STAGE_SMEM_BYTES, st>>>(dc, F, s, alfa, beta, adt, kc);
+  stage_kernel<double, false, LES, VISC, false, 0, NV0><<<grid, SNT, stage_smem<double, false, NV0>(), st>>>(dc, F, s, alfa, beta, adt, kc);
 }
 template <bool NV0>
 void f64_batched_any(bool les, bool visc, const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int s,
@@ -130,7 +130,7 @@ void f64_block_any(bool les, bool visc, const DevCfg &dc, const DevFields &F, di
 }
 template <bool NV0>
 cudaError_t f64_attrs() {
-  const int sm = (int)STAGE_SMEM_BYTES;
+  const int sm = (int)stage_smem<double, false, NV0>();
   const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaFuncSetAttribute(stage_batched_kernel<double, false, true, true, NV0>, a, sm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_batched_kernel<double, false, true, false, NV0>, a, sm);

@@ -14,7 +14,7 @@ cudaError_t attr1() {
   cudaError_t e = cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM, 0>, attr, sm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM, 1>, attr, sm);
   if constexpr (!RHSM) {  // the no-IBM variants of the time step
-    if (e == cudaSuccess) e = stage_nv0_attrs<float, true, LES, VISC>(sm);
+    if (e == cudaSuccess) e = stage_nv0_attrs<float, true, LES, VISC>();
   }
   return e;
 }
@@ -24,9 +24,13 @@ void launch1(const DevCfg &c, const DevFields &F, int istage, double alfa, doubl
   const dim3 grid = stage_grid(c, kchunk, slots);
   const bool roe = (fl & FLUX_ROE) != 0;
   auto kern = roe ? stage_kernel<float, true, LES, VISC, RHSM, 1> : stage_kernel<float, true, LES, VISC, RHSM, 0>;
+  size_t smem = STAGE_SMEM_BYTES_MIXED;
   if constexpr (!RHSM)
-    if (nv0) kern = stage_nv0_kernel<float, true, LES, VISC>(fl);
-  kern<<<grid, SNT, STAGE_SMEM_BYTES_MIXED, s>>>(c, F, istage, alfa, beta, adt, kchunk);
+    if (nv0) {
+      kern = stage_nv0_kernel<float, true, LES, VISC>(fl);
+      smem = stage_smem<float, true, true>();
+    }
+  kern<<<grid, SNT, smem, s>>>(c, F, istage, alfa, beta, adt, kchunk);
 }
 
 __global__ void mixed_prep_kernel(const DevCfg c, const double *const *met, const double *delta2, const double *aj,
@@ -90,13 +94,15 @@ cudaError_t battr1() {
   const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC>, a, (int)STAGE_SMEM_BYTES_MIXED);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC, true>, a, (int)STAGE_SMEM_BYTES_MIXED);
+  return cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC, true>, a,
+                              (int)stage_smem<float, true, true>());
 }
 template <bool LES, bool VISC>
 void blaunch1(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int istage, double alfa,
               double beta, double adt, bool nv0, int ctas, cudaStream_t s) {
   auto kern = nv0 ? stage_batched_kernel<float, true, LES, VISC, true> : stage_batched_kernel<float, true, LES, VISC, false>;
-  kern<<<ctas, SNT, STAGE_SMEM_BYTES_MIXED, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
+  const size_t smem = nv0 ? stage_smem<float, true, true>() : STAGE_SMEM_BYTES_MIXED;
+  kern<<<ctas, SNT, smem, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
 }
 }  // namespace
 

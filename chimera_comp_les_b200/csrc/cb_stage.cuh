@@ -610,20 +610,24 @@ using STile = TileShape<SBX, SBY>;
 constexpr int S_NXF = STile::NXF;  // 231
 constexpr int S_NYF = STile::NYF;  // 256
 constexpr int S_NZF = SBX * SBY;   // 224
-template <typename R, bool MIX>
+template <typename R, bool MIX, bool NV0 = false>
 struct StageSmem {
   static constexpr int NG = FaceWidth<MIX>::NG;
-  // FP64 staging fields per plane: 5 state fields + nvert, and in the FP64 form
-  // the pressure carried from an immersed step's interpolation (the mixed form
-  // keeps that shared memory as L1: the carried value differs from the EOS by
-  // <= 1e-12, inside its bar)
-  static constexpr int NSTG = MIX ? 6 : 7;
+  // FP64 staging fields per plane: 5 state fields, nvert (not with NV0), and
+  // in the FP64 form the pressure carried from an immersed step's
+  // interpolation (the mixed form keeps that shared memory as L1: the carried
+  // value differs from the EOS by <= 1e-12, inside its bar)
+  static constexpr int NSTG = 5 + (NV0 ? 0 : 1) + (MIX ? 0 : 1);
   // ring + face buffers, FP64 staging of the next plane, nvert byte ring [4][PN]
+  // (not with NV0: the no-IBM variants leave that memory to the L1)
   static constexpr size_t bytes = sizeof(R) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF)) +
-                                  sizeof(double) * (size_t)NSTG * STile::PN + (size_t)4 * STile::PN;
+                                  sizeof(double) * (size_t)NSTG * STile::PN + (NV0 ? 0 : (size_t)4 * STile::PN);
 };
 constexpr size_t STAGE_SMEM_BYTES = StageSmem<double, false>::bytes;
 constexpr size_t STAGE_SMEM_BYTES_MIXED = StageSmem<float, true>::bytes;
+// dynamic shared memory of a stage-kernel launch
+template <typename R, bool MIX, bool NV0>
+constexpr size_t stage_smem() { return StageSmem<R, MIX, NV0>::bytes; }
 static_assert(S_NXF <= 256 && S_NYF <= 256 && S_NZF <= 224, "face schedule segments");
 static_assert(STAGE_SMEM_BYTES <= 232448, "shared memory budget of one block");
 static_assert(2 * (STAGE_SMEM_BYTES_MIXED + 1024) <= 233472, "mixed form: two blocks per SM");
@@ -703,7 +707,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
                                            int istage, double alfa, double beta, double adt, double *smem_d) {
   constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
   constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
-  constexpr int NSTG = StageSmem<R, MIX>::NSTG;
+  constexpr int NSTG = StageSmem<R, MIX, NV0>::NSTG;
   double *stg = smem_d;  // [NSTG][PN] raw FP64 Q, nvert and carried pressure of the next plane
   R *smem = reinterpret_cast<R *>(smem_d + (size_t)NSTG * PN);
   Ring<R, BX, BY> Rg;
@@ -950,7 +954,8 @@ StageKern stage_nv0_kernel(int fl) {
   }
 }
 template <typename R, bool MIX, bool LES, bool VISC>
-cudaError_t stage_nv0_attrs(int smem) {
+cudaError_t stage_nv0_attrs() {
+  const int smem = (int)stage_smem<R, MIX, true>();
   cudaError_t e = cudaSuccess;
   for (int fl = 0; fl < (LES ? 6 : 2) && e == cudaSuccess; fl++)
     e = cudaFuncSetAttribute(stage_nv0_kernel<R, MIX, LES, VISC>(fl), cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

@@ -167,7 +167,9 @@ int cb_cfl_dt(cb_ctx *ctx, double cfl, double *dt, double *lambda_max);
  * times one stage launch per candidate on the current state (ncand = 0: every
  * k-chunk from 4 to mz-2 that changes the chunk count, then 0) and keeps the
  * fastest.  k-chunk 0 is the balanced-segment shape: one CTA per resident slot,
- * each marching an equal share of the tile columns' planes laid end to end.
+ * each marching an equal share of the tile columns' planes laid end to end; it
+ * is kept only when 3 % faster than the best chunked grid (it moves more DRAM
+ * bytes).
  * ms_out/nout (optional): per-candidate milliseconds (*nout in: capacity,
  * out: candidates timed).  Does not advance the state.  No counterpart in the
  * reference (CPU loops have no launch shape). */
