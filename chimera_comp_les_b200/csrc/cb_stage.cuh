@@ -721,7 +721,6 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   const bool pst = !MIX && F.pin != nullptr;
   const bool nvs = c.nvq && !NV0;
   const int pslot = nvs ? 6 : 5;
-  const int nstg = pslot + (pst ? 1 : 0);
 
   const int tid = threadIdx.x;
   const int i0 = 1 + bxi * BX, j0 = 1 + byi * BY;
@@ -730,19 +729,21 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   const int ugi = i0 + utx, ugj = j0 + uty;
   const bool uact = uty < BY && ugi <= c.mx - 2 && ugj <= c.my - 2;
 
-  // async copy of the raw state of plane kk (with its halo) into the staging buffer
+  // async copy of the raw state of plane kk (with its halo) into the staging
+  // buffer: node-major, one index computation per node and one 8-byte copy
+  // per staged field (consecutive threads take consecutive nodes of a row, so
+  // each field's copies stay coalesced)
   auto issue_stage = [&](int kk) {
-    for (int e = tid; e < nstg * PN; e += NT) {
-      const int q = e / PN, idx = e - q * PN;
-      const int lx = idx % PX, ly = idx / PX;
+    const bool kok = kk >= -2 && kk <= c.mz + 1;
+    for (int idx = tid; idx < PN; idx += NT) {
+      const int ly = idx / PX, lx = idx - ly * PX;
       const int xi = i0 - 2 + lx, yj = j0 - 2 + ly;
-      const bool ok = xi <= c.mx + 1 && yj <= c.my + 1 && kk >= -2 && kk <= c.mz + 1;
-      // field pointer by selects (a dynamic index into the parameter struct
-      // would copy the whole struct to local memory)
-      const double *base = q == 0 ? F.q[0] : q == 1 ? F.q[1] : q == 2 ? F.q[2] : q == 3 ? F.q[3] : q == 4 ? F.q[4]
-                           : q == pslot ? F.pin : F.nvert;
-      const double *src = ok ? base + gidx(c, xi, yj, kk) : base;
-      cp_async8(stg + e, src, ok);
+      const bool ok = kok && xi <= c.mx + 1 && yj <= c.my + 1;
+      const long long go = ok ? gidx(c, xi, yj, kk) : 0;  // src-size 0 below: nothing is read
+#pragma unroll
+      for (int q = 0; q < 5; q++) cp_async8(stg + q * PN + idx, F.q[q] + go, ok);
+      if (nvs) cp_async8(stg + 5 * PN + idx, F.nvert + go, ok);
+      if (pst) cp_async8(stg + pslot * PN + idx, F.pin + go, ok);
     }
     cp_async_commit();
   };
@@ -755,12 +756,24 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       for (int q = 0; q < 5; q++) v[q] = stg[q * PN + idx];
       if (v[0] != 0.0) {
         const double r = v[0];
-        v[F_P] = pst ? stg[pslot * PN + idx]
-                     : (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / r);
-        v[F_U] = v[1] / r;
-        v[F_V] = v[2] / r;
-        v[F_W] = v[3] / r;
-        v[F_T] = v[F_P] / r;
+        if (MIX) {
+          // one FP64 reciprocal instead of five divisions: the products differ
+          // from the quotients by at most an FP64 ulp, far below the FP32
+          // rounding of the shifted values stored next
+          const double ri = 1.0 / r;
+          v[F_P] = (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) * ri);
+          v[F_U] = v[1] * ri;
+          v[F_V] = v[2] * ri;
+          v[F_W] = v[3] * ri;
+          v[F_T] = v[F_P] * ri;
+        } else {  // the reference's quotients (EqOfState rhs.c:4850, CalcUCat rhs.c:1349)
+          v[F_P] = pst ? stg[pslot * PN + idx]
+                       : (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / r);
+          v[F_U] = v[1] / r;
+          v[F_V] = v[2] / r;
+          v[F_W] = v[3] / r;
+          v[F_T] = v[F_P] / r;
+        }
         if (MIX) {
           v[F_RE] -= c.e_ref;
           v[F_P] -= c.p_ref;
