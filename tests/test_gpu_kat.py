@@ -4,8 +4,8 @@
   differences telescope, so the sum of Rhs/aj over the interior vanishes for
   every conserved field (non-LES scheme: its faces at the periodic seam use
   only the two adjacent nodes, rhs.c:2665-2666);
-* the isentropic (Shu) vortex, SURVEY config 1 in the reference's scheme set
-  (inviscid, WENO3 + Rusanov, SSP-RK3): the solution after t is the initial
+* the isentropic (Shu) vortex advected on the periodic box [0, 10]^3 with the
+  reference's scheme set (inviscid, WENO3 + Rusanov, SSP-RK3): the solution after t is the initial
   vortex translated by t*(1, 1, 0); the error must shrink under refinement.
 """
 import math
