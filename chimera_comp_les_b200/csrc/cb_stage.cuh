@@ -820,11 +820,32 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
     // the only plane k-1 value the update needs, read before that slot is refilled
     const NRef n{0, uty + 2, utx + 2};
     const R rho_km1 = (LES && VISC && uact) ? Rg.get(F_RHO, nshift(n, 2, -1)) : R(0.);
+    // the update's global operands, issued before the barrier so that their
+    // latency overlaps the wait for the other warps' faces
+    const long long g = gidx(c, ugi, ugj, k);
+    double qo_r[5], qi_r[5], gcl_r[3], aj_r = 0.;
+#pragma unroll
+    for (int q = 0; q < 5; q++) qo_r[q] = qi_r[q] = 0.;
+    gcl_r[0] = gcl_r[1] = gcl_r[2] = 0.;
+    if (uact) {
+      aj_r = ldg(F.aj + g);
+      if (!RHS_MODE) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) qo_r[q] = ldg(F.qold[q] + g);
+      }
+      if (MIX) {
+        if (!RHS_MODE) {
+#pragma unroll
+          for (int q = 0; q < 5; q++) qi_r[q] = ldg(F.q[q] + g);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) gcl_r[a] = ldg(F.gcl[a] + g);
+      }
+    }
     cp_async_wait_all();
     __syncthreads();
 
     if (uact) {
-      const long long g = gidx(c, ugi, ugj, k);
       const double nv = nvert_v<NV0>(c, F, Rg, n, g);
       const int fxr = uty * (BX + 1) + utx + 1, fxl = fxr - 1;   // i+1/2, i-1/2
       const int fyu = (uty + 1) * BX + utx, fyd = uty * BX + utx;  // j+1/2, j-1/2
@@ -860,10 +881,10 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 #pragma unroll
         for (int q = 0; q < 5; q++) d4[q] = fdiff(q);
         if (les_e) d4[4] += les_energy();
-        const double aj = ldg(F.aj + g);
+        const double aj = aj_r;
         rhs[0] = (double)d4[0];
 #pragma unroll
-        for (int q = 1; q < 4; q++) rhs[q] = (double)d4[q] - c.p_ref * ldg(F.gcl[q - 1] + g);
+        for (int q = 1; q < 4; q++) rhs[q] = (double)d4[q] - c.p_ref * gcl_r[q - 1];
         rhs[4] = (double)d4[4];
 #pragma unroll
         for (int q = 0; q < 5; q++) rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;
@@ -875,12 +896,12 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 #pragma unroll
         for (int q = 1; q < 5; q++) visc[q] = VISC ? fdiff(VOFF + q) : R(0.);
         if (LES && nv < BLANK && c.ratio != 0.0) {  // channel forcing (rhs.c:4226-4235); exact no-op at ratio 0
-          const double ajn = ldg(F.aj + g);
+          const double ajn = aj_r;
           conv[3] = conv[3] - c.ratio / ajn * Rg.get(F_RHO, n) / c.dt;
           conv[4] = conv[4] - c.ratio / ajn * Rg.get(F_RW, n) / c.dt;
         }
         if (les_e) visc[4] += les_energy();
-        const double aj = ldg(F.aj + g);
+        const double aj = aj_r;
 #pragma unroll
         for (int q = 0; q < 5; q++) {
           rhs[q] = visc[q] - conv[q];                 // VecWAXPY(Rhs, -1, Conv, Visc)
@@ -894,8 +915,8 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
         double out[5];
 #pragma unroll
         for (int q = 0; q < 5; q++) {
-          const double qo = ldg(F.qold[q] + g);
-          const double qi = MIX ? ldg(F.q[q] + g) : (double)Rg.get(F_RHO + q, n);
+          const double qo = qo_r[q];
+          const double qi = MIX ? qi_r[q] : (double)Rg.get(F_RHO + q, n);
           // solvers.c:257 (VecWAXPY) and 269 (VecAXPBYPCZ), FP64 in every form
           out[q] = (istage == 0) ? qo + adt * rhs[q] : beta * qo + adt * rhs[q] + alfa * qi;
           F.qout[q][g] = out[q];
