@@ -461,43 +461,69 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
                           const double *delta2, const double *nvert, double *nut, int kchunk,
                           const double *const *qn = nullptr, const double *csp = nullptr) {
   __shared__ double us[3][3][EDDY_PN];  // [slot][component][node]
+  __shared__ double stq[4][EDDY_PN];    // raw rho, rhoU, rhoV, rhoW of the plane in flight
+  __shared__ unsigned char stv[EDDY_PN];  // the staged node has a velocity source
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * EDDY_BX + tx;
   const int i0 = 1 + blockIdx.x * EDDY_BX, j0 = 1 + blockIdx.y * EDDY_BY;
   const int kb = 1 + blockIdx.z * kchunk, ke = min(c.mz - 1, kb + kchunk);
   const int i = i0 + tx, j = j0 + ty;
   const bool act = i <= c.mx - 2 && j <= c.my - 2;
-  // velocity of plane kk into slot s (halo entries beyond the owned nodes are never read)
-  auto load = [&](int kk, int s) {
+  // asynchronous copy of plane kk's raw state into the staging area (halo
+  // entries beyond the owned nodes get no source and stay zero velocity)
+  auto issue = [&](int kk) {
     for (int e = tid; e < EDDY_PN; e += EDDY_BX * EDDY_BY) {
-      const int lx = e % EDDY_PX, ly = e / EDDY_PX;
+      const int ly = e / EDDY_PX, lx = e - ly * EDDY_PX;
       const int xi = i0 - 1 + lx, yj = j0 - 1 + ly;
-      double u0 = 0., u1 = 0., u2 = 0.;
+      const double *const *src = nullptr;
+      long long n = 0;
       if (xi <= c.mx - 1 && yj <= c.my - 1) {
-        const long long n = gidx(c, xi, yj, kk);
+        n = gidx(c, xi, yj, kk);
+        src = qu;
         // after the dynamic model (qn set) lUcat holds the current state's
         // velocity at interior nodes with nvert <= 1.1 (les.c:234-238)
-        const double *const *src = qu;
         if (qn && xi >= 1 && xi <= c.mx - 2 && yj >= 1 && yj <= c.my - 2 && kk >= 1 && kk <= c.mz - 2 &&
             ldg(nvert + n) <= 1.1)
           src = qn;
-        if (src) {
-          const double r = ldg(src[0] + n);
-          u0 = ldg(src[1] + n) / r;
-          u1 = ldg(src[2] + n) / r;
-          u2 = ldg(src[3] + n) / r;
-        }
+      }
+      const bool v = src != nullptr;
+      stv[e] = v ? 1 : 0;
+#pragma unroll
+      for (int f = 0; f < 4; f++) cp_async8(&stq[f][e], v ? src[f] + n : (const double *)nut, v);
+    }
+    cp_async_commit();
+  };
+  // staged plane -> velocity slot s: the same quotients as before
+  auto convert = [&](int s) {
+    for (int e = tid; e < EDDY_PN; e += EDDY_BX * EDDY_BY) {
+      double u0 = 0., u1 = 0., u2 = 0.;
+      if (stv[e]) {
+        const double r = stq[0][e];
+        u0 = stq[1][e] / r;
+        u1 = stq[2][e] / r;
+        u2 = stq[3][e] / r;
       }
       us[s][0][e] = u0;
       us[s][1][e] = u1;
       us[s][2][e] = u2;
     }
   };
-  load(kb - 1, (kb - 1) % 3);
-  load(kb, kb % 3);
+  auto stage_sync = [&](int kk) {
+    issue(kk);
+    cp_async_wait_all();
+    __syncthreads();
+    convert(kk % 3);
+    __syncthreads();
+  };
+  stage_sync(kb - 1);
+  stage_sync(kb);
+  issue(kb + 1);
   const int e0 = (ty + 1) * EDDY_PX + tx + 1;
   for (int k = kb; k < ke; k++) {
-    load(k + 1, (k + 1) % 3);
+    cp_async_wait_all();
+    __syncthreads();  // plane k+1 staged; every thread is past plane k-1, whose slot (k+1) % 3 is refilled now
+    convert((k + 1) % 3);
     __syncthreads();
+    if (k + 1 < ke) issue(k + 2);  // in flight while plane k is computed
     if (act) {
       const long long n = gidx(c, i, j, k);
       if (ldg(nvert + n) > 0.1) {
@@ -528,7 +554,6 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
         nut[n] = (csp ? ldg(csp + n) : c.cs_const) * ldg(delta2 + n) * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
       }
     }
-    __syncthreads();  // the slot of plane k-1 is refilled next
   }
 }
 // k-chunk of the eddy-viscosity march: the fewest whole waves of resident

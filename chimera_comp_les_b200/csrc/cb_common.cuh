@@ -72,6 +72,15 @@ struct DevFields {
   const double *pin;
 };
 
+// 8-byte asynchronous global -> shared copy (valid false: zero-fill, nothing read)
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  const int sz = valid ? 8 : 0;  // src-size 0 zero-fills the destination
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __host__ __device__ __forceinline__ long long gidx(const DevCfg &c, int i, int j, int k) {
   return ((long long)(k + 2) * c.py + (j + 2)) * (long long)c.px + (i + 2);
 }

@@ -692,13 +692,6 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
   }
 }
 
-__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc, bool valid) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  const int sz = valid ? 8 : 0;  // src-size 0 zero-fills the destination
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(sz) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // One tile column (bxi, byi) of one block over the planes kb .. ke-1: the
 // whole k march, with its prologue.
