@@ -216,7 +216,8 @@ class Batch:
                  eno_order: int = 2, central: int = 2, isothermal: int = 0, s_x: float = 1.0, s_y: float = 1.0,
                  s_z: float = 1.0, ren: float = 3000.0, ma: float = 2.81, pr: float = 0.72, gamma: float = 1.4,
                  dt: float = 0.01, st: float = 1.0, cs_const: float = 0.03, ci: float = 0.06, ratio: float = 0.0,
-                 precision: str = "fp64", device: int = 0, calc_sigma: int = 0):
+                 precision: str = "fp64", device: int = 0, calc_sigma: int = 0, visT: int = 0,
+                 tref: float = 273.15):
         self.lib = _lib.load()
         self.dims = [tuple(int(x) for x in d) for d in dims]
         cfg = CbConfig()
@@ -225,7 +226,7 @@ class Batch:
         for k, v in dict(les=les, inviscid=inviscid, fluxorder=fluxorder, eno_order=eno_order, central=central,
                          isothermal=isothermal, s_x=s_x, s_y=s_y, s_z=s_z, ren=ren, ma=ma, pr=pr, gamma=gamma,
                          dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device,
-                         calc_sigma=calc_sigma).items():
+                         calc_sigma=calc_sigma, visT=visT, tref=tref).items():
             setattr(cfg, k, v)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]
         self.cfg = cfg

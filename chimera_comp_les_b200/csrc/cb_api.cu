@@ -571,6 +571,8 @@ void cb_config_default(cb_config *cfg, int mx, int my, int mz) {
   cfg->max_cs = 0.05;          // les.c:151
   cfg->twall = 1.;             // rhs.c:486
   cfg->twod = 0;
+  cfg->visT = 0;
+  cfg->tref = 273.15;          // rhs.c:1410
 }
 
 int cb_create(const cb_config *cfg, cb_ctx **out) {
@@ -598,6 +600,8 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   if (cfg->eno_order != 2 && cfg->eno_order != 3) return bail(CB_E_ARG, "ENOorder must be 2 or 3");
   if (cfg->les < 0) return bail(CB_E_ARG, "les must be >= 0");
   if (les_dynamic(*cfg) && !(cfg->max_cs >= 0.0)) return bail(CB_E_ARG, "max_cs must be >= 0");
+  if (cfg->visT && !(cfg->tref > 0.0)) return bail(CB_E_ARG, "Tref must be > 0 with visT");
+  c->nv0 = !cfg->visT;  // nvert starts zero; the no-IBM variants carry no Sutherland law
   if (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) return bail(CB_E_ARG, "precision must be CB_FP64 or CB_MIXED");
   if (cfg->flux != 0 && cfg->flux != 1) return bail(CB_E_ARG, "flux must be 0 (Rusanov) or 1 (Roe)");
   c->dev = cfg->device;
@@ -621,6 +625,7 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.cs_const = cfg->cs_const; d.ci = cfg->ci; d.ratio = cfg->ratio;
   d.inv_ren = 1. / cfg->ren;
   d.inv_ren_half = 1. / cfg->ren * 0.5;
+  set_sutherland(d, cfg->visT, cfg->tref, cfg->ren, cfg->gamma, cfg->ma);
   d.gm1 = cfg->gamma - 1.0;
   d.nvq = 1;  // nvert starts zero
   if ((long long)(cfg->mx + 4) * (cfg->my + 4) * (cfg->mz + 4) >= (1LL << 31))
@@ -841,9 +846,10 @@ int cb_set_nvert(cb_ctx *c, const double *nvert) {
   const int q = nvert_codes_exact(nvert, nn);
   bool zero = true;
   for (size_t t = 0; t < nn && zero; t++) zero = nvert[t] == 0.0;
-  if (q != c->dc.nvq || zero != c->nv0) {
+  const bool nv0 = zero && !c->cfg.visT;  // the no-IBM variants carry no Sutherland law
+  if (q != c->dc.nvq || nv0 != c->nv0) {
     c->dc.nvq = q;
-    c->nv0 = zero;
+    c->nv0 = nv0;
     invalidate_graphs(c);  // the graphs carry the config and the kernel variant
   }
   return CB_OK;

@@ -187,6 +187,7 @@ struct cb_batch {
 
 // every block's nvert is zero: the stage kernels' no-IBM variant
 static bool batch_nv0(const cb_batch *b) {
+  if (b->cfg.visT) return false;  // the no-IBM variants carry no Sutherland law
   for (const auto &bh : b->blk)
     if (!bh.nvz) return false;
   return true;
@@ -321,6 +322,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
       (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
       (cfg->les && cfg->calc_sigma) || cfg->flux != 0)
     return bail(CB_E_UNSUPPORTED, "option combination not built");
+  if (cfg->visT && !(cfg->tref > 0.0)) return bail(CB_E_ARG, "Tref must be > 0 with visT");
   b->dev = cfg->device;
   if (cudaSetDevice(b->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice");
   cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->dev);
@@ -345,6 +347,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.cs_const = cfg->cs_const; d.ci = cfg->ci; d.ratio = cfg->ratio;
     d.inv_ren = 1. / cfg->ren;
     d.inv_ren_half = 1. / cfg->ren * 0.5;
+    set_sutherland(d, cfg->visT, cfg->tref, cfg->ren, cfg->gamma, cfg->ma);
     d.gm1 = cfg->gamma - 1.0;
     d.nvq = 1;  // nvert starts zero
     d.calc_sigma = 0;  // the shock sensor is built for single-block contexts
@@ -760,10 +763,11 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
         if (cost < best) { best = cost; kc = cand; }
       }
       if (mixed) {
-        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, 0, bh.nvz, 2 * b->sms, b->stream));
+        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, 0, bh.nvz && !b->cfg.visT,
+                                    2 * b->sms, b->stream));
       } else {
         dim3 grid(bh.tiles_x, bh.tiles_y, (nk + kc - 1) / kc);
-        if (bh.nvz) f64_block_any<true>(les, visc, bh.dc, F, grid, s, alfa, beta, adt, kc, b->stream);
+        if (bh.nvz && !b->cfg.visT) f64_block_any<true>(les, visc, bh.dc, F, grid, s, alfa, beta, adt, kc, b->stream);
         else f64_block_any<false>(les, visc, bh.dc, F, grid, s, alfa, beta, adt, kc, b->stream);
       }
     }

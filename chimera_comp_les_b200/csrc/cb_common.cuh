@@ -39,7 +39,23 @@ struct DevCfg {
   int flux;  // 0 Rusanov (the reference's), 1 Roe with Harten's entropy fix
   double twall;  // -Twall of the characteristic isothermal wall
   int twod;      // -twoD (1 drops that wall's x velocity term)
+  // -visT: Sutherland's law nu = sut_k1 / (Tr + sut_k2) * Tr^1.5 on the face
+  // temperature Tr = gm2 * (p0 + p1) / (rho0 + rho1) (rhs.c:1627-1637)
+  int sutherland;
+  double sut_k1;  // 1./ren*(1+C/Tref), C = 110.4 (rhs.c:1410)
+  double sut_k2;  // C/Tref
+  double gm2;     // gamma*Ma*Ma
 };
+
+// The Sutherland constants of DevCfg from the options, in the reference's
+// evaluation order.
+inline void set_sutherland(DevCfg &d, int visT, double tref, double ren, double gamma, double ma) {
+  const double C_sutherland = 110.4;
+  d.sutherland = visT != 0;
+  d.sut_k1 = 1. / ren * (1 + C_sutherland / tref);
+  d.sut_k2 = C_sutherland / tref;
+  d.gm2 = gamma * ma * ma;
+}
 
 // Host check of an nvert array for the byte code of DevCfg::nvq.
 inline int nvert_codes_exact(const double *nv, size_t n) {

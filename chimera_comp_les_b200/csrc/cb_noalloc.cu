@@ -81,6 +81,7 @@ extern "C" int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const 
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
       (cfg->les != 0 && cfg->les != 1) || cfg->precision != CB_FP64 || (cfg->les && cfg->calc_sigma) || cfg->flux != 0)
     return na_fail(CB_E_UNSUPPORTED, "option combination not built");
+  if (cfg->visT && !(cfg->tref > 0.0)) return na_fail(CB_E_ARG, "Tref must be > 0 with visT");
   DevCfg d{};
   d.mx = cfg->mx; d.my = cfg->my; d.mz = cfg->mz;
   d.px = ((cfg->mx + 4 + 15) / 16) * 16;
@@ -101,6 +102,7 @@ extern "C" int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const 
   d.cs_const = cfg->cs_const; d.ci = cfg->ci; d.ratio = cfg->ratio;
   d.inv_ren = 1. / cfg->ren;
   d.inv_ren_half = 1. / cfg->ren * 0.5;
+  set_sutherland(d, cfg->visT, cfg->tref, cfg->ren, cfg->gamma, cfg->ma);
   d.gm1 = cfg->gamma - 1.0;
   d.nvq = 0;  // nvert is a caller-owned device array: read it from global memory
   d.flux = 0;

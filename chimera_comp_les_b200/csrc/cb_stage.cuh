@@ -520,6 +520,15 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
     const R rhs_rho = (d == 0) ? Rg.get(F_RHO, b) : Rg.get(F_RHO, nshift(a, 0, 1));
     nu = R(c.inv_ren_half) * (Rg.get(F_RHO, a) + rhs_rho);  // (1./ren*0.5)*(...)
   }
+  // Sutherland's law on the face temperature (rhs.c:1627-1637, 1837-1846,
+  // 2036-2045); the hosts never launch the no-IBM variants with it, which
+  // keeps their registers for the common path
+  if (!NV0 && c.sutherland) {
+    const R psum = MIX ? (Rg.get(F_P, a) + Rg.get(F_P, b)) + R(2.0 * c.p_ref) : Rg.get(F_P, a) + Rg.get(F_P, b);
+    const R Tr = R(c.gm2) * psum / (Rg.get(F_RHO, a) + Rg.get(F_RHO, b));
+    if (Tr < R(0)) nu = R(c.inv_ren);
+    else nu = R(c.sut_k1) / (Tr + R(c.sut_k2)) * (MIX ? Tr * sqrt(Tr) : R(pow((double)Tr, 1.5)));
+  }
   const R div = R(2.) / R(3.) * (dudc * csi0 + dude * eta0 + dudz * zet0 + dvdc * csi1 + dvde * eta1 + dvdz * zet1 +
                                  dwdc * csi2 + dwde * eta2 + dwdz * zet2);
   const R tu = g11 * dudc + g21 * dude + g31 * dudz + r11 * md0 + r21 * md1 + r31 * md2;

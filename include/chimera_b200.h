@@ -91,6 +91,9 @@ typedef struct {
                            three over the box; j or k alone only takes LM / MM node by node */
   int testfilter_ik;    /* -testfilter_ik: test-filter width 5^(1/3) instead of 2 filter widths
                            (les.c:598) */
+  int visT;             /* -visT: Sutherland's law for the molecular viscosity on each face
+                           (rhs.c:1412-1414, 1627-1637) */
+  double tref;          /* -Tref: its reference temperature (default 273.15, rhs.c:1410) */
 } cb_config;
 
 /* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */

@@ -76,6 +76,8 @@ class Config:
     j_homo_filter: int = 0
     k_homo_filter: int = 0
     testfilter_ik: int = 0  # -testfilter_ik: test-filter width 5^(1/3) filter widths (les.c:598)
+    visT: int = 0           # -visT: Sutherland's law for the viscosity (rhs.c:1412-1414)
+    tref: float = 273.15    # -Tref: its reference temperature (rhs.c:1410)
 
     def ref_options(self) -> str:
         o = [
@@ -85,7 +87,8 @@ class Config:
             ("-s_y", repr(float(self.s_y))), ("-s_z", repr(float(self.s_z))),
             ("-ren", repr(float(self.ren))), ("-Ma", repr(float(self.ma))),
             ("-Pr", repr(float(self.pr))), ("-gamma", repr(float(self.gamma))),
-            ("-dt", repr(float(self.dt))), ("-visT", 0), ("-twoD", self.twoD), ("-TwoD", 0),
+            ("-dt", repr(float(self.dt))), ("-visT", self.visT), ("-Tref", repr(float(self.tref))),
+            ("-twoD", self.twoD), ("-TwoD", 0),
             ("-imm", self.immersed), ("-wallfunction", self.wallfunction), ("-max_cs", repr(float(self.max_cs))),
             ("-Twall", repr(float(self.twall))),
             ("-calc_sigma", self.calc_sigma), ("-s_x_min", repr(float(self.s_x_min))),
@@ -117,7 +120,7 @@ class _CCfg(C.Structure):
         ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double), ("sigma_thrsh", C.c_double),
         ("flux", C.c_int), ("max_cs", C.c_double), ("twall", C.c_double), ("twod", C.c_int),
         ("i_homo_filter", C.c_int), ("j_homo_filter", C.c_int), ("k_homo_filter", C.c_int),
-        ("testfilter_ik", C.c_int),
+        ("testfilter_ik", C.c_int), ("visT", C.c_int), ("tref", C.c_double),
     ]
 
 

@@ -676,6 +676,12 @@ static void visc_face(const ctx_t *C, const visc_t *V, int d, int i, int j, int 
     ptrdiff_t nr = (d == 0) ? n1 : n0 + G->s[0];
     nu = 1. / c->ren * 0.5 * (C->q[0][n0] + C->q[0][nr]);
   }
+  if (c->visT) { /* Sutherland's law on the face temperature (rhs.c:1627-1637, 1837-1846, 2036-2045) */
+    const double C_sutherland = 110.4; /* rhs.c:1410 */
+    const double Tr = c->gamma * c->ma * c->ma * (C->p[n0] + C->p[n1]) / (C->q[0][n0] + C->q[0][n1]);
+    if (Tr < 0) nu = 1. / c->ren;
+    else nu = 1. / c->ren * (1 + C_sutherland / c->tref) / (Tr + C_sutherland / c->tref) * pow(Tr, 1.5);
+  }
   double div = 2. / 3. * (dudc * csi0 + dude * eta0 + dudz * zet0 + dvdc * csi1 + dvde * eta1 + dvdz * zet1 +
                           dwdc * csi2 + dwde * eta2 + dwdz * zet2);
 

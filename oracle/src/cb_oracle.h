@@ -45,6 +45,8 @@ typedef struct {
   int i_homo_filter, j_homo_filter, k_homo_filter; /* -i/-j/-k_homo_filter: homogeneous averaging of the
                               dynamic model's LM and MM (les.c:916-1115) */
   int testfilter_ik;       /* -testfilter_ik: test-filter width 5^(1/3) instead of 2 filter widths (les.c:598) */
+  int visT;                /* -visT: Sutherland's law for the molecular viscosity (rhs.c:1412-1414) */
+  double tref;             /* -Tref: its reference temperature (default 273.15, rhs.c:1410) */
 } cbo_config;
 
 /* Fill the two ghost layers of each periodic direction of one padded plane

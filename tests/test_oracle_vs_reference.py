@@ -260,3 +260,42 @@ def test_les10_runs_without_a_model_bitexact_vs_reference():
     o.steps(3, st, met, nvp)
     assert np.array_equal(O.from_padded(st["q"]), ref.Q())
     assert not np.array_equal(ref.Q(), q)
+
+
+SUTHERLAND_CASES = [
+    ("les_mask", dict(les=1, fluxorder=3, ren=800.), True),
+    ("dns_muscl", dict(les=0, fluxorder=2, ren=500., tref=300.0), False),
+    ("dynamic_walls", dict(les=2, fluxorder=3, ren=600., max_cs=0.2, bctype=(7, 7, 3, 3, 44, 44)), True),
+]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference sources not present")
+@pytest.mark.parametrize("name,kw,mask", SUTHERLAND_CASES, ids=[c[0] for c in SUTHERLAND_CASES])
+def test_sutherland_viscosity_bitexact_vs_reference(name, kw, mask):
+    """-visT 1: Sutherland's law on each face's temperature replaces 1/Re
+    (and the LES density weighting) in formViscous (rhs.c:1627-1637,
+    1837-1846, 2036-2045); RHS and 3-step trajectories."""
+    from _common import oracle_run
+    from test_gpu_parity import _mask
+    n = (17, 15, 16)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, inviscid=0, ma=0.3, pr=0.71, dt=0.002, visT=1, **kw)
+    q = W.isotropic_turbulence(n, seed=9, k_peak=3.0, mach_t=0.3)
+    nv = _mask(shape, 4, True) if mask else np.zeros(shape)
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q)
+    if cfg.les:
+        ref.calc_ucat()
+        ref.eddy_viscosity()
+    got = oracle_run(cfg, coords, q, nv, steps=3)
+    assert np.array_equal(got["rhs"], ref.rhs(0))
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q)
+    ref.steps(3)
+    assert np.array_equal(got["q_steps"], ref.Q())
+    # the law changes the flux: same case without it differs
+    plain = oracle_run(O.Config(**{**cfg.__dict__, "visT": 0}), coords, q, nv)
+    assert not np.array_equal(plain["rhs"], got["rhs"])
