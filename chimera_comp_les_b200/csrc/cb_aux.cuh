@@ -498,7 +498,7 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
       double u0 = 0., u1 = 0., u2 = 0.;
       if (stv[e]) {
         const double r = stq[0][e];
-        u0 = stq[1][e] / r;
+        u0 = c.twod == 1 ? 0. : stq[1][e] / r;  // lUcat x = 0 with -twoD 1 (rhs.c:1349)
         u1 = stq[2][e] / r;
         u2 = stq[3][e] / r;
       }

@@ -348,6 +348,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.inv_ren = 1. / cfg->ren;
     d.inv_ren_half = 1. / cfg->ren * 0.5;
     set_sutherland(d, cfg->visT, cfg->tref, cfg->ren, cfg->gamma, cfg->ma);
+    d.twod = cfg->twod;  // -twoD 1: no i-face fluxes
     d.gm1 = cfg->gamma - 1.0;
     d.nvq = 1;  // nvert starts zero
     d.calc_sigma = 0;  // the shock sensor is built for single-block contexts

@@ -46,7 +46,7 @@ __global__ void mixed_prep_kernel(const DevCfg c, const double *const *met, cons
     for (int a = 0; a < 3; a++) {
       double s = 0.;
       if (interior) {
-        for (int d = 0; d < 3; d++) {
+        for (int d = c.twod == 1 ? 1 : 0; d < 3; d++) {  // -twoD 1 has no i-faces, so no i share
           const long long sd = gstride(c, d);
           const double *m = met[3 * d + a];
           const double hp = 0.5 * (m[t] + m[t + sd]), hm = 0.5 * (m[t - sd] + m[t]);

@@ -478,6 +478,7 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
       }
     }
   }
+  if (c.twod == 1) D[0][0] = D[0][1] = D[0][2] = R(0.);  // lUcat x = 0 (CalcUCat rhs.c:1349)
   const R dudc = D[0][0], dude = D[0][1], dudz = D[0][2];
   const R dvdc = D[1][0], dvde = D[1][1], dvdz = D[1][2];
   const R dwdc = D[2][0], dwde = D[2][1], dwdz = D[2][2];
@@ -553,6 +554,7 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
 #pragma unroll
     for (int q = 0; q < 3; q++) uh[q] = R(0.5) * (Rg.get(F_U + q, b) + Rg.get(F_U + q, a));
   }
+  if (c.twod == 1) uh[0] = R(0.);
   const R gm = R(c.gamma);
   Fv[4] = (Fv[1] * uh[0] + Fv[2] * uh[1] + Fv[3] * uh[2]) +
           (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (gm * nu / R(c.pr) / R(c.gm1));
@@ -680,7 +682,8 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
       dst = gzb; nslot = S_NZF;
     }
     R G[NG];
-    if (fi <= c.mx - 2 && fj <= c.my - 2) {
+    // -twoD 1 forms no i-face flux (rhs.c:1487, 2646, 3465): it stays zero
+    if (fi <= c.mx - 2 && fj <= c.my - 2 && !(d == 0 && c.twod == 1)) {
       if (MIX) {
         // one instantiation per direction (d is warp-uniform): 16 % faster
         // for the FP32 arithmetic of the mixed form
@@ -888,6 +891,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 #pragma unroll
         for (int q = 1; q < 4; q++) rhs[q] = (double)d4[q] - c.p_ref * gcl_r[q - 1];
         rhs[4] = (double)d4[4];
+        if (c.twod == 1) rhs[1] = 0.;  // no x-momentum right-hand side (rhs.c:2135, 3168, 4215)
 #pragma unroll
         for (int q = 0; q < 5; q++) rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;
       } else {
@@ -897,6 +901,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
         visc[0] = R(0.);
 #pragma unroll
         for (int q = 1; q < 5; q++) visc[q] = VISC ? fdiff(VOFF + q) : R(0.);
+        if (c.twod == 1) conv[1] = visc[1] = R(0.);  // rhs.c:2135-2140, 3168-3173, 4215-4220
         if (LES && nv < BLANK && c.ratio != 0.0) {  // channel forcing (rhs.c:4226-4235); exact no-op at ratio 0
           const double ajn = aj_r;
           conv[3] = conv[3] - c.ratio / ajn * Rg.get(F_RHO, n) / c.dt;

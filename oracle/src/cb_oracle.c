@@ -757,8 +757,10 @@ static int rhs_impl(const cbo_config *c, const double *const q[5], const double 
     for (int a = 0; a < 3; a++) Al[d][a] = buf + G.n * (d * 13 + 10 + a);
   }
 
-  /* face ranges: along d from 0 to m-2, transverse interior (rhs.c:2647 etc.) */
+  /* face ranges: along d from 0 to m-2, transverse interior (rhs.c:2647 etc.);
+   * -twoD 1 computes no i-faces, whose fluxes stay zero (rhs.c:2646, 3465) */
   for (int d = 0; d < 3; d++) {
+    if (d == 0 && c->twod == 1) continue;
     int lo[3] = {1, 1, 1}, hi[3] = {mx - 1, my - 1, mz - 1};
     lo[d] = 0;
     for (int k = lo[2]; k < hi[2]; k++)
@@ -779,7 +781,7 @@ static int rhs_impl(const cbo_config *c, const double *const q[5], const double 
     ucat = (double *)malloc(G.n * 4 * sizeof(double));
     for (size_t n = 0; n < G.n; n++) {
       double r = q[0][n];
-      ucat[n] = r != 0.0 ? q[1][n] / r : 0.0;
+      ucat[n] = (r != 0.0 && c->twod != 1) ? q[1][n] / r : 0.0; /* x zero with -twoD 1 (rhs.c:1349) */
       ucat[G.n + n] = r != 0.0 ? q[2][n] / r : 0.0;
       ucat[2 * G.n + n] = r != 0.0 ? q[3][n] / r : 0.0;
       ucat[3 * G.n + n] = r != 0.0 ? p[n] / r : 0.0;
@@ -787,6 +789,7 @@ static int rhs_impl(const cbo_config *c, const double *const q[5], const double 
     V.u[0] = ucat; V.u[1] = ucat + G.n; V.u[2] = ucat + 2 * G.n; V.T = ucat + 3 * G.n;
     V.nut = nut; V.sig = sig; V.aj = aj;
     for (int d = 0; d < 3; d++) {
+      if (d == 0 && c->twod == 1) continue; /* rhs.c:1487 */
       int lo[3] = {1, 1, 1}, hi[3] = {mx - 1, my - 1, mz - 1};
       lo[d] = 0;
       for (int k = lo[2]; k < hi[2]; k++)
@@ -811,6 +814,7 @@ static int rhs_impl(const cbo_config *c, const double *const q[5], const double 
         if (nvert[n] < BLANK) { /* rhs.c:3159-3205 / 4205-4246 */
           for (int a = 0; a < 5; a++)
             conv[a] = Fc[0][a][n] - Fc[0][a][n - si] + Fc[1][a][n] - Fc[1][a][n - sj] + Fc[2][a][n] - Fc[2][a][n - sk];
+          if (c->twod == 1) conv[1] = 0.; /* rhs.c:3168-3173, 4215-4220 */
           if (c->les) {
             conv[3] = conv[3] - c->ratio / aj[n] * q[0][n] / c->dt;
             conv[4] = conv[4] - c->ratio / aj[n] * q[3][n] / c->dt;
@@ -819,6 +823,7 @@ static int rhs_impl(const cbo_config *c, const double *const q[5], const double 
         if (!c->inviscid) { /* rhs.c:2123-2199 */
           for (int a = 1; a < 5; a++)
             visc[a] = Fv[0][a][n] - Fv[0][a][n - si] + Fv[1][a][n] - Fv[1][a][n - sj] + Fv[2][a][n] - Fv[2][a][n - sk];
+          if (c->twod == 1) visc[1] = 0.; /* rhs.c:2135-2140 */
           if (c->les && j > 2 && j < my - 2 && nvert[n] < 0.5) {
             double rL = (q[0][n] + q[0][n - si]) * 0.5, rR = (q[0][n + si] + q[0][n]) * 0.5;
             double rD = (q[0][n] + q[0][n - sj]) * 0.5, rU = (q[0][n + sj] + q[0][n]) * 0.5;
@@ -874,7 +879,8 @@ void cbo_eddy_viscosity(const cbo_config *c, const double *const qu[5], const do
         if (nvert[n] > 0.1) { nut[n] = 0; continue; }
         double d[3][3]; /* d[comp][dir] central differences of velocity */
         for (int a = 0; a < 3; a++) {
-          if (!qu) { d[a][0] = d[a][1] = d[a][2] = 0.0; continue; }
+          /* lUcat x is zero with -twoD 1 (CalcUCat rhs.c:1349) */
+          if (!qu || (a == 0 && c->twod == 1)) { d[a][0] = d[a][1] = d[a][2] = 0.0; continue; }
           const double *r = qu[0], *m = qu[1 + a];
           d[a][0] = (m[n + si] / r[n + si] - m[n - si] / r[n - si]) * 0.5;
           d[a][1] = (m[n + sj] / r[n + sj] - m[n - sj] / r[n - sj]) * 0.5;
@@ -1550,6 +1556,7 @@ int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const
   geom G = mkgeom(c);
   const int mx = G.m[0], my = G.m[1], mz = G.m[2];
   if (!cbo_les_dynamic(c)) return 5;
+  if (c->twod == 1) return 5; /* the dynamic model with -twoD 1 is not restated */
   /* -les 3 and the homogeneous filters take LM / MM node by node and skip
    * the final 1/aj-weighted mean (les.c:916-922, 1302) */
   const int pointwise = c->i_homo_filter || c->j_homo_filter || c->k_homo_filter || c->les == 3;

@@ -299,3 +299,43 @@ def test_sutherland_viscosity_bitexact_vs_reference(name, kw, mask):
     # the law changes the flux: same case without it differs
     plain = oracle_run(O.Config(**{**cfg.__dict__, "visT": 0}), coords, q, nv)
     assert not np.array_equal(plain["rhs"], got["rhs"])
+
+
+TWOD_CASES = [
+    ("les_periodic", dict(les=1, fluxorder=3, ren=800.), True),
+    ("dns_iso1_walls", dict(les=0, fluxorder=2, ren=500., isothermal=1, bctype=(7, 7, 1, 1, 7, 7)), False),
+    ("les_iso2_walls", dict(les=1, fluxorder=3, ren=400., isothermal=2, twall=1.1, s_x=0.6, s_y=0.6, s_z=0.6,
+                            bctype=(7, 7, 1, 1, 7, 7)), False),
+]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference sources not present")
+@pytest.mark.parametrize("name,kw,mask", TWOD_CASES, ids=[c[0] for c in TWOD_CASES])
+def test_twoD1_bitexact_vs_reference(name, kw, mask):
+    """-twoD 1: no i-face fluxes (convective, viscous, SGS), zero x-momentum
+    right-hand side and lUcat x = 0 (rhs.c:1349, 1487, 2135, 2646, 3168, 3465,
+    4215); RHS and 3-step trajectories."""
+    from _common import oracle_run
+    from test_gpu_parity import _mask
+    n = (17, 15, 16)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, inviscid=0, ma=0.3, pr=0.71, dt=0.002, twoD=1, **kw)
+    q = W.random_smooth_state(shape, seed=11, periodic=False) if cfg.bctype[2] != 7 else \
+        W.isotropic_turbulence(n, seed=11, k_peak=3.0, mach_t=0.3)
+    nv = _mask(shape, 6, True) if mask else np.zeros(shape)
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q)
+    if cfg.les:
+        ref.calc_ucat()
+        ref.eddy_viscosity()
+    got = oracle_run(cfg, coords, q, nv, steps=3)
+    r0 = ref.rhs(0)
+    assert np.array_equal(got["rhs"], r0)
+    assert not np.any(r0[1:-1, 1:-1, 1:-1, 1])  # no x-momentum right-hand side
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q)
+    ref.steps(3)
+    assert np.array_equal(got["q_steps"], ref.Q())
