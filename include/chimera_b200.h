@@ -83,8 +83,10 @@ typedef struct {
                            les.c:151, default 0.05) */
   double twall;         /* -Twall: wall temperature of the characteristic isothermal wall
                            (-isothermal 2 with j-wall code 1; rhs.c:486, default 1) */
-  int twod;             /* -twoD: 1 drops that wall's x-velocity term (rhs.c:724); the immersed
-                           boundary takes its own value from cb_ibm_set_options */
+  int twod;             /* -twoD: 1 is the reference's 2-D mode in i -- no i-face fluxes, a zero
+                           x-momentum right-hand side, lUcat x = 0 (rhs.c:1349, 1487, 2135, 2646,
+                           3168, 3465, 4215) and no x term in the characteristic wall (rhs.c:719);
+                           the immersed boundary takes its own value from cb_ibm_set_options */
   int i_homo_filter, j_homo_filter, k_homo_filter;
                         /* -i/-j/-k_homo_filter: homogeneous averaging of the dynamic model's LM and
                            MM (les.c:916-1115): i alone per (k, j) line, i and k per j plane, all

@@ -41,7 +41,8 @@ typedef struct {
   int flux;                /* upwind flux: 0 Rusanov (the reference's), 1 Roe with Harten's entropy fix */
   double max_cs;           /* -max_cs: upper clip of the dynamic Smagorinsky coefficient (default 0.05) */
   double twall;            /* -Twall: wall temperature of the characteristic isothermal wall (default 1) */
-  int twod;                /* -twoD: 1 drops the x velocity term of that wall (and x in the IB) */
+  int twod;                /* -twoD: 1 is the 2-D mode in i (no i-face fluxes, zero x-momentum
+                              right-hand side, lUcat x = 0) and drops the x term of that wall (and x in the IB) */
   int i_homo_filter, j_homo_filter, k_homo_filter; /* -i/-j/-k_homo_filter: homogeneous averaging of the
                               dynamic model's LM and MM (les.c:916-1115) */
   int testfilter_ik;       /* -testfilter_ik: test-filter width 5^(1/3) instead of 2 filter widths (les.c:598) */
