@@ -41,7 +41,7 @@ class CbConfig(C.Structure):
         ("calc_sigma", C.c_int), ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double),
         ("sigma_thrsh", C.c_double), ("flux", C.c_int), ("max_cs", C.c_double), ("twall", C.c_double),
         ("twod", C.c_int), ("i_homo_filter", C.c_int), ("j_homo_filter", C.c_int), ("k_homo_filter", C.c_int),
-        ("testfilter_ik", C.c_int), ("visT", C.c_int), ("tref", C.c_double),
+        ("testfilter_ik", C.c_int), ("visT", C.c_int), ("tref", C.c_double), ("abc", C.c_int),
     ]
 
 

@@ -638,6 +638,7 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.flux = cfg->flux;
   d.twall = cfg->twall;
   d.twod = cfg->twod;
+  d.abc = cfg->abc;
   c->plane = (size_t)d.plane;
   // planes: 15 state + 9 metrics + aj + nvert + nut + LES filter width = 28
   const int nplanes = 28;

@@ -620,13 +620,17 @@ static __global__ void sigma_sensor_kernel(const DevCfg c, const double *const *
     if (i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2) {
       const long long n = t;
       const double p0 = eos_node(c, q, n);
-      if (i < c.mx - 4 && i > 2)
+      const bool absorb = c.abc != 0 && k > c.abc;  // -ABC layer: raw weight 0 (rhs.c:3341, 3355, 3368)
+      if (absorb) sx = 0.;
+      else if (i < c.mx - 4 && i > 2)
         sx = sensor_ramp(eos_node(c, q, n - si), p0, eos_node(c, q, n + si), eos_node(c, q, n + 2 * si), c.ks);
       sx = pmax(c.s_x_min, pmin(c.s_x, sx));
-      if (c.bctype[4] == 7 || (k < c.mz - 4 && k > 4))
+      if (absorb) sz = 0.;
+      else if (c.bctype[4] == 7 || (k < c.mz - 4 && k > 4))
         sz = sensor_ramp(eos_node(c, q, n - sk), p0, eos_node(c, q, n + sk), eos_node(c, q, n + 2 * sk), c.ks);
       sz = pmax(c.s_z_min, pmin(c.s_z, sz));
-      if (j < c.my - 4 && j > 4)
+      if (absorb) sy = 0.;
+      else if (j < c.my - 4 && j > 4)
         sy = sensor_ramp(eos_node(c, q, n - sj), p0, eos_node(c, q, n + sj), eos_node(c, q, n + 2 * sj), c.ks);
       sy = pmax(c.s_y_min, pmin(c.s_y, sy));
     }

@@ -36,6 +36,7 @@ struct DevCfg {
   // LES shock sensor (rhs.c:3333-3433): hybrid weights from per-node planes
   int calc_sigma;
   double s_x_min, s_y_min, s_z_min, ks;
+  int abc;  // -ABC: raw sensor weights 0 above plane k = abc (0: off)
   int flux;  // 0 Rusanov (the reference's), 1 Roe with Harten's entropy fix
   double twall;  // -Twall of the characteristic isothermal wall
   int twod;      // -twoD (1 drops that wall's x velocity term)

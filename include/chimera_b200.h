@@ -96,6 +96,8 @@ typedef struct {
   int visT;             /* -visT: Sutherland's law for the molecular viscosity on each face
                            (rhs.c:1412-1414, 1627-1637) */
   double tref;          /* -Tref: its reference temperature (default 273.15, rhs.c:1410) */
+  int abc;              /* -ABC: with -calc_sigma, the raw sensor weights are 0 above plane
+                           k = ABC (an absorbing layer; rhs.c:3311, 3341-3368); 0 off */
 } cb_config;
 
 /* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */

@@ -78,6 +78,7 @@ class Config:
     testfilter_ik: int = 0  # -testfilter_ik: test-filter width 5^(1/3) filter widths (les.c:598)
     visT: int = 0           # -visT: Sutherland's law for the viscosity (rhs.c:1412-1414)
     tref: float = 273.15    # -Tref: its reference temperature (rhs.c:1410)
+    abc: int = 0            # -ABC: absorbing layer of the shock sensor above plane k (rhs.c:3311)
 
     def ref_options(self) -> str:
         o = [
@@ -88,6 +89,7 @@ class Config:
             ("-ren", repr(float(self.ren))), ("-Ma", repr(float(self.ma))),
             ("-Pr", repr(float(self.pr))), ("-gamma", repr(float(self.gamma))),
             ("-dt", repr(float(self.dt))), ("-visT", self.visT), ("-Tref", repr(float(self.tref))),
+            ("-ABC", self.abc),
             ("-twoD", self.twoD), ("-TwoD", 0),
             ("-imm", self.immersed), ("-wallfunction", self.wallfunction), ("-max_cs", repr(float(self.max_cs))),
             ("-Twall", repr(float(self.twall))),
@@ -120,7 +122,7 @@ class _CCfg(C.Structure):
         ("s_x_min", C.c_double), ("s_y_min", C.c_double), ("s_z_min", C.c_double), ("sigma_thrsh", C.c_double),
         ("flux", C.c_int), ("max_cs", C.c_double), ("twall", C.c_double), ("twod", C.c_int),
         ("i_homo_filter", C.c_int), ("j_homo_filter", C.c_int), ("k_homo_filter", C.c_int),
-        ("testfilter_ik", C.c_int), ("visT", C.c_int), ("tref", C.c_double),
+        ("testfilter_ik", C.c_int), ("visT", C.c_int), ("tref", C.c_double), ("abc", C.c_int),
     ]
 
 

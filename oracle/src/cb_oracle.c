@@ -248,7 +248,8 @@ void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *con
     for (int j = 1; j < my - 1; j++)
       for (int i = 1; i < mx - 1; i++) {
         ptrdiff_t n = IX(&G, i, j, k);
-        if (i < mx - 4 && i > 2) sig[0][n] = sigma_cent(p[n - si], p[n], p[n + si], p[n + 2 * si], ks);
+        if (c->abc != 0 && k > c->abc) sig[0][n] = 0.; /* -ABC absorbing layer (rhs.c:3341) */
+        else if (i < mx - 4 && i > 2) sig[0][n] = sigma_cent(p[n - si], p[n], p[n + si], p[n + 2 * si], ks);
         sig[0][n] = PMIN(c->s_x, sig[0][n]);
         sig[0][n] = PMAX(c->s_x_min, sig[0][n]);
       }
@@ -256,7 +257,8 @@ void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *con
     for (int j = 1; j < my - 1; j++)
       for (int i = 1; i < mx - 1; i++) {
         ptrdiff_t n = IX(&G, i, j, k);
-        if (c->bctype[4] == 7 || (k < mz - 4 && k > 4))
+        if (c->abc != 0 && k > c->abc) sig[2][n] = 0.; /* rhs.c:3355 */
+        else if (c->bctype[4] == 7 || (k < mz - 4 && k > 4))
           sig[2][n] = sigma_cent(p[n - sk], p[n], p[n + sk], p[n + 2 * sk], ks);
         sig[2][n] = PMIN(c->s_z, sig[2][n]);
         sig[2][n] = PMAX(c->s_z_min, sig[2][n]);
@@ -265,7 +267,8 @@ void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *con
     for (int j = 1; j < my - 1; j++)
       for (int i = 1; i < mx - 1; i++) {
         ptrdiff_t n = IX(&G, i, j, k);
-        if (j < my - 4 && j > 4) sig[1][n] = sigma_cent(p[n - sj], p[n], p[n + sj], p[n + 2 * sj], ks);
+        if (c->abc != 0 && k > c->abc) sig[1][n] = 0.; /* rhs.c:3368 */
+        else if (j < my - 4 && j > 4) sig[1][n] = sigma_cent(p[n - sj], p[n], p[n + sj], p[n + 2 * sj], ks);
         sig[1][n] = PMIN(c->s_y, sig[1][n]);
         sig[1][n] = PMAX(c->s_y_min, sig[1][n]);
       }

@@ -48,6 +48,7 @@ typedef struct {
   int testfilter_ik;       /* -testfilter_ik: test-filter width 5^(1/3) instead of 2 filter widths (les.c:598) */
   int visT;                /* -visT: Sutherland's law for the molecular viscosity (rhs.c:1412-1414) */
   double tref;             /* -Tref: its reference temperature (default 273.15, rhs.c:1410) */
+  int abc;                 /* -ABC: sensor weights 0 (then clamped) above plane k = ABC (rhs.c:3311, 3341-3368) */
 } cbo_config;
 
 /* Fill the two ghost layers of each periodic direction of one padded plane

@@ -27,6 +27,9 @@ CASES = [
                                 pr=0.71, dt=0.002, calc_sigma=1)),
     ("inv_min", (33, 40, 19), dict(les=1, inviscid=1, fluxorder=2, s_x=1.0, s_y=1.0, s_z=0.7, dt=0.002, calc_sigma=1,
                                    s_x_min=0.2, s_y_min=0.1, s_z_min=0.3)),
+    # -ABC: raw weights 0 above plane k = 15 (rhs.c:3341-3368)
+    ("visc_abc", (37, 21, 26), dict(les=1, inviscid=0, fluxorder=3, s_x=0.9, s_y=0.8, s_z=1.0, ren=250., ma=0.3,
+                                    pr=0.71, dt=0.002, calc_sigma=1, s_x_min=0.1, s_y_min=0.2, s_z_min=0.05, abc=15)),
 ]
 
 

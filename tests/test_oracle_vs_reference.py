@@ -73,14 +73,16 @@ def _state_with_jump(shape, seed):
     return q
 
 
-@pytest.mark.parametrize("inv,smin", [(0, (0.0, 0.0, 0.0)), (1, (0.2, 0.1, 0.3))])
-def test_shock_sensor_restatement_bitexact_vs_reference(inv, smin):
+@pytest.mark.parametrize("inv,smin,abc", [(0, (0.0, 0.0, 0.0), 0), (1, (0.2, 0.1, 0.3), 0),
+                                          (0, (0.1, 0.2, 0.05), 9)])
+def test_shock_sensor_restatement_bitexact_vs_reference(inv, smin, abc):
+    """abc > 0: the -ABC absorbing layer above plane k = abc (rhs.c:3311, 3341-3368)."""
     n = (17, 16, 15)
     coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
     shape = coords.shape[:3]
     cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=1, inviscid=inv, fluxorder=3, s_x=0.9, s_y=0.8,
                    s_z=1.0, ren=250., ma=0.3, pr=0.71, dt=0.002, calc_sigma=1, s_x_min=smin[0], s_y_min=smin[1],
-                   s_z_min=smin[2])
+                   s_z_min=smin[2], abc=abc)
     q = _state_with_jump(shape, 5)
     nv = np.zeros(shape)
     ref = O.RefOracle(cfg, coords)
