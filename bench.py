@@ -4,11 +4,13 @@ Workload (the configuration the metric is quoted on): viscous LES of the
 compressible Taylor-Green vortex, 128^3 unique nodes (DMDA 130^3 with the
 periodic boundary layers) on [0, 2*pi]^3, curvilinear grid perturbed by
 x_i += 0.05 sin(xi_j) sin(xi_k), Ma 0.1, Re 1600, Pr 0.71, gamma 1.4, constant
-viscosity, the reference's LES scheme: WENO3 + Rusanov upwind blended with the
-4-point skew-symmetric central flux (-central 2, -s_x/y/z 1), constant
-Smagorinsky eddy viscosity (CS 0.03) with Yoshizawa term; SSP-RK3
-(-fluxorder 3: the reference ties the RK stage count to the flux order), dt
-2e-3 (CFL ~0.44).  Synthetic inputs from a formula (no dataset).
+viscosity, in the reference's flags for MUSCL-minmod upwind with a
+Smagorinsky model: -les 1 -fluxorder 2 -s_x 0 -s_y 0 -s_z 0 (MUSCL-minmod
+reconstruction, Rusanov flux, hybrid weight 0: pure upwind on every face;
+the reference ties the RK stage count to the flux order, so 2 stages per
+step), constant Smagorinsky eddy viscosity (CS 0.03), dt 2e-3.  The same
+workload with Roe's flux is reported beside it.  Synthetic inputs from a
+formula (no dataset).
 
 A "step" is one physical time step (eddy viscosity + every RK stage with its
 periodic boundary/ghost fill).  value = interior nodes x stages x steps x
@@ -49,21 +51,27 @@ B_ALG = {
 }
 ACC_STEPS = 100
 
-CFG = dict(les=1, inviscid=0, fluxorder=3, eno_order=2, central=2, s_x=1.0, s_y=1.0, s_z=1.0,
+# -les 1 -fluxorder 2 -s_x 0 -s_y 0 -s_z 0: MUSCL-minmod + Rusanov, pure upwind
+CFG = dict(les=1, inviscid=0, fluxorder=2, eno_order=2, central=2, s_x=0.0, s_y=0.0, s_z=0.0,
            ren=1600.0, ma=0.1, pr=0.71, gamma=1.4, dt=2e-3)
+# the reference's default hybrid blend on the same TGV: WENO3 (-fluxorder 3,
+# SSP-RK3) blended with the 4-point central flux by the weight sigma
+CFG_WENO3_BLEND = dict(CFG, fluxorder=3)
 
 
 def workload_config(n):
     return {
         "workload": f"compressible Taylor-Green vortex LES, {n}^3 (DMDA {n + 2}^3), perturbed curvilinear grid, "
-                    "WENO3+Rusanov blended with skew-symmetric central (sigma=1), Smagorinsky CS=0.03, "
-                    "viscous Re 1600 Ma 0.1, SSP-RK3 (fluxorder 3, 3 stages/step), dt 2e-3",
-        "flux_variant": "sigma = 1 on every face (the reference's default s_x = s_y = s_z = 1, sensor off): the "
-                        "blend (1 - sigma) * upwind + sigma * central equals the central flux, so the stage kernel "
-                        "forms only that; the 'blend_sigma_half' object times the same workload with both parts",
+                    "MUSCL-minmod + Rusanov upwind (-les 1 -fluxorder 2 -s_x 0 -s_y 0 -s_z 0), Smagorinsky CS=0.03, "
+                    "viscous Re 1600 Ma 0.1, RK2 (fluxorder 2: the reference runs 2 stages/step), dt 2e-3",
+        "flux_variant": "sigma = 0 on every face (-s_x = -s_y = -s_z = 0, sensor off): the blend (1 - sigma) * "
+                        "upwind + sigma * central equals the upwind flux, so the stage kernel forms only that; the "
+                        "reference also multiplies the eddy viscosity and Yoshizawa terms by sigma, so the "
+                        "Smagorinsky model is inert in this flag set (its kernel still runs every step and the "
+                        "stage kernel still forms the SGS terms)",
         "grid": [n + 2, n + 2, n + 2],
         "interior_nodes": n ** 3,
-        "stages_per_step": 3,
+        "stages_per_step": CFG["fluxorder"],
         "l2_policy": "inputs larger than L2 (~0.5 GB resident per stage vs 126 MB L2); no flush",
         "parallelism": "replicas (one independent block per GPU)",
     }
@@ -347,6 +355,131 @@ def run_batched(args, local):
     return out
 
 
+def _forms(coords, q0, nv, cfg, args, ws, local, clocks_for=None):
+    """Both forms of one workload: device-timed steps, per-launch stage-kernel
+    time and its HBM rate.  Returns (per-form dict, open blocks)."""
+    out, blocks = {}, {}
+    for prec in ("fp64", "mixed"):
+        blk = _block(prec, local, coords, q0, nv, **cfg)
+        blocks[prec] = blk
+        ms, clocks = _timed(blk, args.steps, args.warmup, ws, local, sample_clocks=(prec == clocks_for))
+        interior, stages = blk.interior_nodes, blk.stages
+        kms = _kernel_ms(blk, max(3, min(args.steps, 10)))
+        out[prec] = {"value": ws * interior * stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                     "kernel_avg_ms": kms, "achieved_gbs": B_ALG[prec] * interior / (kms / 1e3) / 1e9,
+                     "launches_per_step": blk.launches_per_step, "kchunk_autotuned": blk.kchunk}
+        if clocks is not None:
+            out[prec]["clocks"] = clocks
+    return out, blocks
+
+
+def pipe_peaks(local):
+    """Measured FP64 / FP32 FMA peaks (TFLOP/s) of this GPU (cb_pipe_peaks)."""
+    import ctypes
+
+    from chimera_comp_les_b200 import _lib
+    lib = _lib.load()
+    f64, f32 = ctypes.c_double(), ctypes.c_double()
+    if lib.cb_pipe_peaks(local, ctypes.byref(f64), ctypes.byref(f32)) != 0:
+        return None
+    return {"fp64_tflops": f64.value, "fp32_tflops": f32.value,
+            "source": "measured here by cb_pipe_peaks (dependent-FMA kernel on every SM, 2 flops per FMA)"}
+
+
+def compute_roofline(form, cfgkw, kernel_ms, interior, peaks):
+    """Compute-side roofline of the stage kernel: operations per cell-update
+    counted on the restatement (oracle/flops.py) x cell-updates per launch /
+    launch time, against the measured FMA peak of the form's arithmetic pipe.
+    The FP64 form is built without FMA contraction (every add and multiply
+    issues alone), so its attainable flop rate is half the FMA peak."""
+    from chimera_comp_les_b200 import workloads as W
+    from oracle import flops as FL
+    n = 16
+    coords = W.periodic_grid(n, 2 * math.pi, amp=0.05)
+    q = W.tgv_state(coords, gamma=1.4, ma=0.1)
+    c = FL.count_per_cell({k: v for k, v in cfgkw.items()}, coords, q)
+    fl = c["stage_flops"]
+    achieved = fl * interior / (kernel_ms / 1e3) / 1e12
+    pk = peaks["fp64_tflops"] if form == "fp64" else peaks["fp32_tflops"]
+    ceiling = pk / 2 if form == "fp64" else pk
+    return {"flops_per_cell": fl, "ops_per_cell": {k: round(v, 2) for k, v in c["stage"].items()},
+            "counted_on": "oracle restatement (operation-counting build) of this scheme, one time step / "
+                          "(interior nodes x stages); it forms every flux the reference forms, including "
+                          "any the blend multiplies by zero",
+            "achieved_tflops": achieved, "pipe": "FP64" if form == "fp64" else "FP32",
+            "peak_tflops": pk, "peak_source": peaks["source"], "frac": achieved / pk,
+            "attainable_tflops": ceiling, "frac_of_attainable": achieved / ceiling,
+            "attainable_note": ("no FMA contraction in the FP64 parity form: one flop per pipe instruction, "
+                                "half the FMA peak" if form == "fp64" else "FMA contraction on: FMA peak")}
+
+
+def _vs_oracle(n, coords, q0, nv, blocks, cfgkw):
+    """One full-size step of the oracle restatement against one step of each
+    GPU form from the same state."""
+    import oracle as O
+    from chimera_comp_les_b200 import diagnostics as D
+    ocfg = O.Config(mx=n + 2, my=n + 2, mz=n + 2, **{k: v for k, v in cfgkw.items()})
+    ora = O.Oracle(ocfg)
+    met = ora.metrics(O.to_padded(ocfg, coords))
+    nvp = ora.fill_ghosts(O.to_padded(ocfg, nv))
+    st = ora.initial_state(q0)
+    ora.steps(1, st, met, nvp)
+    q_ora = O.from_padded(st["q"])
+    out = {"steps": 1, "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]}
+    for prec, blk in blocks.items():
+        blk.SetInitialCondition(q0)
+        blk.RungeKutta(1)
+        l2, linf = D.field_errors(blk.Q(), q_ora)
+        out[prec] = {"rel_l2": l2, "rel_linf": linf}
+    return out
+
+
+def run_config5(args, local, n=512):
+    """BASELINE config 5 at its largest size on one GPU: decaying compressible
+    isotropic turbulence on a periodic [0, 2*pi]^3 Cartesian box of n^3 unique
+    nodes (DMDA (n+2)^3), Passot-Pouquet spectrum k0 4, u_rms 1, Mt 0.4, seed
+    5, rho 1, uniform p; Roe flux with the WENO reconstruction built here,
+    pure upwind (-les 1 -s_x 0 -s_y 0 -s_z 0), Smagorinsky CS 0.17^2, SSP-RK3,
+    dt from CFL 0.4.  Per form: cell-updates/s, stage-kernel GB/s, then the
+    per-field mixed-vs-FP64 error after ACC_STEPS steps."""
+    import torch
+
+    from chimera_comp_les_b200 import diagnostics as D
+    from chimera_comp_les_b200 import workloads as W
+    torch.cuda.set_device(local)
+    coords = W.periodic_grid(n, 2 * math.pi, amp=0.0)
+    q0 = W.isotropic_turbulence(n, 5, k_peak=4.0, mach_t=0.4, spectrum="passot_pouquet", u_rms=1.0)
+    r = q0[..., 0]
+    c = np.sqrt(1.4 * 0.4 * (q0[..., 4] - 0.5 * (q0[..., 1] ** 2 + q0[..., 2] ** 2 + q0[..., 3] ** 2) / r) / r)
+    lam = sum(float((np.abs(q0[..., 1 + a] / r) + c).max()) for a in range(3)) * n / (2 * math.pi)
+    del r, c
+    dt = math.floor(0.4 / lam * 1e6) / 1e6
+    opts = dict(CFG, fluxorder=3, flux="roe", s_x=0.0, s_y=0.0, s_z=0.0, ren=10000.0, ma=0.4, cs_const=0.17 ** 2,
+                dt=dt)
+    nv = np.zeros(coords.shape[:3])
+    out = {"workload": f"decaying isotropic turbulence {n}^3 (DMDA {n + 2}^3), Passot-Pouquet k0 4, u_rms 1, Mt 0.4, "
+                       "seed 5; WENO3 + Roe, pure upwind (sigma 0), Smagorinsky CS 0.17^2, SSP-RK3, dt from CFL 0.4",
+           "grid": [n + 2] * 3, "dt": dt, "interior_nodes": n ** 3}
+    final = {}
+    for prec in ("fp64", "mixed"):
+        blk = _block(prec, local, coords, q0, nv, **opts)
+        ms, _ = _timed(blk, args.steps, args.warmup, 1, local)
+        kms = _kernel_ms(blk, 3)
+        interior = blk.interior_nodes
+        out[prec] = {"value": interior * blk.stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                     "kernel_avg_ms": kms, "achieved_gbs": B_ALG[prec] * interior / (kms / 1e3) / 1e9,
+                     "kchunk_autotuned": blk.kchunk}
+        blk.SetInitialCondition(q0)
+        blk.RungeKutta(ACC_STEPS)
+        final[prec] = blk.Q()
+        blk.close()
+    l2, linf = D.field_errors(final["mixed"], final["fp64"])
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["mixed_vs_fp64_error"] = {"steps": ACC_STEPS, "rel_l2": l2, "rel_linf": linf,
+                                  "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]}
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import ctypes
     import torch
@@ -360,18 +493,7 @@ def run_ours(args, ws, rank, local):
     nv = np.zeros(coords.shape[:3])
     peak, peak_kind = measured_peaks()
 
-    forms = {}
-    blocks = {}
-    for prec in ("fp64", "mixed"):
-        blk = _block(prec, local, coords, q0, nv)
-        blocks[prec] = blk
-        ms, clocks = _timed(blk, args.steps, args.warmup, ws, local, sample_clocks=(prec == args.precision))
-        interior, stages = blk.interior_nodes, blk.stages
-        kms = _kernel_ms(blk, max(3, min(args.steps, 10)))
-        achieved = B_ALG[prec] * interior / (kms / 1e3) / 1e9
-        forms[prec] = {"value": ws * interior * stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
-                       "clocks": clocks, "kernel_avg_ms": kms, "achieved_gbs": achieved,
-                       "launches_per_step": blk.launches_per_step, "kchunk_autotuned": blk.kchunk}
+    forms, blocks = _forms(coords, q0, nv, {}, args, ws, local, clocks_for=args.precision)
     head = forms[args.precision]
     acc = _accuracy(blocks["fp64"], blocks["mixed"], q0) if rank == 0 else None
 
@@ -405,77 +527,83 @@ def run_ours(args, ws, rank, local):
     if not np.isfinite(q_out).all():
         raise RuntimeError("non-finite state after end-to-end steps")
 
-    # the same workload at sigma 0.5: every face forms the WENO3 + Rusanov
-    # upwind flux and the central flux and blends them
-    blend = None
-    if not args.no_blend:
-        blend = {"sigma": 0.5}
-        for prec in ("fp64", "mixed"):
-            bb = _block(prec, local, coords, q0, nv, s_x=0.5, s_y=0.5, s_z=0.5)
-            ms, _ = _timed(bb, args.steps, args.warmup, ws, local)
-            kms = _kernel_ms(bb, max(3, min(args.steps, 10)))
-            blend[prec] = {"value": ws * bb.interior_nodes * bb.stages * args.steps / (ms / 1e3),
-                           "ms_per_step": ms / args.steps, "kernel_avg_ms": kms,
-                           "achieved_gbs": B_ALG[prec] * bb.interior_nodes / (kms / 1e3) / 1e9}
-            bb.close()
-
-    batched = run_batched(args, local) if (ws == 1 and not args.no_batched) else None
-
     cpu = None
     vs_oracle = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import cpu_baseline as cb
         r = cb.run(n, steps=1, warmup=0, cfgkw=CFG)
         cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
-        # the same CPU leg, as the checker: one full-size step of the oracle
-        # against one step of each GPU form from the same state
-        import oracle as O
-        from chimera_comp_les_b200 import diagnostics as D
-        ocfg = O.Config(mx=n + 2, my=n + 2, mz=n + 2, **{k: v for k, v in CFG.items()})
-        ora = O.Oracle(ocfg)
-        met = ora.metrics(O.to_padded(ocfg, coords))
-        nvp = ora.fill_ghosts(O.to_padded(ocfg, nv))
-        st = ora.initial_state(q0)
-        ora.steps(1, st, met, nvp)
-        q_ora = O.from_padded(st["q"])
-        vs_oracle = {"steps": 1, "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]}
-        for prec, blk in blocks.items():
-            blk.SetInitialCondition(q0)
-            blk.RungeKutta(1)
-            l2, linf = D.field_errors(blk.Q(), q_ora)
-            vs_oracle[prec] = {"rel_l2": l2, "rel_linf": linf}
+        # the same CPU leg, as the checker
+        vs_oracle = _vs_oracle(n, coords, q0, nv, blocks, CFG)
+    for b in blocks.values():
+        b.close()
+
+    # the same workload with Roe's flux (no counterpart in the reference)
+    roe = None
+    if not args.no_extras:
+        roe_f, roe_b = _forms(coords, q0, nv, {"flux": "roe"}, args, ws, local)
+        roe = {"flux": "Roe with Harten's entropy fix, otherwise the headline workload", **roe_f,
+               "speedup_mixed_vs_fp64": roe_f["mixed"]["value"] / roe_f["fp64"]["value"]}
+        roe["mixed_vs_fp64_error"] = _accuracy(roe_b["fp64"], roe_b["mixed"], q0) if rank == 0 else None
+        for b in roe_b.values():
+            b.close()
+
+    # the reference's default hybrid scheme on the same TGV: WENO3 + Rusanov
+    # blended with the central flux, sigma 1 (central only) and 0.5 (both)
+    blends = None
+    if not args.no_blend:
+        blends = {}
+        for name, sig in (("sigma_1", 1.0), ("sigma_half", 0.5)):
+            f, bb = _forms(coords, q0, nv, dict(CFG_WENO3_BLEND, s_x=sig, s_y=sig, s_z=sig), args, ws, local)
+            blends[name] = {"sigma": sig, **{k: {kk: vv for kk, vv in v.items() if kk != "launches_per_step"}
+                                              for k, v in f.items()}}
+            for b in bb.values():
+                b.close()
+        blends["scheme"] = "WENO3 + Rusanov blended with the 4-point skew-symmetric central flux (-fluxorder 3, SSP-RK3)"
+
+    batched = run_batched(args, local) if (ws == 1 and not args.no_batched) else None
+    config5 = run_config5(args, local) if (ws == 1 and not args.no_config5) else None
 
     if rank == 0:
+        peaks = pipe_peaks(local)
+        comp = compute_roofline(args.precision, CFG, head["kernel_avg_ms"], n ** 3, peaks) if peaks else None
+        other_comp = (compute_roofline("fp64" if args.precision == "mixed" else "mixed", CFG,
+                                       forms["fp64" if args.precision == "mixed" else "mixed"]["kernel_avg_ms"],
+                                       n ** 3, peaks) if peaks else None)
         cfg = workload_config(n)
-        cfg["precision_form"] = args.precision
         other = "fp64" if args.precision == "mixed" else "mixed"
+        other_d = {k: v for k, v in forms[other].items() if k != "clocks"}
+        other_d["roofline_compute"] = other_comp
         line = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32-flux/f64-state" if args.precision == "mixed" else "f64",
+            "precision_form": args.precision,
             "data": "synthetic", "config": cfg,
             "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
                          "frac": head["achieved_gbs"] / peak,
                          "traffic": profile_traffic(args.precision),
                          "kernel": f"stage_kernel ({args.precision} form: fused RHS + RK combine)",
                          "kernel_avg_ms": head["kernel_avg_ms"], "bytes_per_cell": B_ALG[args.precision],
-                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
-            "clocks": head["clocks"],
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "compute": comp},
+            "clocks": head.get("clocks"),
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(q0.nbytes), "d2h_bytes_per_step": int(q0.nbytes)},
             "gpu_launches": head["launches_per_step"] * args.steps,
             "cpu_baseline": cpu,
-            other: {k: v for k, v in forms[other].items() if k != "clocks"},
+            other: other_d,
             "speedup_mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"],
             "mixed_vs_fp64_error": acc,
-            "blend_sigma_half": blend,
+            "roe": roe,
+            "weno3_blend": blends,
+            "config5_512": config5,
             "batched": batched,
             "vs_oracle": vs_oracle,
+            "pipe_peaks": peaks,
         }
         print(json.dumps(line), flush=True)
-    for b in blocks.values():
-        b.close()
 
 
 # ------------------------------------------------------------ size sweep --
@@ -712,12 +840,13 @@ def run_sharded(args, ws, rank, local):
         cfg.update({"workload": cfg["workload"].replace(f"{n}^3 (DMDA {n + 2}^3)",
                                                         f"{n}x{n}x{n * ws} box in {ws} k-slabs of {n}^3 (DMDA {n + 2}^3 each)"),
                     "parallelism": f"k-slabs over {ws} GPUs, 2-node halo exchange per stage (NCCL send/recv)",
-                    "precision_form": prec, "interior_nodes": interior * ws})
+                    "interior_nodes": interior * ws})
         line = {
             "metric": METRIC, "value": ws * interior * stages * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32-flux/f64-state" if prec == "mixed" else "f64", "data": "synthetic", "config": cfg,
+            "dtype": "f32-flux/f64-state" if prec == "mixed" else "f64", "precision_form": prec,
+            "data": "synthetic", "config": cfg,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profile_traffic(prec),
                          "kernel": f"stage phase ({prec} form: persistent stage kernel + local halo gather + pack)",
@@ -744,7 +873,9 @@ def main():
                     help="form reported as the headline value (both are measured)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the multi-block batched measurement")
-    ap.add_argument("--no-blend", action="store_true", help="skip the sigma 0.5 measurement of the headline workload")
+    ap.add_argument("--no-blend", action="store_true", help="skip the WENO3 blend (sigma 1 and 0.5) on the headline TGV")
+    ap.add_argument("--no-extras", action="store_true", help="skip the Roe-flux measurement of the headline workload")
+    ap.add_argument("--no-config5", action="store_true", help="skip the 512^3 isotropic-turbulence measurement")
     ap.add_argument("--sweep", default="", help="comma-separated sizes, e.g. 128,256,384,512: isotropic-turbulence "
                                                   "size sweep, one JSON line per size instead of the bench line")
     ap.add_argument("--workload", default="tgv", choices=["tgv", "sphere"],

@@ -98,6 +98,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.cb_launches_per_step.restype = C.c_int
     lib.cb_last_error.argtypes = [P]
     lib.cb_last_error.restype = C.c_char_p
+    lib.cb_pipe_peaks.argtypes = [C.c_int, D, D]
+    lib.cb_pipe_peaks.restype = C.c_int
     # immersed bodies
     for name, args in [
         ("cb_ibm_set_surface", [P, C.c_int, C.c_int, C.c_int, P, P, P, D, D, D]),

@@ -23,6 +23,7 @@ SOURCES = [
     (os.path.join(PKG_DIR, "csrc", "cb_noalloc.cu"), FP64_FLAGS),
     (os.path.join(PKG_DIR, "csrc", "cb_batch.cu"), FP64_FLAGS),
     (os.path.join(PKG_DIR, "csrc", "cb_mixed.cu"), MIXED_FLAGS),
+    (os.path.join(PKG_DIR, "csrc", "cb_peaks.cu"), FP64_FLAGS),
 ]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 NVCC_FLAGS = [

@@ -7,17 +7,21 @@
 // memory they own.  Everything this computation needs beyond those inputs
 // and that output -- the padded SoA planes of the state, metrics, mask, eddy
 // viscosity, filter width and RHS, plus a pointer table -- lives in the
-// file-scope arrays below.  They are part of the library's device image: every
-// GPU that loads the library holds them (about 20 MB) until the process
-// exits, whether or not this entry point is ever called.
+// file-scope __device__ arrays below (in an anonymous namespace: internal to
+// this translation unit).  They are part of this file's device module: once
+// the module is loaded on a GPU (on first use of a kernel of the library under
+// CUDA's default lazy loading, at start-up with CUDA_MODULE_LOADING=EAGER) that
+// GPU holds them (about 20 MB) until the process exits.
 //
 // Sharing: every call uses the same arrays and they keep the last call's
 // contents.  Calls that overlap on the GPU (different streams or threads)
 // race on them; serialise calls, e.g. one stream.
 //
-// Set-up: the first call on a device (with that device current) looks up the
-// arrays' device addresses with cudaGetSymbolAddress and opts the RHS kernels
-// into their shared memory; make that first call before any stream capture.
+// Set-up: every call, with the caller's device current, looks up the arrays'
+// device addresses with cudaGetSymbolAddress (no allocation).  The first call
+// on a device, and the first after a device reset moved the arrays, also opts
+// the RHS kernels into their shared memory; make that first call before any
+// stream capture.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -111,16 +115,25 @@ extern "C" int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return na_fail(CB_E_CUDA, "no current CUDA device");
   NaDevice &nd = g_dev[dev];
-  if (!nd.ready) {
-    // once per device, with that device current: device addresses of the arrays
-    cudaError_t e = cudaGetSymbolAddress((void **)&nd.scratch, na_scratch);
+  {
+    // device addresses of the arrays on the current device, every call: a
+    // device reset since the last call would have moved them
+    double *scratch = nullptr, **ptab = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&scratch, na_scratch);
     if (e != cudaSuccess) return na_fail(CB_E_CUDA, cudaGetErrorString(e));
-    e = cudaGetSymbolAddress((void **)&nd.ptab, na_ptab);
+    e = cudaGetSymbolAddress((void **)&ptab, na_ptab);
     if (e != cudaSuccess) return na_fail(CB_E_CUDA, cudaGetErrorString(e));
-    if ((e = na_attr<true, true>()) != cudaSuccess || (e = na_attr<true, false>()) != cudaSuccess ||
-        (e = na_attr<false, true>()) != cudaSuccess || (e = na_attr<false, false>()) != cudaSuccess)
-      return na_fail(CB_E_CUDA, cudaGetErrorString(e));
-    nd.ready = true;
+    if (!nd.ready || scratch != nd.scratch || ptab != nd.ptab) {
+      // first call on this device (or the module was reloaded): the kernels'
+      // shared-memory opt-in
+      nd.ready = false;
+      if ((e = na_attr<true, true>()) != cudaSuccess || (e = na_attr<true, false>()) != cudaSuccess ||
+          (e = na_attr<false, true>()) != cudaSuccess || (e = na_attr<false, false>()) != cudaSuccess)
+        return na_fail(CB_E_CUDA, cudaGetErrorString(e));
+      nd.scratch = scratch;
+      nd.ptab = ptab;
+      nd.ready = true;
+    }
   }
   cudaStream_t s = (cudaStream_t)stream;
   int sms = 148;

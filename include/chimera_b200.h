@@ -257,6 +257,13 @@ int cb_launches_per_step(const cb_ctx *ctx);
 const char *cb_last_error(const cb_ctx *ctx);
 int cb_abi_version(void);
 
+/* Arithmetic-pipe peaks of GPU `device` in TFLOP/s (2 flops per fused
+ * multiply-add), measured by a dependent-FMA kernel over every SM: the
+ * ceiling of the compute roofline of the stage kernels.  A measurement
+ * helper with no counterpart in the reference.  Allocates a small buffer,
+ * synchronises. */
+int cb_pipe_peaks(int device, double *fp64_tflops, double *fp32_tflops);
+
 /* formRHS without any device allocation, for callers that may not call
  * cudaMalloc (a solver running inside a memory pool owned by another
  * framework, or a host that forbids device allocation after start-up).
@@ -269,14 +276,17 @@ int cb_abi_version(void);
  * boundary nodes).  Work is enqueued on `stream` (a cudaStream_t, NULL for the
  * default stream); the caller synchronises.
  *
- * Scratch lives in a file-scope device array sized for
+ * Scratch lives in a file-scope __device__ array sized for
  * CB_NOALLOC_MAX_PLANE padded nodes per field, (mx+4 rounded up to 16) *
- * (my+4) * (mz+4); larger grids are rejected with CB_E_ARG.  The array
- * (about 20 MB) is held by every GPU that loads the library until the
- * process exits.  All calls share it and it keeps the last call's contents,
- * so calls that overlap on the GPU race: serialise them.  The first call on a
- * device does a one-time set-up (symbol lookup, kernel attributes); make it
- * before any stream capture.  Only fully periodic blocks are accepted. */
+ * (my+4) * (mz+4); larger grids are rejected with CB_E_ARG.  A GPU holds the
+ * array (about 20 MB) from the time the library's device module is loaded
+ * there (first kernel use under CUDA's default lazy loading, start-up with
+ * CUDA_MODULE_LOADING=EAGER) until the process exits.  All calls share it and
+ * it keeps the last call's contents, so calls that overlap on the GPU race:
+ * serialise them.  Every call looks the array's address up on the current
+ * device (cudaGetSymbolAddress, no allocation); the first call on a device
+ * also sets the kernels' shared-memory attributes: make it before any stream
+ * capture.  Only fully periodic blocks are accepted. */
 #define CB_NOALLOC_MAX_PLANE 98304LL
 int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const double *d_q, const double *d_nvert,
                    const double *d_nut, double *d_rhs, void *stream);

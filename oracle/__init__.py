@@ -29,9 +29,12 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(_HERE, "_build", "liboracle.so")
+ORACLE_COUNT_SO = os.path.join(_HERE, "_build", "liboracle_count.so")
 REF_SO = os.path.join(_HERE, "_ref", "libchimera_ref.so")
 REF_SO_O3 = os.path.join(_HERE, "_ref", "libchimera_ref_O3.so")
-REF_SRC_DIR = os.environ.get("CHIMERA_REF_DIR", "/root/reference")
+# the reference checkout: CHIMERA_REF_DIR, else a sibling directory of this
+# repository named "reference"
+REF_SRC_DIR = os.environ.get("CHIMERA_REF_DIR") or os.path.normpath(os.path.join(_HERE, "..", "..", "reference"))
 
 
 @dataclass
@@ -184,12 +187,26 @@ def build_oracle(force: bool = False) -> str:
     return ORACLE_SO
 
 
-class Oracle:
-    """ctypes front end of oracle/src/cb_oracle.c (padded SoA numpy arrays)."""
+def build_oracle_count(force: bool = False) -> str:
+    """Compile the operation-counting build of the restatement if missing."""
+    if force or not os.path.exists(ORACLE_COUNT_SO):
+        subprocess.run(["make", "-s", "-C", _HERE, "_build/liboracle_count.so"], check=True)
+    return ORACLE_COUNT_SO
 
-    def __init__(self, cfg: Config):
+
+class Oracle:
+    """ctypes front end of oracle/src/cb_oracle.c (padded SoA numpy arrays).
+
+    counting=True loads the operation-counting build of the same source
+    (identical results; ``count_reset`` / ``count_read`` give the number of
+    floating-point operations by kind since the last reset)."""
+
+    COUNT_KINDS = ("add", "mul", "div", "sqrt", "pow", "cmp", "abs")
+
+    def __init__(self, cfg: Config, counting: bool = False):
         self.cfg = cfg
-        self.lib = C.CDLL(build_oracle())
+        self.lib = C.CDLL(build_oracle_count() if counting else build_oracle())
+        self.counting = counting
         self.c = _ccfg(cfg)
         PP = C.POINTER(C.POINTER(C.c_double))
         D = C.POINTER(C.c_double)
@@ -219,6 +236,14 @@ class Oracle:
         L.cbo_dynamic_smagorinsky.restype = C.c_int
         L.cbo_eddy_viscosity_dyn.argtypes = [C.c_void_p, PP, PP, PP, PP, PP, D, D, D, D]
         self._cp = C.byref(self.c)
+
+    def count_reset(self) -> None:
+        self.lib.cbo_count_reset()
+
+    def count_read(self) -> dict:
+        buf = (C.c_longlong * len(self.COUNT_KINDS))()
+        self.lib.cbo_count_read(buf)
+        return dict(zip(self.COUNT_KINDS, (int(v) for v in buf)))
 
     def zeros(self, nc: int) -> np.ndarray:
         return np.zeros((nc,) + self.cfg.padded_shape)
