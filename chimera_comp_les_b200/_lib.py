@@ -42,6 +42,7 @@ class CbConfig(C.Structure):
         ("sigma_thrsh", C.c_double), ("flux", C.c_int), ("max_cs", C.c_double), ("twall", C.c_double),
         ("twod", C.c_int), ("i_homo_filter", C.c_int), ("j_homo_filter", C.c_int), ("k_homo_filter", C.c_int),
         ("testfilter_ik", C.c_int), ("visT", C.c_int), ("tref", C.c_double), ("abc", C.c_int),
+        ("weno_order", C.c_int),
     ]
 
 

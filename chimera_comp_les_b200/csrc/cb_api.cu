@@ -158,14 +158,7 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t set_stage_attr() {
-  const int sm = (int)STAGE_SMEM_BYTES;
-  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 0>, attr, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, LES, VISC, RHSM, 1>, attr, sm);
-  if constexpr (!RHSM) {  // the no-IBM variants of the time step
-    if (e == cudaSuccess) e = stage_nv0_attrs<double, false, LES, VISC>();
-  }
-  return e;
+  return stage_attrs<double, false, LES, VISC, RHSM>();
 }
 
 // Opt every stage-kernel variant into its dynamic shared memory on the
@@ -182,10 +175,10 @@ static cudaError_t set_stage_attrs() {
   return set_stage_attr<false, false, true>();
 }
 
-// Flux bits of the stage kernel: Roe, and with LES and the sensor off the
-// constant blend weight s_x = s_y = s_z when it is exactly 1 or 0.
+// Flux bits of the stage kernel: Roe, WENO5-JS, and with LES and the sensor
+// off the constant blend weight s_x = s_y = s_z when it is exactly 1 or 0.
 static int flux_bits(const cb_ctx *c) {
-  int fl = c->dc.flux == 1 ? FLUX_ROE : 0;
+  int fl = (c->dc.flux == 1 ? FLUX_ROE : 0) | (c->cfg.weno_order == 5 ? FLUX_W5 : 0);
   const cb_config &f = c->cfg;
   if (f.les && !f.calc_sigma && f.s_x == f.s_y && f.s_y == f.s_z) {
     if (f.s_x == 1.0) fl |= FLUX_SIGMA1;
@@ -196,14 +189,13 @@ static int flux_bits(const cb_ctx *c) {
 
 template <bool LES, bool VISC, bool RHSM>
 static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt) {
-  auto kern = c->dc.flux == 1 ? stage_kernel<double, false, LES, VISC, RHSM, 1> : stage_kernel<double, false, LES, VISC, RHSM, 0>;
-  size_t smem = STAGE_SMEM_BYTES;
+  const int fl = flux_bits(c);
+  auto kern = stage_gen_kernel<double, false, LES, VISC, RHSM>(fl);
+  const bool nv = !RHSM && c->nv0;
   if constexpr (!RHSM)
-    if (c->nv0) {
-      kern = stage_nv0_kernel<double, false, LES, VISC>(flux_bits(c));
-      smem = stage_smem<double, false, true>();
-    }
-  kern<<<stage_grid(c->dc, c->kchunk, c->sms), SNT, smem, c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
+    if (c->nv0) kern = stage_nv0_kernel<double, false, LES, VISC>(fl);
+  kern<<<stage_grid(c->dc, c->kchunk, c->sms, stage_tile_rows(fl)), stage_threads(fl), stage_smem_for<double, false>(fl, nv),
+         c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
   return cudaGetLastError();
 }
 
@@ -573,6 +565,8 @@ void cb_config_default(cb_config *cfg, int mx, int my, int mz) {
   cfg->twod = 0;
   cfg->visT = 0;
   cfg->tref = 273.15;          // rhs.c:1410
+  cfg->abc = 0;
+  cfg->weno_order = 3;         // the reference's WENO3
 }
 
 int cb_create(const cb_config *cfg, cb_ctx **out) {
@@ -597,6 +591,8 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
     for (int b = 0; b < 6; b++) c->fully_periodic = c->fully_periodic && bc[b] == 7;
   }
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3) return bail(CB_E_ARG, "fluxorder must be 1, 2 or 3");
+  if (cfg->weno_order != 3 && cfg->weno_order != 5) return bail(CB_E_ARG, "weno_order must be 3 or 5");
+  if (cfg->weno_order == 5 && cfg->fluxorder != 3) return bail(CB_E_ARG, "weno_order 5 needs fluxorder 3");
   if (cfg->eno_order != 2 && cfg->eno_order != 3) return bail(CB_E_ARG, "ENOorder must be 2 or 3");
   if (cfg->les < 0) return bail(CB_E_ARG, "les must be >= 0");
   if (les_dynamic(*cfg) && !(cfg->max_cs >= 0.0)) return bail(CB_E_ARG, "max_cs must be >= 0");
@@ -692,7 +688,8 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   // 2 in the mixed form); a chunk's prologue costs about one plane.  The
   // autotuner (cb_autotune) refines this by measurement.
   {
-    const int tiles = ((cfg->mx - 2 + BX - 1) / BX) * ((cfg->my - 2 + BY - 1) / BY);
+    const int by = cfg->weno_order == 5 ? SBY_W5 : BY;
+    const int tiles = ((cfg->mx - 2 + BX - 1) / BX) * ((cfg->my - 2 + by - 1) / by);
     const int nk = cfg->mz - 2;
     const int slots = c->sms * (cfg->precision == CB_MIXED ? 2 : 1);
     double best = 1e30;

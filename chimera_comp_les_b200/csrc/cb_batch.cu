@@ -320,7 +320,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
   };
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
       (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
-      (cfg->les && cfg->calc_sigma) || cfg->flux != 0)
+      (cfg->les && cfg->calc_sigma) || cfg->flux != 0 || cfg->weno_order != 3)
     return bail(CB_E_UNSUPPORTED, "option combination not built");
   if (cfg->visT && !(cfg->tref > 0.0)) return bail(CB_E_ARG, "Tref must be > 0 with visT");
   b->dev = cfg->device;

@@ -13,12 +13,14 @@ cudaError_t set_stage_attrs_mixed();
 // Grid of a stage-kernel launch: (tile columns in i, in j, k-chunks) for
 // kchunk > 0; `slots` CTAs (the resident ones) for the balanced segments of
 // kchunk == 0.
-inline dim3 stage_grid(const DevCfg &c, int kchunk, int slots) {
+// by: the tile height of the variant (StageGeo::BY).
+inline dim3 stage_grid(const DevCfg &c, int kchunk, int slots, int by = SBY) {
   if (kchunk <= 0) return dim3((unsigned)slots);
-  return dim3((c.mx - 2 + SBX - 1) / SBX, (c.my - 2 + SBY - 1) / SBY, (c.mz - 2 + kchunk - 1) / kchunk);
+  return dim3((c.mx - 2 + SBX - 1) / SBX, (c.my - 2 + by - 1) / by, (c.mz - 2 + kchunk - 1) / kchunk);
 }
+inline int stage_tile_rows(int fl) { return (fl & FLUX_W5) ? SBY_W5 : SBY; }
 
-// fl: flux bits (FLUX_ROE; the constant-sigma bits apply with nv0 only);
+// fl: flux bits (FLUX_ROE, FLUX_W5; the constant-sigma bits apply with nv0 only);
 // nv0: nvert is zero everywhere, the variant without any nvert test (time step
 // only); slots: CTAs of the balanced-segment shape (kchunk 0)
 cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt,

@@ -9,28 +9,17 @@ namespace cb {
 namespace {
 template <bool LES, bool VISC, bool RHSM>
 cudaError_t attr1() {
-  const int sm = (int)STAGE_SMEM_BYTES_MIXED;
-  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM, 0>, attr, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, true, LES, VISC, RHSM, 1>, attr, sm);
-  if constexpr (!RHSM) {  // the no-IBM variants of the time step
-    if (e == cudaSuccess) e = stage_nv0_attrs<float, true, LES, VISC>();
-  }
-  return e;
+  return stage_attrs<float, true, LES, VISC, RHSM>();
 }
 template <bool LES, bool VISC, bool RHSM>
 void launch1(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt, int kchunk,
              int fl, bool nv0, int slots, cudaStream_t s) {
-  const dim3 grid = stage_grid(c, kchunk, slots);
-  const bool roe = (fl & FLUX_ROE) != 0;
-  auto kern = roe ? stage_kernel<float, true, LES, VISC, RHSM, 1> : stage_kernel<float, true, LES, VISC, RHSM, 0>;
-  size_t smem = STAGE_SMEM_BYTES_MIXED;
+  const dim3 grid = stage_grid(c, kchunk, slots, stage_tile_rows(fl));
+  auto kern = stage_gen_kernel<float, true, LES, VISC, RHSM>(fl);
+  const bool nv = !RHSM && nv0;
   if constexpr (!RHSM)
-    if (nv0) {
-      kern = stage_nv0_kernel<float, true, LES, VISC>(fl);
-      smem = stage_smem<float, true, true>();
-    }
-  kern<<<grid, SNT, smem, s>>>(c, F, istage, alfa, beta, adt, kchunk);
+    if (nv0) kern = stage_nv0_kernel<float, true, LES, VISC>(fl);
+  kern<<<grid, stage_threads(fl), stage_smem_for<float, true>(fl, nv), s>>>(c, F, istage, alfa, beta, adt, kchunk);
 }
 
 __global__ void mixed_prep_kernel(const DevCfg c, const double *const *met, const double *delta2, const double *aj,

@@ -83,7 +83,8 @@ extern "C" int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const 
   for (int b = 0; b < 6; b++)
     if (cfg->bctype[b] != 7) return na_fail(CB_E_UNSUPPORTED, "only fully periodic blocks (bctype 7) are built");
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
-      (cfg->les != 0 && cfg->les != 1) || cfg->precision != CB_FP64 || (cfg->les && cfg->calc_sigma) || cfg->flux != 0)
+      (cfg->les != 0 && cfg->les != 1) || cfg->precision != CB_FP64 || (cfg->les && cfg->calc_sigma) || cfg->flux != 0 ||
+      cfg->weno_order != 3)
     return na_fail(CB_E_UNSUPPORTED, "option combination not built");
   if (cfg->visT && !(cfg->tref > 0.0)) return na_fail(CB_E_ARG, "Tref must be > 0 with visT");
   DevCfg d{};

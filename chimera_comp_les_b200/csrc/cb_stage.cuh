@@ -19,13 +19,13 @@
 //     gcl = sum_d (h_d(+1/2) - h_d(-1/2)); the constant part H_ref = E_ref + p_ref of the
 //     energy flux is carried in FP32 (its error is relative to H_ref * dU).
 //
-// Execution shape (B200): a block owns a SBX x SBY column of interior nodes and
-// marches along k through a chunk of planes.  A ring of four node planes
-// (k-1 .. k+2, each with a two-node halo in i and j) lives in shared memory
-// holding the conserved state and the derived p, u, v, w, T=p/rho, so every
-// division of the EOS / CalcUCat happens once per node.  Each face flux is
-// computed exactly once per plane.  Metrics, nvert and nu_t are read through
-// the read-only cache.
+// Execution shape (B200): a block owns a 32 x BY column of interior nodes and
+// marches along k through a chunk of planes.  A ring of node planes (k-1 ..
+// k+2, each with a two-node halo in i and j; k-2 .. k+3 for the WENO5-JS
+// variants) lives in shared memory holding the conserved state and the
+// derived p, u, v, w, T=p/rho, so every division of the EOS / CalcUCat happens
+// once per node.  Each face flux is computed exactly once per plane.
+// Metrics, nvert and nu_t are read through the read-only cache.
 #pragma once
 #include "cb_common.cuh"
 
@@ -54,6 +54,27 @@ struct TileShape {
   static constexpr int PX = BX + 4, PY = BY + 4, PN = PX * PY;
   static constexpr int NXF = (BX + 1) * BY;
   static constexpr int NYF = BX * (BY + 1);
+};
+
+// FLUX bits of the stage kernel (see conv_face): Roe's flux, a constant LES
+// blend weight of exactly 1 or 0, and WENO5-JS reconstruction.
+constexpr int FLUX_ROE = 1, FLUX_SIGMA1 = 2, FLUX_SIGMA0 = 4, FLUX_W5 = 8;
+
+// Tile geometry of a stage-kernel variant.  The WENO3/MUSCL stencil reaches
+// one node beyond the face's two nodes: a ring of 4 planes (k-1 .. k+2) and a
+// 32 x 7 tile of 256 threads.  WENO5-JS reaches two: a ring of 6 planes
+// (k-2 .. k+3), which fits the shared memory of one block (FP64) or two
+// (mixed) per SM with a 32 x 5 tile of 192 threads.  The i/j halo stays two
+// nodes: the few stencil nodes beyond it are read from global memory.
+template <int FLUX>
+struct StageGeo {
+  static constexpr bool W5 = (FLUX & FLUX_W5) != 0;
+  static constexpr int BX = 32, BY = W5 ? 5 : 7, NT = BX * (BY + 1);
+  static constexpr int NPL = W5 ? 6 : 4;  // ring planes
+  static constexpr int H = W5 ? 2 : 1;    // ring planes below the current one
+  using Tile = TileShape<BX, BY>;
+  static constexpr int NXF = Tile::NXF, NYF = Tile::NYF, NZF = BX * BY;
+  static_assert(NXF <= NT && NYF <= NT && NZF <= NT, "one face direction per round of the schedule");
 };
 
 // Selections by a runtime direction d without dynamic indexing (which would
@@ -103,33 +124,43 @@ __device__ __forceinline__ NRef nshift(NRef n, int d, int s) {
   return n;
 }
 
-template <typename R, int BX, int BY>
+template <typename R, int BX, int BY, int NPL = 4>
 struct Ring {
+  static constexpr int PX = TileShape<BX, BY>::PX, PY = TileShape<BX, BY>::PY;
+  static constexpr int H = (NPL - 2) / 2;  // ring planes below the current one
   R *pl;
-  const unsigned char *nvc;  // [4][PN] nvert * 4 (exact when DevCfg::nvq)
-  int sb;  // slot of relative plane r is (sb + r + 1) & 3: a rotation, no table
-  __device__ __forceinline__ int slot(int r) const { return (sb + r + 1) & 3; }
-  __device__ __forceinline__ R get(int f, NRef n) const {
-    return pl[((slot(n.r) * NF + f) * TileShape<BX, BY>::PY + n.y) * TileShape<BX, BY>::PX + n.x];
+  const unsigned char *nvc;  // [NPL][PN] nvert * 4 (exact when DevCfg::nvq)
+  // slot of relative plane r (-H .. NPL-H-1) is sb + r + H modulo NPL, with
+  // sb the slot of the lowest plane: a rotation, no table
+  int sb;
+  __device__ __forceinline__ int slot(int r) const {
+    if constexpr (NPL == 4) return (sb + r + 1) & 3;
+    const int t = sb + r + H;
+    return t >= NPL ? t - NPL : t;
   }
-  __device__ __forceinline__ double nv(NRef n) const {
-    return 0.25 * (double)nvc[(slot(n.r) * TileShape<BX, BY>::PY + n.y) * TileShape<BX, BY>::PX + n.x];
-  }
+  __device__ __forceinline__ R get(int f, NRef n) const { return pl[((slot(n.r) * NF + f) * PY + n.y) * PX + n.x]; }
+  __device__ __forceinline__ double nv(NRef n) const { return 0.25 * (double)nvc[(slot(n.r) * PY + n.y) * PX + n.x]; }
+  // a node of the i/j halo rows the ring holds (the k range is always held)
+  __device__ __forceinline__ bool holds(NRef n) const { return n.x >= 0 && n.x < PX && n.y >= 0 && n.y < PY; }
 };
 
 // nvert of a ring node: from shared memory when the byte code is exact, else
 // from global memory at g
-template <typename R, int BX, int BY>
-__device__ __forceinline__ double nvert_at(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef n,
-                                           long long g) {
+template <class RG>
+__device__ __forceinline__ double nvert_at(const DevCfg &c, const DevFields &F, const RG &Rg, NRef n, long long g) {
   return c.nvq ? Rg.nv(n) : ldg(F.nvert + g);
 }
 // NV0: the block's nvert is zero everywhere (no immersed body), known on the
 // host, so every nvert test folds away at compile time
-template <bool NV0, typename R, int BX, int BY>
-__device__ __forceinline__ double nvert_v(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef n,
-                                          long long g) {
+template <bool NV0, class RG>
+__device__ __forceinline__ double nvert_v(const DevCfg &c, const DevFields &F, const RG &Rg, NRef n, long long g) {
   return NV0 ? 0.0 : nvert_at(c, F, Rg, n, g);
+}
+// the same for a node that may lie beyond the ring's i/j halo
+template <bool NV0, class RG>
+__device__ __forceinline__ double nvert_far(const DevCfg &c, const DevFields &F, const RG &Rg, NRef n, long long g) {
+  if (NV0) return 0.0;
+  return (c.nvq && Rg.holds(n)) ? Rg.nv(n) : ldg(F.nvert + g);
 }
 
 // ---------------------------------------------------------------- recon --
@@ -172,6 +203,55 @@ template <typename R>
 __device__ __forceinline__ R eno_l(R qm, R q0, R qp, int k) {
   if (k == 2) return R(0.5) * q0 + R(0.5) * qm;
   return qm * R(0.3333333333333333) + q0 * R(0.8333333333333333) - qp * R(0.1666666666666666);
+}
+
+// WENO5-JS (Jiang & Shu, J. Comput. Phys. 126 (1996) 202-228; no counterpart
+// in the reference): value at x_{i+1/2} from a..e = v_{i-2..i+2}, left-biased;
+// candidates q_k (times 6), smoothness beta_k = 13/12 (2nd difference)^2 +
+// 1/4 (slope)^2, weights d_k / (eps + beta_k)^2 with d = (0.1, 0.6, 0.3) and
+// eps = 1e-6, value sum(alpha_k q_k) / (6 sum(alpha_k)).  The right-biased
+// value at x_{i+1/2} is weno5(v_{i+3}, .., v_{i-1}).  Same operation order as
+// the oracle's restatement (bit-identical in the FP64 form).
+template <typename R>
+__device__ __forceinline__ R weno5(R a, R b, R c, R d, R e) {
+  const R eps = R(1e-6), c13 = R(13.0 / 12.0);
+  const R q0 = (R(2.0) * a - R(7.0) * b) + R(11.0) * c;
+  const R q1 = (R(5.0) * c - b) + R(2.0) * d;
+  const R q2 = (R(2.0) * c + R(5.0) * d) - e;
+  const R t0 = (a - R(2.0) * b) + c, u0 = (a - R(4.0) * b) + R(3.0) * c;
+  const R t1 = (b - R(2.0) * c) + d, u1 = b - d;
+  const R t2 = (c - R(2.0) * d) + e, u2 = (R(3.0) * c - R(4.0) * d) + e;
+  const R b0 = c13 * (t0 * t0) + R(0.25) * (u0 * u0);
+  const R b1 = c13 * (t1 * t1) + R(0.25) * (u1 * u1);
+  const R b2 = c13 * (t2 * t2) + R(0.25) * (u2 * u2);
+  const R a0 = R(0.1) / ((eps + b0) * (eps + b0));
+  const R a1 = R(0.6) / ((eps + b1) * (eps + b1));
+  const R a2 = R(0.3) / ((eps + b2) * (eps + b2));
+  return ((a0 * q0 + a1 * q1) + a2 * q2) / (R(6.0) * ((a0 + a1) + a2));
+}
+
+// Conserved state and pressure of one node as the ring stores them, from its
+// raw FP64 state v (EqOfState rhs.c:4850; the mixed form shifts by the
+// reference state); pst/pin: the carried pressure of the FP64 form.  The
+// ring's derive pass and the global-memory path of far stencil nodes share
+// this arithmetic.
+template <typename R, bool MIX>
+__device__ __forceinline__ void node_qp(const DevCfg &c, const double v[5], bool pst, double pin, R q[5], R &p) {
+  double pp = 0.0, e = v[4];
+  if (v[0] != 0.0) {
+    if (MIX) {
+      const double ri = 1.0 / v[0];
+      pp = (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) * ri);
+      e -= c.e_ref;
+      pp -= c.p_ref;
+    } else {
+      pp = pst ? pin : (c.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++) q[a] = R(v[a]);
+  q[4] = R(e);
+  p = R(pp);
 }
 
 // Rusanov flux on reconstructed states (rhs.c:2769-2810), same operation
@@ -246,6 +326,53 @@ __device__ __forceinline__ void roe(const R QL[5], const R QR[5], R pL, R pR, co
 }
 
 // ------------------------------------------------------- inviscid face ----
+// WENO5-JS states of the face pos+1/2 along d (node a at stencil offset 0);
+// Q/P hold offsets -1 .. 2 from the ring.  Returns false, leaving the states
+// alone, where the stencil pos-2 .. pos+3 leaves the nodes 0 .. m-1 or holds
+// a wall node (nvert > 2.9).  Offsets -2 and +3 come from the ring when it
+// holds them (always along k) and otherwise from global memory through the
+// ring's own node arithmetic.
+template <typename R, bool MIX, bool NV0, class RG>
+__device__ __forceinline__ bool weno5_face(const DevCfg &c, const DevFields &F, const RG &Rg, NRef a, int d, int pos,
+                                           int m, long long g0, long long sd, const R Q[4][5], const R P[4], R QL[5],
+                                           R QR[5], R &pL, R &pR) {
+  if (pos < 2 || pos > m - 4) return false;
+  const NRef nm2 = nshift(a, d, -2), np3 = nshift(a, d, 3);
+  if (!NV0) {
+    if (nvert_far<NV0>(c, F, Rg, nm2, g0 - 2 * sd) > BLANKWALL || nvert_v<NV0>(c, F, Rg, nshift(a, d, -1), g0 - sd) > BLANKWALL ||
+        nvert_v<NV0>(c, F, Rg, nshift(a, d, 2), g0 + 2 * sd) > BLANKWALL ||
+        nvert_far<NV0>(c, F, Rg, np3, g0 + 3 * sd) > BLANKWALL)
+      return false;
+  }
+  R Qm[5], Pm, Qp[5], Pp;
+  const bool pst = !MIX && F.pin != nullptr;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const NRef n = t ? np3 : nm2;
+    R *qd = t ? Qp : Qm;
+    R &pd = t ? Pp : Pm;
+    if (d == 2 || Rg.holds(n)) {
+#pragma unroll
+      for (int q = 0; q < 5; q++) qd[q] = Rg.get(F_RHO + q, n);
+      pd = Rg.get(F_P, n);
+    } else {
+      const long long g = g0 + (t ? 3 : -2) * sd;
+      double v[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) v[q] = ldg(F.q[q] + g);
+      node_qp<R, MIX>(c, v, pst, pst ? ldg(F.pin + g) : 0.0, qd, pd);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 5; q++) {
+    QL[q] = weno5(Qm[q], Q[0][q], Q[1][q], Q[2][q], Q[3][q]);
+    QR[q] = weno5(Qp[q], Q[3][q], Q[2][q], Q[1][q], Q[0][q]);
+  }
+  pL = weno5(Pm, P[0], P[1], P[2], P[3]);
+  pR = weno5(Pp, P[3], P[2], P[1], P[0]);
+  return true;
+}
+
 // Face between node A (tile ref a, global (gi,gj,gk)) and A + e_d.
 // DIR >= 0: the face direction as a compile-time constant, so every stencil
 // shift, stride and metric selection folds into fixed offsets; DIR = -1: the
@@ -256,9 +383,12 @@ __device__ __forceinline__ void roe(const R QL[5], const R QR[5], R pL, R pR, co
 // is 0, and the face then skips the part the blend multiplies by exactly
 // zero: (1 - 1) * Fw + 1 * Fc = Fc and (1 - 0) * Fw + 0 * Fc = Fw for finite
 // fluxes (the sign of a zero flux aside), so the result is the reference's.
-constexpr int FLUX_ROE = 1, FLUX_SIGMA1 = 2, FLUX_SIGMA0 = 4;
-template <typename R, bool MIX, bool LES, int BX, int BY, int DIR, int FLUX = 0, bool NV0 = false>
-__device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a,
+// FLUX_W5: where the reference would reconstruct by WENO3 (fluxorder 3),
+// faces whose six-node stencil pos-2 .. pos+3 lies on the nodes 0 .. m-1 and
+// holds no wall node take WENO5-JS; the others keep the reference's path, and
+// the (j < 30 && k < 7) MUSCL override of the non-LES scheme is off.
+template <typename R, bool MIX, bool LES, class RG, int DIR, int FLUX = 0, bool NV0 = false>
+__device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, const RG &Rg, NRef a,
                                           int gi, int gj, int gk, int drt, R Fc[5]) {
   const int d = DIR >= 0 ? DIR : drt;
   const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d);
@@ -285,6 +415,7 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   }
 
   constexpr bool ROE = (FLUX & FLUX_ROE) != 0;
+  constexpr bool W5 = (FLUX & FLUX_W5) != 0;
   constexpr bool CEN_ONLY = LES && (FLUX & FLUX_SIGMA1) != 0;
   constexpr bool UPW_ONLY = LES && (FLUX & FLUX_SIGMA0) != 0;
   R Fw[5], Ufw = R(0);
@@ -317,7 +448,7 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   #pragma unroll
       for (int q = 0; q < 5; q++) { QL[q] = Q[1][q]; QR[q] = Q[2][q]; }
       pL = P[1]; pR = P[2];
-    } else if (fo == 2 || (!LES && d > 0 && gj < 30 && gk < 7)) {  // quirk rhs.c:2840, 2997
+    } else if (fo == 2 || (!LES && !W5 && d > 0 && gj < 30 && gk < 7)) {  // quirk rhs.c:2840, 2997
       const bool wm = nvm > BLANKWALL;  // qm = q[i+1] when i-1 is a wall
       const bool wp = nv2 > BLANKWALL;  // qp = q[i] when i+2 is a wall
   #pragma unroll
@@ -327,6 +458,8 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
       }
       pL = muscl_l(wm ? P[2] : P[0], P[1], P[2]);
       pR = muscl_r(P[1], P[2], wp ? P[1] : P[3]);
+    } else if (W5 && weno5_face<R, MIX, NV0>(c, F, Rg, a, d, pos, m, g0, sd, Q, P, QL, QR, pL, pR)) {
+      // WENO5-JS reconstruction of Q and p
     } else {
       const int ord = c.eno_order;
       const bool el = nvm > BLANKWALL && (d != 0 || (gi + 2) < c.mx);
@@ -440,8 +573,8 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
 // -------------------------------------------------------- viscous face ----
 __device__ __forceinline__ bool blocked(double v) { return v > SOLID && v < INNERBLANK; }
 
-template <typename R, bool MIX, bool LES, int BX, int BY, int DIR, bool NV0 = false>
-__device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a,
+template <typename R, bool MIX, bool LES, class RG, int DIR, bool NV0 = false>
+__device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, const RG &Rg, NRef a,
                                           int gi, int gj, int gk, int drt, R Fv[5], R A[3]) {
   const int d = DIR >= 0 ? DIR : drt;
   const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d), g1 = g0 + sd;
@@ -587,14 +720,14 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
 
 // Everything one face contributes: the FP64 form keeps conv, visc and the LES
 // stress apart (G[0..4], G[5..9], G[10..12]), the mixed form stores visc - conv.
-template <typename R, bool MIX, bool LES, bool VISC, int BX, int BY, int DIR, int FLUX = 0, bool NV0 = false>
-__device__ __forceinline__ void face_flux(const DevCfg &c, const DevFields &F, const Ring<R, BX, BY> &Rg, NRef a, int fi,
+template <typename R, bool MIX, bool LES, bool VISC, class RG, int DIR, int FLUX = 0, bool NV0 = false>
+__device__ __forceinline__ void face_flux(const DevCfg &c, const DevFields &F, const RG &Rg, NRef a, int fi,
                                           int fj, int k, int drt, R *G) {
   constexpr int VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
   R Fc[5], Fv[5], A[3];
-  conv_face<R, MIX, LES, BX, BY, DIR, FLUX, NV0>(c, F, Rg, a, fi, fj, k, drt, Fc);
+  conv_face<R, MIX, LES, RG, DIR, FLUX, NV0>(c, F, Rg, a, fi, fj, k, drt, Fc);
   if (VISC) {
-    visc_face<R, MIX, LES, BX, BY, DIR, NV0>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
+    visc_face<R, MIX, LES, RG, DIR, NV0>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
   } else {
 #pragma unroll
     for (int q = 0; q < 5; q++) Fv[q] = R(0.);
@@ -611,97 +744,99 @@ __device__ __forceinline__ void face_flux(const DevCfg &c, const DevFields &F, c
 }
 
 // ---------------------------------------------------------- the kernel ----
-// Tile of SBX x SBY interior nodes, SNT threads.  Per plane the block
-// computes (SBX+1)*SBY i-faces, SBX*(SBY+1) j-faces and SBX*SBY k-faces in
-// three warp-uniform rounds: virtual face v = round*SNT + tid maps to
-// [0,256) i-faces, [256,512) j-faces, [512,736) k-faces, so every warp runs
-// one face direction per round (no divergence between directions).
-constexpr int SBX = 32, SBY = 7, SNT = 256;
-using STile = TileShape<SBX, SBY>;
-constexpr int S_NXF = STile::NXF;  // 231
-constexpr int S_NYF = STile::NYF;  // 256
-constexpr int S_NZF = SBX * SBY;   // 224
-template <typename R, bool MIX, bool NV0 = false>
+// Tile of 32 x BY interior nodes, NT = 32 (BY + 1) threads (StageGeo).  Per
+// plane the block computes 33*BY i-faces, 32*(BY+1) j-faces and 32*BY k-faces
+// in three warp-uniform rounds: virtual face v = round*NT + tid maps to
+// [0,NT) i-faces, [NT,2NT) j-faces, [2NT,3NT) k-faces, so every warp runs one
+// face direction per round (no divergence between directions).
+constexpr int SBX = 32, SBY = StageGeo<0>::BY, SNT = StageGeo<0>::NT;  // the WENO3/MUSCL tile: 32 x 7, 256 threads
+constexpr int SBY_W5 = StageGeo<FLUX_W5>::BY, SNT_W5 = StageGeo<FLUX_W5>::NT;  // WENO5: 32 x 5, 192 threads
+template <typename R, bool MIX, bool NV0 = false, bool W5 = false>
 struct StageSmem {
+  using G = StageGeo<W5 ? FLUX_W5 : 0>;
   static constexpr int NG = FaceWidth<MIX>::NG;
+  static constexpr int PN = G::Tile::PN;
   // FP64 staging fields per plane: 5 state fields, nvert (not with NV0), and
   // in the FP64 form the pressure carried from an immersed step's
   // interpolation (the mixed form keeps that shared memory as L1: the carried
   // value differs from the EOS by <= 1e-12, inside its bar)
   static constexpr int NSTG = 5 + (NV0 ? 0 : 1) + (MIX ? 0 : 1);
-  // ring + face buffers, FP64 staging of the next plane, nvert byte ring [4][PN]
-  // (not with NV0: the no-IBM variants leave that memory to the L1)
-  static constexpr size_t bytes = sizeof(R) * ((size_t)4 * NF * STile::PN + (size_t)NG * (S_NXF + S_NYF + S_NZF)) +
-                                  sizeof(double) * (size_t)NSTG * STile::PN + (NV0 ? 0 : (size_t)4 * STile::PN);
+  // ring + face buffers, FP64 staging of the next plane, nvert byte ring
+  // [NPL][PN] (not with NV0: the no-IBM variants leave that memory to the L1)
+  static constexpr size_t bytes = sizeof(R) * ((size_t)G::NPL * NF * PN + (size_t)NG * (G::NXF + G::NYF + G::NZF)) +
+                                  sizeof(double) * (size_t)NSTG * PN + (NV0 ? 0 : (size_t)G::NPL * PN);
 };
 constexpr size_t STAGE_SMEM_BYTES = StageSmem<double, false>::bytes;
 constexpr size_t STAGE_SMEM_BYTES_MIXED = StageSmem<float, true>::bytes;
 // dynamic shared memory of a stage-kernel launch
-template <typename R, bool MIX, bool NV0>
-constexpr size_t stage_smem() { return StageSmem<R, MIX, NV0>::bytes; }
-static_assert(S_NXF <= 256 && S_NYF <= 256 && S_NZF <= 224, "face schedule segments");
+template <typename R, bool MIX, bool NV0, bool W5 = false>
+constexpr size_t stage_smem() { return StageSmem<R, MIX, NV0, W5>::bytes; }
 static_assert(STAGE_SMEM_BYTES <= 232448, "shared memory budget of one block");
+static_assert(StageSmem<double, false, false, true>::bytes <= 232448, "WENO5 FP64: shared memory of one block");
 static_assert(2 * (STAGE_SMEM_BYTES_MIXED + 1024) <= 233472, "mixed form: two blocks per SM");
+static_assert(2 * (StageSmem<float, true, false, true>::bytes + 1024) <= 233472, "WENO5 mixed: two blocks per SM");
 
 // All face fluxes of plane k of a tile into the face buffers (ZONLY: just the
 // k-faces, for the prologue).  A function rather than a lambda so that it is
 // always inlined: an outlined call would copy the kernel parameters to local
 // memory.
-template <typename R, bool MIX, bool LES, bool VISC, bool ZONLY, int FLUX = 0, bool NV0 = false>
-__device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F, const Ring<R, SBX, SBY> &Rg, int i0,
-                                            int j0, int k, R *gxb, R *gyb, R *gzb) {
-  constexpr int BX = SBX, BY = SBY, NT = SNT, NG = FaceWidth<MIX>::NG;
+template <typename R, bool MIX, bool LES, bool VISC, bool ZONLY, int FLUX, bool NV0, class RG>
+__device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F, const RG &Rg, int i0, int j0, int k,
+                                            R *gxb, R *gyb, R *gzb) {
+  using G = StageGeo<FLUX>;
+  constexpr int BX = G::BX, NT = G::NT, NG = FaceWidth<MIX>::NG;
   const int tid = threadIdx.x;
 #pragma unroll 1
   for (int r = ZONLY ? 2 : 0; r < 3; r++) {
-    const int v = r * NT + tid;
-    int d, u, fi, fj;
+    const int u = tid;  // face index within this round's direction
+    int d, fi, fj;
     NRef a;
     R *dst;
     int nslot;
-    if (v < 256) {
-      d = 0; u = v;
+    if (r == 0) {
+      d = 0;
+      if (u >= G::NXF) continue;
       const int fx = u % (BX + 1), fy = u / (BX + 1);
       fi = i0 - 1 + fx; fj = j0 + fy;
       a = NRef{0, fy + 2, fx + 1};
-      dst = gxb; nslot = S_NXF;
-      if (u >= S_NXF) continue;
-    } else if (v < 512) {
-      d = 1; u = v - 256;
-      if (u >= S_NYF) continue;  // (exactly full for the 32 x 7 tile)
+      dst = gxb; nslot = G::NXF;
+    } else if (r == 1) {
+      d = 1;
+      if (u >= G::NYF) continue;
       const int fx = u % BX, fy = u / BX;
       fi = i0 + fx; fj = j0 - 1 + fy;
       a = NRef{0, fy + 1, fx + 2};
-      dst = gyb; nslot = S_NYF;
+      dst = gyb; nslot = G::NYF;
     } else {
-      d = 2; u = v - 512;
-      if (u >= S_NZF) continue;
+      d = 2;
+      if (u >= G::NZF) continue;
       const int fx = u % BX, fy = u / BX;
       fi = i0 + fx; fj = j0 + fy;
       a = NRef{0, fy + 2, fx + 2};
-      dst = gzb; nslot = S_NZF;
+      dst = gzb; nslot = G::NZF;
     }
-    R G[NG];
+    R Gf[NG];
     // -twoD 1 forms no i-face flux (rhs.c:1487, 2646, 3465): it stays zero
     if (fi <= c.mx - 2 && fj <= c.my - 2 && !(d == 0 && c.twod == 1)) {
       if (MIX) {
         // one instantiation per direction (d is warp-uniform): 16 % faster
         // for the FP32 arithmetic of the mixed form
-        if (d == 0) face_flux<R, MIX, LES, VISC, BX, BY, 0, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, G);
-        else if (d == 1) face_flux<R, MIX, LES, VISC, BX, BY, 1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, G);
-        else face_flux<R, MIX, LES, VISC, BX, BY, 2, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, G);
+        if (d == 0) face_flux<R, MIX, LES, VISC, RG, 0, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, Gf);
+        else if (d == 1) face_flux<R, MIX, LES, VISC, RG, 1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, Gf);
+        else face_flux<R, MIX, LES, VISC, RG, 2, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, Gf);
       } else {
         // one copy for all directions: the FP64 form at 255 registers runs
         // 12 % slower with three
-        face_flux<R, MIX, LES, VISC, BX, BY, -1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, G);
+        face_flux<R, MIX, LES, VISC, RG, -1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, Gf);
       }
     } else {
 #pragma unroll
-      for (int q = 0; q < NG; q++) G[q] = R(0.);
+      for (int q = 0; q < NG; q++) Gf[q] = R(0.);
     }
 #pragma unroll
-    for (int q = 0; q < NG; q++) dst[(size_t)q * nslot + u] = G[q];
+    for (int q = 0; q < NG; q++) dst[(size_t)q * nslot + u] = Gf[q];
   }
+  (void)NT;
 }
 
 
@@ -710,17 +845,20 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
 template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0, bool NV0 = false>
 __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, int bxi, int byi, int kb, int ke,
                                            int istage, double alfa, double beta, double adt, double *smem_d) {
-  constexpr int BX = SBX, BY = SBY, NT = SNT, PX = STile::PX, PN = STile::PN;
+  using G = StageGeo<FLUX>;
+  constexpr int BX = G::BX, BY = G::BY, NT = G::NT, NPL = G::NPL, H = G::H;
+  constexpr int PX = G::Tile::PX, PN = G::Tile::PN, NXF = G::NXF, NYF = G::NYF, NZF = G::NZF;
   constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
-  constexpr int NSTG = StageSmem<R, MIX, NV0>::NSTG;
+  constexpr int NSTG = StageSmem<R, MIX, NV0, G::W5>::NSTG;
+  using RG = Ring<R, BX, BY, NPL>;
   double *stg = smem_d;  // [NSTG][PN] raw FP64 Q, nvert and carried pressure of the next plane
   R *smem = reinterpret_cast<R *>(smem_d + (size_t)NSTG * PN);
-  Ring<R, BX, BY> Rg;
+  RG Rg;
   Rg.pl = smem;
-  R *gxb = smem + (size_t)4 * NF * PN;  // [NG][S_NXF]
-  R *gyb = gxb + (size_t)NG * S_NXF;    // [NG][S_NYF]
-  R *gzb = gyb + (size_t)NG * S_NYF;    // [NG][S_NZF]
-  unsigned char *nvc = reinterpret_cast<unsigned char *>(gzb + (size_t)NG * S_NZF);  // [4][PN]
+  R *gxb = smem + (size_t)NPL * NF * PN;  // [NG][NXF]
+  R *gyb = gxb + (size_t)NG * NXF;        // [NG][NYF]
+  R *gzb = gyb + (size_t)NG * NYF;        // [NG][NZF]
+  unsigned char *nvc = reinterpret_cast<unsigned char *>(gzb + (size_t)NG * NZF);  // [NPL][PN]
   Rg.nvc = nvc;
   // staged fields per plane: Q, then nvert (byte-exact codes), then lP (carried pressure)
   const bool pst = !MIX && F.pin != nullptr;
@@ -729,7 +867,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 
   const int tid = threadIdx.x;
   const int i0 = 1 + bxi * BX, j0 = 1 + byi * BY;
-  // node updated by this thread (threads 224..255 only load and compute faces)
+  // node updated by this thread (the last warp only loads and computes faces)
   const int utx = tid % BX, uty = tid / BX;
   const int ugi = i0 + utx, ugj = j0 + uty;
   const bool uact = uty < BY && ugi <= c.mx - 2 && ugj <= c.my - 2;
@@ -802,25 +940,24 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
     __syncthreads();
   };
 
-  // prologue: planes kb-2 .. kb+1 in slots 0..3, k-face kb-1/2, then kb+2
+  // prologue: planes kb-1-H .. kb+H in slots 0 .. NPL-1, k-face kb-1/2 (its
+  // stencil is exactly those planes), then plane kb+H+1 into slot 0
   Rg.sb = 0;
-  load_plane_sync(kb - 2, 0);
-  load_plane_sync(kb - 1, 1);
-  load_plane_sync(kb, 2);
-  load_plane_sync(kb + 1, 3);
+#pragma unroll 1
+  for (int t = 0; t < NPL; t++) load_plane_sync(kb - 1 - H + t, t);
   plane_faces<R, MIX, LES, VISC, true, FLUX, NV0>(c, F, Rg, i0, j0, kb - 1, gxb, gyb, gzb);  // k-face kb-1/2
   __syncthreads();
   R Gzp[NG];  // k-face k-1/2 of the node this thread updates
 #pragma unroll
-  for (int q = 0; q < NG; q++) Gzp[q] = uact ? gzb[(size_t)q * S_NZF + tid] : R(0.);
+  for (int q = 0; q < NG; q++) Gzp[q] = uact ? gzb[(size_t)q * NZF + tid] : R(0.);
   __syncthreads();
-  load_plane_sync(kb + 2, 0);
-  int base = 1;  // slot of plane k-1
+  load_plane_sync(kb + H + 1, 0);
+  int base = 1;  // slot of plane k-H
 
   for (int k = kb; k < ke; k++) {
     Rg.sb = base;
     const bool more = k + 1 < ke;
-    if (more) issue_stage(k + 3);  // overlaps the face computation
+    if (more) issue_stage(k + H + 2);  // overlaps the face computation
     plane_faces<R, MIX, LES, VISC, false, FLUX, NV0>(c, F, Rg, i0, j0, k, gxb, gyb, gzb);
     // the only plane k-1 value the update needs, read before that slot is refilled
     const NRef n{0, uty + 2, utx + 2};
@@ -858,8 +995,8 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       // flux differences in the reference's order (rhs.c:3159-3205, 2123-2151):
       // ((((F_i - F_i-1) + F_j) - F_j-1) + F_k) - F_k-1
       auto fdiff = [&](int q) {
-        return gxb[(size_t)q * S_NXF + fxr] - gxb[(size_t)q * S_NXF + fxl] + gyb[(size_t)q * S_NYF + fyu] -
-               gyb[(size_t)q * S_NYF + fyd] + gzb[(size_t)q * S_NZF + fz] - Gzp[q];
+        return gxb[(size_t)q * NXF + fxr] - gxb[(size_t)q * NXF + fxl] + gyb[(size_t)q * NYF + fyu] -
+               gyb[(size_t)q * NYF + fyd] + gzb[(size_t)q * NZF + fz] - Gzp[q];
       };
       // LES energy term (rhs.c:2153-2197): u . sum of rho_face * stress differences
       auto les_energy = [&]() -> R {
@@ -871,9 +1008,9 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 #pragma unroll
         for (int q = 0; q < 3; q++) {
           const int a = AOFF + q;
-          const R t = rR * gxb[(size_t)a * S_NXF + fxr] - rL * gxb[(size_t)a * S_NXF + fxl] +
-                      rU * gyb[(size_t)a * S_NYF + fyu] - rD * gyb[(size_t)a * S_NYF + fyd] +
-                      rF * gzb[(size_t)a * S_NZF + fz] - rB * Gzp[a];
+          const R t = rR * gxb[(size_t)a * NXF + fxr] - rL * gxb[(size_t)a * NXF + fxl] +
+                      rU * gyb[(size_t)a * NYF + fyu] - rD * gyb[(size_t)a * NYF + fyd] +
+                      rF * gzb[(size_t)a * NZF + fz] - rB * Gzp[a];
           e = (q == 0) ? Rg.get(F_U + q, n) * t : e + Rg.get(F_U + q, n) * t;
         }
         return e;
@@ -936,10 +1073,10 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
         if (st) atomicOr(F.status, st);
       }
 #pragma unroll
-      for (int q = 0; q < NG; q++) Gzp[q] = gzb[(size_t)q * S_NZF + fz];
+      for (int q = 0; q < NG; q++) Gzp[q] = gzb[(size_t)q * NZF + fz];
     }
-    if (more) derive(base & 3);  // plane k+3 into the slot of plane k-1
-    base++;
+    if (more) derive(base);  // plane k+H+2 into the slot of plane k-H
+    base = base + 1 == NPL ? 0 : base + 1;
     __syncthreads();
   }
 }
@@ -951,9 +1088,10 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 // its range with its own prologue.  Every node gets the same arithmetic in
 // both shapes (a chunk start recomputes its first k-face from the same data).
 template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0, bool NV0 = false>
-__global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
+__global__ void __launch_bounds__(StageGeo<FLUX>::NT, MIX ? 2 : 1)
     stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
   extern __shared__ double smem_d[];
+  constexpr int BY = StageGeo<FLUX>::BY;
   const int nk = c.mz - 2, tiles_x = (c.mx - 2 + SBX - 1) / SBX;
   long long s, e;  // range of (column, plane) units, column-major
   if (kchunk > 0) {
@@ -962,7 +1100,7 @@ __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     s = col * nk + k0;
     e = col * nk + min(nk, k0 + kchunk);
   } else {
-    const long long total = (long long)tiles_x * ((c.my - 2 + SBY - 1) / SBY) * nk;
+    const long long total = (long long)tiles_x * ((c.my - 2 + BY - 1) / BY) * nk;
     const long long per = (total + gridDim.x - 1) / gridDim.x;
     s = min(total, (long long)blockIdx.x * per);
     e = min(total, s + per);
@@ -976,30 +1114,59 @@ __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
   }
 }
 
-// The time-step kernel without nvert (NV0) for FLUX bits fl: Roe, and with
-// LES the constant-sigma variants; fl outside them runs the general blend.
+// The time-step kernel without nvert (NV0) for FLUX bits fl: Roe, with LES
+// the constant-sigma variants, and WENO5-JS; fl outside them runs the
+// general blend.
 using StageKern = void (*)(const DevCfg, const DevFields, int, double, double, double, int);
-template <typename R, bool MIX, bool LES, bool VISC>
-StageKern stage_nv0_kernel(int fl) {
+template <typename R, bool MIX, bool LES, bool VISC, int W>
+StageKern stage_nv0_kernel_w(int fl) {
   if constexpr (LES) {
-    switch (fl) {
-      case 1: return stage_kernel<R, MIX, LES, VISC, false, 1, true>;
-      case 2: return stage_kernel<R, MIX, LES, VISC, false, 2, true>;
-      case 3: return stage_kernel<R, MIX, LES, VISC, false, 3, true>;
-      case 4: return stage_kernel<R, MIX, LES, VISC, false, 4, true>;
-      case 5: return stage_kernel<R, MIX, LES, VISC, false, 5, true>;
-      default: return stage_kernel<R, MIX, LES, VISC, false, 0, true>;
+    switch (fl & 7) {
+      case 1: return stage_kernel<R, MIX, LES, VISC, false, W | 1, true>;
+      case 2: return stage_kernel<R, MIX, LES, VISC, false, W | 2, true>;
+      case 3: return stage_kernel<R, MIX, LES, VISC, false, W | 3, true>;
+      case 4: return stage_kernel<R, MIX, LES, VISC, false, W | 4, true>;
+      case 5: return stage_kernel<R, MIX, LES, VISC, false, W | 5, true>;
+      default: return stage_kernel<R, MIX, LES, VISC, false, W, true>;
     }
   } else {
-    return (fl & FLUX_ROE) ? stage_kernel<R, MIX, LES, VISC, false, 1, true> : stage_kernel<R, MIX, LES, VISC, false, 0, true>;
+    return (fl & FLUX_ROE) ? stage_kernel<R, MIX, LES, VISC, false, W | 1, true> : stage_kernel<R, MIX, LES, VISC, false, W, true>;
   }
 }
 template <typename R, bool MIX, bool LES, bool VISC>
-cudaError_t stage_nv0_attrs() {
-  const int smem = (int)stage_smem<R, MIX, true>();
+StageKern stage_nv0_kernel(int fl) {
+  return (fl & FLUX_W5) ? stage_nv0_kernel_w<R, MIX, LES, VISC, FLUX_W5>(fl) : stage_nv0_kernel_w<R, MIX, LES, VISC, 0>(fl);
+}
+// The general (nvert-reading) kernel for the Roe and WENO5 bits of fl.
+template <typename R, bool MIX, bool LES, bool VISC, bool RHSM>
+StageKern stage_gen_kernel(int fl) {
+  switch (fl & (FLUX_ROE | FLUX_W5)) {
+    case FLUX_ROE: return stage_kernel<R, MIX, LES, VISC, RHSM, FLUX_ROE>;
+    case FLUX_W5: return stage_kernel<R, MIX, LES, VISC, RHSM, FLUX_W5>;
+    case FLUX_ROE | FLUX_W5: return stage_kernel<R, MIX, LES, VISC, RHSM, FLUX_ROE | FLUX_W5>;
+    default: return stage_kernel<R, MIX, LES, VISC, RHSM, 0>;
+  }
+}
+// Threads and dynamic shared memory of a stage-kernel launch for FLUX bits fl.
+inline int stage_threads(int fl) { return (fl & FLUX_W5) ? SNT_W5 : SNT; }
+template <typename R, bool MIX>
+size_t stage_smem_for(int fl, bool nv0) {
+  const bool w5 = (fl & FLUX_W5) != 0;
+  if (nv0) return w5 ? stage_smem<R, MIX, true, true>() : stage_smem<R, MIX, true, false>();
+  return w5 ? stage_smem<R, MIX, false, true>() : stage_smem<R, MIX, false, false>();
+}
+// Opt every variant of one (LES, VISC, RHSM) into its dynamic shared memory.
+template <typename R, bool MIX, bool LES, bool VISC, bool RHSM>
+cudaError_t stage_attrs() {
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaSuccess;
-  for (int fl = 0; fl < (LES ? 6 : 2) && e == cudaSuccess; fl++)
-    e = cudaFuncSetAttribute(stage_nv0_kernel<R, MIX, LES, VISC>(fl), cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  for (int fl : {0, FLUX_ROE, FLUX_W5, FLUX_ROE | FLUX_W5})
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_gen_kernel<R, MIX, LES, VISC, RHSM>(fl), attr, (int)stage_smem_for<R, MIX>(fl, false));
+  if constexpr (!RHSM) {  // the no-IBM variants of the time step
+    for (int w : {0, FLUX_W5})
+      for (int fl = 0; fl < (LES ? 6 : 2) && e == cudaSuccess; fl++)
+        e = cudaFuncSetAttribute(stage_nv0_kernel<R, MIX, LES, VISC>(w | fl), attr, (int)stage_smem_for<R, MIX>(w | fl, true));
+  }
   return e;
 }
 

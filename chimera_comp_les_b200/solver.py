@@ -67,7 +67,7 @@ class Block:
                  s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5,
                  flux: str = "rusanov", max_cs: float = 0.05, twall: float = 1.0, twod: int = 0,
                  i_homo_filter: int = 0, j_homo_filter: int = 0, k_homo_filter: int = 0, testfilter_ik: int = 0,
-                 visT: int = 0, tref: float = 273.15, abc: int = 0):
+                 visT: int = 0, tref: float = 273.15, abc: int = 0, weno_order: int = 3):
         self.lib = _lib.load()
         cfg = CbConfig()
         self.lib.cb_config_default(C.byref(cfg), mx, my, mz)
@@ -78,7 +78,8 @@ class Block:
                          s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh,
                          max_cs=max_cs, twall=twall, twod=twod, i_homo_filter=i_homo_filter,
                          j_homo_filter=j_homo_filter, k_homo_filter=k_homo_filter,
-                         testfilter_ik=testfilter_ik, visT=visT, tref=tref, abc=abc).items():
+                         testfilter_ik=testfilter_ik, visT=visT, tref=tref, abc=abc,
+                         weno_order=weno_order).items():
             setattr(cfg, k, v)
         cfg.flux = {"rusanov": 0, "roe": 1}[flux] if isinstance(flux, str) else int(flux)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]

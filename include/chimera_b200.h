@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CB_ABI_VERSION 1
+#define CB_ABI_VERSION 2
 
 /* status codes */
 #define CB_OK 0
@@ -98,6 +98,11 @@ typedef struct {
   double tref;          /* -Tref: its reference temperature (default 273.15, rhs.c:1410) */
   int abc;              /* -ABC: with -calc_sigma, the raw sensor weights are 0 above plane
                            k = ABC (an absorbing layer; rhs.c:3311, 3341-3368); 0 off */
+  int weno_order;       /* 3 (default): the reference's WENO3 with fluxorder 3; 5: WENO5-JS (Jiang & Shu,
+                           J. Comput. Phys. 126 (1996)) on every face whose six-node stencil lies on the
+                           nodes 0 .. m-1 and holds no wall node, the reference's path elsewhere, and no
+                           (j < 30 && k < 7) MUSCL override; needs fluxorder 3.  No counterpart in the
+                           reference.  Single-block contexts. */
 } cb_config;
 
 /* Fills *cfg with the reference's defaults (init.c:45-103, main.c:14-75). */

@@ -82,6 +82,7 @@ class Config:
     visT: int = 0           # -visT: Sutherland's law for the viscosity (rhs.c:1412-1414)
     tref: float = 273.15    # -Tref: its reference temperature (rhs.c:1410)
     abc: int = 0            # -ABC: absorbing layer of the shock sensor above plane k (rhs.c:3311)
+    weno_order: int = 3     # 5: WENO5-JS (Jiang & Shu 1996) where its stencil fits; no reference counterpart
 
     def ref_options(self) -> str:
         o = [
@@ -126,6 +127,7 @@ class _CCfg(C.Structure):
         ("flux", C.c_int), ("max_cs", C.c_double), ("twall", C.c_double), ("twod", C.c_int),
         ("i_homo_filter", C.c_int), ("j_homo_filter", C.c_int), ("k_homo_filter", C.c_int),
         ("testfilter_ik", C.c_int), ("visT", C.c_int), ("tref", C.c_double), ("abc", C.c_int),
+        ("weno_order", C.c_int),
     ]
 
 
@@ -212,6 +214,8 @@ class Oracle:
         D = C.POINTER(C.c_double)
         L = self.lib
         L.cbo_fill_ghosts.argtypes = [C.c_void_p, D]
+        L.cbo_weno5.argtypes = [C.c_double] * 5
+        L.cbo_weno5.restype = C.c_double
         L.cbo_metrics.argtypes = [C.c_void_p, PP, PP, PP, PP, D]
         L.cbo_eos.argtypes = [C.c_void_p, PP, D]
         L.cbo_sigma.argtypes = [C.c_void_p, PP]
@@ -244,6 +248,10 @@ class Oracle:
         buf = (C.c_longlong * len(self.COUNT_KINDS))()
         self.lib.cbo_count_read(buf)
         return dict(zip(self.COUNT_KINDS, (int(v) for v in buf)))
+
+    def weno5(self, a: float, b: float, c: float, d: float, e: float) -> float:
+        """WENO5-JS value at x_{i+1/2} from v_{i-2..i+2} (left-biased)."""
+        return float(self.lib.cbo_weno5(a, b, c, d, e))
 
     def zeros(self, nc: int) -> np.ndarray:
         return np.zeros((nc,) + self.cfg.padded_shape)
@@ -460,6 +468,8 @@ class RefOracle:
     def __init__(self, cfg: Config, coords_nat: np.ndarray, optimized: bool = False):
         if cfg.flux != 0:
             raise ValueError("the reference has no Roe flux (flux 1); check it against the restatement")
+        if cfg.weno_order != 3:
+            raise ValueError("the reference has no WENO5 (weno_order 5); check it against the restatement")
         self.cfg = cfg
         self.lib = C.CDLL(build_ref(optimized=optimized))
         L = self.lib

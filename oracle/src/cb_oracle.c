@@ -334,6 +334,32 @@ static inline double weno3_r(double qm, double q0, double qp) {
   double as = a0 + a1;
   return (a0 / as) * r0 + (a1 / as) * r1;
 }
+/* WENO5-JS (G.-S. Jiang and C.-W. Shu, "Efficient implementation of weighted
+ * ENO schemes", J. Comput. Phys. 126 (1996) 202-228, eqs. 2.10-2.17 with
+ * p = 2): no counterpart in the reference, whose WENO is the 3rd-order one
+ * above.  Value at x_{i+1/2} from a..e = v_{i-2..i+2}:
+ *   candidates (times 6)  q0 = 2a - 7b + 11c,  q1 = -b + 5c + 2d,  q2 = 2c + 5d - e
+ *   smoothness            beta_k = 13/12 (second difference)^2 + 1/4 (first-derivative estimate)^2
+ *   weights               alpha_k = d_k / (eps + beta_k)^2,  d = (1/10, 6/10, 3/10),  eps = 1e-6
+ *   value                 (alpha0 q0 + alpha1 q1 + alpha2 q2) / (6 (alpha0 + alpha1 + alpha2))
+ * The operation order here is the one the device code follows. */
+double cbo_weno5(double a, double b, double c, double d, double e) {
+  const double eps = 1e-6, c13 = 13.0 / 12.0;
+  const double q0 = (2.0 * a - 7.0 * b) + 11.0 * c;
+  const double q1 = (5.0 * c - b) + 2.0 * d;
+  const double q2 = (2.0 * c + 5.0 * d) - e;
+  const double t0 = (a - 2.0 * b) + c, u0 = (a - 4.0 * b) + 3.0 * c;
+  const double t1 = (b - 2.0 * c) + d, u1 = b - d;
+  const double t2 = (c - 2.0 * d) + e, u2 = (3.0 * c - 4.0 * d) + e;
+  const double b0 = c13 * (t0 * t0) + 0.25 * (u0 * u0);
+  const double b1 = c13 * (t1 * t1) + 0.25 * (u1 * u1);
+  const double b2 = c13 * (t2 * t2) + 0.25 * (u2 * u2);
+  const double a0 = 0.1 / ((eps + b0) * (eps + b0));
+  const double a1 = 0.6 / ((eps + b1) * (eps + b1));
+  const double a2 = 0.3 / ((eps + b2) * (eps + b2));
+  return ((a0 * q0 + a1 * q1) + a2 * q2) / (6.0 * ((a0 + a1) + a2));
+}
+
 static inline double eno_r(double qm, double q0, double qp, int k) {
   if (k == 2) return 0.5 * q0 + 0.5 * qp;
   return -qm * 0.1666666666666666 + q0 * 0.8333333333333333 + qp * 0.3333333333333333;
@@ -462,6 +488,32 @@ static void recon_weno(const ctx_t *C, int d, int pos, ptrdiff_t n0, int eno_l_c
   }
 }
 
+/* WENO5-JS on the face pos+1/2 (between n0 and n0+e_d) where its six-node
+ * stencil pos-2 .. pos+3 lies on the DMDA's nodes 0 .. m-1 (so no stencil
+ * reaches the wrap-around ghosts of a periodic direction) and holds no wall
+ * node (nvert > 2.9); returns 0 when that does not hold, and the caller then
+ * takes the reference's WENO3 path. */
+static int recon_weno5(const ctx_t *C, int d, int pos, ptrdiff_t n0, double QL[5], double QR[5], double *pL,
+                       double *pR) {
+  const ptrdiff_t s = C->G.s[d];
+  const int m = C->G.m[d];
+  const double *nv = C->nv;
+  if (pos < 2 || pos > m - 4) return 0;
+  if (nv[n0 - 2 * s] > BLANKWALL || nv[n0 - s] > BLANKWALL || nv[n0 + 2 * s] > BLANKWALL ||
+      nv[n0 + 3 * s] > BLANKWALL)
+    return 0;
+  const double *const *q = C->q;
+  const double *p = C->p;
+  for (int a = 0; a < 5; a++) {
+    const double *v = q[a];
+    QL[a] = cbo_weno5(v[n0 - 2 * s], v[n0 - s], v[n0], v[n0 + s], v[n0 + 2 * s]);
+    QR[a] = cbo_weno5(v[n0 + 3 * s], v[n0 + 2 * s], v[n0 + s], v[n0], v[n0 - s]);
+  }
+  *pL = cbo_weno5(p[n0 - 2 * s], p[n0 - s], p[n0], p[n0 + s], p[n0 + 2 * s]);
+  *pR = cbo_weno5(p[n0 + 3 * s], p[n0 + 2 * s], p[n0 + s], p[n0], p[n0 - s]);
+  return 1;
+}
+
 static void recon_muscl(const ctx_t *C, int d, ptrdiff_t n0, double QL[5], double QR[5], double *pL, double *pR) {
   const ptrdiff_t s = C->G.s[d];
   const double *const *q = C->q;
@@ -498,9 +550,9 @@ static void conv_face_std(const ctx_t *C, int d, int i, int j, int k, double F[5
     ld5(C, n1, QL); ld5(C, n1, QR); pL = pR = C->p[n1];
   } else if (fo == 1 || pos == 0 || pos == m - 2 || (nv[n0] + nv[n1]) > BLANKWALL) {
     ld5(C, n0, QL); ld5(C, n1, QR); pL = C->p[n0]; pR = C->p[n1];
-  } else if (fo == 2 || (d > 0 && j < 30 && k < 7)) { /* quirk: rhs.c:2840, 2997 */
+  } else if (fo == 2 || (c->weno_order != 5 && d > 0 && j < 30 && k < 7)) { /* quirk: rhs.c:2840, 2997 */
     recon_muscl(C, d, n0, QL, QR, &pL, &pR);
-  } else {
+  } else if (!(c->weno_order == 5 && recon_weno5(C, d, pos, n0, QL, QR, &pL, &pR))) {
     /* ENO fallbacks: xi also requires i+2 < mx (rhs.c:2706); eta/zeta do not */
     int el = nv[n0 - s] > BLANKWALL && (d != 0 || (i + 2) < C->G.m[0]);
     int er = nv[n0 + 2 * s] > BLANKWALL;
@@ -591,7 +643,7 @@ static void conv_face_les(const ctx_t *C, int d, int i, int j, int k, const doub
     ld5(C, n0, QL); ld5(C, n1, QR); pL = p[n0]; pR = p[n1];
   } else if (fo == 2) {
     recon_muscl(C, d, n0, QL, QR, &pL, &pR);
-  } else {
+  } else if (!(c->weno_order == 5 && recon_weno5(C, d, pos, n0, QL, QR, &pL, &pR))) {
     int el = nv[n0 - s] > BLANKWALL && (d != 0 || (i + 2) < C->G.m[0]);
     int er = nv[n0 + 2 * s] > BLANKWALL;
     recon_weno(C, d, pos, n0, el, er, 0, QL, QR, &pL, &pR);

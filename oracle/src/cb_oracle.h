@@ -49,7 +49,14 @@ typedef struct {
   int visT;                /* -visT: Sutherland's law for the molecular viscosity (rhs.c:1412-1414) */
   double tref;             /* -Tref: its reference temperature (default 273.15, rhs.c:1410) */
   int abc;                 /* -ABC: sensor weights 0 (then clamped) above plane k = ABC (rhs.c:3311, 3341-3368) */
+  int weno_order;          /* 3: the reference's WENO3 (fluxorder 3); 5: WENO5-JS (Jiang & Shu 1996) where its
+                              six-node stencil fits (no reference counterpart) */
 } cbo_config;
+
+/* WENO5-JS reconstruction at the face x_{i+1/2} from v_{i-2..i+2}, biased to
+ * the left (the right-biased value at x_{i+1/2} is cbo_weno5(v_{i+3}, ...,
+ * v_{i-1})).  Exposed for the known-answer tests of the reconstruction. */
+double cbo_weno5(double a, double b, double c, double d, double e);
 
 /* Fill the two ghost layers of each periodic direction of one padded plane
  * from the owned nodes by wrap-around (DMGlobalToLocal semantics). */

@@ -62,7 +62,7 @@ def gpu_block(cfg, precision="fp64"):
                  s_y_min=cfg.s_y_min, s_z_min=cfg.s_z_min, sigma_thrsh=cfg.sigma_thrsh, flux=cfg.flux,
                  max_cs=cfg.max_cs, twall=cfg.twall, twod=cfg.twoD, i_homo_filter=cfg.i_homo_filter,
                  j_homo_filter=cfg.j_homo_filter, k_homo_filter=cfg.k_homo_filter, testfilter_ik=cfg.testfilter_ik,
-                 visT=cfg.visT, tref=cfg.tref, abc=cfg.abc)
+                 visT=cfg.visT, tref=cfg.tref, abc=cfg.abc, weno_order=cfg.weno_order)
 
 
 def per_field_rel_l2(a, b):

@@ -21,6 +21,7 @@ int main(void) {
   F(cb_config, sigma_thrsh); F(cb_config, flux); F(cb_config, max_cs); F(cb_config, twall); F(cb_config, twod);
   F(cb_config, i_homo_filter); F(cb_config, j_homo_filter); F(cb_config, k_homo_filter);
   F(cb_config, testfilter_ik); F(cb_config, visT); F(cb_config, tref); F(cb_config, abc);
+  F(cb_config, weno_order);
   first = 1;
   printf("}}, \"cb_ibm_info\": {\"size\": %zu, \"fields\": {", sizeof(cb_ibm_info));
   F(cb_ibm_info, ni); F(cb_ibm_info, nj); F(cb_ibm_info, nk); F(cb_ibm_info, cell);

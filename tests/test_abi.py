@@ -32,7 +32,7 @@ def test_library_loads_and_exports_all_declared_symbols():
     lib = ctypes.CDLL(_lib_path())
     missing = [n for n in declared_functions() if not hasattr(lib, n)]
     assert not missing, missing
-    assert lib.cb_abi_version() == 1
+    assert lib.cb_abi_version() == 2
 
 
 def test_config_default_matches_reference_defaults():
@@ -45,6 +45,7 @@ def test_config_default_matches_reference_defaults():
     assert c.ren == 3000.0 and c.ma == 2.81 and c.gamma == 1.4 and c.pr == 0.72 and c.dt == 0.01
     assert c.central == 2 and c.fluxorder == 3 and c.eno_order == 2
     assert list(c.bctype) == [7] * 6
+    assert c.weno_order == 3
 
 
 def test_product_has_no_cpu_fallback():

@@ -1,0 +1,130 @@
+"""WENO5-JS on the GPU (weno_order 5; no counterpart in the reference): both
+forms against the oracle's restatement (Jiang & Shu 1996), and the isentropic
+vortex (BASELINE config 1's scheme: inviscid, WENO5-JS + Rusanov, SSP-RK3,
+CFL 0.5) against its analytic translation.
+
+The cases cover every stage-kernel variant the option reaches: the general
+kernel (cb_rhs, immersed masks), the no-IBM time-step variants with a blend
+weight of 0, 1 or neither, Rusanov and Roe, walls with inflow/outflow codes,
+and grids of several 32 x 5 tiles so that stencil nodes beyond the tile's
+two-node halo come from global memory.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from _common import RTOL_L2, gpu_block, oracle_run, per_field_rel_l2
+import oracle as O
+from chimera_comp_les_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("les_blend", (37, 21, 26), dict(les=1, inviscid=0, s_x=0.5, s_y=0.5, s_z=0.5, ren=500., ma=0.3, pr=0.71),
+     False),
+    ("les_sigma0_roe", (40, 19, 24), dict(les=1, inviscid=0, s_x=0.0, s_y=0.0, s_z=0.0, flux=1, ren=500., ma=0.3,
+                                          pr=0.71), False),
+    ("les_sigma1", (33, 12, 14), dict(les=1, inviscid=0, ren=500., ma=0.3, pr=0.71), False),
+    ("les_mask", (36, 23, 22), dict(les=1, inviscid=0, s_x=0.5, s_y=0.5, s_z=0.5, ren=500., ma=0.3, pr=0.71), True),
+    ("std_inv", (34, 16, 20), dict(les=0, inviscid=1), False),
+    ("std_visc_walls_roe", (35, 17, 23), dict(les=0, inviscid=0, bctype=(3, 3, 1, 1, 45, 44), flux=1, ren=250.,
+                                              ma=0.3, pr=0.71), False),
+    ("std_mask", (38, 18, 21), dict(les=0, inviscid=0, ren=250., ma=0.3, pr=0.71), True),
+]
+
+
+def _mask(shape):
+    nv = np.zeros(shape)
+    nv[8:12, 7:11, 12:17] = 3.0
+    band = nv[7:13, 6:12, 11:18]
+    band[band == 0] = 1.0
+    return nv
+
+
+@pytest.mark.parametrize("name,n,kw,mask", CASES, ids=[c[0] for c in CASES])
+def test_weno5_gpu_matches_restatement(name, n, kw, mask):
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, fluxorder=3, weno_order=5, dt=0.002, **kw)
+    periodic = all(b == 7 for b in cfg.bctype)
+    q = W.random_smooth_state(shape, seed=13, periodic=periodic)
+    nv = _mask(shape) if mask else np.zeros(shape)
+    ref = oracle_run(cfg, coords, q, nv, steps=2)
+    # the restatement's WENO5 differs from its WENO3 on this case
+    ref3 = oracle_run(O.Config(**{**cfg.__dict__, "weno_order": 3}), coords, q, nv)
+    assert max(per_field_rel_l2(ref3["rhs"], ref["rhs"])) > 1e-9
+    with gpu_block(cfg) as b:
+        b.FormMetrics(coords)
+        b.set_nvert(nv)
+        b.SetInitialCondition(q)
+        if cfg.les:
+            b.CalcUCat()
+            b.Compute_eddy_viscosity_LES()
+        assert max(per_field_rel_l2(b.formRHS(0), ref["rhs"])) <= RTOL_L2
+    for prec, tol in (("fp64", RTOL_L2), ("mixed", 1e-5)):
+        with gpu_block(cfg, precision=prec) as b:
+            b.FormMetrics(coords)
+            b.set_nvert(nv)
+            b.SetInitialCondition(q)
+            b.RungeKutta(2)
+            assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= tol, prec
+
+
+def test_weno5_balanced_segments_equal_k_chunks():
+    """The k-march's six-plane ring gives the same FP64 result for every
+    launch shape (chunk starts rebuild their prologue planes)."""
+    n = (35, 16, 29)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    q = W.random_smooth_state(coords.shape[:3], seed=17)
+    out = []
+    for kc in (29, 5, 0):
+        with gpu_block(O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=1, inviscid=0, fluxorder=3, weno_order=5,
+                                s_x=0.5, s_y=0.5, s_z=0.5, ren=500., ma=0.3, pr=0.71, dt=0.002)) as b:
+            b.FormMetrics(coords)
+            b.set_nvert(np.zeros(coords.shape[:3]))
+            b.SetInitialCondition(q)
+            best, _ = b.autotune([kc])
+            assert best == kc
+            b.RungeKutta(2)
+            out.append(b.Q())
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+
+
+def _vortex_error(n, t_end, weno_order):
+    from chimera_comp_les_b200 import Block
+    L = 10.0
+    coords = W.periodic_grid(n, L, amp=0.0)
+    q0 = W.vortex_state(coords)
+    dx = L / n
+    r = q0[..., 0]
+    u = np.abs(q0[..., 1] / r) + np.abs(q0[..., 2] / r)
+    c = np.sqrt(1.4 * 0.4 * (q0[..., 4] - 0.5 * (q0[..., 1] ** 2 + q0[..., 2] ** 2 + q0[..., 3] ** 2) / r) / r)
+    dt0 = 0.5 * dx / float((u + c).max())  # CFL 0.5
+    steps = int(math.ceil(t_end / dt0))
+    with Block(n + 2, n + 2, n + 2, les=0, inviscid=1, fluxorder=3, weno_order=weno_order, dt=t_end / steps) as b:
+        b.FormMetrics(coords)
+        b.SetInitialCondition(q0)
+        b.RungeKutta(steps)
+        q = b.Q()
+    shifted = coords.copy()
+    shifted[..., 0] = np.mod(coords[..., 0] - t_end, L)
+    shifted[..., 1] = np.mod(coords[..., 1] - t_end, L)
+    qe = W.vortex_state(shifted)
+    inner = (slice(1, -1),) * 3
+    d = q[inner + (0,)] - qe[inner + (0,)]
+    return float(np.linalg.norm(d) / np.linalg.norm(qe[inner + (0,)] - 1.0))
+
+
+def test_isentropic_vortex_weno5_converges_and_beats_weno3():
+    """Config 1's scheme (WENO5-JS + Rusanov, SSP-RK3, CFL 0.5) on [0, 10]^3:
+    the density after t = 2 against the vortex translated by t (1, 1, 0).
+    The reconstruction acts on point values of a nonlinear system, so the
+    scheme is second order overall (fifth order on the linear entropy wave,
+    tests/test_weno5.py); its error must fall at least at that rate under
+    refinement and stay well below the WENO3 path's."""
+    e32 = _vortex_error(32, 2.0, 5)
+    e64 = _vortex_error(64, 2.0, 5)
+    e64_w3 = _vortex_error(64, 2.0, 3)
+    assert e64 < 0.3 * e32, (e32, e64)
+    assert e64 < 0.35 * e64_w3, (e64, e64_w3)
