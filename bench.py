@@ -8,8 +8,10 @@ viscosity, in the reference's flags for MUSCL-minmod upwind with a
 Smagorinsky model: -les 1 -fluxorder 2 -s_x 0 -s_y 0 -s_z 0 (MUSCL-minmod
 reconstruction, Rusanov flux, hybrid weight 0: pure upwind on every face;
 the reference ties the RK stage count to the flux order, so 2 stages per
-step), constant Smagorinsky eddy viscosity (CS 0.03), dt 2e-3.  The same
-workload with Roe's flux is reported beside it.  Synthetic inputs from a
+step), constant Smagorinsky eddy viscosity (CS 0.03), dt 1e-3 (the CFL number
+summed over the three directions is 0.67; at 2e-3 it is 1.34 and this purely
+upwind RK2 scheme loses positivity within 35 steps).  The same workload with
+Roe's flux is reported beside it.  Synthetic inputs from a
 formula (no dataset).
 
 A "step" is one physical time step (eddy viscosity + every RK stage with its
@@ -53,17 +55,17 @@ ACC_STEPS = 100
 
 # -les 1 -fluxorder 2 -s_x 0 -s_y 0 -s_z 0: MUSCL-minmod + Rusanov, pure upwind
 CFG = dict(les=1, inviscid=0, fluxorder=2, eno_order=2, central=2, s_x=0.0, s_y=0.0, s_z=0.0,
-           ren=1600.0, ma=0.1, pr=0.71, gamma=1.4, dt=2e-3)
+           ren=1600.0, ma=0.1, pr=0.71, gamma=1.4, dt=1e-3)
 # the reference's default hybrid blend on the same TGV: WENO3 (-fluxorder 3,
-# SSP-RK3) blended with the 4-point central flux by the weight sigma
-CFG_WENO3_BLEND = dict(CFG, fluxorder=3)
+# SSP-RK3) blended with the 4-point central flux by the weight sigma, dt 2e-3
+CFG_WENO3_BLEND = dict(CFG, fluxorder=3, dt=2e-3)
 
 
 def workload_config(n):
     return {
         "workload": f"compressible Taylor-Green vortex LES, {n}^3 (DMDA {n + 2}^3), perturbed curvilinear grid, "
                     "MUSCL-minmod + Rusanov upwind (-les 1 -fluxorder 2 -s_x 0 -s_y 0 -s_z 0), Smagorinsky CS=0.03, "
-                    "viscous Re 1600 Ma 0.1, RK2 (fluxorder 2: the reference runs 2 stages/step), dt 2e-3",
+                    "viscous Re 1600 Ma 0.1, RK2 (fluxorder 2: the reference runs 2 stages/step), dt 1e-3",
         "flux_variant": "sigma = 0 on every face (-s_x = -s_y = -s_z = 0, sensor off): the blend (1 - sigma) * "
                         "upwind + sigma * central equals the upwind flux, so the stage kernel forms only that; the "
                         "reference also multiplies the eddy viscosity and Yoshizawa terms by sigma, so the "

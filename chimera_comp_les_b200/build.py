@@ -18,12 +18,21 @@ LIB_PATH = os.path.join(PKG_DIR, "libchimera_b200.so")
 # mixed form (FP32 fluxes) is compiled with contraction and fast FP32 division.
 FP64_FLAGS = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]
 MIXED_FLAGS = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]
+_C = os.path.join(PKG_DIR, "csrc")
+# (source, flags, object name): cb_stage_parts.cu is compiled once per form
+# (FP64 / mixed), LES value and launch kind (single block / batched) so the
+# stage-kernel template variants build in parallel
 SOURCES = [
-    (os.path.join(PKG_DIR, "csrc", "cb_api.cu"), FP64_FLAGS),
-    (os.path.join(PKG_DIR, "csrc", "cb_noalloc.cu"), FP64_FLAGS),
-    (os.path.join(PKG_DIR, "csrc", "cb_batch.cu"), FP64_FLAGS),
-    (os.path.join(PKG_DIR, "csrc", "cb_mixed.cu"), MIXED_FLAGS),
-    (os.path.join(PKG_DIR, "csrc", "cb_peaks.cu"), FP64_FLAGS),
+    (os.path.join(_C, "cb_api.cu"), FP64_FLAGS, "cb_api"),
+    (os.path.join(_C, "cb_noalloc.cu"), FP64_FLAGS, "cb_noalloc"),
+    (os.path.join(_C, "cb_batch.cu"), FP64_FLAGS, "cb_batch"),
+    (os.path.join(_C, "cb_mixed.cu"), MIXED_FLAGS, "cb_mixed"),
+    (os.path.join(_C, "cb_peaks.cu"), FP64_FLAGS, "cb_peaks"),
+] + [
+    (os.path.join(_C, "cb_stage_parts.cu"),
+     (MIXED_FLAGS if mix else FP64_FLAGS) + [f"-DCB_PART_MIX={mix}", f"-DCB_PART_LES={les}", f"-DCB_PART_BATCH={bat}"],
+     f"cb_stage_{'mixed' if mix else 'fp64'}_{'les' if les else 'std'}{'_batch' if bat else ''}")
+    for mix in (0, 1) for les in (1, 0) for bat in (0, 1)
 ]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 NVCC_FLAGS = [
@@ -57,14 +66,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB_PATH
     objdir = os.path.join(PKG_DIR, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs, procs = [], []
-    for src, flags in SOURCES:  # the translation units compile in parallel
-        obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
-        cmd = [NVCC] + NVCC_FLAGS + flags + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj, src]
-        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    objs, cmds = [], []
+    for src, flags, name in SOURCES:
+        obj = os.path.join(objdir, name + ".o")
+        cmds.append([NVCC] + NVCC_FLAGS + flags + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj, src])
         objs.append(obj)
+    # the translation units compile in parallel, at most one per core
     failed = None
-    for cmd, p in procs:
+    jobs = max(1, min(len(cmds), os.cpu_count() or 1))
+    pending, running = list(cmds), []
+    while pending or running:
+        while pending and len(running) < jobs:
+            cmd = pending.pop(0)
+            running.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+        cmd, p = running.pop(0)
         out, err = p.communicate()
         if p.returncode != 0:
             sys.stderr.write(out + err)

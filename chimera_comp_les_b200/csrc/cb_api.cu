@@ -156,25 +156,6 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
   return F;
 }
 
-template <bool LES, bool VISC, bool RHSM>
-static cudaError_t set_stage_attr() {
-  return stage_attrs<double, false, LES, VISC, RHSM>();
-}
-
-// Opt every stage-kernel variant into its dynamic shared memory on the
-// current device (done at context creation, never during graph capture).
-static cudaError_t set_stage_attrs() {
-  cudaError_t e;
-  if ((e = set_stage_attr<true, true, false>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<true, false, false>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<false, true, false>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<false, false, false>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<true, true, true>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<true, false, true>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<false, true, true>()) != cudaSuccess) return e;
-  return set_stage_attr<false, false, true>();
-}
-
 // Flux bits of the stage kernel: Roe, WENO5-JS, and with LES and the sensor
 // off the constant blend weight s_x = s_y = s_z when it is exactly 1 or 0.
 static int flux_bits(const cb_ctx *c) {
@@ -187,33 +168,10 @@ static int flux_bits(const cb_ctx *c) {
   return fl;
 }
 
-template <bool LES, bool VISC, bool RHSM>
-static cudaError_t launch_stage_t(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt) {
-  const int fl = flux_bits(c);
-  auto kern = stage_gen_kernel<double, false, LES, VISC, RHSM>(fl);
-  const bool nv = !RHSM && c->nv0;
-  if constexpr (!RHSM)
-    if (c->nv0) kern = stage_nv0_kernel<double, false, LES, VISC>(fl);
-  kern<<<stage_grid(c->dc, c->kchunk, c->sms, stage_tile_rows(fl)), stage_threads(fl), stage_smem_for<double, false>(fl, nv),
-         c->stream>>>(c->dc, F, istage, alfa, beta, adt, c->kchunk);
-  return cudaGetLastError();
-}
-
 static cudaError_t launch_stage(cb_ctx *c, const DevFields &F, int istage, double alfa, double beta, double adt, bool rhs_mode) {
-  const bool les = c->cfg.les != 0, visc = c->cfg.inviscid == 0;
-  if (c->cfg.precision == CB_MIXED)
-    return launch_stage_mixed(c->dc, F, istage, alfa, beta, adt, c->kchunk, les, visc, rhs_mode, flux_bits(c),
-                              c->nv0 && !rhs_mode, 2 * c->sms, c->stream);
-  if (rhs_mode) {
-    if (les && visc) return launch_stage_t<true, true, true>(c, F, istage, alfa, beta, adt);
-    if (les) return launch_stage_t<true, false, true>(c, F, istage, alfa, beta, adt);
-    if (visc) return launch_stage_t<false, true, true>(c, F, istage, alfa, beta, adt);
-    return launch_stage_t<false, false, true>(c, F, istage, alfa, beta, adt);
-  }
-  if (les && visc) return launch_stage_t<true, true, false>(c, F, istage, alfa, beta, adt);
-  if (les) return launch_stage_t<true, false, false>(c, F, istage, alfa, beta, adt);
-  if (visc) return launch_stage_t<false, true, false>(c, F, istage, alfa, beta, adt);
-  return launch_stage_t<false, false, false>(c, F, istage, alfa, beta, adt);
+  const bool les = c->cfg.les != 0, visc = c->cfg.inviscid == 0, mix = c->cfg.precision == CB_MIXED;
+  return launch_stage_any(mix, les, c->dc, F, istage, alfa, beta, adt, c->kchunk, visc, rhs_mode, flux_bits(c),
+                          c->nv0 && !rhs_mode, (mix ? 2 : 1) * c->sms, c->stream);
 }
 
 static cudaEvent_t ev_get(cb_ctx *c, int idx) {
@@ -606,9 +564,8 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   if (cudaSetDevice(c->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice failed");
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(CB_E_CUDA, "stream");
-  if (set_stage_attrs() != cudaSuccess) return bail(CB_E_CUDA, "stage kernel shared-memory opt-in failed");
-  if (cfg->precision == CB_MIXED && set_stage_attrs_mixed() != cudaSuccess)
-    return bail(CB_E_CUDA, "mixed stage kernel shared-memory opt-in failed");
+  if (stage_attrs_all(cfg->precision == CB_MIXED) != cudaSuccess)
+    return bail(CB_E_CUDA, "stage kernel shared-memory opt-in failed");
   DevCfg &d = c->dc;
   d.mx = cfg->mx; d.my = cfg->my; d.mz = cfg->mz;
   d.px = ((cfg->mx + 4 + 15) / 16) * 16;

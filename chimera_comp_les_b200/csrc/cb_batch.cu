@@ -99,50 +99,6 @@ struct BlockHost {
   bool nvz = true;      // the block's nvert is zero everywhere
 };
 
-// FP64 stage launches of one (LES, VISC, no-IBM) variant: the persistent
-// work-queue kernel or one block's grid
-template <bool LES, bool VISC, bool NV0>
-void f64_batched(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int s, double alfa,
-                 double beta, double adt, int ctas, cudaStream_t st) {
-  stage_batched_kernel<double, false, LES, VISC, NV0><<<ctas, SNT, stage_smem<double, false, NV0>(), st>>>(tab, items, nitems, counter, s,
-                                                                                          alfa, beta, adt);
-}
-template <bool LES, bool VISC, bool NV0>
-void f64_block(const DevCfg &dc, const DevFields &F, dim3 grid, int s, double alfa, double beta, double adt, int kc,
-               cudaStream_t st) {
-  stage_kernel<double, false, LES, VISC, false, 0, NV0><<<grid, SNT, stage_smem<double, false, NV0>(), st>>>(dc, F, s, alfa, beta, adt, kc);
-}
-template <bool NV0>
-void f64_batched_any(bool les, bool visc, const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int s,
-                     double alfa, double beta, double adt, int ctas, cudaStream_t st) {
-  if (les && visc) f64_batched<true, true, NV0>(tab, items, nitems, counter, s, alfa, beta, adt, ctas, st);
-  else if (les) f64_batched<true, false, NV0>(tab, items, nitems, counter, s, alfa, beta, adt, ctas, st);
-  else if (visc) f64_batched<false, true, NV0>(tab, items, nitems, counter, s, alfa, beta, adt, ctas, st);
-  else f64_batched<false, false, NV0>(tab, items, nitems, counter, s, alfa, beta, adt, ctas, st);
-}
-template <bool NV0>
-void f64_block_any(bool les, bool visc, const DevCfg &dc, const DevFields &F, dim3 grid, int s, double alfa, double beta,
-                   double adt, int kc, cudaStream_t st) {
-  if (les && visc) f64_block<true, true, NV0>(dc, F, grid, s, alfa, beta, adt, kc, st);
-  else if (les) f64_block<true, false, NV0>(dc, F, grid, s, alfa, beta, adt, kc, st);
-  else if (visc) f64_block<false, true, NV0>(dc, F, grid, s, alfa, beta, adt, kc, st);
-  else f64_block<false, false, NV0>(dc, F, grid, s, alfa, beta, adt, kc, st);
-}
-template <bool NV0>
-cudaError_t f64_attrs() {
-  const int sm = (int)stage_smem<double, false, NV0>();
-  const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(stage_batched_kernel<double, false, true, true, NV0>, a, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_batched_kernel<double, false, true, false, NV0>, a, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_batched_kernel<double, false, false, true, NV0>, a, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_batched_kernel<double, false, false, false, NV0>, a, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, true, true, false, 0, NV0>, a, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, true, false, false, 0, NV0>, a, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, false, true, false, 0, NV0>, a, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, false, false, false, false, 0, NV0>, a, sm);
-  return e;
-}
-
 }  // namespace
 
 struct cb_batch {
@@ -184,6 +140,18 @@ struct cb_batch {
   bool have_refs = false;
   std::string err;
 };
+
+// FLUX bits of the batch's stage kernels: Roe, WENO5-JS, and with LES the
+// constant blend weight s_x = s_y = s_z when it is exactly 1 or 0 (the
+// single-block context's rule; the sensor is not built here)
+static int batch_flux_bits(const cb_config &f) {
+  int fl = (f.flux == 1 ? FLUX_ROE : 0) | (f.weno_order == 5 ? FLUX_W5 : 0);
+  if (f.les && f.s_x == f.s_y && f.s_y == f.s_z) {
+    if (f.s_x == 1.0) fl |= FLUX_SIGMA1;
+    else if (f.s_x == 0.0) fl |= FLUX_SIGMA0;
+  }
+  return fl;
+}
 
 // every block's nvert is zero: the stage kernels' no-IBM variant
 static bool batch_nv0(const cb_batch *b) {
@@ -264,7 +232,8 @@ static int build_tables(cb_batch *b) {
     for (int z = 0; z < nch; z++)
       for (int y = 0; y < bh.tiles_y; y++)
         for (int x = 0; x < bh.tiles_x; x++) {
-          const int nxn = std::min(SBX, bh.mx - 2 - x * SBX), nyn = std::min(SBY, bh.my - 2 - y * SBY);
+          const int by = stage_tile_rows(batch_flux_bits(b->cfg));
+          const int nxn = std::min(SBX, bh.mx - 2 - x * SBX), nyn = std::min(by, bh.my - 2 - y * by);
           const int nzn = std::min(b->kchunk, bh.mz - 2 - z * b->kchunk);
           // interior nodes plus the 3-plane prologue of each chunk
           items.push_back({k, (z * bh.tiles_y + y) * bh.tiles_x + x, (long long)nxn * nyn * (nzn + 3)});
@@ -320,8 +289,10 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
   };
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
       (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
-      (cfg->les && cfg->calc_sigma) || cfg->flux != 0 || cfg->weno_order != 3)
+      (cfg->les && cfg->calc_sigma) || (cfg->flux != 0 && cfg->flux != 1) ||
+      (cfg->weno_order != 3 && cfg->weno_order != 5))
     return bail(CB_E_UNSUPPORTED, "option combination not built");
+  if (cfg->weno_order == 5 && cfg->fluxorder != 3) return bail(CB_E_ARG, "weno_order 5 needs fluxorder 3");
   if (cfg->visT && !(cfg->tref > 0.0)) return bail(CB_E_ARG, "Tref must be > 0 with visT");
   b->dev = cfg->device;
   if (cudaSetDevice(b->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice");
@@ -352,12 +323,13 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.gm1 = cfg->gamma - 1.0;
     d.nvq = 1;  // nvert starts zero
     d.calc_sigma = 0;  // the shock sensor is built for single-block contexts
-    d.flux = 0;  // the Roe flux is built for single-block contexts
+    d.flux = cfg->flux;
     if (shell_count(d) >= (1LL << 31)) return bail(CB_E_ARG, "block too large for 32-bit boundary indexing");
     bh.off = off;
     off += (d.plane + 31) / 32 * 32;  // 256-byte aligned block starts
     bh.tiles_x = (bh.mx - 2 + SBX - 1) / SBX;
-    bh.tiles_y = (bh.my - 2 + SBY - 1) / SBY;
+    const int by = stage_tile_rows(batch_flux_bits(*cfg));  // the variant's tile height
+    bh.tiles_y = (bh.my - 2 + by - 1) / by;
     maxnn = std::max(maxnn, (size_t)bh.mx * bh.my * bh.mz);
     b->blk.push_back(bh);
   }
@@ -383,10 +355,12 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     double *g = (double *)(f + (size_t)b->total * 3);
     for (int a = 0; a < 3; a++) b->gcl[a] = g + (size_t)b->total * a;
     if (cudaMalloc(&b->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "ptab4");
-    if (set_stage_attrs_mixed() != cudaSuccess || set_batched_attrs_mixed() != cudaSuccess)
-      return bail(CB_E_CUDA, "mixed kernel attributes");
   }
-  if (f64_attrs<false>() != cudaSuccess || f64_attrs<true>() != cudaSuccess) return bail(CB_E_CUDA, "kernel attributes");
+  {
+    const bool mix = cfg->precision == CB_MIXED;
+    if (stage_attrs_all(mix) != cudaSuccess || batch_attrs_all(mix) != cudaSuccess)
+      return bail(CB_E_CUDA, "stage kernel attributes");
+  }
   if (cudaMalloc(&b->staging, sizeof(double) * 5 * maxnn) != cudaSuccess) return bail(CB_E_CUDA, "staging");
   if (cudaMalloc(&b->ptab, sizeof(double *) * 64) != cudaSuccess) return bail(CB_E_CUDA, "ptab");
   if (cudaMalloc(&b->d_counter, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "counter");
@@ -738,15 +712,8 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
   if (!per_block) {
     BCUDA(b, cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream));
     const int ctas = b->sms * (mixed ? 2 : 1);
-    const bool nv0 = batch_nv0(b);
-    if (mixed) {
-      BCUDA(b, launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, les, visc, nv0, ctas,
-                                    b->stream));
-    } else if (nv0) {
-      f64_batched_any<true>(les, visc, tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, ctas, b->stream);
-    } else {
-      f64_batched_any<false>(les, visc, tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, ctas, b->stream);
-    }
+    BCUDA(b, launch_batched_any(mixed, les, tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, visc,
+                                batch_flux_bits(b->cfg), batch_nv0(b), ctas, b->stream));
   } else {
     for (int k = 0; k < b->nb; k++) {
       const BlockHost &bh = b->blk[k];
@@ -763,14 +730,8 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
         const double cost = (double)((blocks + slots - 1) / slots) * (cand + 1.0);
         if (cost < best) { best = cost; kc = cand; }
       }
-      if (mixed) {
-        BCUDA(b, launch_stage_mixed(bh.dc, F, s, alfa, beta, adt, kc, les, visc, false, 0, bh.nvz && !b->cfg.visT,
-                                    2 * b->sms, b->stream));
-      } else {
-        dim3 grid(bh.tiles_x, bh.tiles_y, (nk + kc - 1) / kc);
-        if (bh.nvz && !b->cfg.visT) f64_block_any<true>(les, visc, bh.dc, F, grid, s, alfa, beta, adt, kc, b->stream);
-        else f64_block_any<false>(les, visc, bh.dc, F, grid, s, alfa, beta, adt, kc, b->stream);
-      }
+      BCUDA(b, launch_stage_any(mixed, les, bh.dc, F, s, alfa, beta, adt, kc, visc, false, batch_flux_bits(b->cfg),
+                                bh.nvz && !b->cfg.visT, slots, b->stream));
     }
   }
   BCUDA(b, cudaGetLastError());
@@ -1044,14 +1005,8 @@ int cb_batch_autotune(cb_batch *b, int *best_kchunk, double *best_ms) {
       cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream);
       cudaEventRecord(e0, b->stream);
       const int ctas = b->sms * (mixed ? 2 : 1);
-      const bool nv0 = batch_nv0(b);
-      if (mixed) {
-        launch_batched_mixed(tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, les, visc, nv0, ctas, b->stream);
-      } else if (nv0) {
-        f64_batched_any<true>(les, visc, tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, ctas, b->stream);
-      } else {
-        f64_batched_any<false>(les, visc, tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, ctas, b->stream);
-      }
+      launch_batched_any(mixed, les, tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, visc,
+                         batch_flux_bits(b->cfg), batch_nv0(b), ctas, b->stream);
       cudaEventRecord(e1, b->stream);
       BCUDA(b, cudaEventSynchronize(e1));
       float ms = 0.f;

@@ -1,27 +1,13 @@
-// Mixed-precision form of the stage kernel (FP32 flux arithmetic, FP64 state,
-// EOS and RK combination).  Compiled with FMA contraction and fast FP32
-// division/sqrt; see cb_stage.cuh for the shift of the reference state.
+// Set-up kernel of the mixed-precision form: the FP32 metric vectors and the
+// FP64 metric divergence the stage kernel's FP32 fluxes are restored with
+// (see cb_stage.cuh for the shift of the reference state).  The mixed stage
+// kernels themselves are built from cb_stage_parts.cu.
 #include "cb_launch.h"
 #include "cb_stage.cuh"
 
 namespace cb {
 
 namespace {
-template <bool LES, bool VISC, bool RHSM>
-cudaError_t attr1() {
-  return stage_attrs<float, true, LES, VISC, RHSM>();
-}
-template <bool LES, bool VISC, bool RHSM>
-void launch1(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt, int kchunk,
-             int fl, bool nv0, int slots, cudaStream_t s) {
-  const dim3 grid = stage_grid(c, kchunk, slots, stage_tile_rows(fl));
-  auto kern = stage_gen_kernel<float, true, LES, VISC, RHSM>(fl);
-  const bool nv = !RHSM && nv0;
-  if constexpr (!RHSM)
-    if (nv0) kern = stage_nv0_kernel<float, true, LES, VISC>(fl);
-  kern<<<grid, stage_threads(fl), stage_smem_for<float, true>(fl, nv), s>>>(c, F, istage, alfa, beta, adt, kchunk);
-}
-
 __global__ void mixed_prep_kernel(const DevCfg c, const double *const *met, const double *delta2, const double *aj,
                                   float4 *const *met4, double *const *gcl) {
   const long long total = (long long)c.px * c.py * c.pz;
@@ -47,71 +33,6 @@ __global__ void mixed_prep_kernel(const DevCfg c, const double *const *met, cons
   }
 }
 }  // namespace
-
-cudaError_t set_stage_attrs_mixed() {
-  cudaError_t e;
-  if ((e = attr1<true, true, false>()) != cudaSuccess) return e;
-  if ((e = attr1<true, false, false>()) != cudaSuccess) return e;
-  if ((e = attr1<false, true, false>()) != cudaSuccess) return e;
-  if ((e = attr1<false, false, false>()) != cudaSuccess) return e;
-  if ((e = attr1<true, true, true>()) != cudaSuccess) return e;
-  if ((e = attr1<true, false, true>()) != cudaSuccess) return e;
-  if ((e = attr1<false, true, true>()) != cudaSuccess) return e;
-  return attr1<false, false, true>();
-}
-
-cudaError_t launch_stage_mixed(const DevCfg &c, const DevFields &F, int istage, double alfa, double beta, double adt,
-                               int kchunk, bool les, bool visc, bool rhs_mode, int fl, bool nv0, int slots,
-                               cudaStream_t s) {
-  if (rhs_mode) {
-    if (les && visc) launch1<true, true, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, slots, s);
-    else if (les) launch1<true, false, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, slots, s);
-    else if (visc) launch1<false, true, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, slots, s);
-    else launch1<false, false, true>(c, F, istage, alfa, beta, adt, kchunk, fl, false, slots, s);
-  } else {
-    if (les && visc) launch1<true, true, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, slots, s);
-    else if (les) launch1<true, false, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, slots, s);
-    else if (visc) launch1<false, true, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, slots, s);
-    else launch1<false, false, false>(c, F, istage, alfa, beta, adt, kchunk, fl, nv0, slots, s);
-  }
-  return cudaGetLastError();
-}
-
-namespace {
-template <bool LES, bool VISC>
-cudaError_t battr1() {
-  const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC>, a, (int)STAGE_SMEM_BYTES_MIXED);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_batched_kernel<float, true, LES, VISC, true>, a,
-                              (int)stage_smem<float, true, true>());
-}
-template <bool LES, bool VISC>
-void blaunch1(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int istage, double alfa,
-              double beta, double adt, bool nv0, int ctas, cudaStream_t s) {
-  auto kern = nv0 ? stage_batched_kernel<float, true, LES, VISC, true> : stage_batched_kernel<float, true, LES, VISC, false>;
-  const size_t smem = nv0 ? stage_smem<float, true, true>() : STAGE_SMEM_BYTES_MIXED;
-  kern<<<ctas, SNT, smem, s>>>(tab, items, nitems, counter, istage, alfa, beta, adt);
-}
-}  // namespace
-
-cudaError_t set_batched_attrs_mixed() {
-  cudaError_t e;
-  if ((e = battr1<true, true>()) != cudaSuccess) return e;
-  if ((e = battr1<true, false>()) != cudaSuccess) return e;
-  if ((e = battr1<false, true>()) != cudaSuccess) return e;
-  return battr1<false, false>();
-}
-
-cudaError_t launch_batched_mixed(const BatchBlock *tab, const int2 *items, int nitems, unsigned *counter, int istage,
-                                 double alfa, double beta, double adt, bool les, bool visc, bool nv0, int ctas,
-                                 cudaStream_t s) {
-  if (les && visc) blaunch1<true, true>(tab, items, nitems, counter, istage, alfa, beta, adt, nv0, ctas, s);
-  else if (les) blaunch1<true, false>(tab, items, nitems, counter, istage, alfa, beta, adt, nv0, ctas, s);
-  else if (visc) blaunch1<false, true>(tab, items, nitems, counter, istage, alfa, beta, adt, nv0, ctas, s);
-  else blaunch1<false, false>(tab, items, nitems, counter, istage, alfa, beta, adt, nv0, ctas, s);
-  return cudaGetLastError();
-}
 
 cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, const double *aj,
                               float4 *const *met4, double *const *gcl, int grid, cudaStream_t s) {

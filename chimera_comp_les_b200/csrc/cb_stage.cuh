@@ -1174,7 +1174,9 @@ cudaError_t stage_attrs() {
 // Several blocks of uneven sizes advanced by ONE persistent launch: every CTA
 // takes work items (block, tile column, k-chunk) from a device counter until
 // the list is exhausted (a bounded loop, no waiting on other CTAs).  Items are
-// listed largest-first by the host so the tail of the launch is short.
+// listed largest-first by the host so the tail of the launch is short.  The
+// blocks share the options, hence the FLUX bits and the tile geometry
+// (StageGeo<FLUX>) the host cut the tile columns with.
 struct BatchBlock {
   DevCfg c;
   DevFields F;
@@ -1182,8 +1184,8 @@ struct BatchBlock {
   long long first_item;  // index of this block's first item in the global list
 };
 
-template <typename R, bool MIX, bool LES, bool VISC, bool NV0 = false>
-__global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
+template <typename R, bool MIX, bool LES, bool VISC, bool NV0 = false, int FLUX = 0>
+__global__ void __launch_bounds__(StageGeo<FLUX>::NT, MIX ? 2 : 1)
     stage_batched_kernel(const BatchBlock *__restrict__ blocks, const int2 *__restrict__ items, int nitems,
                          unsigned *__restrict__ counter, int istage, double alfa, double beta, double adt) {
   extern __shared__ double smem_d[];
@@ -1201,8 +1203,8 @@ __global__ void __launch_bounds__(SNT, MIX ? 2 : 1)
     const int bzi = ib.y / txy, rem = ib.y - bzi * txy;
     const int byi = rem / bb.tiles_x, bxi = rem - byi * bb.tiles_x;
     const int kb = 1 + bzi * bb.kchunk;
-    stage_tile<R, MIX, LES, VISC, false, 0, NV0>(bb.c, bb.F, bxi, byi, kb, min(bb.c.mz - 1, kb + bb.kchunk), istage, alfa,
-                                                beta, adt, smem_d);
+    stage_tile<R, MIX, LES, VISC, false, FLUX, NV0>(bb.c, bb.F, bxi, byi, kb, min(bb.c.mz - 1, kb + bb.kchunk), istage,
+                                                   alfa, beta, adt, smem_d);
     __syncthreads();  // bb and item are rewritten by the next iteration
   }
 }

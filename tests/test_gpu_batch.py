@@ -62,6 +62,39 @@ def test_self_periodic_batch_equals_single_blocks(per_block):
         assert np.array_equal(g, want), max(per_field_rel_l2(g, want))
 
 
+# the stage-kernel variants of the options: Roe's flux, WENO5-JS (its 32 x 5
+# tile and six-plane ring), and the constant blend weights 0 and 1
+VARIANTS = [
+    ("roe", dict(flux="roe")),
+    ("weno5", dict(weno_order=5, s_x=0.5, s_y=0.5, s_z=0.5)),
+    ("weno5_roe_sigma0", dict(weno_order=5, flux="roe", s_x=0.0, s_y=0.0, s_z=0.0)),
+    ("sigma1", dict(s_x=1.0, s_y=1.0, s_z=1.0)),
+]
+
+
+@pytest.mark.parametrize("per_block", [False, True])
+@pytest.mark.parametrize("name,over", VARIANTS, ids=[v[0] for v in VARIANTS])
+def test_batch_variants_equal_single_blocks(name, over, per_block):
+    """Every option the single-block context builds for the stage kernel runs
+    in the batch too: FP64 bit for bit against the same blocks alone, the
+    mixed form within 1e-12 of its own single-block runs (FMA contraction
+    makes two launch shapes differ in the last bits)."""
+    opts = dict(OPTS, **over)
+    inputs = _inputs(DIMS, seed0=3)
+    steps = 2
+    for prec in ("fp64", "mixed"):
+        with _batch(DIMS, inputs, precision=prec, opts=opts) as bt:
+            bt.halo_periodic()
+            bt.RungeKutta(steps, per_block=per_block)
+            got = [bt.Q(k) for k in range(len(DIMS))]
+        for d, (coords, q), g in zip(DIMS, inputs, got):
+            want = _single(d, coords, q, steps, precision=prec, opts=opts)
+            if prec == "fp64":
+                assert np.array_equal(g, want), max(per_field_rel_l2(g, want))
+            else:
+                assert max(per_field_rel_l2(g, want)) <= 1e-8
+
+
 def test_batch_block_matches_oracle():
     """First block of a batch against the CPU restatement (2 steps)."""
     d = (14, 12, 11)

@@ -51,9 +51,11 @@ def test_weno5_gpu_matches_restatement(name, n, kw, mask):
     q = W.random_smooth_state(shape, seed=13, periodic=periodic)
     nv = _mask(shape) if mask else np.zeros(shape)
     ref = oracle_run(cfg, coords, q, nv, steps=2)
-    # the restatement's WENO5 differs from its WENO3 on this case
-    ref3 = oracle_run(O.Config(**{**cfg.__dict__, "weno_order": 3}), coords, q, nv)
-    assert max(per_field_rel_l2(ref3["rhs"], ref["rhs"])) > 1e-9
+    # the restatement's WENO5 differs from its WENO3 on this case (not at a
+    # blend weight of 1, which multiplies every upwind flux by zero)
+    if not (cfg.les and cfg.s_x == cfg.s_y == cfg.s_z == 1.0):
+        ref3 = oracle_run(O.Config(**{**cfg.__dict__, "weno_order": 3}), coords, q, nv)
+        assert max(per_field_rel_l2(ref3["rhs"], ref["rhs"])) > 1e-9
     with gpu_block(cfg) as b:
         b.FormMetrics(coords)
         b.set_nvert(nv)
