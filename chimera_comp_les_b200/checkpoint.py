@@ -7,10 +7,11 @@ File names: ``Qfield%05d_%1d.dat`` (5 per node), ``pfield%05d_%1d.dat``,
 Each is one PETSc binary Vec: big-endian int32 class id 1211214
 (VEC_FILE_CLASSID), int32 global length, then the values as big-endian
 float64 in the DMDA's natural order (i fastest, components interleaved) --
-the layout PETSc's VecView writes for a DMDA vector on a binary viewer, which
-also writes a ``.info`` side file carrying ``-vecload_block_size`` for
-multi-component vectors.  The PETSc library is not vendored with the
-reference; this is its documented binary format (PETSc 3.12, main.c:4).
+the layout PETSc's VecView writes for a DMDA vector on a binary viewer.  The
+viewer also opens a ``.info`` side file with every file it writes, to which
+VecView adds ``-vecload_block_size <n>`` for an n-component vector (empty for
+one component).  The PETSc library is not vendored with the reference; this
+is its documented binary format (PETSc 3.12, main.c:4).
 """
 from __future__ import annotations
 
@@ -28,8 +29,8 @@ def write_vec(path: str, a: np.ndarray, block_size: int = 1) -> None:
     with open(path, "wb") as f:
         f.write(np.array([VEC_FILE_CLASSID, flat.size], dtype=">i4").tobytes())
         f.write(flat.astype(">f8").tobytes())
-    if block_size > 1:
-        with open(path + ".info", "w") as f:
+    with open(path + ".info", "w") as f:
+        if block_size > 1:
             f.write(f"-vecload_block_size {block_size}\n")
 
 
@@ -63,6 +64,22 @@ def sigma_field(shape, les: bool, s_x: float, s_y: float, s_z: float) -> np.ndar
     return sig
 
 
+def write_fields(ti: int, this: int, directory: str, q: np.ndarray, p: np.ndarray, nvert: np.ndarray,
+                 sigma: Optional[np.ndarray] = None, nut: Optional[np.ndarray] = None):
+    """The files of main.c:247-304 from natural-order arrays, in its order:
+    Qfield, sigma (LES), pfield, nvfield, nu_t (LES); the averaging files of
+    -averaging are not written.  Returns the paths."""
+    out = []
+    for stem, a, bs in (("Qfield", q, 5), ("sigma", sigma, 3), ("pfield", p, 1), ("nvfield", nvert, 1),
+                        ("nu_t", nut, 1)):
+        if a is None:
+            continue
+        path = _name(stem, ti, this, directory)
+        write_vec(path, a, bs)
+        out.append(path)
+    return out
+
+
 def Q_P_Binary_Output(block, ti: int, this: int = 0, directory: str = ".", nvert: Optional[np.ndarray] = None):
     """Writes the checkpoint of a ``solver.Block`` (Q, P from the EOS, nvert,
     and with LES nu_t and Sigma) as main.c:247-304 does; returns the paths."""
@@ -70,26 +87,10 @@ def Q_P_Binary_Output(block, ti: int, this: int = 0, directory: str = ".", nvert
     p = np.empty(block.shape)
     block.download(q, p)
     nv = np.zeros(block.shape) if nvert is None else np.asarray(nvert, dtype=np.float64).reshape(block.shape)
-    out = []
-    path = _name("Qfield", ti, this, directory)
-    write_vec(path, q, 5)
-    out.append(path)
     cfg = block.cfg
-    if cfg.les:
-        path = _name("sigma", ti, this, directory)
-        write_vec(path, sigma_field(block.shape, True, cfg.s_x, cfg.s_y, cfg.s_z), 3)
-        out.append(path)
-    path = _name("pfield", ti, this, directory)
-    write_vec(path, p)
-    out.append(path)
-    path = _name("nvfield", ti, this, directory)
-    write_vec(path, nv)
-    out.append(path)
-    if cfg.les:
-        path = _name("nu_t", ti, this, directory)
-        write_vec(path, block.nu_t())
-        out.append(path)
-    return out
+    les = bool(cfg.les)
+    sig = sigma_field(block.shape, True, cfg.s_x, cfg.s_y, cfg.s_z) if les else None
+    return write_fields(ti, this, directory, q, p, nv, sig, block.nu_t() if les else None)
 
 
 def Q_P_Binary_Input(block, ti: int, this: int = 0, directory: str = ".") -> np.ndarray:

@@ -32,6 +32,8 @@ ORACLE_SO = os.path.join(_HERE, "_build", "liboracle.so")
 ORACLE_COUNT_SO = os.path.join(_HERE, "_build", "liboracle_count.so")
 REF_SO = os.path.join(_HERE, "_ref", "libchimera_ref.so")
 REF_SO_O3 = os.path.join(_HERE, "_ref", "libchimera_ref_O3.so")
+# the same objects plus the reference's main.c: its checkpoint writer/reader
+REF_IO_SO = os.path.join(_HERE, "_ref", "libchimera_ref_io.so")
 # the reference checkout: CHIMERA_REF_DIR, else a sibling directory of this
 # repository named "reference"
 REF_SRC_DIR = os.environ.get("CHIMERA_REF_DIR") or os.path.normpath(os.path.join(_HERE, "..", "..", "reference"))
@@ -452,8 +454,8 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO) or os.path.isdir(REF_SRC_DIR)
 
 
-def build_ref(force: bool = False, optimized: bool = False) -> str:
-    so = REF_SO_O3 if optimized else REF_SO
+def build_ref(force: bool = False, optimized: bool = False, io: bool = False) -> str:
+    so = REF_IO_SO if io else (REF_SO_O3 if optimized else REF_SO)
     if force or not os.path.exists(so):
         if not os.path.isdir(REF_SRC_DIR):
             raise FileNotFoundError("reference sources not present; cannot build oracle/_ref")
@@ -465,13 +467,14 @@ class RefOracle:
     """The reference's own hot-path C (via the PETSc shim); one live instance
     per process (the reference keeps its state in globals)."""
 
-    def __init__(self, cfg: Config, coords_nat: np.ndarray, optimized: bool = False):
+    def __init__(self, cfg: Config, coords_nat: np.ndarray, optimized: bool = False, io: bool = False):
         if cfg.flux != 0:
             raise ValueError("the reference has no Roe flux (flux 1); check it against the restatement")
         if cfg.weno_order != 3:
             raise ValueError("the reference has no WENO5 (weno_order 5); check it against the restatement")
         self.cfg = cfg
-        self.lib = C.CDLL(build_ref(optimized=optimized))
+        self.lib = C.CDLL(build_ref(optimized=optimized, io=io))
+        self.io = io
         L = self.lib
         D = C.POINTER(C.c_double)
         L.ref_setup.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), D, C.c_char_p]
@@ -497,6 +500,18 @@ class RefOracle:
         a = np.ascontiguousarray(nvert_nat, dtype=np.float64).reshape(-1)
         assert a.size == self.nnodes
         self.lib.ref_set_nvert(_dp(a))
+
+    def write_checkpoint(self, ti: int) -> None:
+        """The reference's Q_P_Binary_Output (main.c:247-304) as time step ti,
+        block 0, into the working directory (needs io=True)."""
+        if not self.io or self.lib.ref_write_checkpoint(ti):
+            raise RuntimeError("Q_P_Binary_Output failed")
+
+    def restart(self, ti: int) -> None:
+        """The reference's RestartApplication (main.c:620-693) from the files
+        of time step ti in the working directory (needs io=True)."""
+        if not self.io or self.lib.ref_restart(ti):
+            raise RuntimeError("RestartApplication failed")
 
     def set_state(self, q_nat: np.ndarray):
         a = np.ascontiguousarray(q_nat, dtype=np.float64).reshape(-1)

@@ -227,4 +227,19 @@ PetscErrorCode DMGetCoordinateDM(DM dm, DM *cdm);
 PetscErrorCode DMGetCoordinatesLocal(DM dm, Vec *c);
 PetscErrorCode DMGetCoordinates(DM dm, Vec *c);
 
+/* ---- objects and the binary viewer (checkpoint files, main.c:215-304) ---- */
+typedef struct _p_PetscObject *PetscObject;
+#define PETSCVIEWERVTK "vtk"
+PetscErrorCode PetscViewerBinaryOpen(MPI_Comm c, const char *name, PetscFileMode mode, PetscViewer *v);
+PetscErrorCode PetscViewerDestroy(PetscViewer *v);
+PetscErrorCode VecView(Vec x, PetscViewer v);
+PetscErrorCode VecLoad(Vec x, PetscViewer v);
+PetscErrorCode PetscViewerCreate(MPI_Comm c, PetscViewer *v);
+PetscErrorCode PetscViewerSetType(PetscViewer v, const char *t);
+PetscErrorCode PetscViewerFileSetMode(PetscViewer v, PetscFileMode m);
+PetscErrorCode PetscViewerFileSetName(PetscViewer v, const char *n);
+PetscErrorCode PetscObjectSetName(PetscObject o, const char *n);
+PetscErrorCode PetscObjectSetOptionsPrefix(PetscObject o, const char *p);
+PetscErrorCode PetscOptionsClearValue(void *o, const char *n);
+
 #endif

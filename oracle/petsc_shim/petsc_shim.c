@@ -506,3 +506,87 @@ PetscErrorCode DMGetCoordinatesLocal(DM dm, Vec *c) {
   return 0;
 }
 PetscErrorCode DMGetCoordinates(DM dm, Vec *c) { ensure_cdm(dm); *c = dm->coords; return 0; }
+
+/* ------------------------------------------------------------------ */
+/* Binary viewer: PetscViewerBinaryOpen / VecView / VecLoad in PETSc's */
+/* binary Vec format -- int32 VEC_FILE_CLASSID (1211214), int32 global */
+/* length, the values as big-endian float64; a DMDA Vec in natural     */
+/* (k-j-i, dof-interleaved) order, which on one rank is the global     */
+/* Vec's own order.  Opening a file for writing also opens its ".info" */
+/* side file, to which VecView adds "-vecload_block_size <dof>" for a  */
+/* Vec of more than one component (what VecLoad reads back).           */
+/* ------------------------------------------------------------------ */
+#define SHIM_VEC_FILE_CLASSID 1211214
+struct _p_PetscViewer {
+  FILE *f, *info;
+  PetscFileMode mode;
+};
+
+static void put_be32(FILE *f, int v) {
+  unsigned char b[4] = {(unsigned char)(v >> 24), (unsigned char)(v >> 16), (unsigned char)(v >> 8), (unsigned char)v};
+  fwrite(b, 1, 4, f);
+}
+static int get_be32(FILE *f, int *v) {
+  unsigned char b[4];
+  if (fread(b, 1, 4, f) != 4) return 1;
+  *v = (int)(((unsigned)b[0] << 24) | ((unsigned)b[1] << 16) | ((unsigned)b[2] << 8) | (unsigned)b[3]);
+  return 0;
+}
+
+PetscErrorCode PetscViewerBinaryOpen(MPI_Comm c, const char *name, PetscFileMode mode, PetscViewer *v) {
+  (void)c;
+  PetscViewer w = (PetscViewer)calloc(1, sizeof(struct _p_PetscViewer));
+  w->mode = mode;
+  w->f = fopen(name, mode == FILE_MODE_READ ? "rb" : "wb");
+  if (!w->f) { free(w); *v = NULL; return 1; }
+  if (mode != FILE_MODE_READ) {
+    char info[PETSC_MAX_PATH_LEN];
+    snprintf(info, sizeof info, "%s.info", name);
+    w->info = fopen(info, "w");
+  }
+  *v = w;
+  return 0;
+}
+PetscErrorCode PetscViewerDestroy(PetscViewer *v) {
+  if (!v || !*v) return 0;
+  if ((*v)->f) fclose((*v)->f);
+  if ((*v)->info) fclose((*v)->info);
+  free(*v);
+  *v = NULL;
+  return 0;
+}
+PetscErrorCode VecView(Vec x, PetscViewer v) {
+  if (!v || !v->f || v->mode == FILE_MODE_READ || x->local) return 1;
+  put_be32(v->f, SHIM_VEC_FILE_CLASSID);
+  put_be32(v->f, x->n);
+  for (PetscInt t = 0; t < x->n; t++) {
+    unsigned long long u;
+    memcpy(&u, &x->a[t], 8);
+    unsigned char b[8];
+    for (int k = 0; k < 8; k++) b[k] = (unsigned char)(u >> (56 - 8 * k));
+    fwrite(b, 1, 8, v->f);
+  }
+  if (v->info && x->dm && x->dm->dof > 1) fprintf(v->info, "-vecload_block_size %d\n", (int)x->dm->dof);
+  return 0;
+}
+PetscErrorCode VecLoad(Vec x, PetscViewer v) {
+  int cls = 0, n = 0;
+  if (!v || !v->f || v->mode != FILE_MODE_READ || x->local) return 1;
+  if (get_be32(v->f, &cls) || cls != SHIM_VEC_FILE_CLASSID || get_be32(v->f, &n) || n != x->n) return 1;
+  for (PetscInt t = 0; t < x->n; t++) {
+    unsigned char b[8];
+    if (fread(b, 1, 8, v->f) != 8) return 1;
+    unsigned long long u = 0;
+    for (int k = 0; k < 8; k++) u = (u << 8) | b[k];
+    memcpy(&x->a[t], &u, 8);
+  }
+  return 0;
+}
+/* VTK viewer calls of the reference's Q_P_VTK_Input (never run here) */
+PetscErrorCode PetscViewerCreate(MPI_Comm c, PetscViewer *v) { (void)c; *v = (PetscViewer)calloc(1, sizeof(struct _p_PetscViewer)); return 0; }
+PetscErrorCode PetscViewerSetType(PetscViewer v, const char *t) { (void)v; (void)t; return 0; }
+PetscErrorCode PetscViewerFileSetMode(PetscViewer v, PetscFileMode m) { if (v) v->mode = m; return 0; }
+PetscErrorCode PetscViewerFileSetName(PetscViewer v, const char *n) { (void)v; (void)n; return 1; }
+PetscErrorCode PetscObjectSetName(PetscObject o, const char *n) { (void)o; (void)n; return 0; }
+PetscErrorCode PetscObjectSetOptionsPrefix(PetscObject o, const char *p) { (void)o; (void)p; return 0; }
+PetscErrorCode PetscOptionsClearValue(void *o, const char *n) { (void)o; (void)n; return 0; }

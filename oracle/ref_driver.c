@@ -25,7 +25,11 @@
  */
 #include "variables.h"
 
-/* ---- globals the reference expects from main.c (defaults main.c:14-75) ---- */
+/* ---- globals the reference expects from main.c (defaults main.c:14-75) ----
+ * With CHIMERA_REF_WITH_MAIN the reference's main.c itself is linked (its
+ * checkpoint writer/reader and RestartApplication, main.c:215-304, 620-693)
+ * and defines these; the driver then keeps only those main.c lacks. */
+#ifndef CHIMERA_REF_WITH_MAIN
 PetscInt tistart = 0;
 PetscBool rstart_flg = PETSC_FALSE;
 PetscInt immersed = 0;
@@ -54,6 +58,18 @@ PetscInt channel = 0;
 PetscInt block_number = 1;
 PetscReal max_cs = 0.5;
 PetscInt thin = 0;  /* main.c:45, read by ibm_search_advanced */
+#else
+extern PetscInt tistart;
+extern PetscBool rstart_flg;
+extern PetscInt immersed, wavy, isothermal, calc_sigma, invicid, movefsi, rotatefsi, sediment;
+extern PetscReal CMx_c, CMy_c, CMz_c;
+extern PetscInt TwoD, STRONG_COUPLING, fish, NumberOfBodies, moveframe, rotateframe, central, les, rans;
+extern PetscInt wallfunction, averaging, mixed, clark, dynamic_freq, i_periodic, j_periodic, k_periodic;
+extern PetscInt testfilter_ik, testfilter_1d, i_homo_filter, j_homo_filter, k_homo_filter, channel, thin;
+extern PetscReal max_cs;
+PetscInt ii_periodic = 0, jj_periodic = 0, kk_periodic = 0;
+PetscInt block_number = 1;
+#endif
 
 /* ---- reference entry points (prototypes live only under __cplusplus) ---- */
 PetscErrorCode FormMetrics(UserCtx *user);
@@ -72,7 +88,9 @@ void AddIBMNode(IBMList *ilist, IBMInfo ibm_intp);
 void DestroyIBMList(IBMList *ilist);
 
 /* ---- stubs for subsystems outside the hot path (IBM, FSI, output) ---- */
+#ifndef CHIMERA_REF_WITH_MAIN
 PetscErrorCode Q_P_Binary_Output(UserCtx *u) { (void)u; return 0; }
+#endif
 PetscErrorCode Calc_forces_SI2() { return 0; }
 PetscErrorCode Calc_FSI_pos_intg() { return 0; }
 PetscErrorCode fish_swim() { return 0; }
@@ -466,3 +484,28 @@ int ref_formbcs(double alfa) {
   if (!U) return 1;
   return FormBCS(U, alfa);
 }
+
+#ifdef CHIMERA_REF_WITH_MAIN
+/* ---- checkpoint files through the reference's own main.c ---- */
+PetscErrorCode Q_P_Binary_Output(UserCtx *user);
+PetscErrorCode RestartApplication(UserCtx *user, IBMNodes *ibm, FSInfo *fsi, Cstart *cstart, PetscInt tistart);
+
+/* Q_P_Binary_Output (main.c:247-304) of the current state as time step ti,
+ * block 0, into the working directory. */
+int ref_write_checkpoint(int ti) {
+  if (!U) return 1;
+  U->ti = ti;
+  U->_this = 0;
+  return Q_P_Binary_Output(U);
+}
+
+/* RestartApplication (main.c:620-693) from the files of time step ti in the
+ * working directory: Q, P and Nvert read back, their ghosted copies, Qold;
+ * the driver's step counter continues from ti. */
+int ref_restart(int ti) {
+  if (!U) return 1;
+  int e = RestartApplication(U, NULL, NULL, NULL, ti);
+  g_ti = ti;
+  return e;
+}
+#endif
