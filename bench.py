@@ -865,6 +865,28 @@ def run_sharded(args, ws, rank, local):
     bt.close()
 
 
+def run_profile(args, local):
+    """The headline workload for a profiler: one form (--precision), the
+    k-chunk given by --profile-kchunk (one autotuner candidate: 3 stage
+    launches), then --steps time steps; no timing, no other workloads."""
+    import torch
+
+    from chimera_comp_les_b200 import workloads as W
+    torch.cuda.set_device(local)
+    n = N_UNIQUE
+    coords = W.periodic_grid(n, 2 * math.pi, amp=0.05)
+    q0 = W.tgv_state(coords, gamma=CFG["gamma"], ma=CFG["ma"])
+    from chimera_comp_les_b200 import Block
+    with Block(n + 2, n + 2, n + 2, precision=args.precision, device=local, **CFG) as blk:
+        blk.FormMetrics(coords)
+        blk.set_nvert(np.zeros(coords.shape[:3]))
+        blk.SetInitialCondition(q0)
+        kc, ms = blk.autotune([args.profile_kchunk])
+        blk.RungeKutta(args.steps)
+        print(json.dumps({"profile_case": workload_config(n)["workload"], "precision_form": args.precision,
+                          "kchunk": kc, "stage_ms": ms, "steps": args.steps}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -878,6 +900,9 @@ def main():
     ap.add_argument("--no-blend", action="store_true", help="skip the WENO3 blend (sigma 1 and 0.5) on the headline TGV")
     ap.add_argument("--no-extras", action="store_true", help="skip the Roe-flux measurement of the headline workload")
     ap.add_argument("--no-config5", action="store_true", help="skip the 512^3 isotropic-turbulence measurement")
+    ap.add_argument("--profile", action="store_true",
+                    help="run the headline workload in one form for a profiler (no timing, no other workloads)")
+    ap.add_argument("--profile-kchunk", type=int, default=10, help="k-chunk of the --profile run")
     ap.add_argument("--sweep", default="", help="comma-separated sizes, e.g. 128,256,384,512: isotropic-turbulence "
                                                   "size sweep, one JSON line per size instead of the bench line")
     ap.add_argument("--workload", default="tgv", choices=["tgv", "sphere"],
@@ -895,6 +920,8 @@ def main():
         layout = args.layout if args.layout != "auto" else ("slabs" if ws > 1 else "replicas")
         if args.impl == "reference":
             run_reference(args, ws, rank)
+        elif args.profile:
+            run_profile(args, local)
         elif args.sweep:
             run_sweep(args, local)
         elif args.workload == "sphere":
