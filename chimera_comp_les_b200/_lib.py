@@ -99,6 +99,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.cb_launches_per_step.restype = C.c_int
     lib.cb_last_error.argtypes = [P]
     lib.cb_last_error.restype = C.c_char_p
+    lib.cb_set_time_index.argtypes = [P, C.c_int]
+    lib.cb_set_time_index.restype = C.c_int
     lib.cb_pipe_peaks.argtypes = [C.c_int, D, D]
     lib.cb_pipe_peaks.restype = C.c_int
     # immersed bodies

@@ -95,6 +95,8 @@ struct cb_ctx {
   IbmBody ibm[CB_IBM_MAX_BODIES];
   double *ibm_arena = nullptr;  // 7 planes: spare (5) and psnap (1), the Q and P FormBCS reads, and pl
   double *spare = nullptr, *psnap = nullptr;
+  double *coorxy = nullptr;  // node coordinates x, y (k-lo inflow codes 52 and 47), padded planes
+  int *ti_dev = nullptr;     // step index user->ti on the device (code 47)
   double *pl = nullptr;  // the reference's P / lP after an immersed step
   bool p_carry = false;  // pl holds lP of the current state (no EqOfState since the interpolation)
   int ibm_twoD = 0, ibm_wallfunction = 0;
@@ -153,6 +155,9 @@ static DevFields fields_for(cb_ctx *c, int in, int old, int out) {
   for (int a = 0; a < 3; a++) F.sig[a] = c->sig_a[a];
   for (int a = 0; a < 3; a++) F.gcl[a] = c->gcl[a];
   F.status = c->status;
+  F.cx = c->coorxy;
+  F.cy = c->coorxy ? c->coorxy + c->plane : nullptr;
+  F.ti = c->ti_dev;
   return F;
 }
 
@@ -408,6 +413,7 @@ static int formbcs_zero(cb_ctx *c, int old) {
 
 // Enqueue one time step (no graph).
 static int enqueue_step(cb_ctx *c) {
+  if (c->dc.bctype[4] == 47) step_index_advance_kernel<<<1, 1, 0, c->stream>>>(c->ti_dev);
   if (c->cfg.les && c->cfg.les != 10 && !c->cfg.inviscid) {  // solvers.c:28
     int e = nut_update(c);
     if (e) return e;
@@ -505,6 +511,13 @@ extern "C" {
 
 int cb_abi_version(void) { return CB_ABI_VERSION; }
 
+int cb_set_time_index(cb_ctx *c, int ti) {
+  if (!c) return CB_E_ARG;
+  CB_CUDA(c, cudaMemcpyAsync(c->ti_dev, &ti, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
 void cb_config_default(cb_config *cfg, int mx, int my, int mz) {
   std::memset(cfg, 0, sizeof(*cfg));
   cfg->mx = mx; cfg->my = my; cfg->mz = mz;
@@ -543,8 +556,6 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
     for (int d = 0; d < 3; d++)
       if ((bc[2 * d] == 7) != (bc[2 * d + 1] == 7))
         return bail(CB_E_UNSUPPORTED, "a periodic direction needs bctype 7 on both faces");
-    if (bc[4] == 52 || bc[4] == 47)
-      return bail(CB_E_UNSUPPORTED, "boundary codes 52 and 47 (profile inlets from the coordinates) are not built");
     c->fully_periodic = true;
     for (int b = 0; b < 6; b++) c->fully_periodic = c->fully_periodic && bc[b] == 7;
   }
@@ -639,6 +650,12 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   }
   if (cudaMalloc(&c->ptab, sizeof(double *) * PT_N) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc ptab");
   if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc status");
+  if (cudaMalloc(&c->ti_dev, sizeof(int)) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc step index");
+  cudaMemsetAsync(c->ti_dev, 0, sizeof(int), c->stream);
+  if (cfg->bctype[4] == 52 || cfg->bctype[4] == 47) {  // the inflow codes read the node coordinates
+    if (cudaMalloc(&c->coorxy, sizeof(double) * c->plane * 2) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc coordinates");
+    cudaMemsetAsync(c->coorxy, 0, sizeof(double) * c->plane * 2, c->stream);
+  }
   cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream);
   if (fill_ptab(c)) return bail(CB_E_CUDA, "pointer table");
   // k-chunk: whole waves of the resident blocks (1 per SM in the FP64 form,
@@ -681,6 +698,8 @@ void cb_destroy(cb_ctx *c) {
   if (c->ibm_arena) cudaFree(c->ibm_arena);
   if (c->ptab) cudaFree(c->ptab);
   if (c->status) cudaFree(c->status);
+  if (c->ti_dev) cudaFree(c->ti_dev);
+  if (c->coorxy) cudaFree(c->coorxy);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -751,6 +770,10 @@ int cb_set_grid(cb_ctx *c, const double *coor) {
   if (c->cfg.precision == CB_MIXED)
     CB_CUDA(c, launch_mixed_prep(c->dc, (const double *const *)(c->ptab + PT_MET), c->delta2, c->aj, c->ptab4,
                                  c->ptab + PT_GCL, grid_for(c, (long long)c->plane), c->stream));
+  if (c->coorxy)  // x and y kept for the inflow codes that read them
+    for (int q = 0; q < 2; q++)
+      CB_CUDA(c, cudaMemcpyAsync(c->coorxy + c->plane * q, X[q], sizeof(double) * c->plane, cudaMemcpyDeviceToDevice,
+                                 c->stream));
   // scrub buffer 2 (coordinates) so later ghost reads see zeros until written
   for (int q = 0; q < 3; q++) CB_CUDA(c, cudaMemsetAsync(X[q], 0, sizeof(double) * c->plane, c->stream));
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1137,6 +1160,8 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
   if (e) return e;
   if (n < 0 || (n > 0 && (!list || !coor))) return CB_E_ARG;
   if (n > 0 && !b->surf) return fail(c, CB_E_STATE, "set the body's surface first");
+  if (n > 0 && (c->cfg.bctype[4] == 52 || c->cfg.bctype[4] == 47))
+    return fail(c, CB_E_UNSUPPORTED, "immersed bodies with the inflow codes 52 and 47 are not built");
   if (n > 0 && c->cfg.isothermal == 2)
     return fail(c, CB_E_UNSUPPORTED, "the characteristic isothermal IB wall (isothermal 2) is not built");
   if (n > 0 && c->dc.calc_sigma)

@@ -156,6 +156,10 @@ static __global__ void bc_combine_kernel(const DevCfg c, DevFields F, int istage
   }
 }
 
+// user->ti of the step about to run: the time loop advances it before
+// each step (main.c:887-974); the k-lo inflow code 47 reads it on the device
+static __global__ void step_index_advance_kernel(int *ti) { *ti += 1; }
+
 __device__ __forceinline__ double lp_at(const DevCfg &c, const DevFields &F, long long n) {
   if (F.pin) return F.pin[n];  // the pressure carried in lP
   const double r = F.q[0][n];
@@ -266,6 +270,55 @@ static __global__ void bc_face_kernel(const DevCfg c, DevFields F, int dir, doub
         q[0][n] = 0.445; q[3][n] = 0.311; q[4][n] = 8.928;
       } else if (bc[4] == 10) {
         q[0][n] = 1.; q[1][n] = 0.; q[2][n] = 0.; q[3][n] = 1.; q[4][n] = 1. / 0.4 + 0.5;
+      } else if (bc[4] == 52) {
+        // characteristic inlet imposing w = cos^2(pi/2 (y - 1)) (rhs.c:854-874),
+        // with FormBCS's own truncated pi (rhs.c:488)
+        const double pi = 3.14159265;
+        const double *const *lq = F.q;
+        const long long n1 = n + sk, n2 = n + 2 * sk;
+        const double yy = F.cy[n];
+        const double AA = cos(pi / 2 * (yy - 1.)) * cos(pi / 2 * (yy - 1.));
+        const double lp1 = lp_at(c, F, n1), lp2 = lp_at(c, F, n2);
+        const double a_sound = sqrt(g * lp1 / lq[0][n1]);
+        const double Lam0 = lq[3][n1] / lq[0][n1] - a_sound;
+        const double L0 = Lam0 * F.aj[n1] * F.met[2][2][n1] * ((lp2 - lp1) - lq[0][n1] * a_sound * (lq[3][n1] / lq[0][n1] - AA));
+        const double L1 = (g - 1.) * L0, L4 = L0;
+        const double d0 = 1. / (a_sound * a_sound) * (L1 + 0.5 * (L4 + L0));
+        q[0][n] = F.qold[0][n] - c.dt * alfa * d0;
+        const double lpn = q[0][n] / (g * Ma * Ma);
+        q[3][n] = q[0][n] * AA;
+        q[1][n] = 0.;
+        q[2][n] = 0.;
+        q[4][n] = 0.5 * q[3][n] * q[3][n] / q[0][n] + lpn / (g - 1);
+      } else if (bc[4] == 47) {
+        // power-law inflow with travelling perturbations in x and time
+        // (rhs.c:904-950); ti: the running step's index
+        const double pi = 3.141592;
+        const double c1 = 0.03, c2 = -0.0032, c3 = 0.02, c4 = -0.01, yp1 = 1.0, yp2 = 1.5, yp3 = 2.0;
+        const double w0 = 0.1, w1 = 0.25, w2 = 0.125, w3 = 0.0625;
+        const double phi1 = 0.0, phi2 = 0.1, phi3 = 0.15, b0 = 0.5 * pi, b1 = 0.75 * pi, b2 = 0.5 * pi, b3 = 0.25 * pi;
+        const double yy = F.cy[n], xx = F.cx[n];
+        const double yplus = yy * 0.065 * c.ren;
+        const int ti = *F.ti;
+        if (yy < 8.0) {
+          q[3][n] = pow(yy / 8.0, 0.1428);
+        } else {
+          q[3][n] = 1.0;
+          q[1][n] = 0.0;
+        }
+        if (yy < 8.0) {
+          q[3][n] += c1 * yplus * exp(-yplus / 12.5) * sin(w0 * ti * c.dt) * cos(b0 * xx);
+          q[2][n] = c2 * yplus * yplus * exp(-yplus * yplus / 12.5 / 12.5) * sin(w0 * ti * c.dt) * cos(b0 * xx);
+        } else if (yy >= 8.0) {
+          q[3][n] += c3 * yy / yp1 * exp(-yy / yp1) * sin(w1 * ti * c.dt) * cos(b1 * xx + phi1) +
+                     c3 * yy / yp2 * exp(-yy / yp2) * sin(w2 * ti * c.dt) * cos(b2 * xx + phi2) +
+                     c3 * yy / yp3 * exp(-yy / yp3) * sin(w3 * ti * c.dt) * cos(b3 * xx + phi3);
+          q[2][n] = c4 * yy * yy / yp1 / yp1 * exp(-yy * yy / yp1 / yp1) * sin(w1 * ti * c.dt) * cos(b1 * xx + phi1) +
+                    c4 * yy * yy / yp2 / yp2 * exp(-yy * yy / yp2 / yp2) * sin(w2 * ti * c.dt) * cos(b2 * xx + phi2) +
+                    c4 * yy * yy / yp3 / yp3 * exp(-yy * yy / yp3 / yp3) * sin(w3 * ti * c.dt) * cos(b3 * xx + phi3);
+        }
+        q[0][n] = 1.0;
+        q[4][n] = 0.5 * q[3][n] * q[3][n] + 1. / (Ma * Ma * g * (g - 1.));
       }
       n = gidx(c, a, j, c.mz - 1);
       const long long m1 = n - sk, m2 = n - 2 * sk;

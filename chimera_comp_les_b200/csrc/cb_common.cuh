@@ -87,6 +87,10 @@ struct DevFields {
   // after an immersed step, whose FormBCS(user, 0) is followed by no
   // EqOfState; the FP64 stage kernel and FormBCS read it); nullptr: EqOfState of q
   const double *pin;
+  // node coordinates x, y (the k-lo inflow codes 52 and 47 read them) and the
+  // step index user->ti of the running step (code 47), or nullptr
+  const double *cx, *cy;
+  const int *ti;
 };
 
 // 8-byte asynchronous global -> shared copy (valid false: zero-fill, nothing read)

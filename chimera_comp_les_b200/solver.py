@@ -237,6 +237,11 @@ class Block:
         self._check(self.lib.cb_get_nut(self._ctx, dptr(out)))
         return out
 
+    def set_time_index(self, ti: int) -> None:
+        """user->ti of the last completed step (the next RungeKutta step is
+        ti + 1); read by the k-lo inflow code 47 (cb_set_time_index)."""
+        self._check(self.lib.cb_set_time_index(self._ctx, int(ti)))
+
     def RungeKutta(self, nsteps: int = 1, sync: bool = True):
         self._check(self.lib.cb_rk_step(self._ctx, int(nsteps)))
         if sync:

@@ -51,7 +51,9 @@ extern "C" {
  * path; names in the comments are the reference's command-line flags. */
 typedef struct {
   int mx, my, mz;       /* -im/-jm/-km (DMDA node counts) */
-  int bctype[6];        /* bcs.dat: i-lo,i-hi,j-lo,j-hi,k-lo,k-hi; 7 = periodic */
+  int bctype[6];        /* bcs.dat: i-lo,i-hi,j-lo,j-hi,k-lo,k-hi; 7 = periodic; the face codes of
+                           FormBCS (rhs.c:477-1106): i 3, 51; j 3, 10, 1; k-lo 3, 52, 55, 44, 45, 51,
+                           10, 47; k-hi 3, 44, 45, 49, 51, 10, 8 */
   int les;              /* -les     : 0 off, 1 constant Smagorinsky, 2 (and every other value but 3
                            and 10) dynamic Smagorinsky with local averaging, 3 dynamic node by
                            node, 10 the LES terms without a model (nu_t stays 0); the dynamic
@@ -261,6 +263,12 @@ int cb_launches_per_step(const cb_ctx *ctx);
 
 const char *cb_last_error(const cb_ctx *ctx);
 int cb_abi_version(void);
+
+/* Index user->ti of the last completed time step (0 after cb_create): the
+ * next cb_rk_step runs step ti + 1, as the time loop of main.c:887-974 and
+ * RestartApplication with tistart = ti (main.c:620) do.  Only the k-lo inflow
+ * code 47 (rhs.c:904-950) reads it. */
+int cb_set_time_index(cb_ctx *ctx, int ti);
 
 /* Arithmetic-pipe peaks of GPU `device` in TFLOP/s (2 flops per fused
  * multiply-add), measured by a dependent-FMA kernel over every SM: the

@@ -85,6 +85,7 @@ class Config:
     tref: float = 273.15    # -Tref: its reference temperature (rhs.c:1410)
     abc: int = 0            # -ABC: absorbing layer of the shock sensor above plane k (rhs.c:3311)
     weno_order: int = 3     # 5: WENO5-JS (Jiang & Shu 1996) where its stencil fits; no reference counterpart
+    ti0: int = 1            # user->ti of the first step (the k-lo inflow code 47 reads it)
 
     def ref_options(self) -> str:
         o = [
@@ -129,13 +130,15 @@ class _CCfg(C.Structure):
         ("flux", C.c_int), ("max_cs", C.c_double), ("twall", C.c_double), ("twod", C.c_int),
         ("i_homo_filter", C.c_int), ("j_homo_filter", C.c_int), ("k_homo_filter", C.c_int),
         ("testfilter_ik", C.c_int), ("visT", C.c_int), ("tref", C.c_double), ("abc", C.c_int),
-        ("weno_order", C.c_int),
+        ("weno_order", C.c_int), ("coor_x", C.c_void_p), ("coor_y", C.c_void_p), ("ti0", C.c_int),
     ]
 
 
 def _ccfg(cfg: Config) -> _CCfg:
     c = _CCfg()
     for f, _ in _CCfg._fields_:
+        if f in ("coor_x", "coor_y"):
+            continue  # set by Oracle.set_coordinates
         if f == "bctype":
             c.bctype = (C.c_int * 6)(*cfg.bctype)
         elif f == "twod":
@@ -242,6 +245,13 @@ class Oracle:
         L.cbo_dynamic_smagorinsky.restype = C.c_int
         L.cbo_eddy_viscosity_dyn.argtypes = [C.c_void_p, PP, PP, PP, PP, PP, D, D, D, D]
         self._cp = C.byref(self.c)
+
+    def set_coordinates(self, coor_pad: np.ndarray) -> None:
+        """Node coordinates (3, padded) for the boundary codes that read them
+        (k-lo inflow 52 and 47)."""
+        self._coor = np.ascontiguousarray(coor_pad, dtype=np.float64)
+        self.c.coor_x = self._coor[0].ctypes.data
+        self.c.coor_y = self._coor[1].ctypes.data
 
     def count_reset(self) -> None:
         self.lib.cbo_count_reset()

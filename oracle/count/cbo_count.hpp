@@ -86,6 +86,8 @@ inline cdbl pow(cdbl a, double b) { return pow(a, cdbl(b)); }
 inline cdbl pow(double a, cdbl b) { return pow(cdbl(a), b); }
 inline cdbl tanh(cdbl a) { cbo_cnt[CNT_POW]++; return cdbl(std::tanh(a.v)); }
 inline cdbl exp(cdbl a) { cbo_cnt[CNT_POW]++; return cdbl(std::exp(a.v)); }
+inline cdbl sin(cdbl a) { cbo_cnt[CNT_POW]++; return cdbl(std::sin(a.v)); }
+inline cdbl cos(cdbl a) { cbo_cnt[CNT_POW]++; return cdbl(std::cos(a.v)); }
 inline cdbl log(cdbl a) { cbo_cnt[CNT_POW]++; return cdbl(std::log(a.v)); }
 inline cdbl fmin(cdbl a, cdbl b) { cbo_cnt[CNT_ABS]++; return cdbl(std::fmin(a.v, b.v)); }
 inline cdbl fmax(cdbl a, cdbl b) { cbo_cnt[CNT_ABS]++; return cdbl(std::fmax(a.v, b.v)); }
@@ -95,5 +97,8 @@ using std::sqrt;
 using std::fabs;
 using std::pow;
 using std::tanh;
+using std::sin;
+using std::cos;
+using std::exp;
 
 #define double cdbl

@@ -1033,23 +1033,23 @@ int cbo_bc_periodic(const cbo_config *c, const double *const qin[5], double *con
 /* the stale ghosted stage input (its pressure lp from the EOS); qold: the   */
 /* step's initial state.  Face order i, j, k, then the periodic copies, then */
 /* the wrap of periodic directions (DMGlobalToLocal).  Codes: i 3, 51; j 3,   */
-/* 10, 1 (isothermal 0/1); k-lo 3, 55, 44, 45, 51, 10; k-hi 3, 44, 45, 49,   */
-/* 51, 10, 8; 7 periodic; any other code leaves the face as the RK update    */
-/* left it, as in the reference.  Not restated (returns 5): k-lo 52 and 47   */
-/* (they read the coordinates and the step index) and the characteristic    */
-/* isothermal wall (isothermal 2 with a j wall).                             */
+/* 10, 1 (isothermal 0/1/2); k-lo 3, 52, 55, 44, 45, 51, 10, 47; k-hi 3,    */
+/* 44, 45, 49, 51, 10, 8; 7 periodic; any other code leaves the face as the  */
+/* RK update left it, as in the reference.  52 and 47 read the node          */
+/* coordinates (c->coor_x/coor_y; 5 is returned without them) and 47 the     */
+/* step index ti.                                                            */
 /* ------------------------------------------------------------------------ */
 /* lp_in: the local pressure lP (NULL: EqOfState of lq); p (may be NULL): the
  * global P, which receives the periodic copies and then the ghost wrap. */
 static int nvert_ok(const double *nv, ptrdiff_t n) { return !nv || nv[n] < 1.5; }
 
-static int formbcs_impl(const cbo_config *c, double alfa, const double *const lq[5], const double *lp_in,
+static int formbcs_impl(const cbo_config *c, int ti, double alfa, const double *const lq[5], const double *lp_in,
                         const double *const qold[5], const double *const eta[3], const double *const zet[3],
                         const double *aj, const double *nvert_in, double *const q[5], double *p) {
   geom G = mkgeom(c);
   const int mx = G.m[0], my = G.m[1], mz = G.m[2];
   const int *bc = c->bctype;
-  if (bc[4] == 52 || bc[4] == 47) return 5;
+  if ((bc[4] == 52 || bc[4] == 47) && (!c->coor_x || !c->coor_y)) return 5;
   if ((bc[0] == 7) != (bc[1] == 7) || (bc[2] == 7) != (bc[3] == 7) || (bc[4] == 7) != (bc[5] == 7)) return 5;
   const ptrdiff_t si = G.s[0], sj = G.s[1], sk = G.s[2];
   const double g = c->gamma, Ma = c->ma;
@@ -1157,6 +1157,54 @@ static int formbcs_impl(const cbo_config *c, double alfa, const double *const lq
         RO(n) = 0.445; RW(n) = 0.311; RE(n) = 8.928;
       } else if (bc[4] == 10) {
         RO(n) = 1.; RU(n) = 0.; RV(n) = 0.; RW(n) = 1.; RE(n) = 1. / 0.4 + 0.5;
+      } else if (bc[4] == 52) {
+        /* characteristic inlet imposing w = cos^2(pi/2 (y - 1)) (rhs.c:854-874);
+         * pi is FormBCS's own truncated value (rhs.c:488) */
+        const double pi = 3.14159265;
+        const ptrdiff_t n1 = n + sk, n2 = n + 2 * sk;
+        const double yy = c->coor_y[n];
+        const double AA = cos(pi / 2 * (yy - 1.)) * cos(pi / 2 * (yy - 1.));
+        const double a_sound = sqrt(g * lp[n1] / lq[0][n1]);
+        const double Lam0 = lq[3][n1] / lq[0][n1] - a_sound;
+        const double L0 = Lam0 * aj[n1] * zet[2][n1] * ((lp[n2] - lp[n1]) - lq[0][n1] * a_sound * (lq[3][n1] / lq[0][n1] - AA));
+        const double L1 = (g - 1.) * L0, L4 = L0;
+        const double d0 = 1. / (a_sound * a_sound) * (L1 + 0.5 * (L4 + L0));
+        RO(n) = qold[0][n] - c->dt * alfa * d0;
+        lp[n] = RO(n) / (g * Ma * Ma);
+        RW(n) = RO(n) * AA;
+        RU(n) = 0.;
+        RV(n) = 0.;
+        RE(n) = 0.5 * RW(n) * RW(n) / RO(n) + lp[n] / (g - 1);
+      } else if (bc[4] == 47) {
+        /* power-law inflow with travelling perturbations in x and time
+         * (rhs.c:904-950): below y = 8 w = (y/8)^0.1428 plus a near-wall
+         * mode (u is left as the RK update left it), above w = 1, u = 0 plus
+         * three modes; rho = 1 */
+        const double pi = 3.141592;
+        const double c1 = 0.03, c2 = -0.0032, c3 = 0.02, c4 = -0.01, yp1 = 1.0, yp2 = 1.5, yp3 = 2.0;
+        const double w0 = 0.1, w1 = 0.25, w2 = 0.125, w3 = 0.0625;
+        const double phi1 = 0.0, phi2 = 0.1, phi3 = 0.15, b0 = 0.5 * pi, b1 = 0.75 * pi, b2 = 0.5 * pi, b3 = 0.25 * pi;
+        const double yy = c->coor_y[n], xx = c->coor_x[n];
+        const double yplus = yy * 0.065 * c->ren;
+        if (yy < 8.0) {
+          RW(n) = pow(yy / 8.0, 0.1428);
+        } else {
+          RW(n) = 1.0;
+          RU(n) = 0.0;
+        }
+        if (yy < 8.0) {
+          RW(n) += c1 * yplus * exp(-yplus / 12.5) * sin(w0 * ti * c->dt) * cos(b0 * xx);
+          RV(n) = c2 * yplus * yplus * exp(-yplus * yplus / 12.5 / 12.5) * sin(w0 * ti * c->dt) * cos(b0 * xx);
+        } else if (yy >= 8.0) {
+          RW(n) += c3 * yy / yp1 * exp(-yy / yp1) * sin(w1 * ti * c->dt) * cos(b1 * xx + phi1) +
+                   c3 * yy / yp2 * exp(-yy / yp2) * sin(w2 * ti * c->dt) * cos(b2 * xx + phi2) +
+                   c3 * yy / yp3 * exp(-yy / yp3) * sin(w3 * ti * c->dt) * cos(b3 * xx + phi3);
+          RV(n) = c4 * yy * yy / yp1 / yp1 * exp(-yy * yy / yp1 / yp1) * sin(w1 * ti * c->dt) * cos(b1 * xx + phi1) +
+                  c4 * yy * yy / yp2 / yp2 * exp(-yy * yy / yp2 / yp2) * sin(w2 * ti * c->dt) * cos(b2 * xx + phi2) +
+                  c4 * yy * yy / yp3 / yp3 * exp(-yy * yy / yp3 / yp3) * sin(w3 * ti * c->dt) * cos(b3 * xx + phi3);
+        }
+        RO(n) = 1.0;
+        RE(n) = 0.5 * RW(n) * RW(n) + 1. / (Ma * Ma * g * (g - 1.));
       }
       n = IX(&G, i, j, mz - 1);
       const ptrdiff_t m1 = n - sk, m2 = n - 2 * sk;
@@ -1286,13 +1334,13 @@ static int formbcs_impl(const cbo_config *c, double alfa, const double *const lq
 int cbo_formbcs(const cbo_config *c, double alfa, const double *const lq[5], const double *const qold[5],
                 const double *const eta[3], const double *const zet[3], const double *aj, const double *nvert,
                 double *const q[5]) {
-  return formbcs_impl(c, alfa, lq, NULL, qold, eta, zet, aj, nvert, q, NULL);
+  return formbcs_impl(c, c->ti0, alfa, lq, NULL, qold, eta, zet, aj, nvert, q, NULL);
 }
 
 int cbo_formbcs_lp(const cbo_config *c, double alfa, const double *const lq[5], const double *lp,
                    const double *const qold[5], const double *const eta[3], const double *const zet[3],
                    const double *aj, const double *nvert, double *const q[5], double *p) {
-  return formbcs_impl(c, alfa, lq, lp, qold, eta, zet, aj, nvert, q, p);
+  return formbcs_impl(c, c->ti0, alfa, lq, lp, qold, eta, zet, aj, nvert, q, p);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1330,7 +1378,8 @@ int cbo_steps(const cbo_config *c, int nsteps, double *const q[5], double *const
       {
         double al[3] = {1., 1 / 4., 2 / 3.};
         if (c->fluxorder < 3) al[1] = 1 / 2.;
-        err = cbo_formbcs(c, al[s], (const double *const *)q, (const double *const *)qold, eta, zet, aj, nvert, qn);
+        err = formbcs_impl(c, c->ti0 + step, al[s], (const double *const *)q, NULL, (const double *const *)qold, eta, zet,
+                           aj, nvert, qn, NULL);
       }
       for (int a = 0; a < 5; a++) memcpy(q[a], qn[a], G.n * sizeof(double));
     }
@@ -1468,7 +1517,7 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
         *have_uc = 1;
       }
       cbo_rk_combine(c, s, (const double *const *)qold, (const double *const *)q, (const double *const *)rhs, qn);
-      err = formbcs_impl(c, al[s], (const double *const *)q, lps, (const double *const *)qold, eta, zet, aj, nvert, qn,
+      err = formbcs_impl(c, c->ti0 + step, al[s], (const double *const *)q, lps, (const double *const *)qold, eta, zet, aj, nvert, qn,
                          NULL);
       for (int a = 0; a < 5; a++) memcpy(q[a], qn[a], G.n * sizeof(double));
     }
@@ -1479,7 +1528,7 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
     if (err) break;
     for (int a = 0; a < 5; a++) memcpy(lq[a], q[a], G.n * sizeof(double));
     memcpy(lpc, lp, G.n * sizeof(double));
-    err = formbcs_impl(c, 0.0, (const double *const *)lq, lpc, (const double *const *)qold, eta, zet, aj, nvert, q,
+    err = formbcs_impl(c, c->ti0 + step, 0.0, (const double *const *)lq, lpc, (const double *const *)qold, eta, zet, aj, nvert, q,
                        lp);
     *lp_valid = 1;
     for (int a = 0; a < 5; a++) memcpy(qold[a], q[a], G.n * sizeof(double));

@@ -51,6 +51,10 @@ typedef struct {
   int abc;                 /* -ABC: sensor weights 0 (then clamped) above plane k = ABC (rhs.c:3311, 3341-3368) */
   int weno_order;          /* 3: the reference's WENO3 (fluxorder 3); 5: WENO5-JS (Jiang & Shu 1996) where its
                               six-node stencil fits (no reference counterpart) */
+  const double *coor_x;    /* node coordinates x and y (padded planes) for the k-lo inflow codes 52 and 47, */
+  const double *coor_y;    /* which read them (rhs.c:854-874, 904-950); may be NULL otherwise */
+  int ti0;                 /* user->ti of the first time step cbo_steps takes (the driver's first step is 1);
+                              code 47 reads it */
 } cbo_config;
 
 /* WENO5-JS reconstruction at the face x_{i+1/2} from v_{i-2..i+2}, biased to

@@ -30,6 +30,8 @@ def load_golden(name):
 def oracle_run(cfg, coords, q, nvert, steps=0):
     """Restatement: metrics, (nut), rhs at istage 0, Q after `steps` steps."""
     ora = O.Oracle(cfg)
+    if cfg.bctype[4] in (52, 47):  # the inflow codes read the node coordinates
+        ora.set_coordinates(O.to_padded(cfg, coords))
     met = ora.metrics(O.to_padded(cfg, coords))
     nvp = ora.fill_ghosts(O.to_padded(cfg, nvert))
     st = ora.initial_state(q)

@@ -76,3 +76,33 @@ def test_characteristic_isothermal_walls_match_oracle(bct, les, twoD, twall):
             b.SetInitialCondition(q)
             b.RungeKutta(3)
             assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= tol, prec
+
+
+INFLOW = [(7, 7, 3, 3, 52, 44), (7, 7, 3, 3, 47, 45), (3, 3, 1, 1, 52, 49), (7, 7, 7, 7, 47, 8)]
+
+
+@pytest.mark.parametrize("bct", INFLOW)
+@pytest.mark.parametrize("les,ti0", [(0, 1), (1, 6)])
+def test_inflow_codes_52_47_match_oracle(bct, les, ti0):
+    """The k-lo inflow codes that read the node coordinates: the
+    characteristic cos^2 inlet 52 (rhs.c:854-874) and the power-law inlet 47
+    with perturbations travelling in x and time (rhs.c:904-950), whose step
+    index comes from cb_set_time_index (a restart at step ti0 - 1)."""
+    n = (35, 17, 23)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.04)
+    coords[..., 1] = 1.5 * coords[..., 1] + 1.0  # y on both sides of 47's y = 8
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, bctype=bct, les=les, inviscid=0, fluxorder=3,
+                   s_x=0.4 if les else 1.0, s_y=0.7, s_z=0.9, ren=250., ma=0.3, pr=0.71, dt=0.002, ti0=ti0)
+    q = W.random_smooth_state(shape, seed=19, periodic=False)
+    nv = np.zeros(shape)
+    ref = oracle_run(cfg, coords, q, nv, steps=3)
+    assert np.isfinite(ref["q_steps"]).all()
+    for prec, tol in (("fp64", RTOL_L2), ("mixed", 1e-5)):
+        with gpu_block(cfg, precision=prec) as b:
+            b.FormMetrics(coords)
+            b.set_nvert(nv)
+            b.SetInitialCondition(q)
+            b.set_time_index(ti0 - 1)
+            b.RungeKutta(3)
+            assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= tol, prec

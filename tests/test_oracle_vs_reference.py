@@ -341,3 +341,40 @@ def test_twoD1_bitexact_vs_reference(name, kw, mask):
     ref.set_state(q)
     ref.steps(3)
     assert np.array_equal(got["q_steps"], ref.Q())
+
+
+INFLOW_CASES = [(7, 7, 3, 3, 52, 44), (7, 7, 3, 3, 47, 45), (3, 3, 1, 1, 52, 49), (7, 7, 7, 7, 47, 8)]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference sources not present")
+@pytest.mark.parametrize("bct", INFLOW_CASES)
+@pytest.mark.parametrize("les", [0, 1])
+def test_inflow_codes_52_47_bitexact_vs_reference(bct, les):
+    """The k-lo inflow codes that read the node coordinates: the
+    characteristic cos^2 inlet 52 (rhs.c:854-874) and the power-law inlet
+    with travelling perturbations 47 (rhs.c:904-950, which also reads the
+    step index): three RK steps, y spanning both sides of 47's y = 8."""
+    n = (12, 13, 11)
+    coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
+    coords[..., 1] = 1.5 * coords[..., 1] + 1.0
+    shape = coords.shape[:3]
+    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, bctype=bct, les=les, inviscid=0, fluxorder=3,
+                   s_x=0.4 if les else 1.0, s_y=0.7, s_z=0.9, ren=250., ma=0.3, pr=0.71, dt=0.002)
+    q = W.random_smooth_state(shape, seed=19, periodic=False)
+    nv = np.zeros(shape)
+    ref = O.RefOracle(cfg, coords)
+    ref.set_nvert(nv)
+    ref.set_state(q)
+    ref.steps(3)
+    ora = O.Oracle(cfg)
+    cp = O.to_padded(cfg, coords)
+    ora.set_coordinates(cp)
+    met = ora.metrics(cp)
+    nvp = ora.fill_ghosts(O.to_padded(cfg, nv))
+    st = ora.initial_state(q)
+    ora.steps(3, st, met, nvp)
+    got = O.from_padded(st["q"])
+    assert np.isfinite(ref.Q()).all()
+    assert np.array_equal(got, ref.Q())
+    # the inflow plane carries the imposed profile
+    assert not np.array_equal(got[0], q[0])
