@@ -99,6 +99,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.cb_launches_per_step.restype = C.c_int
     lib.cb_last_error.argtypes = [P]
     lib.cb_last_error.restype = C.c_char_p
+    for name, args in [("cb_upload_state_async", [P, P]), ("cb_download_state_async", [P, P]),
+                       ("cb_join_transfers", [P])]:
+        getattr(lib, name).argtypes = args
+        getattr(lib, name).restype = C.c_int
     lib.cb_set_time_index.argtypes = [P, C.c_int]
     lib.cb_set_time_index.restype = C.c_int
     lib.cb_pipe_peaks.argtypes = [C.c_int, D, D]

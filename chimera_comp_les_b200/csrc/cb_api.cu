@@ -81,6 +81,12 @@ struct cb_ctx {
   double dyn_tf_mult = 2.0;  // test-filter width over the filter width (les.c:598-601)
   bool have_refs = false;
   double *staging = nullptr;  // AoS upload/download buffer (5 doubles per node)
+  // asynchronous host transfers (cb_upload_state_async / cb_download_state_async):
+  // copy streams and two staging buffers per direction, allocated on first use
+  cudaStream_t up_stream = nullptr, down_stream = nullptr;
+  double *stg_in[2] = {}, *stg_out[2] = {};
+  cudaEvent_t ev_in_copied[2] = {}, ev_in_free[2] = {}, ev_out_ready[2] = {}, ev_out_done[2] = {};
+  int in_slot = 0, out_slot = 0;
   double **ptab = nullptr;    // device pointer tables
   unsigned *status = nullptr;
   bool fully_periodic = true;  // every face bctype 7: one fused periodic BC kernel
@@ -687,6 +693,16 @@ void cb_destroy(cb_ctx *c) {
   if (c->rhsb[0]) cudaFree(c->rhsb[0]);
   if (c->arena) cudaFree(c->arena);
   if (c->staging) cudaFree(c->staging);
+  if (c->up_stream) cudaStreamSynchronize(c->up_stream);
+  if (c->down_stream) cudaStreamSynchronize(c->down_stream);
+  for (int i = 0; i < 2; i++) {
+    if (c->stg_in[i]) cudaFree(c->stg_in[i]);
+    if (c->stg_out[i]) cudaFree(c->stg_out[i]);
+    for (cudaEvent_t e : {c->ev_in_copied[i], c->ev_in_free[i], c->ev_out_ready[i], c->ev_out_done[i]})
+      if (e) cudaEventDestroy(e);
+  }
+  if (c->up_stream) cudaStreamDestroy(c->up_stream);
+  if (c->down_stream) cudaStreamDestroy(c->down_stream);
   if (c->arena_mixed) cudaFree(c->arena_mixed);
   if (c->ptab4) cudaFree(c->ptab4);
   if (c->sig_arena) cudaFree(c->sig_arena);
@@ -865,6 +881,77 @@ int cb_upload_state(cb_ctx *c, const double *q) {
   if (e) return e;
   CB_CUDA(c, cudaMemsetAsync(c->nut, 0, sizeof(double) * c->plane, c->stream));
   c->have_state = true;
+  return CB_OK;
+}
+
+// Copy streams, staging buffers and events of the asynchronous transfers
+// (once per context).
+static int xfer_init(cb_ctx *c) {
+  if (c->up_stream) return CB_OK;
+  const size_t bytes = sizeof(double) * 5 * (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  CB_CUDA(c, cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking));
+  CB_CUDA(c, cudaStreamCreateWithFlags(&c->down_stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; i++) {
+    CB_CUDA(c, cudaMalloc(&c->stg_in[i], bytes));
+    CB_CUDA(c, cudaMalloc(&c->stg_out[i], bytes));
+    for (cudaEvent_t *e : {&c->ev_in_copied[i], &c->ev_in_free[i], &c->ev_out_ready[i], &c->ev_out_done[i]})
+      CB_CUDA(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
+  return CB_OK;
+}
+
+int cb_upload_state_async(cb_ctx *c, const double *q) {
+  if (!c || !q) return CB_E_ARG;
+  int e = xfer_init(c);
+  if (e) return e;
+  if (c->cfg.precision == CB_MIXED && !c->have_refs) set_reference_state(c, q);
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  const int i = c->in_slot;
+  c->in_slot ^= 1;
+  // the copy into staging buffer i waits until its previous contents were unpacked
+  CB_CUDA(c, cudaStreamWaitEvent(c->up_stream, c->ev_in_free[i], 0));
+  CB_CUDA(c, cudaMemcpyAsync(c->stg_in[i], q, sizeof(double) * 5 * nn, cudaMemcpyHostToDevice, c->up_stream));
+  CB_CUDA(c, cudaEventRecord(c->ev_in_copied[i], c->up_stream));
+  // the state update itself is ordered on the compute stream, as cb_upload_state's
+  CB_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_in_copied[i], 0));
+  c->cur = 0;
+  c->uc = -1;
+  c->p_carry = false;
+  unpack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, c->stg_in[i], 5, c->ptab + PT_Q0);
+  CB_CUDA(c, cudaGetLastError());
+  const long long all = (long long)(c->dc.mx + 4) * (c->dc.my + 4) * (c->dc.mz + 4);
+  ghost_fill_kernel<<<grid_for(c, all), 256, 0, c->stream>>>(c->dc, c->ptab + PT_Q0, 5);
+  CB_CUDA(c, cudaGetLastError());
+  CB_CUDA(c, cudaEventRecord(c->ev_in_free[i], c->stream));
+  CB_CUDA(c, cudaMemsetAsync(c->nut, 0, sizeof(double) * c->plane, c->stream));
+  c->have_state = true;
+  return CB_OK;
+}
+
+int cb_download_state_async(cb_ctx *c, double *q) {
+  if (!c || !q) return CB_E_ARG;
+  if (!c->have_state) return fail(c, CB_E_STATE, "no state uploaded");
+  int e = xfer_init(c);
+  if (e) return e;
+  const size_t nn = (size_t)c->cfg.mx * c->cfg.my * c->cfg.mz;
+  const int o = c->out_slot;
+  c->out_slot ^= 1;
+  // the pack into staging buffer o waits until its previous copy to the host finished
+  CB_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_out_done[o], 0));
+  pack_kernel<<<grid_for(c, (long long)nn), 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), 5,
+                                                                   c->stg_out[o]);
+  CB_CUDA(c, cudaGetLastError());
+  CB_CUDA(c, cudaEventRecord(c->ev_out_ready[o], c->stream));
+  CB_CUDA(c, cudaStreamWaitEvent(c->down_stream, c->ev_out_ready[o], 0));
+  CB_CUDA(c, cudaMemcpyAsync(q, c->stg_out[o], sizeof(double) * 5 * nn, cudaMemcpyDeviceToHost, c->down_stream));
+  CB_CUDA(c, cudaEventRecord(c->ev_out_done[o], c->down_stream));
+  return CB_OK;
+}
+
+int cb_join_transfers(cb_ctx *c) {
+  if (!c) return CB_E_ARG;
+  if (!c->up_stream) return CB_OK;
+  for (int i = 0; i < 2; i++) CB_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_out_done[i], 0));
   return CB_OK;
 }
 

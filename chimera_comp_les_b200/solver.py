@@ -237,6 +237,23 @@ class Block:
         self._check(self.lib.cb_get_nut(self._ctx, dptr(out)))
         return out
 
+    def upload_async(self, q: np.ndarray) -> None:
+        """cb_upload_state_async: Q (natural AoS, ideally pinned host memory)
+        as the new state; returns after enqueueing.  Keep q unchanged until
+        join_transfers() and sync()."""
+        assert q.dtype == np.float64 and q.flags.c_contiguous and q.size == 5 * self.nnodes
+        self._check(self.lib.cb_upload_state_async(self._ctx, q.ctypes.data))
+
+    def download_async(self, q_out: np.ndarray) -> None:
+        """cb_download_state_async: Q into q_out after the work enqueued so far;
+        returns after enqueueing (q_out is valid after join_transfers() and sync())."""
+        assert q_out.dtype == np.float64 and q_out.flags.c_contiguous and q_out.size == 5 * self.nnodes
+        self._check(self.lib.cb_download_state_async(self._ctx, q_out.ctypes.data))
+
+    def join_transfers(self) -> None:
+        """cb_join_transfers: later work on the context's stream follows every copy."""
+        self._check(self.lib.cb_join_transfers(self._ctx))
+
     def set_time_index(self, ti: int) -> None:
         """user->ti of the last completed step (the next RungeKutta step is
         ti + 1); read by the k-lo inflow code 47 (cb_set_time_index)."""

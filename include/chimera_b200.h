@@ -19,7 +19,8 @@
  *     not thread-safe (one context per host thread, as the reference runs one
  *     rank per process).
  *   - No function allocates device memory except cb_create, cb_rhs (first
- *     call: its output planes), cb_capture_graph (graph instantiation),
+ *     call: its output planes), the first asynchronous transfer call
+ *     (staging buffers), cb_capture_graph (graph instantiation),
  *     cb_ibm_set_surface and cb_ibm_set_list (immersed-body arrays) and,
  *     in the batched form, cb_batch_create, cb_batch_set_halo_map and
  *     cb_batch_autotune (item lists, maps, graphs).
@@ -141,6 +142,25 @@ int cb_upload_state(cb_ctx *ctx, const double *q);
 /* Copies Q (5 per node) and, if p != NULL, the EOS pressure (1 per node) back.
  * Replaces reading user->Q / user->P after RungeKutta. */
 int cb_download_state(cb_ctx *ctx, double *q, double *p);
+
+/* Streaming host transfers, for a host that hands every step its input state
+ * and takes every step's result (the reference's VecGetArray buffers, pinned
+ * for the copies to overlap).  cb_upload_state_async is cb_upload_state, and
+ * cb_download_state_async the Q part of cb_download_state, but each returns
+ * after enqueueing: the host-to-device copy runs on an upload copy stream and
+ * the device-to-host copy on a download copy stream, each through two staging
+ * buffers, so the download of one step's result, the upload of the next
+ * step's input and the steps themselves overlap.  The state update and the
+ * packing stay ordered on the context's stream with every other call.  The
+ * host may reuse an input buffer, and read an output buffer, only after
+ * cb_join_transfers and cb_sync.  The first call allocates the copy streams
+ * and four staging buffers (5 doubles per node each).  No counterpart in the
+ * reference (its state never leaves the host). */
+int cb_upload_state_async(cb_ctx *ctx, const double *q);
+int cb_download_state_async(cb_ctx *ctx, double *q);
+/* Orders the context's stream after every transfer enqueued so far (no host
+ * wait): work or events enqueued afterwards follow the last copy. */
+int cb_join_transfers(cb_ctx *ctx);
 
 /* formRHS(user, Rhs, istage) (rhs.c:4703) on the current state: writes Rhs,
  * 5 doubles per node, zero on boundary nodes.  In LES mode the current eddy

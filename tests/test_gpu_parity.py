@@ -166,9 +166,10 @@ def test_nonfinite_state_reports_status_not_fault():
 
 
 def test_unsupported_options_fail_loudly():
-    for bct, iso in [((7, 3, 7, 7, 7, 7), 0), ((7, 7, 7, 7, 52, 44), 0), ((7, 7, 7, 7, 47, 44), 0)]:
+    # a direction periodic on one face only; WENO5 without the WENO path (fluxorder 2)
+    for kw in (dict(bctype=(7, 3, 7, 7, 7, 7)), dict(fluxorder=2, weno_order=5), dict(weno_order=4)):
         with pytest.raises(ChimeraError):
-            gpu_block(O.Config(mx=12, my=12, mz=12, bctype=bct, isothermal=iso))
+            gpu_block(O.Config(mx=12, my=12, mz=12, **kw))
 
 
 def test_autotune_changes_launch_shape_not_results():
