@@ -52,6 +52,8 @@ B_ALG = {
     "mixed": 200,  # Q in/old/out 120, FP32 metrics 36, aj 8, nu_t 8, FP64 metric divergence 24, FP32 filter width 4
 }
 ACC_STEPS = 100
+# names the headline workload in the committed ncu traffic summaries
+WORKLOAD_ID = "tgv128-muscl-rusanov-sigma0-rk2"
 
 # -les 1 -fluxorder 2 -s_x 0 -s_y 0 -s_z 0: MUSCL-minmod + Rusanov, pure upwind
 CFG = dict(les=1, inviscid=0, fluxorder=2, eno_order=2, central=2, s_x=0.0, s_y=0.0, s_z=0.0,
@@ -163,7 +165,7 @@ def profile_traffic(precision):
         return None
     with open(p) as f:
         d = json.load(f)
-    if d.get("workload_id") != "tgv128-fluxorder3":
+    if d.get("workload_id") != WORKLOAD_ID:
         return None
     return d.get("dram_bytes_per_launch_scaled_to_bench")
 
@@ -388,6 +390,29 @@ def pipe_peaks(local):
             "source": "measured here by cb_pipe_peaks (dependent-FMA kernel on every SM, 2 flops per FMA)"}
 
 
+def hbm_copy_gbs(local, nbytes=1 << 31, reps=10):
+    """Device-to-device copy bandwidth of this GPU (read + write bytes / time):
+    a STREAM-style copy of a 2 GiB buffer, CUDA events around `reps` copies
+    after three warm-up copies."""
+    import torch
+    n = nbytes // 8
+    a = torch.ones(n, dtype=torch.float64, device=f"cuda:{local}")
+    b = torch.empty_like(a)
+    for _ in range(3):
+        b.copy_(a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        b.copy_(a)
+    e1.record()
+    torch.cuda.synchronize()
+    gbs = 2 * nbytes * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
+    del a, b
+    torch.cuda.empty_cache()
+    return gbs
+
+
 def compute_roofline(form, cfgkw, kernel_ms, interior, peaks):
     """Compute-side roofline of the stage kernel: operations per cell-update
     counted on the restatement (oracle/flops.py) x cell-updates per launch /
@@ -436,31 +461,41 @@ def _vs_oracle(n, coords, q0, nv, blocks, cfgkw):
     return out
 
 
-def run_config5(args, local, n=512):
-    """BASELINE config 5 at its largest size on one GPU: decaying compressible
-    isotropic turbulence on a periodic [0, 2*pi]^3 Cartesian box of n^3 unique
-    nodes (DMDA (n+2)^3), Passot-Pouquet spectrum k0 4, u_rms 1, Mt 0.4, seed
-    5, rho 1, uniform p; Roe flux with the WENO reconstruction built here,
-    pure upwind (-les 1 -s_x 0 -s_y 0 -s_z 0), Smagorinsky CS 0.17^2, SSP-RK3,
-    dt from CFL 0.4.  Per form: cell-updates/s, stage-kernel GB/s, then the
-    per-field mixed-vs-FP64 error after ACC_STEPS steps."""
-    import torch
-
-    from chimera_comp_les_b200 import diagnostics as D
+def config5_case(n):
+    """Config 5's inputs and options at n^3: coordinates, state, dt (CFL 0.4)
+    and the scheme (WENO5-JS + Roe, pure upwind, Smagorinsky CS 0.17^2,
+    SSP-RK3)."""
     from chimera_comp_les_b200 import workloads as W
-    torch.cuda.set_device(local)
     coords = W.periodic_grid(n, 2 * math.pi, amp=0.0)
     q0 = W.isotropic_turbulence(n, 5, k_peak=4.0, mach_t=0.4, spectrum="passot_pouquet", u_rms=1.0)
     r = q0[..., 0]
     c = np.sqrt(1.4 * 0.4 * (q0[..., 4] - 0.5 * (q0[..., 1] ** 2 + q0[..., 2] ** 2 + q0[..., 3] ** 2) / r) / r)
     lam = sum(float((np.abs(q0[..., 1 + a] / r) + c).max()) for a in range(3)) * n / (2 * math.pi)
-    del r, c
     dt = math.floor(0.4 / lam * 1e6) / 1e6
-    opts = dict(CFG, fluxorder=3, flux="roe", s_x=0.0, s_y=0.0, s_z=0.0, ren=10000.0, ma=0.4, cs_const=0.17 ** 2,
-                dt=dt)
+    opts = dict(CFG, fluxorder=3, weno_order=5, flux="roe", s_x=0.0, s_y=0.0, s_z=0.0, ren=10000.0, ma=0.4,
+                cs_const=0.17 ** 2, dt=dt)
+    return coords, q0, dt, opts
+
+
+CONFIG5_SCHEME = "WENO5-JS + Roe, pure upwind (sigma 0), Smagorinsky CS 0.17^2, SSP-RK3, dt from CFL 0.4"
+
+
+def run_config5(args, local, n=512):
+    """BASELINE config 5 at its largest size on one GPU: decaying compressible
+    isotropic turbulence on a periodic [0, 2*pi]^3 Cartesian box of n^3 unique
+    nodes (DMDA (n+2)^3), Passot-Pouquet spectrum k0 4, u_rms 1, Mt 0.4, seed
+    5, rho 1, uniform p; WENO5-JS reconstruction with the Roe flux, pure
+    upwind (-les 1 -s_x 0 -s_y 0 -s_z 0), Smagorinsky CS 0.17^2, SSP-RK3, dt
+    from CFL 0.4.  Per form: cell-updates/s, stage-kernel GB/s, then the
+    per-field mixed-vs-FP64 error after ACC_STEPS steps."""
+    import torch
+
+    from chimera_comp_les_b200 import diagnostics as D
+    torch.cuda.set_device(local)
+    coords, q0, dt, opts = config5_case(n)
     nv = np.zeros(coords.shape[:3])
     out = {"workload": f"decaying isotropic turbulence {n}^3 (DMDA {n + 2}^3), Passot-Pouquet k0 4, u_rms 1, Mt 0.4, "
-                       "seed 5; WENO3 + Roe, pure upwind (sigma 0), Smagorinsky CS 0.17^2, SSP-RK3, dt from CFL 0.4",
+                       f"seed 5; {CONFIG5_SCHEME}",
            "grid": [n + 2] * 3, "dt": dt, "interior_nodes": n ** 3}
     final = {}
     for prec in ("fp64", "mixed"):
@@ -589,6 +624,7 @@ def run_ours(args, ws, rank, local):
 
     if rank == 0:
         peaks = pipe_peaks(local)
+        copy_gbs = hbm_copy_gbs(local)
         comp = compute_roofline(args.precision, CFG, head["kernel_avg_ms"], n ** 3, peaks) if peaks else None
         other_comp = (compute_roofline("fp64" if args.precision == "mixed" else "mixed", CFG,
                                        forms["fp64" if args.precision == "mixed" else "mixed"]["kernel_avg_ms"],
@@ -610,6 +646,8 @@ def run_ours(args, ws, rank, local):
                          "kernel": f"stage_kernel ({args.precision} form: fused RHS + RK combine)",
                          "kernel_avg_ms": head["kernel_avg_ms"], "bytes_per_cell": B_ALG[args.precision],
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "copy_gbs_measured_here": copy_gbs,
+                         "frac_of_copy_measured_here": head["achieved_gbs"] / copy_gbs,
                          "compute": comp},
             "clocks": head.get("clocks"),
             "e2e": {"value": e2e_value, "unit": UNIT,
@@ -638,26 +676,18 @@ def run_sweep(args, local):
     Cartesian box at 128^3 .. 512^3 (Passot-Pouquet spectrum, k0 4, u_rms 1,
     Mt 0.4, seed 5; rho 1, uniform p): per size and form cell-updates/s per
     stage, stage-kernel HBM GB/s, and the mixed-vs-FP64 per-field error after
-    ACC_STEPS steps.  The reference's LES scheme (WENO3 + Rusanov blended with
-    the central flux at sigma 0.5, CS 0.03 = 0.17^2), SSP-RK3, dt from CFL 0.4.
-    One JSON line per size (not the contract line)."""
+    ACC_STEPS steps, in config 5's scheme (config5_case).  One JSON line per
+    size (not the contract line)."""
     import torch
 
     from chimera_comp_les_b200 import Block
     from chimera_comp_les_b200 import diagnostics as D
-    from chimera_comp_les_b200 import workloads as W
     torch.cuda.set_device(local)
     peak, peak_kind = measured_peaks()
     for n in [int(x) for x in args.sweep.split(",")]:
-        coords = W.periodic_grid(n, 2 * math.pi, amp=0.0)
-        q0 = W.isotropic_turbulence(n, 5, k_peak=4.0, mach_t=0.4, spectrum="passot_pouquet", u_rms=1.0)
-        r = q0[..., 0]
-        c = np.sqrt(1.4 * 0.4 * (q0[..., 4] - 0.5 * (q0[..., 1] ** 2 + q0[..., 2] ** 2 + q0[..., 3] ** 2) / r) / r)
-        lam = sum(float((np.abs(q0[..., 1 + a] / r) + c).max()) for a in range(3)) * n / (2 * math.pi)
-        dt = math.floor(0.4 / lam * 1e6) / 1e6
-        opts = dict(CFG, s_x=0.5, s_y=0.5, s_z=0.5, ren=10000.0, ma=0.4, dt=dt)
+        coords, q0, dt, opts = config5_case(n)
         nv = np.zeros(coords.shape[:3])
-        out = {"sweep": "isotropic turbulence", "n": n, "grid": [n + 2] * 3, "dt": dt}
+        out = {"sweep": "isotropic turbulence", "scheme": CONFIG5_SCHEME, "n": n, "grid": [n + 2] * 3, "dt": dt}
         final = {}
         for prec in ("fp64", "mixed"):
             blk = Block(n + 2, n + 2, n + 2, precision=prec, device=local, **opts)
@@ -690,17 +720,17 @@ def run_sweep(args, local):
 # velocities now and one step back 144 and its vertex indices 12, the new Q
 # and P written 48, then read 48 and stored at the node 48
 B_IBM_ENTRY = 16 + 24 + 88 + 144 + 144 + 12 + 48 + 48 + 48
-# sigma 0.5: the Roe upwind flux and the central flux both enter every face
-SPHERE_OPTS = dict(les=1, inviscid=0, fluxorder=3, eno_order=2, central=2, s_x=0.5, s_y=0.5, s_z=0.5, ren=300.0,
-                   ma=0.3, pr=0.71, gamma=1.4, dt=1e-3, cs_const=0.1, isothermal=0, flux="roe")
+# WENO5-JS + Roe, pure upwind (sigma 0); Smagorinsky Cs 0.1 (CS = Cs^2 = 0.01)
+SPHERE_OPTS = dict(les=1, inviscid=0, fluxorder=3, eno_order=2, central=2, s_x=0.0, s_y=0.0, s_z=0.0, ren=300.0,
+                   ma=0.3, pr=0.71, gamma=1.4, dt=1e-3, cs_const=0.01, isothermal=0, flux="roe", weno_order=5)
 
 
 def run_sphere(args, local):
     """Flow past a stationary sphere with the immersed boundary on the device:
     DMDA 192 x 192 x 256 (i, j across, k streamwise on [-5, 15] D), nodes
     clustered toward the sphere (spacing 0.01 D there), slip walls in i and j,
-    inflow / outflow 45 in k, Re 300, Ma 0.3, WENO3 with the Roe flux blended
-    with the central flux at sigma 0.5, Smagorinsky CS 0.1, dt 1e-3; uniform stream plus seeded 1e-3 white noise.
+    inflow / outflow 45 in k, Re 300, Ma 0.3, WENO5-JS with the Roe flux (pure
+    upwind), Smagorinsky Cs 0.1, dt 1e-3; uniform stream plus seeded 1e-3 white noise.
     The interpolation list comes from workloads.sphere_ibm_list (an analytic
     stand-in for the reference's host search).  Per form: cell-updates/s per
     stage with the interpolation in every step, the interpolation's share of
@@ -719,8 +749,7 @@ def run_sphere(args, local):
     build_s = time.perf_counter() - t0
     info = case["info"]
     out = {"workload": f"sphere D=1, DMDA {n[0]}x{n[1]}x{n[2]}, clustered to 0.01 D, slip i/j, inflow/outflow 45 in k, "
-                       "Re 300 Ma 0.3, WENO3 + Roe blended with the central flux at sigma 0.5, Smagorinsky CS 0.1, "
-                       "SSP-RK3, dt 1e-3",
+                       "Re 300 Ma 0.3, WENO5-JS + Roe (pure upwind), Smagorinsky Cs 0.1 (CS 0.01), SSP-RK3, dt 1e-3",
            "interface_nodes": int(info.size), "list_build_s": build_s, "unit": UNIT}
     final = {}
     peak, peak_kind = measured_peaks()

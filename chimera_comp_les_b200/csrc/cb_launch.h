@@ -40,6 +40,21 @@ struct BatchLaunch {
                             cudaStream_t s);
 };
 
+// Each (form, LES) instantiation is defined in exactly one object, the part
+// built with that form's floating-point flags.  Without these declarations a
+// part would also instantiate the other parts' launchers (the inline
+// dispatchers below name all of them) and compile their kernels with its own
+// flags: an FP64 kernel built with FMA contraction, registered beside the
+// right one under the same host symbol.
+extern template struct StageLaunch<double, false, false>;
+extern template struct StageLaunch<double, false, true>;
+extern template struct StageLaunch<float, true, false>;
+extern template struct StageLaunch<float, true, true>;
+extern template struct BatchLaunch<double, false, false>;
+extern template struct BatchLaunch<double, false, true>;
+extern template struct BatchLaunch<float, true, false>;
+extern template struct BatchLaunch<float, true, true>;
+
 inline cudaError_t stage_attrs_all(bool mix) {
   cudaError_t e = mix ? StageLaunch<float, true, true>::attrs() : StageLaunch<double, false, true>::attrs();
   if (e == cudaSuccess) e = mix ? StageLaunch<float, true, false>::attrs() : StageLaunch<double, false, false>::attrs();

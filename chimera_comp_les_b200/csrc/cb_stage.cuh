@@ -1088,7 +1088,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 // its range with its own prologue.  Every node gets the same arithmetic in
 // both shapes (a chunk start recomputes its first k-face from the same data).
 template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0, bool NV0 = false>
-__global__ void __launch_bounds__(StageGeo<FLUX>::NT, MIX ? 2 : 1)
+static __global__ void __launch_bounds__(StageGeo<FLUX>::NT, MIX ? 2 : 1)
     stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
   extern __shared__ double smem_d[];
   constexpr int BY = StageGeo<FLUX>::BY;
@@ -1185,7 +1185,7 @@ struct BatchBlock {
 };
 
 template <typename R, bool MIX, bool LES, bool VISC, bool NV0 = false, int FLUX = 0>
-__global__ void __launch_bounds__(StageGeo<FLUX>::NT, MIX ? 2 : 1)
+static __global__ void __launch_bounds__(StageGeo<FLUX>::NT, MIX ? 2 : 1)
     stage_batched_kernel(const BatchBlock *__restrict__ blocks, const int2 *__restrict__ items, int nitems,
                          unsigned *__restrict__ counter, int istage, double alfa, double beta, double adt) {
   extern __shared__ double smem_d[];

@@ -56,3 +56,22 @@ def test_product_has_no_cpu_fallback():
         if f.endswith(".py"):
             src += open(os.path.join(os.path.dirname(pkg.__file__), f)).read()
     assert "import oracle" not in src and "from oracle" not in src
+
+
+def test_every_kernel_is_local_to_the_object_that_compiled_it():
+    """The FP64 parity form and the mixed form are compiled with different
+    floating-point flags (no FMA contraction / IEEE division versus
+    contraction and fast division).  A kernel whose host symbol is global or
+    weak can be defined by several objects -- with different flags -- and the
+    runtime then launches whichever copy it bound to that symbol.  Every
+    kernel symbol of the library must therefore have local binding."""
+    import shutil
+    import subprocess
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm not available")
+    out = subprocess.run([nm, "-C", _lib_path()], capture_output=True, text=True, check=True).stdout
+    kern = [ln.split(" ", 2) for ln in out.splitlines() if re.search(r"\bcb::\w+_kernel\b", ln)]
+    assert len(kern) > 100, "kernel symbols not found"
+    shared = [name for _, kind, name in kern if kind not in ("t", "r", "d", "b")]
+    assert not shared, shared[:5]

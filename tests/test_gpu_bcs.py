@@ -78,7 +78,10 @@ def test_characteristic_isothermal_walls_match_oracle(bct, les, twoD, twall):
             assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= tol, prec
 
 
-INFLOW = [(7, 7, 3, 3, 52, 44), (7, 7, 3, 3, 47, 45), (3, 3, 1, 1, 52, 49), (7, 7, 7, 7, 47, 8)]
+# with this seeded state, k-hi code 49 behind the 52 inlet on walled j faces
+# drives the restatement itself to rho, p < 0 at the outlet, so that pairing
+# uses the outflow code 45
+INFLOW = [(7, 7, 3, 3, 52, 44), (7, 7, 3, 3, 47, 45), (3, 3, 1, 1, 52, 45), (7, 7, 7, 7, 47, 8)]
 
 
 @pytest.mark.parametrize("bct", INFLOW)
@@ -97,7 +100,10 @@ def test_inflow_codes_52_47_match_oracle(bct, les, ti0):
     q = W.random_smooth_state(shape, seed=19, periodic=False)
     nv = np.zeros(shape)
     ref = oracle_run(cfg, coords, q, nv, steps=3)
-    assert np.isfinite(ref["q_steps"]).all()
+    qs = ref["q_steps"]
+    assert np.isfinite(qs).all()
+    ke = 0.5 * (qs[..., 1] ** 2 + qs[..., 2] ** 2 + qs[..., 3] ** 2) / qs[..., 0]
+    assert qs[..., 0].min() > 0 and (qs[..., 4] - ke).min() > 0  # a physical case: the device flags rho, p <= 0
     for prec, tol in (("fp64", RTOL_L2), ("mixed", 1e-5)):
         with gpu_block(cfg, precision=prec) as b:
             b.FormMetrics(coords)
