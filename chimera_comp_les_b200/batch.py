@@ -217,7 +217,9 @@ class Batch:
                  s_z: float = 1.0, ren: float = 3000.0, ma: float = 2.81, pr: float = 0.72, gamma: float = 1.4,
                  dt: float = 0.01, st: float = 1.0, cs_const: float = 0.03, ci: float = 0.06, ratio: float = 0.0,
                  precision: str = "fp64", device: int = 0, calc_sigma: int = 0, visT: int = 0,
-                 tref: float = 273.15, twod: int = 0, flux: str = "rusanov", weno_order: int = 3):
+                 tref: float = 273.15, twod: int = 0, flux: str = "rusanov", weno_order: int = 3,
+                 s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5,
+                 abc: int = 0):
         self.lib = _lib.load()
         self.dims = [tuple(int(x) for x in d) for d in dims]
         cfg = CbConfig()
@@ -226,7 +228,9 @@ class Batch:
         for k, v in dict(les=les, inviscid=inviscid, fluxorder=fluxorder, eno_order=eno_order, central=central,
                          isothermal=isothermal, s_x=s_x, s_y=s_y, s_z=s_z, ren=ren, ma=ma, pr=pr, gamma=gamma,
                          dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device,
-                         calc_sigma=calc_sigma, visT=visT, tref=tref, twod=twod, weno_order=weno_order).items():
+                         calc_sigma=calc_sigma, visT=visT, tref=tref, twod=twod, weno_order=weno_order,
+                         s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh,
+                         abc=abc).items():
             setattr(cfg, k, v)
         cfg.flux = {"rusanov": 0, "roe": 1}[flux] if isinstance(flux, str) else int(flux)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]

@@ -113,6 +113,12 @@ struct cb_batch {
   double *qb[3][5] = {};
   double *met[3][3] = {};
   double *aj = nullptr, *nvert = nullptr, *nut = nullptr, *delta2 = nullptr;
+  // shock sensor (calc_sigma): the hybrid weights (s_x, s_y, s_z) and the
+  // planes of the filter pass, each `total` long; per block a device table of
+  // its six plane pointers (weights, then filter planes)
+  double *sig_arena = nullptr;
+  double *sig_a[3] = {}, *sig_b[3] = {};
+  double **d_sigptr = nullptr;
   void *arena_mixed = nullptr;
   float4 *met4[3] = {};
   double *gcl[3] = {};
@@ -142,11 +148,11 @@ struct cb_batch {
 };
 
 // FLUX bits of the batch's stage kernels: Roe, WENO5-JS, and with LES the
-// constant blend weight s_x = s_y = s_z when it is exactly 1 or 0 (the
-// single-block context's rule; the sensor is not built here)
+// constant blend weight s_x = s_y = s_z when it is exactly 1 or 0 and the
+// sensor is off (the single-block context's rule)
 static int batch_flux_bits(const cb_config &f) {
   int fl = (f.flux == 1 ? FLUX_ROE : 0) | (f.weno_order == 5 ? FLUX_W5 : 0);
-  if (f.les && f.s_x == f.s_y && f.s_y == f.s_z) {
+  if (f.les && !f.calc_sigma && f.s_x == f.s_y && f.s_y == f.s_z) {
     if (f.s_x == 1.0) fl |= FLUX_SIGMA1;
     else if (f.s_x == 0.0) fl |= FLUX_SIGMA0;
   }
@@ -202,6 +208,7 @@ static DevFields block_fields(const cb_batch *b, int blk, int in, int old, int o
   F.nut = b->nut + o;
   F.delta2 = b->delta2 + o;
   for (int a = 0; a < 3; a++) F.gcl[a] = b->gcl[a] ? b->gcl[a] + o : nullptr;
+  for (int a = 0; a < 3; a++) F.sig[a] = b->sig_a[a] ? b->sig_a[a] + o : nullptr;
   F.status = b->status;
   return F;
 }
@@ -289,7 +296,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
   };
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
       (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
-      (cfg->les && cfg->calc_sigma) || (cfg->flux != 0 && cfg->flux != 1) ||
+      (cfg->flux != 0 && cfg->flux != 1) ||
       (cfg->weno_order != 3 && cfg->weno_order != 5))
     return bail(CB_E_UNSUPPORTED, "option combination not built");
   if (cfg->weno_order == 5 && cfg->fluxorder != 3) return bail(CB_E_ARG, "weno_order 5 needs fluxorder 3");
@@ -322,7 +329,10 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.twod = cfg->twod;  // -twoD 1: no i-face fluxes
     d.gm1 = cfg->gamma - 1.0;
     d.nvq = 1;  // nvert starts zero
-    d.calc_sigma = 0;  // the shock sensor is built for single-block contexts
+    d.calc_sigma = (cfg->les && cfg->calc_sigma) ? 1 : 0;
+    d.s_x_min = cfg->s_x_min; d.s_y_min = cfg->s_y_min; d.s_z_min = cfg->s_z_min;
+    d.ks = cfg->sigma_thrsh;
+    d.abc = cfg->abc;
     d.flux = cfg->flux;
     if (shell_count(d) >= (1LL << 31)) return bail(CB_E_ARG, "block too large for 32-bit boundary indexing");
     bh.off = off;
@@ -356,6 +366,24 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     for (int a = 0; a < 3; a++) b->gcl[a] = g + (size_t)b->total * a;
     if (cudaMalloc(&b->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "ptab4");
   }
+  if (cfg->les && cfg->calc_sigma) {
+    const size_t sb = sizeof(double) * (size_t)b->total * 6;
+    if (cudaMalloc(&b->sig_arena, sb) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc sensor planes");
+    cudaMemsetAsync(b->sig_arena, 0, sb, b->stream);
+    for (int a = 0; a < 3; a++) {
+      b->sig_a[a] = b->sig_arena + (size_t)b->total * a;
+      b->sig_b[a] = b->sig_arena + (size_t)b->total * (3 + a);
+    }
+    std::vector<double *> hp((size_t)6 * nblocks);
+    for (int k = 0; k < nblocks; k++)
+      for (int a = 0; a < 3; a++) {
+        hp[6 * k + a] = b->sig_a[a] + b->blk[k].off;
+        hp[6 * k + 3 + a] = b->sig_b[a] + b->blk[k].off;
+      }
+    if (cudaMalloc(&b->d_sigptr, sizeof(double *) * hp.size()) != cudaSuccess) return bail(CB_E_CUDA, "sensor table");
+    if (cudaMemcpy(b->d_sigptr, hp.data(), sizeof(double *) * hp.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(CB_E_CUDA, "sensor table");
+  }
   {
     const bool mix = cfg->precision == CB_MIXED;
     if (stage_attrs_all(mix) != cudaSuccess || batch_attrs_all(mix) != cudaSuccess)
@@ -375,7 +403,8 @@ void cb_batch_destroy(cb_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
   destroy_graphs(b);
-  void *ptrs[] = {b->arena, b->arena_mixed, b->staging, b->ptab, b->ptab4, b->d_tables, b->d_items, b->d_counter,
+  void *ptrs[] = {b->arena, b->arena_mixed, b->sig_arena, b->d_sigptr, b->staging, b->ptab, b->ptab4, b->d_tables,
+                  b->d_items, b->d_counter,
                   b->status, b->d_hdst, b->d_hsrc, b->d_hin, b->d_wdst, b->d_wsrc,
                   b->xs.d_src, b->xs.d_dst, b->xs.d_fin, b->xw.d_src, b->xw.d_dst, b->xw.d_fin};
   for (void *p : ptrs)
@@ -701,6 +730,46 @@ static int enqueue_nut(cb_batch *b) {
   return CB_OK;
 }
 
+// Ghost layers of the three planes of one sensor pass (arena pointers `ar`,
+// per-block pointer tables at offset `toff` of a block's six): the wrap map
+// when the batch has one, else each block's own periodic wrap.
+static int sigma_ghosts(cb_batch *b, double *const ar[3], int toff) {
+  if (b->nwrap) {
+    for (int a = 0; a < 3; a++)
+      plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, ar[a]);
+  } else {
+    for (int k = 0; k < b->nb; k++)
+      ghost_fill_kernel<<<bgrid(b, shell_count(b->blk[k].dc)), 256, 0, b->stream>>>(b->blk[k].dc,
+                                                                                    b->d_sigptr + 6 * k + toff, 3);
+  }
+  BCUDA(b, cudaGetLastError());
+  return CB_OK;
+}
+
+// Hybrid weights of the shock sensor per block from the step's input state
+// (formConvectionLES at istage 0, rhs.c:3328-3433): the single-block
+// context's three passes, each followed by the ghost fill.  Every block's
+// weights come from its own arrays, as each block of the reference computes
+// them on its own DMDA.
+static int enqueue_sigma(cb_batch *b, int in) {
+  const char *tab = reinterpret_cast<const char *>(b->d_tables + (size_t)(in * 13) * b->nb);
+  for (int k = 0; k < b->nb; k++) {
+    const BlockHost &bh = b->blk[k];
+    const char *ent = tab + sizeof(BatchBlock) * k;
+    const double *const *q = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
+    sigma_sensor_kernel<<<bgrid(b, bh.dc.plane), 256, 0, b->stream>>>(bh.dc, q, b->d_sigptr + 6 * k);
+  }
+  if (int e = sigma_ghosts(b, b->sig_a, 0)) return e;
+  for (int k = 0; k < b->nb; k++)
+    sigma_filter_kernel<<<bgrid(b, b->blk[k].dc.plane), 256, 0, b->stream>>>(
+        b->blk[k].dc, (const double *const *)(b->d_sigptr + 6 * k), b->d_sigptr + 6 * k + 3);
+  if (int e = sigma_ghosts(b, b->sig_b, 3)) return e;
+  for (int k = 0; k < b->nb; k++)
+    sigma_post_kernel<<<bgrid(b, b->blk[k].dc.plane), 256, 0, b->stream>>>(
+        b->blk[k].dc, (const double *const *)(b->d_sigptr + 6 * k + 3), b->d_sigptr + 6 * k);
+  return sigma_ghosts(b, b->sig_a, 0);
+}
+
 // Stage s of the step that started from buffer `old`: the stage kernel over
 // all blocks (persistent or one launch per block), then the local halo gather.
 static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int out) {
@@ -762,6 +831,10 @@ static int enqueue_batch_step(cb_batch *b, int per_block) {
   int in = b->cur, out = b->cur;
   for (int s = 0; s < ns; s++) {
     stage_buffers(old, s, &in, &out);
+    if (s == 0 && b->sig_arena) {
+      int e = enqueue_sigma(b, in);
+      if (e) return e;
+    }
     int e = enqueue_stage(b, s, per_block, in, old, out);
     if (e) return e;
     if (!b->cfg.inviscid) b->uc = in;
@@ -819,6 +892,8 @@ int cb_batch_set_exchange(cb_batch *b, int kind, long long nsend, const int *sen
   if (!b || (kind != CB_HALO_STAGE && kind != CB_HALO_WRAP) || nsend < 0 || nrecv < 0 || (nsend && (!send || !d_send)) ||
       (nrecv && (!recv || !d_recv)))
     return CB_E_ARG;
+  if (b->sig_arena && (nsend || nrecv))
+    return bfail(b, CB_E_UNSUPPORTED, "the shock sensor with a cross-process exchange is not built");
   const int sw = kind == CB_HALO_STAGE ? 5 : 4;
   std::vector<long long> hs((size_t)nsend), hd((size_t)nrecv);
   std::vector<unsigned char> hf((size_t)nsend);
@@ -888,6 +963,7 @@ static FieldSet field_set(const double *const *in, const double *const *out, int
 //                   map, pack of the stage values (5 per entry)
 int cb_batch_phase(cb_batch *b, int phase, int stage, int mode) {
   if (!b || (mode != 0 && mode != 1)) return CB_E_ARG;
+  if (b->sig_arena) return bfail(b, CB_E_UNSUPPORTED, "the shock sensor with a cross-process exchange is not built");
   for (auto &bh : b->blk)
     if (!bh.have_grid || !bh.have_state) return bfail(b, CB_E_STATE, "every block needs a grid and a state");
   if (phase == CB_PHASE_STATE) {

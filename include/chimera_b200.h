@@ -333,7 +333,10 @@ int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const double *d_q
  * on-device gather that fills every block's boundary and ghost nodes from a
  * halo map.  A whole step runs as a CUDA graph.  Blocks share the cb_config
  * (bctype is ignored: block faces are interfaces filled by the halo map);
- * their sizes may differ.
+ * their sizes may differ.  With les and calc_sigma every block computes the
+ * shock sensor's weights from its own arrays at the first stage of a step,
+ * each pass followed by the wrap map (a batch with a cross-process exchange
+ * refuses the sensor with CB_E_UNSUPPORTED).
  *
  * Per block k: cb_batch_set_grid (coordinates, 3 per node, AoS, as
  * cb_set_grid), cb_batch_set_nvert (optional; default 0), cb_batch_upload_state

@@ -69,6 +69,11 @@ VARIANTS = [
     ("weno5", dict(weno_order=5, s_x=0.5, s_y=0.5, s_z=0.5)),
     ("weno5_roe_sigma0", dict(weno_order=5, flux="roe", s_x=0.0, s_y=0.0, s_z=0.0)),
     ("sigma1", dict(s_x=1.0, s_y=1.0, s_z=1.0)),
+    # the shock sensor: per-block weights from the step's input state, each
+    # pass followed by the wrap map (with -ABC above plane 9 in the blocks
+    # that reach it)
+    ("sensor", dict(calc_sigma=1, s_x=0.5, s_y=0.6, s_z=0.7, s_x_min=0.05, sigma_thrsh=1e-4, abc=9)),
+    ("sensor_weno5_roe", dict(calc_sigma=1, weno_order=5, flux="roe", s_x=0.8, s_y=0.8, s_z=0.8)),
 ]
 
 
@@ -252,3 +257,18 @@ def test_batch_cfl_dt_is_the_max_over_blocks():
                     lams.append(blk.cfl_dt(0.4)[1])
             assert lam == max(lams) and lam > 0
             assert dt == 0.4 / lam
+
+
+def test_sensor_refused_with_a_cross_process_exchange():
+    """The sensor's ghost layers cross blocks through the local wrap map only:
+    a batch with the sensor refuses exchange lists with CB_E_UNSUPPORTED."""
+    import torch
+    from chimera_comp_les_b200._lib import CB_E_UNSUPPORTED, ChimeraError
+    from chimera_comp_les_b200 import batch as B
+    d = (14, 12, 11)
+    inputs = _inputs([d], seed0=5)
+    buf = torch.zeros(5, dtype=torch.float64, device="cuda:0")
+    with _batch([d], inputs, opts=dict(OPTS, calc_sigma=1)) as bt:
+        with pytest.raises(ChimeraError) as e:
+            bt.set_exchange(B.HALO_STAGE, np.array([[0, 1, 1, 1, 0]]), buf.data_ptr(), np.zeros((0, 4)), 0)
+        assert e.value.code == CB_E_UNSUPPORTED

@@ -63,9 +63,3 @@ def test_sensor_rhs_and_steps_match_oracle(name, n, kw):
         b.RungeKutta(2)
         assert max(per_field_rel_l2(b.Q(), ref["q_steps"])) <= 1e-5
 
-
-def test_sensor_refused_where_not_built():
-    from chimera_comp_les_b200.batch import Batch
-    from chimera_comp_les_b200._lib import ChimeraError
-    with pytest.raises(ChimeraError):
-        Batch([(20, 20, 20)], les=1, calc_sigma=1)
