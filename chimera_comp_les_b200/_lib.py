@@ -112,7 +112,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         ("cb_ibm_set_surface", [P, C.c_int, C.c_int, C.c_int, P, P, P, D, D, D]),
         ("cb_ibm_set_velocity", [P, C.c_int, D, D]), ("cb_ibm_set_list", [P, C.c_int, C.c_int, P, D]),
         ("cb_ibm_count", [P, C.c_int]), ("cb_ibm_set_options", [P, C.c_int, C.c_int]),
-        ("cb_ibm_interpolate", [P, C.c_int, C.c_int]),
+        ("cb_ibm_interpolate", [P, C.c_int, C.c_int]), ("cb_ibm_get_ustar", [P, C.c_int, D]),
     ]:
         f = getattr(lib, name)
         f.argtypes = args

@@ -46,10 +46,13 @@ struct IbmBody {
   int *tri = nullptr;
   int4 *node = nullptr;
   long long *don = nullptr;
-  double *w = nullptr, *out = nullptr;
+  double *w = nullptr, *out = nullptr, *ustar = nullptr;
+  unsigned char *last = nullptr;          // -isothermal 2: the entry that writes its node
+  double *iso = nullptr, *pa = nullptr;   // -isothermal 2: per-entry terms, the chain's carried pressure
   IbmDev dev() const {
     IbmDev d;
     d.n = n; d.node = node; d.don = don; d.w = w; d.tri = tri; d.nf = nf; d.u = u; d.uold = uold; d.out = out;
+    d.ustar = ustar; d.last = last; d.iso = iso; d.pa = pa;
     return d;
   }
 };
@@ -232,12 +235,14 @@ static void harvest_timing(cb_ctx *c) {
 
 // Hybrid weights of the shock sensor from the stage input `in` (istage 0 of
 // formConvectionLES): three passes, each followed by the DMGlobalToLocal wrap.
-static int sigma_update(cb_ctx *c, int in) {
+// P: the pressure plane the first stage reads after an immersed step (lP
+// carried from the interpolation), else null (the EOS of the input).
+static int sigma_update(cb_ctx *c, int in, const double *P) {
   if (!c->dc.calc_sigma) return CB_OK;
   TimedScope ts(c, false);
   const int g = grid_for(c, (long long)c->plane);
   const long long sh = shell_count(c->dc);
-  sigma_sensor_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * in), c->ptab + PT_SIGA);
+  sigma_sensor_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * in), c->ptab + PT_SIGA, P);
   ghost_fill_kernel<<<grid_for(c, sh), 256, 0, c->stream>>>(c->dc, c->ptab + PT_SIGA, 3);
   sigma_filter_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + PT_SIGA), c->ptab + PT_SIGB);
   ghost_fill_kernel<<<grid_for(c, sh), 256, 0, c->stream>>>(c->dc, c->ptab + PT_SIGB, 3);
@@ -354,14 +359,23 @@ static bool ibm_active(const cb_ctx *c) {
 }
 
 // Five sweeps of ibm_interpolation_advanced for one body on the current state.
-static int ibm_sweeps(cb_ctx *c, const IbmBody &b, int add_dundt) {
+// rho_old: the density plane of Qold, which -isothermal 2 reads.
+static int ibm_sweeps(cb_ctx *c, const IbmBody &b, int add_dundt, const double *rho_old) {
   const IbmDev d = b.dev();
   const int g = grid_for(c, b.n);
   const int slip = (c->cfg.inviscid || c->ibm_wallfunction == 3) ? 1 : 0;  // ibm_iso.c:2721
   const int iso1 = c->cfg.isothermal == 1 ? 1 : 0;
+  const int wf2 = c->ibm_wallfunction == 2 ? 1 : 0;
+  const bool iso2 = c->cfg.isothermal == 2;
+  const double a_sound = sqrt(c->cfg.twall / (c->cfg.ma * c->cfg.ma));  // ibm_iso.c:2768, the host's sqrt
   for (int s = 0; s < IBM_SWEEPS; s++) {
     ibm_interp_kernel<<<g, 256, 0, c->stream>>>(c->dc, (const double *const *)(c->ptab + 5 * c->cur), c->pl, d,
-                                                add_dundt, c->ibm_twoD, slip, iso1);
+                                                add_dundt, c->ibm_twoD, slip, iso1, wf2, iso2 ? rho_old : nullptr,
+                                                a_sound);
+    if (iso2) {
+      ibm_iso2_chain_kernel<<<1, IBM_CHAIN_NT, 0, c->stream>>>(c->dc, d, s == 0 ? 1 : 0, a_sound);
+      ibm_iso2_finish_kernel<<<g, 256, 0, c->stream>>>(c->dc, d, add_dundt);
+    }
     ibm_scatter_kernel<<<g, 256, 0, c->stream>>>(c->dc, c->ptab + 5 * c->cur, c->pl, d);
   }
   CB_CUDA(c, cudaGetLastError());
@@ -437,7 +451,7 @@ static int enqueue_step(cb_ctx *c) {
     DevFields F = fields_for(c, in, old, out);
     if (s == 0 && c->p_carry) F.pin = c->pl;  // lP carried from the interpolation of the previous step
     if (s == 0) {
-      int e = sigma_update(c, in);
+      int e = sigma_update(c, in, c->p_carry ? c->pl : nullptr);
       if (e) return e;
     }
     {
@@ -471,7 +485,7 @@ static int enqueue_step(cb_ctx *c) {
     if (e) return e;
     for (const auto &b : c->ibm)
       if (b.n > 0) {
-        e = ibm_sweeps(c, b, 1);
+        e = ibm_sweeps(c, b, 1, c->qb[old][0]);  // Qold: the step's input, untouched by its stages
         if (e) return e;
       }
     e = formbcs_zero(c, old);
@@ -992,7 +1006,7 @@ int cb_rhs(cb_ctx *c, int istage, double *rhs) {
   DevFields F = fields_for(c, c->cur, c->cur, -1);
   if (c->p_carry) F.pin = c->pl;
   if (istage == 0) {
-    int e = sigma_update(c, c->cur);
+    int e = sigma_update(c, c->cur, c->p_carry ? c->pl : nullptr);
     if (e) return e;
   }
   CB_CUDA(c, launch_stage(c, F, istage, alfa, beta, 0.0, true));
@@ -1188,7 +1202,8 @@ static int ibm_body(cb_ctx *c, int ibi, IbmBody **b) {
 static void ibm_drop_list(IbmBody &b) {
   if (b.list) cudaFree(b.list);
   b.list = nullptr;
-  b.node = nullptr; b.don = nullptr; b.w = nullptr; b.out = nullptr;
+  b.node = nullptr; b.don = nullptr; b.w = nullptr; b.out = nullptr; b.ustar = nullptr;
+  b.last = nullptr; b.iso = nullptr; b.pa = nullptr;
   b.n = 0;
 }
 
@@ -1249,10 +1264,6 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
   if (n > 0 && !b->surf) return fail(c, CB_E_STATE, "set the body's surface first");
   if (n > 0 && (c->cfg.bctype[4] == 52 || c->cfg.bctype[4] == 47))
     return fail(c, CB_E_UNSUPPORTED, "immersed bodies with the inflow codes 52 and 47 are not built");
-  if (n > 0 && c->cfg.isothermal == 2)
-    return fail(c, CB_E_UNSUPPORTED, "the characteristic isothermal IB wall (isothermal 2) is not built");
-  if (n > 0 && c->dc.calc_sigma)
-    return fail(c, CB_E_UNSUPPORTED, "the shock sensor with immersed bodies is not built");
   const int m[3] = {c->cfg.mx, c->cfg.my, c->cfg.mz};
   const bool per[3] = {c->cfg.bctype[0] == 7, c->cfg.bctype[2] == 7, c->cfg.bctype[4] == 7};
   // a node listed twice keeps its last entry
@@ -1270,11 +1281,17 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
     if (f.cell < -1 || f.cell >= b->n_elmt) return fail(c, CB_E_ARG, "surface element index out of range");
     last[((long long)f.nk * m[1] + f.nj) * m[0] + f.ni] = t;
   }
+  // -isothermal 2 walks every entry (the chain of Pa); the scatter then
+  // writes each node from its last entry only
+  const bool iso2 = c->cfg.isothermal == 2;
   std::vector<int> keep;
-  keep.reserve(last.size());
+  std::vector<unsigned char> lastf;
+  keep.reserve(iso2 ? n : last.size());
   for (int t = 0; t < n; t++) {
     const cb_ibm_info &f = list[t];
-    if (last[((long long)f.nk * m[1] + f.nj) * m[0] + f.ni] == t) keep.push_back(t);
+    const bool is_last = last[((long long)f.nk * m[1] + f.nj) * m[0] + f.ni] == t;
+    if (iso2) lastf.push_back(is_last ? 1 : 0);
+    if (iso2 || is_last) keep.push_back(t);
   }
   const int nk = (int)keep.size();
   std::vector<int4> node(nk);
@@ -1304,13 +1321,23 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
     int fe = fill_ptab(c);
     if (fe) return fe;
   }
-  const size_t bytes = sizeof(int4) * nk + sizeof(long long) * 3 * nk + sizeof(double) * (IBM_NW + 6) * nk;
+  const size_t iso_d = iso2 ? (size_t)IBM_ISO_NS * nk + 1 : 0;  // terms, then the carried pressure
+  const size_t bytes = sizeof(int4) * nk + sizeof(long long) * 3 * nk + sizeof(double) * ((IBM_NW + 7) * (size_t)nk + iso_d) +
+                       (iso2 ? (size_t)nk : 0);
   CB_CUDA(c, cudaMalloc(&b->list, bytes));
   b->node = (int4 *)b->list;
   b->don = (long long *)(b->node + nk);
   b->w = (double *)(b->don + 3 * (size_t)nk);
   b->out = b->w + (size_t)IBM_NW * nk;
+  b->ustar = b->out + (size_t)6 * nk;
+  if (iso2) {
+    b->iso = b->ustar + nk;
+    b->pa = b->iso + (size_t)IBM_ISO_NS * nk;
+    b->last = (unsigned char *)(b->pa + 1);
+    CB_CUDA(c, cudaMemcpyAsync(b->last, lastf.data(), (size_t)nk, cudaMemcpyHostToDevice, c->stream));
+  }
   b->n = nk;
+  CB_CUDA(c, cudaMemsetAsync(b->ustar, 0, sizeof(double) * nk, c->stream));
   CB_CUDA(c, cudaMemcpyAsync(b->node, node.data(), sizeof(int4) * nk, cudaMemcpyHostToDevice, c->stream));
   CB_CUDA(c, cudaMemcpyAsync(b->don, don.data(), sizeof(long long) * don.size(), cudaMemcpyHostToDevice, c->stream));
   CB_CUDA(c, cudaMemcpyAsync(b->w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, c->stream));
@@ -1326,12 +1353,26 @@ int cb_ibm_count(const cb_ctx *c, int ibi) {
 int cb_ibm_set_options(cb_ctx *c, int twoD, int wallfunction) {
   if (!c) return CB_E_ARG;
   if (twoD < 0 || twoD > 3) return fail(c, CB_E_ARG, "twoD must be 0..3");
-  if (wallfunction == 1 || wallfunction == 2)
-    return fail(c, CB_E_UNSUPPORTED, "log-law wall functions (wallfunction 1/2) are not built");
-  if (wallfunction != 0 && wallfunction != 3) return fail(c, CB_E_ARG, "wallfunction must be 0 or 3");
+  // wallfunction 1 reads a table that pre_integrate builds in a stack array of
+  // its own frame (wallfunction.c:113-145): its values are undefined
+  if (wallfunction == 1) return fail(c, CB_E_UNSUPPORTED, "the wall function of -wallfunction 1 is not built");
+  if (wallfunction != 0 && wallfunction != 2 && wallfunction != 3)
+    return fail(c, CB_E_ARG, "wallfunction must be 0, 2 or 3");
   c->ibm_twoD = twoD;
   c->ibm_wallfunction = wallfunction;
   invalidate_graphs(c);
+  return CB_OK;
+}
+
+int cb_ibm_get_ustar(cb_ctx *c, int ibi, double *ustar) {
+  IbmBody *b;
+  int e = ibm_body(c, ibi, &b);
+  if (e) return e;
+  if (b->n > 0) {
+    if (!ustar) return fail(c, CB_E_ARG, "null ustar");
+    CB_CUDA(c, cudaMemcpyAsync(ustar, b->ustar, sizeof(double) * b->n, cudaMemcpyDeviceToHost, c->stream));
+    CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   return CB_OK;
 }
 
@@ -1345,7 +1386,16 @@ int cb_ibm_interpolate(cb_ctx *c, int ibi, int add_dundt) {
       e = eos_to_plane(c);
       if (e) return e;
     }
-    e = ibm_sweeps(c, *b, add_dundt ? 1 : 0);
+    // Qold between steps is the state itself (main.c:971 copies Q to Qold
+    // after every step); the sweeps rewrite the state, so -isothermal 2 reads
+    // a copy of its density taken first
+    const double *rho_old = nullptr;
+    if (c->cfg.isothermal == 2) {
+      CB_CUDA(c, cudaMemcpyAsync(c->spare, c->qb[c->cur][0], sizeof(double) * c->plane, cudaMemcpyDeviceToDevice,
+                                 c->stream));
+      rho_old = c->spare;
+    }
+    e = ibm_sweeps(c, *b, add_dundt ? 1 : 0, rho_old);
     if (e) return e;
     c->p_carry = true;
   }

@@ -663,8 +663,14 @@ __device__ __forceinline__ double eos_node(const DevCfg &c, const double *const 
 __device__ __forceinline__ double pmin(double a, double b) { return (a < b) ? a : b; }
 __device__ __forceinline__ double pmax(double a, double b) { return (a < b) ? b : a; }
 
-// pass 1: every node (s_x, s_y, s_z); interior nodes the clipped ramp of p
-static __global__ void sigma_sensor_kernel(const DevCfg c, const double *const *q, double *const *sig) {
+// pass 1: every node (s_x, s_y, s_z); interior nodes the clipped ramp of p:
+// the plane P when given (the pressure an immersed step carries into the next
+// step's first stage, which formConvectionLES reads as lP), else the EOS of q
+__device__ __forceinline__ double sensor_p(const DevCfg &c, const double *const *q, const double *P, long long n) {
+  return P ? P[n] : eos_node(c, q, n);
+}
+static __global__ void sigma_sensor_kernel(const DevCfg c, const double *const *q, double *const *sig,
+                                           const double *P) {
   const long long total = (long long)c.px * c.py * c.pz;
   const long long si = 1, sj = c.px, sk = (long long)c.px * c.py;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -672,19 +678,19 @@ static __global__ void sigma_sensor_kernel(const DevCfg c, const double *const *
     double sx = c.s_x, sy = c.s_y, sz = c.s_z;
     if (i >= 1 && i <= c.mx - 2 && j >= 1 && j <= c.my - 2 && k >= 1 && k <= c.mz - 2) {
       const long long n = t;
-      const double p0 = eos_node(c, q, n);
+      const double p0 = sensor_p(c, q, P, n);
       const bool absorb = c.abc != 0 && k > c.abc;  // -ABC layer: raw weight 0 (rhs.c:3341, 3355, 3368)
       if (absorb) sx = 0.;
       else if (i < c.mx - 4 && i > 2)
-        sx = sensor_ramp(eos_node(c, q, n - si), p0, eos_node(c, q, n + si), eos_node(c, q, n + 2 * si), c.ks);
+        sx = sensor_ramp(sensor_p(c, q, P, n - si), p0, sensor_p(c, q, P, n + si), sensor_p(c, q, P, n + 2 * si), c.ks);
       sx = pmax(c.s_x_min, pmin(c.s_x, sx));
       if (absorb) sz = 0.;
       else if (c.bctype[4] == 7 || (k < c.mz - 4 && k > 4))
-        sz = sensor_ramp(eos_node(c, q, n - sk), p0, eos_node(c, q, n + sk), eos_node(c, q, n + 2 * sk), c.ks);
+        sz = sensor_ramp(sensor_p(c, q, P, n - sk), p0, sensor_p(c, q, P, n + sk), sensor_p(c, q, P, n + 2 * sk), c.ks);
       sz = pmax(c.s_z_min, pmin(c.s_z, sz));
       if (absorb) sy = 0.;
       else if (j < c.my - 4 && j > 4)
-        sy = sensor_ramp(eos_node(c, q, n - sj), p0, eos_node(c, q, n + sj), eos_node(c, q, n + 2 * sj), c.ks);
+        sy = sensor_ramp(sensor_p(c, q, P, n - sj), p0, sensor_p(c, q, P, n + sj), sensor_p(c, q, P, n + 2 * sj), c.ks);
       sy = pmax(c.s_y_min, pmin(c.s_y, sy));
     }
     sig[0][t] = sx;

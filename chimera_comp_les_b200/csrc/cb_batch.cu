@@ -757,7 +757,7 @@ static int enqueue_sigma(cb_batch *b, int in) {
     const BlockHost &bh = b->blk[k];
     const char *ent = tab + sizeof(BatchBlock) * k;
     const double *const *q = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
-    sigma_sensor_kernel<<<bgrid(b, bh.dc.plane), 256, 0, b->stream>>>(bh.dc, q, b->d_sigptr + 6 * k);
+    sigma_sensor_kernel<<<bgrid(b, bh.dc.plane), 256, 0, b->stream>>>(bh.dc, q, b->d_sigptr + 6 * k, nullptr);
   }
   if (int e = sigma_ghosts(b, b->sig_a, 0)) return e;
   for (int k = 0; k < b->nb; k++)

@@ -184,6 +184,13 @@ class Block:
     def set_ibm_options(self, twoD: int = 0, wallfunction: int = 0):
         self._check(self.lib.cb_ibm_set_options(self._ctx, twoD, wallfunction))
 
+    def ibm_ustar(self, ibi: int = 0) -> np.ndarray:
+        """u_tau of every entry of body ibi's list from the last sweep with
+        -wallfunction 2 (cb_ibm_get_ustar)."""
+        out = np.zeros(max(self.lib.cb_ibm_count(self._ctx, ibi), 0))
+        self._check(self.lib.cb_ibm_get_ustar(self._ctx, ibi, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
     def ibm_interpolation_advanced(self, ibi: int = 0, Add_dUndt: int = 1):
         self._check(self.lib.cb_ibm_interpolate(self._ctx, ibi, Add_dUndt))
 

@@ -245,14 +245,27 @@ int cb_ibm_set_velocity(cb_ctx *ctx, int ibi, const double *u, const double *uol
 /* The interpolation list of body ibi in the order the reference walks it
  * (IBMList head first), with coor the node coordinates passed to
  * cb_set_grid.  A node listed twice keeps its last entry (the later write
- * wins in the reference).  n = 0 removes the body's list.  Allocates. */
+ * wins in the reference).  n = 0 removes the body's list.  Allocates.
+ * With -isothermal 2 (the characteristic wall of ibm_iso.c:2744-2786) each
+ * sweep also walks the list in order on one block for the pressure Pa that
+ * the reference carries from entry to entry. */
 int cb_ibm_set_list(cb_ctx *ctx, int ibi, int n, const cb_ibm_info *list, const double *coor);
-/* Entries of body ibi's list after duplicate nodes were dropped. */
+/* Entries of body ibi's list after duplicate nodes were dropped (with
+ * -isothermal 2 every entry is kept: its characteristic wall links each entry
+ * to the one before it, and a node listed twice is written by its later
+ * entry). */
 int cb_ibm_count(const cb_ctx *ctx, int ibi);
 /* -twoD (0, or 1/2/3: drop x/y/z from the normal and the velocity) and
- * -wallfunction (0: noslip unless -inv, 3: freeslip; 1 and 2, the log-law wall
- * functions, return CB_E_UNSUPPORTED). */
+ * -wallfunction (ibm_iso.c:2708-2728): 0 noslip unless -inv (then freeslip),
+ * 2 the hydset log law of the wall with roughness 1e-16 (wall_function_loglaw,
+ * wallfunction.c:376-420; Newton's method for u_tau), 3 freeslip.  1 returns
+ * CB_E_UNSUPPORTED: the reference's Cabot wall function reads a table that
+ * pre_integrate leaves in a dead stack frame (wallfunction.c:113-145). */
 int cb_ibm_set_options(cb_ctx *ctx, int twoD, int wallfunction);
+/* u_tau of every entry of body ibi's list (cb_ibm_count doubles, list order)
+ * from the last sweep with -wallfunction 2: the values the reference keeps in
+ * user->lUstar at the interface nodes (ibm_iso.c:2714-2719); 0 before. */
+int cb_ibm_get_ustar(cb_ctx *ctx, int ibi, double *ustar);
 /* One call of ibm_interpolation_advanced(user, ibm, ibi, Add_dUndt) on the
  * current state: five sweeps, each ending with the ghost update. */
 int cb_ibm_interpolate(cb_ctx *ctx, int ibi, int add_dundt);

@@ -234,8 +234,8 @@ class Oracle:
         L.cbo_bc_periodic.restype = C.c_int
         L.cbo_formbcs.argtypes = [C.c_void_p, C.c_double, PP, PP, PP, PP, D, D, PP]
         L.cbo_formbcs.restype = C.c_int
-        L.cbo_ibm_interpolate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, PP, PP, D, C.c_int,
-                                          C.c_int, C.c_int]
+        L.cbo_ibm_interpolate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, PP, PP, D, PP, C.c_int,
+                                          C.c_int, C.c_int, D]
         L.cbo_ibm_interpolate.restype = C.c_int
         L.cbo_steps_ibm.argtypes = [C.c_void_p, C.c_int, PP, PP, PP, C.POINTER(C.c_int), D, PP, PP, PP, D, D,
                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, PP, D, C.POINTER(C.c_int),
@@ -363,12 +363,20 @@ class Oracle:
         return q
 
     def ibm_interpolate(self, surface: "IbmSurface", info: np.ndarray, coor_pad: np.ndarray, q: np.ndarray,
-                        p: np.ndarray, add_dundt: int = 1) -> None:
-        """ibm_interpolation_advanced on q (padded 5) and p (padded 1), in place."""
+                        p: np.ndarray, add_dundt: int = 1, ustar: Optional[np.ndarray] = None,
+                        qold: Optional[np.ndarray] = None) -> None:
+        """ibm_interpolation_advanced on q (padded 5) and p (padded 1), in
+        place; with -wallfunction 2, ustar (one double per list entry) receives
+        u_tau of the last sweep; qold (padded 5): the state whose density the
+        -isothermal 2 wall reads (default: q as given)."""
         info = np.ascontiguousarray(info, dtype=IBM_INFO_DTYPE)
+        if ustar is not None:
+            assert ustar.dtype == np.float64 and ustar.size >= info.size and ustar.flags.c_contiguous
         e = self.lib.cbo_ibm_interpolate(self._cp, C.byref(surface.c), info.size, info.ctypes.data,
-                                         _ptrs(list(coor_pad)), _ptrs(list(q)), _dp(p[0]), add_dundt,
-                                         self.cfg.twoD, self.cfg.wallfunction)
+                                         _ptrs(list(coor_pad)), _ptrs(list(q)), _dp(p[0]),
+                                         _ptrs(list(qold)) if qold is not None else None, add_dundt,
+                                         self.cfg.twoD, self.cfg.wallfunction,
+                                         _dp(ustar) if ustar is not None else None)
         if e:
             raise RuntimeError(f"cbo_ibm_interpolate failed with status {e}")
 

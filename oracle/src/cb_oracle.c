@@ -233,13 +233,12 @@ static double sigma_cent(double fL, double f0, double fR, double fRR, double ks)
  * ramp of the pressure smoothness along each direction (x for 2 < i < mx-4,
  * y for 4 < j < my-4, z everywhere in a periodic k), clipped to
  * [s_min, s]; a product filter of square roots of neighbour pairs; then the
- * curvature rule and y = z = min(y, z).  Boundary nodes keep (s_x, s_y, s_z). */
-void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *const sig[3]) {
+ * curvature rule and y = z = min(y, z).  Boundary nodes keep (s_x, s_y, s_z).
+ * p: the ghosted pressure formConvectionLES reads as lP. */
+void cbo_sigma_sensor_p(const cbo_config *c, const double *p, double *const sig[3]) {
   geom G = mkgeom(c);
-  double *p = (double *)malloc(G.n * sizeof(double));
   double *ls[3];
   for (int a = 0; a < 3; a++) ls[a] = (double *)malloc(G.n * sizeof(double));
-  cbo_eos(c, q, p);
   const double ks = c->sigma_thrsh;
   const ptrdiff_t si = 1, sj = G.m[0] + 4, sk = (ptrdiff_t)(G.m[0] + 4) * (G.m[1] + 4);
   const int mx = G.m[0], my = G.m[1], mz = G.m[2];
@@ -302,8 +301,17 @@ void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *con
         sig[1][n] = sig[2][n];
       }
   for (int a = 0; a < 3; a++) cbo_fill_ghosts(c, sig[a]);
-  free(p);
   for (int a = 0; a < 3; a++) free(ls[a]);
+}
+
+/* The sensor on the EqOfState of q (the lP of a step without a carried
+ * pressure). */
+void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *const sig[3]) {
+  geom G = mkgeom(c);
+  double *p = (double *)malloc(G.n * sizeof(double));
+  cbo_eos(c, q, p);
+  cbo_sigma_sensor_p(c, p, sig);
+  free(p);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1403,15 +1411,91 @@ static void ibm_surface_u(const cbo_ibm_surface *s, const double *u, int cell, c
   for (int d = 0; d < 3; d++) U[d] = u[3 * a + d] * b->cs1 + u[3 * m + d] * b->cs2 + u[3 * z + d] * b->cs3;
 }
 
+/* The hydset log law of the wall (wall_function_loglaw with
+ * find_utau_hydset, wallfunction.c:49-100, 376-420), the model of
+ * -wallfunction 2.  kappa = 0.41, B = 5.5 (wallfunction.c:10); ks is the
+ * roughness (1e-16 from ibm_interpolation_advanced, ibm_iso.c:2715).  The
+ * reference's operation order throughout; u_tau by Newton's method with a
+ * central-difference derivative, at most 30 iterations. */
+static const double WF_KAPPA = 0.41, WF_B = 5.5;
+
+static double wf_E(double utau, double ks, double nu) { /* E_coeff, wallfunction.c:49-56 */
+  double kplus = utau * ks / nu, dB;
+  if (kplus <= 2.25) dB = 0.0;
+  else if (kplus > 2.25 && kplus < 90.) dB = (WF_B - 8.5 + 1. / WF_KAPPA * log(kplus)) * sin(0.4258 * (log(kplus) - 0.811));
+  else dB = WF_B - 8.5 + 1. / WF_KAPPA * log(kplus);
+  return exp(WF_KAPPA * (WF_B - dB));
+}
+
+static double wf_u(double nu, double y, double utau, double ks) { /* u_hydset_roughness, wallfunction.c:58-67 */
+  const double yplus = utau * y / nu;
+  if (yplus <= 11.53) return utau * yplus;
+  if (yplus <= 300) return utau / WF_KAPPA * log(wf_E(utau, ks, nu) * yplus);
+  return -1.;
+}
+
+static double wf_f(double nu, double u, double y, double utau0, double ks) { /* f_hydset, wallfunction.c:69-76 */
+  const double yplus = utau0 * y / nu;
+  if (yplus <= 11.53) return utau0 * yplus - u;
+  return utau0 * (1. / WF_KAPPA * log(wf_E(utau0, ks, nu) * yplus)) - u;
+}
+
+static double wf_find_utau(double nu, double u, double y, double guess, double ks) { /* wallfunction.c:78-100 */
+  const double eps = 1.e-7;
+  double utau = guess, utau0 = guess;
+  for (int ii = 0; ii < 30; ii++) {
+    const double df = (wf_f(nu, u, y, utau0 + eps, ks) - wf_f(nu, u, y, utau0 - eps, ks)) / (2. * eps);
+    utau = utau0 - wf_f(nu, u, y, utau0, ks) / df;
+    if (fabs(utau - utau0) < 1.e-7) break;
+    utau0 = utau;
+  }
+  return utau;
+}
+
+/* Ub of the log-law wall (wall_function_loglaw, wallfunction.c:376-420):
+ * the tangential part of the donor velocity scaled to the modelled
+ * magnitude at sb, the normal part linear in the distance. */
+static void wf_loglaw(double nu, double ks, double sc, double sb, const double Ua[3], const double Uc[3], double Ub[3],
+                      double *ustar, double nx, double ny, double nz) {
+  const double u_c = Uc[0] - Ua[0], v_c = Uc[1] - Ua[1], w_c = Uc[2] - Ua[2];
+  const double un = u_c * nx + v_c * ny + w_c * nz;
+  double ut = u_c - un * nx, vt = v_c - un * ny, wt = w_c - un * nz;
+  const double ut_mag = sqrt(ut * ut + vt * vt + wt * wt);
+  *ustar = wf_find_utau(nu, ut_mag, sc, 0.001, ks);
+  double model = wf_u(nu, sb, *ustar, ks);
+  if (model < 0.) model = ut_mag;
+  if (ut_mag > 1.e-10) {
+    ut *= model / ut_mag;
+    vt *= model / ut_mag;
+    wt *= model / ut_mag;
+  } else {
+    ut = vt = wt = 0;
+  }
+  Ub[0] = ut + (sb / sc * un) * nx;
+  Ub[1] = vt + (sb / sc * un) * ny;
+  Ub[2] = wt + (sb / sc * un) * nz;
+  Ub[0] += Ua[0];
+  Ub[1] += Ua[1];
+  Ub[2] += Ua[2];
+}
+
 int cbo_ibm_interpolate(const cbo_config *c, const cbo_ibm_surface *s, int n, const cbo_ibm_info *list,
-                        const double *const coor[3], double *const q[5], double *p, int add_dundt, int twoD,
-                        int wallfunction) {
-  if (c->isothermal == 2 || wallfunction == 1 || wallfunction == 2) return 5; /* not restated */
+                        const double *const coor[3], double *const q[5], double *p, const double *const qold[5],
+                        int add_dundt, int twoD, int wallfunction, double *ustar) {
+  /* -wallfunction 1 reads a table that pre_integrate builds in a stack array
+   * of its own frame (wallfunction.c:113-145): undefined once it returns */
+  if (wallfunction == 1) return 5; /* not restated */
   geom G = mkgeom(c);
-  double *buf = (double *)malloc(G.n * 6 * sizeof(double));
-  double *lq[5], *lp = buf + G.n * 5;
+  double *buf = (double *)malloc(G.n * 7 * sizeof(double));
+  double *lq[5], *lp = buf + G.n * 5, *rho_old = buf + G.n * 6;
   for (int a = 0; a < 5; a++) lq[a] = buf + G.n * a;
+  /* Qold's density for the characteristic wall: the step's start state, or
+   * the state as given */
+  memcpy(rho_old, qold ? qold[0] : q[0], G.n * sizeof(double));
   const double gm2 = c->gamma * c->ma * c->ma;
+  /* -isothermal 2 (ibm_iso.c:2744-2786): one scalar Pa, the pressure of the
+   * previous entry walked (the entry's own at sweep 0), links the entries */
+  double Pa = 0.;
   const int slip = c->inviscid || wallfunction == 3; /* ibm_iso.c:2721 */
   for (int sweep = 0; sweep < IBM_SWEEPS; sweep++) {
     /* the sweep reads the local vectors lQ / lP and writes the global Q / P */
@@ -1447,7 +1531,11 @@ int cbo_ibm_interpolate(const cbo_config *c, const cbo_ibm_surface *s, int n, co
       for (int d = 0; d < 3; d++)
         Uc[d] = lq[1 + d][d1] / lq[0][d1] * sk1 + lq[1 + d][d2] / lq[0][d2] * sk2 + lq[1 + d][d3] / lq[0][d3] * sk3;
       double Ub[3];
-      if (slip) { /* freeslip: normal part linear in the distance, tangential part of the donor */
+      if (wallfunction == 2) { /* ibm_iso.c:2714-2719, 1/user->ren as the reference */
+        double us;
+        wf_loglaw(1. / c->ren, 1.e-16, sc, sb, Ua, Uc, Ub, &us, nfx, nfy, nfz);
+        if (ustar) ustar[e] = us;
+      } else if (slip) { /* freeslip: normal part linear in the distance, tangential part of the donor */
         const double Uan = Ua[0] * nfx + Ua[1] * nfy + Ua[2] * nfz;
         const double Ucn = Uc[0] * nfx + Uc[1] * nfy + Uc[2] * nfz;
         const double Ubn = Uan + (Ucn - Uan) * sb / sc;
@@ -1461,8 +1549,28 @@ int cbo_ibm_interpolate(const cbo_config *c, const cbo_ibm_surface *s, int n, co
       if (twoD == 2) Ub[1] = 0.;
       if (twoD == 3) Ub[2] = 0.;
       double rho;
-      if (c->isothermal == 1) rho = pb * gm2 / 1.0; /* wall temperature Tb = 1 (ibm_iso.c:2795-2803) */
-      else rho = lq[0][d1] * sk1 + lq[0][d2] * sk2 + lq[0][d3] * sk3; /* d rho / dn = 0 */
+      if (c->isothermal == 2) {
+        /* the no-slip isothermal wall of Poinsot & Lele (J. Comput. Phys. 101,
+         * 1992) through the incoming characteristic u_n - a, with a^2 = Twall
+         * / Ma^2 and the wall temperature Tb interpolated like the velocity */
+        const double rhoc = lq[0][d1] * sk1 + lq[0][d2] * sk2 + lq[0][d3] * sk3;
+        double Tc = pb / rhoc * gm2;
+        if (Tc < 0.) Tc = 0.;
+        const double Tb = (Tc - c->twall) * sb / sc + c->twall;
+        const double a_sound = sqrt(c->twall / (c->ma * c->ma));
+        const double Lambda1 = Ua_n - a_sound;
+        if (sweep == 0) Pa = pb;
+        const double L1 = Lambda1 / sc *
+                          ((pb - Pa) - rhoc * a_sound * ((Uc[0] - Ua[0]) * nfx + (Uc[1] - Ua[1]) * nfy +
+                                                         (Uc[2] - Ua[2]) * nfz));
+        rho = rho_old[o] - c->dt * L1 / a_sound / a_sound;
+        pb = rho * Tb / gm2;
+        Pa = pb;
+      } else if (c->isothermal == 1) {
+        rho = pb * gm2 / 1.0; /* wall temperature Tb = 1 (ibm_iso.c:2795-2803) */
+      } else {
+        rho = lq[0][d1] * sk1 + lq[0][d2] * sk2 + lq[0][d3] * sk3; /* d rho / dn = 0 */
+      }
       if (add_dundt) pb += rho * (Ua_n - Ua_nold) / c->dt * (sc - sb);
       const double ru = rho * Ub[0], rv = rho * Ub[1], rw = rho * Ub[2];
       q[0][o] = rho; q[1][o] = ru; q[2][o] = rv; q[3][o] = rw;
@@ -1489,7 +1597,6 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
                   const double *nvert, int nbodies, const cbo_ibm_surface *surf, const int *nlist,
                   const cbo_ibm_info *const *lists, const double *const coor[3], double *lp, int *lp_valid,
                   int twoD, int wallfunction) {
-  if (c->calc_sigma) return 5; /* the sensor with a carried pressure is not restated */
   geom G = mkgeom(c);
   int ns = cbo_nstages(c);
   double *buf = (double *)calloc(G.n * 20, sizeof(double));
@@ -1509,6 +1616,10 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
       cbo_eddy_viscosity(c, *have_uc ? (const double *const *)quc : NULL, csi, eta, zet, aj, nvert, nut);
     for (int s = 0; s < ns && !err; s++) {
       const double *lps = (s == 0 && *lp_valid) ? lp : NULL;
+      if (c->les && c->calc_sigma && s == 0) { /* istage 0 reads lP: the carried pressure when there is one */
+        if (lps) cbo_sigma_sensor_p(c, lps, sig);
+        else cbo_sigma_sensor(c, (const double *const *)q, sig);
+      }
       err = rhs_impl(c, (const double *const *)q, lps, csi, eta, zet, aj, nvert, nut, (const double *const *)sig,
                      rhs);
       if (err) break;
@@ -1524,7 +1635,9 @@ int cbo_steps_ibm(const cbo_config *c, int nsteps, double *const q[5], double *c
     if (err) break;
     cbo_eos(c, (const double *const *)q, lp); /* EqOfState after the last stage (solvers.c:279) */
     for (int b = 0; b < nbodies && !err; b++)
-      if (nlist[b] > 0) err = cbo_ibm_interpolate(c, &surf[b], nlist[b], lists[b], coor, q, lp, 1, twoD, wallfunction);
+      if (nlist[b] > 0)
+        err = cbo_ibm_interpolate(c, &surf[b], nlist[b], lists[b], coor, q, lp, (const double *const *)qold, 1, twoD,
+                                  wallfunction, NULL);
     if (err) break;
     for (int a = 0; a < 5; a++) memcpy(lq[a], q[a], G.n * sizeof(double));
     memcpy(lpc, lp, G.n * sizeof(double));

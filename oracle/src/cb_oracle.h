@@ -81,6 +81,9 @@ void cbo_sigma(const cbo_config *c, double *const sig[3]);
 /* Hybrid weights with the pressure shock sensor (-calc_sigma 1), as
  * formConvectionLES sets them at istage 0 from the ghosted stage state q. */
 void cbo_sigma_sensor(const cbo_config *c, const double *const q[5], double *const sig[3]);
+/* The same from a ghosted pressure p (the lP formConvectionLES reads: after
+ * an immersed step, the pressure carried from the interpolation). */
+void cbo_sigma_sensor_p(const cbo_config *c, const double *p, double *const sig[3]);
 
 /* formRHS: q = ghosted stage state, nut/sig may be NULL when les == 0.
  * rhs: 5 padded planes; interior nodes written, every other node zeroed. */
@@ -144,11 +147,15 @@ typedef struct {
 
 /* ibm_interpolation_advanced (ibm_iso.c:2572-2880): five Jacobi sweeps over
  * the list; q (ghosted, in/out) serves as both Q and lQ, p (ghosted, in/out)
- * as P and lP, coor the node coordinates (3 padded planes).  Returns 5 for
- * the variants that are not restated (wall functions 1/2, isothermal 2). */
+ * as P and lP, coor the node coordinates (3 padded planes), qold the step's
+ * start state whose density the characteristic wall of -isothermal 2 reads
+ * (NULL: q as given).  wallfunction 0 (noslip, freeslip with -inv), 2 (the
+ * hydset log law; ustar, if not NULL, receives u_tau of every entry from the
+ * last sweep) or 3 (freeslip).  Returns 5 for wall function 1, which is not
+ * restated. */
 int cbo_ibm_interpolate(const cbo_config *c, const cbo_ibm_surface *s, int n, const cbo_ibm_info *list,
-                        const double *const coor[3], double *const q[5], double *p, int add_dundt, int twoD,
-                        int wallfunction);
+                        const double *const coor[3], double *const q[5], double *p, const double *const qold[5],
+                        int add_dundt, int twoD, int wallfunction, double *ustar);
 
 /* formRHS / FormBCS reading the local pressure lp (padded) the reference
  * carries in lP instead of the EqOfState of the stage input; cbo_formbcs_lp

@@ -10,7 +10,7 @@ compgeom.c, variables.c and wallfunction.c are compiled unmodified against the
 serial PETSc shim with the rest of the hot path (oracle/_ref).  Run from the
 repo root in a checkout that has the reference sources:
 
-    python tests/golden/make_ibm_golden.py
+    python tests/golden/make_ibm_golden.py [case ...]
 
 The reference builds a list only with -isothermal 1 or 2 (ibm_iso.c:534-760);
 the "iso0" case reuses the list of an isothermal-1 search for an
@@ -62,6 +62,14 @@ CASES = {
     # the dynamic Smagorinsky model (-les 2) around the body
     "sphere_les2_dynamic": (dict(les=2, inviscid=0, fluxorder=3, ren=400., ma=0.3, pr=0.71, dt=0.002, isothermal=1,
                                  max_cs=0.1), None, 7, 3),
+    # the shock sensor, which reads the pressure carried from the interpolation
+    # at the first stage of every step after the first
+    "sphere_les_sensor": (dict(les=1, inviscid=0, fluxorder=3, ren=400., ma=0.3, pr=0.71, dt=0.002, isothermal=1,
+                               calc_sigma=1, s_x=0.7, s_y=0.8, s_z=0.9, s_y_min=0.05, sigma_thrsh=1e-3), None, 8, 3),
+    # the characteristic isothermal wall (-isothermal 2, ibm_iso.c:2744-2786)
+    # with a wall temperature of 1.2
+    "sphere_iso2": (dict(les=0, inviscid=0, fluxorder=3, ren=300., ma=0.3, pr=0.71, dt=0.002, isothermal=2,
+                         twall=1.2), None, 9, 3),
 }
 
 
@@ -119,5 +127,6 @@ def make(name, spec):
 
 
 if __name__ == "__main__":
-    for n, s in CASES.items():
-        make(n, s)
+    # python tests/golden/make_ibm_golden.py [name ...]: the named cases, else all
+    for n in sys.argv[1:] or list(CASES):
+        make(n, CASES[n])

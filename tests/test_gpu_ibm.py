@@ -73,6 +73,15 @@ SYN = [
     ("les_noslip_periodic", {}),
     ("inviscid_iso0_kflow", dict(les=0, inviscid=1, isothermal=0, bctype=(7, 7, 7, 7, 45, 45))),
     ("visc_wf3_walls", dict(les=0, wallfunction=3, bctype=(7, 7, 3, 3, 44, 44))),
+    # the hydset log law of -wallfunction 2 (wallfunction.c:376-420): at Re
+    # 30000 the donor points sit in the log layer and beyond y+ = 300
+    ("les_wf2_loglaw", dict(wallfunction=2, ren=30000.)),
+    ("visc_wf2_walls_iso0", dict(les=0, wallfunction=2, isothermal=0, ren=3000., bctype=(7, 7, 3, 3, 44, 44))),
+    # the characteristic isothermal wall of -isothermal 2 (ibm_iso.c:2744-2786):
+    # the pressure Pa chains every entry, duplicates included, to the one
+    # walked before it; with the j walls of code 1 its FormBCS counterpart
+    ("visc_iso2_walls44", dict(les=0, isothermal=2, twall=1.2, bctype=(7, 7, 3, 3, 44, 44))),
+    ("les_iso2_jwalls1_wf2", dict(isothermal=2, twall=1.1, wallfunction=2, ren=3000., bctype=(7, 7, 1, 1, 7, 7))),
 ]
 
 
@@ -88,7 +97,9 @@ def test_synthetic_list_steps_match_oracle(name, kw):
     o.steps_immersed(3, st, met, o.fill_ghosts(O.to_padded(cfg, nv)), O.IbmSurface(surf, u, uold), info,
                      O.to_padded(cfg, coords))
     with gpu_ibm_block(cfg, coords, nv, q, surf, info, u, uold) as b:
-        assert b.ibm_count(0) == len({(a, c, d) for a, c, d in zip(info["ni"], info["nj"], info["nk"])})
+        unique = len({(a, c, d) for a, c, d in zip(info["ni"], info["nj"], info["nk"])})
+        assert b.ibm_count(0) == (info.size if cfg.isothermal == 2 else unique)
+        assert unique < info.size  # the list has duplicates
         b.RungeKutta(3)
         qd = b.Q()
         pd = b.EqOfState()
@@ -173,20 +184,14 @@ def test_invalid_lists_and_options_fail_loudly():
         bad[0]["cell"] = len(surf["nv1"])
         with pytest.raises(ChimeraError):
             b.set_ibm_list(0, bad, coords)
-        for wf in (1, 2):
-            with pytest.raises(ChimeraError) as ei:
-                b.set_ibm_options(0, wf)
-            assert ei.value.code == 5
+        with pytest.raises(ChimeraError) as ei:  # -wallfunction 1: the reference's table is undefined
+            b.set_ibm_options(0, 1)
+        assert ei.value.code == 5
+        with pytest.raises(ChimeraError) as ei:
+            b.set_ibm_options(0, 4)
+        assert ei.value.code == 1
         with pytest.raises(ChimeraError):
             b.set_ibm_surface(16, surf)  # body index out of range (CB_IBM_MAX_BODIES)
-    cfg2 = O.Config(**{**cfg.__dict__, "isothermal": 2})
-    with gpu_block(cfg2) as b:
-        b.FormMetrics(coords)
-        b.SetInitialCondition(q)
-        b.set_ibm_surface(0, surf)
-        with pytest.raises(ChimeraError) as ei:
-            b.set_ibm_list(0, info, coords)
-        assert ei.value.code == 5
 
 
 def test_sphere_workload_small_matches_oracle():
@@ -209,3 +214,47 @@ def test_sphere_workload_small_matches_oracle():
             b.RungeKutta(3)
             errs = per_field_rel_l2(b.Q(), want)
         assert max(errs) <= tol, (prec, errs)
+
+
+def test_wall_function_ustar_matches_oracle():
+    """-wallfunction 2: one interpolation (five sweeps); the state and u_tau of
+    every kept entry (cb_ibm_get_ustar: the last entry of a node listed
+    twice) against the restatement, which is bit-exact against the
+    reference (tests/test_oracle_ibm.py).  The device's log / exp may differ
+    from the host's in the last bit, so the bar is relative L2."""
+    cfg, coords, q, nv, surf, info, u, uold = _synthetic_case(seed=6, wallfunction=2, ren=30000.)
+    o = O.Oracle(cfg)
+    qp = o.fill_ghosts(O.to_padded(cfg, q))
+    p = o.eos(qp)
+    us = np.zeros(info.size)
+    o.ibm_interpolate(O.IbmSurface(surf, u, uold), info, O.to_padded(cfg, coords), qp, p, 1, ustar=us)
+    last = {}
+    for t, nd in enumerate(zip(info["ni"], info["nj"], info["nk"])):
+        last[nd] = t
+    keep = [t for t, nd in enumerate(zip(info["ni"], info["nj"], info["nk"])) if last[nd] == t]
+    with gpu_ibm_block(cfg, coords, nv, q, surf, info, u, uold) as b:
+        assert np.all(b.ibm_ustar(0) == 0)
+        b.ibm_interpolation_advanced(0, 1)
+        qd = b.Q()
+        usd = b.ibm_ustar(0)
+    assert usd.shape == (len(keep),) and np.all(usd > 0)
+    assert O.rel_l2(usd, us[keep]) <= RTOL_L2
+    assert max(per_field_rel_l2(qd, O.from_padded(qp))) <= RTOL_L2
+
+
+def test_iso2_interpolation_matches_oracle():
+    """-isothermal 2 alone (five sweeps, the chained Pa over a list with
+    duplicates and donor chains) against the restatement, which is bit-exact
+    against the reference (tests/test_oracle_ibm.py)."""
+    cfg, coords, q, nv, surf, info, u, uold = _synthetic_case(seed=11, isothermal=2, twall=1.15, les=0)
+    o = O.Oracle(cfg)
+    qp = o.fill_ghosts(O.to_padded(cfg, q))
+    p = o.eos(qp)
+    o.ibm_interpolate(O.IbmSurface(surf, u, uold), info, O.to_padded(cfg, coords), qp, p, 1)
+    with gpu_ibm_block(cfg, coords, nv, q, surf, info, u, uold) as b:
+        b.ibm_interpolation_advanced(0, 1)
+        qd = b.Q()
+        pd = b.EqOfState()
+    assert max(per_field_rel_l2(qd, O.from_padded(qp))) <= RTOL_L2
+    k, j, i = info["nk"], info["nj"], info["ni"]
+    assert O.rel_l2(pd[k, j, i], O.from_padded(p)[..., 0][k, j, i]) <= RTOL_L2

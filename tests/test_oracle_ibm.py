@@ -67,7 +67,8 @@ def test_flat_list_round_trip():
 
 def test_unsupported_variants_are_refused():
     cfg, meta, g, info, surf = load_ibm_golden(NAMES[0])
-    for kw in (dict(wallfunction=1), dict(wallfunction=2), dict(isothermal=2)):
+    # -wallfunction 1 reads a table left in a dead stack frame (wallfunction.c:113-145)
+    for kw in (dict(wallfunction=1),):
         c2 = O.Config(**{**cfg.__dict__, **kw})
         with pytest.raises(RuntimeError):
             _oracle_interp(c2, g, info, surf)
@@ -94,6 +95,16 @@ SYN_CASES = [
     ("noslip_iso1", dict(inviscid=0, isothermal=1)),
     ("freeslip_iso0", dict(inviscid=1, isothermal=0)),
     ("wf3_twoD3_iso1", dict(inviscid=0, isothermal=1, wallfunction=3, twoD=3)),
+    # the hydset log law of the wall (wallfunction.c:376-420), which takes
+    # precedence over freeslip with -inv (ibm_iso.c:2708-2728)
+    # (Re 30000 puts the donor points at y+ from 11.53 to beyond 300: the
+    # viscous sublayer, the log law and the reference's y+ > 300 fallback)
+    ("wf2_loglaw", dict(inviscid=0, isothermal=0, wallfunction=2, ren=30000.)),
+    ("wf2_sublayer_inv_iso1_twoD2", dict(inviscid=1, isothermal=1, wallfunction=2, twoD=2)),
+    # the characteristic isothermal wall (ibm_iso.c:2744-2786): the scalar Pa
+    # links each entry to the one walked before it, duplicates included
+    ("iso2_noslip", dict(inviscid=0, isothermal=2)),
+    ("iso2_twall_wf2_twoD1", dict(inviscid=0, isothermal=2, twall=1.3, wallfunction=2, twoD=1, ren=3000.)),
 ]
 
 
@@ -105,8 +116,8 @@ def test_oracle_interpolation_bitwise_vs_reference_synthetic_list(name, kw):
     n = (19, 17, 18)
     coords = W.periodic_grid(n, 2 * np.pi, amp=0.05)
     shape = coords.shape[:3]
-    cfg = O.Config(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=0, fluxorder=3, ren=300., ma=0.3, pr=0.71,
-                   dt=0.002, **kw)
+    cfg = O.Config(**{**dict(mx=n[0] + 2, my=n[1] + 2, mz=n[2] + 2, les=0, fluxorder=3, ren=300., ma=0.3, pr=0.71,
+                             dt=0.002), **kw})
     surf = W.sphere_surface(2.0, coords[shape[0] // 2, shape[1] // 2, shape[2] // 2], 2)
     info = synthetic_ibm_list(cfg, coords, len(surf["nv1"]), seed=7)
     rng = np.random.default_rng(8)
