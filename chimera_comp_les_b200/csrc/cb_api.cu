@@ -1262,8 +1262,6 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
   if (e) return e;
   if (n < 0 || (n > 0 && (!list || !coor))) return CB_E_ARG;
   if (n > 0 && !b->surf) return fail(c, CB_E_STATE, "set the body's surface first");
-  if (n > 0 && (c->cfg.bctype[4] == 52 || c->cfg.bctype[4] == 47))
-    return fail(c, CB_E_UNSUPPORTED, "immersed bodies with the inflow codes 52 and 47 are not built");
   const int m[3] = {c->cfg.mx, c->cfg.my, c->cfg.mz};
   const bool per[3] = {c->cfg.bctype[0] == 7, c->cfg.bctype[2] == 7, c->cfg.bctype[4] == 7};
   // a node listed twice keeps its last entry

@@ -70,12 +70,22 @@ CASES = {
     # with a wall temperature of 1.2
     "sphere_iso2": (dict(les=0, inviscid=0, fluxorder=3, ren=300., ma=0.3, pr=0.71, dt=0.002, isothermal=2,
                          twall=1.2), None, 9, 3),
+    # the k-lo inflow codes that read the node coordinates: the characteristic
+    # cos^2 inlet 52 with slip j walls, the power-law inlet 47 (step index)
+    "sphere_inflow52": (dict(les=1, inviscid=0, fluxorder=3, ren=400., ma=0.3, pr=0.71, dt=0.002, isothermal=1,
+                             bctype=(7, 7, 3, 3, 52, 45)), None, 10, 3),
+    "sphere_inflow47": (dict(les=0, inviscid=0, fluxorder=3, ren=400., ma=0.3, pr=0.71, dt=0.002, isothermal=1,
+                             bctype=(7, 7, 7, 7, 47, 45)), None, 11, 3),
 }
 
 
 def make(name, spec):
     kw, list_kw, seed, steps = spec
     coords = W.periodic_grid(N, 2 * np.pi, amp=0.03)
+    if kw.get("bctype", (7,) * 6)[4] in (52, 47):
+        # y from about 1 to 10.4: 47's power law (y/8)^0.1428 needs y > 0, and
+        # both of its branches (y < 8, y >= 8) are met
+        coords[..., 1] = 1.5 * coords[..., 1] + 1.0
     shape = coords.shape[:3]
     cfg = O.Config(mx=N[0] + 2, my=N[1] + 2, mz=N[2] + 2, immersed=1, **kw)
     ctr = coords[shape[0] // 2, shape[1] // 2, shape[2] // 2]
@@ -110,6 +120,7 @@ def make(name, spec):
     ref.steps(steps)
     q_steps = ref.Q()
 
+    assert np.isfinite(q_interp).all() and np.isfinite(q_steps).all(), name
     # the interpolation writes Q and P at the listed nodes only
     k, j, i = info["nk"], info["nj"], info["ni"]
     rest = np.ones(shape, dtype=bool)
