@@ -586,8 +586,6 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   if (cfg->les < 0) return bail(CB_E_ARG, "les must be >= 0");
   if (les_dynamic(*cfg) && !(cfg->max_cs >= 0.0)) return bail(CB_E_ARG, "max_cs must be >= 0");
   if (cfg->visT && !(cfg->tref > 0.0)) return bail(CB_E_ARG, "Tref must be > 0 with visT");
-  if (les_dynamic(*cfg) && cfg->twod == 1)
-    return bail(CB_E_UNSUPPORTED, "the dynamic model with twoD 1 is not built");
   c->nv0 = !cfg->visT;  // nvert starts zero; the no-IBM variants carry no Sutherland law
   if (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) return bail(CB_E_ARG, "precision must be CB_FP64 or CB_MIXED");
   if (cfg->flux != 0 && cfg->flux != 1) return bail(CB_E_ARG, "flux must be 0 (Rusanov) or 1 (Roe)");

@@ -515,7 +515,7 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
                           const double *const *qn = nullptr, const double *csp = nullptr) {
   __shared__ double us[3][3][EDDY_PN];  // [slot][component][node]
   __shared__ double stq[4][EDDY_PN];    // raw rho, rhoU, rhoV, rhoW of the plane in flight
-  __shared__ unsigned char stv[EDDY_PN];  // the staged node has a velocity source
+  __shared__ unsigned char stv[EDDY_PN];  // the staged node's velocity source: 0 none, 1 qu, 2 qn
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * EDDY_BX + tx;
   const int i0 = 1 + blockIdx.x * EDDY_BX, j0 = 1 + blockIdx.y * EDDY_BY;
   const int kb = 1 + blockIdx.z * kchunk, ke = min(c.mz - 1, kb + kchunk);
@@ -529,17 +529,21 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
       const int xi = i0 - 1 + lx, yj = j0 - 1 + ly;
       const double *const *src = nullptr;
       long long n = 0;
+      unsigned char sv = 0;
       if (xi <= c.mx - 1 && yj <= c.my - 1) {
         n = gidx(c, xi, yj, kk);
         src = qu;
+        sv = qu ? 1 : 0;
         // after the dynamic model (qn set) lUcat holds the current state's
         // velocity at interior nodes with nvert <= 1.1 (les.c:234-238)
         if (qn && xi >= 1 && xi <= c.mx - 2 && yj >= 1 && yj <= c.my - 2 && kk >= 1 && kk <= c.mz - 2 &&
-            ldg(nvert + n) <= 1.1)
+            ldg(nvert + n) <= 1.1) {
           src = qn;
+          sv = 2;
+        }
       }
       const bool v = src != nullptr;
-      stv[e] = v ? 1 : 0;
+      stv[e] = sv;
 #pragma unroll
       for (int f = 0; f < 4; f++) cp_async8(&stq[f][e], v ? src[f] + n : (const double *)nut, v);
     }
@@ -551,7 +555,9 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
       double u0 = 0., u1 = 0., u2 = 0.;
       if (stv[e]) {
         const double r = stq[0][e];
-        u0 = c.twod == 1 ? 0. : stq[1][e] / r;  // lUcat x = 0 with -twoD 1 (rhs.c:1349)
+        // lUcat x = 0 with -twoD 1 (rhs.c:1349), except where the dynamic
+        // model rewrote it from the state (les.c:255)
+        u0 = (c.twod == 1 && stv[e] == 1) ? 0. : stq[1][e] / r;
         u1 = stq[2][e] / r;
         u2 = stq[3][e] / r;
       }

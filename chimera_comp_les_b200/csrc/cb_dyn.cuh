@@ -27,7 +27,8 @@ __device__ __forceinline__ bool dyn_interior(const DevCfg &c, int i, int j, int 
 __device__ __forceinline__ double dyn_u(const DevCfg &c, const double *const *q, const double *const *qu,
                                         const double *nvert, int a, int i, int j, int k, bool reached) {
   const long long m = gidx(c, i, j, k);
-  if (reached && dyn_interior(c, i, j, k) && nvert[m] <= 1.1) return q[1 + a][m] / q[0][m];
+  if (reached && dyn_interior(c, i, j, k) && nvert[m] <= 1.1) return q[1 + a][m] / q[0][m];  // les.c:255, x kept
+  if (a == 0 && c.twod == 1) return 0.0;  // the last CalcUCat's x with -twoD 1 (rhs.c:1349)
   return qu ? qu[1 + a][m] / qu[0][m] : 0.0;
 }
 

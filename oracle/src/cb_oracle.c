@@ -1698,9 +1698,10 @@ static void dyn_periodic_copies(const cbo_config *c, const geom *G, double *f) {
  * reached, when `reached` restricts it), else the value CalcUCat left from
  * quc (zero before any CalcUCat). */
 static double dyn_u(const geom *G, const double *const q[5], const double *const quc[5], const double *nvert, int a,
-                    int i, int j, int k, int reached) {
+                    int i, int j, int k, int reached, int twod) {
   const ptrdiff_t m = IX(G, i, j, k);
-  if (reached && interior(G, i, j, k) && nvert[m] <= 1.1) return q[1 + a][m] / q[0][m];
+  if (reached && interior(G, i, j, k) && nvert[m] <= 1.1) return q[1 + a][m] / q[0][m]; /* les.c:255 ignores -twoD */
+  if (a == 0 && twod == 1) return 0.0; /* the last CalcUCat's x with -twoD 1 (rhs.c:1349) */
   return quc ? quc[1 + a][m] / quc[0][m] : 0.0;
 }
 
@@ -1773,7 +1774,6 @@ int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const
   geom G = mkgeom(c);
   const int mx = G.m[0], my = G.m[1], mz = G.m[2];
   if (!cbo_les_dynamic(c)) return 5;
-  if (c->twod == 1) return 5; /* the dynamic model with -twoD 1 is not restated */
   /* -les 3 and the homogeneous filters take LM / MM node by node and skip
    * the final 1/aj-weighted mean (les.c:916-922, 1302) */
   const int pointwise = c->i_homo_filter || c->j_homo_filter || c->k_homo_filter || c->les == 3;
@@ -1789,9 +1789,9 @@ int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const
         if (nvert[n] > 1.1) continue;
         double d[3][3];
         for (int a = 0; a < 3; a++) {
-          d[a][0] = (dyn_u(&G, q, quc, nvert, a, i + 1, j, k, 0) - dyn_u(&G, q, quc, nvert, a, i - 1, j, k, 1)) * 0.5;
-          d[a][2] = (dyn_u(&G, q, quc, nvert, a, i, j, k + 1, 0) - dyn_u(&G, q, quc, nvert, a, i, j, k - 1, 1)) * 0.5;
-          d[a][1] = (dyn_u(&G, q, quc, nvert, a, i, j + 1, k, 0) - dyn_u(&G, q, quc, nvert, a, i, j - 1, k, 1)) * 0.5;
+          d[a][0] = (dyn_u(&G, q, quc, nvert, a, i + 1, j, k, 0, c->twod) - dyn_u(&G, q, quc, nvert, a, i - 1, j, k, 1, c->twod)) * 0.5;
+          d[a][2] = (dyn_u(&G, q, quc, nvert, a, i, j, k + 1, 0, c->twod) - dyn_u(&G, q, quc, nvert, a, i, j, k - 1, 1, c->twod)) * 0.5;
+          d[a][1] = (dyn_u(&G, q, quc, nvert, a, i, j + 1, k, 0, c->twod) - dyn_u(&G, q, quc, nvert, a, i, j - 1, k, 1, c->twod)) * 0.5;
         }
         const double ajc = aj[n];
         const double c0 = csi[0][n], c1 = csi[1][n], c2 = csi[2][n];
@@ -1835,9 +1835,9 @@ int cbo_dynamic_smagorinsky(const cbo_config *c, const double *const q[5], const
               const int t = (R * 3 + Q) * 3 + P;
               const int II = i + P - 1, JJ = j + Q - 1, KK = k + R - 1;
               const ptrdiff_t m = IX(&G, II, JJ, KK);
-              u[t] = dyn_u(&G, q, quc, nvert, 0, II, JJ, KK, 1);
-              v[t] = dyn_u(&G, q, quc, nvert, 1, II, JJ, KK, 1);
-              ww[t] = dyn_u(&G, q, quc, nvert, 2, II, JJ, KK, 1);
+              u[t] = dyn_u(&G, q, quc, nvert, 0, II, JJ, KK, 1, c->twod);
+              v[t] = dyn_u(&G, q, quc, nvert, 1, II, JJ, KK, 1, c->twod);
+              ww[t] = dyn_u(&G, q, quc, nvert, 2, II, JJ, KK, 1, c->twod);
               ru[t] = q[1][m]; rv[t] = q[2][m]; rw[t] = q[3][m]; rho[t] = q[0][m];
               ruu[t] = ru[t] * u[t]; ruv[t] = ru[t] * v[t]; ruw[t] = ru[t] * ww[t];
               rvv[t] = rv[t] * v[t]; rvw[t] = rv[t] * ww[t]; rww[t] = rw[t] * ww[t];
@@ -1967,9 +1967,9 @@ void cbo_eddy_viscosity_dyn(const cbo_config *c, const double *const q[5], const
         if (nvert[n] > 0.1) { nut[n] = 0; continue; }
         double d[3][3];
         for (int a = 0; a < 3; a++) {
-          d[a][0] = (dyn_u(&G, q, quc, nvert, a, i + 1, j, k, 1) - dyn_u(&G, q, quc, nvert, a, i - 1, j, k, 1)) * 0.5;
-          d[a][1] = (dyn_u(&G, q, quc, nvert, a, i, j + 1, k, 1) - dyn_u(&G, q, quc, nvert, a, i, j - 1, k, 1)) * 0.5;
-          d[a][2] = (dyn_u(&G, q, quc, nvert, a, i, j, k + 1, 1) - dyn_u(&G, q, quc, nvert, a, i, j, k - 1, 1)) * 0.5;
+          d[a][0] = (dyn_u(&G, q, quc, nvert, a, i + 1, j, k, 1, c->twod) - dyn_u(&G, q, quc, nvert, a, i - 1, j, k, 1, c->twod)) * 0.5;
+          d[a][1] = (dyn_u(&G, q, quc, nvert, a, i, j + 1, k, 1, c->twod) - dyn_u(&G, q, quc, nvert, a, i, j - 1, k, 1, c->twod)) * 0.5;
+          d[a][2] = (dyn_u(&G, q, quc, nvert, a, i, j, k + 1, 1, c->twod) - dyn_u(&G, q, quc, nvert, a, i, j, k - 1, 1, c->twod)) * 0.5;
         }
         const double ajc = aj[n];
         const double c0 = csi[0][n], c1 = csi[1][n], c2 = csi[2][n];

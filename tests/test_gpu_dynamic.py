@@ -105,6 +105,10 @@ VARIANTS = [
     ("ijk_homo_box", dict(i_homo_filter=1, j_homo_filter=1, k_homo_filter=1), True),
     ("k_homo_pointwise", dict(k_homo_filter=1), False),
     ("les7_as_local", dict(les=7), False),
+    # -twoD 1: the model's in-place lUcat keeps x = rhoU/rho where its loop
+    # reached, CalcUCat's x = 0 elsewhere (les.c:234-238, rhs.c:1349)
+    ("twoD1", dict(twoD=1), True),
+    ("twoD1_ik_homo_planes", dict(twoD=1, i_homo_filter=1, k_homo_filter=1), False),
 ]
 
 

@@ -9,7 +9,6 @@ import numpy as np
 import pytest
 
 import oracle as O
-from chimera_comp_les_b200 import ChimeraError
 from chimera_comp_les_b200 import workloads as W
 
 from _common import RTOL_L2, gpu_block, oracle_run, per_field_rel_l2
@@ -78,10 +77,3 @@ def test_twoD1_batch_equals_single_block():
             blk.SetInitialCondition(q)
             blk.RungeKutta(3)
             assert np.array_equal(g, blk.Q())
-
-
-def test_twoD1_with_the_dynamic_model_is_refused():
-    cfg = O.Config(mx=18, my=16, mz=14, les=2, inviscid=0, twoD=1)
-    with pytest.raises(ChimeraError) as ei:
-        gpu_block(cfg)
-    assert ei.value.code == 5

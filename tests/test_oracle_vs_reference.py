@@ -196,6 +196,10 @@ DYN_VARIANTS = [
     ("j_homo_pointwise", dict(j_homo_filter=1)),
     ("k_homo_ik_filter", dict(k_homo_filter=1, testfilter_ik=1)),
     ("les7_as_local", dict(les=7)),
+    # -twoD 1: les.c rewrites lUcat from the state without zeroing x, so only
+    # the nodes its loop has not reached keep CalcUCat's x = 0
+    ("twoD1", dict(twoD=1)),
+    ("twoD1_ik_homo_planes", dict(twoD=1, i_homo_filter=1, k_homo_filter=1)),
 ]
 
 
