@@ -66,7 +66,7 @@ template <bool LES, bool VISC>
 void na_launch_rhs(const DevCfg &dc, const DevFields &F, int kchunk, cudaStream_t s) {
   const int nkin = dc.mz - 2;
   dim3 grid((dc.mx - 2 + SBX - 1) / SBX, (dc.my - 2 + SBY - 1) / SBY, (nkin + kchunk - 1) / kchunk);
-  stage_kernel<double, false, LES, VISC, true><<<grid, SNT, STAGE_SMEM_BYTES, s>>>(dc, F, 0, 0., 0., 0., kchunk);
+  stage_kernel<double, false, LES, VISC, true><<<grid, StageThreads<0, false>::N, STAGE_SMEM_BYTES, s>>>(dc, F, 0, 0., 0., 0., kchunk);
 }
 
 int na_fail(int code, const char *msg) {

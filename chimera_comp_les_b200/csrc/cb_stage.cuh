@@ -77,6 +77,18 @@ struct StageGeo {
   static_assert(NXF <= NT && NYF <= NT && NZF <= NT, "one face direction per round of the schedule");
 };
 
+// Threads of a stage-kernel block.  The FP64 form runs two threads per face:
+// the first NT compute the faces' inviscid fluxes, the next NT their viscous
+// and SGS fluxes, so each thread holds half the live FP64 values and a block
+// of 2 NT threads fits the register file (16 warps per SM at 32 x 7 instead of
+// 8).  The mixed form keeps one thread per face and two blocks per SM.
+template <int FLUX, bool MIX>
+struct StageThreads {
+  static constexpr bool SPLIT = !MIX;
+  static constexpr int N = StageGeo<FLUX>::NT * (SPLIT ? 2 : 1);
+  static constexpr int MIN_BLOCKS = MIX ? 2 : 1;
+};
+
 // Selections by a runtime direction d without dynamic indexing (which would
 // place the indexed array in local memory).
 template <typename R>
@@ -743,6 +755,31 @@ __device__ __forceinline__ void face_flux(const DevCfg &c, const DevFields &F, c
   G[AOFF] = A[0]; G[AOFF + 1] = A[1]; G[AOFF + 2] = A[2];
 }
 
+// The inviscid half (G[0..4]) or the viscous and SGS half (G[VOFF..VOFF+4],
+// G[AOFF..AOFF+2]) of face_flux, for the FP64 form's two threads per face;
+// the same calls, so the same values.
+template <typename R, bool MIX, bool LES, bool VISC, class RG, int DIR, int FLUX = 0, bool NV0 = false>
+__device__ __forceinline__ void face_flux_half(const DevCfg &c, const DevFields &F, const RG &Rg, NRef a, int fi,
+                                               int fj, int k, int drt, int role, R *G) {
+  constexpr int VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
+  static_assert(!MIX, "the mixed form stores visc - conv per face");
+  if (role == 0) {
+    conv_face<R, MIX, LES, RG, DIR, FLUX, NV0>(c, F, Rg, a, fi, fj, k, drt, G);
+  } else {
+    R Fv[5], A[3];
+    if (VISC) {
+      visc_face<R, MIX, LES, RG, DIR, NV0>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 5; q++) Fv[q] = R(0.);
+      A[0] = A[1] = A[2] = R(0.);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; q++) G[VOFF + q] = Fv[q];
+    G[AOFF] = A[0]; G[AOFF + 1] = A[1]; G[AOFF + 2] = A[2];
+  }
+}
+
 // ---------------------------------------------------------- the kernel ----
 // Tile of 32 x BY interior nodes, NT = 32 (BY + 1) threads (StageGeo).  Per
 // plane the block computes 33*BY i-faces, 32*(BY+1) j-faces and 32*BY k-faces
@@ -785,10 +822,15 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
                                             R *gxb, R *gyb, R *gzb) {
   using G = StageGeo<FLUX>;
   constexpr int BX = G::BX, NT = G::NT, NG = FaceWidth<MIX>::NG;
+  constexpr bool SPLIT = StageThreads<FLUX, MIX>::SPLIT;
+  constexpr int VOFF = FaceWidth<MIX>::VOFF;
   const int tid = threadIdx.x;
+  // role 0: the faces' inviscid fluxes; role 1 (FP64 form): their viscous
+  // and SGS fluxes (warp-uniform: NT is a multiple of 32)
+  const int role = SPLIT ? tid / NT : 0;
 #pragma unroll 1
   for (int r = ZONLY ? 2 : 0; r < 3; r++) {
-    const int u = tid;  // face index within this round's direction
+    const int u = SPLIT ? tid - role * NT : tid;  // face index within this round's direction
     int d, fi, fj;
     NRef a;
     R *dst;
@@ -817,7 +859,22 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
     }
     R Gf[NG];
     // -twoD 1 forms no i-face flux (rhs.c:1487, 2646, 3465): it stays zero
-    if (fi <= c.mx - 2 && fj <= c.my - 2 && !(d == 0 && c.twod == 1)) {
+    const bool live = fi <= c.mx - 2 && fj <= c.my - 2 && !(d == 0 && c.twod == 1);
+    if constexpr (SPLIT) {
+      // this thread's half of the face: G[0..4], or G[VOFF..NG-1]
+      const int q0 = role == 0 ? 0 : VOFF, q1 = role == 0 ? VOFF : NG;
+      if (live) {
+        face_flux_half<R, MIX, LES, VISC, RG, -1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
+      } else {
+#pragma unroll
+        for (int q = 0; q < NG; q++) Gf[q] = R(0.);
+      }
+#pragma unroll
+      for (int q = 0; q < NG; q++)
+        if (q >= q0 && q < q1) dst[(size_t)q * nslot + u] = Gf[q];
+      continue;
+    }
+    if (live) {
       if (MIX) {
         // one instantiation per direction (d is warp-uniform): 16 % faster
         // for the FP32 arithmetic of the mixed form
@@ -837,6 +894,7 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
     for (int q = 0; q < NG; q++) dst[(size_t)q * nslot + u] = Gf[q];
   }
   (void)NT;
+  (void)VOFF;
 }
 
 
@@ -846,7 +904,8 @@ template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0
 __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, int bxi, int byi, int kb, int ke,
                                            int istage, double alfa, double beta, double adt, double *smem_d) {
   using G = StageGeo<FLUX>;
-  constexpr int BX = G::BX, BY = G::BY, NT = G::NT, NPL = G::NPL, H = G::H;
+  constexpr int BX = G::BX, BY = G::BY, NPL = G::NPL, H = G::H;
+  constexpr int NT = StageThreads<FLUX, MIX>::N;  // threads of the block
   constexpr int PX = G::Tile::PX, PN = G::Tile::PN, NXF = G::NXF, NYF = G::NYF, NZF = G::NZF;
   constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
   constexpr int NSTG = StageSmem<R, MIX, NV0, G::W5>::NSTG;
@@ -1088,7 +1147,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 // its range with its own prologue.  Every node gets the same arithmetic in
 // both shapes (a chunk start recomputes its first k-face from the same data).
 template <typename R, bool MIX, bool LES, bool VISC, bool RHS_MODE, int FLUX = 0, bool NV0 = false>
-static __global__ void __launch_bounds__(StageGeo<FLUX>::NT, MIX ? 2 : 1)
+static __global__ void __launch_bounds__(StageThreads<FLUX, MIX>::N, StageThreads<FLUX, MIX>::MIN_BLOCKS)
     stage_kernel(const DevCfg c, const DevFields F, int istage, double alfa, double beta, double adt, int kchunk) {
   extern __shared__ double smem_d[];
   constexpr int BY = StageGeo<FLUX>::BY;
@@ -1148,7 +1207,10 @@ StageKern stage_gen_kernel(int fl) {
   }
 }
 // Threads and dynamic shared memory of a stage-kernel launch for FLUX bits fl.
-inline int stage_threads(int fl) { return (fl & FLUX_W5) ? SNT_W5 : SNT; }
+template <bool MIX>
+inline int stage_threads(int fl) {
+  return (fl & FLUX_W5) ? StageThreads<FLUX_W5, MIX>::N : StageThreads<0, MIX>::N;
+}
 template <typename R, bool MIX>
 size_t stage_smem_for(int fl, bool nv0) {
   const bool w5 = (fl & FLUX_W5) != 0;
@@ -1185,7 +1247,7 @@ struct BatchBlock {
 };
 
 template <typename R, bool MIX, bool LES, bool VISC, bool NV0 = false, int FLUX = 0>
-static __global__ void __launch_bounds__(StageGeo<FLUX>::NT, MIX ? 2 : 1)
+static __global__ void __launch_bounds__(StageThreads<FLUX, MIX>::N, StageThreads<FLUX, MIX>::MIN_BLOCKS)
     stage_batched_kernel(const BatchBlock *__restrict__ blocks, const int2 *__restrict__ items, int nitems,
                          unsigned *__restrict__ counter, int istage, double alfa, double beta, double adt) {
   extern __shared__ double smem_d[];

@@ -43,7 +43,7 @@ void launch_one(const DevCfg &c, const DevFields &F, int istage, double alfa, do
   const bool nv = !RHSM && nv0;
   if constexpr (!RHSM)
     if (nv0) kern = stage_nv0_kernel<R, MIX, LES, VISC>(fl);
-  kern<<<stage_grid(c, kchunk, slots, stage_tile_rows(fl)), stage_threads(fl), stage_smem_for<R, MIX>(fl, nv), s>>>(
+  kern<<<stage_grid(c, kchunk, slots, stage_tile_rows(fl)), stage_threads<MIX>(fl), stage_smem_for<R, MIX>(fl, nv), s>>>(
       c, F, istage, alfa, beta, adt, kchunk);
 }
 }  // namespace
@@ -124,7 +124,7 @@ cudaError_t BatchLaunch<R, MIX, LES>::launch(const BatchBlock *tab, const int2 *
                                              int istage, double alfa, double beta, double adt, bool visc, int fl,
                                              bool nv0, int ctas, cudaStream_t s) {
   auto kern = visc ? batched_kernel<R, MIX, LES, true>(fl, nv0) : batched_kernel<R, MIX, LES, false>(fl, nv0);
-  kern<<<ctas, stage_threads(fl), stage_smem_for<R, MIX>(fl, nv0), s>>>(tab, items, nitems, counter, istage, alfa, beta,
+  kern<<<ctas, stage_threads<MIX>(fl), stage_smem_for<R, MIX>(fl, nv0), s>>>(tab, items, nitems, counter, istage, alfa, beta,
                                                                        adt);
   return cudaGetLastError();
 }
