@@ -99,6 +99,13 @@ __device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc, bool val
   const int sz = valid ? 8 : 0;  // src-size 0 zero-fills the destination
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(sz) : "memory");
 }
+// 16-byte asynchronous global -> shared copy through L2 only (both addresses
+// 16-byte aligned; valid false: zero-fill, nothing read)
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(sz) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 

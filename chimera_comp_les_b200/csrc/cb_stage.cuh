@@ -89,6 +89,17 @@ struct StageThreads {
   static constexpr int MIN_BLOCKS = MIX ? 2 : 1;
 };
 
+// The mixed form's no-IBM MUSCL/WENO3 variants read the FP32 metric vectors
+// and nu_t of the current plane from a shared-memory slot that the block
+// fills with 16-byte cp.async copies one plane ahead of use, instead of about
+// 18 metric loads per node through the L1; only the k-faces' far node (plane
+// k+1) is still read from global memory.  The kernel reads the same values
+// either way.
+template <bool MIX, bool NV0, int FLUX>
+struct StageMet {
+  static constexpr bool on = MIX && NV0 && (FLUX & FLUX_W5) == 0;
+};
+
 // Selections by a runtime direction d without dynamic indexing (which would
 // place the indexed array in local memory).
 template <typename R>
@@ -142,6 +153,14 @@ struct Ring {
   static constexpr int H = (NPL - 2) / 2;  // ring planes below the current one
   R *pl;
   const unsigned char *nvc;  // [NPL][PN] nvert * 4 (exact when DevCfg::nvq)
+  // mixed no-IBM variants (StageMet): the FP32 metric vectors [3][MPN] and
+  // nu_t [MPN] of the current plane over the (BX+2) x (BY+2) node box that
+  // starts one node before the tile in i and j (every face's two nodes)
+  static constexpr int MPX = BX + 2, MPY = BY + 2, MPN = MPX * MPY;
+  const float4 *mt;
+  const double *nt;
+  __device__ __forceinline__ float4 met(int e, NRef n) const { return mt[e * MPN + (n.y - 1) * MPX + (n.x - 1)]; }
+  __device__ __forceinline__ double nut(NRef n) const { return nt[(n.y - 1) * MPX + (n.x - 1)]; }
   // slot of relative plane r (-H .. NPL-H-1) is sb + r + H modulo NPL, with
   // sb the slot of the lowest plane: a rotation, no table
   int sb;
@@ -409,7 +428,18 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   const double nvm = nvert_v<NV0>(c, F, Rg, nshift(a, d, -1), g0 - sd), nv0 = nvert_v<NV0>(c, F, Rg, a, g0),
                nv1 = nvert_v<NV0>(c, F, Rg, nshift(a, d, 1), g0 + sd),
                nv2 = nvert_v<NV0>(c, F, Rg, nshift(a, d, 2), g0 + 2 * sd);
-  const MetV<R> m0 = met_load<R, MIX>(F, d, g0), m1 = met_load<R, MIX>(F, d, g0 + sd);
+  constexpr bool SMET = StageMet<MIX, NV0, FLUX>::on;
+  MetV<R> m0, m1;
+  if constexpr (SMET) {
+    static_assert(DIR >= 0, "the metric slot needs the face direction at compile time");
+    const float4 a0 = Rg.met(d, a);
+    const float4 a1 = d < 2 ? Rg.met(d, nshift(a, d, 1)) : __ldg(F.met4[2] + g0 + sd);  // k-face: plane k+1
+    m0 = MetV<R>{R(a0.x), R(a0.y), R(a0.z), R(a0.w)};
+    m1 = MetV<R>{R(a1.x), R(a1.y), R(a1.z), R(a1.w)};
+  } else {
+    m0 = met_load<R, MIX>(F, d, g0);
+    m1 = met_load<R, MIX>(F, d, g0 + sd);
+  }
   R h[3];
   h[0] = R(0.5) * (m0.x + m1.x);
   h[1] = R(0.5) * (m0.y + m1.y);
@@ -585,9 +615,12 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
 // -------------------------------------------------------- viscous face ----
 __device__ __forceinline__ bool blocked(double v) { return v > SOLID && v < INNERBLANK; }
 
-template <typename R, bool MIX, bool LES, class RG, int DIR, bool NV0 = false>
+// SMET: the metric vectors and nu_t of the face's plane-k nodes come from the
+// block's shared-memory slot (StageMet)
+template <typename R, bool MIX, bool LES, class RG, int DIR, bool NV0 = false, bool SMET = false>
 __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, const RG &Rg, NRef a,
                                           int gi, int gj, int gk, int drt, R Fv[5], R A[3]) {
+  static_assert(!SMET || (MIX && DIR >= 0), "the metric slot holds FP32 vectors, selected at compile time");
   const int d = DIR >= 0 ? DIR : drt;
   const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d), g1 = g0 + sd;
   const int pos = d == 0 ? gi : (d == 1 ? gj : gk);
@@ -633,7 +666,16 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   R w0[2], w1[2];  // mixed form: filter width and aj at g0 / g1
 #pragma unroll
   for (int e = 0; e < 3; e++) {
-    const MetV<R> p0 = met_load<R, MIX>(F, e, g0), p1 = met_load<R, MIX>(F, e, g1);
+    MetV<R> p0, p1;
+    if constexpr (SMET) {
+      const float4 a0 = Rg.met(e, a);
+      const float4 a1 = d < 2 ? Rg.met(e, b) : __ldg((e == 0 ? F.met4[0] : (e == 1 ? F.met4[1] : F.met4[2])) + g1);
+      p0 = MetV<R>{R(a0.x), R(a0.y), R(a0.z), R(a0.w)};
+      p1 = MetV<R>{R(a1.x), R(a1.y), R(a1.z), R(a1.w)};
+    } else {
+      p0 = met_load<R, MIX>(F, e, g0);
+      p1 = met_load<R, MIX>(F, e, g1);
+    }
     mh[e][0] = R(0.5) * (p0.x + p1.x);
     mh[e][1] = R(0.5) * (p0.y + p1.y);
     mh[e][2] = R(0.5) * (p0.z + p1.z);
@@ -709,7 +751,9 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
     const R sa = R(sigma_at(c, F, d, gi, gj, gk));
     const int bi = gi + (d == 0), bj = gj + (d == 1), bk = gk + (d == 2);
     const R sb = R(sigma_at(c, F, d, bi, bj, bk));
-    R nut = R(0.5) * (R(ldg(F.nut + g0)) * sa + R(ldg(F.nut + g1)) * sb);
+    const double nu0 = SMET ? Rg.nut(a) : ldg(F.nut + g0);
+    const double nu1 = (SMET && d < 2) ? Rg.nut(b) : ldg(F.nut + g1);
+    R nut = R(0.5) * (R(nu0) * sa + R(nu1) * sb);
     const R rho_c = R(0.5) * (Rg.get(F_RHO, a) + Rg.get(F_RHO, b));
     const R sigma_c = R(0.5) * (sa + sb);
     if ((bc_lo(c, d) == 1 && pos == 0) || (bc_hi(c, d) == 1 && pos == m - 2)) nut = R(0);
@@ -739,7 +783,7 @@ __device__ __forceinline__ void face_flux(const DevCfg &c, const DevFields &F, c
   R Fc[5], Fv[5], A[3];
   conv_face<R, MIX, LES, RG, DIR, FLUX, NV0>(c, F, Rg, a, fi, fj, k, drt, Fc);
   if (VISC) {
-    visc_face<R, MIX, LES, RG, DIR, NV0>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
+    visc_face<R, MIX, LES, RG, DIR, NV0, StageMet<MIX, NV0, FLUX>::on>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
   } else {
 #pragma unroll
     for (int q = 0; q < 5; q++) Fv[q] = R(0.);
@@ -798,10 +842,20 @@ struct StageSmem {
   // interpolation (the mixed form keeps that shared memory as L1: the carried
   // value differs from the EOS by <= 1e-12, inside its bar)
   static constexpr int NSTG = 5 + (NV0 ? 0 : 1) + (MIX ? 0 : 1);
-  // ring + face buffers, FP64 staging of the next plane, nvert byte ring
-  // [NPL][PN] (not with NV0: the no-IBM variants leave that memory to the L1)
-  static constexpr size_t bytes = sizeof(R) * ((size_t)G::NPL * NF * PN + (size_t)NG * (G::NXF + G::NYF + G::NZF)) +
-                                  sizeof(double) * (size_t)NSTG * PN + (NV0 ? 0 : (size_t)G::NPL * PN);
+  // the metric / nu_t slot of the current plane (StageMet): [3][MPN] float4
+  // and [MPN] double
+  static constexpr bool SMET = StageMet<MIX, NV0, W5 ? FLUX_W5 : 0>::on;
+  static constexpr int MPN = (G::BX + 2) * (G::BY + 2);
+  static constexpr size_t MET_BYTES = SMET ? (size_t)MPN * (3 * sizeof(float4) + sizeof(double)) : 0;
+  // FP64 staging of the next plane, metric slot, ring, face buffers (with the
+  // metric slot the k-faces stay in registers: the thread that forms a k-face
+  // is the thread that updates its node), nvert byte ring [NPL][PN] (not with
+  // NV0: the no-IBM variants leave that memory to the L1)
+  static constexpr size_t bytes =
+      sizeof(double) * (size_t)NSTG * PN + MET_BYTES +
+      sizeof(R) * ((size_t)G::NPL * NF * PN + (size_t)NG * (G::NXF + G::NYF + (SMET ? 0 : G::NZF))) +
+      (NV0 ? 0 : (size_t)G::NPL * PN);
+  static_assert((sizeof(double) * NSTG * PN) % 16 == 0, "the metric slot takes 16-byte copies");
 };
 constexpr size_t STAGE_SMEM_BYTES = StageSmem<double, false>::bytes;
 constexpr size_t STAGE_SMEM_BYTES_MIXED = StageSmem<float, true>::bytes;
@@ -812,14 +866,18 @@ static_assert(STAGE_SMEM_BYTES <= 232448, "shared memory budget of one block");
 static_assert(StageSmem<double, false, false, true>::bytes <= 232448, "WENO5 FP64: shared memory of one block");
 static_assert(2 * (STAGE_SMEM_BYTES_MIXED + 1024) <= 233472, "mixed form: two blocks per SM");
 static_assert(2 * (StageSmem<float, true, false, true>::bytes + 1024) <= 233472, "WENO5 mixed: two blocks per SM");
+static_assert(2 * (StageSmem<float, true, true, false>::bytes + 1024) <= 233472, "mixed with the metric slot: two blocks per SM");
 
 // All face fluxes of plane k of a tile into the face buffers (ZONLY: just the
 // k-faces, for the prologue).  A function rather than a lambda so that it is
 // always inlined: an outlined call would copy the kernel parameters to local
 // memory.
+// With the metric slot (StageMet) the k-face comes back in gzr (registers:
+// thread u of the k round is the thread that updates node u); otherwise it
+// goes to gzb (the FP64 form forms the two halves of a face in two threads).
 template <typename R, bool MIX, bool LES, bool VISC, bool ZONLY, int FLUX, bool NV0, class RG>
 __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F, const RG &Rg, int i0, int j0, int k,
-                                            R *gxb, R *gyb, R *gzb) {
+                                            R *gxb, R *gyb, R *gzb, R *gzr) {
   using G = StageGeo<FLUX>;
   constexpr int BX = G::BX, NT = G::NT, NG = FaceWidth<MIX>::NG;
   constexpr bool SPLIT = StageThreads<FLUX, MIX>::SPLIT;
@@ -875,7 +933,7 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
       continue;
     }
     if (live) {
-      if (MIX) {
+      if constexpr (MIX) {
         // one instantiation per direction (d is warp-uniform): 16 % faster
         // for the FP32 arithmetic of the mixed form
         if (d == 0) face_flux<R, MIX, LES, VISC, RG, 0, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, Gf);
@@ -890,11 +948,17 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
 #pragma unroll
       for (int q = 0; q < NG; q++) Gf[q] = R(0.);
     }
+    if (StageMet<MIX, NV0, FLUX>::on && r == 2) {
+#pragma unroll
+      for (int q = 0; q < NG; q++) gzr[q] = Gf[q];
+      continue;
+    }
 #pragma unroll
     for (int q = 0; q < NG; q++) dst[(size_t)q * nslot + u] = Gf[q];
   }
   (void)NT;
   (void)VOFF;
+  (void)gzb;
 }
 
 
@@ -910,14 +974,20 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   constexpr int NG = FaceWidth<MIX>::NG, VOFF = FaceWidth<MIX>::VOFF, AOFF = FaceWidth<MIX>::AOFF;
   constexpr int NSTG = StageSmem<R, MIX, NV0, G::W5>::NSTG;
   using RG = Ring<R, BX, BY, NPL>;
+  constexpr bool SMET = StageMet<MIX, NV0, FLUX>::on;
+  constexpr int MPX = RG::MPX, MPN = RG::MPN;
   double *stg = smem_d;  // [NSTG][PN] raw FP64 Q, nvert and carried pressure of the next plane
-  R *smem = reinterpret_cast<R *>(smem_d + (size_t)NSTG * PN);
+  float4 *mts = reinterpret_cast<float4 *>(smem_d + (size_t)NSTG * PN);  // [3][MPN] metric slot (SMET)
+  double *nts = reinterpret_cast<double *>(mts + (SMET ? 3 * MPN : 0));   // [MPN] nu_t slot (SMET)
+  R *smem = reinterpret_cast<R *>(nts + (SMET ? MPN : 0));
   RG Rg;
   Rg.pl = smem;
+  Rg.mt = mts;
+  Rg.nt = nts;
   R *gxb = smem + (size_t)NPL * NF * PN;  // [NG][NXF]
   R *gyb = gxb + (size_t)NG * NXF;        // [NG][NYF]
-  R *gzb = gyb + (size_t)NG * NYF;        // [NG][NZF]
-  unsigned char *nvc = reinterpret_cast<unsigned char *>(gzb + (size_t)NG * NZF);  // [NPL][PN]
+  R *gzb = gyb + (size_t)NG * NYF;        // [NG][NZF] (not with the metric slot)
+  unsigned char *nvc = reinterpret_cast<unsigned char *>(gzb + (SMET ? 0 : (size_t)NG * NZF));  // [NPL][PN]
   Rg.nvc = nvc;
   // staged fields per plane: Q, then nvert (byte-exact codes), then lP (carried pressure)
   const bool pst = !MIX && F.pin != nullptr;
@@ -991,6 +1061,22 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       if (nvs) nvc[s * PN + idx] = (unsigned char)(stg[5 * PN + idx] * 4.0);
     }
   };
+  // async copy of plane kk's FP32 metric vectors and nu_t over the slot's
+  // node box into the slot (SMET)
+  auto issue_met = [&](int kk) {
+    if constexpr (SMET) {
+      for (int idx = tid; idx < MPN; idx += NT) {
+        const int ly = idx / MPX, lx = idx - ly * MPX;
+        const int xi = i0 - 1 + lx, yj = j0 - 1 + ly;
+        const bool ok = xi <= c.mx + 1 && yj <= c.my + 1;
+        const long long go = ok ? gidx(c, xi, yj, kk) : 0;  // src-size 0 below: nothing is read
+#pragma unroll
+        for (int e = 0; e < 3; e++) cp_async16(mts + e * MPN + idx, F.met4[e] + go, ok);
+        if (LES) cp_async8(nts + idx, F.nut + go, ok);
+      }
+      cp_async_commit();
+    }
+  };
   auto load_plane_sync = [&](int kk, int s) {
     issue_stage(kk);
     cp_async_wait_all();
@@ -1002,14 +1088,17 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   // prologue: planes kb-1-H .. kb+H in slots 0 .. NPL-1, k-face kb-1/2 (its
   // stencil is exactly those planes), then plane kb+H+1 into slot 0
   Rg.sb = 0;
+  issue_met(kb - 1);  // the metric slot holds plane kb-1 for the prologue's k-face
 #pragma unroll 1
   for (int t = 0; t < NPL; t++) load_plane_sync(kb - 1 - H + t, t);
-  plane_faces<R, MIX, LES, VISC, true, FLUX, NV0>(c, F, Rg, i0, j0, kb - 1, gxb, gyb, gzb);  // k-face kb-1/2
+  R gzr[NG];  // with the metric slot: k-face k+1/2 of the node this thread updates
+  plane_faces<R, MIX, LES, VISC, true, FLUX, NV0>(c, F, Rg, i0, j0, kb - 1, gxb, gyb, gzb, gzr);  // k-face kb-1/2
   __syncthreads();
   R Gzp[NG];  // k-face k-1/2 of the node this thread updates
 #pragma unroll
-  for (int q = 0; q < NG; q++) Gzp[q] = uact ? gzb[(size_t)q * NZF + tid] : R(0.);
+  for (int q = 0; q < NG; q++) Gzp[q] = uact ? (SMET ? gzr[q] : gzb[(size_t)q * NZF + tid]) : R(0.);
   __syncthreads();
+  issue_met(kb);
   load_plane_sync(kb + H + 1, 0);
   int base = 1;  // slot of plane k-H
 
@@ -1017,7 +1106,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
     Rg.sb = base;
     const bool more = k + 1 < ke;
     if (more) issue_stage(k + H + 2);  // overlaps the face computation
-    plane_faces<R, MIX, LES, VISC, false, FLUX, NV0>(c, F, Rg, i0, j0, k, gxb, gyb, gzb);
+    plane_faces<R, MIX, LES, VISC, false, FLUX, NV0>(c, F, Rg, i0, j0, k, gxb, gyb, gzb, gzr);
     // the only plane k-1 value the update needs, read before that slot is refilled
     const NRef n{0, uty + 2, utx + 2};
     const R rho_km1 = (LES && VISC && uact) ? Rg.get(F_RHO, nshift(n, 2, -1)) : R(0.);
@@ -1035,7 +1124,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
         for (int q = 0; q < 5; q++) qo_r[q] = ldg(F.qold[q] + g);
       }
       if (MIX) {
-        if (!RHS_MODE) {
+        if (!RHS_MODE && istage != 0) {  // the first stage's combine has no Q term
 #pragma unroll
           for (int q = 0; q < 5; q++) qi_r[q] = ldg(F.q[q] + g);
         }
@@ -1045,6 +1134,9 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
     }
     cp_async_wait_all();
     __syncthreads();
+    // the faces are done with the metric slot: plane k+1's copies land during
+    // the update and the derive pass
+    if (more) issue_met(k + 1);
 
     if (uact) {
       const double nv = nvert_v<NV0>(c, F, Rg, n, g);
@@ -1055,7 +1147,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
       // ((((F_i - F_i-1) + F_j) - F_j-1) + F_k) - F_k-1
       auto fdiff = [&](int q) {
         return gxb[(size_t)q * NXF + fxr] - gxb[(size_t)q * NXF + fxl] + gyb[(size_t)q * NYF + fyu] -
-               gyb[(size_t)q * NYF + fyd] + gzb[(size_t)q * NZF + fz] - Gzp[q];
+               gyb[(size_t)q * NYF + fyd] + (SMET ? gzr[q] : gzb[(size_t)q * NZF + fz]) - Gzp[q];
       };
       // LES energy term (rhs.c:2153-2197): u . sum of rho_face * stress differences
       auto les_energy = [&]() -> R {
@@ -1069,7 +1161,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
           const int a = AOFF + q;
           const R t = rR * gxb[(size_t)a * NXF + fxr] - rL * gxb[(size_t)a * NXF + fxl] +
                       rU * gyb[(size_t)a * NYF + fyu] - rD * gyb[(size_t)a * NYF + fyd] +
-                      rF * gzb[(size_t)a * NZF + fz] - rB * Gzp[a];
+                      rF * (SMET ? gzr[a] : gzb[(size_t)a * NZF + fz]) - rB * Gzp[a];
           e = (q == 0) ? Rg.get(F_U + q, n) * t : e + Rg.get(F_U + q, n) * t;
         }
         return e;
@@ -1132,10 +1224,11 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
         if (st) atomicOr(F.status, st);
       }
 #pragma unroll
-      for (int q = 0; q < NG; q++) Gzp[q] = gzb[(size_t)q * NZF + fz];
+      for (int q = 0; q < NG; q++) Gzp[q] = SMET ? gzr[q] : gzb[(size_t)q * NZF + fz];
     }
     if (more) derive(base);  // plane k+H+2 into the slot of plane k-H
     base = base + 1 == NPL ? 0 : base + 1;
+    if (SMET) cp_async_wait_all();  // the metric slot of plane k+1
     __syncthreads();
   }
 }
