@@ -611,6 +611,7 @@ int cb_create(const cb_config *cfg, cb_ctx **out) {
   d.inv_ren_half = 1. / cfg->ren * 0.5;
   set_sutherland(d, cfg->visT, cfg->tref, cfg->ren, cfg->gamma, cfg->ma);
   d.gm1 = cfg->gamma - 1.0;
+  d.kheat = cfg->gamma / cfg->pr / (cfg->gamma - 1.0);
   d.nvq = 1;  // nvert starts zero
   if ((long long)(cfg->mx + 4) * (cfg->my + 4) * (cfg->mz + 4) >= (1LL << 31))
     return bail(CB_E_ARG, "grid too large for 32-bit boundary indexing");

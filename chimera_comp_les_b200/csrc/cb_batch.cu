@@ -328,6 +328,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     set_sutherland(d, cfg->visT, cfg->tref, cfg->ren, cfg->gamma, cfg->ma);
     d.twod = cfg->twod;  // -twoD 1: no i-face fluxes
     d.gm1 = cfg->gamma - 1.0;
+    d.kheat = cfg->gamma / cfg->pr / (cfg->gamma - 1.0);
     d.nvq = 1;  // nvert starts zero
     d.calc_sigma = (cfg->les && cfg->calc_sigma) ? 1 : 0;
     d.s_x_min = cfg->s_x_min; d.s_y_min = cfg->s_y_min; d.s_z_min = cfg->s_z_min;

@@ -28,6 +28,7 @@ struct DevCfg {
   double inv_ren;       // 1./ren
   double inv_ren_half;  // 1./ren*0.5
   double gm1;           // gamma-1.0
+  double kheat;         // gamma / Pr / (gamma - 1): the mixed form's heat-flux factor
   // mixed form: reference state subtracted before FP32 rounding
   double p_ref, e_ref, t_ref, h_ref;  // h_ref = e_ref + p_ref
   // 1: every nvert value is k/4 with 0 <= k <= 255, so the stage kernel keeps

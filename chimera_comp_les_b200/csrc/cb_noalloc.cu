@@ -110,6 +110,7 @@ extern "C" int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const 
   set_sutherland(d, cfg->visT, cfg->tref, cfg->ren, cfg->gamma, cfg->ma);
   d.twod = cfg->twod;  // -twoD 1: no i-face fluxes
   d.gm1 = cfg->gamma - 1.0;
+  d.kheat = cfg->gamma / cfg->pr / (cfg->gamma - 1.0);
   d.nvq = 0;  // nvert is a caller-owned device array: read it from global memory
   d.flux = 0;
 

@@ -195,13 +195,14 @@ __device__ __forceinline__ double nvert_far(const DevCfg &c, const DevFields &F,
 }
 
 // ---------------------------------------------------------------- recon --
-template <typename R>
-__device__ __forceinline__ R r_sgn(R a) { return (a >= R(0)) ? ((a == R(0)) ? R(0.) : R(1.)) : R(-1.); }
+// minmod (rhs.c:2256-2307): 0 where a and b have opposite signs, else
+// sgn(a) * min(|a|, |b|), formed here branch-free as the smaller magnitude
+// with the sign of a -- the same value (a zero slope may come out as -0,
+// which the MUSCL sum q0 +- 0.5 * slope absorbs)
 template <typename R>
 __device__ __forceinline__ R r_minmod(R a, R b) {
-  if (a * b < R(0)) return R(0.);
-  R fa = fabs(a), fb = fabs(b);
-  return r_sgn(a) * ((fa < fb) ? fa : fb);
+  const R m = copysign(fmin(fabs(a), fabs(b)), a);
+  return (a * b < R(0)) ? R(0.) : m;
 }
 template <typename R>
 __device__ __forceinline__ R muscl_l(R qm, R q0, R qp) { return q0 + R(0.5) * r_minmod(qp - q0, q0 - qm); }
@@ -289,14 +290,27 @@ __device__ __forceinline__ void node_qp(const DevCfg &c, const double v[5], bool
 // order as the reference (divisions, no reciprocal reuse).  In the mixed form
 // pL/pR are p - p_ref (the sound speed adds p_ref back) and Uf returns the
 // face velocity measure 0.5*(uconL + uconR) that multiplies H_ref.
+// The mixed form multiplies by one reciprocal of each state's density
+// instead of dividing by it four times (FP32 rounding differences only).
 template <typename R, bool MIX>
 __device__ __forceinline__ void rusanov(const R QL[5], const R QR[5], R pL, R pR, const R h[3], bool use_qr_for_l,
                                         bool r_from_l, R pref, R F[5], R &Uf) {
-  R uconL = use_qr_for_l ? (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]))
+  R uconL, uconR, cL, cR;
+  if constexpr (MIX) {
+    const R ril = R(1) / QL[0], rir = R(1) / QR[0];
+    const R UR = (h[0] * QR[1] + h[1] * QR[2] + h[2] * QR[3]) * rir;
+    uconL = use_qr_for_l ? UR : (h[0] * QL[1] + h[1] * QL[2] + h[2] * QL[3]) * ril;
+    uconR = r_from_l ? uconL : UR;
+    cL = R(GAMMA_CONV) * (pL + pref) * ril;
+    cR = R(GAMMA_CONV) * (pR + pref) * rir;
+  } else {
+    uconL = use_qr_for_l ? (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]))
                          : (h[0] * (QL[1] / QL[0]) + h[1] * (QL[2] / QL[0]) + h[2] * (QL[3] / QL[0]));
-  R uconR = r_from_l ? uconL : (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
+    uconR = r_from_l ? uconL : (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
+    cL = R(GAMMA_CONV) * pL / QL[0];
+    cR = R(GAMMA_CONV) * pR / QR[0];
+  }
   R gii = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
-  R cL = R(GAMMA_CONV) * (MIX ? pL + pref : pL) / QL[0], cR = R(GAMMA_CONV) * (MIX ? pR + pref : pR) / QR[0];
   R saL = fabs(uconL) + sqrt(fabs(cL) * gii);
   R saR = fabs(uconR) + sqrt(fabs(cR) * gii);
   R SA = (saL < saR) ? saR : saL;
@@ -318,18 +332,28 @@ __device__ __forceinline__ void rusanov(const R QL[5], const R QR[5], R pL, R pR
 template <typename R, bool MIX>
 __device__ __forceinline__ void roe(const R QL[5], const R QR[5], R pL, R pR, const R h[3], bool use_qr_for_l,
                                     bool r_from_l, R pref, R href, R F[5], R &Uf) {
-  R uconL = use_qr_for_l ? (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]))
-                         : (h[0] * (QL[1] / QL[0]) + h[1] * (QL[2] / QL[0]) + h[2] * (QL[3] / QL[0]));
-  R uconR = r_from_l ? uconL : (h[0] * (QR[1] / QR[0]) + h[1] * (QR[2] / QR[0]) + h[2] * (QR[3] / QR[0]));
   (void)pref;
   const R g = R(GAMMA_CONV);
+  // the mixed form multiplies by reciprocals of the densities, the face area
+  // and the root sum (FP32 rounding differences only)
+  const R ril = MIX ? R(1) / QL[0] : R(0), rir = MIX ? R(1) / QR[0] : R(0);
+#define CB_DIVL(x) (MIX ? (x) * ril : (x) / QL[0])
+#define CB_DIVR(x) (MIX ? (x) * rir : (x) / QR[0])
+  R uconL = use_qr_for_l ? (h[0] * CB_DIVR(QR[1]) + h[1] * CB_DIVR(QR[2]) + h[2] * CB_DIVR(QR[3]))
+                         : (h[0] * CB_DIVL(QL[1]) + h[1] * CB_DIVL(QL[2]) + h[2] * CB_DIVL(QL[3]));
+  R uconR = r_from_l ? uconL : (h[0] * CB_DIVR(QR[1]) + h[1] * CB_DIVR(QR[2]) + h[2] * CB_DIVR(QR[3]));
   const R area = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
-  const R nx = h[0] / area, ny = h[1] / area, nz = h[2] / area;
-  const R sl = sqrt(QL[0]), sr = sqrt(QR[0]), wl = sl / (sl + sr), wr = sr / (sl + sr);
-  const R uL = QL[1] / QL[0], vL = QL[2] / QL[0], zL = QL[3] / QL[0];
-  const R uR = QR[1] / QR[0], vR = QR[2] / QR[0], zR = QR[3] / QR[0];
-  const R HL = (MIX ? (QL[4] + pL + href) : (QL[4] + pL)) / QL[0];
-  const R HR = (MIX ? (QR[4] + pR + href) : (QR[4] + pR)) / QR[0];
+  const R ria = MIX ? R(1) / area : R(0);
+  const R nx = MIX ? h[0] * ria : h[0] / area, ny = MIX ? h[1] * ria : h[1] / area, nz = MIX ? h[2] * ria : h[2] / area;
+  const R sl = sqrt(QL[0]), sr = sqrt(QR[0]);
+  const R ris = MIX ? R(1) / (sl + sr) : R(0);
+  const R wl = MIX ? sl * ris : sl / (sl + sr), wr = MIX ? sr * ris : sr / (sl + sr);
+  const R uL = CB_DIVL(QL[1]), vL = CB_DIVL(QL[2]), zL = CB_DIVL(QL[3]);
+  const R uR = CB_DIVR(QR[1]), vR = CB_DIVR(QR[2]), zR = CB_DIVR(QR[3]);
+  const R HL = CB_DIVL(MIX ? (QL[4] + pL + href) : (QL[4] + pL));
+  const R HR = CB_DIVR(MIX ? (QR[4] + pR + href) : (QR[4] + pR));
+#undef CB_DIVL
+#undef CB_DIVR
   const R rt = sl * sr, ut = wl * uL + wr * uR, vt = wl * vL + wr * vR, zt = wl * zL + wr * zR;
   const R Ht = wl * HL + wr * HR, q2 = ut * ut + vt * vt + zt * zt;
   const R c2 = (g - R(1.0)) * (Ht - R(0.5) * q2), ct = sqrt(fabs(c2));
@@ -615,11 +639,16 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
 // -------------------------------------------------------- viscous face ----
 __device__ __forceinline__ bool blocked(double v) { return v > SOLID && v < INNERBLANK; }
 
-// SMET: the metric vectors and nu_t of the face's plane-k nodes come from the
-// block's shared-memory slot (StageMet)
-template <typename R, bool MIX, bool LES, class RG, int DIR, bool NV0 = false, bool SMET = false>
+// FLUX bits as for conv_face: with the metric slot (StageMet) the metric
+// vectors and nu_t of the face's plane-k nodes come from shared memory, and a
+// constant blend weight (FLUX_SIGMA0 / FLUX_SIGMA1) is the value the sigma of
+// every node takes.  The mixed form groups its FP32 terms for FMA: the
+// divergence as the trace of r, one factor aj*nu, the heat-flux constant
+// gamma / (Pr (gamma - 1)) from the host.
+template <typename R, bool MIX, bool LES, class RG, int DIR, bool NV0 = false, int FLUX = 0>
 __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, const RG &Rg, NRef a,
                                           int gi, int gj, int gk, int drt, R Fv[5], R A[3]) {
+  constexpr bool SMET = StageMet<MIX, NV0, FLUX>::on;
   static_assert(!SMET || (MIX && DIR >= 0), "the metric slot holds FP32 vectors, selected at compile time");
   const int d = DIR >= 0 ? DIR : drt;
   const long long g0 = gidx(c, gi, gj, gk), sd = gstride(c, d), g1 = g0 + sd;
@@ -717,18 +746,28 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
     if (Tr < R(0)) nu = R(c.inv_ren);
     else nu = R(c.sut_k1) / (Tr + R(c.sut_k2)) * (MIX ? Tr * sqrt(Tr) : R(pow((double)Tr, 1.5)));
   }
-  const R div = R(2.) / R(3.) * (dudc * csi0 + dude * eta0 + dudz * zet0 + dvdc * csi1 + dvde * eta1 + dvdz * zet1 +
-                                 dwdc * csi2 + dwde * eta2 + dwdz * zet2);
+  const R div = MIX ? R(2. / 3.) * ((r11 + r22) + r33)
+                    : R(2.) / R(3.) * (dudc * csi0 + dude * eta0 + dudz * zet0 + dvdc * csi1 + dvde * eta1 +
+                                       dvdz * zet1 + dwdc * csi2 + dwde * eta2 + dwdz * zet2);
   const R tu = g11 * dudc + g21 * dude + g31 * dudz + r11 * md0 + r21 * md1 + r31 * md2;
   const R tv = g11 * dvdc + g21 * dvde + g31 * dvdz + r12 * md0 + r22 * md1 + r32 * md2;
   const R tw = g11 * dwdc + g21 * dwde + g31 * dwdz + r13 * md0 + r23 * md1 + r33 * md2;
+  // deviatoric stress vectors along the face normal (mixed form)
+  const R eu = MIX ? tu - div * md0 : R(0), ev = MIX ? tv - div * md1 : R(0), ew = MIX ? tw - div * md2 : R(0);
   Fv[0] = R(0.);
-  Fv[1] = tu * ajc * (nu);
-  Fv[2] = tv * ajc * (nu);
-  Fv[3] = tw * ajc * (nu);
-  Fv[1] -= div * md0 * ajc * nu;
-  Fv[2] -= div * md1 * ajc * nu;
-  Fv[3] -= div * md2 * ajc * nu;
+  if constexpr (MIX) {
+    const R s = ajc * nu;
+    Fv[1] = eu * s;
+    Fv[2] = ev * s;
+    Fv[3] = ew * s;
+  } else {
+    Fv[1] = tu * ajc * (nu);
+    Fv[2] = tv * ajc * (nu);
+    Fv[3] = tw * ajc * (nu);
+    Fv[1] -= div * md0 * ajc * nu;
+    Fv[2] -= div * md1 * ajc * nu;
+    Fv[3] -= div * md2 * ajc * nu;
+  }
 
   R uh[3];
   if (pos == 0 && bc_lo(c, d) == 1) {
@@ -744,30 +783,40 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   if (c.twod == 1) uh[0] = R(0.);
   const R gm = R(c.gamma);
   Fv[4] = (Fv[1] * uh[0] + Fv[2] * uh[1] + Fv[3] * uh[2]) +
-          (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (gm * nu / R(c.pr) / R(c.gm1));
+          (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (MIX ? nu * R(c.kheat) : gm * nu / R(c.pr) / R(c.gm1));
 
   A[0] = A[1] = A[2] = R(0.);
   if (LES) {  // rhs.c:1677-1710
-    const R sa = R(sigma_at(c, F, d, gi, gj, gk));
+    // the node weights: the constant the host chose the variant for, or sigma_at
+    constexpr bool S0 = (FLUX & FLUX_SIGMA0) != 0, S1 = (FLUX & FLUX_SIGMA1) != 0;
     const int bi = gi + (d == 0), bj = gj + (d == 1), bk = gk + (d == 2);
-    const R sb = R(sigma_at(c, F, d, bi, bj, bk));
+    const R sa = S0 ? R(0.) : (S1 ? R(1.) : R(sigma_at(c, F, d, gi, gj, gk)));
+    const R sb = S0 ? R(0.) : (S1 ? R(1.) : R(sigma_at(c, F, d, bi, bj, bk)));
     const double nu0 = SMET ? Rg.nut(a) : ldg(F.nut + g0);
     const double nu1 = (SMET && d < 2) ? Rg.nut(b) : ldg(F.nut + g1);
     R nut = R(0.5) * (R(nu0) * sa + R(nu1) * sb);
     const R rho_c = R(0.5) * (Rg.get(F_RHO, a) + Rg.get(F_RHO, b));
     const R sigma_c = R(0.5) * (sa + sb);
     if ((bc_lo(c, d) == 1 && pos == 0) || (bc_hi(c, d) == 1 && pos == m - 2)) nut = R(0);
-    const R tx = (tu - div * md0) * ajc * (nut * rho_c);
-    const R ty = (tv - div * md1) * ajc * (nut * rho_c);
-    const R tz = (tw - div * md2) * ajc * (nut * rho_c);
     const R S2 = R(.5) * ((r11 - div) * (r11 - div) + r12 * r12 + r13 * r13 + r21 * r21 + (r22 - div) * (r22 - div) +
                           r23 * r23 + r31 * r31 + r32 * r32 + (r33 - div) * (r33 - div));
     // pow(pow(1/aj, 1/3), 2) of the left node, precomputed once per node
     const R pf = MIX ? w0[0] : R(ldg(F.delta2 + g0));
-    const R sgs = -S2 * pf * R(c.ci) * R(2.0) / R(3.0);
-    A[0] = tx + sgs * md0 * rho_c * sigma_c;
-    A[1] = ty + sgs * md1 * rho_c * sigma_c;
-    A[2] = tz + sgs * md2 * rho_c * sigma_c;
+    if constexpr (MIX) {
+      const R sn = ajc * (nut * rho_c);
+      const R ks = -S2 * pf * R(c.ci * (2.0 / 3.0)) * (rho_c * sigma_c);
+      A[0] = eu * sn + ks * md0;
+      A[1] = ev * sn + ks * md1;
+      A[2] = ew * sn + ks * md2;
+    } else {
+      const R tx = (tu - div * md0) * ajc * (nut * rho_c);
+      const R ty = (tv - div * md1) * ajc * (nut * rho_c);
+      const R tz = (tw - div * md2) * ajc * (nut * rho_c);
+      const R sgs = -S2 * pf * R(c.ci) * R(2.0) / R(3.0);
+      A[0] = tx + sgs * md0 * rho_c * sigma_c;
+      A[1] = ty + sgs * md1 * rho_c * sigma_c;
+      A[2] = tz + sgs * md2 * rho_c * sigma_c;
+    }
     Fv[1] += A[0];
     Fv[2] += A[1];
     Fv[3] += A[2];
@@ -783,7 +832,7 @@ __device__ __forceinline__ void face_flux(const DevCfg &c, const DevFields &F, c
   R Fc[5], Fv[5], A[3];
   conv_face<R, MIX, LES, RG, DIR, FLUX, NV0>(c, F, Rg, a, fi, fj, k, drt, Fc);
   if (VISC) {
-    visc_face<R, MIX, LES, RG, DIR, NV0, StageMet<MIX, NV0, FLUX>::on>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
+    visc_face<R, MIX, LES, RG, DIR, NV0, FLUX>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
   } else {
 #pragma unroll
     for (int q = 0; q < 5; q++) Fv[q] = R(0.);
@@ -812,7 +861,7 @@ __device__ __forceinline__ void face_flux_half(const DevCfg &c, const DevFields 
   } else {
     R Fv[5], A[3];
     if (VISC) {
-      visc_face<R, MIX, LES, RG, DIR, NV0>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
+      visc_face<R, MIX, LES, RG, DIR, NV0, FLUX>(c, F, Rg, a, fi, fj, k, drt, Fv, A);
     } else {
 #pragma unroll
       for (int q = 0; q < 5; q++) Fv[q] = R(0.);
