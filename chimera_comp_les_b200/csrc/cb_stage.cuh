@@ -971,7 +971,12 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
       // this thread's half of the face: G[0..4], or G[VOFF..NG-1]
       const int q0 = role == 0 ? 0 : VOFF, q1 = role == 0 ? VOFF : NG;
       if (live) {
-        face_flux_half<R, MIX, LES, VISC, RG, -1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
+        // one instantiation per direction (d is warp-uniform): the index
+        // arithmetic of every stencil shift folds into constants (4 % faster
+        // than one copy for all directions at 128 registers)
+        if (d == 0) face_flux_half<R, MIX, LES, VISC, RG, 0, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
+        else if (d == 1) face_flux_half<R, MIX, LES, VISC, RG, 1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
+        else face_flux_half<R, MIX, LES, VISC, RG, 2, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
       } else {
 #pragma unroll
         for (int q = 0; q < NG; q++) Gf[q] = R(0.);
