@@ -1059,9 +1059,15 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   // buffer: node-major, one index computation per node and one 8-byte copy
   // per staged field (consecutive threads take consecutive nodes of a row, so
   // each field's copies stay coalesced)
+  // In the FP64 form the threads of the inviscid half issue the copies and
+  // those of the viscous half run the derive pass: the viscous face takes
+  // longer, and the inviscid threads also run the node update, in the same
+  // phase as the derive pass.
+  constexpr bool SPLIT = StageThreads<FLUX, MIX>::SPLIT;
+  constexpr int HT = SPLIT ? NT / 2 : NT;  // threads of one half
   auto issue_stage = [&](int kk) {
     const bool kok = kk >= -2 && kk <= c.mz + 1;
-    for (int idx = tid; idx < PN; idx += NT) {
+    for (int idx = tid; idx < PN && tid < HT; idx += HT) {
       const int ly = idx / PX, lx = idx - ly * PX;
       const int xi = i0 - 2 + lx, yj = j0 - 2 + ly;
       const bool ok = kok && xi <= c.mx + 1 && yj <= c.my + 1;
@@ -1076,7 +1082,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   // staging -> ring slot s with the derived p, u, v, w, T (EqOfState rhs.c:4850,
   // CalcUCat rhs.c:1349), all in FP64; the mixed form stores shifted FP32 values
   auto derive = [&](int s) {
-    for (int idx = tid; idx < PN; idx += NT) {
+    for (int idx = SPLIT ? tid - HT : tid; idx < PN && idx >= 0; idx += HT) {
       double v[NF];
 #pragma unroll
       for (int q = 0; q < 5; q++) v[q] = stg[q * PN + idx];
