@@ -179,6 +179,11 @@ static int flux_bits(const cb_ctx *c) {
     if (f.s_x == 1.0) fl |= FLUX_SIGMA1;
     else if (f.s_x == 0.0) fl |= FLUX_SIGMA0;
   }
+  // every face periodic or an interface, no 2-D mode, MUSCL (or WENO5-JS,
+  // whose reconstruction the W5 bit selects): the PLAIN variants
+  bool per = f.twod == 0 && (f.fluxorder == 2 || f.weno_order == 5);
+  for (int s = 0; s < 6; s++) per = per && f.bctype[s] == 7;
+  if (per) fl |= FLUX_PLAIN;
   return fl;
 }
 

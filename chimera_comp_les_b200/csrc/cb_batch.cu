@@ -156,6 +156,9 @@ static int batch_flux_bits(const cb_config &f) {
     if (f.s_x == 1.0) fl |= FLUX_SIGMA1;
     else if (f.s_x == 0.0) fl |= FLUX_SIGMA0;
   }
+  // block faces are interfaces (bctype 7): with no 2-D mode and MUSCL (or
+  // WENO5-JS, whose reconstruction the W5 bit selects) the PLAIN variants
+  if (f.twod == 0 && (f.fluxorder == 2 || f.weno_order == 5)) fl |= FLUX_PLAIN;
   return fl;
 }
 

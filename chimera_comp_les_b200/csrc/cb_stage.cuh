@@ -57,8 +57,12 @@ struct TileShape {
 };
 
 // FLUX bits of the stage kernel (see conv_face): Roe's flux, a constant LES
-// blend weight of exactly 1 or 0, and WENO5-JS reconstruction.
-constexpr int FLUX_ROE = 1, FLUX_SIGMA1 = 2, FLUX_SIGMA0 = 4, FLUX_W5 = 8;
+// blend weight of exactly 1 or 0, and WENO5-JS reconstruction.  FLUX_PLAIN
+// (no-IBM variants): every face of the block is periodic or an interface
+// (bctype 7 on all six sides), -twoD is 0, and without FLUX_W5 the
+// reconstruction is MUSCL (fluxorder 2) -- the options the host checked, as
+// compile-time constants, so the kernel carries no other branch of them.
+constexpr int FLUX_ROE = 1, FLUX_SIGMA1 = 2, FLUX_SIGMA0 = 4, FLUX_W5 = 8, FLUX_PLAIN = 16;
 
 // Tile geometry of a stage-kernel variant.  The WENO3/MUSCL stencil reaches
 // one node beyond the face's two nodes: a ring of 4 planes (k-1 .. k+2) and a
@@ -489,16 +493,17 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   for (int q = 0; q < 5; q++) Fw[q] = R(0);
   if constexpr (!CEN_ONLY) {  // reconstruction and the upwind flux
     R QL[5], QR[5], pL, pR;
-    const int fo = c.fluxorder;
+    constexpr bool PLAIN = (FLUX & FLUX_PLAIN) != 0;
+    const int fo = (PLAIN && !W5) ? 2 : c.fluxorder;
     bool first;
     if (LES) {
       double nsum2 = (d == 2) ? nv0 + (NV0 ? 0.0 : ldg(F.nvert + gidx(c, 1, gj, gk + 1))) : nv0 + nv1;  // quirk rhs.c:4046
-      first = fo == 1 || ((pos == 0 || pos == m - 2) && bc_lo(c, d) != 7) || nsum2 > BLANKWALL;
+      first = fo == 1 || (!PLAIN && (pos == 0 || pos == m - 2) && bc_lo(c, d) != 7) || nsum2 > BLANKWALL;
     } else {
       first = fo == 1 || pos == 0 || pos == m - 2 || (nv0 + nv1) > BLANKWALL;
     }
     int iso_case = 0;
-    if (!LES && d == 1 && c.isothermal) {
+    if (!LES && !PLAIN && d == 1 && c.isothermal) {
       if (gj == 0 && c.bctype[2] == 1) iso_case = 1;           // rhs.c:2822
       else if (gj == m - 2 && c.bctype[3] == 1) iso_case = 2;  // rhs.c:2828
     }
@@ -538,7 +543,7 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
   #pragma unroll
         for (int q = 0; q < 5; q++) QL[q] = weno3_l(Q[0][q], Q[1][q], Q[2][q]);
         pL = weno3_l(P[0], P[1], P[2]);
-        if (!LES && d == 1 && gj == 1 && c.isothermal && c.bctype[2] == 1) {  // rhs.c:2926
+        if (!LES && !PLAIN && d == 1 && gj == 1 && c.isothermal && c.bctype[2] == 1) {  // rhs.c:2926
           QL[0] = eno_l(Q[1][0], Q[2][0], Q[3][0], ord);
           QL[4] = eno_l(Q[1][4], Q[2][4], Q[3][4], ord);
           pL = eno_l(P[1], P[2], P[3], ord);
@@ -558,8 +563,8 @@ __device__ __forceinline__ void conv_face(const DevCfg &c, const DevFields &F, c
       if (ROE) roe<R, MIX>(QL, QR, pL, pR, h, false, false, pref, href, Fw, Ufw);
       else rusanov<R, MIX>(QL, QR, pL, pR, h, false, false, pref, Fw, Ufw);
     } else {
-      const bool use_qr_l = (pos == m - 2 && bc_hi(c, d) == 1);
-      const bool r_from_l = (pos == 0 && bc_lo(c, d) == 1);
+      const bool use_qr_l = !PLAIN && (pos == m - 2 && bc_hi(c, d) == 1);
+      const bool r_from_l = !PLAIN && (pos == 0 && bc_lo(c, d) == 1);
       if (ROE) roe<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, href, Fw, Ufw);
       else rusanov<R, MIX>(QL, QR, pL, pR, h, use_qr_l, r_from_l, pref, Fw, Ufw);
     }
@@ -685,7 +690,8 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
       }
     }
   }
-  if (c.twod == 1) D[0][0] = D[0][1] = D[0][2] = R(0.);  // lUcat x = 0 (CalcUCat rhs.c:1349)
+  constexpr bool PLAIN = (FLUX & FLUX_PLAIN) != 0;
+  if (!PLAIN && c.twod == 1) D[0][0] = D[0][1] = D[0][2] = R(0.);  // lUcat x = 0 (CalcUCat rhs.c:1349)
   const R dudc = D[0][0], dude = D[0][1], dudz = D[0][2];
   const R dvdc = D[1][0], dvde = D[1][1], dvdz = D[1][2];
   const R dwdc = D[2][0], dwde = D[2][1], dwdz = D[2][2];
@@ -770,17 +776,17 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
   }
 
   R uh[3];
-  if (pos == 0 && bc_lo(c, d) == 1) {
+  if (!PLAIN && pos == 0 && bc_lo(c, d) == 1) {
 #pragma unroll
     for (int q = 0; q < 3; q++) uh[q] = Rg.get(F_U + q, a);
-  } else if (pos == m - 2 && bc_hi(c, d) == 1) {
+  } else if (!PLAIN && pos == m - 2 && bc_hi(c, d) == 1) {
 #pragma unroll
     for (int q = 0; q < 3; q++) uh[q] = Rg.get(F_U + q, b);
   } else {
 #pragma unroll
     for (int q = 0; q < 3; q++) uh[q] = R(0.5) * (Rg.get(F_U + q, b) + Rg.get(F_U + q, a));
   }
-  if (c.twod == 1) uh[0] = R(0.);
+  if (!PLAIN && c.twod == 1) uh[0] = R(0.);
   const R gm = R(c.gamma);
   Fv[4] = (Fv[1] * uh[0] + Fv[2] * uh[1] + Fv[3] * uh[2]) +
           (g11 * dpdc + g21 * dpde + g31 * dpdz) * ajc * (MIX ? nu * R(c.kheat) : gm * nu / R(c.pr) / R(c.gm1));
@@ -797,7 +803,7 @@ __device__ __forceinline__ void visc_face(const DevCfg &c, const DevFields &F, c
     R nut = R(0.5) * (R(nu0) * sa + R(nu1) * sb);
     const R rho_c = R(0.5) * (Rg.get(F_RHO, a) + Rg.get(F_RHO, b));
     const R sigma_c = R(0.5) * (sa + sb);
-    if ((bc_lo(c, d) == 1 && pos == 0) || (bc_hi(c, d) == 1 && pos == m - 2)) nut = R(0);
+    if (!PLAIN && ((bc_lo(c, d) == 1 && pos == 0) || (bc_hi(c, d) == 1 && pos == m - 2))) nut = R(0);
     const R S2 = R(.5) * ((r11 - div) * (r11 - div) + r12 * r12 + r13 * r13 + r21 * r21 + (r22 - div) * (r22 - div) +
                           r23 * r23 + r31 * r31 + r32 * r32 + (r33 - div) * (r33 - div));
     // pow(pow(1/aj, 1/3), 2) of the left node, precomputed once per node
@@ -966,15 +972,18 @@ __device__ __forceinline__ void plane_faces(const DevCfg &c, const DevFields &F,
     }
     R Gf[NG];
     // -twoD 1 forms no i-face flux (rhs.c:1487, 2646, 3465): it stays zero
-    const bool live = fi <= c.mx - 2 && fj <= c.my - 2 && !(d == 0 && c.twod == 1);
+    const bool live = fi <= c.mx - 2 && fj <= c.my - 2 && !(d == 0 && (FLUX & FLUX_PLAIN) == 0 && c.twod == 1);
     if constexpr (SPLIT) {
       // this thread's half of the face: G[0..4], or G[VOFF..NG-1]
       const int q0 = role == 0 ? 0 : VOFF, q1 = role == 0 ? VOFF : NG;
       if (live) {
         // one instantiation per direction (d is warp-uniform): the index
         // arithmetic of every stencil shift folds into constants (4 % faster
-        // than one copy for all directions at 128 registers)
-        if (d == 0) face_flux_half<R, MIX, LES, VISC, RG, 0, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
+        // than one copy for all directions at 128 registers); the WENO5-JS
+        // variants, at 168 registers, keep one copy (13 % faster there)
+        if constexpr ((FLUX & FLUX_W5) != 0)
+          face_flux_half<R, MIX, LES, VISC, RG, -1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
+        else if (d == 0) face_flux_half<R, MIX, LES, VISC, RG, 0, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
         else if (d == 1) face_flux_half<R, MIX, LES, VISC, RG, 1, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
         else face_flux_half<R, MIX, LES, VISC, RG, 2, FLUX, NV0>(c, F, Rg, a, fi, fj, k, d, role, Gf);
       } else {
@@ -1030,6 +1039,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
   using RG = Ring<R, BX, BY, NPL>;
   constexpr bool SMET = StageMet<MIX, NV0, FLUX>::on;
   constexpr int MPX = RG::MPX, MPN = RG::MPN;
+  constexpr bool PLAIN = (FLUX & FLUX_PLAIN) != 0;
   double *stg = smem_d;  // [NSTG][PN] raw FP64 Q, nvert and carried pressure of the next plane
   float4 *mts = reinterpret_cast<float4 *>(smem_d + (size_t)NSTG * PN);  // [3][MPN] metric slot (SMET)
   double *nts = reinterpret_cast<double *>(mts + (SMET ? 3 * MPN : 0));   // [MPN] nu_t slot (SMET)
@@ -1239,7 +1249,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 #pragma unroll
         for (int q = 1; q < 4; q++) rhs[q] = (double)d4[q] - c.p_ref * gcl_r[q - 1];
         rhs[4] = (double)d4[4];
-        if (c.twod == 1) rhs[1] = 0.;  // no x-momentum right-hand side (rhs.c:2135, 3168, 4215)
+        if (!PLAIN && c.twod == 1) rhs[1] = 0.;  // no x-momentum right-hand side (rhs.c:2135, 3168, 4215)
 #pragma unroll
         for (int q = 0; q < 5; q++) rhs[q] = (nv < BLANK) ? rhs[q] * aj : 0.;
       } else {
@@ -1249,7 +1259,7 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
         visc[0] = R(0.);
 #pragma unroll
         for (int q = 1; q < 5; q++) visc[q] = VISC ? fdiff(VOFF + q) : R(0.);
-        if (c.twod == 1) conv[1] = visc[1] = R(0.);  // rhs.c:2135-2140, 3168-3173, 4215-4220
+        if (!PLAIN && c.twod == 1) conv[1] = visc[1] = R(0.);  // rhs.c:2135-2140, 3168-3173, 4215-4220
         if (LES && nv < BLANK && c.ratio != 0.0) {  // channel forcing (rhs.c:4226-4235); exact no-op at ratio 0
           const double ajn = aj_r;
           conv[3] = conv[3] - c.ratio / ajn * Rg.get(F_RHO, n) / c.dt;
@@ -1331,7 +1341,7 @@ static __global__ void __launch_bounds__(StageThreads<FLUX, MIX>::N, StageThread
 // general blend.
 using StageKern = void (*)(const DevCfg, const DevFields, int, double, double, double, int);
 template <typename R, bool MIX, bool LES, bool VISC, int W>
-StageKern stage_nv0_kernel_w(int fl) {
+static StageKern stage_nv0_kernel_w(int fl) {
   if constexpr (LES) {
     switch (fl & 7) {
       case 1: return stage_kernel<R, MIX, LES, VISC, false, W | 1, true>;
@@ -1345,13 +1355,19 @@ StageKern stage_nv0_kernel_w(int fl) {
     return (fl & FLUX_ROE) ? stage_kernel<R, MIX, LES, VISC, false, W | 1, true> : stage_kernel<R, MIX, LES, VISC, false, W, true>;
   }
 }
+// (static, like the kernels: each object's selector returns its own kernels)
 template <typename R, bool MIX, bool LES, bool VISC>
-StageKern stage_nv0_kernel(int fl) {
-  return (fl & FLUX_W5) ? stage_nv0_kernel_w<R, MIX, LES, VISC, FLUX_W5>(fl) : stage_nv0_kernel_w<R, MIX, LES, VISC, 0>(fl);
+static StageKern stage_nv0_kernel(int fl) {
+  switch (fl & (FLUX_W5 | FLUX_PLAIN)) {
+    case FLUX_W5: return stage_nv0_kernel_w<R, MIX, LES, VISC, FLUX_W5>(fl);
+    case FLUX_PLAIN: return stage_nv0_kernel_w<R, MIX, LES, VISC, FLUX_PLAIN>(fl);
+    case FLUX_W5 | FLUX_PLAIN: return stage_nv0_kernel_w<R, MIX, LES, VISC, FLUX_W5 | FLUX_PLAIN>(fl);
+    default: return stage_nv0_kernel_w<R, MIX, LES, VISC, 0>(fl);
+  }
 }
 // The general (nvert-reading) kernel for the Roe and WENO5 bits of fl.
 template <typename R, bool MIX, bool LES, bool VISC, bool RHSM>
-StageKern stage_gen_kernel(int fl) {
+static StageKern stage_gen_kernel(int fl) {
   switch (fl & (FLUX_ROE | FLUX_W5)) {
     case FLUX_ROE: return stage_kernel<R, MIX, LES, VISC, RHSM, FLUX_ROE>;
     case FLUX_W5: return stage_kernel<R, MIX, LES, VISC, RHSM, FLUX_W5>;
@@ -1372,13 +1388,13 @@ size_t stage_smem_for(int fl, bool nv0) {
 }
 // Opt every variant of one (LES, VISC, RHSM) into its dynamic shared memory.
 template <typename R, bool MIX, bool LES, bool VISC, bool RHSM>
-cudaError_t stage_attrs() {
+static cudaError_t stage_attrs() {
   const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaSuccess;
   for (int fl : {0, FLUX_ROE, FLUX_W5, FLUX_ROE | FLUX_W5})
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_gen_kernel<R, MIX, LES, VISC, RHSM>(fl), attr, (int)stage_smem_for<R, MIX>(fl, false));
   if constexpr (!RHSM) {  // the no-IBM variants of the time step
-    for (int w : {0, FLUX_W5})
+    for (int w : {0, FLUX_W5, FLUX_PLAIN, FLUX_W5 | FLUX_PLAIN})
       for (int fl = 0; fl < (LES ? 6 : 2) && e == cudaSuccess; fl++)
         e = cudaFuncSetAttribute(stage_nv0_kernel<R, MIX, LES, VISC>(w | fl), attr, (int)stage_smem_for<R, MIX>(w | fl, true));
   }

@@ -89,7 +89,14 @@ BatchKern batched_nv0_w(int fl) {
 }
 template <typename R, bool MIX, bool LES, bool VISC>
 BatchKern batched_kernel(int fl, bool nv0) {
-  if (nv0) return (fl & FLUX_W5) ? batched_nv0_w<R, MIX, LES, VISC, FLUX_W5>(fl) : batched_nv0_w<R, MIX, LES, VISC, 0>(fl);
+  if (nv0) {
+    switch (fl & (FLUX_W5 | FLUX_PLAIN)) {
+      case FLUX_W5: return batched_nv0_w<R, MIX, LES, VISC, FLUX_W5>(fl);
+      case FLUX_PLAIN: return batched_nv0_w<R, MIX, LES, VISC, FLUX_PLAIN>(fl);
+      case FLUX_W5 | FLUX_PLAIN: return batched_nv0_w<R, MIX, LES, VISC, FLUX_W5 | FLUX_PLAIN>(fl);
+      default: return batched_nv0_w<R, MIX, LES, VISC, 0>(fl);
+    }
+  }
   switch (fl & (FLUX_ROE | FLUX_W5)) {
     case FLUX_ROE: return stage_batched_kernel<R, MIX, LES, VISC, false, FLUX_ROE>;
     case FLUX_W5: return stage_batched_kernel<R, MIX, LES, VISC, false, FLUX_W5>;
@@ -104,7 +111,7 @@ cudaError_t batched_attrs() {
   for (int fl : {0, FLUX_ROE, FLUX_W5, FLUX_ROE | FLUX_W5})
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(batched_kernel<R, MIX, LES, VISC>(fl, false), attr, (int)stage_smem_for<R, MIX>(fl, false));
-  for (int w : {0, FLUX_W5})
+  for (int w : {0, FLUX_W5, FLUX_PLAIN, FLUX_W5 | FLUX_PLAIN})
     for (int fl = 0; fl < (LES ? 6 : 2) && e == cudaSuccess; fl++)
       e = cudaFuncSetAttribute(batched_kernel<R, MIX, LES, VISC>(w | fl, true), attr,
                                (int)stage_smem_for<R, MIX>(w | fl, true));
