@@ -94,6 +94,7 @@ struct cb_ctx {
   unsigned *status = nullptr;
   bool fully_periodic = true;  // every face bctype 7: one fused periodic BC kernel
   bool nv0 = true;             // nvert is zero everywhere: the stage kernel's no-IBM variant
+  bool nvz = true;             // nvert is zero everywhere (the eddy viscosity reads no nvert)
   int cur = 0;                // buffer with the current Q (== Qold between steps)
   int uc = -1;                // buffer of the last CalcUCat state, -1: none
   bool have_grid = false, have_state = false;
@@ -339,7 +340,7 @@ static int nut_update(cb_ctx *c) {
     const int ekc = eddy_kchunk(c->dc, c->sms);
     eddy_viscosity_kernel<<<eddy_grid(c->dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, c->stream>>>(
         c->dc, c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr,
-        (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvert, c->nut, ekc,
+        (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvz ? nullptr : c->nvert, c->nut, ekc,
         dyn ? (const double *const *)(c->ptab + 5 * c->cur) : nullptr, dyn ? c->dyn_arena + 12 * c->plane : nullptr);
   }
   {
@@ -861,9 +862,10 @@ int cb_set_nvert(cb_ctx *c, const double *nvert) {
   bool zero = true;
   for (size_t t = 0; t < nn && zero; t++) zero = nvert[t] == 0.0;
   const bool nv0 = zero && !c->cfg.visT;  // the no-IBM variants carry no Sutherland law
-  if (q != c->dc.nvq || nv0 != c->nv0) {
+  if (q != c->dc.nvq || nv0 != c->nv0 || zero != c->nvz) {
     c->dc.nvq = q;
     c->nv0 = nv0;
+    c->nvz = zero;
     invalidate_graphs(c);  // the graphs carry the config and the kernel variant
   }
   return CB_OK;

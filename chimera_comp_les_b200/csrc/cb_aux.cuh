@@ -508,8 +508,11 @@ static __global__ void ghost_fill_kernel(const DevCfg c, double *const *planes, 
 // planes (k-1, k, k+1, with a one-node halo in i and j) sits in shared
 // memory, so each node's three divisions happen once instead of at each of
 // its six neighbours (the same IEEE quotients the reference forms there).
+// nvert nullptr: nvert is zero everywhere (no immersed body).  The node's
+// metrics, aj, filter width and nvert are loaded before the plane barrier so
+// their latency overlaps the velocity conversion of the next plane.
 constexpr int EDDY_BX = 32, EDDY_BY = 8, EDDY_PX = EDDY_BX + 2, EDDY_PN = EDDY_PX * (EDDY_BY + 2);
-static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
+static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY, 4)
     eddy_viscosity_kernel(const DevCfg c, const double *const *qu, const double *const *met, const double *aj,
                           const double *delta2, const double *nvert, double *nut, int kchunk,
                           const double *const *qn = nullptr, const double *csp = nullptr) {
@@ -537,7 +540,7 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
         // after the dynamic model (qn set) lUcat holds the current state's
         // velocity at interior nodes with nvert <= 1.1 (les.c:234-238)
         if (qn && xi >= 1 && xi <= c.mx - 2 && yj >= 1 && yj <= c.my - 2 && kk >= 1 && kk <= c.mz - 2 &&
-            ldg(nvert + n) <= 1.1) {
+            (!nvert || ldg(nvert + n) <= 1.1)) {
           src = qn;
           sv = 2;
         }
@@ -578,14 +581,27 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
   issue(kb + 1);
   const int e0 = (ty + 1) * EDDY_PX + tx + 1;
   for (int k = kb; k < ke; k++) {
+    // the node's own operands of plane k, in flight across the barriers
+    const long long n = gidx(c, i, j, k);
+    double mv[3][3], ajc = 0., d2 = 0., cs = 0.;
+    bool solid = false;
+    if (act) {
+#pragma unroll
+      for (int e = 0; e < 3; e++)
+#pragma unroll
+        for (int x = 0; x < 3; x++) mv[e][x] = ldg(met[e * 3 + x] + n);
+      ajc = ldg(aj + n);
+      d2 = ldg(delta2 + n);
+      cs = csp ? ldg(csp + n) : c.cs_const;
+      solid = nvert && ldg(nvert + n) > 0.1;
+    }
     cp_async_wait_all();
     __syncthreads();  // plane k+1 staged; every thread is past plane k-1, whose slot (k+1) % 3 is refilled now
     convert((k + 1) % 3);
     __syncthreads();
     if (k + 1 < ke) issue(k + 2);  // in flight while plane k is computed
     if (act) {
-      const long long n = gidx(c, i, j, k);
-      if (ldg(nvert + n) > 0.1) {
+      if (solid) {
         nut[n] = 0.;
       } else {
         const int sm = (k - 1) % 3, s0 = k % 3, sp = (k + 1) % 3;
@@ -596,21 +612,19 @@ static __global__ void __launch_bounds__(EDDY_BX *EDDY_BY)
           dd[a][1] = (us[s0][a][e0 + EDDY_PX] - us[s0][a][e0 - EDDY_PX]) * 0.5;
           dd[a][2] = (us[sp][a][e0] - us[sm][a][e0]) * 0.5;
         }
-        const double ajc = ldg(aj + n);
         double g[3][3];
 #pragma unroll
         for (int a = 0; a < 3; a++)
 #pragma unroll
           for (int x = 0; x < 3; x++)
-            g[a][x] = (dd[a][0] * ldg(met[0 * 3 + x] + n) + dd[a][1] * ldg(met[1 * 3 + x] + n) +
-                       dd[a][2] * ldg(met[2 * 3 + x] + n)) * ajc;
+            g[a][x] = (dd[a][0] * mv[0][x] + dd[a][1] * mv[1][x] + dd[a][2] * mv[2][x]) * ajc;
         const double Sdd = 2. / 3. * (g[0][0] + g[1][1] + g[2][2]);
         const double Sxx = 0.5 * (g[0][0] + g[0][0]) - Sdd, Sxy = 0.5 * (g[0][1] + g[1][0]), Sxz = 0.5 * (g[0][2] + g[2][0]);
         const double Syy = 0.5 * (g[1][1] + g[1][1]) - Sdd, Syz = 0.5 * (g[1][2] + g[2][1]);
         const double Szz = 0.5 * (g[2][2] + g[2][2]) - Sdd;
         const double Sabs = sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Sxy * Sxy + Syy * Syy + Syz * Syz +
                                         Sxz * Sxz + Syz * Syz + Szz * Szz));
-        nut[n] = (csp ? ldg(csp + n) : c.cs_const) * ldg(delta2 + n) * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
+        nut[n] = cs * d2 * Sabs;  // CS * pow(pow(1/aj,1/3),2) * |S|
       }
     }
   }

@@ -717,7 +717,7 @@ static int enqueue_nut(cb_batch *b) {
     const double *const *mt = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, met));
     const int ekc = eddy_kchunk(bh.dc, b->sms);
     eddy_viscosity_kernel<<<eddy_grid(bh.dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
-                                                                 b->delta2 + o, b->nvert + o, b->nut + o, ekc);
+                                                                 b->delta2 + o, bh.nvz ? nullptr : b->nvert + o, b->nut + o, ekc);
   }
   if (b->nwrap || b->xw.nsend || b->xw.nrecv) {
     if (b->nwrap) plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, b->nut);
