@@ -173,7 +173,20 @@ struct Ring {
     const int t = sb + r + H;
     return t >= NPL ? t - NPL : t;
   }
-  __device__ __forceinline__ R get(int f, NRef n) const { return pl[((slot(n.r) * NF + f) * PY + n.y) * PX + n.x]; }
+  // FP64 form: field-major planes [slot][field][y][x] (consecutive x in
+  // consecutive banks).  Mixed form: the NF fields of a node side by side
+  // [slot][y][x][field], read in 8-byte pairs (fields 2m, 2m+1): a node's
+  // state, pressure and velocity come in 5 loads instead of 10, and a warp's
+  // 8-byte loads at the 40-byte node stride hit distinct banks.
+  static constexpr bool AOS = sizeof(R) == 4;
+  __device__ __forceinline__ R get(int f, NRef n) const {
+    if constexpr (AOS) {
+      const float2 v = *reinterpret_cast<const float2 *>(pl + ((slot(n.r) * PY + n.y) * PX + n.x) * NF + (f & ~1));
+      return (f & 1) ? v.y : v.x;
+    } else {
+      return pl[((slot(n.r) * NF + f) * PY + n.y) * PX + n.x];
+    }
+  }
   __device__ __forceinline__ double nv(NRef n) const { return 0.25 * (double)nvc[(slot(n.r) * PY + n.y) * PX + n.x]; }
   // a node of the i/j halo rows the ring holds (the k range is always held)
   __device__ __forceinline__ bool holds(NRef n) const { return n.x >= 0 && n.x < PX && n.y >= 0 && n.y < PY; }
@@ -1125,9 +1138,15 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 #pragma unroll
         for (int q = 5; q < NF; q++) v[q] = 0.0;
       }
-      R *base = Rg.pl + (size_t)s * NF * PN + idx;
+      if constexpr (RG::AOS) {
+        float2 *base = reinterpret_cast<float2 *>(Rg.pl + ((size_t)s * PN + idx) * NF);
 #pragma unroll
-      for (int q = 0; q < NF; q++) base[(size_t)q * PN] = R(v[q]);
+        for (int q = 0; q < NF; q += 2) base[q / 2] = make_float2(float(v[q]), float(v[q + 1]));
+      } else {
+        R *base = Rg.pl + (size_t)s * NF * PN + idx;
+#pragma unroll
+        for (int q = 0; q < NF; q++) base[(size_t)q * PN] = R(v[q]);
+      }
       if (nvs) nvc[s * PN + idx] = (unsigned char)(stg[5 * PN + idx] * 4.0);
     }
   };
