@@ -647,7 +647,8 @@ def run_ours(args, ws, rank, local):
                          "frac": head["achieved_gbs"] / peak,
                          "traffic": profile_traffic(args.precision),
                          "kernel": f"stage_kernel ({args.precision} form: fused RHS + RK combine)",
-                         "kernel_avg_ms": head["kernel_avg_ms"], "bytes_per_cell": B_ALG[args.precision],
+                         "kernel_avg_ms": head["kernel_avg_ms"], "kchunk_autotuned": head["kchunk_autotuned"],
+                         "bytes_per_cell": B_ALG[args.precision],
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "copy_gbs_measured_here": copy_gbs,
                          "frac_of_copy_measured_here": head["achieved_gbs"] / copy_gbs,
