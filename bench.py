@@ -480,6 +480,115 @@ def config5_case(n):
 CONFIG5_SCHEME = "WENO5-JS + Roe, pure upwind (sigma 0), Smagorinsky CS 0.17^2, SSP-RK3, dt from CFL 0.4"
 
 
+def _ke_enstrophy_device(q, csi, eta, zet, aj, local):
+    """diagnostics.kinetic_energy / enstrophy of a host state, evaluated with
+    torch on the GPU in FP64 (the same formulas; for the 512^3 box, where the
+    host versions take tens of seconds)."""
+    import torch
+    dev = f"cuda:{local}"
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    s = (slice(1, -1),) * 3
+    qd = t(q)
+    rho = qd[..., 0]
+    ajc = t(aj)[s]
+    vol = 1.0 / ajc
+    ke = float((0.5 * (qd[s + (1,)] ** 2 + qd[s + (2,)] ** 2 + qd[s + (3,)] ** 2) / rho[s] * vol).sum() / vol.sum())
+    u = [qd[..., a] / rho for a in (1, 2, 3)]
+    del qd
+    m = [t(csi)[s], t(eta)[s], t(zet)[s]]
+
+    def dc(f):
+        return (0.5 * (f[1:-1, 1:-1, 2:] - f[1:-1, 1:-1, :-2]), 0.5 * (f[1:-1, 2:, 1:-1] - f[1:-1, :-2, 1:-1]),
+                0.5 * (f[2:, 1:-1, 1:-1] - f[:-2, 1:-1, 1:-1]))
+
+    def grad(a, x):
+        d = dc(u[a])
+        return (d[0] * m[0][..., x] + d[1] * m[1][..., x] + d[2] * m[2][..., x]) * ajc
+
+    w2 = (grad(2, 1) - grad(1, 2)) ** 2
+    w2 += (grad(0, 2) - grad(2, 0)) ** 2
+    w2 += (grad(1, 0) - grad(0, 1)) ** 2
+    en = float((0.5 * rho[s] * w2 * vol).sum() / vol.sum())
+    del u, m, w2
+    torch.cuda.empty_cache()
+    return ke, en
+
+
+def _histories(blocks, q0, steps, every, diag):
+    """Both forms from q0 for `steps` steps: (KE, enstrophy) every `every`
+    steps and the final states."""
+    hist, final = {}, {}
+    for name, blk in blocks.items():
+        blk.SetInitialCondition(q0)
+        h = []
+        for c in range(steps // every + 1):
+            if c:
+                blk.RungeKutta(every)
+            q = blk.Q()
+            h.append(diag(q))
+        hist[name], final[name] = h, q
+    return hist, final
+
+
+def _history_devs(hist):
+    ke = max(abs(m[0] - f[0]) / abs(f[0]) for m, f in zip(hist["mixed"], hist["fp64"]))
+    en = max(abs(m[1] - f[1]) / abs(f[1]) for m, f in zip(hist["mixed"], hist["fp64"]))
+    return ke, en
+
+
+def run_config1(args, local, n=64):
+    """3-D inviscid isentropic vortex advection (Shu
+    vortex, beta 5, centre (5, 5), free stream rho = p = 1, u = (1, 1, 0)),
+    n^3 unique nodes on the periodic box [0, 10]^3 with identity metrics,
+    WENO5-JS + Rusanov, SSP-RK3, CFL 0.5, 200 steps, no viscosity, no LES.
+    Per form: cell-updates/s and the density error against the vortex
+    translated by t (1, 1, 0); mixed vs FP64: per-field error after the 200
+    steps and the kinetic-energy / enstrophy history deviation."""
+    import torch
+
+    from chimera_comp_les_b200 import diagnostics as D
+    from chimera_comp_les_b200 import workloads as W
+    torch.cuda.set_device(local)
+    L, steps = 10.0, 200
+    coords = W.periodic_grid(n, L, amp=0.0)
+    q0 = W.vortex_state(coords)
+    r = q0[..., 0]
+    u = np.abs(q0[..., 1] / r) + np.abs(q0[..., 2] / r)
+    c = np.sqrt(1.4 * 0.4 * (q0[..., 4] - 0.5 * (q0[..., 1] ** 2 + q0[..., 2] ** 2 + q0[..., 3] ** 2) / r) / r)
+    dt = 0.5 * (L / n) / float((u + c).max())  # CFL 0.5
+    opts = dict(les=0, inviscid=1, fluxorder=3, weno_order=5, dt=dt)
+    nv = np.zeros(coords.shape[:3])
+    out = {"workload": f"isentropic vortex {n}^3 (DMDA {n + 2}^3), periodic [0,10]^3, identity metrics, beta 5, "
+                       f"u = (1, 1, 0); WENO5-JS + Rusanov, inviscid, SSP-RK3, CFL 0.5, {steps} steps",
+           "grid": [n + 2] * 3, "dt": dt, "steps": steps}
+    blocks = {}
+    for prec in ("fp64", "mixed"):
+        blk = _block(prec, local, coords, q0, nv, **opts)
+        ms, _ = _timed(blk, args.steps, args.warmup, 1, local)
+        out[prec] = {"value": blk.interior_nodes * blk.stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps}
+        blocks[prec] = blk
+    csi, eta, zet, aj = blocks["fp64"].metrics()
+    hist, final = _histories(blocks, q0, steps, steps // 4,
+                             lambda q: (D.kinetic_energy(q, aj), D.enstrophy(q, csi, eta, zet, aj)))
+    t_end = steps * dt
+    shifted = coords.copy()
+    shifted[..., 0] = np.mod(coords[..., 0] - t_end, L)
+    shifted[..., 1] = np.mod(coords[..., 1] - t_end, L)
+    qe = W.vortex_state(shifted)
+    inner = (slice(1, -1),) * 3
+    for prec in ("fp64", "mixed"):
+        d = final[prec][inner + (0,)] - qe[inner + (0,)]
+        out[prec]["rho_error_vs_translated_vortex"] = float(np.linalg.norm(d) / np.linalg.norm(qe[inner + (0,)] - 1.0))
+        blocks[prec].close()
+    l2, linf = D.field_errors(final["mixed"], final["fp64"])
+    ke, en = _history_devs(hist)
+    out["mixed_vs_fp64_error"] = {"steps": steps, "rel_l2": l2, "rel_linf": linf,
+                                  "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"],
+                                  "ke_history_max_rel_dev": ke, "enstrophy_history_max_rel_dev": en,
+                                  "checkpoints_every": steps // 4}
+    return out
+
+
 def run_config5(args, local, n=512):
     """BASELINE config 5 at its largest size on one GPU: decaying compressible
     isotropic turbulence on a periodic [0, 2*pi]^3 Cartesian box of n^3 unique
@@ -497,7 +606,7 @@ def run_config5(args, local, n=512):
     out = {"workload": f"decaying isotropic turbulence {n}^3 (DMDA {n + 2}^3), Passot-Pouquet k0 4, u_rms 1, Mt 0.4, "
                        f"seed 5; {CONFIG5_SCHEME}",
            "grid": [n + 2] * 3, "dt": dt, "interior_nodes": n ** 3}
-    final = {}
+    final, hist = {}, {}
     for prec in ("fp64", "mixed"):
         blk = _block(prec, local, coords, q0, nv, **opts)
         ms, _ = _timed(blk, args.steps, args.warmup, 1, local)
@@ -506,14 +615,19 @@ def run_config5(args, local, n=512):
         out[prec] = {"value": interior * blk.stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
                      "kernel_avg_ms": kms, "achieved_gbs": B_ALG[prec] * interior / (kms / 1e3) / 1e9,
                      "kchunk_autotuned": blk.kchunk}
-        blk.SetInitialCondition(q0)
-        blk.RungeKutta(ACC_STEPS)
-        final[prec] = blk.Q()
+        if prec == "fp64":
+            met = blk.metrics()
+        h, f = _histories({prec: blk}, q0, ACC_STEPS, ACC_STEPS // 4,
+                          lambda q: _ke_enstrophy_device(q, *met, local))
+        hist[prec], final[prec] = h[prec], f[prec]
         blk.close()
     l2, linf = D.field_errors(final["mixed"], final["fp64"])
+    ke, en = _history_devs(hist)
     out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     out["mixed_vs_fp64_error"] = {"steps": ACC_STEPS, "rel_l2": l2, "rel_linf": linf,
-                                  "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]}
+                                  "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"],
+                                  "ke_history_max_rel_dev": ke, "enstrophy_history_max_rel_dev": en,
+                                  "checkpoints_every": ACC_STEPS // 4}
     return out
 
 
@@ -624,6 +738,7 @@ def run_ours(args, ws, rank, local):
 
     batched = run_batched(args, local) if (ws == 1 and not args.no_batched) else None
     config5 = run_config5(args, local) if (ws == 1 and not args.no_config5) else None
+    config1 = run_config1(args, local) if (ws == 1 and not args.no_config1) else None
 
     if rank == 0:
         peaks = pipe_peaks(local)
@@ -667,6 +782,7 @@ def run_ours(args, ws, rank, local):
             "roe": roe,
             "weno3_blend": blends,
             "config5_512": config5,
+            "config1_vortex": config1,
             "batched": batched,
             "vs_oracle": vs_oracle,
             "pipe_peaks": peaks,
@@ -957,6 +1073,7 @@ def main():
     ap.add_argument("--no-blend", action="store_true", help="skip the WENO3 blend (sigma 1 and 0.5) on the headline TGV")
     ap.add_argument("--no-extras", action="store_true", help="skip the Roe-flux measurement of the headline workload")
     ap.add_argument("--no-config5", action="store_true", help="skip the 512^3 isotropic-turbulence measurement")
+    ap.add_argument("--no-config1", action="store_true", help="skip the 64^3 isentropic-vortex measurement")
     ap.add_argument("--profile", action="store_true",
                     help="run the headline workload in one form for a profiler (no timing, no other workloads)")
     ap.add_argument("--profile-kchunk", type=int, default=10, help="k-chunk of the --profile run")
