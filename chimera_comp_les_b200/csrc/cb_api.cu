@@ -337,11 +337,16 @@ static int nut_update(cb_ctx *c) {
   }
   {
     TimedScope ts(c, false);
-    const int ekc = eddy_kchunk(c->dc, c->sms);
-    eddy_viscosity_kernel<<<eddy_grid(c->dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, c->stream>>>(
-        c->dc, c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr,
-        (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvz ? nullptr : c->nvert, c->nut, ekc,
-        dyn ? (const double *const *)(c->ptab + 5 * c->cur) : nullptr, dyn ? c->dyn_arena + 12 * c->plane : nullptr);
+    const double *const *qu = c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr;
+    if (c->cfg.precision == CB_MIXED && !dyn) {  // the mixed form's SGS terms run in FP32
+      CB_CUDA(c, launch_eddy_mixed(c->dc, qu, c->met4, c->nvz ? nullptr : c->nvert, c->nut, c->sms, c->stream));
+    } else {
+      const int ekc = eddy_kchunk(c->dc, c->sms);
+      eddy_viscosity_kernel<<<eddy_grid(c->dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, c->stream>>>(
+          c->dc, qu, (const double *const *)(c->ptab + PT_MET), c->aj, c->delta2, c->nvz ? nullptr : c->nvert, c->nut,
+          ekc, dyn ? (const double *const *)(c->ptab + 5 * c->cur) : nullptr,
+          dyn ? c->dyn_arena + 12 * c->plane : nullptr);
+    }
   }
   {
     TimedScope ts(c, false);

@@ -715,6 +715,12 @@ static int enqueue_nut(cb_batch *b) {
     const char *ent = reinterpret_cast<const char *>(b->d_tables + (size_t)(u * 13) * b->nb + k);
     const double *const *qu = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
     const double *const *mt = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, met));
+    if (b->cfg.precision == CB_MIXED) {  // the mixed form's SGS terms run in FP32
+      const float4 *m4[3] = {b->met4[0] + o, b->met4[1] + o, b->met4[2] + o};
+      BCUDA(b, launch_eddy_mixed(bh.dc, b->uc >= 0 ? qu : nullptr, m4, bh.nvz ? nullptr : b->nvert + o, b->nut + o,
+                                 b->sms, b->stream));
+      continue;
+    }
     const int ekc = eddy_kchunk(bh.dc, b->sms);
     eddy_viscosity_kernel<<<eddy_grid(bh.dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
                                                                  b->delta2 + o, bh.nvz ? nullptr : b->nvert + o, b->nut + o, ekc);

@@ -88,5 +88,11 @@ inline cudaError_t launch_batched_any(bool mix, bool les, const BatchBlock *tab,
 // (sum over directions of h(+1/2) - h(-1/2)) for the mixed form.
 cudaError_t launch_mixed_prep(const DevCfg &c, const double *const *met, const double *delta2, const double *aj,
                               float4 *const *met4, double *const *gcl, int grid, cudaStream_t s);
+// Compute_eddy_viscosity_LES with constant CS for the mixed form: FP32
+// velocity gradients and |S| from the FP32 metric vectors, nu_t into the FP64
+// plane nut (interior nodes); qu: the recorded state (nullptr: zero velocity);
+// nvert nullptr: no immersed body.  Defined in cb_mixed.cu.
+cudaError_t launch_eddy_mixed(const DevCfg &c, const double *const *qu, const float4 *const *met4, const double *nvert,
+                              double *nut, int sms, cudaStream_t s);
 
 }  // namespace cb
