@@ -134,6 +134,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.cb_batch_work_items.restype = I
     for name, args in [
         ("cb_batch_set_grid", [P, I, D]), ("cb_batch_set_nvert", [P, I, D]),
+        ("cb_batch_set_bctype", [P, I, IP]),
         ("cb_batch_upload_state", [P, I, D]), ("cb_batch_download_state", [P, I, D]),
         ("cb_batch_get_metrics", [P, I, D, D, D, D]),
         ("cb_batch_set_halo_map", [P, I, C.c_longlong, IP]), ("cb_batch_halo_periodic", [P]),

@@ -270,6 +270,14 @@ class Batch:
         n = np.ascontiguousarray(nvert, dtype=np.float64).reshape(self.shape(k))
         self._check(self.lib.cb_batch_set_nvert(self._b, k, dptr(n)))
 
+    def set_bctype(self, k: int, bctype: Sequence[int]):
+        """Face codes of block k (i-lo, i-hi, j-lo, j-hi, k-lo, k-hi), as one
+        line of the reference's bcs.dat per block (init.c:556-559): with a
+        code other than 7 the block runs its own FormBCS after every stage and
+        takes no halo-map destination."""
+        bc = (C.c_int * 6)(*[int(x) for x in bctype])
+        self._check(self.lib.cb_batch_set_bctype(self._b, k, bc))
+
     def SetInitialCondition(self, k: int, q: np.ndarray):
         a = np.ascontiguousarray(q, dtype=np.float64).reshape(self.shape(k) + (5,))
         self._check(self.lib.cb_batch_upload_state(self._b, k, dptr(a)))

@@ -97,6 +97,7 @@ struct BlockHost {
   int tiles_x, tiles_y;
   bool have_grid = false, have_state = false;
   bool nvz = true;      // the block's nvert is zero everywhere
+  bool phys = false;    // a physical face code: the block runs its own FormBCS
 };
 
 }  // namespace
@@ -137,6 +138,10 @@ struct cb_batch {
   long long *d_hdst = nullptr, *d_hsrc = nullptr, *d_wdst = nullptr, *d_wsrc = nullptr;
   unsigned char *d_hin = nullptr;
   bool ghosts_dirty = false;  // uploaded state still carries per-block ghosts
+  // blocks with a physical face code (cb_batch_set_bctype), and per map kind
+  // the blocks that hold a destination of that map
+  int nphys = 0;
+  std::vector<char> map_dst[2];
   // cross-process exchange (stage values, wrap values) and the phase state
   Xchg xs, xw;
   int xcur0 = -1, xnext = 0, xin = -1, xout = -1;
@@ -160,6 +165,13 @@ static int batch_flux_bits(const cb_config &f) {
   // WENO5-JS, whose reconstruction the W5 bit selects) the PLAIN variants
   if (f.twod == 0 && (f.fluxorder == 2 || f.weno_order == 5)) fl |= FLUX_PLAIN;
   return fl;
+}
+
+// The bits the batch launches with: a block with a physical face code needs
+// the boundary-code branches the PLAIN variants fold away.
+static int batch_bits(const cb_batch *b) {
+  const int fl = batch_flux_bits(b->cfg);
+  return b->nphys ? (fl & ~FLUX_PLAIN) : fl;
 }
 
 // every block's nvert is zero: the stage kernels' no-IBM variant
@@ -242,7 +254,7 @@ static int build_tables(cb_batch *b) {
     for (int z = 0; z < nch; z++)
       for (int y = 0; y < bh.tiles_y; y++)
         for (int x = 0; x < bh.tiles_x; x++) {
-          const int by = stage_tile_rows(batch_flux_bits(b->cfg));
+          const int by = stage_tile_rows(batch_bits(b));
           const int nxn = std::min(SBX, bh.mx - 2 - x * SBX), nyn = std::min(by, bh.my - 2 - y * by);
           const int nzn = std::min(b->kchunk, bh.mz - 2 - z * b->kchunk);
           // interior nodes plus the 3-plane prologue of each chunk
@@ -338,6 +350,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     d.ks = cfg->sigma_thrsh;
     d.abc = cfg->abc;
     d.flux = cfg->flux;
+    d.twall = cfg->twall;
     if (shell_count(d) >= (1LL << 31)) return bail(CB_E_ARG, "block too large for 32-bit boundary indexing");
     bh.off = off;
     off += (d.plane + 31) / 32 * 32;  // 256-byte aligned block starts
@@ -482,6 +495,42 @@ int cb_batch_set_nvert(cb_batch *b, int k, const double *nvert) {
   return CB_OK;
 }
 
+// Face codes of block k.  The reference reads one bcs.dat line per block
+// (init.c:556-559) and each block's RungeKutta ends every stage with its own
+// FormBCS (solvers.c:246-273, rhs.c:477-1227).  A block with a physical code
+// on any face runs that sequence here, on its own arrays, after every stage:
+// the RK combine of the boundary shell, the coded faces, the periodic
+// directions (code 7 on both faces wraps the block onto itself) and the
+// ghost layers -- the kernels and order of the single-block context, so the
+// block evolves exactly as it would alone.  Such a block takes no halo-map
+// destination; all six codes 7 make it an interface block again.
+int cb_batch_set_bctype(cb_batch *b, int k, const int *bctype) {
+  if (check_block(b, k) || !bctype) return CB_E_ARG;
+  for (int d = 0; d < 3; d++)
+    if ((bctype[2 * d] == 7) != (bctype[2 * d + 1] == 7))
+      return bfail(b, CB_E_UNSUPPORTED, "a periodic direction needs bctype 7 on both faces");
+  bool phys = false;
+  for (int f = 0; f < 6; f++) {
+    if (bctype[f] == 52 || bctype[f] == 47)
+      return bfail(b, CB_E_UNSUPPORTED,
+                   "inflow codes 52 and 47 (node coordinates and step index) are not built in the batched form");
+    phys = phys || bctype[f] != 7;
+  }
+  if (phys) {
+    for (int kind = 0; kind < 2; kind++)
+      if (!b->map_dst[kind].empty() && b->map_dst[kind][k])
+        return bfail(b, CB_E_ARG, "the block holds halo-map destinations; set face codes before the halo maps");
+    if (b->xs.nsend || b->xs.nrecv || b->xw.nsend || b->xw.nrecv)
+      return bfail(b, CB_E_UNSUPPORTED, "physical face codes with a cross-process exchange are not built");
+  }
+  BlockHost &bh = b->blk[k];
+  for (int f = 0; f < 6; f++) bh.dc.bctype[f] = bctype[f];
+  bh.phys = phys;
+  b->nphys = 0;
+  for (const auto &x : b->blk) b->nphys += x.phys ? 1 : 0;
+  return build_tables(b);  // the tables carry each block's config; graphs are rebuilt
+}
+
 // State of block k (5 per node, AoS) into the CURRENT buffer, ghosts by
 // periodic wrap (the halo gather replaces them at every stage).  Resets the
 // velocity record of the eddy viscosity, as cb_upload_state does.
@@ -593,10 +642,13 @@ int cb_batch_set_halo_map(cb_batch *b, int kind, long long n, const int *e) {
   if (!b || n < 0 || (n && !e) || (kind != CB_HALO_STAGE && kind != CB_HALO_WRAP)) return CB_E_ARG;
   std::vector<long long> hd((size_t)n), hs((size_t)n);
   std::vector<unsigned char> hin((size_t)n);
+  std::vector<char> dblk((size_t)b->nb, 0);
   for (long long t = 0; t < n; t++) {
     const int *r = e + 9 * t;
     if (r[0] < 0 || r[0] >= b->nb || r[4] < 0 || r[4] >= b->nb) return bfail(b, CB_E_ARG, "halo map: block index");
     const BlockHost &db = b->blk[r[0]], &sb = b->blk[r[4]];
+    if (db.phys) return bfail(b, CB_E_ARG, "halo map: destination in a block with a physical face code");
+    dblk[r[0]] = 1;
     if (r[1] < -2 || r[1] > db.mx + 1 || r[2] < -2 || r[2] > db.my + 1 || r[3] < -2 || r[3] > db.mz + 1 ||
         r[5] < -2 || r[5] > sb.mx + 1 || r[6] < -2 || r[6] > sb.my + 1 || r[7] < -2 || r[7] > sb.mz + 1)
       return bfail(b, CB_E_ARG, "halo map: node outside the padded box");
@@ -637,6 +689,7 @@ int cb_batch_set_halo_map(cb_batch *b, int kind, long long n, const int *e) {
       BCUDA(b, cudaMemcpy(b->d_hin, hin.data(), n, cudaMemcpyHostToDevice));
     }
   }
+  b->map_dst[kind] = dblk;
   if (kind == CB_HALO_WRAP) b->ghosts_dirty = true;
   destroy_graphs(b);
   return CB_OK;
@@ -651,6 +704,7 @@ int cb_batch_halo_periodic(cb_batch *b) {
   auto wrapi = [](int x, int m) { return x < 0 ? x + m : (x >= m ? x - m : x); };
   for (int k = 0; k < b->nb; k++) {
     const BlockHost &bh = b->blk[k];
+    if (bh.phys) continue;  // its own FormBCS wraps its periodic directions
     for (int kk = -2; kk <= bh.mz + 1; kk++)
       for (int j = -2; j <= bh.my + 1; j++)
         for (int i = -2; i <= bh.mx + 1; i++) {
@@ -725,11 +779,14 @@ static int enqueue_nut(cb_batch *b) {
     eddy_viscosity_kernel<<<eddy_grid(bh.dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
                                                                  b->delta2 + o, bh.nvz ? nullptr : b->nvert + o, b->nut + o, ekc);
   }
-  if (b->nwrap || b->xw.nsend || b->xw.nrecv) {
-    if (b->nwrap) plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, b->nut);
-  } else {
+  const bool mapped = b->nwrap || b->xw.nsend || b->xw.nrecv;
+  if (b->nwrap) plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, b->nut);
+  if (!mapped || b->nphys) {
+    // each block's own ghost fill (a block with physical faces always: the
+    // single-block context's rule)
     for (int k = 0; k < b->nb; k++) {
       const BlockHost &bh = b->blk[k];
+      if (mapped && !bh.phys) continue;
       // a one-entry pointer table: the nut plane of block k sits in the table's nut member
       const char *ent = reinterpret_cast<const char *>(b->d_tables + k);
       double *const *np = reinterpret_cast<double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, nut));
@@ -742,16 +799,17 @@ static int enqueue_nut(cb_batch *b) {
 
 // Ghost layers of the three planes of one sensor pass (arena pointers `ar`,
 // per-block pointer tables at offset `toff` of a block's six): the wrap map
-// when the batch has one, else each block's own periodic wrap.
+// when the batch has one, else each block's own periodic wrap; a block with a
+// physical face code always takes its own.
 static int sigma_ghosts(cb_batch *b, double *const ar[3], int toff) {
   if (b->nwrap) {
     for (int a = 0; a < 3; a++)
       plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, ar[a]);
-  } else {
-    for (int k = 0; k < b->nb; k++)
+  }
+  for (int k = 0; k < b->nb; k++)
+    if (!b->nwrap || b->blk[k].phys)
       ghost_fill_kernel<<<bgrid(b, shell_count(b->blk[k].dc)), 256, 0, b->stream>>>(b->blk[k].dc,
                                                                                     b->d_sigptr + 6 * k + toff, 3);
-  }
   BCUDA(b, cudaGetLastError());
   return CB_OK;
 }
@@ -792,7 +850,7 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
     BCUDA(b, cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream));
     const int ctas = b->sms * (mixed ? 2 : 1);
     BCUDA(b, launch_batched_any(mixed, les, tab, b->d_items, b->nitems, b->d_counter, s, alfa, beta, adt, visc,
-                                batch_flux_bits(b->cfg), batch_nv0(b), ctas, b->stream));
+                                batch_bits(b), batch_nv0(b), ctas, b->stream));
   } else {
     for (int k = 0; k < b->nb; k++) {
       const BlockHost &bh = b->blk[k];
@@ -809,7 +867,7 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
         const double cost = (double)((blocks + slots - 1) / slots) * (cand + 1.0);
         if (cost < best) { best = cost; kc = cand; }
       }
-      BCUDA(b, launch_stage_any(mixed, les, bh.dc, F, s, alfa, beta, adt, kc, visc, false, batch_flux_bits(b->cfg),
+      BCUDA(b, launch_stage_any(mixed, les, bh.dc, F, s, alfa, beta, adt, kc, visc, false, batch_bits(b),
                                 bh.nvz && !b->cfg.visT, slots, b->stream));
     }
   }
@@ -818,6 +876,27 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
     DevFields G{};
     for (int q = 0; q < 5; q++) { G.q[q] = b->qb[in][q]; G.qout[q] = b->qb[out][q]; }
     halo_gather_kernel<<<bgrid(b, b->nhalo), 256, 0, b->stream>>>(b->d_hdst, b->d_hsrc, b->d_hin, b->nhalo, G);
+    BCUDA(b, cudaGetLastError());
+  }
+  // blocks with a physical face code: FormBCS with boundary codes on the
+  // block's own arrays (rhs.c:477-1227), the single-block context's kernels
+  // in its order; no halo-map entry writes into these blocks
+  for (int k = 0; k < b->nb && b->nphys; k++) {
+    const BlockHost &bh = b->blk[k];
+    if (!bh.phys) continue;
+    const DevCfg &d = bh.dc;
+    const DevFields F = block_fields(b, k, in, old, out);
+    const long long shell = shell_count(d);
+    bc_combine_kernel<<<bgrid(b, shell), 256, 0, b->stream>>>(d, F, s, alfa, beta, adt);
+    const long long face = (long long)std::max(d.mx, d.my) * std::max(d.my, d.mz);
+    for (int dir = 0; dir < 3; dir++) bc_face_kernel<<<bgrid(b, face), 256, 0, b->stream>>>(d, F, dir, alfa);
+    for (int dir = 0; dir < 3; dir++)
+      if (d.bctype[2 * dir] == 7) bc_periodic_dir_kernel<<<bgrid(b, face), 256, 0, b->stream>>>(d, F, dir);
+    // the stage output's five plane pointers: the qout member of the block's
+    // table entry for this buffer triple (device memory)
+    const char *ent = reinterpret_cast<const char *>(tab + k);
+    double *const *qo = reinterpret_cast<double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, qout));
+    ghost_fill_kernel<<<bgrid(b, shell), 256, 0, b->stream>>>(d, qo, 5);
     BCUDA(b, cudaGetLastError());
   }
   return CB_OK;
@@ -859,7 +938,8 @@ int cb_batch_rk_step(cb_batch *b, int nsteps, int mode) {
   if (!b || nsteps < 0 || (mode != 0 && mode != 1)) return CB_E_ARG;
   for (auto &bh : b->blk)
     if (!bh.have_grid || !bh.have_state) return bfail(b, CB_E_STATE, "every block needs a grid and a state");
-  if (!b->nhalo) return bfail(b, CB_E_STATE, "no halo map (cb_batch_set_halo_map / cb_batch_halo_periodic)");
+  if (!b->nhalo && b->nphys < b->nb)
+    return bfail(b, CB_E_STATE, "no halo map (cb_batch_set_halo_map / cb_batch_halo_periodic)");
   if (b->xs.nsend || b->xs.nrecv || b->xw.nsend || b->xw.nrecv)
     return bfail(b, CB_E_STATE, "a batch with a cross-process exchange steps through cb_batch_phase");
   if (b->ghosts_dirty && fill_ghosts(b)) return CB_E_CUDA;
@@ -904,6 +984,8 @@ int cb_batch_set_exchange(cb_batch *b, int kind, long long nsend, const int *sen
     return CB_E_ARG;
   if (b->sig_arena && (nsend || nrecv))
     return bfail(b, CB_E_UNSUPPORTED, "the shock sensor with a cross-process exchange is not built");
+  if (b->nphys && (nsend || nrecv))
+    return bfail(b, CB_E_UNSUPPORTED, "physical face codes with a cross-process exchange are not built");
   const int sw = kind == CB_HALO_STAGE ? 5 : 4;
   std::vector<long long> hs((size_t)nsend), hd((size_t)nrecv);
   std::vector<unsigned char> hf((size_t)nsend);
@@ -1092,7 +1174,7 @@ int cb_batch_autotune(cb_batch *b, int *best_kchunk, double *best_ms) {
       cudaEventRecord(e0, b->stream);
       const int ctas = b->sms * (mixed ? 2 : 1);
       launch_batched_any(mixed, les, tab, b->d_items, b->nitems, b->d_counter, 0, 1.0, 1.0, 0.0, visc,
-                         batch_flux_bits(b->cfg), batch_nv0(b), ctas, b->stream);
+                         batch_bits(b), batch_nv0(b), ctas, b->stream);
       cudaEventRecord(e1, b->stream);
       BCUDA(b, cudaEventSynchronize(e1));
       float ms = 0.f;

@@ -345,8 +345,9 @@ int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const double *d_q
  * k-chunk) work items, largest first, from a device counter, then one
  * on-device gather that fills every block's boundary and ghost nodes from a
  * halo map.  A whole step runs as a CUDA graph.  Blocks share the cb_config
- * (bctype is ignored: block faces are interfaces filled by the halo map);
- * their sizes may differ.  With les and calc_sigma every block computes the
+ * (its bctype is ignored); their sizes may differ.  By default every block
+ * face is an interface filled by the halo map; cb_batch_set_bctype gives a
+ * block its own face codes instead.  With les and calc_sigma every block computes the
  * shock sensor's weights from its own arrays at the first stage of a step,
  * each pass followed by the wrap map (a batch with a cross-process exchange
  * refuses the sensor with CB_E_UNSUPPORTED).
@@ -366,6 +367,19 @@ void *cb_batch_stream(cb_batch *b);
 int cb_batch_work_items(const cb_batch *b);
 int cb_batch_set_grid(cb_batch *b, int block, const double *coor);
 int cb_batch_set_nvert(cb_batch *b, int block, const double *nvert);
+/* Face codes of one block (6 ints: i-lo, i-hi, j-lo, j-hi, k-lo, k-hi, the
+ * codes of cb_config.bctype), replacing the reference's per-block bcs.dat line
+ * (init.c:556-559) and that block's FormBCS inside RungeKutta (solvers.c:246-273,
+ * rhs.c:477-1227).  With a code other than 7 on any face the block runs the
+ * single-block context's FormBCS on its own arrays after every stage (code 7
+ * on both faces of a direction wraps the block onto itself), so it evolves
+ * exactly as a cb_ctx with the same codes; it may then hold no halo-map
+ * destination (set codes before the halo maps; cb_batch_halo_periodic skips
+ * such blocks) and the batch takes no cross-process exchange.  Six codes 7
+ * make it an interface block again.  CB_E_UNSUPPORTED for a direction with 7
+ * on one face only and for the inflow codes 52 and 47; CB_E_ARG if the block
+ * already holds a halo-map destination. */
+int cb_batch_set_bctype(cb_batch *b, int block, const int *bctype);
 int cb_batch_upload_state(cb_batch *b, int block, const double *q);
 int cb_batch_download_state(cb_batch *b, int block, double *q);
 /* CFL time step over all blocks: dt = cfl / (largest spectral radius of any
