@@ -219,7 +219,8 @@ class Batch:
                  precision: str = "fp64", device: int = 0, calc_sigma: int = 0, visT: int = 0,
                  tref: float = 273.15, twod: int = 0, flux: str = "rusanov", weno_order: int = 3,
                  s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5,
-                 abc: int = 0):
+                 abc: int = 0, max_cs: float = 0.05, i_homo_filter: int = 0, j_homo_filter: int = 0,
+                 k_homo_filter: int = 0, testfilter_ik: int = 0):
         self.lib = _lib.load()
         self.dims = [tuple(int(x) for x in d) for d in dims]
         cfg = CbConfig()
@@ -230,7 +231,8 @@ class Batch:
                          dt=dt, st=st, cs_const=cs_const, ci=ci, ratio=ratio, device=device,
                          calc_sigma=calc_sigma, visT=visT, tref=tref, twod=twod, weno_order=weno_order,
                          s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh,
-                         abc=abc).items():
+                         abc=abc, max_cs=max_cs, i_homo_filter=i_homo_filter, j_homo_filter=j_homo_filter,
+                         k_homo_filter=k_homo_filter, testfilter_ik=testfilter_ik).items():
             setattr(cfg, k, v)
         cfg.flux = {"rusanov": 0, "roe": 1}[flux] if isinstance(flux, str) else int(flux)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]

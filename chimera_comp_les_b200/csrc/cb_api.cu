@@ -264,62 +264,13 @@ static int dynamic_cs(cb_ctx *c) {
   TimedScope ts(c, false);
   const double *const *q = (const double *const *)(c->ptab + 5 * c->cur);
   const double *const *qu = c->uc >= 0 ? (const double *const *)(c->ptab + 5 * c->uc) : nullptr;
-  double *const *D = c->ptab + PT_DYN;
   double *base = c->dyn_arena;
-  double *Sabs = base + 9 * c->plane, *LM = base + 10 * c->plane, *MM = base + 11 * c->plane;
-  double *CS = base + 12 * c->plane, *CT = base + 13 * c->plane;
-  const int gp = grid_for(c, (long long)c->plane);
-  const long long shell = shell_count(c->dc);
-  const long long faces = (long long)(c->dc.my - 2) * (c->dc.mz - 2) + (long long)(c->dc.mx - 2) * (c->dc.mz - 2) +
-                          (long long)(c->dc.mx - 2) * (c->dc.my - 2);
-  dyn_grad_kernel<<<gp, 256, 0, c->stream>>>(c->dc, q, qu, (const double *const *)(c->ptab + PT_MET), c->aj,
-                                             c->nvert, D, Sabs);
-  ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D, 10);  // DMLocalToLocal
-  dyn_copy_kernel<<<grid_for(c, faces), 256, 0, c->stream>>>(c->dc, D, 9);
-  // LM / MM: zero on the whole box (the reference's VecSet), then the interior tiles
-  CB_CUDA(c, cudaMemsetAsync(LM, 0, sizeof(double) * 2 * c->plane, c->stream));
-  {
-    const int kc = std::min(8, c->dc.mz - 2);
-    const dim3 grid((c->dc.mx - 2 + DYN_BX - 1) / DYN_BX, (c->dc.my - 2 + DYN_BY - 1) / DYN_BY,
-                    (c->dc.mz - 2 + kc - 1) / kc);
-    dyn_lm_tiled_kernel<<<grid, dim3(DYN_BX, DYN_BY), DYN_LM_SMEM, c->stream>>>(
-        c->dc, q, qu, c->aj, c->nvert, (const double *const *)D, Sabs, LM, MM, kc, c->dyn_tf_mult);
-  }
-  ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D + 10, 2);
+  const size_t pl = c->plane;
+  const DynPlanes P{c->ptab + PT_DYN, base + 9 * pl, base + 10 * pl, base + 11 * pl, base + 12 * pl, base + 13 * pl};
   const cb_config &f = c->cfg;
-  const bool homo = f.i_homo_filter || f.j_homo_filter || f.k_homo_filter;
-  const bool pointwise = homo || f.les == 3;  // les.c:916-922
-  const long long owned = (long long)c->dc.mx * c->dc.my * c->dc.mz;
-  dyn_cs_kernel<<<grid_for(c, owned), 256, 0, c->stream>>>(c->dc, c->nvert, LM, MM, CS, f.max_cs, pointwise ? 1 : 0,
-                                                          homo ? 0 : 1);
-  if (homo) {
-    // the reference's homogeneous branches in order; with all three filters
-    // the box value overwrites every node the plane means wrote
-    const bool box = f.i_homo_filter && f.j_homo_filter && f.k_homo_filter;
-    if (f.i_homo_filter && f.k_homo_filter && !box)
-      dyn_homo_plane_kernel<<<c->dc.my - 2, DYN_RED, 0, c->stream>>>(c->dc, c->nvert, LM, MM, CS);
-    if (f.i_homo_filter && !f.k_homo_filter)
-      dyn_homo_line_kernel<<<grid_for(c, (long long)(c->dc.my - 2) * (c->dc.mz - 2)), 256, 0, c->stream>>>(
-          c->dc, c->nvert, LM, MM, CS);
-    // CT is scratch here: 2 * nparts + 1 doubles of its plane
-    const int nparts = (int)std::max(1LL, std::min((long long)2 * c->sms, (long long)(c->plane - 1) / 2));
-    if (box) {
-      dyn_homo_box_partial_kernel<<<nparts, DYN_RED, 0, c->stream>>>(c->dc, LM, MM, CT);
-      dyn_homo_box_final_kernel<<<1, DYN_RED, 0, c->stream>>>(CT, nparts);
-    }
-    dyn_clip_kernel<<<grid_for(c, owned), 256, 0, c->stream>>>(c->dc, c->nvert, CS, f.max_cs,
-                                                              box ? CT + 2 * nparts : nullptr);
-  }
-  if (pointwise) {  // no final weighted mean (les.c:1302)
-    CB_CUDA(c, cudaGetLastError());
-    return CB_OK;
-  }
-  CB_CUDA(c, cudaMemcpyAsync(CT, CS, sizeof(double) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
-  ghost_fill_kernel<<<grid_for(c, shell), 256, 0, c->stream>>>(c->dc, D + 13, 1);  // DMGlobalToLocal
-  dyn_copy_kernel<<<grid_for(c, faces), 256, 0, c->stream>>>(c->dc, D + 13, 1);
-  dyn_avg_kernel<<<grid_for(c, (long long)(c->dc.mx - 2) * (c->dc.my - 2) * (c->dc.mz - 2)), 256, 0, c->stream>>>(
-      c->dc, c->aj, c->nvert, CT, CS);
-  CB_CUDA(c, cudaGetLastError());
+  const DynOpts o{f.les, f.max_cs, c->dyn_tf_mult, f.i_homo_filter, f.j_homo_filter, f.k_homo_filter};
+  CB_CUDA(c, dyn_cs_enqueue(c->dc, o, q, qu, (const double *const *)(c->ptab + PT_MET), c->aj, c->nvert, P, c->sms,
+                            c->stream));
   return CB_OK;
 }
 

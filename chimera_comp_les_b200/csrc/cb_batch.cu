@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -31,6 +32,7 @@
 #include "../../include/chimera_b200.h"
 #include "cb_aux.cuh"
 #include "cb_common.cuh"
+#include "cb_dyn.cuh"
 #include "cb_launch.h"
 #include "cb_stage.cuh"
 
@@ -120,6 +122,11 @@ struct cb_batch {
   double *sig_arena = nullptr;
   double *sig_a[3] = {}, *sig_b[3] = {};
   double **d_sigptr = nullptr;
+  // dynamic Smagorinsky model (-les 2/3): 14 planes, each `total` long, and
+  // per block a device table of its 14 plane pointers
+  double *dyn_arena = nullptr;
+  double **d_dynptr = nullptr;
+  double dyn_tf_mult = 2.0;
   void *arena_mixed = nullptr;
   float4 *met4[3] = {};
   double *gcl[3] = {};
@@ -166,6 +173,9 @@ static int batch_flux_bits(const cb_config &f) {
   if (f.twod == 0 && (f.fluxorder == 2 || f.weno_order == 5)) fl |= FLUX_PLAIN;
   return fl;
 }
+
+// -les 2, 3, ... (not 10): the dynamic model (Compute_Smagorinsky_Constant_1)
+static bool batch_dynamic(const cb_config &f) { return f.les >= 2 && f.les != 10; }
 
 // The bits the batch launches with: a block with a physical face code needs
 // the boundary-code branches the PLAIN variants fold away.
@@ -310,12 +320,13 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     return code;
   };
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
-      (cfg->les != 0 && cfg->les != 1) || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
+      cfg->les < 0 || cfg->les == 10 || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
       (cfg->flux != 0 && cfg->flux != 1) ||
       (cfg->weno_order != 3 && cfg->weno_order != 5))
     return bail(CB_E_UNSUPPORTED, "option combination not built");
   if (cfg->weno_order == 5 && cfg->fluxorder != 3) return bail(CB_E_ARG, "weno_order 5 needs fluxorder 3");
   if (cfg->visT && !(cfg->tref > 0.0)) return bail(CB_E_ARG, "Tref must be > 0 with visT");
+  if (batch_dynamic(*cfg) && !(cfg->max_cs >= 0.0)) return bail(CB_E_ARG, "max_cs must be >= 0");
   b->dev = cfg->device;
   if (cudaSetDevice(b->dev) != cudaSuccess) return bail(CB_E_CUDA, "cudaSetDevice");
   cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->dev);
@@ -383,6 +394,21 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     for (int a = 0; a < 3; a++) b->gcl[a] = g + (size_t)b->total * a;
     if (cudaMalloc(&b->ptab4, sizeof(float4 *) * 3) != cudaSuccess) return bail(CB_E_CUDA, "ptab4");
   }
+  if (batch_dynamic(*cfg)) {
+    b->dyn_tf_mult = cfg->testfilter_ik ? pow(5.0, 1. / 3.) : 2.0;  // the host's pow, as the reference's
+    if (cudaFuncSetAttribute(dyn_lm_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DYN_LM_SMEM) !=
+        cudaSuccess)
+      return bail(CB_E_CUDA, "dynamic-model kernel attributes");
+    const size_t db = sizeof(double) * (size_t)b->total * 14;
+    if (cudaMalloc(&b->dyn_arena, db) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc dynamic-model planes");
+    cudaMemsetAsync(b->dyn_arena, 0, db, b->stream);
+    std::vector<double *> hp((size_t)14 * nblocks);
+    for (int k = 0; k < nblocks; k++)
+      for (int a = 0; a < 14; a++) hp[14 * k + a] = b->dyn_arena + (size_t)b->total * a + b->blk[k].off;
+    if (cudaMalloc(&b->d_dynptr, sizeof(double *) * hp.size()) != cudaSuccess) return bail(CB_E_CUDA, "dynamic table");
+    if (cudaMemcpy(b->d_dynptr, hp.data(), sizeof(double *) * hp.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(CB_E_CUDA, "dynamic table");
+  }
   if (cfg->les && cfg->calc_sigma) {
     const size_t sb = sizeof(double) * (size_t)b->total * 6;
     if (cudaMalloc(&b->sig_arena, sb) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc sensor planes");
@@ -420,7 +446,8 @@ void cb_batch_destroy(cb_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
   destroy_graphs(b);
-  void *ptrs[] = {b->arena, b->arena_mixed, b->sig_arena, b->d_sigptr, b->staging, b->ptab, b->ptab4, b->d_tables,
+  void *ptrs[] = {b->arena, b->arena_mixed, b->sig_arena, b->d_sigptr, b->dyn_arena, b->d_dynptr, b->staging, b->ptab,
+                  b->ptab4, b->d_tables,
                   b->d_items, b->d_counter,
                   b->status, b->d_hdst, b->d_hsrc, b->d_hin, b->d_wdst, b->d_wsrc,
                   b->xs.d_src, b->xs.d_dst, b->xs.d_fin, b->xw.d_src, b->xw.d_dst, b->xw.d_fin};
@@ -762,6 +789,9 @@ static int enqueue_nut(cb_batch *b) {
   // pointer arrays are the q and met members of the block's (uc, uc, uc)
   // table entry in device memory
   const int u = b->uc < 0 ? 0 : b->uc;
+  const bool dyn = batch_dynamic(b->cfg);
+  const cb_config &f = b->cfg;
+  const DynOpts dopt{f.les, f.max_cs, b->dyn_tf_mult, f.i_homo_filter, f.j_homo_filter, f.k_homo_filter};
   for (int k = 0; k < b->nb; k++) {
     const BlockHost &bh = b->blk[k];
     const long long o = bh.off;
@@ -769,15 +799,31 @@ static int enqueue_nut(cb_batch *b) {
     const char *ent = reinterpret_cast<const char *>(b->d_tables + (size_t)(u * 13) * b->nb + k);
     const double *const *qu = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
     const double *const *mt = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, met));
-    if (b->cfg.precision == CB_MIXED) {  // the mixed form's SGS terms run in FP32
+    // the current state's planes: the q member of the block's (cur, cur, cur) entry
+    const char *ecur = reinterpret_cast<const char *>(b->d_tables + (size_t)(b->cur * 13) * b->nb + k);
+    const double *const *qc = reinterpret_cast<const double *const *>(ecur + offsetof(BatchBlock, F) + offsetof(DevFields, q));
+    double *cs = nullptr;
+    if (dyn) {
+      // the model on the block's own arrays and ghost layers, as each block of
+      // the reference computes it on its own DMDA
+      double *const *D = b->d_dynptr + 14 * k;
+      double *pl[14];
+      for (int a = 0; a < 14; a++) pl[a] = b->dyn_arena + (size_t)b->total * a + o;
+      const DynPlanes P{D, pl[9], pl[10], pl[11], pl[12], pl[13]};
+      BCUDA(b, dyn_cs_enqueue(bh.dc, dopt, qc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o, b->nvert + o, P, b->sms,
+                              b->stream));
+      cs = pl[12];
+    }
+    if (b->cfg.precision == CB_MIXED && !dyn) {  // the mixed form's SGS terms run in FP32
       const float4 *m4[3] = {b->met4[0] + o, b->met4[1] + o, b->met4[2] + o};
       BCUDA(b, launch_eddy_mixed(bh.dc, b->uc >= 0 ? qu : nullptr, m4, bh.nvz ? nullptr : b->nvert + o, b->nut + o,
                                  b->sms, b->stream));
       continue;
     }
     const int ekc = eddy_kchunk(bh.dc, b->sms);
-    eddy_viscosity_kernel<<<eddy_grid(bh.dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, b->stream>>>(bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o,
-                                                                 b->delta2 + o, bh.nvz ? nullptr : b->nvert + o, b->nut + o, ekc);
+    eddy_viscosity_kernel<<<eddy_grid(bh.dc, ekc), dim3(EDDY_BX, EDDY_BY), 0, b->stream>>>(
+        bh.dc, b->uc >= 0 ? qu : nullptr, mt, b->aj + o, b->delta2 + o, bh.nvz ? nullptr : b->nvert + o, b->nut + o, ekc,
+        dyn ? qc : nullptr, cs);
   }
   const bool mapped = b->nwrap || b->xw.nsend || b->xw.nrecv;
   if (b->nwrap) plane_gather_kernel<<<bgrid(b, b->nwrap), 256, 0, b->stream>>>(b->d_wdst, b->d_wsrc, b->nwrap, b->nut);

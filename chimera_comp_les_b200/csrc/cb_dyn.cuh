@@ -414,4 +414,84 @@ static __global__ void dyn_avg_kernel(const DevCfg c, const double *aj, const do
   }
 }
 
+// ------------------------------------------------------ launch sequence ----
+// The options of the model (the -les value, -max_cs, -i/-j/-k_homo_filter
+// and the test-filter width ratio of -testfilter_ik).
+struct DynOpts {
+  int les;
+  double max_cs, tf_mult;
+  int i_homo, j_homo, k_homo;
+};
+// The plane pointers of one block: d a device table of 14 (du/dx .. dw/dz,
+// |S|, LM, MM, CS, lCS), the rest the same planes as host-held pointers.
+struct DynPlanes {
+  double *const *d;
+  double *sabs, *lm, *mm, *cs, *ct;
+};
+
+static inline int dyn_grid(long long work, int sms) {
+  long long b = (work + 255) / 256, cap = (long long)sms * 8;
+  return (int)(b > cap ? cap : (b < 1 ? 1 : b));
+}
+
+// Compute_Smagorinsky_Constant_1 with a dynamic -les on one block, enqueued
+// on `st`: q the current state, qu the last CalcUCat state (nullptr: zero
+// velocity), met the 9 metric planes (device table).  CS ends in P.cs.  The
+// kernels' dynamic shared memory (DYN_LM_SMEM) must have been opted in by the
+// calling translation unit.
+static cudaError_t dyn_cs_enqueue(const DevCfg &dc, const DynOpts &o, const double *const *q, const double *const *qu,
+                                  const double *const *met, const double *aj, const double *nvert, const DynPlanes &P,
+                                  int sms, cudaStream_t st) {
+  double *const *D = P.d;
+  const long long plane = dc.plane;
+  const int gp = dyn_grid(plane, sms);
+  const long long shell = shell_count(dc);
+  const long long faces = (long long)(dc.my - 2) * (dc.mz - 2) + (long long)(dc.mx - 2) * (dc.mz - 2) +
+                          (long long)(dc.mx - 2) * (dc.my - 2);
+  dyn_grad_kernel<<<gp, 256, 0, st>>>(dc, q, qu, met, aj, nvert, D, P.sabs);
+  ghost_fill_kernel<<<dyn_grid(shell, sms), 256, 0, st>>>(dc, D, 10);  // DMLocalToLocal
+  dyn_copy_kernel<<<dyn_grid(faces, sms), 256, 0, st>>>(dc, D, 9);
+  // LM / MM: zero on the whole box (the reference's VecSet), then the interior tiles
+  cudaError_t e = cudaMemsetAsync(P.lm, 0, sizeof(double) * plane, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(P.mm, 0, sizeof(double) * plane, st);
+  if (e != cudaSuccess) return e;
+  {
+    const int kc = dc.mz - 2 < 8 ? dc.mz - 2 : 8;
+    const dim3 grid((dc.mx - 2 + DYN_BX - 1) / DYN_BX, (dc.my - 2 + DYN_BY - 1) / DYN_BY, (dc.mz - 2 + kc - 1) / kc);
+    dyn_lm_tiled_kernel<<<grid, dim3(DYN_BX, DYN_BY), DYN_LM_SMEM, st>>>(dc, q, qu, aj, nvert, (const double *const *)D,
+                                                                          P.sabs, P.lm, P.mm, kc, o.tf_mult);
+  }
+  ghost_fill_kernel<<<dyn_grid(shell, sms), 256, 0, st>>>(dc, D + 10, 2);
+  const bool homo = o.i_homo || o.j_homo || o.k_homo;
+  const bool pointwise = homo || o.les == 3;  // les.c:916-922
+  const long long owned = (long long)dc.mx * dc.my * dc.mz;
+  dyn_cs_kernel<<<dyn_grid(owned, sms), 256, 0, st>>>(dc, nvert, P.lm, P.mm, P.cs, o.max_cs, pointwise ? 1 : 0,
+                                                      homo ? 0 : 1);
+  if (homo) {
+    // the reference's homogeneous branches in order; with all three filters
+    // the box value overwrites every node the plane means wrote
+    const bool box = o.i_homo && o.j_homo && o.k_homo;
+    if (o.i_homo && o.k_homo && !box) dyn_homo_plane_kernel<<<dc.my - 2, DYN_RED, 0, st>>>(dc, nvert, P.lm, P.mm, P.cs);
+    if (o.i_homo && !o.k_homo)
+      dyn_homo_line_kernel<<<dyn_grid((long long)(dc.my - 2) * (dc.mz - 2), sms), 256, 0, st>>>(dc, nvert, P.lm, P.mm,
+                                                                                                 P.cs);
+    // lCS is scratch here: 2 * nparts + 1 doubles of its plane
+    const long long np = (plane - 1) / 2 < 2LL * sms ? (plane - 1) / 2 : 2LL * sms;
+    const int nparts = (int)(np < 1 ? 1 : np);
+    if (box) {
+      dyn_homo_box_partial_kernel<<<nparts, DYN_RED, 0, st>>>(dc, P.lm, P.mm, P.ct);
+      dyn_homo_box_final_kernel<<<1, DYN_RED, 0, st>>>(P.ct, nparts);
+    }
+    dyn_clip_kernel<<<dyn_grid(owned, sms), 256, 0, st>>>(dc, nvert, P.cs, o.max_cs, box ? P.ct + 2 * nparts : nullptr);
+  }
+  if (pointwise) return cudaGetLastError();  // no final weighted mean (les.c:1302)
+  e = cudaMemcpyAsync(P.ct, P.cs, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return e;
+  ghost_fill_kernel<<<dyn_grid(shell, sms), 256, 0, st>>>(dc, D + 13, 1);  // DMGlobalToLocal
+  dyn_copy_kernel<<<dyn_grid(faces, sms), 256, 0, st>>>(dc, D + 13, 1);
+  dyn_avg_kernel<<<dyn_grid((long long)(dc.mx - 2) * (dc.my - 2) * (dc.mz - 2), sms), 256, 0, st>>>(dc, aj, nvert, P.ct,
+                                                                                                     P.cs);
+  return cudaGetLastError();
+}
+
 }  // namespace cb

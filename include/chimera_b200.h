@@ -350,7 +350,10 @@ int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const double *d_q
  * block its own face codes instead.  With les and calc_sigma every block computes the
  * shock sensor's weights from its own arrays at the first stage of a step,
  * each pass followed by the wrap map (a batch with a cross-process exchange
- * refuses the sensor with CB_E_UNSUPPORTED).
+ * refuses the sensor with CB_E_UNSUPPORTED).  With a dynamic -les (2, 3, not
+ * 10) every block computes its Smagorinsky coefficient from its own arrays
+ * and ghost layers once per step, as each block of the reference does on its
+ * own DMDA (les.c:151-1472); -les 10 is refused with CB_E_UNSUPPORTED.
  *
  * Per block k: cb_batch_set_grid (coordinates, 3 per node, AoS, as
  * cb_set_grid), cb_batch_set_nvert (optional; default 0), cb_batch_upload_state

@@ -74,6 +74,12 @@ VARIANTS = [
     # that reach it)
     ("sensor", dict(calc_sigma=1, s_x=0.5, s_y=0.6, s_z=0.7, s_x_min=0.05, sigma_thrsh=1e-4, abc=9)),
     ("sensor_weno5_roe", dict(calc_sigma=1, weno_order=5, flux="roe", s_x=0.8, s_y=0.8, s_z=0.8)),
+    # the dynamic Smagorinsky model per block (Germano 27-node means, -les 3
+    # pointwise, the homogeneous plane and box means, the -testfilter_ik width)
+    ("dynamic", dict(les=2, max_cs=0.1)),
+    ("dynamic_les3", dict(les=3, max_cs=0.1)),
+    ("dynamic_homo_ik", dict(les=2, i_homo_filter=1, k_homo_filter=1, max_cs=0.1)),
+    ("dynamic_box_tf", dict(les=2, i_homo_filter=1, j_homo_filter=1, k_homo_filter=1, testfilter_ik=1, max_cs=0.1)),
 ]
 
 

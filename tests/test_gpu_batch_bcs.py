@@ -32,6 +32,8 @@ CASES = [
     ("muscl_roe", dict(les=0, fluxorder=2, flux="roe")),
     # the shock sensor: a coded block fills its planes' ghosts itself
     ("sensor", dict(les=1, fluxorder=3, calc_sigma=1, s_x=0.5, s_y=0.6, s_z=0.7, s_x_min=0.05, sigma_thrsh=1e-4)),
+    # the dynamic model on a coded block's own arrays
+    ("dynamic", dict(les=2, fluxorder=3, max_cs=0.1, s_x=0.4, s_y=0.7, s_z=0.9)),
 ]
 
 
