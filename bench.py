@@ -514,9 +514,10 @@ def _ke_enstrophy_device(q, csi, eta, zet, aj, local):
     return ke, en
 
 
-def _histories(blocks, q0, steps, every, diag):
+def _histories(blocks, q0, steps, every, diag, keep=None):
     """Both forms from q0 for `steps` steps: (KE, enstrophy) every `every`
-    steps and the final states."""
+    steps and the final states; with `keep` (a dict) also the states after
+    the step counts it lists as keys, into keep[step][form]."""
     hist, final = {}, {}
     for name, blk in blocks.items():
         blk.SetInitialCondition(q0)
@@ -526,6 +527,8 @@ def _histories(blocks, q0, steps, every, diag):
                 blk.RungeKutta(every)
             q = blk.Q()
             h.append(diag(q))
+            if keep is not None and c * every in keep:
+                keep[c * every][name] = q
         hist[name], final[name] = h, q
     return hist, final
 
@@ -568,8 +571,9 @@ def run_config1(args, local, n=64):
         out[prec] = {"value": blk.interior_nodes * blk.stages * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps}
         blocks[prec] = blk
     csi, eta, zet, aj = blocks["fp64"].metrics()
+    keep = {100: {}}  # the step count the mixed-vs-FP64 bar is stated at
     hist, final = _histories(blocks, q0, steps, steps // 4,
-                             lambda q: (D.kinetic_energy(q, aj), D.enstrophy(q, csi, eta, zet, aj)))
+                             lambda q: (D.kinetic_energy(q, aj), D.enstrophy(q, csi, eta, zet, aj)), keep=keep)
     t_end = steps * dt
     shifted = coords.copy()
     shifted[..., 0] = np.mod(coords[..., 0] - t_end, L)
@@ -582,10 +586,12 @@ def run_config1(args, local, n=64):
         blocks[prec].close()
     l2, linf = D.field_errors(final["mixed"], final["fp64"])
     ke, en = _history_devs(hist)
+    l2h, linfh = D.field_errors(keep[100]["mixed"], keep[100]["fp64"])
     out["mixed_vs_fp64_error"] = {"steps": steps, "rel_l2": l2, "rel_linf": linf,
                                   "fields": ["rho", "rhoU", "rhoV", "rhoW", "rhoE"],
                                   "ke_history_max_rel_dev": ke, "enstrophy_history_max_rel_dev": en,
-                                  "checkpoints_every": steps // 4}
+                                  "checkpoints_every": steps // 4,
+                                  "after_100_steps": {"rel_l2": l2h, "rel_linf": linfh}}
     return out
 
 
@@ -708,6 +714,15 @@ def run_ours(args, ws, rank, local):
         from oracle import cpu_baseline as cb
         r = cb.run(n, steps=1, warmup=0, cfgkw=CFG)
         cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
+        # the same slab per process on one core and with the shipped -O0 build
+        slab = max(2, n // r["cores"])
+        variants = []
+        if r["kind"] == "reference":
+            for procs, opt in ((1, True), (1, False), (r["cores"], False)):
+                v = cb.run(n, steps=1, warmup=0, procs=procs, cfgkw=CFG, optimized=opt, nz=slab)
+                variants.append({"value": v["value"], "cores": procs, "build": "-O3" if opt else "-O0 (as shipped)",
+                                 "sample": v["sample"]})
+        cpu["variants"] = variants
         # the same CPU leg, as the checker
         vs_oracle = _vs_oracle(n, coords, q0, nv, blocks, CFG)
     for b in blocks.values():

@@ -320,7 +320,7 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     return code;
   };
   if (cfg->fluxorder < 1 || cfg->fluxorder > 3 || (cfg->eno_order != 2 && cfg->eno_order != 3) ||
-      cfg->les < 0 || cfg->les == 10 || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
+      cfg->les < 0 || (cfg->precision != CB_FP64 && cfg->precision != CB_MIXED) ||
       (cfg->flux != 0 && cfg->flux != 1) ||
       (cfg->weno_order != 3 && cfg->weno_order != 5))
     return bail(CB_E_UNSUPPORTED, "option combination not built");
@@ -788,6 +788,10 @@ static int enqueue_nut(cb_batch *b) {
   // Compute_eddy_viscosity_LES per block from the recorded state; the
   // pointer arrays are the q and met members of the block's (uc, uc, uc)
   // table entry in device memory
+  if (b->cfg.les == 10) {  // Cs = 0 (les.c:134-137): nu_t stays zero
+    BCUDA(b, cudaMemsetAsync(b->nut, 0, sizeof(double) * b->total, b->stream));
+    return CB_OK;
+  }
   const int u = b->uc < 0 ? 0 : b->uc;
   const bool dyn = batch_dynamic(b->cfg);
   const cb_config &f = b->cfg;

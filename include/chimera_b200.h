@@ -353,7 +353,7 @@ int cb_rhs_noalloc(const cb_config *cfg, const double *d_coor, const double *d_q
  * refuses the sensor with CB_E_UNSUPPORTED).  With a dynamic -les (2, 3, not
  * 10) every block computes its Smagorinsky coefficient from its own arrays
  * and ghost layers once per step, as each block of the reference does on its
- * own DMDA (les.c:151-1472); -les 10 is refused with CB_E_UNSUPPORTED.
+ * own DMDA (les.c:151-1472); -les 10 keeps nu_t zero, as in a cb_ctx.
  *
  * Per block k: cb_batch_set_grid (coordinates, 3 per node, AoS, as
  * cb_set_grid), cb_batch_set_nvert (optional; default 0), cb_batch_upload_state

@@ -56,13 +56,15 @@ def available_kind() -> str:
     return "reference" if os.path.exists(O.REF_SO_O3) or os.path.isdir(O.REF_SRC_DIR) else "port"
 
 
-def run(n: int, steps: int, warmup: int = 0, procs: int = 0, cfgkw=None, kind: str = "", optimized: bool = True):
+def run(n: int, steps: int, warmup: int = 0, procs: int = 0, cfgkw=None, kind: str = "", optimized: bool = True,
+        nz: int = 0):
     """Returns dict(value=cell-updates/s per stage over all processes, cores,
-    kind, seconds, sample)."""
+    kind, seconds, sample).  nz: interior planes of each process's slab
+    (default n // procs, the workload cut into procs slabs)."""
     cfgkw = dict(cfgkw or {})
     kind = kind or available_kind()
     procs = procs or min(os.cpu_count() or 1, 64)
-    nz = max(2, n // procs)
+    nz = nz or max(2, n // procs)
     ctx = mp.get_context("spawn")
     with ctx.Manager() as mgr:
         barrier = mgr.Barrier(procs)
@@ -78,6 +80,6 @@ def run(n: int, steps: int, warmup: int = 0, procs: int = 0, cfgkw=None, kind: s
         "kind": kind,
         "seconds": secs,
         "sample": (f"{procs} processes x {steps} RK steps of a {n}x{n}x{nz}-interior periodic k-slab "
-                   f"({'reference rhs.c/les.c/solvers.c via PETSc shim, -O3' if kind == 'reference' else 'oracle C restatement'})"
+                   f"({('reference rhs.c/les.c/solvers.c via PETSc shim, ' + ('-O3' if optimized else '-O0 as shipped')) if kind == 'reference' else 'oracle C restatement'})"
                    f"; no inter-slab halo exchange (upper bound of the MPI path)"),
     }

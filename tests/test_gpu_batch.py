@@ -80,6 +80,8 @@ VARIANTS = [
     ("dynamic_les3", dict(les=3, max_cs=0.1)),
     ("dynamic_homo_ik", dict(les=2, i_homo_filter=1, k_homo_filter=1, max_cs=0.1)),
     ("dynamic_box_tf", dict(les=2, i_homo_filter=1, j_homo_filter=1, k_homo_filter=1, testfilter_ik=1, max_cs=0.1)),
+    # -les 10: Cs = 0, the eddy viscosity stays zero
+    ("les10", dict(les=10)),
 ]
 
 
