@@ -135,6 +135,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     for name, args in [
         ("cb_batch_set_grid", [P, I, D]), ("cb_batch_set_nvert", [P, I, D]),
         ("cb_batch_set_bctype", [P, I, IP]),
+        ("cb_batch_ibm_set_surface", [P, I, I, I, P, P, P, D, D, D]),
+        ("cb_batch_ibm_set_velocity", [P, I, D, D]), ("cb_batch_ibm_set_list", [P, I, I, I, P, D]),
+        ("cb_batch_ibm_set_options", [P, I, I]),
         ("cb_batch_upload_state", [P, I, D]), ("cb_batch_download_state", [P, I, D]),
         ("cb_batch_get_metrics", [P, I, D, D, D, D]),
         ("cb_batch_set_halo_map", [P, I, C.c_longlong, IP]), ("cb_batch_halo_periodic", [P]),

@@ -280,6 +280,31 @@ class Batch:
         bc = (C.c_int * 6)(*[int(x) for x in bctype])
         self._check(self.lib.cb_batch_set_bctype(self._b, k, bc))
 
+    # ------------------------------------------------------ immersed bodies --
+    def set_ibm_surface(self, ibi: int, surface: dict):
+        """IBMNodes of body ibi, shared by every block (as Block.set_ibm_surface)."""
+        tri = [np.ascontiguousarray(surface[k], dtype=np.int32) for k in ("nv1", "nv2", "nv3")]
+        nf = [np.ascontiguousarray(surface[k], dtype=np.float64) for k in ("nf_x", "nf_y", "nf_z")]
+        n_v = int(surface["n_v"]) if "n_v" in surface else len(surface["x"])
+        self._check(self.lib.cb_batch_ibm_set_surface(self._b, ibi, n_v, len(tri[0]), *[t.ctypes.data for t in tri],
+                                                      *[dptr(a) for a in nf]))
+
+    def set_ibm_velocity(self, ibi: int, u: np.ndarray, uold: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        uold = np.ascontiguousarray(uold, dtype=np.float64)
+        self._check(self.lib.cb_batch_ibm_set_velocity(self._b, ibi, dptr(u), dptr(uold)))
+
+    def set_ibm_list(self, k: int, ibi: int, info: np.ndarray, coor: np.ndarray):
+        """Interpolation list of body ibi on block k (a block with face codes)
+        and that block's node coordinates."""
+        a = np.ascontiguousarray(info, dtype=_lib.IBM_INFO_DTYPE)
+        c = np.ascontiguousarray(coor, dtype=np.float64).reshape(self.shape(k) + (3,))
+        self._check(self.lib.cb_batch_ibm_set_list(self._b, k, ibi, a.size, a.ctypes.data if a.size else None,
+                                                   dptr(c)))
+
+    def set_ibm_options(self, twoD: int = 0, wallfunction: int = 0):
+        self._check(self.lib.cb_batch_ibm_set_options(self._b, twoD, wallfunction))
+
     def SetInitialCondition(self, k: int, q: np.ndarray):
         a = np.ascontiguousarray(q, dtype=np.float64).reshape(self.shape(k) + (5,))
         self._check(self.lib.cb_batch_upload_state(self._b, k, dptr(a)))

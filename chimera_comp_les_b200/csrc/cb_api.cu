@@ -23,6 +23,7 @@
 #include "cb_common.cuh"
 #include "cb_dyn.cuh"
 #include "cb_ibm.cuh"
+#include "cb_ibm_host.h"
 #include "cb_launch.h"
 #include "cb_stage.cuh"
 
@@ -34,27 +35,6 @@ constexpr int BX = SBX, BY = SBY;
 
 struct GraphSlot {
   cudaGraphExec_t exec = nullptr;
-};
-
-// One immersed body: its surface (IBMNodes) and interpolation list (IBMList)
-// in device memory.
-struct IbmBody {
-  int n_v = 0, n_elmt = 0, n = 0;
-  void *surf = nullptr;  // nf (3 per element), u, uold (3 per vertex), tri (3 per element)
-  void *list = nullptr;  // node, donors, weights, sweep output
-  double *nf = nullptr, *u = nullptr, *uold = nullptr;
-  int *tri = nullptr;
-  int4 *node = nullptr;
-  long long *don = nullptr;
-  double *w = nullptr, *out = nullptr, *ustar = nullptr;
-  unsigned char *last = nullptr;          // -isothermal 2: the entry that writes its node
-  double *iso = nullptr, *pa = nullptr;   // -isothermal 2: per-entry terms, the chain's carried pressure
-  IbmDev dev() const {
-    IbmDev d;
-    d.n = n; d.node = node; d.don = don; d.w = w; d.tri = tri; d.nf = nf; d.u = u; d.uold = uold; d.out = out;
-    d.ustar = ustar; d.last = last; d.iso = iso; d.pa = pa;
-    return d;
-  }
 };
 
 }  // namespace
@@ -1161,14 +1141,6 @@ static int ibm_body(cb_ctx *c, int ibi, IbmBody **b) {
   return CB_OK;
 }
 
-static void ibm_drop_list(IbmBody &b) {
-  if (b.list) cudaFree(b.list);
-  b.list = nullptr;
-  b.node = nullptr; b.don = nullptr; b.w = nullptr; b.out = nullptr; b.ustar = nullptr;
-  b.last = nullptr; b.iso = nullptr; b.pa = nullptr;
-  b.n = 0;
-}
-
 int cb_ibm_set_surface(cb_ctx *c, int ibi, int n_v, int n_elmt, const int *nv1, const int *nv2, const int *nv3,
                        const double *nf_x, const double *nf_y, const double *nf_z) {
   IbmBody *b;
@@ -1176,31 +1148,14 @@ int cb_ibm_set_surface(cb_ctx *c, int ibi, int n_v, int n_elmt, const int *nv1, 
   if (e) return e;
   if (n_v < 1 || n_elmt < 1 || !nv1 || !nv2 || !nv3 || !nf_x || !nf_y || !nf_z)
     return fail(c, CB_E_ARG, "surface needs n_v, n_elmt >= 1 and all arrays");
-  std::vector<int> tri(3 * (size_t)n_elmt);
-  std::vector<double> h(3 * (size_t)n_elmt + 6 * (size_t)n_v, 0.0);
-  for (int t = 0; t < n_elmt; t++) {
-    const int v[3] = {nv1[t], nv2[t], nv3[t]};
-    for (int a = 0; a < 3; a++) {
-      if (v[a] < 0 || v[a] >= n_v) return fail(c, CB_E_ARG, "element vertex index out of range");
-      tri[3 * (size_t)t + a] = v[a];
-    }
-    h[3 * (size_t)t] = nf_x[t]; h[3 * (size_t)t + 1] = nf_y[t]; h[3 * (size_t)t + 2] = nf_z[t];
-  }
   CB_CUDA(c, cudaStreamSynchronize(c->stream));  // graphs in flight may read the old arrays
   ibm_drop_list(*b);
   if (b->surf) cudaFree(b->surf);
   b->surf = nullptr;
-  const size_t nd = h.size();
-  CB_CUDA(c, cudaMalloc(&b->surf, sizeof(double) * nd + sizeof(int) * tri.size()));
-  b->nf = (double *)b->surf;
-  b->u = b->nf + 3 * (size_t)n_elmt;
-  b->uold = b->u + 3 * (size_t)n_v;
-  b->tri = (int *)(b->nf + nd);
-  b->n_v = n_v;
-  b->n_elmt = n_elmt;
-  CB_CUDA(c, cudaMemcpyAsync(b->nf, h.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
-  CB_CUDA(c, cudaMemcpyAsync(b->tri, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice, c->stream));
-  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  const char *err = "";
+  const int rc = ibm_surface_to_device(*b, n_v, n_elmt, nv1, nv2, nv3, nf_x, nf_y, nf_z, c->stream, &err);
+  if (rc == CB_E_ARG) return fail(c, CB_E_ARG, err);
+  if (rc) return fail(c, CB_E_CUDA, "surface upload");
   invalidate_graphs(c);
   return CB_OK;
 }
@@ -1224,54 +1179,13 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
   if (e) return e;
   if (n < 0 || (n > 0 && (!list || !coor))) return CB_E_ARG;
   if (n > 0 && !b->surf) return fail(c, CB_E_STATE, "set the body's surface first");
-  const int m[3] = {c->cfg.mx, c->cfg.my, c->cfg.mz};
-  const bool per[3] = {c->cfg.bctype[0] == 7, c->cfg.bctype[2] == 7, c->cfg.bctype[4] == 7};
-  // a node listed twice keeps its last entry
-  std::unordered_map<long long, int> last;
-  for (int t = 0; t < n; t++) {
-    const cb_ibm_info &f = list[t];
-    const int nd[3] = {f.ni, f.nj, f.nk};
-    for (int d = 0; d < 3; d++)
-      if (nd[d] < 0 || nd[d] >= m[d]) return fail(c, CB_E_ARG, "interface node outside the block");
-    const int dn[9] = {f.i1, f.j1, f.k1, f.i2, f.j2, f.k2, f.i3, f.j3, f.k3};
-    for (int a = 0; a < 9; a++) {
-      const int d = a % 3, lo = per[d] ? -2 : 0, hi = per[d] ? m[d] + 1 : m[d] - 1;
-      if (dn[a] < lo || dn[a] > hi) return fail(c, CB_E_ARG, "donor node outside the ghosted block");
-    }
-    if (f.cell < -1 || f.cell >= b->n_elmt) return fail(c, CB_E_ARG, "surface element index out of range");
-    last[((long long)f.nk * m[1] + f.nj) * m[0] + f.ni] = t;
-  }
-  // -isothermal 2 walks every entry (the chain of Pa); the scatter then
-  // writes each node from its last entry only
-  const bool iso2 = c->cfg.isothermal == 2;
-  std::vector<int> keep;
-  std::vector<unsigned char> lastf;
-  keep.reserve(iso2 ? n : last.size());
-  for (int t = 0; t < n; t++) {
-    const cb_ibm_info &f = list[t];
-    const bool is_last = last[((long long)f.nk * m[1] + f.nj) * m[0] + f.ni] == t;
-    if (iso2) lastf.push_back(is_last ? 1 : 0);
-    if (iso2 || is_last) keep.push_back(t);
-  }
-  const int nk = (int)keep.size();
-  std::vector<int4> node(nk);
-  std::vector<long long> don(3 * (size_t)nk);
-  std::vector<double> w((size_t)IBM_NW * nk);
-  for (int t = 0; t < nk; t++) {
-    const cb_ibm_info &f = list[keep[t]];
-    node[t] = make_int4(f.ni, f.nj, f.nk, f.cell);
-    don[3 * (size_t)t] = gidx(c->dc, f.i1, f.j1, f.k1);
-    don[3 * (size_t)t + 1] = gidx(c->dc, f.i2, f.j2, f.k2);
-    don[3 * (size_t)t + 2] = gidx(c->dc, f.i3, f.j3, f.k3);
-    const double *x = coor + 3 * (((size_t)f.nk * m[1] + f.nj) * m[0] + f.ni);
-    const double v[IBM_NW] = {f.cr1, f.cr2, f.cr3, f.cs1, f.cs2, f.cs3, f.d_s, f.d_s + f.d_i,
-                              x[0] - f.pmin[0], x[1] - f.pmin[1], x[2] - f.pmin[2]};  // ibm_iso.c:2653, 2662-2664
-    for (int a = 0; a < IBM_NW; a++) w[(size_t)a * nk + t] = v[a];
-  }
+  IbmHostList h;
+  const char *err = "";
+  if (ibm_build_list(c->dc, c->cfg.isothermal == 2, b->n_elmt, n, list, coor, h, &err)) return fail(c, CB_E_ARG, err);
   CB_CUDA(c, cudaStreamSynchronize(c->stream));
   ibm_drop_list(*b);
   invalidate_graphs(c);
-  if (nk == 0) return CB_OK;
+  if (h.n() == 0) return CB_OK;
   if (!c->ibm_arena) {
     CB_CUDA(c, cudaMalloc(&c->ibm_arena, sizeof(double) * 7 * c->plane));
     CB_CUDA(c, cudaMemsetAsync(c->ibm_arena, 0, sizeof(double) * 7 * c->plane, c->stream));
@@ -1281,27 +1195,7 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
     int fe = fill_ptab(c);
     if (fe) return fe;
   }
-  const size_t iso_d = iso2 ? (size_t)IBM_ISO_NS * nk + 1 : 0;  // terms, then the carried pressure
-  const size_t bytes = sizeof(int4) * nk + sizeof(long long) * 3 * nk + sizeof(double) * ((IBM_NW + 7) * (size_t)nk + iso_d) +
-                       (iso2 ? (size_t)nk : 0);
-  CB_CUDA(c, cudaMalloc(&b->list, bytes));
-  b->node = (int4 *)b->list;
-  b->don = (long long *)(b->node + nk);
-  b->w = (double *)(b->don + 3 * (size_t)nk);
-  b->out = b->w + (size_t)IBM_NW * nk;
-  b->ustar = b->out + (size_t)6 * nk;
-  if (iso2) {
-    b->iso = b->ustar + nk;
-    b->pa = b->iso + (size_t)IBM_ISO_NS * nk;
-    b->last = (unsigned char *)(b->pa + 1);
-    CB_CUDA(c, cudaMemcpyAsync(b->last, lastf.data(), (size_t)nk, cudaMemcpyHostToDevice, c->stream));
-  }
-  b->n = nk;
-  CB_CUDA(c, cudaMemsetAsync(b->ustar, 0, sizeof(double) * nk, c->stream));
-  CB_CUDA(c, cudaMemcpyAsync(b->node, node.data(), sizeof(int4) * nk, cudaMemcpyHostToDevice, c->stream));
-  CB_CUDA(c, cudaMemcpyAsync(b->don, don.data(), sizeof(long long) * don.size(), cudaMemcpyHostToDevice, c->stream));
-  CB_CUDA(c, cudaMemcpyAsync(b->w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, c->stream));
-  CB_CUDA(c, cudaStreamSynchronize(c->stream));
+  CB_CUDA(c, ibm_list_to_device(*b, h, c->stream));
   return CB_OK;
 }
 

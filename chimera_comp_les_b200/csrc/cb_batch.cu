@@ -33,6 +33,8 @@
 #include "cb_aux.cuh"
 #include "cb_common.cuh"
 #include "cb_dyn.cuh"
+#include "cb_ibm.cuh"
+#include "cb_ibm_host.h"
 #include "cb_launch.h"
 #include "cb_stage.cuh"
 
@@ -122,6 +124,14 @@ struct cb_batch {
   double *sig_arena = nullptr;
   double *sig_a[3] = {}, *sig_b[3] = {};
   double **d_sigptr = nullptr;
+  // immersed bodies (blocks with face codes only): the bodies' surfaces; per
+  // block its list of each body, its seven planes (Q snapshot 5, P snapshot,
+  // the carried P) and a device table of their pointers
+  IbmBody body[CB_IBM_MAX_BODIES];
+  std::vector<IbmBody> ibl;        // [nb][CB_IBM_MAX_BODIES]: list part (the surface is body[ibi]'s)
+  std::vector<double *> ib_arena;  // per block: 7 planes of its padded box, or null
+  double **d_ibtab = nullptr;      // [nb][7]
+  int ibm_twoD = 0, ibm_wallfunction = 0;
   // dynamic Smagorinsky model (-les 2/3): 14 planes, each `total` long, and
   // per block a device table of its 14 plane pointers
   double *dyn_arena = nullptr;
@@ -214,7 +224,20 @@ static void destroy_graphs(cb_batch *b) {
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
-// Pointers of one block (all fields at the block's offset) for a buffer triple.
+// Block k holds an interpolation list of some body.
+static bool block_ib(const cb_batch *b, int k) {
+  if (b->ib_arena.empty() || !b->ib_arena[k]) return false;
+  for (int i = 0; i < CB_IBM_MAX_BODIES; i++)
+    if (b->ibl[(size_t)k * CB_IBM_MAX_BODIES + i].n > 0) return true;
+  return false;
+}
+// the pressure plane block k carries from its interpolation into the next
+// step's first stage (the reference's lP)
+static double *ib_pl(const cb_batch *b, int k) { return b->ib_arena[k] + 6 * b->blk[k].dc.plane; }
+
+// Pointers of one block (all fields at the block's offset) for a buffer
+// triple; a first stage (in == old) of a block with bodies reads the carried
+// pressure, as the single-block context does after an immersed step.
 static DevFields block_fields(const cb_batch *b, int blk, int in, int old, int out) {
   const long long o = b->blk[blk].off;
   DevFields F{};
@@ -235,6 +258,7 @@ static DevFields block_fields(const cb_batch *b, int blk, int in, int old, int o
   for (int a = 0; a < 3; a++) F.gcl[a] = b->gcl[a] ? b->gcl[a] + o : nullptr;
   for (int a = 0; a < 3; a++) F.sig[a] = b->sig_a[a] ? b->sig_a[a] + o : nullptr;
   F.status = b->status;
+  if (in == old && block_ib(b, blk)) F.pin = ib_pl(b, blk);
   return F;
 }
 
@@ -372,6 +396,8 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
     b->blk.push_back(bh);
   }
   b->total = off;
+  b->ibl.resize((size_t)nblocks * CB_IBM_MAX_BODIES);
+  b->ib_arena.assign(nblocks, nullptr);
   const size_t bytes = sizeof(double) * (size_t)b->total * 28;
   if (cudaMalloc(&b->arena, bytes) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc arena");
   cudaMemsetAsync(b->arena, 0, bytes, b->stream);
@@ -446,6 +472,12 @@ void cb_batch_destroy(cb_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
   destroy_graphs(b);
+  for (auto &l : b->ibl) ibm_drop_list(l);
+  for (auto &s : b->body)
+    if (s.surf) cudaFree(s.surf);
+  for (double *p : b->ib_arena)
+    if (p) cudaFree(p);
+  if (b->d_ibtab) cudaFree(b->d_ibtab);
   void *ptrs[] = {b->arena, b->arena_mixed, b->sig_arena, b->d_sigptr, b->dyn_arena, b->d_dynptr, b->staging, b->ptab,
                   b->ptab4, b->d_tables,
                   b->d_items, b->d_counter,
@@ -550,12 +582,105 @@ int cb_batch_set_bctype(cb_batch *b, int k, const int *bctype) {
     if (b->xs.nsend || b->xs.nrecv || b->xw.nsend || b->xw.nrecv)
       return bfail(b, CB_E_UNSUPPORTED, "physical face codes with a cross-process exchange are not built");
   }
+  if (!phys && block_ib(b, k))
+    return bfail(b, CB_E_STATE, "a block with immersed-body lists keeps face codes; clear its lists first");
   BlockHost &bh = b->blk[k];
   for (int f = 0; f < 6; f++) bh.dc.bctype[f] = bctype[f];
   bh.phys = phys;
   b->nphys = 0;
   for (const auto &x : b->blk) b->nphys += x.phys ? 1 : 0;
   return build_tables(b);  // the tables carry each block's config; graphs are rebuilt
+}
+
+// ---- immersed bodies: the reference's RungeKutta interpolates every body
+// on every block after the block's stages (solvers.c:279-288, one IBMList per
+// block and body).  Surfaces are shared by all blocks; lists go to blocks
+// with face codes, whose FormBCS(user, 0) follows the interpolation.
+static int batch_body(cb_batch *b, int ibi) {
+  if (!b) return CB_E_ARG;
+  if (ibi < 0 || ibi >= CB_IBM_MAX_BODIES) return bfail(b, CB_E_ARG, "body index out of range");
+  return CB_OK;
+}
+
+int cb_batch_ibm_set_surface(cb_batch *b, int ibi, int n_v, int n_elmt, const int *nv1, const int *nv2,
+                             const int *nv3, const double *nf_x, const double *nf_y, const double *nf_z) {
+  if (int e = batch_body(b, ibi)) return e;
+  if (n_v < 1 || n_elmt < 1 || !nv1 || !nv2 || !nv3 || !nf_x || !nf_y || !nf_z)
+    return bfail(b, CB_E_ARG, "surface needs n_v, n_elmt >= 1 and all arrays");
+  BCUDA(b, cudaStreamSynchronize(b->stream));  // graphs in flight may read the old arrays
+  for (int k = 0; k < b->nb; k++) ibm_drop_list(b->ibl[(size_t)k * CB_IBM_MAX_BODIES + ibi]);
+  IbmBody &sf = b->body[ibi];
+  if (sf.surf) cudaFree(sf.surf);
+  sf = IbmBody();
+  const char *err = "";
+  const int rc = ibm_surface_to_device(sf, n_v, n_elmt, nv1, nv2, nv3, nf_x, nf_y, nf_z, b->stream, &err);
+  if (rc == CB_E_ARG) return bfail(b, CB_E_ARG, err);
+  if (rc) return bfail(b, CB_E_CUDA, "surface upload");
+  return build_tables(b);  // lists dropped: the first-stage pressure source changes
+}
+
+int cb_batch_ibm_set_velocity(cb_batch *b, int ibi, const double *u, const double *uold) {
+  if (int e = batch_body(b, ibi)) return e;
+  if (!u || !uold) return CB_E_ARG;
+  IbmBody &sf = b->body[ibi];
+  if (!sf.surf) return bfail(b, CB_E_STATE, "set the body's surface first");
+  BCUDA(b, cudaMemcpyAsync(sf.u, u, sizeof(double) * 3 * sf.n_v, cudaMemcpyHostToDevice, b->stream));
+  BCUDA(b, cudaMemcpyAsync(sf.uold, uold, sizeof(double) * 3 * sf.n_v, cudaMemcpyHostToDevice, b->stream));
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  return CB_OK;
+}
+
+int cb_batch_ibm_set_list(cb_batch *b, int k, int ibi, int n, const cb_ibm_info *list, const double *coor) {
+  if (check_block(b, k)) return CB_E_ARG;
+  if (int e = batch_body(b, ibi)) return e;
+  if (n < 0 || (n > 0 && (!list || !coor))) return CB_E_ARG;
+  if (n > 0 && !b->body[ibi].surf) return bfail(b, CB_E_STATE, "set the body's surface first");
+  BlockHost &bh = b->blk[k];
+  if (n > 0 && !bh.phys)
+    return bfail(b, CB_E_UNSUPPORTED, "immersed bodies need a block with face codes (cb_batch_set_bctype)");
+  IbmHostList h;
+  const char *err = "";
+  if (ibm_build_list(bh.dc, b->cfg.isothermal == 2, b->body[ibi].n_elmt, n, list, coor, h, &err))
+    return bfail(b, CB_E_ARG, err);
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  IbmBody &l = b->ibl[(size_t)k * CB_IBM_MAX_BODIES + ibi];
+  ibm_drop_list(l);
+  const bool had = block_ib(b, k);
+  if (h.n() > 0) {
+    if (!b->ib_arena[k]) {
+      const size_t pb = sizeof(double) * 7 * bh.dc.plane;
+      BCUDA(b, cudaMalloc(&b->ib_arena[k], pb));
+      BCUDA(b, cudaMemsetAsync(b->ib_arena[k], 0, pb, b->stream));
+      if (!b->d_ibtab) {
+        BCUDA(b, cudaMalloc(&b->d_ibtab, sizeof(double *) * 7 * b->nb));
+        BCUDA(b, cudaMemsetAsync(b->d_ibtab, 0, sizeof(double *) * 7 * b->nb, b->stream));
+      }
+      double *t[7];
+      for (int a = 0; a < 7; a++) t[a] = b->ib_arena[k] + bh.dc.plane * a;
+      BCUDA(b, cudaMemcpyAsync(b->d_ibtab + 7 * k, t, sizeof(t), cudaMemcpyHostToDevice, b->stream));
+    }
+    BCUDA(b, ibm_list_to_device(l, h, b->stream));
+    if (!had && bh.have_state) {  // P starts as the EqOfState of the current state
+      if (block_ptab(b, k)) return CB_E_CUDA;
+      eos_plane_kernel<<<bgrid(b, bh.dc.plane), 256, 0, b->stream>>>(
+          bh.dc, (const double *const *)(b->ptab + 5 * b->cur), ib_pl(b, k));
+      BCUDA(b, cudaGetLastError());
+      BCUDA(b, cudaStreamSynchronize(b->stream));
+    }
+  }
+  return build_tables(b);  // the first-stage pressure source of the block
+}
+
+int cb_batch_ibm_set_options(cb_batch *b, int twoD, int wallfunction) {
+  if (!b) return CB_E_ARG;
+  if (twoD < 0 || twoD > 3) return bfail(b, CB_E_ARG, "twoD must be 0..3");
+  if (wallfunction == 1) return bfail(b, CB_E_UNSUPPORTED, "the wall function of -wallfunction 1 is not built");
+  if (wallfunction != 0 && wallfunction != 2 && wallfunction != 3)
+    return bfail(b, CB_E_ARG, "wallfunction must be 0, 2 or 3");
+  b->ibm_twoD = twoD;
+  b->ibm_wallfunction = wallfunction;
+  destroy_graphs(b);
+  return CB_OK;
 }
 
 // State of block k (5 per node, AoS) into the CURRENT buffer, ghosts by
@@ -583,6 +708,9 @@ int cb_batch_upload_state(cb_batch *b, int k, const double *q) {
   unpack_kernel<<<bgrid(b, (long long)nn), 256, 0, b->stream>>>(bh.dc, b->staging, 5, b->ptab + 5 * b->cur);
   const long long all = (long long)(bh.mx + 4) * (bh.my + 4) * (bh.mz + 4);
   ghost_fill_kernel<<<bgrid(b, all), 256, 0, b->stream>>>(bh.dc, b->ptab + 5 * b->cur, 5);
+  if (block_ib(b, k))  // P starts as the EqOfState of the state, as in a cb_ctx after an upload
+    eos_plane_kernel<<<bgrid(b, bh.dc.plane), 256, 0, b->stream>>>(bh.dc, (const double *const *)(b->ptab + 5 * b->cur),
+                                                                    ib_pl(b, k));
   BCUDA(b, cudaGetLastError());
   BCUDA(b, cudaMemsetAsync(b->nut + bh.off, 0, sizeof(double) * bh.dc.plane, b->stream));
   BCUDA(b, cudaStreamSynchronize(b->stream));
@@ -875,7 +1003,8 @@ static int enqueue_sigma(cb_batch *b, int in) {
     const BlockHost &bh = b->blk[k];
     const char *ent = tab + sizeof(BatchBlock) * k;
     const double *const *q = reinterpret_cast<const double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, q));
-    sigma_sensor_kernel<<<bgrid(b, bh.dc.plane), 256, 0, b->stream>>>(bh.dc, q, b->d_sigptr + 6 * k, nullptr);
+    sigma_sensor_kernel<<<bgrid(b, bh.dc.plane), 256, 0, b->stream>>>(bh.dc, q, b->d_sigptr + 6 * k,
+                                                                       block_ib(b, k) ? ib_pl(b, k) : nullptr);
   }
   if (int e = sigma_ghosts(b, b->sig_a, 0)) return e;
   for (int k = 0; k < b->nb; k++)
@@ -952,6 +1081,61 @@ static int enqueue_stage(cb_batch *b, int s, int per_block, int in, int old, int
   return CB_OK;
 }
 
+// After the stages of a step, on block k with bodies (solvers.c:279-288):
+// EqOfState into its pressure plane, five sweeps of ibm_interpolation_advanced
+// per body, then FormBCS(user, 0) from snapshots of Q and P (the reference's
+// lQ / lP) -- the single-block context's kernels in its order.  `old` is the
+// step's input buffer (Qold).
+static int enqueue_ib(cb_batch *b, int k, int old) {
+  const BlockHost &bh = b->blk[k];
+  const DevCfg &d = bh.dc;
+  double *pl = ib_pl(b, k), *psnap = b->ib_arena[k] + 5 * d.plane;
+  double *const *tab = b->d_ibtab + 7 * k;  // Q snapshot 0..4, P snapshot, carried P
+  // the current state's planes: the qout member of the block's (cur, cur, cur) entry
+  const char *ent = reinterpret_cast<const char *>(b->d_tables + (size_t)(b->cur * 13) * b->nb + k);
+  double *const *qc = reinterpret_cast<double *const *>(ent + offsetof(BatchBlock, F) + offsetof(DevFields, qout));
+  eos_plane_kernel<<<bgrid(b, d.plane), 256, 0, b->stream>>>(d, (const double *const *)qc, pl);
+  const int slip = (b->cfg.inviscid || b->ibm_wallfunction == 3) ? 1 : 0;  // ibm_iso.c:2721
+  const int iso1 = b->cfg.isothermal == 1 ? 1 : 0;
+  const int wf2 = b->ibm_wallfunction == 2 ? 1 : 0;
+  const bool iso2 = b->cfg.isothermal == 2;
+  const double a_sound = sqrt(b->cfg.twall / (b->cfg.ma * b->cfg.ma));  // ibm_iso.c:2768, the host's sqrt
+  for (int ibi = 0; ibi < CB_IBM_MAX_BODIES; ibi++) {
+    IbmDev dv = b->ibl[(size_t)k * CB_IBM_MAX_BODIES + ibi].dev();
+    if (dv.n <= 0) continue;
+    const IbmBody &sf = b->body[ibi];
+    dv.tri = sf.tri; dv.nf = sf.nf; dv.u = sf.u; dv.uold = sf.uold;
+    const int g = bgrid(b, dv.n);
+    for (int s = 0; s < IBM_SWEEPS; s++) {
+      ibm_interp_kernel<<<g, 256, 0, b->stream>>>(d, (const double *const *)qc, pl, dv, 1, b->ibm_twoD, slip, iso1, wf2,
+                                                  iso2 ? b->qb[old][0] + bh.off : nullptr, a_sound);
+      if (iso2) {
+        ibm_iso2_chain_kernel<<<1, IBM_CHAIN_NT, 0, b->stream>>>(d, dv, s == 0 ? 1 : 0, a_sound);
+        ibm_iso2_finish_kernel<<<g, 256, 0, b->stream>>>(d, dv, 1);
+      }
+      ibm_scatter_kernel<<<g, 256, 0, b->stream>>>(d, qc, pl, dv);
+    }
+  }
+  // FormBCS(user, 0): Q and P within five layers of the faces into the snapshots
+  const long long thick = thick_shell_count(d, 5);
+  thick_shell_copy_kernel<<<bgrid(b, thick), 256, 0, b->stream>>>(d, 5, (const double *const *)qc, tab, 5);
+  thick_shell_copy_kernel<<<bgrid(b, thick), 256, 0, b->stream>>>(d, 5, (const double *const *)(tab + 6), tab + 5, 1);
+  DevFields F = block_fields(b, k, b->cur, old, b->cur);
+  for (int q = 0; q < 5; q++) F.q[q] = b->ib_arena[k] + d.plane * q;
+  F.pin = psnap;
+  const long long face = (long long)std::max(d.mx, d.my) * std::max(d.my, d.mz), shell = shell_count(d);
+  for (int dir = 0; dir < 3; dir++) bc_face_kernel<<<bgrid(b, face), 256, 0, b->stream>>>(d, F, dir, 0.0);
+  for (int dir = 0; dir < 3; dir++)
+    if (d.bctype[2 * dir] == 7) {
+      bc_periodic_dir_kernel<<<bgrid(b, face), 256, 0, b->stream>>>(d, F, dir);
+      bc_periodic_dir_p_kernel<<<bgrid(b, face), 256, 0, b->stream>>>(d, psnap, pl, dir);
+    }
+  ghost_fill_kernel<<<bgrid(b, shell), 256, 0, b->stream>>>(d, qc, 5);
+  ghost_fill_kernel<<<bgrid(b, shell), 256, 0, b->stream>>>(d, tab + 6, 1);
+  BCUDA(b, cudaGetLastError());
+  return CB_OK;
+}
+
 // Buffers of stage s when the step starts from buffer cur0.
 static void stage_buffers(int cur0, int s, int *in, int *out) {
   const int A = (cur0 + 1) % 3, B = (cur0 + 2) % 3;
@@ -979,6 +1163,11 @@ static int enqueue_batch_step(cb_batch *b, int per_block) {
     if (!b->cfg.inviscid) b->uc = in;
   }
   b->cur = out;
+  for (int k = 0; k < b->nb; k++)
+    if (block_ib(b, k)) {
+      int e = enqueue_ib(b, k, old);
+      if (e) return e;
+    }
   return CB_OK;
 }
 
@@ -1105,6 +1294,8 @@ static FieldSet field_set(const double *const *in, const double *const *out, int
 //                   map, pack of the stage values (5 per entry)
 int cb_batch_phase(cb_batch *b, int phase, int stage, int mode) {
   if (!b || (mode != 0 && mode != 1)) return CB_E_ARG;
+  for (int k = 0; k < b->nb; k++)
+    if (block_ib(b, k)) return bfail(b, CB_E_UNSUPPORTED, "immersed bodies with the phase API are not built");
   if (b->sig_arena) return bfail(b, CB_E_UNSUPPORTED, "the shock sensor with a cross-process exchange is not built");
   for (auto &bh : b->blk)
     if (!bh.have_grid || !bh.have_state) return bfail(b, CB_E_STATE, "every block needs a grid and a state");

@@ -71,7 +71,7 @@ __device__ __forceinline__ double wf_f(double nu, double u, double y, double uta
   if (yplus <= 11.53) return utau0 * yplus - u;
   return utau0 * (1. / WF_KAPPA * log(wf_E(utau0, ks, nu) * yplus)) - u;
 }
-__device__ __noinline__ double wf_find_utau(double nu, double u, double y, double guess, double ks) {
+static __device__ __noinline__ double wf_find_utau(double nu, double u, double y, double guess, double ks) {
   const double eps = 1.e-7;  // find_utau_hydset, wallfunction.c:85-100
   double utau = guess, utau0 = guess;
   for (int ii = 0; ii < 30; ii++) {

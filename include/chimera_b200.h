@@ -383,6 +383,23 @@ int cb_batch_set_nvert(cb_batch *b, int block, const double *nvert);
  * on one face only and for the inflow codes 52 and 47; CB_E_ARG if the block
  * already holds a halo-map destination. */
 int cb_batch_set_bctype(cb_batch *b, int block, const int *bctype);
+/* Immersed bodies in the batched form: after a block's stages the reference
+ * interpolates every body on that block (ibm_interpolation_advanced with its
+ * IBMList of the block), then runs FormBCS(user, 0) (solvers.c:279-288).
+ * Surfaces, vertex velocities and the options are shared by all blocks (the
+ * reference's ibm[ibi]; arguments as cb_ibm_set_surface / _velocity /
+ * _options); each block takes its own list of each body, built as by
+ * cb_ibm_set_list from that block's node coordinates.  Lists go only to
+ * blocks with face codes (cb_batch_set_bctype; CB_E_UNSUPPORTED otherwise;
+ * such a block then keeps its codes, CB_E_STATE).  A block with lists
+ * advances as a cb_ctx with the same lists; its first stage reads the
+ * pressure carried from its interpolation (after an upload: the EqOfState of
+ * the state).  A batch with lists refuses the phase API (CB_E_UNSUPPORTED). */
+int cb_batch_ibm_set_surface(cb_batch *b, int ibi, int n_v, int n_elmt, const int *nv1, const int *nv2,
+                             const int *nv3, const double *nf_x, const double *nf_y, const double *nf_z);
+int cb_batch_ibm_set_velocity(cb_batch *b, int ibi, const double *u, const double *uold);
+int cb_batch_ibm_set_list(cb_batch *b, int block, int ibi, int n, const cb_ibm_info *list, const double *coor);
+int cb_batch_ibm_set_options(cb_batch *b, int twoD, int wallfunction);
 int cb_batch_upload_state(cb_batch *b, int block, const double *q);
 int cb_batch_download_state(cb_batch *b, int block, double *q);
 /* CFL time step over all blocks: dt = cfl / (largest spectral radius of any
