@@ -134,7 +134,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.cb_batch_work_items.restype = I
     for name, args in [
         ("cb_batch_set_grid", [P, I, D]), ("cb_batch_set_nvert", [P, I, D]),
-        ("cb_batch_set_bctype", [P, I, IP]),
+        ("cb_batch_set_bctype", [P, I, IP]), ("cb_batch_set_time_index", [P, I]),
         ("cb_batch_ibm_set_surface", [P, I, I, I, P, P, P, D, D, D]),
         ("cb_batch_ibm_set_velocity", [P, I, D, D]), ("cb_batch_ibm_set_list", [P, I, I, I, P, D]),
         ("cb_batch_ibm_set_options", [P, I, I]),

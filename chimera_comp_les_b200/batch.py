@@ -280,6 +280,11 @@ class Batch:
         bc = (C.c_int * 6)(*[int(x) for x in bctype])
         self._check(self.lib.cb_batch_set_bctype(self._b, k, bc))
 
+    def set_time_index(self, ti: int) -> None:
+        """user->ti of the last completed step (the next step runs ti + 1),
+        read by the k-lo inflow code 47 (cb_batch_set_time_index)."""
+        self._check(self.lib.cb_batch_set_time_index(self._b, int(ti)))
+
     # ------------------------------------------------------ immersed bodies --
     def set_ibm_surface(self, ibi: int, surface: dict):
         """IBMNodes of body ibi, shared by every block (as Block.set_ibm_surface)."""

@@ -132,6 +132,10 @@ struct cb_batch {
   std::vector<double *> ib_arena;  // per block: 7 planes of its padded box, or null
   double **d_ibtab = nullptr;      // [nb][7]
   int ibm_twoD = 0, ibm_wallfunction = 0;
+  // k-lo inflow codes 52 and 47: per block its node coordinates x, y (two
+  // padded planes, or null), and the step index user->ti of the running step
+  std::vector<double *> coorxy;
+  int *ti_dev = nullptr;
   // dynamic Smagorinsky model (-les 2/3): 14 planes, each `total` long, and
   // per block a device table of its 14 plane pointers
   double *dyn_arena = nullptr;
@@ -259,6 +263,10 @@ static DevFields block_fields(const cb_batch *b, int blk, int in, int old, int o
   for (int a = 0; a < 3; a++) F.sig[a] = b->sig_a[a] ? b->sig_a[a] + o : nullptr;
   F.status = b->status;
   if (in == old && block_ib(b, blk)) F.pin = ib_pl(b, blk);
+  const double *xy = b->coorxy.empty() ? nullptr : b->coorxy[blk];
+  F.cx = xy;
+  F.cy = xy ? xy + b->blk[blk].dc.plane : nullptr;
+  F.ti = b->ti_dev;
   return F;
 }
 
@@ -398,6 +406,9 @@ int cb_batch_create(const cb_config *cfg, int nblocks, const int *dims, cb_batch
   b->total = off;
   b->ibl.resize((size_t)nblocks * CB_IBM_MAX_BODIES);
   b->ib_arena.assign(nblocks, nullptr);
+  b->coorxy.assign(nblocks, nullptr);
+  if (cudaMalloc(&b->ti_dev, sizeof(int)) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc step index");
+  cudaMemsetAsync(b->ti_dev, 0, sizeof(int), b->stream);
   const size_t bytes = sizeof(double) * (size_t)b->total * 28;
   if (cudaMalloc(&b->arena, bytes) != cudaSuccess) return bail(CB_E_CUDA, "cudaMalloc arena");
   cudaMemsetAsync(b->arena, 0, bytes, b->stream);
@@ -477,6 +488,9 @@ void cb_batch_destroy(cb_batch *b) {
     if (s.surf) cudaFree(s.surf);
   for (double *p : b->ib_arena)
     if (p) cudaFree(p);
+  for (double *p : b->coorxy)
+    if (p) cudaFree(p);
+  if (b->ti_dev) cudaFree(b->ti_dev);
   if (b->d_ibtab) cudaFree(b->d_ibtab);
   void *ptrs[] = {b->arena, b->arena_mixed, b->sig_arena, b->d_sigptr, b->dyn_arena, b->d_dynptr, b->staging, b->ptab,
                   b->ptab4, b->d_tables,
@@ -524,6 +538,10 @@ int cb_batch_set_grid(cb_batch *b, int k, const double *coor) {
   if (b->cfg.precision == CB_MIXED)
     BCUDA(b, launch_mixed_prep(d, (const double *const *)(b->ptab + 15), b->delta2 + bh.off, b->aj + bh.off, b->ptab4,
                                b->ptab + 27, bgrid(b, d.plane), b->stream));
+  if (b->coorxy[k])  // x and y kept for the inflow codes that read them
+    for (int q = 0; q < 2; q++)
+      BCUDA(b, cudaMemcpyAsync(b->coorxy[k] + d.plane * q, b->qb[2][q] + bh.off, sizeof(double) * d.plane,
+                               cudaMemcpyDeviceToDevice, b->stream));
   for (int q = 0; q < 3; q++) BCUDA(b, cudaMemsetAsync(b->qb[2][q] + bh.off, 0, sizeof(double) * d.plane, b->stream));
   BCUDA(b, cudaStreamSynchronize(b->stream));
   bh.have_grid = true;
@@ -569,12 +587,12 @@ int cb_batch_set_bctype(cb_batch *b, int k, const int *bctype) {
     if ((bctype[2 * d] == 7) != (bctype[2 * d + 1] == 7))
       return bfail(b, CB_E_UNSUPPORTED, "a periodic direction needs bctype 7 on both faces");
   bool phys = false;
-  for (int f = 0; f < 6; f++) {
-    if (bctype[f] == 52 || bctype[f] == 47)
-      return bfail(b, CB_E_UNSUPPORTED,
-                   "inflow codes 52 and 47 (node coordinates and step index) are not built in the batched form");
-    phys = phys || bctype[f] != 7;
-  }
+  for (int f = 0; f < 6; f++) phys = phys || bctype[f] != 7;
+  // the k-lo inflow codes 52 and 47 read the node coordinates x, y, which
+  // the block keeps from its grid upload
+  const bool inflow_xy = bctype[4] == 52 || bctype[4] == 47;
+  if (inflow_xy && b->blk[k].have_grid && !b->coorxy[k])
+    return bfail(b, CB_E_STATE, "set the inflow codes 52 / 47 before the block's grid");
   if (phys) {
     for (int kind = 0; kind < 2; kind++)
       if (!b->map_dst[kind].empty() && b->map_dst[kind][k])
@@ -585,11 +603,24 @@ int cb_batch_set_bctype(cb_batch *b, int k, const int *bctype) {
   if (!phys && block_ib(b, k))
     return bfail(b, CB_E_STATE, "a block with immersed-body lists keeps face codes; clear its lists first");
   BlockHost &bh = b->blk[k];
+  if (inflow_xy && !b->coorxy[k]) {
+    BCUDA(b, cudaMalloc(&b->coorxy[k], sizeof(double) * 2 * bh.dc.plane));
+    BCUDA(b, cudaMemsetAsync(b->coorxy[k], 0, sizeof(double) * 2 * bh.dc.plane, b->stream));
+  }
   for (int f = 0; f < 6; f++) bh.dc.bctype[f] = bctype[f];
   bh.phys = phys;
   b->nphys = 0;
   for (const auto &x : b->blk) b->nphys += x.phys ? 1 : 0;
   return build_tables(b);  // the tables carry each block's config; graphs are rebuilt
+}
+
+// user->ti of the last completed step (the next step runs ti + 1), read by
+// the k-lo inflow code 47; stream-ordered.
+int cb_batch_set_time_index(cb_batch *b, int ti) {
+  if (!b) return CB_E_ARG;
+  BCUDA(b, cudaMemcpyAsync(b->ti_dev, &ti, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  return CB_OK;
 }
 
 // ---- immersed bodies: the reference's RungeKutta interpolates every body
@@ -1146,6 +1177,12 @@ static void stage_buffers(int cur0, int s, int *in, int *out) {
 // One step: eddy viscosity per block, then per stage one stage launch
 // (persistent over all blocks, or one per block) and one halo gather.
 static int enqueue_batch_step(cb_batch *b, int per_block) {
+  // user->ti of the step about to run (the time loop advances it, main.c:887-974)
+  for (const auto &bh : b->blk)
+    if (bh.dc.bctype[4] == 47) {
+      step_index_advance_kernel<<<1, 1, 0, b->stream>>>(b->ti_dev);
+      break;
+    }
   if (b->cfg.les && !b->cfg.inviscid) {
     int e = enqueue_nut(b);
     if (e) return e;

@@ -379,10 +379,14 @@ int cb_batch_set_nvert(cb_batch *b, int block, const double *nvert);
  * exactly as a cb_ctx with the same codes; it may then hold no halo-map
  * destination (set codes before the halo maps; cb_batch_halo_periodic skips
  * such blocks) and the batch takes no cross-process exchange.  Six codes 7
- * make it an interface block again.  CB_E_UNSUPPORTED for a direction with 7
- * on one face only and for the inflow codes 52 and 47; CB_E_ARG if the block
- * already holds a halo-map destination. */
+ * make it an interface block again.  The k-lo inflow codes 52 and 47 read
+ * the node coordinates, which the block keeps from cb_batch_set_grid: give
+ * them before the grid (CB_E_STATE after it); code 47's step index comes from
+ * cb_batch_set_time_index, as cb_set_time_index.  CB_E_UNSUPPORTED for a
+ * direction with 7 on one face only; CB_E_ARG if the block already holds a
+ * halo-map destination. */
 int cb_batch_set_bctype(cb_batch *b, int block, const int *bctype);
+int cb_batch_set_time_index(cb_batch *b, int ti);
 /* Immersed bodies in the batched form: after a block's stages the reference
  * interpolates every body on that block (ibm_interpolation_advanced with its
  * IBMList of the block), then runs FormBCS(user, 0) (solvers.c:279-288).

@@ -123,7 +123,7 @@ def test_all_coded_batch_needs_no_halo_map():
 
 def test_face_code_errors():
     import torch
-    from chimera_comp_les_b200._lib import CB_E_ARG, CB_E_UNSUPPORTED, ChimeraError
+    from chimera_comp_les_b200._lib import CB_E_ARG, CB_E_STATE, CB_E_UNSUPPORTED, ChimeraError
     from chimera_comp_les_b200 import batch as B
     opts = dict(BASE, les=1, fluxorder=3)
     inputs = _inputs()
@@ -132,10 +132,13 @@ def test_face_code_errors():
         with pytest.raises(ChimeraError) as e:
             bt.set_bctype(1, (3, 3, 1, 1, 45, 44))
         assert e.value.code == CB_E_ARG
-        for bad in [(7, 3, 1, 1, 45, 44), (3, 3, 1, 1, 52, 44), (3, 3, 1, 1, 47, 44)]:
-            with pytest.raises(ChimeraError) as e:
-                bt.set_bctype(0, bad)
-            assert e.value.code == CB_E_UNSUPPORTED
+        with pytest.raises(ChimeraError) as e:
+            bt.set_bctype(0, (7, 3, 1, 1, 45, 44))
+        assert e.value.code == CB_E_UNSUPPORTED
+        # the inflow codes 52 / 47 keep the coordinates of the grid upload
+        with pytest.raises(ChimeraError) as e:
+            bt.set_bctype(0, (3, 3, 1, 1, 52, 44))
+        assert e.value.code == CB_E_STATE
         # a halo map may not write into a coded block
         st, _ = B.halo_maps_self_periodic(DIMS)
         with pytest.raises(ChimeraError) as e:
@@ -146,3 +149,43 @@ def test_face_code_errors():
         with pytest.raises(ChimeraError) as e:
             bt.set_exchange(B.HALO_STAGE, np.array([[1, 1, 1, 1, 0]]), buf.data_ptr(), np.zeros((0, 4)), 0)
         assert e.value.code == CB_E_UNSUPPORTED
+
+
+@pytest.mark.parametrize("les,ti0", [(0, 1), (1, 6)])
+def test_inflow_codes_52_47_on_coded_blocks(les, ti0):
+    """The k-lo inflow codes that read the node coordinates (52: the
+    characteristic cos^2 inlet, rhs.c:854-874; 47: the power-law inlet with
+    perturbations travelling in x and time, rhs.c:904-950, its step index from
+    cb_batch_set_time_index) on two coded blocks beside an interface block,
+    3 steps, bit for bit against single-block contexts."""
+    from chimera_comp_les_b200 import Block
+    from chimera_comp_les_b200.batch import Batch
+    dims = [(37, 19, 25), (26, 22, 20), (34, 18, 24)]
+    bcs = [(7, 7, 3, 3, 52, 44), None, (7, 7, 3, 3, 47, 45)]
+    opts = dict(BASE, les=les, fluxorder=3, s_x=0.4 if les else 1.0, s_y=0.7, s_z=0.9, ren=250.)
+    inputs = []
+    for b, (d, bc) in enumerate(zip(dims, bcs)):
+        coords = W.periodic_grid((d[0] - 2, d[1] - 2, d[2] - 2), 2 * np.pi, amp=0.04)
+        if bc is not None:
+            coords[..., 1] = 1.5 * coords[..., 1] + 1.0  # y on both sides of 47's y = 8
+        inputs.append((coords, W.random_smooth_state(coords.shape[:3], seed=40 + b, periodic=bc is None)))
+    with Batch(dims, **opts) as bt:
+        for k, bc in enumerate(bcs):
+            if bc is not None:
+                bt.set_bctype(k, bc)
+        for k, (coords, q) in enumerate(inputs):
+            bt.FormMetrics(k, coords)
+            bt.SetInitialCondition(k, q)
+        bt.halo_periodic()
+        bt.set_time_index(ti0 - 1)
+        bt.RungeKutta(3)
+        got = [bt.Q(k) for k in range(len(dims))]
+    for d, bc, (coords, q), g in zip(dims, bcs, inputs, got):
+        with Block(*d, bctype=bc or (7,) * 6, **opts) as blk:
+            blk.FormMetrics(coords)
+            blk.SetInitialCondition(q)
+            blk.set_time_index(ti0 - 1)
+            blk.RungeKutta(3)
+            want = blk.Q()
+        assert np.isfinite(g).all()
+        assert np.array_equal(g, want), (bc, max(per_field_rel_l2(g, want)))
