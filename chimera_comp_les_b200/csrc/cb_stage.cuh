@@ -1195,6 +1195,18 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
     Rg.sb = base;
     const bool more = k + 1 < ke;
     if (more) issue_stage(k + H + 2);  // overlaps the face computation
+    if constexpr (SMET) {
+      // the k-face k+1/2 of this thread's node reads its far node's metric
+      // vectors and nu_t (plane k+1) from global memory in the last face
+      // round: start those lines toward L1 while the i and j faces run
+      const int fx = tid % BX, fy = tid / BX;
+      if (tid < NZF && i0 + fx <= c.mx - 2 && j0 + fy <= c.my - 2) {
+        const long long g1 = gidx(c, i0 + fx, j0 + fy, k + 1);
+#pragma unroll
+        for (int e = 0; e < 3; e++) prefetch_l1(F.met4[e] + g1);
+        if (LES) prefetch_l1(F.nut + g1);
+      }
+    }
     plane_faces<R, MIX, LES, VISC, false, FLUX, NV0>(c, F, Rg, i0, j0, k, gxb, gyb, gzb, gzr);
     // the only plane k-1 value the update needs, read before that slot is refilled
     const NRef n{0, uty + 2, utx + 2};
