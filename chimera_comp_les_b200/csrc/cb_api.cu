@@ -1195,7 +1195,11 @@ int cb_ibm_set_list(cb_ctx *c, int ibi, int n, const cb_ibm_info *list, const do
     int fe = fill_ptab(c);
     if (fe) return fe;
   }
-  CB_CUDA(c, ibm_list_to_device(*b, h, c->stream));
+  const cudaError_t le = ibm_list_to_device(*b, h, c->stream);
+  if (le != cudaSuccess) {  // no half-uploaded list stays behind
+    ibm_drop_list(*b);
+    return fail(c, CB_E_CUDA, std::string("list upload: ") + cudaGetErrorString(le));
+  }
   return CB_OK;
 }
 

@@ -690,7 +690,11 @@ int cb_batch_ibm_set_list(cb_batch *b, int k, int ibi, int n, const cb_ibm_info 
       for (int a = 0; a < 7; a++) t[a] = b->ib_arena[k] + bh.dc.plane * a;
       BCUDA(b, cudaMemcpyAsync(b->d_ibtab + 7 * k, t, sizeof(t), cudaMemcpyHostToDevice, b->stream));
     }
-    BCUDA(b, ibm_list_to_device(l, h, b->stream));
+    const cudaError_t le = ibm_list_to_device(l, h, b->stream);
+    if (le != cudaSuccess) {  // no half-uploaded list stays behind
+      ibm_drop_list(l);
+      return bfail(b, CB_E_CUDA, std::string("list upload: ") + cudaGetErrorString(le));
+    }
     if (!had && bh.have_state) {  // P starts as the EqOfState of the current state
       if (block_ptab(b, k)) return CB_E_CUDA;
       eos_plane_kernel<<<bgrid(b, bh.dc.plane), 256, 0, b->stream>>>(
