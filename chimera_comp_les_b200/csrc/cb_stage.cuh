@@ -1236,8 +1236,12 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
     cp_async_wait_all();
     __syncthreads();
     // the faces are done with the metric slot: plane k+1's copies land during
-    // the update and the derive pass
+    // the derive pass and the update
     if (more) issue_met(k + 1);
+    // plane k+H+2 into the slot of plane k-H (the update reads no value of
+    // that plane: rho_km1 above), ahead of the update so that the update's
+    // global operands have the derive pass to arrive
+    if (more) derive(base);
 
     if (uact) {
       const double nv = nvert_v<NV0>(c, F, Rg, n, g);
@@ -1327,7 +1331,6 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
 #pragma unroll
       for (int q = 0; q < NG; q++) Gzp[q] = SMET ? gzr[q] : gzb[(size_t)q * NZF + fz];
     }
-    if (more) derive(base);  // plane k+H+2 into the slot of plane k-H
     base = base + 1 == NPL ? 0 : base + 1;
     if (SMET) cp_async_wait_all();  // the metric slot of plane k+1
     __syncthreads();
