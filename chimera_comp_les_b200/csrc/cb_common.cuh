@@ -110,6 +110,8 @@ __device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc, bool va
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 // brings the line holding p toward this SM's L1 (a hint: nothing is returned)
 __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];\n" ::"l"(p)); }
+// brings the line holding p into L2 (a hint: nothing is returned)
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 __host__ __device__ __forceinline__ long long gidx(const DevCfg &c, int i, int j, int k) {

@@ -1207,6 +1207,23 @@ __device__ __forceinline__ void stage_tile(const DevCfg &c, const DevFields &F, 
         if (LES) prefetch_l1(F.nut + g1);
       }
     }
+    if constexpr (MIX) {
+      // the node update's global operands of this plane, from DRAM into L2
+      // while the faces run
+      if (uact) {
+        const long long gu = gidx(c, ugi, ugj, k);
+        if (!RHS_MODE) {
+#pragma unroll
+          for (int q = 0; q < 5; q++) prefetch_l2(F.qold[q] + gu);
+          if (istage != 0)
+#pragma unroll
+            for (int q = 0; q < 5; q++) prefetch_l2(F.q[q] + gu);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) prefetch_l2(F.gcl[a] + gu);
+        prefetch_l2(F.aj + gu);
+      }
+    }
     plane_faces<R, MIX, LES, VISC, false, FLUX, NV0>(c, F, Rg, i0, j0, k, gxb, gyb, gzb, gzr);
     // the only plane k-1 value the update needs, read before that slot is refilled
     const NRef n{0, uty + 2, utx + 2};
