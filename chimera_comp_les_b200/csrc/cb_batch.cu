@@ -600,8 +600,13 @@ int cb_batch_set_bctype(cb_batch *b, int k, const int *bctype) {
     if (b->xs.nsend || b->xs.nrecv || b->xw.nsend || b->xw.nrecv)
       return bfail(b, CB_E_UNSUPPORTED, "physical face codes with a cross-process exchange are not built");
   }
-  if (!phys && block_ib(b, k))
-    return bfail(b, CB_E_STATE, "a block with immersed-body lists keeps face codes; clear its lists first");
+  if (block_ib(b, k)) {
+    if (!phys) return bfail(b, CB_E_STATE, "a block with immersed-body lists keeps face codes; clear its lists first");
+    // its lists' donors were checked against the periodic directions
+    for (int d = 0; d < 3; d++)
+      if ((bctype[2 * d] == 7) != (b->blk[k].dc.bctype[2 * d] == 7))
+        return bfail(b, CB_E_STATE, "a block with immersed-body lists keeps its periodic directions");
+  }
   BlockHost &bh = b->blk[k];
   if (inflow_xy && !b->coorxy[k]) {
     BCUDA(b, cudaMalloc(&b->coorxy[k], sizeof(double) * 2 * bh.dc.plane));

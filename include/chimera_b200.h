@@ -395,7 +395,8 @@ int cb_batch_set_time_index(cb_batch *b, int ti);
  * _options); each block takes its own list of each body, built as by
  * cb_ibm_set_list from that block's node coordinates.  Lists go only to
  * blocks with face codes (cb_batch_set_bctype; CB_E_UNSUPPORTED otherwise;
- * such a block then keeps its codes, CB_E_STATE).  A block with lists
+ * such a block then keeps face codes and its periodic directions,
+ * CB_E_STATE).  A block with lists
  * advances as a cb_ctx with the same lists; its first stage reads the
  * pressure carried from its interpolation (after an upload: the EqOfState of
  * the state).  A batch with lists refuses the phase API (CB_E_UNSUPPORTED). */

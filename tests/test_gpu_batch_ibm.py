@@ -129,6 +129,9 @@ def test_immersed_list_errors():
         with pytest.raises(ChimeraError) as e:  # a block with a list keeps its codes
             bt.set_bctype(0, (7,) * 6)
         assert e.value.code == CB_E_STATE
+        with pytest.raises(ChimeraError) as e:  # and its periodic directions (the list's donors)
+            bt.set_bctype(0, (3, 3, 7, 7, 45, 45))
+        assert e.value.code == CB_E_STATE
         with pytest.raises(ChimeraError) as e:
             bt.set_ibm_options(0, 1)  # -wallfunction 1 is not built
         assert e.value.code == CB_E_UNSUPPORTED
