@@ -607,6 +607,7 @@ int cb_batch_set_bctype(cb_batch *b, int k, const int *bctype) {
       if ((bctype[2 * d] == 7) != (b->blk[k].dc.bctype[2 * d] == 7))
         return bfail(b, CB_E_STATE, "a block with immersed-body lists keeps its periodic directions");
   }
+  BCUDA(b, cudaStreamSynchronize(b->stream));  // steps in flight read the tables rebuilt below
   BlockHost &bh = b->blk[k];
   if (inflow_xy && !b->coorxy[k]) {
     BCUDA(b, cudaMalloc(&b->coorxy[k], sizeof(double) * 2 * bh.dc.plane));
