@@ -222,6 +222,7 @@ static int bgrid(const cb_batch *b, long long work) {
 }
 
 static void destroy_graphs(cb_batch *b) {
+  if (b->stream) cudaStreamSynchronize(b->stream);  // no graph is destroyed while it runs
   for (auto &m : b->graphs)
     for (auto &r : m)
       for (auto &g : r)
