@@ -220,7 +220,7 @@ class Batch:
                  tref: float = 273.15, twod: int = 0, flux: str = "rusanov", weno_order: int = 3,
                  s_x_min: float = 0.0, s_y_min: float = 0.0, s_z_min: float = 0.0, sigma_thrsh: float = 1e-5,
                  abc: int = 0, max_cs: float = 0.05, i_homo_filter: int = 0, j_homo_filter: int = 0,
-                 k_homo_filter: int = 0, testfilter_ik: int = 0):
+                 k_homo_filter: int = 0, testfilter_ik: int = 0, twall: float = 1.0):
         self.lib = _lib.load()
         self.dims = [tuple(int(x) for x in d) for d in dims]
         cfg = CbConfig()
@@ -232,7 +232,7 @@ class Batch:
                          calc_sigma=calc_sigma, visT=visT, tref=tref, twod=twod, weno_order=weno_order,
                          s_x_min=s_x_min, s_y_min=s_y_min, s_z_min=s_z_min, sigma_thrsh=sigma_thrsh,
                          abc=abc, max_cs=max_cs, i_homo_filter=i_homo_filter, j_homo_filter=j_homo_filter,
-                         k_homo_filter=k_homo_filter, testfilter_ik=testfilter_ik).items():
+                         k_homo_filter=k_homo_filter, testfilter_ik=testfilter_ik, twall=twall).items():
             setattr(cfg, k, v)
         cfg.flux = {"rusanov": 0, "roe": 1}[flux] if isinstance(flux, str) else int(flux)
         cfg.precision = {"fp64": _lib.CB_FP64, "mixed": _lib.CB_MIXED}[precision]

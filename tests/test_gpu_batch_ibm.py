@@ -29,7 +29,7 @@ def _batch_kwargs(cfg):
                 ma=cfg.ma, pr=cfg.pr, gamma=cfg.gamma, dt=cfg.dt, st=cfg.st, cs_const=cfg.cs_const, ci=cfg.ci,
                 ratio=cfg.ratio, calc_sigma=cfg.calc_sigma, s_x_min=cfg.s_x_min, s_y_min=cfg.s_y_min,
                 s_z_min=cfg.s_z_min, sigma_thrsh=cfg.sigma_thrsh, flux=cfg.flux, twod=cfg.twoD, visT=cfg.visT,
-                tref=cfg.tref, abc=cfg.abc, weno_order=cfg.weno_order, max_cs=cfg.max_cs)
+                tref=cfg.tref, abc=cfg.abc, weno_order=cfg.weno_order, max_cs=cfg.max_cs, twall=cfg.twall)
 
 
 def _iface_inputs():
