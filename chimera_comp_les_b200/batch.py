@@ -72,10 +72,15 @@ def _stage_source(gi, gj, gk, M):
     return si, sj, sk, bnd.astype(np.int32)
 
 
-def halo_maps_self_periodic(dims: Sequence[Tuple[int, int, int]]):
-    """Every block periodic on its own: the single-block path, block by block."""
+def halo_maps_self_periodic(dims: Sequence[Tuple[int, int, int]], coded: Sequence[int] = ()):
+    """Every block periodic on its own: the single-block path, block by block.
+    Blocks listed in `coded` (given face codes with Batch.set_bctype, which run
+    their own FormBCS) get no entries, as cb_batch_halo_periodic leaves them."""
     st, wr = [], []
+    skip = set(int(b) for b in coded)
     for b, d in enumerate(dims):
+        if b in skip:
+            continue
         i, j, k, non = _padded_nodes(d)
         i, j, k = i[non], j[non], k[non]
         si, sj, sk, fin = _stage_source(i, j, k, d)

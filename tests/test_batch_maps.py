@@ -82,6 +82,16 @@ def test_self_periodic_matches_scalar_rule():
     B.check_halo_map(dims, wr, B.HALO_WRAP)
 
 
+def test_self_periodic_skips_coded_blocks():
+    """Blocks with face codes run their own FormBCS: the generator leaves them
+    out and keeps every other block's entries unchanged."""
+    dims = [(7, 6, 8), (9, 7, 6), (8, 8, 7)]
+    st, wr = B.halo_maps_self_periodic(dims)
+    st1, wr1 = B.halo_maps_self_periodic(dims, coded=[1])
+    assert not (st1[:, 0] == 1).any() and not (wr1[:, 0] == 1).any()
+    assert np.array_equal(st1, st[st[:, 0] != 1]) and np.array_equal(wr1, wr[wr[:, 0] != 1])
+
+
 def test_decomposed_single_part_equals_self_periodic():
     M = (9, 8, 10)
     parts = B.decompose(M, [[7], [6], [8]])
